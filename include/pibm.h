@@ -1,0 +1,182 @@
+/*
+ * pibm.h -- C ABI of the B200-native PUReIBM-PS2D-FD1D time-step engine.
+ *
+ * The reference has no FFI: its step boundary is the fixed call sequence
+ * inside the driver's rks loop (SRC/FLO/dtibm_main_scal_flo.F90:426-527):
+ *     compute_new_timestep(rks) -> nonlinear(rks) [-> bcset(rks)] -> velstep(sflag,rks)
+ * and every datum moves through module globals (SRC/FLO/global_data.F90:53-338).
+ * This header replaces that boundary with explicit handles.  All arrays that
+ * cross it keep the reference's Fortran layout (column-major, x fastest):
+ *     u, nl  : complex(8) u(nx+1, my2, mz, 3)   (plane nx+1 is the periodic image of plane 1)
+ *     p      : complex(8) p(nx, my2, mz)
+ *     xc, velbdy, pres, visc, force : real(8) (nbody, 3)
+ * complex(8) is passed as interleaved (re, im) doubles.
+ *
+ * Return codes: 0 on success, negative PIBM_ERR_* otherwise (the reference
+ * stops the program instead; see each code).  Calls are synchronous; one host
+ * thread per handle.  Device memory is owned by the handle; host arrays are
+ * only borrowed for the duration of a call.
+ */
+#ifndef PIBM_H
+#define PIBM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes (reference stop conditions they replace). */
+#define PIBM_OK                   0
+#define PIBM_ERR_ARG            (-1)  /* bad argument / unsupported option                         */
+#define PIBM_ERR_BLOWUP         (-2)  /* norm_drag > 1e6: boundary_condition.F90:874-884            */
+#define PIBM_ERR_PIVOT          (-3)  /* zero pivot in Thomas: tridiagonal.F90:62,72-76             */
+#define PIBM_ERR_NAN            (-4)  /* non-finite state detected                                  */
+#define PIBM_ERR_DEM_MOVE       (-5)  /* particle moved >= radius in one DEM sub-step: collision_mod.F90:1421-1428 */
+#define PIBM_ERR_NEIGH_OVERFLOW (-6)  /* neighbour list overflow: collision_mod.F90:845-848          */
+#define PIBM_ERR_TIMEOUT        (-7)  /* a bounded device wait ran out                              */
+#define PIBM_ERR_CUDA           (-8)  /* CUDA runtime error                                         */
+#define PIBM_ERR_NOMEM          (-9)  /* allocation failed                                          */
+
+/* x-flux discretisation (Part_propt DISCR_SCHEME, nl_allflow.F90:98-100,192-207). */
+#define PIBM_SCHEME_CENTER 0
+#define PIBM_SCHEME_UPWIND 1
+/* MUSCL slope limiter (Part_propt LIMITER, nl_allflow.F90:178-207). */
+#define PIBM_LIMITER_NONE   0
+#define PIBM_LIMITER_MINMOD 1
+
+/*
+ * Parsed floparam.in values that define one run (namelists FLOANDGRID,
+ * PART_PROPT, FLAGS; defaults in SRC/FLO/initialize.F90:73-271).
+ * Grid: mx = my+1, nx = mx-1 = my, my2 = my/2+1 (initialize.F90:340-352);
+ * mz = my unless given.  Only the serial x-periodic AB2 path is supported
+ * (PARALLEL=0, XPERIODIC=T, RK3=F, NLCONS=T, AliasFlag=0).
+ */
+typedef struct pibm_params {
+    int32_t my;              /* MY (even)                                      */
+    int32_t mz;              /* MZ (0 -> my)                                   */
+    double  lybyd;           /* LYBYD: box length / diameter                   */
+    double  dbydx;           /* DBYDX: diameter / dx (used by Re<1 dt limit)   */
+    double  dia_phys;        /* DIA_PHYS                                       */
+    double  vis;             /* VIS                                            */
+    double  re;              /* RE                                             */
+    double  cfl;             /* CFL                                            */
+    double  cfl_max;         /* CFL_MAX                                        */
+    double  vfl;             /* VFL                                            */
+    double  dr;              /* DR (reversal-point offset, grid units)         */
+    double  f1, f2;          /* F1, F2 (surface point density)                 */
+    double  flo_ang[3];      /* FLO_ANG (degrees)                              */
+    double  mpg[3];          /* MPG (used when set_mpg)                        */
+    double  rhof, rhos;      /* RHOF, RHOS                                     */
+    double  coeff_rest;      /* COEFF_REST (DEM restitution)                   */
+    int32_t ramp_frac_steps; /* RAMP_FRAC_STEPS (soft start of cf)             */
+    int32_t discr_scheme;    /* PIBM_SCHEME_*                                  */
+    int32_t limiter;         /* PIBM_LIMITER_*                                 */
+    int32_t adaptive;        /* ADAPTIVE                                       */
+    int32_t set_mpg;         /* SET_MPG (or SET_UMEAN)                         */
+    int32_t initialize_zero; /* INITIALIZE_ZERO                                */
+    int32_t dorpr;           /* DORPR                                          */
+    int32_t revernorm;       /* REVERNORM                                      */
+    int32_t include_frmeanfluid; /* INCLUDE_FRMEANFLUID                        */
+    int32_t imove;           /* IMOVE (1 = moving particles, DEM)              */
+    int32_t collision_softsphere; /* COLLISION_TYPE == 'softsphere'            */
+    int32_t iscalon;         /* ISCALON (passive scalar)                       */
+    double  pr_or_sc_nu;     /* PR_OR_SC_NU                                    */
+    double  phisurf;         /* PHISURF                                        */
+    double  phistream;       /* PHISTREAM                                      */
+    int32_t reserved[8];
+} pibm_params;
+
+/* Particle list (the reference's sphr_center.inp after scaling by DBYDX:
+ * initialize_flo.F90:1517-1520).  Positions are in grid units (node i sits at
+ * x = i, i = 1..nx).  velbdy may be NULL (zero velocities). */
+typedef struct pibm_particles {
+    int32_t       nbody;
+    const double *xc;        /* (nbody,3) column-major                        */
+    const double *velbdy;    /* (nbody,3) column-major, or NULL               */
+} pibm_particles;
+
+/* Borrowed view of the evolving state (restart records of
+ * restart_funcs.F90:265-306: t, dt, umean, cf, u, nl, mpg, p). */
+typedef struct pibm_state_view {
+    double *u;               /* complex (nx+1,my2,mz,3) interleaved           */
+    double *nl;              /* complex (nx+1,my2,mz,3) interleaved           */
+    double *p;               /* complex (nx,my2,mz) interleaved               */
+    double  umean[3];
+    double  mpg[3];
+    double  ufmean[3];       /* previous-step fluid mean (for dufmeandt)      */
+    double  t, dt, cf;
+} pibm_state_view;
+
+/* Per-step diagnostics (what the reference prints each step). */
+typedef struct pibm_step_report {
+    double dt, t, cf;
+    double umax;             /* max |u| used for the CFL check                */
+    double divmax;           /* check_divergence, steptheflow.F90:219-240     */
+    double ufmean[3], usmean[3], umean[3];
+    double mpg[3], frmean[3];
+    double pres_total[3], visc_total[3];
+    double norm_drag, ferror;
+    double pres_drag, visc_drag, total_drag;
+    double mixmeanslipmod;
+    int64_t nrpr_active_total;
+} pibm_step_report;
+
+/* Static description of a handle's grid and geometry. */
+typedef struct pibm_info {
+    int32_t nx, my, mz, my2, nbody, nbnd;
+    double  dx, dt, radbdy, maxvolfrac;
+    int64_t count_solid, count_fluid;
+} pibm_info;
+
+typedef struct pibm_handle pibm_handle;
+
+/* initflo (initialize_flo.F90:61-1013) for input_type='default':
+ * grid, wavenumbers, AB2 coefficients, surface points (quadgener,
+ * geom_init.F90:44-242), solid mask (grid_nodes_insphere,
+ * dependent_functions.F90:783-963), DEM neighbour search
+ * (collision_mod.F90:807-1062) and active reversal points
+ * (update_nrpr_array, dependent_functions.F90:966-1051), initial dt. */
+int  pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle **out);
+int  pibm_info_get(pibm_handle *h, pibm_info *info);
+/* Copy a state in (reference layout); the real-space AB2 history is rebuilt. */
+int  pibm_set_state(pibm_handle *h, const pibm_state_view *s);
+/* One rks iteration of the driver loop (dtibm_main_scal_flo.F90:426-527):
+ * compute_new_timestep(rks) -> nonlinear(rks) -> bcset(rks) -> velstep(rks). */
+int  pibm_step(pibm_handle *h, int rks, pibm_step_report *rep);
+/* nsteps steps without per-step host synchronisation (graph-launched). */
+int  pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last);
+int  pibm_get_state(pibm_handle *h, pibm_state_view *s);
+/* pres, visc, force: (nbody,3) column-major, as global_data.F90:115-117;
+ * xc, vel: positions (grid units) and velocities.  Any pointer may be NULL. */
+int  pibm_get_particles(pibm_handle *h, double *pres, double *visc, double *force,
+                        double *xc, double *vel);
+/* Active reversal-point flags (part_array(m)%if_rev), (nbnd, nbody) column-major. */
+int  pibm_get_if_rev(pibm_handle *h, uint8_t *if_rev);
+/* Solid mask fluid_atijk(1:nx,1:my,1:mz) as 0/1 bytes, x fastest. */
+int  pibm_get_fluid_mask(pibm_handle *h, uint8_t *mask);
+void pibm_destroy(pibm_handle *h);
+const char *pibm_last_error(void);
+
+/* ---- plane transforms (the reference's ff2rc / ff2cr,
+ *      fftw_interface.F90:48-133), batched over nplanes planes ----
+ * ff2rc: real (my,mz) -> complex (my2,mz), forward e^{-i}, scaled 1/(my*mz).
+ * ff2cr: complex (my2,mz) -> real (my,mz), inverse e^{+i}, unscaled; the
+ *        imaginary parts of the ky=0 and ky=Nyquist columns are ignored after
+ *        the z transform (FFTW / numpy irfft2 semantics).
+ * Host pointers; y fastest within a plane, planes contiguous. */
+int  pibm_ff2rc(int my, int mz, int nplanes, const double *a, double *b);
+int  pibm_ff2cr(int my, int mz, int nplanes, const double *a, double *b);
+
+/* ---- batched independent realizations (the MIS ensemble of
+ *      sample_inputs/set_mis_3d, run as one graph-captured launch stream) ---- */
+typedef struct pibm_batch pibm_batch;
+int  pibm_batch_create(int n, const pibm_params *prm, const pibm_particles *parts, pibm_batch **out);
+int  pibm_batch_run(pibm_batch *b, int nsteps);
+pibm_handle *pibm_batch_member(pibm_batch *b, int i);
+void pibm_batch_destroy(pibm_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PIBM_H */

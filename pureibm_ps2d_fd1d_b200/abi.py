@@ -1,0 +1,135 @@
+"""ctypes mirror of include/pibm.h (the engine's C ABI).
+
+Every structure here has the same field order and types as the header; the
+tests check the sizes against the compiled library.
+"""
+import ctypes as C
+
+PIBM_OK = 0
+PIBM_ERR_ARG = -1
+PIBM_ERR_BLOWUP = -2
+PIBM_ERR_PIVOT = -3
+PIBM_ERR_NAN = -4
+PIBM_ERR_DEM_MOVE = -5
+PIBM_ERR_NEIGH_OVERFLOW = -6
+PIBM_ERR_TIMEOUT = -7
+PIBM_ERR_CUDA = -8
+PIBM_ERR_NOMEM = -9
+
+ERROR_NAMES = {
+    PIBM_ERR_ARG: "PIBM_ERR_ARG",
+    PIBM_ERR_BLOWUP: "PIBM_ERR_BLOWUP",
+    PIBM_ERR_PIVOT: "PIBM_ERR_PIVOT",
+    PIBM_ERR_NAN: "PIBM_ERR_NAN",
+    PIBM_ERR_DEM_MOVE: "PIBM_ERR_DEM_MOVE",
+    PIBM_ERR_NEIGH_OVERFLOW: "PIBM_ERR_NEIGH_OVERFLOW",
+    PIBM_ERR_TIMEOUT: "PIBM_ERR_TIMEOUT",
+    PIBM_ERR_CUDA: "PIBM_ERR_CUDA",
+    PIBM_ERR_NOMEM: "PIBM_ERR_NOMEM",
+}
+
+PIBM_SCHEME_CENTER = 0
+PIBM_SCHEME_UPWIND = 1
+PIBM_LIMITER_NONE = 0
+PIBM_LIMITER_MINMOD = 1
+
+_i32 = C.c_int32
+_f64 = C.c_double
+
+
+class pibm_params(C.Structure):
+    _fields_ = [
+        ("my", _i32), ("mz", _i32),
+        ("lybyd", _f64), ("dbydx", _f64), ("dia_phys", _f64),
+        ("vis", _f64), ("re", _f64), ("cfl", _f64), ("cfl_max", _f64), ("vfl", _f64),
+        ("dr", _f64), ("f1", _f64), ("f2", _f64),
+        ("flo_ang", _f64 * 3), ("mpg", _f64 * 3),
+        ("rhof", _f64), ("rhos", _f64), ("coeff_rest", _f64),
+        ("ramp_frac_steps", _i32), ("discr_scheme", _i32), ("limiter", _i32),
+        ("adaptive", _i32), ("set_mpg", _i32), ("initialize_zero", _i32),
+        ("dorpr", _i32), ("revernorm", _i32), ("include_frmeanfluid", _i32),
+        ("imove", _i32), ("collision_softsphere", _i32), ("iscalon", _i32),
+        ("pr_or_sc_nu", _f64), ("phisurf", _f64), ("phistream", _f64),
+        ("reserved", _i32 * 8),
+    ]
+
+
+class pibm_particles(C.Structure):
+    _fields_ = [("nbody", _i32), ("xc", C.POINTER(_f64)), ("velbdy", C.POINTER(_f64))]
+
+
+class pibm_state_view(C.Structure):
+    _fields_ = [
+        ("u", C.POINTER(_f64)), ("nl", C.POINTER(_f64)), ("p", C.POINTER(_f64)),
+        ("umean", _f64 * 3), ("mpg", _f64 * 3), ("ufmean", _f64 * 3),
+        ("t", _f64), ("dt", _f64), ("cf", _f64),
+    ]
+
+
+class pibm_step_report(C.Structure):
+    _fields_ = [
+        ("dt", _f64), ("t", _f64), ("cf", _f64), ("umax", _f64), ("divmax", _f64),
+        ("ufmean", _f64 * 3), ("usmean", _f64 * 3), ("umean", _f64 * 3),
+        ("mpg", _f64 * 3), ("frmean", _f64 * 3),
+        ("pres_total", _f64 * 3), ("visc_total", _f64 * 3),
+        ("norm_drag", _f64), ("ferror", _f64),
+        ("pres_drag", _f64), ("visc_drag", _f64), ("total_drag", _f64),
+        ("mixmeanslipmod", _f64),
+        ("nrpr_active_total", C.c_int64),
+    ]
+
+    def as_dict(self):
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+class pibm_info(C.Structure):
+    _fields_ = [
+        ("nx", _i32), ("my", _i32), ("mz", _i32), ("my2", _i32), ("nbody", _i32), ("nbnd", _i32),
+        ("dx", _f64), ("dt", _f64), ("radbdy", _f64), ("maxvolfrac", _f64),
+        ("count_solid", C.c_int64), ("count_fluid", C.c_int64),
+    ]
+
+
+# Exported symbols of libpibm (declared in include/pibm.h).
+EXPORTED = [
+    "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run",
+    "pibm_get_state", "pibm_get_particles", "pibm_get_if_rev", "pibm_get_fluid_mask",
+    "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
+    "pibm_batch_create", "pibm_batch_run", "pibm_batch_member", "pibm_batch_destroy",
+]
+
+
+def bind(lib):
+    """Attach argtypes/restypes for the pibm_* entry points."""
+    P = C.POINTER
+    vp = C.c_void_p
+    lib.pibm_create.argtypes = [P(pibm_params), P(pibm_particles), P(vp)]
+    lib.pibm_info_get.argtypes = [vp, P(pibm_info)]
+    lib.pibm_set_state.argtypes = [vp, P(pibm_state_view)]
+    lib.pibm_step.argtypes = [vp, C.c_int, P(pibm_step_report)]
+    lib.pibm_run.argtypes = [vp, C.c_int, P(pibm_step_report)]
+    lib.pibm_get_state.argtypes = [vp, P(pibm_state_view)]
+    lib.pibm_get_particles.argtypes = [vp] + [P(_f64)] * 5
+    lib.pibm_get_if_rev.argtypes = [vp, P(C.c_uint8)]
+    lib.pibm_get_fluid_mask.argtypes = [vp, P(C.c_uint8)]
+    lib.pibm_destroy.argtypes = [vp]
+    lib.pibm_destroy.restype = None
+    lib.pibm_last_error.argtypes = []
+    lib.pibm_last_error.restype = C.c_char_p
+    for fn in (lib.pibm_ff2rc, lib.pibm_ff2cr):
+        fn.argtypes = [C.c_int, C.c_int, C.c_int, P(_f64), P(_f64)]
+    lib.pibm_batch_create.argtypes = [C.c_int, P(pibm_params), P(pibm_particles), P(vp)]
+    lib.pibm_batch_run.argtypes = [vp, C.c_int]
+    lib.pibm_batch_member.argtypes = [vp, C.c_int]
+    lib.pibm_batch_member.restype = vp
+    lib.pibm_batch_destroy.argtypes = [vp]
+    lib.pibm_batch_destroy.restype = None
+    for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run",
+                 "pibm_get_state", "pibm_get_particles", "pibm_get_if_rev", "pibm_get_fluid_mask",
+                 "pibm_ff2rc", "pibm_ff2cr", "pibm_batch_create", "pibm_batch_run"):
+        getattr(lib, name).restype = C.c_int
+    return lib

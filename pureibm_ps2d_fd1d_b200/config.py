@@ -1,0 +1,242 @@
+"""Run configuration: the reference's input files and the seeded workloads.
+
+* ``default_params`` restates ``set_default`` (SRC/FLO/initialize.F90:73-271)
+  for the keys the step uses.
+* ``read_floparam`` reads a ``RUN_NAME_floparam.in`` (Fortran namelists
+  FLOANDGRID, PART_PROPT, FLAGS, ... read in ``read_nmls``,
+  initialize.F90:274-359) into the same dictionary.
+* ``read_sphr_center`` reads ``RUN_NAME_sphr_center.inp`` like the
+  ``input_type='default'`` branch (initialize_flo.F90:1485-1590): line 1 is
+  skipped, columns are x y z r in diameters, positions are scaled by DBYDX and
+  the radius column is ignored.  The reference's first pass over that file
+  never increments ``nbody`` (initialize_flo.F90:1494-1503), so the reference
+  itself loads no sphere from it; this reader returns every row.
+* ``single_sphere`` / ``random_array`` / ``moving_suspension`` build the
+  seeded synthetic workloads (fixed sphere at the box centre; random
+  sequential addition followed by hard-sphere Monte Carlo moves).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from typing import Dict, Optional
+
+import numpy as np
+
+from .abi import pibm_params, pibm_particles, PIBM_SCHEME_CENTER, PIBM_SCHEME_UPWIND, \
+    PIBM_LIMITER_NONE, PIBM_LIMITER_MINMOD
+
+
+def default_params() -> Dict:
+    """Reference defaults (initialize.F90:73-271) for the keys the step reads."""
+    return dict(
+        my=0, mz=0, lybyd=None, dbydx=None, dia_phys=1.0,
+        vis=0.012, re=100.0, cfl=0.5, cfl_max=None, vfl=1.0,
+        dr=1.0, f1=1.6, f2=1.6, flo_ang=(0.0, 90.0, 90.0), mpg=(0.0, 0.0, 0.0),
+        rhof=1.0, rhos=1.0, coeff_rest=1.0, ramp_frac_steps=20,
+        discr_scheme="center", limiter="none",
+        adaptive=True, set_mpg=False, set_umean=False, initialize_zero=False,
+        dorpr=True, revernorm=1, include_frmeanfluid=False,
+        imove=0, collision_type="none", iscalon=0,
+        pr_or_sc_nu=0.7, phisurf=0.0, phistream=1.0,
+        rk3=False, xperiodic=True, nlcons=True, aliasflag=0, dobnd=True,
+        input_type="default",
+    )
+
+
+_BOOL = {".true.": True, "t": True, ".t.": True, "true": True,
+         ".false.": False, "f": False, ".f.": False, "false": False}
+
+
+def _parse_value(tok: str):
+    tok = tok.strip().rstrip(",").strip()
+    if not tok:
+        return None
+    if tok[0] in "'\"":
+        return tok.strip("'\"")
+    low = tok.lower()
+    if low in _BOOL:
+        return _BOOL[low]
+    parts = [p for p in re.split(r"[,\s]+", tok) if p]
+    vals = []
+    for p in parts:
+        pl = p.lower()
+        if pl in _BOOL:
+            vals.append(_BOOL[pl])
+            continue
+        try:
+            if re.fullmatch(r"[+-]?\d+", p):
+                vals.append(int(p))
+            else:
+                vals.append(float(pl.replace("d", "e")))
+        except ValueError:
+            vals.append(p)
+    return vals[0] if len(vals) == 1 else tuple(vals)
+
+
+def read_floparam(path: str) -> Dict:
+    """Parse the namelist groups of a floparam.in into a parameter dict.
+
+    Group order and unknown keys are not enforced here (the reference aborts
+    on an unknown key); keys are matched case-insensitively.
+    """
+    prm = default_params()
+    text = open(path).read()
+    groups = re.findall(r"&(\w+)(.*?)(?:^\s*/\s*$)", text, flags=re.S | re.M)
+    for _, body in groups:
+        # split "KEY = value" pairs; values may span commas / several numbers
+        for m in re.finditer(r"(\w+)\s*=\s*(.*?)(?=\s+\w+\s*=|\Z)", body, flags=re.S):
+            key = m.group(1).lower()
+            val = _parse_value(m.group(2).replace("\n", " "))
+            prm[key] = val
+    if prm.get("set_umean"):
+        prm["set_mpg"] = True
+    return prm
+
+
+def read_sphr_center(path: str, dbydx: float) -> np.ndarray:
+    """Sphere centres (nbody,3) in grid units from a sphr_center.inp file."""
+    rows = []
+    with open(path) as fh:
+        next(fh)
+        for line in fh:
+            f = line.split()
+            if len(f) >= 3:
+                rows.append([float(v.replace("d", "e").replace("D", "e")) for v in f[:3]])
+    return np.asarray(rows, dtype=np.float64).reshape(-1, 3) * float(dbydx)
+
+
+def write_sphr_center(path: str, xc_grid: np.ndarray, dbydx: float, radius_diam: float = 0.5):
+    """Write centres (grid units) in the reference's sphr_center.inp format."""
+    with open(path, "w") as fh:
+        fh.write(" generated\n")
+        for i, row in enumerate(np.asarray(xc_grid) / dbydx):
+            fh.write("  %.10f  %.10f  %.10f  %.10f  %d\n" % (row[0], row[1], row[2], radius_diam, i + 1))
+
+
+def make_params(prm: Dict) -> pibm_params:
+    """Fill a pibm_params struct from a parameter dict."""
+    p = pibm_params()
+    my = int(prm["my"])
+    p.my = my
+    p.mz = int(prm.get("mz") or my)
+    p.lybyd = float(prm["lybyd"])
+    p.dbydx = float(prm["dbydx"] if prm.get("dbydx") is not None else my / float(prm["lybyd"]))
+    p.dia_phys = float(prm.get("dia_phys", 1.0))
+    p.vis = float(prm["vis"])
+    p.re = float(prm["re"])
+    p.cfl = float(prm["cfl"])
+    p.cfl_max = float(prm["cfl_max"] if prm.get("cfl_max") is not None else prm["cfl"])
+    p.vfl = float(prm.get("vfl", 1.0))
+    p.dr = float(prm.get("dr", 1.0))
+    p.f1 = float(prm.get("f1", 1.6))
+    p.f2 = float(prm.get("f2", 1.6))
+    for d in range(3):
+        p.flo_ang[d] = float(prm["flo_ang"][d])
+        p.mpg[d] = float(prm["mpg"][d]) if isinstance(prm["mpg"], (tuple, list)) else float(prm["mpg"])
+    p.rhof = float(prm.get("rhof", 1.0))
+    p.rhos = float(prm.get("rhos", 1.0))
+    p.coeff_rest = float(prm.get("coeff_rest", 1.0))
+    p.ramp_frac_steps = int(prm.get("ramp_frac_steps", 20))
+    sch = str(prm.get("discr_scheme", "center")).strip().lower()
+    if sch not in ("center", "upwind"):
+        raise ValueError("DISCR_SCHEME must be 'center' or 'upwind'")
+    p.discr_scheme = PIBM_SCHEME_UPWIND if sch == "upwind" else PIBM_SCHEME_CENTER
+    p.limiter = PIBM_LIMITER_MINMOD if str(prm.get("limiter", "none")).lower() == "minmod" else PIBM_LIMITER_NONE
+    p.adaptive = int(bool(prm.get("adaptive", True)))
+    p.set_mpg = int(bool(prm.get("set_mpg", False)))
+    p.initialize_zero = int(bool(prm.get("initialize_zero", False)))
+    p.dorpr = int(bool(prm.get("dorpr", True)))
+    p.revernorm = int(prm.get("revernorm", 1))
+    p.include_frmeanfluid = int(bool(prm.get("include_frmeanfluid", False)))
+    p.imove = int(prm.get("imove", 0))
+    p.collision_softsphere = int(str(prm.get("collision_type", "none")).lower() == "softsphere")
+    p.iscalon = int(prm.get("iscalon", 0))
+    p.pr_or_sc_nu = float(prm.get("pr_or_sc_nu", 0.7))
+    p.phisurf = float(prm.get("phisurf", 0.0))
+    p.phistream = float(prm.get("phistream", 1.0))
+    if prm.get("rk3"):
+        raise ValueError("RK3=T is not supported by this engine (AB2 only)")
+    if not prm.get("xperiodic", True):
+        raise ValueError("XPERIODIC=F is not supported (x-periodic only)")
+    return p
+
+
+class Particles:
+    """Owns the arrays behind a pibm_particles struct (Fortran (nbody,3) layout)."""
+
+    def __init__(self, xc: np.ndarray, vel: Optional[np.ndarray] = None):
+        xc = np.asarray(xc, dtype=np.float64).reshape(-1, 3)
+        self.nbody = xc.shape[0]
+        self.xc_f = np.asfortranarray(xc).ravel(order="F").copy()
+        self.vel_f = None if vel is None else np.asfortranarray(np.asarray(vel, np.float64).reshape(-1, 3)).ravel(order="F").copy()
+        self.struct = pibm_particles()
+        self.struct.nbody = self.nbody
+        self.struct.xc = self.xc_f.ctypes.data_as(C.POINTER(C.c_double)) if self.nbody else None
+        self.struct.velbdy = self.vel_f.ctypes.data_as(C.POINTER(C.c_double)) if self.vel_f is not None else None
+
+
+# --------------------------------------------------------------------------
+# Seeded synthetic workloads
+# --------------------------------------------------------------------------
+
+def _min_image(d, L):
+    return d - L * np.round(d / L)
+
+
+def random_sequential_addition(n: int, L: float, dia: float, rng, origin=1.0, max_tries=2_000_000):
+    """n non-overlapping spheres (centres in [origin, origin+L)^3, periodic)."""
+    pts = np.zeros((0, 3))
+    tries = 0
+    while pts.shape[0] < n:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError("random sequential addition did not converge")
+        c = origin + rng.random(3) * L
+        if pts.shape[0]:
+            d = _min_image(pts - c, L)
+            if np.min(np.einsum("ij,ij->i", d, d)) < dia * dia:
+                continue
+        pts = np.vstack([pts, c])
+    return pts
+
+
+def hard_sphere_mc(pts: np.ndarray, L: float, dia: float, rng, moves: int, step: float, origin=1.0):
+    """Seeded hard-sphere Monte Carlo displacement moves (periodic box)."""
+    pts = pts.copy()
+    n = pts.shape[0]
+    acc = 0
+    for _ in range(moves):
+        i = rng.integers(n)
+        trial = pts[i] + (rng.random(3) * 2.0 - 1.0) * step
+        trial = origin + np.mod(trial - origin, L)
+        d = _min_image(np.delete(pts, i, axis=0) - trial, L)
+        if n == 1 or np.min(np.einsum("ij,ij->i", d, d)) >= dia * dia:
+            pts[i] = trial
+            acc += 1
+    return pts, acc
+
+
+def single_sphere(my: int = 64, dia_cells: float = 16.0, re: float = 20.0, vis: float = 0.012,
+                  cfl: float = 0.1, steps: int = 100):
+    """One fixed sphere at the box centre, fluid at rest, mpg-driven flow."""
+    prm = default_params()
+    prm.update(my=my, lybyd=my / dia_cells, dbydx=dia_cells, re=re, vis=vis, cfl=cfl, cfl_max=0.5,
+               discr_scheme="upwind", initialize_zero=True, dobnd=False, ramp_frac_steps=0)
+    xc = np.array([[1.0 + my / 2.0, 1.0 + my / 2.0, 1.0 + my / 2.0]])
+    return prm, xc
+
+
+def random_array(my: int = 128, dia_cells: float = 20.0, phi: float = 0.2, re: float = 50.0,
+                 seed: int = 1234, mc_moves: int = 1000, vis: float = 0.012, cfl: float = 0.1,
+                 nbody: Optional[int] = None):
+    """Fixed random sphere array: RSA then hard-sphere MC (step 0.1 d)."""
+    prm = default_params()
+    prm.update(my=my, lybyd=my / dia_cells, dbydx=dia_cells, re=re, vis=vis, cfl=cfl, cfl_max=0.5,
+               discr_scheme="upwind", initialize_zero=True, dobnd=False, ramp_frac_steps=0)
+    if nbody is None:
+        nbody = int(round(phi * my ** 3 / (np.pi / 6.0 * dia_cells ** 3)))
+    rng = np.random.default_rng(seed)
+    pts = random_sequential_addition(nbody, float(my), dia_cells, rng)
+    pts, _ = hard_sphere_mc(pts, float(my), dia_cells, rng, mc_moves, 0.1 * dia_cells)
+    return prm, pts
