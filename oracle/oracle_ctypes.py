@@ -51,6 +51,8 @@ def lib():
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_set_threads.restype = None
         L.orc_last_error.restype = C.c_char_p
+        L.orc_sizeof.argtypes = [C.c_int]
+        L.orc_sizeof.restype = C.c_int
         _lib = L
     return _lib
 

@@ -1315,3 +1315,15 @@ int orc_cyclic_solve(int n, const double *a, const double *b, const double *c, c
 }
 
 }  // extern "C"
+
+// sizes of the ABI structs as compiled from include/pibm.h (for the ctypes mirror test)
+extern "C" int orc_sizeof(int which) {
+    switch (which) {
+        case 0: return (int)sizeof(pibm_params);
+        case 1: return (int)sizeof(pibm_particles);
+        case 2: return (int)sizeof(pibm_state_view);
+        case 3: return (int)sizeof(pibm_step_report);
+        case 4: return (int)sizeof(pibm_info);
+        default: return -1;
+    }
+}

@@ -1,1 +1,153 @@
-"""B200-native PUReIBM-PS2D-FD1D time-step engine (host side)."""
+"""B200-native PUReIBM-PS2D-FD1D time-step engine (host side).
+
+The engine itself is ``_lib/libpibm.so`` (CUDA, sm_100a), reached through the
+C ABI of ``include/pibm.h``.  This package is the host-side mirror of the
+reference's step boundary: ``Solver.step()`` is one iteration of the driver's
+rks loop (SRC/FLO/dtibm_main_scal_flo.F90:426-527), i.e. compute_new_timestep
+-> nonlinear -> bcset -> velstep, executed on the GPU.  There is no CPU
+fallback: if the library cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from .abi import pibm_params, pibm_state_view, pibm_step_report, pibm_info
+from . import config
+
+__all__ = ["Solver", "load_library", "ff2rc", "ff2cr", "config", "abi", "PibmError"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libpibm.so")
+_lib = None
+
+
+class PibmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("%s (%d): %s" % (abi.ERROR_NAMES.get(code, "PIBM_ERR"), code, msg))
+        self.code = code
+
+
+def load_library():
+    """Load the in-tree CUDA engine; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libpibm.so not built (run python -m pureibm_ps2d_fd1d_b200.build): " + LIB_PATH)
+        _lib = abi.bind(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise PibmError(rc, load_library().pibm_last_error().decode())
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def ff2rc(a: np.ndarray) -> np.ndarray:
+    """Reference ff2rc on the GPU: real (nplanes, mz, my) -> complex (nplanes, mz, my/2+1)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    npl, mz, my = a.shape
+    b = np.zeros((npl, mz, my // 2 + 1), dtype=np.complex128)
+    _check(load_library().pibm_ff2rc(my, mz, npl, _dp(a), b.ctypes.data_as(C.POINTER(C.c_double))))
+    return b
+
+
+def ff2cr(a: np.ndarray, my: int) -> np.ndarray:
+    """Reference ff2cr on the GPU: complex (nplanes, mz, my/2+1) -> real (nplanes, mz, my)."""
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    npl, mz, _ = a.shape
+    b = np.zeros((npl, mz, my), dtype=np.float64)
+    _check(load_library().pibm_ff2cr(my, mz, npl, a.ctypes.data_as(C.POINTER(C.c_double)), _dp(b)))
+    return b
+
+
+class Solver:
+    """One run on the current CUDA device (one handle of the C ABI)."""
+
+    def __init__(self, params, xc: Optional[np.ndarray] = None, vel: Optional[np.ndarray] = None):
+        lib = load_library()
+        self.params = params if isinstance(params, pibm_params) else config.make_params(params)
+        self.particles = config.Particles(np.zeros((0, 3)) if xc is None else xc, vel)
+        h = C.c_void_p()
+        _check(lib.pibm_create(C.byref(self.params), C.byref(self.particles.struct), C.byref(h)))
+        self.h = h
+        info = pibm_info()
+        _check(lib.pibm_info_get(self.h, C.byref(info)))
+        self.info = info
+        self.nx, self.my, self.mz, self.my2 = info.nx, info.my, info.mz, info.my2
+        self.nbody, self.nbnd = info.nbody, info.nbnd
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().pibm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the step boundary ----------------------------------------------------
+    def step(self, rks: int = 1) -> dict:
+        """compute_new_timestep -> nonlinear -> bcset -> velstep (one rks iteration)."""
+        rep = pibm_step_report()
+        _check(load_library().pibm_step(self.h, rks, C.byref(rep)))
+        return rep.as_dict()
+
+    def run(self, nsteps: int) -> dict:
+        """nsteps steps replayed from CUDA graphs, diagnostics of the last one."""
+        rep = pibm_step_report()
+        _check(load_library().pibm_run(self.h, int(nsteps), C.byref(rep)))
+        return rep.as_dict()
+
+    # -- state in the reference layout -------------------------------------------
+    def get_state(self) -> dict:
+        nx, my2, mz = self.nx, self.my2, self.mz
+        u = np.zeros((3, mz, my2, nx + 1), dtype=np.complex128)
+        nl = np.zeros_like(u)
+        p = np.zeros((mz, my2, nx), dtype=np.complex128)
+        s = pibm_state_view()
+        s.u, s.nl, s.p = (a.ctypes.data_as(C.POINTER(C.c_double)) for a in (u, nl, p))
+        _check(load_library().pibm_get_state(self.h, C.byref(s)))
+        return dict(u=u, nl=nl, p=p, umean=np.array(s.umean[:]), mpg=np.array(s.mpg[:]),
+                    ufmean=np.array(s.ufmean[:]), t=s.t, dt=s.dt, cf=s.cf)
+
+    def set_state(self, st: dict):
+        s = pibm_state_view()
+        keep = []
+        for name in ("u", "nl", "p"):
+            if st.get(name) is not None:
+                a = np.ascontiguousarray(st[name], dtype=np.complex128)
+                keep.append(a)
+                setattr(s, name, a.ctypes.data_as(C.POINTER(C.c_double)))
+        for d in range(3):
+            s.umean[d] = st["umean"][d]; s.mpg[d] = st["mpg"][d]; s.ufmean[d] = st.get("ufmean", np.zeros(3))[d]
+        s.t, s.dt, s.cf = st["t"], st["dt"], st["cf"]
+        _check(load_library().pibm_set_state(self.h, C.byref(s)))
+
+    def get_particles(self):
+        """pres, visc, force, xc, vel as (nbody, 3) arrays."""
+        n = self.nbody
+        out = [np.zeros(3 * n) for _ in range(5)]
+        _check(load_library().pibm_get_particles(self.h, *[_dp(a) for a in out]))
+        return [a.reshape(3, n).T.copy() for a in out]
+
+    def get_if_rev(self) -> np.ndarray:
+        out = np.zeros(self.nbnd * self.nbody, dtype=np.uint8)
+        _check(load_library().pibm_get_if_rev(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return out.reshape(self.nbody, self.nbnd)
+
+    def get_fluid_mask(self) -> np.ndarray:
+        out = np.zeros(self.nx * self.my * self.mz, dtype=np.uint8)
+        _check(load_library().pibm_get_fluid_mask(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return out.reshape(self.mz, self.my, self.nx)

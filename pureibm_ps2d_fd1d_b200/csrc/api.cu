@@ -1,0 +1,398 @@
+// api.cu -- the pibm_* C ABI (include/pibm.h) on top of the sm_100a kernels.
+//
+// A handle owns: the device copy of the run geometry, every field of the
+// step, one stream, and two CUDA graphs of one step each (the nonlinear-term
+// buffers alternate between steps, so even and odd steps differ only in which
+// buffer is "current").  pibm_run replays the graphs without host
+// synchronisation; pibm_step launches one step and reads the diagnostics.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pibm.h"
+#include "engine.cuh"
+#include "host_setup.h"
+
+namespace pibm {
+cudaError_t configure_kernels(int n);
+bool supported_size(int n);
+void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s);
+void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s);
+void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s);
+void enqueue_f2d(const double2 *f, double2 *d, int nx, int nxf, int PS, int ncomp, cudaStream_t s);
+void enqueue_d2f(const double2 *d, double2 *f, int nx, int nxf, int PS, int ncomp, cudaStream_t s);
+}  // namespace pibm
+
+using namespace pibm;
+
+namespace {
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+#define CUDA_OR_FAIL(expr)                                                                  \
+    do {                                                                                    \
+        cudaError_t _e = (expr);                                                            \
+        if (_e != cudaSuccess) return fail(PIBM_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+// e^{-2 pi i m/n} in extended precision, rounded to double.
+std::vector<double2> twiddles(int n) {
+    std::vector<double2> t(n);
+    for (int m = 0; m < n; ++m) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
+        t[m] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    return t;
+}
+}  // namespace
+
+struct pibm_handle {
+    RunSetup S;
+    pibm_params prm;
+    Geo g;
+    DevBufs b;
+    std::vector<void *> allocs;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int cur = 0;          // buffer index the next step writes its nonlinear term to
+    int device = 0;
+
+    template <class T> cudaError_t alloc(T **p, size_t n) {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, n * sizeof(T) > 0 ? n * sizeof(T) : 16);
+        if (e == cudaSuccess) { allocs.push_back(q); cudaMemset(q, 0, n * sizeof(T) > 0 ? n * sizeof(T) : 16); }
+        *p = (T *)q;
+        return e;
+    }
+    template <class T> cudaError_t upload(const T **p, const std::vector<T> &v) {
+        T *q = nullptr;
+        cudaError_t e = alloc(&q, v.size());
+        if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(q, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+        *p = q;
+        return e;
+    }
+    ~pibm_handle() {
+        for (auto &gx : graph) if (gx) cudaGraphExecDestroy(gx);
+        if (stream) cudaStreamDestroy(stream);
+        for (void *q : allocs) cudaFree(q);
+    }
+};
+
+extern "C" {
+
+const char *pibm_last_error(void) { return g_last_error.c_str(); }
+
+int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle **out) {
+    if (!prm || !out) return fail(PIBM_ERR_ARG, "null argument");
+    *out = nullptr;
+    pibm_handle *h = new pibm_handle();
+    h->prm = *prm;
+    std::string err;
+    if (!setup_run(*prm, parts, h->S, err)) { delete h; return fail(PIBM_ERR_ARG, err); }
+    RunSetup &S = h->S;
+    if (!supported_size(S.my)) { delete h; return fail(PIBM_ERR_ARG, "MY must be one of 32, 64, 96, 128"); }
+    int rc;
+    auto guard = [&](cudaError_t e, const char *what) -> bool {
+        if (e != cudaSuccess) { rc = fail(PIBM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)); return false; }
+        return true;
+    };
+    if (!guard(cudaGetDevice(&h->device), "cudaGetDevice") || !guard(configure_kernels(S.my), "configure_kernels") ||
+        !guard(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate")) { delete h; return rc; }
+    Geo &g = h->g;
+    std::memset(&g, 0, sizeof(g));
+    g.nx = S.nx; g.my = S.my; g.mz = S.mz; g.my2 = S.my2;
+    g.PS = S.my2 * S.mz; g.RS = S.my * S.mz;
+    g.dx = S.dx; g.dx2 = S.dx2; g.rdx2 = 1.0 / S.dx2; g.dx3 = S.dx3; g.vis = S.vis;
+    g.nrm = (double)(float)(S.my * S.mz);
+    g.c1 = S.coef[0]; g.c2 = S.coef[1]; g.c3 = S.coef[2]; g.c4 = S.coef[3];
+    g.scheme = prm->discr_scheme; g.limiter = prm->limiter;
+    g.include_frmeanfluid = prm->include_frmeanfluid; g.revernorm = prm->revernorm;
+    g.set_mpg = prm->set_mpg; g.adaptive = prm->adaptive;
+    g.cfl_max = prm->cfl_max; g.ramp_frac_time = S.ramp_frac_time; g.ucharmod = S.ucharmod;
+    g.char_length = S.char_length; g.voldom = S.voldom; g.maxvolfrac = S.maxvolfrac; g.mean_volfrac = S.mean_volfrac;
+    g.count_fluid = S.count_fluid; g.ncell = (long long)S.nx * S.my * S.mz;
+    for (int d = 0; d < 3; ++d) { g.ufmean_des[d] = S.ufmean_des[d]; g.usmean_des[d] = S.usmean_des[d]; g.usmean_act[d] = S.usmean_des[d]; }
+    g.nbody = S.nbody; g.nbnd = S.nbnd; g.npts = (int)S.pt_m.size();
+    g.rb = S.radbdy; g.ri = S.radibdy; g.ro = S.radobdy; g.dr = S.dr;
+    g.da1 = 4.0 * 3.14159265358979323846 * ((S.radbdy * S.dx) * (S.radbdy * S.dx)) / (double)S.nbnd;
+    g.sphere_vol = 3.14159265358979323846 * std::pow(2.0 * S.radbdy * S.dx, 3.0) / 6.0;
+    g.sp_nnodes = (int)S.sp_node.size();
+    std::vector<double> da2(S.nbody);
+    for (int m = 0; m < S.nbody; ++m)
+        da2[m] = 4.0 * 3.14159265358979323846 * ((S.radibdy * S.dx) * (S.radibdy * S.dx)) / (double)S.nrpr_active[m];
+    std::vector<double2> tw = twiddles(S.my);
+    const size_t NC = (size_t)g.nx * g.PS, NR = (size_t)g.nx * g.RS;
+    DevBufs &b = h->b;
+    bool ok = guard(h->upload(&g.tw, tw), "tw") && guard(h->upload(&g.ky, S.ky), "ky") && guard(h->upload(&g.kz, S.kz), "kz") &&
+              guard(h->upload(&g.w2, S.w2), "w2") && guard(h->upload(&g.fluid, S.fluid), "mask") &&
+              guard(h->upload(&g.xc, S.xc), "xc") && guard(h->upload(&g.vel, S.vel), "vel") &&
+              guard(h->upload(&g.bnd, S.bnd), "bnd") && guard(h->upload(&g.cd, S.cd), "cd") &&
+              guard(h->upload(&g.pt_m, S.pt_m), "pt_m") && guard(h->upload(&g.pt_l, S.pt_l), "pt_l") &&
+              guard(h->upload(&g.da2, da2), "da2") && guard(h->upload(&g.sp_node, S.sp_node), "sp_node") &&
+              guard(h->upload(&g.sp_ptr, S.sp_ptr), "sp_ptr") && guard(h->upload(&g.sp_ent, S.sp_ent), "sp_ent") &&
+              guard(h->alloc(&b.u, 3 * NC), "u") && guard(h->alloc(&b.p, NC), "p") &&
+              guard(h->alloc(&b.nl[0], 3 * NC), "nl0") && guard(h->alloc(&b.nl[1], 3 * NC), "nl1") &&
+              guard(h->alloc(&b.ff, 3 * NC), "ff") && guard(h->alloc(&b.ubcp, 3 * NR), "ubcp") &&
+              guard(h->alloc(&b.pbcp, NR), "pbcp") && guard(h->alloc(&b.nlbc[0], 3 * NR), "nlbc0") &&
+              guard(h->alloc(&b.nlbc[1], 3 * NR), "nlbc1") &&
+              (S.nbody == 0 || (guard(h->alloc(&b.diffn, 3 * NR), "diffn") && guard(h->alloc(&b.omega, 3 * NR), "omega") &&
+                                guard(h->alloc(&b.pgr, 3 * NR), "pgr") && guard(h->alloc(&b.fr, 3 * NR), "fr"))) &&
+              guard(h->alloc(&b.part, (size_t)g.nx * 12), "part") &&
+              guard(h->alloc(&b.pres, 3 * (size_t)S.nbody), "pres") && guard(h->alloc(&b.visc, 3 * (size_t)S.nbody), "visc") &&
+              guard(h->alloc(&b.ptot, 3 * (size_t)S.nbody), "ptot") && guard(h->alloc(&b.force, 3 * (size_t)S.nbody), "force") &&
+              guard(h->alloc(&b.rec, 6 * (size_t)g.npts), "rec") &&
+              guard(h->alloc(&b.blockpart, 6 * (size_t)((g.npts + 255) / 256 + 1)), "blockpart") &&
+              guard(h->alloc(&b.sc, 1), "scalars");
+    if (!ok) { delete h; return rc; }
+    Scal sc;
+    std::memset(&sc, 0, sizeof(sc));
+    for (int d = 0; d < 3; ++d) { sc.umean[d] = S.umean0[d]; sc.mpg[d] = prm->mpg[d]; }
+    sc.dt = S.dt; sc.cf = S.cf; sc.cforig = S.cf; sc.t = 0.0; sc.fold = 0.0; sc.ferror = 1.0;
+    if (!guard(cudaMemcpy(b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice), "scalars")) { delete h; return rc; }
+    *out = h;
+    return PIBM_OK;
+}
+
+int pibm_info_get(pibm_handle *h, pibm_info *info) {
+    if (!h || !info) return fail(PIBM_ERR_ARG, "null argument");
+    const RunSetup &S = h->S;
+    info->nx = S.nx; info->my = S.my; info->mz = S.mz; info->my2 = S.my2; info->nbody = S.nbody; info->nbnd = S.nbnd;
+    info->dx = S.dx; info->dt = S.dt; info->radbdy = S.radbdy; info->maxvolfrac = S.maxvolfrac;
+    info->count_solid = S.count_solid; info->count_fluid = S.count_fluid;
+    return PIBM_OK;
+}
+
+static int fill_report(pibm_handle *h, pibm_step_report *rep) {
+    Scal sc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    if (rep) {
+        std::memset(rep, 0, sizeof(*rep));
+        rep->dt = sc.dt; rep->t = sc.t; rep->cf = sc.cf; rep->umax = sc.umax;
+        long long bits = (long long)sc.divmax_bits;
+        std::memcpy(&rep->divmax, &bits, sizeof(double));
+        for (int d = 0; d < 3; ++d) {
+            rep->ufmean[d] = sc.ufmean[d]; rep->usmean[d] = sc.usmean[d]; rep->umean[d] = sc.umean[d];
+            rep->mpg[d] = sc.mpg[d]; rep->frmean[d] = sc.frmean[d];
+            rep->pres_total[d] = sc.pres_total[d]; rep->visc_total[d] = sc.visc_total[d];
+        }
+        rep->norm_drag = sc.norm_drag; rep->ferror = sc.ferror;
+        rep->pres_drag = sc.pres_drag; rep->visc_drag = sc.visc_drag; rep->total_drag = sc.total_drag;
+        rep->mixmeanslipmod = sc.mixmeanslipmod;
+        long long s = 0;
+        for (int v : h->S.nrpr_active) s += v;
+        rep->nrpr_active_total = s;
+    }
+    if (sc.status) return fail(sc.status, "step reported a solver stop condition");
+    return PIBM_OK;
+}
+
+int pibm_step(pibm_handle *h, int rks, pibm_step_report *rep) {
+    if (!h) return fail(PIBM_ERR_ARG, "null handle");
+    if (rks != 1) return fail(PIBM_ERR_ARG, "AB2 has a single sub-step (rks = 1)");
+    enqueue_step(h->g, h->b, h->cur, h->stream);
+    CUDA_OR_FAIL(cudaGetLastError());
+    h->cur ^= 1;
+    return fill_report(h, rep);
+}
+
+int pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last) {
+    if (!h || nsteps < 0) return fail(PIBM_ERR_ARG, "bad argument");
+    for (int par = 0; par < 2; ++par) {
+        if (h->graph[par]) continue;
+        cudaGraph_t gr;
+        CUDA_OR_FAIL(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(h->g, h->b, par, h->stream);
+        CUDA_OR_FAIL(cudaStreamEndCapture(h->stream, &gr));
+        CUDA_OR_FAIL(cudaGraphInstantiate(&h->graph[par], gr, 0));
+        cudaGraphDestroy(gr);
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], h->stream));
+        h->cur ^= 1;
+    }
+    return fill_report(h, last);
+}
+
+int pibm_get_state(pibm_handle *h, pibm_state_view *s) {
+    if (!h || !s) return fail(PIBM_ERR_ARG, "null argument");
+    const Geo &g = h->g;
+    const int nxf = g.nx + 1;
+    const size_t nfu = (size_t)nxf * g.PS * 3, nfp = (size_t)g.nx * g.PS;
+    double2 *tmp = nullptr;
+    CUDA_OR_FAIL(cudaMallocAsync(&tmp, nfu * sizeof(double2), h->stream));
+    const int prev = h->cur ^ 1;   // buffer holding the latest nl
+    if (s->u) {
+        enqueue_d2f(h->b.u, tmp, g.nx, nxf, g.PS, 3, h->stream);
+        CUDA_OR_FAIL(cudaMemcpyAsync(s->u, tmp, nfu * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    }
+    if (s->nl) {
+        enqueue_d2f(h->b.nl[prev], tmp, g.nx, nxf, g.PS, 3, h->stream);
+        CUDA_OR_FAIL(cudaMemcpyAsync(s->nl, tmp, nfu * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    }
+    if (s->p) {
+        enqueue_d2f(h->b.p, tmp, g.nx, g.nx, g.PS, 1, h->stream);
+        CUDA_OR_FAIL(cudaMemcpyAsync(s->p, tmp, nfp * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    }
+    Scal sc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaFreeAsync(tmp, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    for (int d = 0; d < 3; ++d) { s->umean[d] = sc.umean[d]; s->mpg[d] = sc.mpg[d]; s->ufmean[d] = sc.ufmean[d]; }
+    s->t = sc.t; s->dt = sc.dt; s->cf = sc.cf;
+    return PIBM_OK;
+}
+
+int pibm_set_state(pibm_handle *h, const pibm_state_view *s) {
+    if (!h || !s) return fail(PIBM_ERR_ARG, "null argument");
+    const Geo &g = h->g;
+    const int nxf = g.nx + 1;
+    const size_t nfu = (size_t)nxf * g.PS * 3, nfp = (size_t)g.nx * g.PS;
+    double2 *tmp = nullptr;
+    CUDA_OR_FAIL(cudaMallocAsync(&tmp, nfu * sizeof(double2), h->stream));
+    const int prev = h->cur ^ 1;
+    if (s->u) {
+        CUDA_OR_FAIL(cudaMemcpyAsync(tmp, s->u, nfu * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+        enqueue_f2d(tmp, h->b.u, g.nx, nxf, g.PS, 3, h->stream);
+    }
+    if (s->nl) {
+        CUDA_OR_FAIL(cudaMemcpyAsync(tmp, s->nl, nfu * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+        enqueue_f2d(tmp, h->b.nl[prev], g.nx, nxf, g.PS, 3, h->stream);
+        // rebuild the real-space history (onlbc of the next step = c2r(nl))
+        enqueue_c2r(g, h->b.nl[prev], h->b.nlbc[prev], 3 * g.nx, h->stream);
+    }
+    if (s->p) {
+        CUDA_OR_FAIL(cudaMemcpyAsync(tmp, s->p, nfp * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+        enqueue_f2d(tmp, h->b.p, g.nx, g.nx, g.PS, 1, h->stream);
+    }
+    Scal sc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    for (int d = 0; d < 3; ++d) { sc.umean[d] = s->umean[d]; sc.mpg[d] = s->mpg[d]; sc.ufmean[d] = s->ufmean[d]; }
+    sc.t = s->t; sc.dt = s->dt; sc.cf = s->cf;
+    sc.status = 0;
+    CUDA_OR_FAIL(cudaMemcpyAsync(h->b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, h->stream));
+    CUDA_OR_FAIL(cudaFreeAsync(tmp, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    return PIBM_OK;
+}
+
+int pibm_get_particles(pibm_handle *h, double *pres, double *visc, double *force, double *xc, double *vel) {
+    if (!h) return fail(PIBM_ERR_ARG, "null handle");
+    const size_t n = (size_t)h->S.nbody * 3;
+    if (n == 0) return PIBM_OK;
+    if (pres) CUDA_OR_FAIL(cudaMemcpyAsync(pres, h->b.pres, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (visc) CUDA_OR_FAIL(cudaMemcpyAsync(visc, h->b.visc, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (force) CUDA_OR_FAIL(cudaMemcpyAsync(force, h->b.force, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    if (xc) std::memcpy(xc, h->S.xc.data(), n * sizeof(double));
+    if (vel) std::memcpy(vel, h->S.vel.data(), n * sizeof(double));
+    return PIBM_OK;
+}
+
+int pibm_get_if_rev(pibm_handle *h, uint8_t *if_rev) {
+    if (!h || !if_rev) return fail(PIBM_ERR_ARG, "null argument");
+    std::memcpy(if_rev, h->S.if_rev.data(), h->S.if_rev.size());
+    return PIBM_OK;
+}
+
+int pibm_get_fluid_mask(pibm_handle *h, uint8_t *mask) {
+    if (!h || !mask) return fail(PIBM_ERR_ARG, "null argument");
+    const RunSetup &S = h->S;
+    for (int i = 0; i < S.nx; ++i)
+        for (int k = 0; k < S.mz; ++k)
+            for (int j = 0; j < S.my; ++j)
+                mask[(size_t)i + (size_t)S.nx * ((size_t)j + (size_t)S.my * k)] = S.fluid[(size_t)i * S.my * S.mz + (size_t)k * S.my + j];
+    return PIBM_OK;
+}
+
+void pibm_destroy(pibm_handle *h) { delete h; }
+
+static int plane_transform(int my, int mz, int nplanes, const double *a, double *b, bool forward) {
+    if (my != mz || !supported_size(my) || nplanes < 0 || !a || !b) return fail(PIBM_ERR_ARG, "unsupported plane size");
+    if (nplanes == 0) return PIBM_OK;
+    Geo g;
+    std::memset(&g, 0, sizeof(g));
+    g.nx = 1; g.my = my; g.mz = mz; g.my2 = my / 2 + 1; g.PS = g.my2 * mz; g.RS = my * mz;
+    g.nrm = (double)(float)(my * mz);
+    CUDA_OR_FAIL(configure_kernels(my));
+    std::vector<double2> tw = twiddles(my);
+    double2 *dtw = nullptr, *dc = nullptr;
+    double *dr = nullptr;
+    const size_t nc = (size_t)g.PS * nplanes, nr = (size_t)g.RS * nplanes;
+    CUDA_OR_FAIL(cudaMalloc(&dtw, tw.size() * sizeof(double2)));
+    CUDA_OR_FAIL(cudaMalloc(&dc, nc * sizeof(double2)));
+    CUDA_OR_FAIL(cudaMalloc(&dr, nr * sizeof(double)));
+    CUDA_OR_FAIL(cudaMemcpy(dtw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    g.tw = dtw;
+    if (forward) {
+        CUDA_OR_FAIL(cudaMemcpy(dr, a, nr * sizeof(double), cudaMemcpyHostToDevice));
+        enqueue_r2c(g, dr, dc, nplanes, 0);
+        CUDA_OR_FAIL(cudaGetLastError());
+        CUDA_OR_FAIL(cudaMemcpy(b, dc, nc * sizeof(double2), cudaMemcpyDeviceToHost));
+    } else {
+        CUDA_OR_FAIL(cudaMemcpy(dc, a, nc * sizeof(double2), cudaMemcpyHostToDevice));
+        enqueue_c2r(g, dc, dr, nplanes, 0);
+        CUDA_OR_FAIL(cudaGetLastError());
+        CUDA_OR_FAIL(cudaMemcpy(b, dr, nr * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    cudaFree(dtw); cudaFree(dc); cudaFree(dr);
+    return PIBM_OK;
+}
+
+int pibm_ff2rc(int my, int mz, int nplanes, const double *a, double *b) { return plane_transform(my, mz, nplanes, a, b, true); }
+int pibm_ff2cr(int my, int mz, int nplanes, const double *a, double *b) { return plane_transform(my, mz, nplanes, a, b, false); }
+
+// ---- batched independent realizations ----
+struct pibm_batch {
+    std::vector<pibm_handle *> members;
+};
+
+int pibm_batch_create(int n, const pibm_params *prm, const pibm_particles *parts, pibm_batch **out) {
+    if (n <= 0 || !prm || !out) return fail(PIBM_ERR_ARG, "bad argument");
+    pibm_batch *bt = new pibm_batch();
+    for (int q = 0; q < n; ++q) {
+        pibm_handle *h = nullptr;
+        int rc = pibm_create(&prm[q], parts ? &parts[q] : nullptr, &h);
+        if (rc) { for (auto *m : bt->members) pibm_destroy(m); delete bt; return rc; }
+        bt->members.push_back(h);
+    }
+    *out = bt;
+    return PIBM_OK;
+}
+
+int pibm_batch_run(pibm_batch *bt, int nsteps) {
+    if (!bt) return fail(PIBM_ERR_ARG, "null batch");
+    // every member replays its own graphs on its own stream; launches interleave
+    for (auto *h : bt->members)
+        for (int par = 0; par < 2; ++par)
+            if (!h->graph[par]) { int rc = pibm_run(h, 0, nullptr); if (rc) return rc; }
+    for (int s = 0; s < nsteps; ++s)
+        for (auto *h : bt->members) {
+            CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], h->stream));
+            h->cur ^= 1;
+        }
+    int rc = PIBM_OK;
+    for (auto *h : bt->members) { int r = fill_report(h, nullptr); if (r && !rc) rc = r; }
+    return rc;
+}
+
+pibm_handle *pibm_batch_member(pibm_batch *bt, int i) {
+    if (!bt || i < 0 || i >= (int)bt->members.size()) return nullptr;
+    return bt->members[i];
+}
+
+void pibm_batch_destroy(pibm_batch *bt) {
+    if (!bt) return;
+    for (auto *h : bt->members) pibm_destroy(h);
+    delete bt;
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// engine.cuh -- device-side data structures of the time-step engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pibm {
+
+// Per-run constants passed by value to every kernel.
+struct Geo {
+    int nx, my, mz, my2;
+    int PS;             // complex elements per spectral plane (my2*mz)
+    int RS;             // real elements per physical plane (my*mz)
+    double dx, dx2, rdx2, dx3, vis, nrm;   // nrm = float(my*mz) as in ff2rc
+    double c1, c2, c3, c4;
+    int scheme, limiter, include_frmeanfluid, revernorm, set_mpg, adaptive;
+    double cfl_max, ramp_frac_time, ucharmod, char_length, voldom, maxvolfrac, mean_volfrac;
+    long long count_fluid, ncell;
+    double ufmean_des[3], usmean_des[3], usmean_act[3];
+    // particles
+    int nbody, nbnd, npts;
+    double rb, ri, ro, dr, da1, sphere_vol;
+    // device arrays (read-only)
+    const double2 *tw;          // e^{-2 pi i m/my}, m < my (my == mz)
+    const double *ky, *kz, *w2; // wavenumbers
+    const uint8_t *fluid;       // [i][k][j] 1 = fluid
+    const double *xc;           // (nbody,3) column-major
+    const double *vel;          // (nbody,3)
+    const double *bnd, *cd;     // (3,nbnd)
+    const int *pt_m, *pt_l;     // active reversal points
+    const double *da2;          // per sphere
+    const int *sp_node, *sp_ptr, *sp_ent;   // spreading map
+    int sp_nnodes;
+};
+
+// Evolving scalars of a run (one struct in device memory).
+struct Scal {
+    double umean[3], mpg[3], frmean[3], frmeanfluid[3];
+    double ufmean[3], ufmean_old[3], usmean[3], dufmeandt[3];
+    double dt, t, cf, cforig, umax, mixmeanslipmod;
+    double pres_total[3], visc_total[3];
+    double norm_drag, ferror, fold, pres_drag, visc_drag, total_drag;
+    double frame_accln[3];
+    unsigned long long divmax_bits;
+    int status;
+    int pad;
+    long long nsteps;
+};
+
+// Device buffers of one run.
+struct DevBufs {
+    double2 *u, *p, *nl[2], *ff;
+    double *ubcp, *pbcp, *nlbc[2], *diffn, *omega, *pgr, *fr;
+    double *part, *pres, *visc, *ptot, *force, *rec, *blockpart;
+    Scal *sc;
+};
+
+}  // namespace pibm

@@ -1,0 +1,1081 @@
+// kernels.cu -- sm_100a FP64 kernels of one AB2 time step.
+//
+// Data layout in HBM (chosen for the two sweep directions of the step):
+//   spectral fields  double2 [comp][i][k][j]   (plane i contiguous, j fastest, pitch my2)
+//   physical fields  double  [comp][i][k][j]   (pitch my)
+// so an x-plane is one contiguous block (plane kernels) and, for fixed i, the
+// (j,k) lines of a plane are contiguous (line kernel loads are coalesced
+// across consecutive j).  The periodic image plane nx+1 of the reference is
+// never stored; indices wrap instead.
+//
+// Step pipeline (reference routines in brackets):
+//   k_a0      u,p -> ubcp,pbcp + fluid/solid means, max|u|   [compute_new_timestep, calc_pressure]
+//   k_scal_a  CFL dt, t, cf (soft start), ufmean, mean slip   [compute_new_timestep]
+//   k_nl      products, upwind/central x flux, 9 r2c -> nl; 3 c2r -> nlbc   [form_nl, nonlinear]
+//   k_fields  diffn, omega, grad p: 9 c2r                      [calc_visc, compute_omega, calc_pgrad]
+//   k_drag    per-sphere surface quadrature of p and omega     [calc_pres_visc_drag]
+//   k_scal_b  pres/visc totals, mpg, per-sphere force, drag diagnostics   [compute_mpg_at_n, bcset]
+//   k_rev     reversal-point force per active point            [calc_inner_reversal_forcing]
+//   k_scal_c  frmean
+//   k_spread  gather of point forces onto solid nodes in reference order
+//   k_ff      fr - frmean -> ff (3 r2c)                        [bcset]
+//   k_lines   pressure -> ustep -> divcorr per (ky,kz) line     [velstep]
+//   k_scal_d  umean update, divergence, status                 [velstep]
+#include "engine.cuh"
+#include "fft_plane.cuh"
+#include "../../include/pibm.h"
+
+namespace pibm {
+
+__device__ __constant__ double kSmallD = 1.0000000180025095e-35;   // (double)1.0E-35f
+
+template <int N> struct PT;
+template <> struct PT<32>  { static constexpr int RZ = 1, LZ = 32, RY = 1, LY = 16, T = 128, EPT = 5; };
+template <> struct PT<64>  { static constexpr int RZ = 2, LZ = 32, RY = 1, LY = 32, T = 256, EPT = 9; };
+template <> struct PT<96>  { static constexpr int RZ = 3, LZ = 32, RY = 3, LY = 16, T = 256, EPT = 19; };
+template <> struct PT<128> { static constexpr int RZ = 4, LZ = 32, RY = 2, LY = 32, T = 512, EPT = 17; };
+
+template <int N>
+__device__ __forceinline__ void plane_c2r(double2 *buf, const Geo &g, const Tw &tw) {
+    z_pass<PT<N>::RZ, PT<N>::LZ>(buf, g.my2, g.mz, +1.0, tw);
+    __syncthreads();
+    y_c2r_pass<PT<N>::RY, PT<N>::LY>(buf, g.my2, g.mz, tw);
+    __syncthreads();
+}
+template <int N>
+__device__ __forceinline__ void plane_r2c(double2 *buf, const Geo &g, const Tw &tw) {
+    y_r2c_pass<PT<N>::RY, PT<N>::LY>(buf, g.my2, g.mz, tw);
+    __syncthreads();
+    z_pass<PT<N>::RZ, PT<N>::LZ>(buf, g.my2, g.mz, -1.0, tw);
+    __syncthreads();
+}
+
+__device__ __forceinline__ double &rv(double2 *buf, int my2, int k, int j) { return ((double *)buf)[(size_t)k * 2 * my2 + j]; }
+
+template <int N>
+__device__ __forceinline__ void load_tw(double2 *tws, const Geo &g) {
+    for (int t = threadIdx.x; t < N; t += blockDim.x) tws[t] = g.tw[t];
+}
+
+// Deterministic block sum (fixed lane/warp tree).
+__device__ __forceinline__ double block_sum(double v, double *scr) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) scr[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < nw ? scr[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) scr[0] = r;
+    __syncthreads();
+    r = scr[0];
+    __syncthreads();
+    return r;
+}
+__device__ __forceinline__ double block_max(double v, double *scr) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) scr[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < nw ? scr[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) scr[0] = r;
+    __syncthreads();
+    r = scr[0];
+    __syncthreads();
+    return r;
+}
+
+// ============================================================================
+// k_a0: ubcp = c2r(u) + umean, pbcp = c2r(p); per-plane partial means and maxima
+// (dependent_functions.F90:1085-1122, 336-349).  part[i*12 + q]:
+// q 0-2 fluid sums, 3-5 solid sums, 6-8 all sums, 9-11 max |u|.
+// ============================================================================
+template <int N>
+__global__ void __launch_bounds__(PT<N>::T) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
+                                                 double *__restrict__ ubcp, double *__restrict__ pbcp,
+                                                 const Scal *__restrict__ sc, double *__restrict__ part) {
+    extern __shared__ double2 sm[];
+    double2 *buf = sm, *tws = sm + g.PS;
+    __shared__ double scr[32];
+    load_tw<N>(tws, g);
+    const int i = blockIdx.x;
+    const Tw tw{tws, N, 1};
+    const int nx = g.nx, PS = g.PS, RS = g.RS, my = g.my, my2 = g.my2;
+    double acc[12];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) acc[q] = 0.0;
+    acc[9] = acc[10] = acc[11] = kSmallD;
+    for (int n = 0; n < 4; ++n) {
+        const double2 *src = n < 3 ? u + ((size_t)n * nx + i) * PS : p + (size_t)i * PS;
+        for (int e = threadIdx.x; e < PS; e += blockDim.x) buf[e] = src[e];
+        __syncthreads();
+        plane_c2r<N>(buf, g, tw);
+        if (n < 3) {
+            const double um = sc->umean[n];
+            double *dst = ubcp + ((size_t)n * nx + i) * RS;
+            const uint8_t *fl = g.fluid + (size_t)i * RS;
+            for (int e = threadIdx.x; e < RS; e += blockDim.x) {
+                const int k = e / my, j = e - k * my;
+                const double v = rv(buf, my2, k, j) + um;
+                dst[e] = v;
+                if (fl[e]) acc[n] += v; else acc[3 + n] += v;
+                acc[6 + n] += v;
+                acc[9 + n] = fmax(acc[9 + n], fabs(v));
+            }
+        } else {
+            double *dst = pbcp + (size_t)i * RS;
+            for (int e = threadIdx.x; e < RS; e += blockDim.x) {
+                const int k = e / my, j = e - k * my;
+                dst[e] = rv(buf, my2, k, j);
+            }
+        }
+        __syncthreads();
+    }
+    for (int q = 0; q < 9; ++q) {
+        const double s = block_sum(acc[q], scr);
+        if (threadIdx.x == 0) part[(size_t)i * 12 + q] = s;
+    }
+    for (int q = 9; q < 12; ++q) {
+        const double s = block_max(acc[q], scr);
+        if (threadIdx.x == 0) part[(size_t)i * 12 + q] = s;
+    }
+}
+
+// compute_new_timestep's scalar tail (dependent_functions.F90:1137-1280).
+__global__ void k_scal_a(Geo g, Scal *sc, const double *part) {
+    if (threadIdx.x != 0 || sc->status) return;
+    double uf[3] = {0, 0, 0}, mx[3] = {kSmallD, kSmallD, kSmallD};
+    for (int i = 0; i < g.nx; ++i)
+        for (int d = 0; d < 3; ++d) { uf[d] += part[(size_t)i * 12 + d]; mx[d] = fmax(mx[d], part[(size_t)i * 12 + 9 + d]); }
+    const double umax = fmax(fmax(mx[0], mx[1]), mx[2]);
+    sc->umax = umax;
+    double dtnew = sc->dt;
+    if (umax * sc->dt / g.dx > g.cfl_max) dtnew = g.cfl_max * g.dx / umax;
+    for (int d = 0; d < 3; ++d) {
+        sc->ufmean_old[d] = sc->ufmean[d];
+        sc->ufmean[d] = uf[d] / (double)g.count_fluid;
+        sc->dufmeandt[d] = -sc->cf * (sc->ufmean[d] - sc->ufmean_old[d]);
+    }
+    double ms[3];
+    for (int d = 0; d < 3; ++d) {
+        sc->usmean[d] = g.nbody > 0 ? (g.mean_volfrac * g.usmean_act[d]) / g.mean_volfrac : 0.0;
+        ms[d] = (1.0 - g.maxvolfrac) * (sc->usmean[d] - sc->ufmean[d]);
+    }
+    sc->mixmeanslipmod = sqrt(ms[0] * ms[0] + ms[1] * ms[1] + ms[2] * ms[2]);
+    if (g.adaptive) sc->dt = dtnew;
+    sc->t = sc->t + sc->dt * (g.c1 + g.c2);
+    const double tempt = g.ramp_frac_time * (double)(float)(g.nx) * g.dx / g.ucharmod;
+    sc->cf = -1.0 / sc->dt;
+    sc->cforig = sc->cf;
+    if (sc->t < tempt) sc->cf = sc->cf * (sc->t / tempt);
+    sc->divmax_bits = 0ull;
+}
+
+// ============================================================================
+// k_nl: nonlinear term -div(uu) of one plane (nl_allflow.F90:71-327, nl.F90:99-173).
+// nl_c = -( (wy*F(u_a u_b) + wz*F(u_a' u_b')) + F(D_c) ),  D_c = x-flux difference.
+// ============================================================================
+__device__ __forceinline__ double slope_lim(double um1, double u0, double up1, double dx, int limiter) {
+    double s = (up1 - um1) / (2.0 * dx);
+    double phi = 1.0;
+    if (limiter == PIBM_LIMITER_MINMOD) {
+        phi = (u0 - um1) / (up1 - u0 + kSmallD);
+        phi = phi <= 0.0 ? 0.0 : fmin(1.0, phi);
+    }
+    return s * phi * 1.0;
+}
+
+// x-flux difference D_c at plane i for node e of the plane (upwind: MUSCL
+// states + Rusanov flux, nl_allflow.F90:139-294; center: nl_allflow.F90:97-124,298-310).
+__device__ __forceinline__ double xflux_diff(const Geo &g, const double *__restrict__ ubcp, int i, int e, int c) {
+    const int nx = g.nx;
+    const size_t RS = g.RS;
+    auto U = [&](int comp, int ii) -> double {
+        ii = ii < 0 ? ii + nx : (ii >= nx ? ii - nx : ii);
+        return __ldg(ubcp + ((size_t)comp * nx + ii) * RS + e);
+    };
+    const double dx = g.dx;
+    if (g.scheme == PIBM_SCHEME_CENTER) {
+        const double fp = U(0, i + 1) * U(c, i + 1), fm = U(0, i - 1) * U(c, i - 1);
+        return (fp - fm) / (2.0 * dx);
+    }
+    // cells i-2 .. i+2 of component 0 (advecting velocity) and component c
+    double a[5], b[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) { a[q] = U(0, i - 2 + q); b[q] = (c == 0) ? a[q] : U(c, i - 2 + q); }
+    // slopes at cells i-1, i, i+1 (index 1..3 in the window)
+    double sa[3], sb[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        sa[q] = slope_lim(a[q], a[q + 1], a[q + 2], dx, g.limiter);
+        sb[q] = (c == 0) ? sa[q] : slope_lim(b[q], b[q + 1], b[q + 2], dx, g.limiter);
+    }
+    const double h = dx / 2.0;
+    double F[2];
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        // interface between window cells (f+1) and (f+2): global interface m = i-1+f
+        const double uminus = a[f + 1] + sa[f] * h;
+        const double uplus = a[f + 2] - sa[f + 1] * h;
+        const double Um = b[f + 1] + sb[f] * h;
+        const double Up = b[f + 2] - sb[f + 1] * h;
+        const double Am = 0.5 * uminus * Um, Ap = 0.5 * uplus * Up;
+        const double ms = fmax(fabs(uminus), fabs(uplus));
+        int m = i - 1 + f;
+        m = m < 0 ? m + nx : m;
+        // interface nx (m == nx-1 here, 0-based) receives the cell-1 contribution first
+        const double s = (m == nx - 1) ? ((0.0 + Ap) + Am) : ((0.0 + Am) + Ap);
+        F[f] = s - 0.5 * ms * (Up - Um);
+    }
+    return (F[1] - F[0]) / dx;
+}
+
+template <int N>
+__global__ void __launch_bounds__(PT<N>::T) k_nl(Geo g, const double *__restrict__ ubcp, double2 *__restrict__ nl_new,
+                                                 double *__restrict__ nlbc_new, const Scal *__restrict__ sc) {
+    extern __shared__ double2 sm[];
+    double2 *buf = sm, *tws = sm + g.PS;
+    load_tw<N>(tws, g);
+    const int i = blockIdx.x;
+    const Tw tw{tws, N, 1};
+    const int nx = g.nx, PS = g.PS, RS = g.RS, my = g.my, my2 = g.my2;
+    constexpr int EPT = PT<N>::EPT, T = PT<N>::T;
+    const double *U0 = ubcp + ((size_t)0 * nx + i) * RS;
+    const double *U1 = ubcp + ((size_t)1 * nx + i) * RS;
+    const double *U2 = ubcp + ((size_t)2 * nx + i) * RS;
+    // product pairs: comp c uses (wy: pa[c]) and (wz: pb[c])
+    const int pa0[3] = {0, 1, 1}, pa1[3] = {1, 1, 2}, pb0[3] = {0, 1, 2}, pb1[3] = {2, 2, 2};
+    const double *Uc[3] = {U0, U1, U2};
+    for (int c = 0; c < 3; ++c) {
+        double2 acc[EPT];
+        for (int q = 0; q < 3; ++q) {
+            for (int e = threadIdx.x; e < RS; e += blockDim.x) {
+                const int k = e / my, j = e - k * my;
+                double v;
+                if (q == 0) v = Uc[pa0[c]][e] * Uc[pa1[c]][e];
+                else if (q == 1) v = Uc[pb0[c]][e] * Uc[pb1[c]][e];
+                else v = xflux_diff(g, ubcp, i, e, c);
+                rv(buf, my2, k, j) = v;
+            }
+            __syncthreads();
+            plane_r2c<N>(buf, g, tw);
+#pragma unroll
+            for (int s = 0; s < EPT; ++s) {
+                const int e = threadIdx.x + s * T;
+                if (e < PS) {
+                    const double2 X = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
+                    const int k = e / my2, j = e - k * my2;
+                    if (q == 0) { const double ky = g.ky[j]; acc[s] = make_double2(-ky * X.y, ky * X.x); }
+                    else if (q == 1) { const double kz = g.kz[k]; acc[s] = cadd(acc[s], make_double2(-kz * X.y, kz * X.x)); }
+                    else acc[s] = cadd(acc[s], X);
+                }
+            }
+            __syncthreads();
+        }
+        double2 *dst = nl_new + ((size_t)c * nx + i) * PS;
+#pragma unroll
+        for (int s = 0; s < EPT; ++s) {
+            const int e = threadIdx.x + s * T;
+            if (e < PS) {
+                const double2 v = make_double2(-acc[s].x, -acc[s].y);
+                dst[e] = v;
+                buf[e] = v;
+            }
+        }
+        __syncthreads();
+        plane_c2r<N>(buf, g, tw);
+        double *rd = nlbc_new + ((size_t)c * nx + i) * RS;
+        for (int e = threadIdx.x; e < RS; e += blockDim.x) {
+            const int k = e / my, j = e - k * my;
+            rd[e] = rv(buf, my2, k, j);
+        }
+        __syncthreads();
+    }
+}
+
+// ============================================================================
+// k_fields: diffn (calc_visc, boundary_condition.F90:1767-1815), omega
+// (compute_omega :1648-1765; omega_x from one transform of wy*u3 - wz*u2) and
+// grad p without mpg (calc_pgrad :1817-1896; mpg is added per node when
+// interpolated, as the reference adds it per node before interpolation).
+// ============================================================================
+template <int N>
+__global__ void __launch_bounds__(PT<N>::T) k_fields(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
+                                                     const double *__restrict__ ubcp, double *__restrict__ diffn,
+                                                     double *__restrict__ omega, double *__restrict__ pgr) {
+    extern __shared__ double2 sm[];
+    double2 *buf = sm, *tws = sm + g.PS;
+    load_tw<N>(tws, g);
+    const int i = blockIdx.x;
+    const Tw tw{tws, N, 1};
+    const int nx = g.nx, PS = g.PS, RS = g.RS, my = g.my, my2 = g.my2;
+    const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
+    const double tdx = 2.0 * g.dx;
+    for (int t = 0; t < 9; ++t) {
+        for (int e = threadIdx.x; e < PS; e += blockDim.x) {
+            const int k = e / my2, j = e - k * my2;
+            const double ky = g.ky[j], kz = g.kz[k];
+            double2 f;
+            if (t < 3) {
+                const double2 *un = u + (size_t)t * nx * PS;
+                const double2 a = un[(size_t)im * PS + e], b = un[(size_t)i * PS + e], c = un[(size_t)ip * PS + e];
+                double2 s = make_double2(g.rdx2 * ((a.x - 2.0 * b.x) + c.x), g.rdx2 * ((a.y - 2.0 * b.y) + c.y));
+                const double w2 = g.w2[e];
+                s = make_double2(s.x - w2 * b.x, s.y - w2 * b.y);
+                f = make_double2(s.x * g.vis, s.y * g.vis);
+            } else if (t == 3) {   // wy*u1
+                const double2 a = u[(size_t)i * PS + e];
+                f = make_double2(-ky * a.y, ky * a.x);
+            } else if (t == 4) {   // wz*u1
+                const double2 a = u[(size_t)i * PS + e];
+                f = make_double2(-kz * a.y, kz * a.x);
+            } else if (t == 5) {   // wy*u3 - wz*u2
+                const double2 a = u[((size_t)2 * nx + i) * PS + e], b = u[((size_t)1 * nx + i) * PS + e];
+                f = make_double2(-ky * a.y - (-kz * b.y), ky * a.x - kz * b.x);
+            } else if (t == 6) {
+                const double2 a = p[(size_t)ip * PS + e], b = p[(size_t)im * PS + e];
+                f = make_double2((a.x - b.x) / tdx, (a.y - b.y) / tdx);
+            } else if (t == 7) {
+                const double2 a = p[(size_t)i * PS + e];
+                f = make_double2(-a.y * ky, a.x * ky);
+            } else {
+                const double2 a = p[(size_t)i * PS + e];
+                f = make_double2(-a.y * kz, a.x * kz);
+            }
+            buf[e] = f;
+        }
+        __syncthreads();
+        plane_c2r<N>(buf, g, tw);
+        for (int e = threadIdx.x; e < RS; e += blockDim.x) {
+            const int k = e / my, j = e - k * my;
+            const double v = rv(buf, my2, k, j);
+            if (t < 3) diffn[((size_t)t * nx + i) * RS + e] = v;
+            else if (t == 3) {
+                const double *u2 = ubcp + (size_t)1 * nx * RS;
+                omega[((size_t)2 * nx + i) * RS + e] = (u2[(size_t)ip * RS + e] - u2[(size_t)im * RS + e]) / tdx - v;
+            } else if (t == 4) {
+                const double *u3 = ubcp + (size_t)2 * nx * RS;
+                omega[((size_t)1 * nx + i) * RS + e] = v - (u3[(size_t)ip * RS + e] - u3[(size_t)im * RS + e]) / tdx;
+            } else if (t == 5) omega[((size_t)0 * nx + i) * RS + e] = v;
+            else pgr[((size_t)(t - 6) * nx + i) * RS + e] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// ============================================================================
+// Interpolation stencils ('lpi', order 2, periodic): stencil = [pc, pc+1]
+// (dependent_functions.F90:45-275; interpolation.F90:202-381,740-751).
+// Geometry uses explicitly rounded operations so host and device agree.
+// ============================================================================
+struct Sten {
+    int ii[2], jj[2], kk[2];
+    double xv[2], yv[2], zv[2];
+    __device__ __forceinline__ double w(int a, int b, int c) const { return __dmul_rn(__dmul_rn(xv[a], yv[b]), zv[c]); }
+};
+
+__device__ __forceinline__ int cell_of(double x) { return x < 0.0 ? (int)(x - 1.0) : (int)x; }
+
+__device__ __forceinline__ int wrapi(int v, int n) { return v < 1 ? v + n : (v > n ? v - n : v); }
+
+__device__ __forceinline__ void make_sten(const Geo &g, const double pos[3], Sten &s) {
+    int pc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) pc[d] = cell_of(pos[d]);
+    const double zx = __dsub_rn(pos[0], (double)pc[0]);
+    const double zy = __dsub_rn(pos[1], (double)pc[1]);
+    const double zz = __dsub_rn(pos[2], (double)pc[2]);
+    s.xv[0] = __dsub_rn(1.0, zx); s.xv[1] = zx;
+    s.yv[0] = __dsub_rn(1.0, zy); s.yv[1] = zy;
+    s.zv[0] = __dsub_rn(1.0, zz); s.zv[1] = zz;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        s.ii[q] = wrapi(pc[0] + q, g.nx) - 1;   // 0-based
+        s.jj[q] = wrapi(pc[1] + q, g.my) - 1;
+        s.kk[q] = wrapi(pc[2] + q, g.mz) - 1;
+    }
+}
+
+// value at node (i,j,k) of a physical field f (one component)
+__device__ __forceinline__ double fat(const Geo &g, const double *f, int i, int j, int k) {
+    return __ldg(f + (size_t)i * g.RS + (size_t)k * g.my + j);
+}
+// interpolator order (k, j, i)
+__device__ __forceinline__ double interp_kji(const Geo &g, const Sten &s, const double *f, double add = 0.0) {
+    double r = 0.0;
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int a = 0; a < 2; ++a) r = r + (fat(g, f, s.ii[a], s.jj[b], s.kk[c]) + add) * s.w(a, b, c);
+    return r;
+}
+// array_dot_product order (i, j, k)
+__device__ __forceinline__ double dot_ijk(const Geo &g, const Sten &s, const double *f) {
+    double r = 0.0;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) r = r + fat(g, f, s.ii[a], s.jj[b], s.kk[c]) * s.w(a, b, c);
+    return r;
+}
+
+// ============================================================================
+// k_drag: per-sphere pressure and viscous force from the surface quadrature
+// (calc_pres_visc_drag, boundary_condition.F90:1481-1645).  One CTA per sphere.
+// out[0..3*nbody): pres(m,d) ; then visc ; then +pl*cd*da1 sums (pres_total share)
+// ============================================================================
+__global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ pbcp, const double *__restrict__ omega,
+                                              double *__restrict__ pres, double *__restrict__ visc, double *__restrict__ ptot,
+                                              const Scal *__restrict__ sc) {
+    __shared__ double scr[32];
+    const int m = blockIdx.x;
+    const int NB = g.nbody;
+    double xcm[3] = {g.xc[m], g.xc[m + NB], g.xc[m + 2 * NB]};
+    double sa[3] = {0, 0, 0}, sb[3] = {0, 0, 0};
+    const size_t CR = (size_t)g.nx * g.RS;
+    for (int l = threadIdx.x; l < g.nbnd; l += blockDim.x) {
+        double xl[3], xpb[3], cdl[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { xl[d] = __dadd_rn(xcm[d], __dmul_rn(g.bnd[3 * l + d], g.rb)); cdl[d] = g.cd[3 * l + d]; }
+        xpb[0] = __dsub_rn(xl[0], 0.5); xpb[1] = xl[1]; xpb[2] = xl[2];
+        Sten sp, sv;
+        make_sten(g, xpb, sp);
+        make_sten(g, xl, sv);
+        const double pl = dot_ijk(g, sp, pbcp);
+        double vort[3];
+#pragma unroll
+        for (int n = 0; n < 3; ++n) vort[n] = interp_kji(g, sv, omega + n * CR);
+        double df[3];
+        df[0] = vort[2] * cdl[1]; df[0] = df[0] - vort[1] * cdl[2];
+        df[1] = vort[0] * cdl[2]; df[1] = df[1] - vort[2] * cdl[0];
+        df[2] = vort[1] * cdl[0]; df[2] = df[2] - vort[0] * cdl[1];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            sa[d] += pl * cdl[d] * g.da1;
+            sb[d] += (-df[d]) * g.vis * g.da1;
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+        const double a = block_sum(sa[d], scr), b = block_sum(sb[d], scr);
+        if (threadIdx.x == 0) { pres[m + d * NB] = -a; ptot[m + d * NB] = a; visc[m + d * NB] = b; }
+    }
+}
+
+// compute_mpg_at_n tail + bcset diagnostics (boundary_condition.F90:356-464, 701-884).
+__global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, const double *pres, const double *visc, const double *ptot,
+                                                double *force) {
+    __shared__ double scr[32];
+    __shared__ double tot[12];
+    if (sc->status) return;
+    const int NB = g.nbody;
+    for (int d = 0; d < 3; ++d) {
+        double a = 0, b = 0, c = 0;
+        for (int m = threadIdx.x; m < NB; m += blockDim.x) { a += ptot[m + d * NB]; b += visc[m + d * NB]; c += pres[m + d * NB]; }
+        a = block_sum(a, scr); b = block_sum(b, scr); c = block_sum(c, scr);
+        if (threadIdx.x == 0) { tot[d] = a; tot[3 + d] = b; tot[6 + d] = c; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int d = 0; d < 3; ++d) { sc->pres_total[d] = tot[d]; sc->visc_total[d] = tot[3 + d]; }
+        const double nf = (3.0 * 3.14159265358979323846 * g.vis * (sc->mixmeanslipmod + kSmallD) * g.char_length) * (double)NB;
+        const double pa = sqrt(tot[6] * tot[6] + tot[7] * tot[7] + tot[8] * tot[8]);
+        const double va = sqrt(tot[3] * tot[3] + tot[4] * tot[4] + tot[5] * tot[5]);
+        sc->pres_drag = pa / nf / (1.0 - g.maxvolfrac);
+        sc->visc_drag = va / nf / (1.0 - g.maxvolfrac);
+        sc->total_drag = sc->pres_drag + sc->visc_drag;
+        if (!g.set_mpg) {
+            for (int d = 0; d < 3; ++d) {
+                sc->mpg[d] = sc->cf * (g.ufmean_des[d] - sc->ufmean[d]) +
+                             (sc->pres_total[d] / g.voldom - (sc->visc_total[d]) / g.voldom) / (1.0 - g.maxvolfrac);
+                if (g.include_frmeanfluid) sc->mpg[d] = sc->mpg[d] + sc->frmeanfluid[d];
+            }
+        }
+    }
+    __syncthreads();
+    const double c12 = g.c1 + g.c2;
+    const double mp[3] = {sc->mpg[0], sc->mpg[1], sc->mpg[2]};
+    double fs[3] = {0, 0, 0};
+    for (int m = threadIdx.x; m < NB; m += blockDim.x)
+        for (int d = 0; d < 3; ++d) {
+            const double f = c12 * (pres[m + d * NB] + visc[m + d * NB]) - c12 * mp[d] * g.sphere_vol;
+            force[m + d * NB] = f;
+            fs[d] += f;
+        }
+    for (int d = 0; d < 3; ++d) fs[d] = block_sum(fs[d], scr);
+    if (threadIdx.x == 0) {
+        double avg[3];
+        for (int d = 0; d < 3; ++d) avg[d] = (fs[d] / NB) * g.mean_volfrac / g.mean_volfrac;
+        const double nd = sqrt(avg[0] * avg[0] + avg[1] * avg[1] + avg[2] * avg[2]);
+        double nf = 3.0 * 3.14159265358979323846 * g.vis * g.ucharmod * g.char_length;
+        if (g.set_mpg) nf = 3.0 * 3.14159265358979323846 * g.vis * (sc->mixmeanslipmod + kSmallD) * g.char_length;
+        sc->norm_drag = nd / nf;
+        sc->ferror = sc->norm_drag > 0.0 ? fabs(sc->norm_drag - sc->fold) / sc->norm_drag : 1.0;
+        sc->fold = sc->norm_drag;
+        if (sc->norm_drag > 1.0e6) sc->status = PIBM_ERR_BLOWUP;
+    }
+}
+
+// ============================================================================
+// k_rev: direct forcing at the inner reversal points
+// (calc_inner_reversal_forcing, boundary_condition.F90:1104-1479).
+// rec[p*6 + 0..2] = force_tmp, rec[p*6 + 3..5] = force_dist; blockpart = sums of
+// tmppa/dx^3 over all corners (frmean) and over fluid corners (frmeanfluid).
+// ============================================================================
+__device__ __forceinline__ void inner_point(const Geo &g, int m, int l, double xli[3]) {
+    const int NB = g.nbody;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xli[d] = __dadd_rn(g.xc[m + d * NB], __dmul_rn(g.bnd[3 * l + d], g.ri));
+}
+
+__global__ void __launch_bounds__(256) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
+                                             const double *__restrict__ nlbc, const double *__restrict__ onlbc,
+                                             const double *__restrict__ diffn, const Scal *__restrict__ sc,
+                                             double *__restrict__ rec, double *__restrict__ blockpart) {
+    __shared__ double scr[32];
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double fm[3] = {0, 0, 0}, ffl[3] = {0, 0, 0};
+    if (p < g.npts && !sc->status) {
+        const int m = g.pt_m[p], l = g.pt_l[p], NB = g.nbody;
+        const size_t CR = (size_t)g.nx * g.RS;
+        double xli[3], xlo[3], xpi[3], snorm[3];
+        inner_point(g, m, l, xli);
+        double rad = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            xlo[d] = __dadd_rn(g.xc[m + d * NB], __dmul_rn(g.bnd[3 * l + d], g.ro));
+            const double a = __dmul_rn(g.bnd[3 * l + d], g.ri);
+            rad = __dadd_rn(rad, __dmul_rn(a, a));
+        }
+        rad = sqrt(rad);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) snorm[d] = __dmul_rn(g.bnd[3 * l + d], g.ri) / rad;
+        xpi[0] = __dsub_rn(xli[0], 0.5); xpi[1] = xli[1]; xpi[2] = xli[2];
+        Sten so, spi, si;
+        make_sten(g, xlo, so);
+        make_sten(g, xpi, spi);
+        make_sten(g, xli, si);
+        double ulo[3], ppll[3], uli[3], nll[3], onll[3], dfll[3];
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            ulo[n] = interp_kji(g, so, ubcp + n * CR);
+            ppll[n] = interp_kji(g, spi, pgr + n * CR, sc->mpg[n]);
+            uli[n] = interp_kji(g, si, ubcp + n * CR);
+            nll[n] = dot_ijk(g, si, nlbc + n * CR);
+            onll[n] = dot_ijk(g, si, onlbc + n * CR);
+            dfll[n] = dot_ijk(g, si, diffn + n * CR);
+        }
+        double linvel[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) linvel[d] = g.vel[m + d * NB];
+        double unmag = 0.0, ubnmag = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { unmag = unmag + snorm[d] * ulo[d]; ubnmag = ubnmag + snorm[d] * linvel[d]; }
+        const double ro = g.ro, ri = g.ri, rb = g.rb;
+        double ucar[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double unorm = snorm[d] * unmag, utang = ulo[d] - unorm;
+            const double ubnorm = snorm[d] * ubnmag, ubtang = linvel[d] - ubnorm;
+            double utangi = ubtang * (ro - ri) - utang * (rb - ri);
+            utangi = utangi / (ro - rb);
+            double unormi = 0.0;
+            if (g.revernorm == 1) { unormi = ubnorm * (ro - ri) - unorm * (rb - ri); unormi = unormi / (ro - rb); }
+            ucar[d] = utangi + unormi;
+        }
+        const double cf = sc->cf, c12 = g.c1 + g.c2, da2 = g.da2[m];
+        double ft[3];
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            double f = cf * (-ucar[n] + uli[n]);
+            f = f - g.c3 * nll[n] - g.c4 * onll[n];
+            f = f + c12 * (ppll[n] - dfll[n]);
+            ft[n] = f * da2 * g.dr * g.dx;
+        }
+        int count_fl = 0;
+        double force_fl[3] = {0, 0, 0};
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    const bool fl = g.fluid[(size_t)si.ii[a] * g.RS + (size_t)si.kk[c] * g.my + si.jj[b]] != 0;
+                    const double w = si.w(a, b, c);
+#pragma unroll
+                    for (int n = 0; n < 3; ++n) {
+                        const double t = (w * ft[n]) / g.dx3;
+                        if (fl) { force_fl[n] = force_fl[n] + t; ffl[n] += t; }
+                        fm[n] += t;
+                    }
+                    count_fl += fl ? 1 : 0;
+                }
+        const int count_so = 8 - count_fl;
+        double *r = rec + (size_t)p * 6;
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            r[n] = ft[n];
+            r[3 + n] = count_so > 0 ? force_fl[n] / (double)count_so : 0.0;
+        }
+    }
+    for (int n = 0; n < 3; ++n) {
+        const double a = block_sum(fm[n], scr), b = block_sum(ffl[n], scr);
+        if (threadIdx.x == 0) { blockpart[(size_t)blockIdx.x * 6 + n] = a; blockpart[(size_t)blockIdx.x * 6 + 3 + n] = b; }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *blockpart, int nblocks) {
+    __shared__ double scr[32];
+    if (sc->status) return;
+    for (int q = 0; q < 6; ++q) {
+        double a = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) a += blockpart[(size_t)b * 6 + q];
+        a = block_sum(a, scr);
+        if (threadIdx.x == 0) {
+            if (q < 3) sc->frmean[q] = a / (double)g.ncell;
+            else sc->frmeanfluid[q - 3] = a / (double)g.count_fluid;
+        }
+    }
+}
+
+// k_spread: fr at every forced node, accumulated over its (point, corner)
+// contributions in the reference's (sphere, point) order
+// (boundary_condition.F90:1425-1462).
+__global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, double *__restrict__ fr,
+                                                const Scal *__restrict__ sc) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.sp_nnodes || sc->status) return;
+    const int node = g.sp_node[q];
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int e = g.sp_ptr[q]; e < g.sp_ptr[q + 1]; ++e) {
+        const int ent = g.sp_ent[e];
+        const int p = ent >> 3, corner = ent & 7;
+        double xli[3];
+        inner_point(g, g.pt_m[p], g.pt_l[p], xli);
+        Sten s;
+        make_sten(g, xli, s);
+        const double w = s.w(corner & 1, (corner >> 1) & 1, (corner >> 2) & 1);
+        const double *r = rec + (size_t)p * 6;
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            const double t = (w * r[n]) / g.dx3;
+            if (g.include_frmeanfluid) acc[n] = acc[n] + t;
+            else acc[n] = (acc[n] + t) + r[3 + n];
+        }
+    }
+    const size_t CR = (size_t)g.nx * g.RS;
+#pragma unroll
+    for (int n = 0; n < 3; ++n) fr[n * CR + node] = acc[n];
+}
+
+// k_ff: ff = r2c(fr - frmean) (boundary_condition.F90:678-700).
+template <int N>
+__global__ void __launch_bounds__(PT<N>::T) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
+                                                 const Scal *__restrict__ sc) {
+    extern __shared__ double2 sm[];
+    double2 *buf = sm, *tws = sm + g.PS;
+    load_tw<N>(tws, g);
+    const int i = blockIdx.x;
+    const Tw tw{tws, N, 1};
+    const int nx = g.nx, PS = g.PS, RS = g.RS, my = g.my, my2 = g.my2;
+    for (int n = 0; n < 3; ++n) {
+        const double fmn = sc->frmean[n];
+        const double *src = fr + ((size_t)n * nx + i) * RS;
+        for (int e = threadIdx.x; e < RS; e += blockDim.x) {
+            const int k = e / my, j = e - k * my;
+            rv(buf, my2, k, j) = src[e] - fmn;
+        }
+        __syncthreads();
+        plane_r2c<N>(buf, g, tw);
+        double2 *dst = ff + ((size_t)n * nx + i) * PS;
+        for (int e = threadIdx.x; e < PS; e += blockDim.x) dst[e] = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
+        __syncthreads();
+    }
+}
+
+// ============================================================================
+// k_lines: pressure -> ustep -> divcorr for one (ky,kz) line per thread
+// (poisson.F90:55-508, usteptime.F90:45-269, tridiagonal.F90:47-150,
+//  check_divergence steptheflow.F90:219-240).
+// ============================================================================
+template <int NX>
+__device__ __forceinline__ bool thomas3(double a, const double *b, double c, const double *r1, const double *r2, const double *r3,
+                                        double *u1, double *u2, double *u3, double *gam, int n) {
+    double bet = b[0];
+    if (bet == 0.0) return false;
+    u1[0] = r1[0] / bet; u2[0] = r2[0] / bet; u3[0] = r3[0] / bet;
+    for (int j = 1; j < n; ++j) {
+        gam[j] = c / bet;
+        bet = b[j] - a * gam[j];
+        if (bet == 0.0) return false;
+        u1[j] = (r1[j] - a * u1[j - 1]) / bet;
+        u2[j] = (r2[j] - a * u2[j - 1]) / bet;
+        u3[j] = (r3[j] - a * u3[j - 1]) / bet;
+    }
+    for (int j = n - 2; j >= 0; --j) {
+        u1[j] = u1[j] - gam[j + 1] * u1[j + 1];
+        u2[j] = u2[j] - gam[j + 1] * u2[j + 1];
+        u3[j] = u3[j] - gam[j + 1] * u3[j + 1];
+    }
+    return true;
+}
+
+// Cyclic system with constant a (sub), c (super), diagonal bdiag, solved by
+// Sherman-Morrison with u = e_1 + e_n, v = (c/1, 0..0, a/1).
+template <int NX>
+__device__ __forceinline__ bool cyclic(double a, double bdiag, double c, const double *rr, const double *ri, double *outr, double *outi,
+                                       double *auxz, double *gam, double *bb, double *aux, int n) {
+    for (int i = 0; i < n; ++i) { bb[i] = bdiag; aux[i] = 0.0; }
+    aux[0] = 1.0; aux[n - 1] = 1.0;
+    const double v1 = c / aux[n - 1], vn = a / aux[0];
+    bb[0] = bb[0] - aux[0] * v1;
+    bb[n - 1] = bb[n - 1] - aux[n - 1] * vn;
+    if (!thomas3<NX>(a, bb, c, rr, aux, ri, outr, auxz, outi, gam, n)) return false;
+    const double vdotz = v1 * auxz[0] + vn * auxz[n - 1];
+    const double vdotyr = v1 * outr[0] + vn * outr[n - 1];
+    const double vdotyi = v1 * outi[0] + vn * outi[n - 1];
+    for (int i = 0; i < n; ++i) {
+        outr[i] = outr[i] - vdotyr * auxz[i] / (1.0 + vdotz);
+        outi[i] = outi[i] - vdotyi * auxz[i] / (1.0 + vdotz);
+    }
+    return true;
+}
+
+template <int NX>
+__global__ void __launch_bounds__(128) k_lines(Geo g, double2 *__restrict__ u, double2 *__restrict__ p,
+                                               const double2 *__restrict__ nl, const double2 *__restrict__ onl,
+                                               const double2 *__restrict__ ff, Scal *__restrict__ sc) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.PS || sc->status) return;
+    const int nx = NX, PS = g.PS;
+    const int k = q / g.my2, j = q - k * g.my2;
+    const double w2 = g.w2[q], ky = g.ky[j], kz = g.kz[k];
+    const double dx = g.dx, dx2 = g.dx2, dt = sc->dt, vis = g.vis;
+    const double c1 = g.c1, c2 = g.c2, c3 = g.c3, c4 = g.c4;
+    double dv[NX], dvi[NX], outr[NX], outi[NX], auxz[NX], gam[NX], bb[NX], aux[NX];
+    double2 P[NX];
+    auto at = [&](const double2 *f, int comp, int i) -> double2 {
+        i = i >= nx ? i - nx : (i < 0 ? i + nx : i);
+        return f[((size_t)comp * nx + i) * PS + q];
+    };
+    auto mulwy = [&](double2 z) { return make_double2(-ky * z.y, ky * z.x); };   // wy * z
+    auto mulwz = [&](double2 z) { return make_double2(-kz * z.y, kz * z.x); };
+    bool ok = true;
+    // ---------------- pressure (poisson.F90:55-239) ----------------
+    {
+        const double a = 1.0 / dx2 - 0.25 * w2, bd = -2.0 / dx2 - 0.5 * w2, c = 1.0 / dx2 - 0.25 * w2;
+        for (int i = 0; i < nx; ++i) {
+            double2 t = make_double2(0.0, 0.0);
+            double2 d, s;
+            d = csub(at(nl, 0, i + 1), at(nl, 0, i));
+            s = csub(at(ff, 0, i + 1), at(ff, 0, i));
+            t = make_double2(t.x + (c3 * d.x) / dx + s.x / dx, t.y + (c3 * d.y) / dx + s.y / dx);
+            d = mulwy(cadd(at(nl, 1, i + 1), at(nl, 1, i)));
+            s = mulwy(cadd(at(ff, 1, i + 1), at(ff, 1, i)));
+            t = make_double2(t.x + (c3 * d.x) / 2.0 + s.x / 2.0, t.y + (c3 * d.y) / 2.0 + s.y / 2.0);
+            d = mulwz(cadd(at(nl, 2, i + 1), at(nl, 2, i)));
+            s = mulwz(cadd(at(ff, 2, i + 1), at(ff, 2, i)));
+            t = make_double2(t.x + (c3 * d.x) / 2.0 + s.x / 2.0, t.y + (c3 * d.y) / 2.0 + s.y / 2.0);
+            d = csub(at(onl, 0, i + 1), at(onl, 0, i));
+            t = make_double2(t.x + (c4 * d.x) / dx, t.y + (c4 * d.y) / dx);
+            d = mulwy(cadd(at(onl, 1, i + 1), at(onl, 1, i)));
+            t = make_double2(t.x + (c4 * d.x) / 2.0, t.y + (c4 * d.y) / 2.0);
+            d = mulwz(cadd(at(onl, 2, i + 1), at(onl, 2, i)));
+            t = make_double2(t.x + (c4 * d.x) / 2.0, t.y + (c4 * d.y) / 2.0);
+            dv[i] = t.x / (c1 + c2);
+            dvi[i] = t.y / (c1 + c2);
+        }
+        if (q == 0) {
+            for (int i = 0; i < nx - 1; ++i) { bb[i] = bd; aux[i] = 0.0; }
+            ok = ok && thomas3<NX>(a, bb, c, dv, aux, dvi, outr, auxz, outi, gam, nx - 1);
+            outr[nx - 1] = 0.0;
+            for (int i = 0; i < nx; ++i) outi[i] = 0.0;
+        } else {
+            ok = ok && cyclic<NX>(a, bd, c, dv, dvi, outr, outi, auxz, gam, bb, aux, nx);
+        }
+        for (int i = 0; i < nx; ++i) {
+            const double2 po = p[(size_t)i * PS + q];
+            P[i] = make_double2(po.x + 1.0 * (outr[i] - po.x), po.y + 1.0 * (outi[i] - po.y));
+        }
+    }
+    // ---------------- ustep (usteptime.F90:45-269) ----------------
+    {
+        const double a = -(1.0 * dt * vis * c2 / dx2);
+        const double bd = 1.0 + dt * vis * c2 * (1.0 * 2.0 / dx2 + w2);
+        const double c = a;
+        const double alp = dt * (c1 + c2);
+        const double fy = 1.0 - dt * vis * c1 * w2;
+        const double gd = 1.0 * dt * vis * c1;
+        for (int n = 0; n < 3; ++n) {
+            for (int i = 0; i < nx; ++i) {
+                const double2 ui = at(u, n, i);
+                double2 r = make_double2(ui.x * fy, ui.y * fy);
+                const double2 nn = at(nl, n, i), f = at(ff, n, i), on = at(onl, n, i);
+                r = make_double2(r.x + (dt * c3) * nn.x + dt * f.x, r.y + (dt * c3) * nn.y + dt * f.y);
+                r = make_double2(r.x + (dt * c4) * on.x, r.y + (dt * c4) * on.y);
+                const double2 pm = P[i == 0 ? nx - 1 : i - 1], p0 = P[i];
+                double2 gp;
+                if (n == 0) gp = make_double2((alp * (p0.x - pm.x)) / dx, (alp * (p0.y - pm.y)) / dx);
+                else {
+                    const double2 s = make_double2(alp * 0.5 * (pm.x + p0.x), alp * 0.5 * (pm.y + p0.y));
+                    gp = (n == 1) ? mulwy(s) : mulwz(s);
+                }
+                r = csub(r, gp);
+                const double2 um = at(u, n, i - 1), up = at(u, n, i + 1);
+                double2 lap;
+                if (i == 0) lap = make_double2((up.x - 2.0 * ui.x) + um.x, (up.y - 2.0 * ui.y) + um.y);
+                else lap = make_double2((um.x + up.x) - 2.0 * ui.x, (um.y + up.y) - 2.0 * ui.y);
+                r = make_double2(r.x + (gd * lap.x) / dx2, r.y + (gd * lap.y) / dx2);
+                dv[i] = r.x; dvi[i] = r.y;
+            }
+            ok = ok && cyclic<NX>(a, bd, c, dv, dvi, outr, outi, auxz, gam, bb, aux, nx);
+            for (int i = 0; i < nx; ++i) u[((size_t)n * nx + i) * PS + q] = make_double2(outr[i], outi[i]);
+        }
+    }
+    // ---------------- divcorr (poisson.F90:241-508) ----------------
+    {
+        const double a = 1.0 / dx2 - 0.25 * w2, bd = -2.0 / dx2 - 0.5 * w2, c = 1.0 / dx2 - 0.25 * w2;
+        const double alp = (c1 + c2) * dt;
+        for (int i = 0; i < nx; ++i) {
+            const double2 u1p = at(u, 0, i + 1), u1 = at(u, 0, i);
+            double2 t = make_double2((u1p.x - u1.x) / dx, (u1p.y - u1.y) / dx);
+            t = cadd(t, mulwy(cscale(cadd(at(u, 1, i), at(u, 1, i + 1)), 0.5)));
+            t = cadd(t, mulwz(cscale(cadd(at(u, 2, i), at(u, 2, i + 1)), 0.5)));
+            dv[i] = (0.5 * (1.0 + 1.0) * t.x) / alp;
+            dvi[i] = (0.5 * (1.0 + 1.0) * t.y) / alp;
+        }
+        if (q == 0) {
+            for (int i = 0; i < nx - 1; ++i) { bb[i] = bd; aux[i] = 0.0; }
+            ok = ok && thomas3<NX>(a, bb, c, dv, aux, dvi, outr, auxz, outi, gam, nx - 1);
+            outr[nx - 1] = 0.0;
+            for (int i = 0; i < nx; ++i) outi[i] = 0.0;
+        } else {
+            ok = ok && cyclic<NX>(a, bd, c, dv, dvi, outr, outi, auxz, gam, bb, aux, nx);
+        }
+        // u -= grad(phi)
+        for (int i = 0; i < nx; ++i) {
+            const int im = i == 0 ? nx - 1 : i - 1;
+            const double2 d0 = make_double2(outr[i], outi[i]), dm = make_double2(outr[im], outi[im]);
+            double2 u1 = at(u, 0, i), u2 = at(u, 1, i), u3 = at(u, 2, i);
+            u1 = make_double2(u1.x - (alp * (d0.x - dm.x)) / dx, u1.y - (alp * (d0.y - dm.y)) / dx);
+            const double2 s = make_double2(dm.x + d0.x, dm.y + d0.y);
+            // i==0: alp*wy*half*(div(1)+div(nx)); else alp*half*wy*(div(i-1)+div(i))
+            const double2 gy = (i == 0) ? cscale(mulwy(make_double2(alp, 0.0)), 0.5) : mulwy(make_double2(alp * 0.5, 0.0));
+            const double2 gz = (i == 0) ? cscale(mulwz(make_double2(alp, 0.0)), 0.5) : mulwz(make_double2(alp * 0.5, 0.0));
+            u2 = csub(u2, cmul(gy, s));
+            u3 = csub(u3, cmul(gz, s));
+            u[((size_t)0 * nx + i) * PS + q] = u1;
+            u[((size_t)1 * nx + i) * PS + q] = u2;
+            u[((size_t)2 * nx + i) * PS + q] = u3;
+        }
+        const double c2dtv = (c2 * dt) * vis;
+        for (int i = 0; i < nx; ++i) {
+            const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
+            const double2 d0 = make_double2(outr[i], outi[i]), dm = make_double2(outr[im], outi[im]), dp = make_double2(outr[ip], outi[ip]);
+            const double2 lap = make_double2(((dm.x - 2.0 * d0.x) + dp.x) / dx2 - w2 * d0.x, ((dm.y - 2.0 * d0.y) + dp.y) / dx2 - w2 * d0.y);
+            const double2 pn = make_double2((P[i].x + d0.x) - c2dtv * lap.x, (P[i].y + d0.y) - c2dtv * lap.y);
+            p[(size_t)i * PS + q] = pn;
+        }
+        // check_divergence
+        double dmax = 0.0;
+        for (int i = 0; i < nx; ++i) {
+            const double2 u1p = at(u, 0, i + 1), u1 = at(u, 0, i);
+            double2 t = make_double2((u1p.x - u1.x) / dx, (u1p.y - u1.y) / dx);
+            t = cadd(t, mulwy(cscale(cadd(at(u, 1, i), at(u, 1, i + 1)), 0.5)));
+            t = cadd(t, mulwz(cscale(cadd(at(u, 2, i), at(u, 2, i + 1)), 0.5)));
+            dmax = fmax(dmax, sqrt(t.x * t.x + t.y * t.y));
+        }
+        atomicMax(&sc->divmax_bits, (unsigned long long)__double_as_longlong(dmax));
+    }
+    if (!ok) atomicCAS(&sc->status, 0, PIBM_ERR_PIVOT);
+}
+
+// velstep tail: umean update (steptheflow.F90:99) and the NaN check.
+__global__ void k_scal_d(Geo g, Scal *sc) {
+    if (threadIdx.x != 0 || sc->status) return;
+    for (int d = 0; d < 3; ++d) sc->umean[d] = sc->umean[d] + (-sc->mpg[d] + sc->frmean[d] - sc->frame_accln[d]) * sc->dt;
+    const double dm = __longlong_as_double((long long)sc->divmax_bits);
+    if (!(dm == dm) || !(sc->umean[0] == sc->umean[0]) || !(sc->mpg[0] == sc->mpg[0])) sc->status = PIBM_ERR_NAN;
+    sc->nsteps += 1;
+}
+
+// ============================================================================
+// Layout conversion between the reference's Fortran arrays and the device
+// layout (used only by get/set state): u(nx+1,my2,mz,ncomp) <-> [comp][i][k][j].
+// Tiled 32x32 transpose through shared memory.
+// ============================================================================
+__global__ void k_f2d(const double2 *__restrict__ f, double2 *__restrict__ d, int nx, int nxf, int PS, int ncomp) {
+    __shared__ double2 tile[32][33];
+    const int comp = blockIdx.z;
+    const int i0 = blockIdx.x * 32, e0 = blockIdx.y * 32;
+    const double2 *fc = f + (size_t)comp * PS * nxf;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int e = e0 + r, i = i0 + threadIdx.x;
+        if (e < PS && i < nx) tile[r][threadIdx.x] = fc[(size_t)e * nxf + i];
+    }
+    __syncthreads();
+    double2 *dc = d + (size_t)comp * PS * nx;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, e = e0 + threadIdx.x;
+        if (e < PS && i < nx) dc[(size_t)i * PS + e] = tile[threadIdx.x][r];
+    }
+}
+__global__ void k_d2f(const double2 *__restrict__ d, double2 *__restrict__ f, int nx, int nxf, int PS, int ncomp) {
+    __shared__ double2 tile[32][33];
+    const int comp = blockIdx.z;
+    const int i0 = blockIdx.x * 32, e0 = blockIdx.y * 32;
+    const double2 *dc = d + (size_t)comp * PS * nx;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, e = e0 + threadIdx.x;
+        if (e < PS && i < nxf) tile[r][threadIdx.x] = dc[(size_t)(i == nx ? 0 : i) * PS + e];
+    }
+    __syncthreads();
+    double2 *fc = f + (size_t)comp * PS * nxf;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int e = e0 + r, i = i0 + threadIdx.x;
+        if (e < PS && i < nxf) fc[(size_t)e * nxf + i] = tile[threadIdx.x][r];
+    }
+}
+
+// Standalone batched plane transforms (pibm_ff2rc / pibm_ff2cr), planes contiguous.
+template <int N>
+__global__ void __launch_bounds__(PT<N>::T) k_ff2cr(Geo g, const double2 *__restrict__ a, double *__restrict__ b) {
+    extern __shared__ double2 sm[];
+    double2 *buf = sm, *tws = sm + g.PS;
+    load_tw<N>(tws, g);
+    const Tw tw{tws, N, 1};
+    const size_t q = blockIdx.x;
+    for (int e = threadIdx.x; e < g.PS; e += blockDim.x) buf[e] = a[q * g.PS + e];
+    __syncthreads();
+    plane_c2r<N>(buf, g, tw);
+    for (int e = threadIdx.x; e < g.RS; e += blockDim.x) { const int k = e / g.my, j = e - k * g.my; b[q * g.RS + e] = rv(buf, g.my2, k, j); }
+}
+template <int N>
+__global__ void __launch_bounds__(PT<N>::T) k_ff2rc(Geo g, const double *__restrict__ a, double2 *__restrict__ b) {
+    extern __shared__ double2 sm[];
+    double2 *buf = sm, *tws = sm + g.PS;
+    load_tw<N>(tws, g);
+    const Tw tw{tws, N, 1};
+    const size_t q = blockIdx.x;
+    for (int e = threadIdx.x; e < g.RS; e += blockDim.x) { const int k = e / g.my, j = e - k * g.my; rv(buf, g.my2, k, j) = a[q * g.RS + e]; }
+    __syncthreads();
+    plane_r2c<N>(buf, g, tw);
+    for (int e = threadIdx.x; e < g.PS; e += blockDim.x) b[q * g.PS + e] = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
+}
+
+// ============================================================================
+// Host-side launch helpers
+// ============================================================================
+
+template <int N>
+static size_t plane_smem(const Geo &g) { return (size_t)(g.PS + N) * sizeof(double2); }
+
+template <int N>
+static cudaError_t set_attrs() {
+    const int maxs = (int)((size_t)(((N / 2 + 1) * N) + N) * sizeof(double2));
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_a0<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_nl<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_fields<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_ff<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_ff2cr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_ff2rc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+cudaError_t configure_kernels(int n) {
+    switch (n) {
+        case 32: return set_attrs<32>();
+        case 64: return set_attrs<64>();
+        case 96: return set_attrs<96>();
+        case 128: return set_attrs<128>();
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+bool supported_size(int n) { return n == 32 || n == 64 || n == 96 || n == 128; }
+
+// Enqueue one full step on stream s.  cur = index of the nl/nlbc buffers that
+// receive this step's nonlinear term (the other holds the previous step's).
+template <int N>
+static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s) {
+    const size_t sm = plane_smem<N>(g);
+    constexpr int T = PT<N>::T;
+    const int old = 1 - cur;
+    k_a0<N><<<g.nx, T, sm, s>>>(g, b.u, b.p, b.ubcp, b.pbcp, b.sc, b.part);
+    k_scal_a<<<1, 32, 0, s>>>(g, b.sc, b.part);
+    k_nl<N><<<g.nx, T, sm, s>>>(g, b.ubcp, b.nl[cur], b.nlbc[cur], b.sc);
+    if (g.nbody > 0) {
+        k_fields<N><<<g.nx, T, sm, s>>>(g, b.u, b.p, b.ubcp, b.diffn, b.omega, b.pgr);
+        k_drag<<<g.nbody, 256, 0, s>>>(g, b.pbcp, b.omega, b.pres, b.visc, b.ptot, b.sc);
+        k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force);
+        const int nbk = (g.npts + 255) / 256;
+        if (g.npts > 0) {
+            k_rev<<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.nlbc[cur], b.nlbc[old], b.diffn, b.sc, b.rec, b.blockpart);
+            k_scal_c<<<1, 256, 0, s>>>(g, b.sc, b.blockpart, nbk);
+            if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.fr, b.sc);
+        }
+        k_ff<N><<<g.nx, T, sm, s>>>(g, b.fr, b.ff, b.sc);
+    }
+    k_lines<N><<<(g.PS + 127) / 128, 128, 0, s>>>(g, b.u, b.p, b.nl[cur], b.nl[old], b.ff, b.sc);
+    k_scal_d<<<1, 32, 0, s>>>(g, b.sc);
+}
+
+void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s) {
+    switch (g.my) {
+        case 32: enqueue_step_t<32>(g, b, cur, s); break;
+        case 64: enqueue_step_t<64>(g, b, cur, s); break;
+        case 96: enqueue_step_t<96>(g, b, cur, s); break;
+        case 128: enqueue_step_t<128>(g, b, cur, s); break;
+    }
+}
+
+// nlbc of a given spectral nl (used after set_state to rebuild the AB2 history).
+template <int N>
+static void enqueue_c2r_t(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s) {
+    k_ff2cr<N><<<nplanes, PT<N>::T, plane_smem<N>(g), s>>>(g, a, b);
+}
+void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s) {
+    switch (g.my) {
+        case 32: enqueue_c2r_t<32>(g, a, b, nplanes, s); break;
+        case 64: enqueue_c2r_t<64>(g, a, b, nplanes, s); break;
+        case 96: enqueue_c2r_t<96>(g, a, b, nplanes, s); break;
+        case 128: enqueue_c2r_t<128>(g, a, b, nplanes, s); break;
+    }
+}
+template <int N>
+static void enqueue_r2c_t(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s) {
+    k_ff2rc<N><<<nplanes, PT<N>::T, plane_smem<N>(g), s>>>(g, a, b);
+}
+void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s) {
+    switch (g.my) {
+        case 32: enqueue_r2c_t<32>(g, a, b, nplanes, s); break;
+        case 64: enqueue_r2c_t<64>(g, a, b, nplanes, s); break;
+        case 96: enqueue_r2c_t<96>(g, a, b, nplanes, s); break;
+        case 128: enqueue_r2c_t<128>(g, a, b, nplanes, s); break;
+    }
+}
+
+void enqueue_f2d(const double2 *f, double2 *d, int nx, int nxf, int PS, int ncomp, cudaStream_t s) {
+    dim3 grid((nx + 31) / 32, (PS + 31) / 32, ncomp);
+    k_f2d<<<grid, dim3(32, 8), 0, s>>>(f, d, nx, nxf, PS, ncomp);
+}
+void enqueue_d2f(const double2 *d, double2 *f, int nx, int nxf, int PS, int ncomp, cudaStream_t s) {
+    dim3 grid((nxf + 31) / 32, (PS + 31) / 32, ncomp);
+    k_d2f<<<grid, dim3(32, 8), 0, s>>>(d, f, nx, nxf, PS, ncomp);
+}
+
+}  // namespace pibm
