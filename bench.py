@@ -1,0 +1,320 @@
+"""Benchmark: Mcell-steps/s (FP64) of the per-step Navier-Stokes + IBM hot path.
+
+Workload (one GPU): fixed random sphere array, 128^3 grid, 100 spheres of
+diameter 20 cells (volume fraction 0.2), Re = 50, upwind x-flux, positions from
+seeded random sequential addition followed by 1000 hard-sphere Monte Carlo
+moves.  A step is one rks iteration: compute_new_timestep -> nonlinear ->
+bcset -> velstep.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (the step has no in-realization exchange),
+one process per GPU under torch.distributed.run; value = all ranks' cell-steps
+over the max-over-ranks device time.  ``--impl reference`` times the CPU
+restatement of the reference step on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s FP64 at 128³ φ=0.2"
+UNIT = "Mcell-steps/s"
+WORKLOAD = dict(my=128, dia_cells=20.0, phi=0.2, re=50.0, seed=1234, mc_moves=1000)
+PEAK_FALLBACK_GBS = 6650.0
+
+# Algorithmic bytes per launch of each plane/line kernel, in units of one
+# complex spectral field F_c = nx*my2*mz*16 B and one real field F_r = nx*my*mz*8 B:
+# compulsory reads + writes of whole fields.
+KERNEL_BYTES = {
+    "a0_u_p_to_real": (4, 4),     # read u(3), p; write ubcp(3), pbcp
+    "nonlinear": (3, 6),          # read ubcp(3); write nl(3), nlbc(3)
+    "ibm_fields": (4, 11),        # read u(3), p, ubcp(2); write diffn(3), omega(3), grad p(3)
+    "forcing_fft": (3, 3),        # read fr(3); write ff(3)
+    "x_lines": (17, 0),           # read u(3), p, nl(3), onl(3), ff(3); write u(3), p
+}
+KERNEL_NAMES = {
+    "a0_u_p_to_real": "k_a0", "nonlinear": "k_nl", "ibm_fields": "k_fields", "drag_mpg": "k_drag",
+    "reversal_spread": "k_rev", "forcing_fft": "k_ff", "x_lines": "k_lines",
+}
+
+
+def _peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+def _workload():
+    from pureibm_ps2d_fd1d_b200 import config
+    prm, xc = config.random_array(**WORKLOAD)
+    return prm, xc
+
+
+def _config_dict(n_gpus, xc, prm):
+    return {
+        "workload": "fixed random sphere array 128^3, %d spheres d=20 (phi=0.2), Re=50, upwind, AB2" % len(xc),
+        "grid": [prm["my"], prm["my"], prm["my"]],
+        "nbody": int(len(xc)),
+        "parallelism": "replicas%d" % n_gpus if n_gpus > 1 else "single",
+        "l2": "working set ~0.45 GB per replica > 126 MB L2 (no flush needed)",
+        "seed": WORKLOAD["seed"],
+    }
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = str(gpu_index)
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu, "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(prm, xc, steps=2, warmup=1, threads=None):
+    """The oracle (CPU restatement of the reference step) on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_ctypes as oc
+    from pureibm_ps2d_fd1d_b200 import config
+    threads = threads or os.cpu_count() or 1
+    oc.set_threads(threads)
+    P = config.make_params(prm)
+    parts = config.Particles(xc)
+    s = oc.OracleSolver(P, parts.struct)
+    for _ in range(warmup):
+        s.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step()
+    el = time.perf_counter() - t0
+    ncell = s.nx * s.my * s.mz
+    s.close()
+    return {"value": ncell * steps / el / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "%d steps (after %d warm-up) of the same 128^3 workload, oracle on %d threads" % (steps, warmup, threads),
+            "s_per_step": el / steps}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    prm, xc = _workload()
+    threads = os.cpu_count() or 1
+    steps = max(1, args.steps)
+    cb = cpu_baseline(prm, xc, steps=steps, warmup=max(0, min(args.warmup, 1)), threads=threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": cb["s_per_step"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded sphere positions)", "config": _config_dict(1, xc, prm),
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_gpu(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    import numpy as np
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import pureibm_ps2d_fd1d_b200 as pk
+    from pureibm_ps2d_fd1d_b200 import config, abi
+
+    prm, xc = _workload()
+    s = pk.Solver(config.make_params(prm), xc)
+    ncell = s.nx * s.my * s.mz
+    # warm-up (graph path) then the timed region with per-phase events on the engine's stream
+    s.run(max(args.warmup, 3))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    import ctypes as C
+    lib = pk.load_library()
+    rep = abi.pibm_step_report()
+    total = C.c_double()
+    phases = (C.c_double * abi.PIBM_NPHASE)()
+    barrier()
+    with ClockSampler(local if world > 1 else 0) as clk:
+        rc = lib.pibm_run_profiled(s.h, args.steps, C.byref(rep), C.byref(total), phases, abi.PIBM_NPHASE)
+    barrier()
+    if rc != 0:
+        raise RuntimeError("pibm_run_profiled failed: %d %s" % (rc, lib.pibm_last_error().decode()))
+    t_ms = total.value
+    if dist:
+        tt = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = ncell * args.steps * world / (t_ms / 1e3) / 1e6
+    phase_ms = {abi.PHASE_NAMES[q]: phases[q] / args.steps for q in range(abi.PIBM_NPHASE)}
+
+    # end-to-end through the C ABI with host buffers: every step uploads the
+    # state (u, nl, p in the reference layout) from pinned memory, steps, and
+    # downloads it again.
+    nx, my2, mz = s.nx, s.my2, s.mz
+    shp_u, shp_p = (3, mz, my2, nx + 1), (mz, my2, nx)
+    pin = lambda shp: torch.empty(tuple(shp) + (2,), dtype=torch.float64).pin_memory()
+    hu, hnl, hp = pin(shp_u), pin(shp_u), pin(shp_p)
+    view = abi.pibm_state_view()
+    view.u = C.cast(hu.data_ptr(), C.POINTER(C.c_double))
+    view.nl = C.cast(hnl.data_ptr(), C.POINTER(C.c_double))
+    view.p = C.cast(hp.data_ptr(), C.POINTER(C.c_double))
+    assert lib.pibm_get_state(s.h, C.byref(view)) == 0
+    e2e_steps = max(1, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        assert lib.pibm_set_state(s.h, C.byref(view)) == 0
+        assert lib.pibm_step(s.h, 1, C.byref(rep)) == 0
+        assert lib.pibm_get_state(s.h, C.byref(view)) == 0
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    bytes_state = (hu.numel() + hnl.numel() + hp.numel()) * 8
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
+    peak, peak_kind = _peak_gbs()
+    Fc = nx * my2 * mz * 16
+    Fr = nx * s.my * mz * 8
+    dominant = max(KERNEL_BYTES, key=lambda k: phase_ms[k])
+    nc, nr = KERNEL_BYTES[dominant]
+    alg = nc * Fc + nr * Fr
+    achieved = alg / (phase_ms[dominant] / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as fh:
+            tr = json.load(fh)
+        ent = tr.get(KERNEL_NAMES[dominant])
+        if ent:
+            traffic = float(ent["bytes_per_launch_at_128"])
+    except Exception:
+        pass
+    b_alg_step = 30 * Fc
+    info = s.info
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded sphere positions, fluid initially at rest)",
+        "config": _config_dict(world, xc, prm),
+        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dominant], "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg},
+        "step_roofline": {"algorithmic_bytes_per_step": b_alg_step,
+                          "achieved_GBps": b_alg_step / (t_ms / args.steps / 1e3) / 1e9,
+                          "frac": b_alg_step / (t_ms / args.steps / 1e3) / 1e9 / peak},
+        "phase_ms_per_step": phase_ms,
+        "e2e": {"value": ncell * e2e_steps * world / e2e_s / 1e6, "unit": UNIT,
+                "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state + C.sizeof(rep),
+                "path": "pibm_set_state(pinned host) + pibm_step + pibm_get_state(pinned host) per step"},
+        "gpu_launches": int(info.kernels_per_step) * args.steps,
+        "clocks": clk.summary(),
+        "active_reversal_points": int(info.npts_active),
+        "maxvolfrac": info.maxvolfrac,
+        "last_step": {"divmax": rep.divmax, "norm_drag": rep.norm_drag, "dt": rep.dt},
+    }
+    if not args.no_cpu_baseline and world == 1:
+        cb = cpu_baseline(prm, xc, steps=2, warmup=1)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

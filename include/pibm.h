@@ -127,6 +127,8 @@ typedef struct pibm_info {
     int32_t nx, my, mz, my2, nbody, nbnd;
     double  dx, dt, radbdy, maxvolfrac;
     int64_t count_solid, count_fluid;
+    int32_t npts_active;       /* active reversal points over all spheres     */
+    int32_t kernels_per_step;  /* kernels one step launches                   */
 } pibm_info;
 
 typedef struct pibm_handle pibm_handle;
@@ -146,6 +148,13 @@ int  pibm_set_state(pibm_handle *h, const pibm_state_view *s);
 int  pibm_step(pibm_handle *h, int rks, pibm_step_report *rep);
 /* nsteps steps without per-step host synchronisation (graph-launched). */
 int  pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last);
+/* nsteps steps launched without graphs, timed with CUDA events recorded on
+ * the handle's stream: *total_ms = first-to-last event time; phase_ms[q]
+ * (q < nphase <= PIBM_NPHASE) = summed duration of phase q over the steps.
+ * One host synchronisation at the end. */
+#define PIBM_NPHASE 7   /* 0 u,p->real  1 nonlinear  2 IBM fields  3 drag+mpg  4 reversal+spread  5 forcing FFT  6 x-lines */
+int  pibm_run_profiled(pibm_handle *h, int nsteps, pibm_step_report *last,
+                       double *total_ms, double *phase_ms, int nphase);
 int  pibm_get_state(pibm_handle *h, pibm_state_view *s);
 /* pres, visc, force: (nbody,3) column-major, as global_data.F90:115-117;
  * xc, vel: positions (grid units) and velocities.  Any pointer may be NULL. */

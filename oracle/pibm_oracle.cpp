@@ -1214,6 +1214,9 @@ int orc_info(void *h, pibm_info *info) {
     info->nx = o.nx; info->my = o.my; info->mz = o.mz; info->my2 = o.my2; info->nbody = o.nbody; info->nbnd = o.nbnd;
     info->dx = o.dx; info->dt = o.dt; info->radbdy = o.nbody ? o.radbdy[0] : 0.0; info->maxvolfrac = o.maxvolfrac;
     info->count_solid = o.count_solid; info->count_fluid = o.count_fluid;
+    long long s = 0; for (int v : o.nrpr_active) s += v;
+    info->npts_active = (int32_t)s;
+    info->kernels_per_step = 0;
     return PIBM_OK;
 }
 

@@ -32,6 +32,8 @@ PIBM_SCHEME_CENTER = 0
 PIBM_SCHEME_UPWIND = 1
 PIBM_LIMITER_NONE = 0
 PIBM_LIMITER_MINMOD = 1
+PIBM_NPHASE = 7
+PHASE_NAMES = ["a0_u_p_to_real", "nonlinear", "ibm_fields", "drag_mpg", "reversal_spread", "forcing_fft", "x_lines"]
 
 _i32 = C.c_int32
 _f64 = C.c_double
@@ -91,13 +93,14 @@ class pibm_info(C.Structure):
         ("nx", _i32), ("my", _i32), ("mz", _i32), ("my2", _i32), ("nbody", _i32), ("nbnd", _i32),
         ("dx", _f64), ("dt", _f64), ("radbdy", _f64), ("maxvolfrac", _f64),
         ("count_solid", C.c_int64), ("count_fluid", C.c_int64),
+        ("npts_active", _i32), ("kernels_per_step", _i32),
     ]
 
 
 # Exported symbols of libpibm (declared in include/pibm.h).
 EXPORTED = [
     "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run",
-    "pibm_get_state", "pibm_get_particles", "pibm_get_if_rev", "pibm_get_fluid_mask",
+    "pibm_run_profiled", "pibm_get_state", "pibm_get_particles", "pibm_get_if_rev", "pibm_get_fluid_mask",
     "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
     "pibm_batch_create", "pibm_batch_run", "pibm_batch_member", "pibm_batch_destroy",
 ]
@@ -113,6 +116,7 @@ def bind(lib):
     lib.pibm_step.argtypes = [vp, C.c_int, P(pibm_step_report)]
     lib.pibm_run.argtypes = [vp, C.c_int, P(pibm_step_report)]
     lib.pibm_get_state.argtypes = [vp, P(pibm_state_view)]
+    lib.pibm_run_profiled.argtypes = [vp, C.c_int, P(pibm_step_report), P(_f64), P(_f64), C.c_int]
     lib.pibm_get_particles.argtypes = [vp] + [P(_f64)] * 5
     lib.pibm_get_if_rev.argtypes = [vp, P(C.c_uint8)]
     lib.pibm_get_fluid_mask.argtypes = [vp, P(C.c_uint8)]
@@ -128,7 +132,7 @@ def bind(lib):
     lib.pibm_batch_member.restype = vp
     lib.pibm_batch_destroy.argtypes = [vp]
     lib.pibm_batch_destroy.restype = None
-    for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run",
+    for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_profiled",
                  "pibm_get_state", "pibm_get_particles", "pibm_get_if_rev", "pibm_get_fluid_mask",
                  "pibm_ff2rc", "pibm_ff2cr", "pibm_batch_create", "pibm_batch_run"):
         getattr(lib, name).restype = C.c_int

@@ -20,7 +20,8 @@
 namespace pibm {
 cudaError_t configure_kernels(int n);
 bool supported_size(int n);
-void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s);
+void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev);
+int kernels_per_step(const Geo &g);
 void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s);
 void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s);
 void enqueue_f2d(const double2 *f, double2 *d, int nx, int nxf, int PS, int ncomp, cudaStream_t s);
@@ -166,6 +167,8 @@ int pibm_info_get(pibm_handle *h, pibm_info *info) {
     info->nx = S.nx; info->my = S.my; info->mz = S.mz; info->my2 = S.my2; info->nbody = S.nbody; info->nbnd = S.nbnd;
     info->dx = S.dx; info->dt = S.dt; info->radbdy = S.radbdy; info->maxvolfrac = S.maxvolfrac;
     info->count_solid = S.count_solid; info->count_fluid = S.count_fluid;
+    info->npts_active = (int32_t)S.pt_m.size();
+    info->kernels_per_step = kernels_per_step(h->g);
     return PIBM_OK;
 }
 
@@ -197,7 +200,7 @@ static int fill_report(pibm_handle *h, pibm_step_report *rep) {
 int pibm_step(pibm_handle *h, int rks, pibm_step_report *rep) {
     if (!h) return fail(PIBM_ERR_ARG, "null handle");
     if (rks != 1) return fail(PIBM_ERR_ARG, "AB2 has a single sub-step (rks = 1)");
-    enqueue_step(h->g, h->b, h->cur, h->stream);
+    enqueue_step(h->g, h->b, h->cur, h->stream, nullptr);
     CUDA_OR_FAIL(cudaGetLastError());
     h->cur ^= 1;
     return fill_report(h, rep);
@@ -209,7 +212,7 @@ int pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last) {
         if (h->graph[par]) continue;
         cudaGraph_t gr;
         CUDA_OR_FAIL(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_step(h->g, h->b, par, h->stream);
+        enqueue_step(h->g, h->b, par, h->stream, nullptr);
         CUDA_OR_FAIL(cudaStreamEndCapture(h->stream, &gr));
         CUDA_OR_FAIL(cudaGraphInstantiate(&h->graph[par], gr, 0));
         cudaGraphDestroy(gr);
@@ -218,6 +221,32 @@ int pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last) {
         CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], h->stream));
         h->cur ^= 1;
     }
+    return fill_report(h, last);
+}
+
+int pibm_run_profiled(pibm_handle *h, int nsteps, pibm_step_report *last, double *total_ms, double *phase_ms, int nphase) {
+    if (!h || nsteps <= 0 || nphase < 0 || nphase > PIBM_NPHASE) return fail(PIBM_ERR_ARG, "bad argument");
+    std::vector<cudaEvent_t> ev((size_t)nsteps * (PIBM_NPHASE + 1));
+    for (auto &e : ev) CUDA_OR_FAIL(cudaEventCreate(&e));
+    for (int s = 0; s < nsteps; ++s) {
+        enqueue_step(h->g, h->b, h->cur, h->stream, &ev[(size_t)s * (PIBM_NPHASE + 1)]);
+        h->cur ^= 1;
+    }
+    CUDA_OR_FAIL(cudaGetLastError());
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    for (int q = 0; q < nphase; ++q) phase_ms[q] = 0.0;
+    for (int s = 0; s < nsteps; ++s)
+        for (int q = 0; q < nphase; ++q) {
+            float ms = 0.f;
+            CUDA_OR_FAIL(cudaEventElapsedTime(&ms, ev[(size_t)s * (PIBM_NPHASE + 1) + q], ev[(size_t)s * (PIBM_NPHASE + 1) + q + 1]));
+            phase_ms[q] += ms;
+        }
+    if (total_ms) {
+        float ms = 0.f;
+        CUDA_OR_FAIL(cudaEventElapsedTime(&ms, ev.front(), ev.back()));
+        *total_ms = ms;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
     return fill_report(h, last);
 }
 

@@ -152,18 +152,26 @@ __global__ void __launch_bounds__(PT<N>::T) k_a0(Geo g, const double2 *__restric
 }
 
 // compute_new_timestep's scalar tail (dependent_functions.F90:1137-1280).
-__global__ void k_scal_a(Geo g, Scal *sc, const double *part) {
-    if (threadIdx.x != 0 || sc->status) return;
-    double uf[3] = {0, 0, 0}, mx[3] = {kSmallD, kSmallD, kSmallD};
-    for (int i = 0; i < g.nx; ++i)
-        for (int d = 0; d < 3; ++d) { uf[d] += part[(size_t)i * 12 + d]; mx[d] = fmax(mx[d], part[(size_t)i * 12 + 9 + d]); }
-    const double umax = fmax(fmax(mx[0], mx[1]), mx[2]);
+__global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *part) {
+    __shared__ double scr[32];
+    __shared__ double red[6];
+    if (sc->status) return;
+    for (int d = 0; d < 3; ++d) {
+        double a = 0.0, m = kSmallD;
+        for (int i = threadIdx.x; i < g.nx; i += blockDim.x) { a += part[(size_t)i * 12 + d]; m = fmax(m, part[(size_t)i * 12 + 9 + d]); }
+        a = block_sum(a, scr);
+        m = block_max(m, scr);
+        if (threadIdx.x == 0) { red[d] = a; red[3 + d] = m; }
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const double umax = fmax(fmax(red[3], red[4]), red[5]);
     sc->umax = umax;
     double dtnew = sc->dt;
     if (umax * sc->dt / g.dx > g.cfl_max) dtnew = g.cfl_max * g.dx / umax;
     for (int d = 0; d < 3; ++d) {
         sc->ufmean_old[d] = sc->ufmean[d];
-        sc->ufmean[d] = uf[d] / (double)g.count_fluid;
+        sc->ufmean[d] = red[d] / (double)g.count_fluid;
         sc->dufmeandt[d] = -sc->cf * (sc->ufmean[d] - sc->ufmean_old[d]);
     }
     double ms[3];
@@ -707,201 +715,270 @@ __global__ void __launch_bounds__(PT<N>::T) k_ff(Geo g, const double *__restrict
 }
 
 // ============================================================================
-// k_lines: pressure -> ustep -> divcorr for one (ky,kz) line per thread
-// (poisson.F90:55-508, usteptime.F90:45-269, tridiagonal.F90:47-150,
-//  check_divergence steptheflow.F90:219-240).
+// k_lines: pressure -> ustep -> divcorr for a tile of LT (ky,kz) lines per CTA
+// (poisson.F90:55-508, usteptime.F90:45-269, check_divergence
+// steptheflow.F90:219-240).
+//
+// Every cyclic system of velstep has constant coefficients (a = c, b on every
+// row, periodic coupling), i.e. it is a symmetric circulant matrix; the
+// reference solves it with Thomas + Sherman-Morrison (tridiagonal.F90:90-150,
+// usteptime.F90:344-349,457-468).  Here one warp solves one line exactly
+// through its eigen-decomposition: forward FFT along x in registers
+// (group_fft), division by N*lambda_m with lambda_m = b + 2a cos(2 pi m/N),
+// and the exact inverse of the forward stages.  The (ky,kz) = (0,0) line is
+// not circulant (nx-1 unknowns, p(nx) = 0: poisson.F90:127-142, 309-325) and
+// keeps the reference's Thomas recursion.
+// Tiles live in shared memory as [line][i]; global loads and stores run over
+// consecutive lines (contiguous in the [i][k][j] layout).
 // ============================================================================
-template <int NX>
-__device__ __forceinline__ bool thomas3(double a, const double *b, double c, const double *r1, const double *r2, const double *r3,
-                                        double *u1, double *u2, double *u3, double *gam, int n) {
-    double bet = b[0];
+template <int R>
+__device__ __forceinline__ void circulant_solve(double2 *row, double a, double b, const Tw &tw, int lane) {
+    constexpr int N = R * 32;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = row[lane + 32 * r];
+    group_fft<R, 32>(v, lane, -1.0, tw);
+    const int br = bitrev<32>(lane);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int m = r + R * br;
+        const double lam = ((double)N) * (b + 2.0 * a * tw.t[m * tw.stride].x);
+        v[r] = make_double2(v[r].x / lam, v[r].y / lam);
+    }
+    // exact inverse of group_fft's stages (unnormalised; 1/N folded into lam)
+#pragma unroll
+    for (int h = 1; h < 32; h <<= 1) {
+        const bool upper = (lane & h) == 0;
+        const int q = lane & (h - 1);
+        const double2 w = tw.get(q * (N / (2 * h)), +1.0);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const double2 pv = shfl_xor2(v[r], h, 32);
+            v[r] = upper ? cadd(v[r], cmul(pv, w)) : csub(pv, cmul(v[r], w));
+        }
+    }
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw.get((lane * r) % N, +1.0));
+    dft_inlane<R>(v, +1.0, tw);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; ++r) row[lane + 32 * r] = v[r];
+    __syncwarp();
+}
+
+// Thomas recursion (tridag, tridiagonal.F90:47-87) on the real parts of
+// row[0..n-1]; constant a, b, c; result in row[].x, row[].y = 0, row[n] = 0.
+__device__ __forceinline__ bool thomas_real(double2 *row, double *gam, double a, double b, double c, int n) {
+    double bet = b;
     if (bet == 0.0) return false;
-    u1[0] = r1[0] / bet; u2[0] = r2[0] / bet; u3[0] = r3[0] / bet;
+    double prev = row[0].x / bet;
+    row[0] = make_double2(prev, 0.0);
     for (int j = 1; j < n; ++j) {
         gam[j] = c / bet;
-        bet = b[j] - a * gam[j];
+        bet = b - a * gam[j];
         if (bet == 0.0) return false;
-        u1[j] = (r1[j] - a * u1[j - 1]) / bet;
-        u2[j] = (r2[j] - a * u2[j - 1]) / bet;
-        u3[j] = (r3[j] - a * u3[j - 1]) / bet;
+        prev = (row[j].x - a * prev) / bet;
+        row[j] = make_double2(prev, 0.0);
     }
-    for (int j = n - 2; j >= 0; --j) {
-        u1[j] = u1[j] - gam[j + 1] * u1[j + 1];
-        u2[j] = u2[j] - gam[j + 1] * u2[j + 1];
-        u3[j] = u3[j] - gam[j + 1] * u3[j + 1];
-    }
+    for (int j = n - 2; j >= 0; --j) row[j].x = row[j].x - gam[j + 1] * row[j + 1].x;
+    row[n] = make_double2(0.0, 0.0);
     return true;
 }
 
-// Cyclic system with constant a (sub), c (super), diagonal bdiag, solved by
-// Sherman-Morrison with u = e_1 + e_n, v = (c/1, 0..0, a/1).
-template <int NX>
-__device__ __forceinline__ bool cyclic(double a, double bdiag, double c, const double *rr, const double *ri, double *outr, double *outi,
-                                       double *auxz, double *gam, double *bb, double *aux, int n) {
-    for (int i = 0; i < n; ++i) { bb[i] = bdiag; aux[i] = 0.0; }
-    aux[0] = 1.0; aux[n - 1] = 1.0;
-    const double v1 = c / aux[n - 1], vn = a / aux[0];
-    bb[0] = bb[0] - aux[0] * v1;
-    bb[n - 1] = bb[n - 1] - aux[n - 1] * vn;
-    if (!thomas3<NX>(a, bb, c, rr, aux, ri, outr, auxz, outi, gam, n)) return false;
-    const double vdotz = v1 * auxz[0] + vn * auxz[n - 1];
-    const double vdotyr = v1 * outr[0] + vn * outr[n - 1];
-    const double vdotyi = v1 * outi[0] + vn * outi[n - 1];
-    for (int i = 0; i < n; ++i) {
-        outr[i] = outr[i] - vdotyr * auxz[i] / (1.0 + vdotz);
-        outi[i] = outi[i] - vdotyi * auxz[i] / (1.0 + vdotz);
-    }
-    return true;
-}
-
-template <int NX>
-__global__ void __launch_bounds__(128) k_lines(Geo g, double2 *__restrict__ u, double2 *__restrict__ p,
-                                               const double2 *__restrict__ nl, const double2 *__restrict__ onl,
-                                               const double2 *__restrict__ ff, Scal *__restrict__ sc) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= g.PS || sc->status) return;
-    const int nx = NX, PS = g.PS;
-    const int k = q / g.my2, j = q - k * g.my2;
-    const double w2 = g.w2[q], ky = g.ky[j], kz = g.kz[k];
+template <int NX, int LT>
+__global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ u, double2 *__restrict__ p,
+                                                   const double2 *__restrict__ nl, const double2 *__restrict__ onl,
+                                                   const double2 *__restrict__ ff, Scal *__restrict__ sc) {
+    constexpr int R = NX / 32;
+    extern __shared__ double2 sm[];
+    double2 *tws = sm;
+    double2 *RHS = tws + NX;
+    double2 *P = RHS + LT * NX;
+    double2 *U = P + LT * NX;                 // [comp][line][i]
+    double *gam = (double *)(U + 3 * LT * NX);
+    if (sc->status) return;
+    for (int t = threadIdx.x; t < NX; t += blockDim.x) tws[t] = g.tw[t];
+    const int PS = g.PS, nx = NX;
+    const int q0 = blockIdx.x * LT;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const double dx = g.dx, dx2 = g.dx2, dt = sc->dt, vis = g.vis;
     const double c1 = g.c1, c2 = g.c2, c3 = g.c3, c4 = g.c4;
-    double dv[NX], dvi[NX], outr[NX], outi[NX], auxz[NX], gam[NX], bb[NX], aux[NX];
-    double2 P[NX];
-    auto at = [&](const double2 *f, int comp, int i) -> double2 {
+    const Tw tw{tws, NX, 1};
+    auto KY = [&](int q) { return g.ky[q % g.my2]; };
+    auto KZ = [&](int q) { return g.kz[q / g.my2]; };
+    auto G = [&](const double2 *f, int comp, int i, int q) -> double2 {
         i = i >= nx ? i - nx : (i < 0 ? i + nx : i);
         return f[((size_t)comp * nx + i) * PS + q];
     };
-    auto mulwy = [&](double2 z) { return make_double2(-ky * z.y, ky * z.x); };   // wy * z
-    auto mulwz = [&](double2 z) { return make_double2(-kz * z.y, kz * z.x); };
     bool ok = true;
-    // ---------------- pressure (poisson.F90:55-239) ----------------
+    // ---------------- pressure: source (poisson.F90:97-116) and old p ----------------
+    for (int t = threadIdx.x; t < LT * NX; t += blockDim.x) {
+        const int line = t % LT, i = t / LT, q = q0 + line;
+        if (q >= PS) continue;
+        const double ky = KY(q), kz = KZ(q);
+        auto mwy = [&](double2 z) { return make_double2(-ky * z.y, ky * z.x); };
+        auto mwz = [&](double2 z) { return make_double2(-kz * z.y, kz * z.x); };
+        double2 tt = make_double2(0.0, 0.0), d, s;
+        d = csub(G(nl, 0, i + 1, q), G(nl, 0, i, q));
+        s = csub(G(ff, 0, i + 1, q), G(ff, 0, i, q));
+        tt = make_double2(tt.x + (c3 * d.x) / dx + s.x / dx, tt.y + (c3 * d.y) / dx + s.y / dx);
+        d = mwy(cadd(G(nl, 1, i + 1, q), G(nl, 1, i, q)));
+        s = mwy(cadd(G(ff, 1, i + 1, q), G(ff, 1, i, q)));
+        tt = make_double2(tt.x + (c3 * d.x) / 2.0 + s.x / 2.0, tt.y + (c3 * d.y) / 2.0 + s.y / 2.0);
+        d = mwz(cadd(G(nl, 2, i + 1, q), G(nl, 2, i, q)));
+        s = mwz(cadd(G(ff, 2, i + 1, q), G(ff, 2, i, q)));
+        tt = make_double2(tt.x + (c3 * d.x) / 2.0 + s.x / 2.0, tt.y + (c3 * d.y) / 2.0 + s.y / 2.0);
+        d = csub(G(onl, 0, i + 1, q), G(onl, 0, i, q));
+        tt = make_double2(tt.x + (c4 * d.x) / dx, tt.y + (c4 * d.y) / dx);
+        d = mwy(cadd(G(onl, 1, i + 1, q), G(onl, 1, i, q)));
+        tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
+        d = mwz(cadd(G(onl, 2, i + 1, q), G(onl, 2, i, q)));
+        tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
+        RHS[line * NX + i] = make_double2(tt.x / (c1 + c2), tt.y / (c1 + c2));
+        P[line * NX + i] = p[(size_t)i * PS + q];
+    }
+    __syncthreads();
+    const int qw = q0 + w;
+    const bool wact = qw < PS;
+    const double w2w = wact ? g.w2[qw] : 0.0;
     {
-        const double a = 1.0 / dx2 - 0.25 * w2, bd = -2.0 / dx2 - 0.5 * w2, c = 1.0 / dx2 - 0.25 * w2;
-        for (int i = 0; i < nx; ++i) {
-            double2 t = make_double2(0.0, 0.0);
-            double2 d, s;
-            d = csub(at(nl, 0, i + 1), at(nl, 0, i));
-            s = csub(at(ff, 0, i + 1), at(ff, 0, i));
-            t = make_double2(t.x + (c3 * d.x) / dx + s.x / dx, t.y + (c3 * d.y) / dx + s.y / dx);
-            d = mulwy(cadd(at(nl, 1, i + 1), at(nl, 1, i)));
-            s = mulwy(cadd(at(ff, 1, i + 1), at(ff, 1, i)));
-            t = make_double2(t.x + (c3 * d.x) / 2.0 + s.x / 2.0, t.y + (c3 * d.y) / 2.0 + s.y / 2.0);
-            d = mulwz(cadd(at(nl, 2, i + 1), at(nl, 2, i)));
-            s = mulwz(cadd(at(ff, 2, i + 1), at(ff, 2, i)));
-            t = make_double2(t.x + (c3 * d.x) / 2.0 + s.x / 2.0, t.y + (c3 * d.y) / 2.0 + s.y / 2.0);
-            d = csub(at(onl, 0, i + 1), at(onl, 0, i));
-            t = make_double2(t.x + (c4 * d.x) / dx, t.y + (c4 * d.y) / dx);
-            d = mulwy(cadd(at(onl, 1, i + 1), at(onl, 1, i)));
-            t = make_double2(t.x + (c4 * d.x) / 2.0, t.y + (c4 * d.y) / 2.0);
-            d = mulwz(cadd(at(onl, 2, i + 1), at(onl, 2, i)));
-            t = make_double2(t.x + (c4 * d.x) / 2.0, t.y + (c4 * d.y) / 2.0);
-            dv[i] = t.x / (c1 + c2);
-            dvi[i] = t.y / (c1 + c2);
-        }
-        if (q == 0) {
-            for (int i = 0; i < nx - 1; ++i) { bb[i] = bd; aux[i] = 0.0; }
-            ok = ok && thomas3<NX>(a, bb, c, dv, aux, dvi, outr, auxz, outi, gam, nx - 1);
-            outr[nx - 1] = 0.0;
-            for (int i = 0; i < nx; ++i) outi[i] = 0.0;
-        } else {
-            ok = ok && cyclic<NX>(a, bd, c, dv, dvi, outr, outi, auxz, gam, bb, aux, nx);
-        }
-        for (int i = 0; i < nx; ++i) {
-            const double2 po = p[(size_t)i * PS + q];
-            P[i] = make_double2(po.x + 1.0 * (outr[i] - po.x), po.y + 1.0 * (outi[i] - po.y));
+        const double a = 1.0 / dx2 - 0.25 * w2w, bd = -2.0 / dx2 - 0.5 * w2w, c = 1.0 / dx2 - 0.25 * w2w;
+        double2 *row = RHS + w * NX;
+        if (wact) {
+            if (qw == 0) {
+                if (lane == 0) ok = thomas_real(row, gam, a, bd, c, NX - 1) && ok;
+                __syncwarp();
+            } else {
+                circulant_solve<R>(row, a, bd, tw, lane);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = lane + 32 * r;
+                const double2 po = P[w * NX + i], tp = row[i];
+                P[w * NX + i] = make_double2(po.x + 1.0 * (tp.x - po.x), po.y + 1.0 * (tp.y - po.y));
+            }
         }
     }
-    // ---------------- ustep (usteptime.F90:45-269) ----------------
-    {
-        const double a = -(1.0 * dt * vis * c2 / dx2);
-        const double bd = 1.0 + dt * vis * c2 * (1.0 * 2.0 / dx2 + w2);
-        const double c = a;
-        const double alp = dt * (c1 + c2);
-        const double fy = 1.0 - dt * vis * c1 * w2;
-        const double gd = 1.0 * dt * vis * c1;
-        for (int n = 0; n < 3; ++n) {
-            for (int i = 0; i < nx; ++i) {
-                const double2 ui = at(u, n, i);
-                double2 r = make_double2(ui.x * fy, ui.y * fy);
-                const double2 nn = at(nl, n, i), f = at(ff, n, i), on = at(onl, n, i);
-                r = make_double2(r.x + (dt * c3) * nn.x + dt * f.x, r.y + (dt * c3) * nn.y + dt * f.y);
-                r = make_double2(r.x + (dt * c4) * on.x, r.y + (dt * c4) * on.y);
-                const double2 pm = P[i == 0 ? nx - 1 : i - 1], p0 = P[i];
-                double2 gp;
-                if (n == 0) gp = make_double2((alp * (p0.x - pm.x)) / dx, (alp * (p0.y - pm.y)) / dx);
-                else {
-                    const double2 s = make_double2(alp * 0.5 * (pm.x + p0.x), alp * 0.5 * (pm.y + p0.y));
-                    gp = (n == 1) ? mulwy(s) : mulwz(s);
-                }
-                r = csub(r, gp);
-                const double2 um = at(u, n, i - 1), up = at(u, n, i + 1);
-                double2 lap;
-                if (i == 0) lap = make_double2((up.x - 2.0 * ui.x) + um.x, (up.y - 2.0 * ui.y) + um.y);
-                else lap = make_double2((um.x + up.x) - 2.0 * ui.x, (um.y + up.y) - 2.0 * ui.y);
-                r = make_double2(r.x + (gd * lap.x) / dx2, r.y + (gd * lap.y) / dx2);
-                dv[i] = r.x; dvi[i] = r.y;
+    __syncthreads();
+    // ---------------- ustep per component (usteptime.F90:73-470) ----------------
+    for (int n = 0; n < 3; ++n) {
+        for (int t = threadIdx.x; t < LT * NX; t += blockDim.x) {
+            const int line = t % LT, i = t / LT, q = q0 + line;
+            if (q >= PS) continue;
+            const double ky = KY(q), kz = KZ(q), w2 = g.w2[q];
+            const double alp = dt * (c1 + c2);
+            const double fy = 1.0 - dt * vis * c1 * w2;
+            const double gd = 1.0 * dt * vis * c1;
+            const double2 ui = G(u, n, i, q);
+            double2 r = make_double2(ui.x * fy, ui.y * fy);
+            const double2 nn = G(nl, n, i, q), f = G(ff, n, i, q), on = G(onl, n, i, q);
+            r = make_double2(r.x + (dt * c3) * nn.x + dt * f.x, r.y + (dt * c3) * nn.y + dt * f.y);
+            r = make_double2(r.x + (dt * c4) * on.x, r.y + (dt * c4) * on.y);
+            const double2 pm = P[line * NX + (i == 0 ? nx - 1 : i - 1)], p0 = P[line * NX + i];
+            double2 gp;
+            if (n == 0) gp = make_double2((alp * (p0.x - pm.x)) / dx, (alp * (p0.y - pm.y)) / dx);
+            else {
+                const double2 sp = make_double2(alp * 0.5 * (pm.x + p0.x), alp * 0.5 * (pm.y + p0.y));
+                gp = (n == 1) ? make_double2(-ky * sp.y, ky * sp.x) : make_double2(-kz * sp.y, kz * sp.x);
             }
-            ok = ok && cyclic<NX>(a, bd, c, dv, dvi, outr, outi, auxz, gam, bb, aux, nx);
-            for (int i = 0; i < nx; ++i) u[((size_t)n * nx + i) * PS + q] = make_double2(outr[i], outi[i]);
+            r = csub(r, gp);
+            const double2 um = G(u, n, i - 1, q), up = G(u, n, i + 1, q);
+            double2 lap;
+            if (i == 0) lap = make_double2((up.x - 2.0 * ui.x) + um.x, (up.y - 2.0 * ui.y) + um.y);
+            else lap = make_double2((um.x + up.x) - 2.0 * ui.x, (um.y + up.y) - 2.0 * ui.y);
+            RHS[line * NX + i] = make_double2(r.x + (gd * lap.x) / dx2, r.y + (gd * lap.y) / dx2);
         }
+        __syncthreads();
+        if (wact) {
+            const double a = -(1.0 * dt * vis * c2 / dx2);
+            const double bd = 1.0 + dt * vis * c2 * (1.0 * 2.0 / dx2 + w2w);
+            double2 *row = RHS + w * NX;
+            circulant_solve<R>(row, a, bd, tw, lane);
+#pragma unroll
+            for (int r = 0; r < R; ++r) U[(n * LT + w) * NX + lane + 32 * r] = row[lane + 32 * r];
+        }
+        __syncthreads();
     }
     // ---------------- divcorr (poisson.F90:241-508) ----------------
-    {
-        const double a = 1.0 / dx2 - 0.25 * w2, bd = -2.0 / dx2 - 0.5 * w2, c = 1.0 / dx2 - 0.25 * w2;
-        const double alp = (c1 + c2) * dt;
-        for (int i = 0; i < nx; ++i) {
-            const double2 u1p = at(u, 0, i + 1), u1 = at(u, 0, i);
-            double2 t = make_double2((u1p.x - u1.x) / dx, (u1p.y - u1.y) / dx);
-            t = cadd(t, mulwy(cscale(cadd(at(u, 1, i), at(u, 1, i + 1)), 0.5)));
-            t = cadd(t, mulwz(cscale(cadd(at(u, 2, i), at(u, 2, i + 1)), 0.5)));
-            dv[i] = (0.5 * (1.0 + 1.0) * t.x) / alp;
-            dvi[i] = (0.5 * (1.0 + 1.0) * t.y) / alp;
-        }
-        if (q == 0) {
-            for (int i = 0; i < nx - 1; ++i) { bb[i] = bd; aux[i] = 0.0; }
-            ok = ok && thomas3<NX>(a, bb, c, dv, aux, dvi, outr, auxz, outi, gam, nx - 1);
-            outr[nx - 1] = 0.0;
-            for (int i = 0; i < nx; ++i) outi[i] = 0.0;
+    const double alpc = (c1 + c2) * dt;
+    for (int t = threadIdx.x; t < LT * NX; t += blockDim.x) {
+        const int line = t % LT, i = t / LT, q = q0 + line;
+        if (q >= PS) continue;
+        const double ky = KY(q), kz = KZ(q);
+        const int ip = i == nx - 1 ? 0 : i + 1;
+        const double2 *U1 = U + (0 * LT + line) * NX, *U2 = U + (1 * LT + line) * NX, *U3 = U + (2 * LT + line) * NX;
+        double2 tt = make_double2((U1[ip].x - U1[i].x) / dx, (U1[ip].y - U1[i].y) / dx);
+        double2 sy = cscale(cadd(U2[i], U2[ip]), 0.5), sz = cscale(cadd(U3[i], U3[ip]), 0.5);
+        tt = cadd(tt, make_double2(-ky * sy.y, ky * sy.x));
+        tt = cadd(tt, make_double2(-kz * sz.y, kz * sz.x));
+        RHS[line * NX + i] = make_double2((0.5 * (1.0 + 1.0) * tt.x) / alpc, (0.5 * (1.0 + 1.0) * tt.y) / alpc);
+    }
+    __syncthreads();
+    if (wact) {
+        const double a = 1.0 / dx2 - 0.25 * w2w, bd = -2.0 / dx2 - 0.5 * w2w, c = 1.0 / dx2 - 0.25 * w2w;
+        const double ky = KY(qw), kz = KZ(qw);
+        double2 *row = RHS + w * NX;
+        if (qw == 0) {
+            if (lane == 0) ok = thomas_real(row, gam, a, bd, c, NX - 1) && ok;
+            __syncwarp();
         } else {
-            ok = ok && cyclic<NX>(a, bd, c, dv, dvi, outr, outi, auxz, gam, bb, aux, nx);
+            circulant_solve<R>(row, a, bd, tw, lane);
         }
-        // u -= grad(phi)
-        for (int i = 0; i < nx; ++i) {
-            const int im = i == 0 ? nx - 1 : i - 1;
-            const double2 d0 = make_double2(outr[i], outi[i]), dm = make_double2(outr[im], outi[im]);
-            double2 u1 = at(u, 0, i), u2 = at(u, 1, i), u3 = at(u, 2, i);
-            u1 = make_double2(u1.x - (alp * (d0.x - dm.x)) / dx, u1.y - (alp * (d0.y - dm.y)) / dx);
-            const double2 s = make_double2(dm.x + d0.x, dm.y + d0.y);
-            // i==0: alp*wy*half*(div(1)+div(nx)); else alp*half*wy*(div(i-1)+div(i))
-            const double2 gy = (i == 0) ? cscale(mulwy(make_double2(alp, 0.0)), 0.5) : mulwy(make_double2(alp * 0.5, 0.0));
-            const double2 gz = (i == 0) ? cscale(mulwz(make_double2(alp, 0.0)), 0.5) : mulwz(make_double2(alp * 0.5, 0.0));
-            u2 = csub(u2, cmul(gy, s));
-            u3 = csub(u3, cmul(gz, s));
-            u[((size_t)0 * nx + i) * PS + q] = u1;
-            u[((size_t)1 * nx + i) * PS + q] = u2;
-            u[((size_t)2 * nx + i) * PS + q] = u3;
-        }
+        double2 *U1 = U + (0 * LT + w) * NX, *U2 = U + (1 * LT + w) * NX, *U3 = U + (2 * LT + w) * NX;
+        double2 *Pw = P + w * NX;
         const double c2dtv = (c2 * dt) * vis;
-        for (int i = 0; i < nx; ++i) {
+        double2 nu1[R], nu2[R], nu3[R], np[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
             const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
-            const double2 d0 = make_double2(outr[i], outi[i]), dm = make_double2(outr[im], outi[im]), dp = make_double2(outr[ip], outi[ip]);
-            const double2 lap = make_double2(((dm.x - 2.0 * d0.x) + dp.x) / dx2 - w2 * d0.x, ((dm.y - 2.0 * d0.y) + dp.y) / dx2 - w2 * d0.y);
-            const double2 pn = make_double2((P[i].x + d0.x) - c2dtv * lap.x, (P[i].y + d0.y) - c2dtv * lap.y);
-            p[(size_t)i * PS + q] = pn;
+            const double2 d0 = row[i], dm = row[im], dp = row[ip];
+            const double2 s = cadd(dm, d0);
+            double2 gy, gz;
+            if (i == 0) { gy = cscale(make_double2(-ky * 0.0, ky * alpc), 0.5); gz = cscale(make_double2(-kz * 0.0, kz * alpc), 0.5); }
+            else { gy = make_double2(-ky * 0.0, ky * (alpc * 0.5)); gz = make_double2(-kz * 0.0, kz * (alpc * 0.5)); }
+            nu1[r] = make_double2(U1[i].x - (alpc * (d0.x - dm.x)) / dx, U1[i].y - (alpc * (d0.y - dm.y)) / dx);
+            nu2[r] = csub(U2[i], cmul(gy, s));
+            nu3[r] = csub(U3[i], cmul(gz, s));
+            const double2 lap = make_double2(((dm.x - 2.0 * d0.x) + dp.x) / dx2 - w2w * d0.x, ((dm.y - 2.0 * d0.y) + dp.y) / dx2 - w2w * d0.y);
+            np[r] = make_double2((Pw[i].x + d0.x) - c2dtv * lap.x, (Pw[i].y + d0.y) - c2dtv * lap.y);
         }
-        // check_divergence
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r;
+            U1[i] = nu1[r]; U2[i] = nu2[r]; U3[i] = nu3[r]; Pw[i] = np[r];
+        }
+        __syncwarp();
+        // check_divergence for this line
         double dmax = 0.0;
-        for (int i = 0; i < nx; ++i) {
-            const double2 u1p = at(u, 0, i + 1), u1 = at(u, 0, i);
-            double2 t = make_double2((u1p.x - u1.x) / dx, (u1p.y - u1.y) / dx);
-            t = cadd(t, mulwy(cscale(cadd(at(u, 1, i), at(u, 1, i + 1)), 0.5)));
-            t = cadd(t, mulwz(cscale(cadd(at(u, 2, i), at(u, 2, i + 1)), 0.5)));
-            dmax = fmax(dmax, sqrt(t.x * t.x + t.y * t.y));
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = lane + 32 * r, ip = i == nx - 1 ? 0 : i + 1;
+            double2 tt = make_double2((U1[ip].x - U1[i].x) / dx, (U1[ip].y - U1[i].y) / dx);
+            double2 sy = cscale(cadd(U2[i], U2[ip]), 0.5), sz = cscale(cadd(U3[i], U3[ip]), 0.5);
+            tt = cadd(tt, make_double2(-ky * sy.y, ky * sy.x));
+            tt = cadd(tt, make_double2(-kz * sz.y, kz * sz.x));
+            dmax = fmax(dmax, sqrt(tt.x * tt.x + tt.y * tt.y));
         }
-        atomicMax(&sc->divmax_bits, (unsigned long long)__double_as_longlong(dmax));
+        for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+        if (lane == 0) atomicMax(&sc->divmax_bits, (unsigned long long)__double_as_longlong(dmax));
+    }
+    __syncthreads();
+    // coalesced write-back of u and p
+    for (int t = threadIdx.x; t < LT * NX; t += blockDim.x) {
+        const int line = t % LT, i = t / LT, q = q0 + line;
+        if (q >= PS) continue;
+#pragma unroll
+        for (int n = 0; n < 3; ++n) u[((size_t)n * nx + i) * PS + q] = U[(n * LT + line) * NX + i];
+        p[(size_t)i * PS + q] = P[line * NX + i];
     }
     if (!ok) atomicCAS(&sc->status, 0, PIBM_ERR_PIVOT);
 }
+
+template <int NX> struct LinesCfg { static constexpr int LT = NX >= 256 ? 4 : 8; };
+template <int NX>
+static size_t lines_smem() { return (size_t)(NX + 5 * LinesCfg<NX>::LT * NX) * sizeof(double2) + NX * sizeof(double); }
 
 // velstep tail: umean update (steptheflow.F90:99) and the NaN check.
 __global__ void k_scal_d(Geo g, Scal *sc) {
@@ -993,6 +1070,7 @@ static cudaError_t set_attrs() {
     if ((e = cudaFuncSetAttribute(k_ff<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_ff2cr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_ff2rc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_lines<N, LinesCfg<N>::LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>())) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
@@ -1011,35 +1089,53 @@ bool supported_size(int n) { return n == 32 || n == 64 || n == 96 || n == 128; }
 // Enqueue one full step on stream s.  cur = index of the nl/nlbc buffers that
 // receive this step's nonlinear term (the other holds the previous step's).
 template <int N>
-static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s) {
+static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev) {
     const size_t sm = plane_smem<N>(g);
     constexpr int T = PT<N>::T;
     const int old = 1 - cur;
+    auto mark = [&](int q) { if (ev) cudaEventRecord(ev[q], s); };
+    mark(0);
     k_a0<N><<<g.nx, T, sm, s>>>(g, b.u, b.p, b.ubcp, b.pbcp, b.sc, b.part);
-    k_scal_a<<<1, 32, 0, s>>>(g, b.sc, b.part);
+    k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
+    mark(1);
     k_nl<N><<<g.nx, T, sm, s>>>(g, b.ubcp, b.nl[cur], b.nlbc[cur], b.sc);
+    mark(2);
     if (g.nbody > 0) {
         k_fields<N><<<g.nx, T, sm, s>>>(g, b.u, b.p, b.ubcp, b.diffn, b.omega, b.pgr);
+        mark(3);
         k_drag<<<g.nbody, 256, 0, s>>>(g, b.pbcp, b.omega, b.pres, b.visc, b.ptot, b.sc);
         k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force);
+        mark(4);
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {
             k_rev<<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.nlbc[cur], b.nlbc[old], b.diffn, b.sc, b.rec, b.blockpart);
             k_scal_c<<<1, 256, 0, s>>>(g, b.sc, b.blockpart, nbk);
             if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.fr, b.sc);
         }
+        mark(5);
         k_ff<N><<<g.nx, T, sm, s>>>(g, b.fr, b.ff, b.sc);
+    } else {
+        mark(3); mark(4); mark(5);
     }
-    k_lines<N><<<(g.PS + 127) / 128, 128, 0, s>>>(g, b.u, b.p, b.nl[cur], b.nl[old], b.ff, b.sc);
+    mark(6);
+    k_lines<N, LinesCfg<N>::LT><<<(g.PS + LinesCfg<N>::LT - 1) / LinesCfg<N>::LT, LinesCfg<N>::LT * 32, lines_smem<N>(), s>>>(g, b.u, b.p, b.nl[cur], b.nl[old], b.ff, b.sc);
     k_scal_d<<<1, 32, 0, s>>>(g, b.sc);
+    mark(7);
 }
 
-void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s) {
+// Kernels launched per step (for launch accounting).
+int kernels_per_step(const Geo &g) {
+    int n = 5;   // a0, scal_a, nl, lines, scal_d
+    if (g.nbody > 0) n += 4 + (g.npts > 0 ? 2 + (g.sp_nnodes > 0 ? 1 : 0) : 0);
+    return n;
+}
+
+void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev) {
     switch (g.my) {
-        case 32: enqueue_step_t<32>(g, b, cur, s); break;
-        case 64: enqueue_step_t<64>(g, b, cur, s); break;
-        case 96: enqueue_step_t<96>(g, b, cur, s); break;
-        case 128: enqueue_step_t<128>(g, b, cur, s); break;
+        case 32: enqueue_step_t<32>(g, b, cur, s, ev); break;
+        case 64: enqueue_step_t<64>(g, b, cur, s, ev); break;
+        case 96: enqueue_step_t<96>(g, b, cur, s, ev); break;
+        case 128: enqueue_step_t<128>(g, b, cur, s, ev); break;
     }
 }
 
