@@ -36,14 +36,13 @@ PEAK_FALLBACK_GBS = 6650.0
 # complex spectral field F_c = nx*my2*mz*16 B and one real field F_r = nx*my*mz*8 B:
 # compulsory reads + writes of whole fields.
 KERNEL_BYTES = {
-    "a0_u_p_to_real": (4, 4),     # read u(3), p; write ubcp(3), pbcp
-    "nonlinear": (3, 6),          # read ubcp(3); write nl(3), nlbc(3)
-    "ibm_fields": (4, 11),        # read u(3), p, ubcp(2); write diffn(3), omega(3), grad p(3)
-    "forcing_fft": (3, 3),        # read fr(3); write ff(3)
-    "x_lines": (17, 0),           # read u(3), p, nl(3), onl(3), ff(3); write u(3), p
+    "a0_fields_to_real": (4, 10),  # read u(3), p; write ubcp(3), pbcp, omega(3), grad p(3)
+    "nonlinear": (9, 6),           # read ubcp(3), u(3), onl(3); write nl(3), Q(3)
+    "forcing_fft": (3, 3),         # read fr(3); write ff(3)
+    "x_lines": (17, 0),            # read u(3), p, nl(3), onl(3), ff(3); write u(3), p
 }
 KERNEL_NAMES = {
-    "a0_u_p_to_real": "k_a0", "nonlinear": "k_nl", "ibm_fields": "k_fields", "drag_mpg": "k_drag",
+    "a0_fields_to_real": "k_a0", "nonlinear": "k_nl", "drag_mpg": "k_drag",
     "reversal_spread": "k_rev", "forcing_fft": "k_ff", "x_lines": "k_lines",
 }
 

@@ -152,7 +152,7 @@ int  pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last);
  * the handle's stream: *total_ms = first-to-last event time; phase_ms[q]
  * (q < nphase <= PIBM_NPHASE) = summed duration of phase q over the steps.
  * One host synchronisation at the end. */
-#define PIBM_NPHASE 7   /* 0 u,p->real  1 nonlinear  2 IBM fields  3 drag+mpg  4 reversal+spread  5 forcing FFT  6 x-lines */
+#define PIBM_NPHASE 6   /* 0 u,p,omega,grad p -> real  1 nonlinear + IBM field  2 drag+mpg  3 reversal+spread  4 forcing FFT  5 x-lines */
 int  pibm_run_profiled(pibm_handle *h, int nsteps, pibm_step_report *last,
                        double *total_ms, double *phase_ms, int nphase);
 int  pibm_get_state(pibm_handle *h, pibm_state_view *s);

@@ -32,8 +32,8 @@ PIBM_SCHEME_CENTER = 0
 PIBM_SCHEME_UPWIND = 1
 PIBM_LIMITER_NONE = 0
 PIBM_LIMITER_MINMOD = 1
-PIBM_NPHASE = 7
-PHASE_NAMES = ["a0_u_p_to_real", "nonlinear", "ibm_fields", "drag_mpg", "reversal_spread", "forcing_fft", "x_lines"]
+PIBM_NPHASE = 6
+PHASE_NAMES = ["a0_fields_to_real", "nonlinear", "drag_mpg", "reversal_spread", "forcing_fft", "x_lines"]
 
 _i32 = C.c_int32
 _f64 = C.c_double

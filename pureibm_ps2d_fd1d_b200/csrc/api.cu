@@ -26,6 +26,7 @@ void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStr
 void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s);
 void enqueue_f2d(const double2 *f, double2 *d, int nx, int nxf, int PS, int ncomp, cudaStream_t s);
 void enqueue_d2f(const double2 *d, double2 *f, int nx, int nxf, int PS, int ncomp, cudaStream_t s);
+int real_offset(int n, int z, int y);
 }  // namespace pibm
 
 using namespace pibm;
@@ -130,21 +131,33 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
         da2[m] = 4.0 * 3.14159265358979323846 * ((S.radibdy * S.dx) * (S.radibdy * S.dx)) / (double)S.nrpr_active[m];
     std::vector<double2> tw = twiddles(S.my);
     const size_t NC = (size_t)g.nx * g.PS, NR = (size_t)g.nx * g.RS;
+    // physical fields are stored in the plane-transform order: permute the
+    // solid mask and the spreading targets accordingly
+    std::vector<int> roff((size_t)g.RS);
+    for (int z = 0; z < S.mz; ++z)
+        for (int y = 0; y < S.my; ++y) roff[(size_t)z * S.my + y] = real_offset(S.my, z, y);
+    std::vector<uint8_t> fluid_p(S.fluid.size());
+    for (int i = 0; i < S.nx; ++i)
+        for (int e = 0; e < g.RS; ++e) fluid_p[(size_t)i * g.RS + roff[e]] = S.fluid[(size_t)i * g.RS + e];
+    std::vector<int> sp_node_p(S.sp_node.size());
+    for (size_t q = 0; q < S.sp_node.size(); ++q) {
+        const int node = S.sp_node[q], i = node / g.RS, e = node - i * g.RS;
+        sp_node_p[q] = i * g.RS + roff[e];
+    }
     DevBufs &b = h->b;
     bool ok = guard(h->upload(&g.tw, tw), "tw") && guard(h->upload(&g.ky, S.ky), "ky") && guard(h->upload(&g.kz, S.kz), "kz") &&
-              guard(h->upload(&g.w2, S.w2), "w2") && guard(h->upload(&g.fluid, S.fluid), "mask") &&
+              guard(h->upload(&g.w2, S.w2), "w2") && guard(h->upload(&g.fluid, fluid_p), "mask") &&
               guard(h->upload(&g.xc, S.xc), "xc") && guard(h->upload(&g.vel, S.vel), "vel") &&
               guard(h->upload(&g.bnd, S.bnd), "bnd") && guard(h->upload(&g.cd, S.cd), "cd") &&
               guard(h->upload(&g.pt_m, S.pt_m), "pt_m") && guard(h->upload(&g.pt_l, S.pt_l), "pt_l") &&
-              guard(h->upload(&g.da2, da2), "da2") && guard(h->upload(&g.sp_node, S.sp_node), "sp_node") &&
+              guard(h->upload(&g.da2, da2), "da2") && guard(h->upload(&g.sp_node, sp_node_p), "sp_node") &&
               guard(h->upload(&g.sp_ptr, S.sp_ptr), "sp_ptr") && guard(h->upload(&g.sp_ent, S.sp_ent), "sp_ent") &&
               guard(h->alloc(&b.u, 3 * NC), "u") && guard(h->alloc(&b.p, NC), "p") &&
               guard(h->alloc(&b.nl[0], 3 * NC), "nl0") && guard(h->alloc(&b.nl[1], 3 * NC), "nl1") &&
               guard(h->alloc(&b.ff, 3 * NC), "ff") && guard(h->alloc(&b.ubcp, 3 * NR), "ubcp") &&
-              guard(h->alloc(&b.pbcp, NR), "pbcp") && guard(h->alloc(&b.nlbc[0], 3 * NR), "nlbc0") &&
-              guard(h->alloc(&b.nlbc[1], 3 * NR), "nlbc1") &&
-              (S.nbody == 0 || (guard(h->alloc(&b.diffn, 3 * NR), "diffn") && guard(h->alloc(&b.omega, 3 * NR), "omega") &&
-                                guard(h->alloc(&b.pgr, 3 * NR), "pgr") && guard(h->alloc(&b.fr, 3 * NR), "fr"))) &&
+              guard(h->alloc(&b.pbcp, NR), "pbcp") && guard(h->alloc(&b.Q, 3 * NR), "Q") &&
+              guard(h->alloc(&b.omega, 3 * NR), "omega") && guard(h->alloc(&b.pgr, 3 * NR), "pgr") &&
+              (S.nbody == 0 || guard(h->alloc(&b.fr, 3 * NR), "fr")) &&
               guard(h->alloc(&b.part, (size_t)g.nx * 12), "part") &&
               guard(h->alloc(&b.pres, 3 * (size_t)S.nbody), "pres") && guard(h->alloc(&b.visc, 3 * (size_t)S.nbody), "visc") &&
               guard(h->alloc(&b.ptot, 3 * (size_t)S.nbody), "ptot") && guard(h->alloc(&b.force, 3 * (size_t)S.nbody), "force") &&
@@ -294,8 +307,6 @@ int pibm_set_state(pibm_handle *h, const pibm_state_view *s) {
     if (s->nl) {
         CUDA_OR_FAIL(cudaMemcpyAsync(tmp, s->nl, nfu * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
         enqueue_f2d(tmp, h->b.nl[prev], g.nx, nxf, g.PS, 3, h->stream);
-        // rebuild the real-space history (onlbc of the next step = c2r(nl))
-        enqueue_c2r(g, h->b.nl[prev], h->b.nlbc[prev], 3 * g.nx, h->stream);
     }
     if (s->p) {
         CUDA_OR_FAIL(cudaMemcpyAsync(tmp, s->p, nfp * sizeof(double2), cudaMemcpyHostToDevice, h->stream));

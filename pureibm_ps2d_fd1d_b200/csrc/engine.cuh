@@ -49,7 +49,7 @@ struct Scal {
 // Device buffers of one run.
 struct DevBufs {
     double2 *u, *p, *nl[2], *ff;
-    double *ubcp, *pbcp, *nlbc[2], *diffn, *omega, *pgr, *fr;
+    double *ubcp, *pbcp, *Q, *omega, *pgr, *fr;
     double *part, *pres, *visc, *ptot, *force, *rec, *blockpart;
     Scal *sc;
 };

@@ -1,18 +1,21 @@
 // kernels.cu -- sm_100a FP64 kernels of one AB2 time step.
 //
 // Data layout in HBM (chosen for the two sweep directions of the step):
-//   spectral fields  double2 [comp][i][k][j]   (plane i contiguous, j fastest, pitch my2)
-//   physical fields  double  [comp][i][k][j]   (pitch my)
-// so an x-plane is one contiguous block (plane kernels) and, for fixed i, the
-// (j,k) lines of a plane are contiguous (line kernel loads are coalesced
-// across consecutive j).  The periodic image plane nx+1 of the reference is
-// never stored; indices wrap instead.
+//   spectral fields  double2 [comp][i][kz][ky]   (plane i contiguous, pitch my2)
+//   physical fields  double  [comp][i][...]      (one plane = my*mz doubles in the
+//                    order the plane transform leaves them: real_off(z, y))
+// so every plane load/store is a straight contiguous copy, and for fixed i the
+// (ky,kz) lines of a plane are contiguous (line-kernel loads are coalesced
+// across consecutive lines).  The periodic image plane nx+1 of the reference
+// is never stored; x indices wrap instead.
 //
 // Step pipeline (reference routines in brackets):
-//   k_a0      u,p -> ubcp,pbcp + fluid/solid means, max|u|   [compute_new_timestep, calc_pressure]
+//   k_a0      10 c2r per plane: ubcp (+umean), pbcp, omega, grad p (without mpg);
+//             fluid/solid means and max|u|       [compute_new_timestep, calc_pressure,
+//                                                   compute_omega, calc_pgrad]
 //   k_scal_a  CFL dt, t, cf (soft start), ufmean, mean slip   [compute_new_timestep]
-//   k_nl      products, upwind/central x flux, 9 r2c -> nl; 3 c2r -> nlbc   [form_nl, nonlinear]
-//   k_fields  diffn, omega, grad p: 9 c2r                      [calc_visc, compute_omega, calc_pgrad]
+//   k_nl      products + x flux, 9 r2c -> nl; 3 c2r -> Q = -c3 nl - c4 onl - c12 diffn
+//                                                  [form_nl, nonlinear, calc_visc]
 //   k_drag    per-sphere surface quadrature of p and omega     [calc_pres_visc_drag]
 //   k_scal_b  pres/visc totals, mpg, per-sphere force, drag diagnostics   [compute_mpg_at_n, bcset]
 //   k_rev     reversal-point force per active point            [calc_inner_reversal_forcing]
@@ -21,40 +24,35 @@
 //   k_ff      fr - frmean -> ff (3 r2c)                        [bcset]
 //   k_lines   pressure -> ustep -> divcorr per (ky,kz) line     [velstep]
 //   k_scal_d  umean update, divergence, status                 [velstep]
+// The IBM force needs -c3 nl - c4 onl - c12 diffn only at the inner reversal
+// points; by linearity of the transform and of the interpolation it is formed
+// once in spectral space (Q) instead of three separately interpolated fields.
 #include "engine.cuh"
-#include "fft_plane.cuh"
+#include "fft2d.cuh"
 #include "../../include/pibm.h"
 
 namespace pibm {
 
 __device__ __constant__ double kSmallD = 1.0000000180025095e-35;   // (double)1.0E-35f
 
-template <int N> struct PT;
-template <> struct PT<32>  { static constexpr int RZ = 1, LZ = 32, RY = 1, LY = 16, T = 128, EPT = 5; };
-template <> struct PT<64>  { static constexpr int RZ = 2, LZ = 32, RY = 1, LY = 32, T = 256, EPT = 9; };
-template <> struct PT<96>  { static constexpr int RZ = 3, LZ = 32, RY = 3, LY = 16, T = 256, EPT = 19; };
-template <> struct PT<128> { static constexpr int RZ = 4, LZ = 32, RY = 2, LY = 32, T = 512, EPT = 17; };
-
-template <int N>
-__device__ __forceinline__ void plane_c2r(double2 *buf, const Geo &g, const Tw &tw) {
-    z_pass<PT<N>::RZ, PT<N>::LZ>(buf, g.my2, g.mz, +1.0, tw);
-    __syncthreads();
-    y_c2r_pass<PT<N>::RY, PT<N>::LY>(buf, g.my2, g.mz, tw);
-    __syncthreads();
-}
-template <int N>
-__device__ __forceinline__ void plane_r2c(double2 *buf, const Geo &g, const Tw &tw) {
-    y_r2c_pass<PT<N>::RY, PT<N>::LY>(buf, g.my2, g.mz, tw);
-    __syncthreads();
-    z_pass<PT<N>::RZ, PT<N>::LZ>(buf, g.my2, g.mz, -1.0, tw);
-    __syncthreads();
-}
-
-__device__ __forceinline__ double &rv(double2 *buf, int my2, int k, int j) { return ((double *)buf)[(size_t)k * 2 * my2 + j]; }
-
 template <int N>
 __device__ __forceinline__ void load_tw(double2 *tws, const Geo &g) {
     for (int t = threadIdx.x; t < N; t += blockDim.x) tws[t] = g.tw[t];
+}
+// real plane (transform order, N x N doubles) <-> shared memory rows of pitch N+2 doubles
+template <int N>
+__device__ __forceinline__ void real_to_smem(double2 *buf, const double *__restrict__ src, double sub = 0.0) {
+    double *b = (double *)buf;
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) { const int r = e / N, c = e - r * N; b[r * (N + 2) + c] = src[e] - sub; }
+}
+template <int N>
+__device__ __forceinline__ double real_from_smem(const double2 *buf, int e) {
+    const int r = e / N, c = e - r * N;
+    return ((const double *)buf)[r * (N + 2) + c];
+}
+// smem double offset of real node (z, y) (plane_c2r output order)
+template <int N> __device__ __forceinline__ int smem_real_off(int z, int y) {
+    return zrow<N>(z) * (N + 2) + 2 * yslot<N>(y >> 1) + (y & 1);
 }
 
 // Deterministic block sum (fixed lane/warp tree).
@@ -96,48 +94,74 @@ __device__ __forceinline__ double block_max(double v, double *scr) {
 }
 
 // ============================================================================
-// k_a0: ubcp = c2r(u) + umean, pbcp = c2r(p); per-plane partial means and maxima
-// (dependent_functions.F90:1085-1122, 336-349).  part[i*12 + q]:
-// q 0-2 fluid sums, 3-5 solid sums, 6-8 all sums, 9-11 max |u|.
+// k_a0: 10 c2r per plane (dependent_functions.F90:1085-1122, 336-349;
+// boundary_condition.F90:1648-1765, 1817-1896).  The x differences of omega and
+// grad p are taken on the spectral planes before the transform (linear).
+// part[i*12 + q]: q 0-2 fluid sums, 3-5 solid sums, 6-8 all sums, 9-11 max |u|.
 // ============================================================================
 template <int N>
-__global__ void __launch_bounds__(PT<N>::T) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
-                                                 double *__restrict__ ubcp, double *__restrict__ pbcp,
-                                                 const Scal *__restrict__ sc, double *__restrict__ part) {
+__global__ void __launch_bounds__(Plan<N>::T) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
+                                                   double *__restrict__ ubcp, double *__restrict__ pbcp,
+                                                   double *__restrict__ omega, double *__restrict__ pgr,
+                                                   const Scal *__restrict__ sc, double *__restrict__ part) {
     extern __shared__ double2 sm[];
-    double2 *buf = sm, *tws = sm + g.PS;
+    constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
+    double2 *buf = sm, *tws = sm + PS;
     __shared__ double scr[32];
     load_tw<N>(tws, g);
-    const int i = blockIdx.x;
-    const Tw tw{tws, N, 1};
-    const int nx = g.nx, PS = g.PS, RS = g.RS, my = g.my, my2 = g.my2;
+    const int i = blockIdx.x, nx = g.nx;
+    const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
+    const TwT tw{tws, N};
+    const double tdx = 2.0 * g.dx;
+    const double2 *U0 = u + (size_t)i * PS, *U1 = u + ((size_t)nx + i) * PS, *U2 = u + ((size_t)2 * nx + i) * PS;
     double acc[12];
 #pragma unroll
     for (int q = 0; q < 9; ++q) acc[q] = 0.0;
     acc[9] = acc[10] = acc[11] = kSmallD;
-    for (int n = 0; n < 4; ++n) {
-        const double2 *src = n < 3 ? u + ((size_t)n * nx + i) * PS : p + (size_t)i * PS;
-        for (int e = threadIdx.x; e < PS; e += blockDim.x) buf[e] = src[e];
+    for (int t = 0; t < 10; ++t) {
+        for (int e = threadIdx.x; e < PS; e += blockDim.x) {
+            const int kz = e / my2, j = e - kz * my2;
+            const double ky = g.ky[j], kzv = g.kz[kz];
+            double2 f;
+            switch (t) {
+                case 0: f = U0[e]; break;
+                case 1: f = U1[e]; break;
+                case 2: f = U2[e]; break;
+                case 3: f = p[(size_t)i * PS + e]; break;
+                case 4: { const double2 a = U2[e], b = U1[e];   // wy*u3 - wz*u2
+                          f = make_double2(-ky * a.y - (-kzv * b.y), ky * a.x - kzv * b.x); } break;
+                case 5: { const double2 a = U0[e];              // wz*u1 - d(u3)/dx
+                          const double2 hp = u[((size_t)2 * nx + ip) * PS + e], hm = u[((size_t)2 * nx + im) * PS + e];
+                          const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
+                          f = make_double2(-kzv * a.y - d.x, kzv * a.x - d.y); } break;
+                case 6: { const double2 a = U0[e];              // d(u2)/dx - wy*u1
+                          const double2 hp = u[((size_t)nx + ip) * PS + e], hm = u[((size_t)nx + im) * PS + e];
+                          const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
+                          f = make_double2(d.x - (-ky * a.y), d.y - ky * a.x); } break;
+                case 7: { const double2 a = p[(size_t)ip * PS + e], b = p[(size_t)im * PS + e];
+                          f = make_double2((a.x - b.x) / tdx, (a.y - b.y) / tdx); } break;
+                case 8: { const double2 a = p[(size_t)i * PS + e]; f = make_double2(-a.y * ky, a.x * ky); } break;
+                default: { const double2 a = p[(size_t)i * PS + e]; f = make_double2(-a.y * kzv, a.x * kzv); } break;
+            }
+            buf[e] = f;
+        }
         __syncthreads();
-        plane_c2r<N>(buf, g, tw);
-        if (n < 3) {
-            const double um = sc->umean[n];
-            double *dst = ubcp + ((size_t)n * nx + i) * RS;
+        plane_c2r<N>(buf, tw);
+        if (t < 3) {
+            const double um = sc->umean[t];
+            double *dst = ubcp + ((size_t)t * nx + i) * RS;
             const uint8_t *fl = g.fluid + (size_t)i * RS;
             for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-                const int k = e / my, j = e - k * my;
-                const double v = rv(buf, my2, k, j) + um;
+                const double v = real_from_smem<N>(buf, e) + um;
                 dst[e] = v;
-                if (fl[e]) acc[n] += v; else acc[3 + n] += v;
-                acc[6 + n] += v;
-                acc[9 + n] = fmax(acc[9 + n], fabs(v));
+                if (fl[e]) acc[t] += v; else acc[3 + t] += v;
+                acc[6 + t] += v;
+                acc[9 + t] = fmax(acc[9 + t], fabs(v));
             }
         } else {
-            double *dst = pbcp + (size_t)i * RS;
-            for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-                const int k = e / my, j = e - k * my;
-                dst[e] = rv(buf, my2, k, j);
-            }
+            double *dst = t == 3 ? pbcp + (size_t)i * RS
+                        : (t < 7 ? omega + ((size_t)(t - 4) * nx + i) * RS : pgr + ((size_t)(t - 7) * nx + i) * RS);
+            for (int e = threadIdx.x; e < RS; e += blockDim.x) dst[e] = real_from_smem<N>(buf, e);
         }
         __syncthreads();
     }
@@ -249,134 +273,70 @@ __device__ __forceinline__ double xflux_diff(const Geo &g, const double *__restr
 }
 
 template <int N>
-__global__ void __launch_bounds__(PT<N>::T) k_nl(Geo g, const double *__restrict__ ubcp, double2 *__restrict__ nl_new,
-                                                 double *__restrict__ nlbc_new, const Scal *__restrict__ sc) {
+__global__ void __launch_bounds__(Plan<N>::T) k_nl(Geo g, const double *__restrict__ ubcp, const double2 *__restrict__ u,
+                                                   const double2 *__restrict__ onl, double2 *__restrict__ nl_new,
+                                                   double *__restrict__ Q, const Scal *__restrict__ sc) {
     extern __shared__ double2 sm[];
-    double2 *buf = sm, *tws = sm + g.PS;
+    constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
+    constexpr int EPT = Plan<N>::EPT, T = Plan<N>::T;
+    double2 *buf = sm, *tws = sm + PS;
     load_tw<N>(tws, g);
-    const int i = blockIdx.x;
-    const Tw tw{tws, N, 1};
-    const int nx = g.nx, PS = g.PS, RS = g.RS, my = g.my, my2 = g.my2;
-    constexpr int EPT = PT<N>::EPT, T = PT<N>::T;
-    const double *U0 = ubcp + ((size_t)0 * nx + i) * RS;
-    const double *U1 = ubcp + ((size_t)1 * nx + i) * RS;
-    const double *U2 = ubcp + ((size_t)2 * nx + i) * RS;
-    // product pairs: comp c uses (wy: pa[c]) and (wz: pb[c])
+    const int i = blockIdx.x, nx = g.nx;
+    const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
+    const TwT tw{tws, N};
+    const double *Uc[3] = {ubcp + (size_t)i * RS, ubcp + ((size_t)nx + i) * RS, ubcp + ((size_t)2 * nx + i) * RS};
+    // product pairs: component c uses (wy: pa) and (wz: pb)
     const int pa0[3] = {0, 1, 1}, pa1[3] = {1, 1, 2}, pb0[3] = {0, 1, 2}, pb1[3] = {2, 2, 2};
-    const double *Uc[3] = {U0, U1, U2};
+    const double c12 = g.c1 + g.c2;
     for (int c = 0; c < 3; ++c) {
         double2 acc[EPT];
         for (int q = 0; q < 3; ++q) {
+            double *b = (double *)buf;
             for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-                const int k = e / my, j = e - k * my;
                 double v;
                 if (q == 0) v = Uc[pa0[c]][e] * Uc[pa1[c]][e];
                 else if (q == 1) v = Uc[pb0[c]][e] * Uc[pb1[c]][e];
                 else v = xflux_diff(g, ubcp, i, e, c);
-                rv(buf, my2, k, j) = v;
+                const int r = e / N, cc = e - r * N;
+                b[r * (N + 2) + cc] = v;
             }
             __syncthreads();
-            plane_r2c<N>(buf, g, tw);
+            plane_r2c<N>(buf, tw);
 #pragma unroll
             for (int s = 0; s < EPT; ++s) {
                 const int e = threadIdx.x + s * T;
                 if (e < PS) {
                     const double2 X = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
-                    const int k = e / my2, j = e - k * my2;
+                    const int kz = e / my2, j = e - kz * my2;
                     if (q == 0) { const double ky = g.ky[j]; acc[s] = make_double2(-ky * X.y, ky * X.x); }
-                    else if (q == 1) { const double kz = g.kz[k]; acc[s] = cadd(acc[s], make_double2(-kz * X.y, kz * X.x)); }
+                    else if (q == 1) { const double kzv = g.kz[kz]; acc[s] = cadd(acc[s], make_double2(-kzv * X.y, kzv * X.x)); }
                     else acc[s] = cadd(acc[s], X);
                 }
             }
             __syncthreads();
         }
+        // nl = -(...) (nl.F90:146-152); Q = -c3 nl - c4 onl - c12 diffn (calc_visc spectrum)
         double2 *dst = nl_new + ((size_t)c * nx + i) * PS;
+        const double2 *on = onl + ((size_t)c * nx + i) * PS;
+        const double2 *uc = u + (size_t)c * nx * PS;
 #pragma unroll
         for (int s = 0; s < EPT; ++s) {
             const int e = threadIdx.x + s * T;
             if (e < PS) {
                 const double2 v = make_double2(-acc[s].x, -acc[s].y);
                 dst[e] = v;
-                buf[e] = v;
-            }
-        }
-        __syncthreads();
-        plane_c2r<N>(buf, g, tw);
-        double *rd = nlbc_new + ((size_t)c * nx + i) * RS;
-        for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-            const int k = e / my, j = e - k * my;
-            rd[e] = rv(buf, my2, k, j);
-        }
-        __syncthreads();
-    }
-}
-
-// ============================================================================
-// k_fields: diffn (calc_visc, boundary_condition.F90:1767-1815), omega
-// (compute_omega :1648-1765; omega_x from one transform of wy*u3 - wz*u2) and
-// grad p without mpg (calc_pgrad :1817-1896; mpg is added per node when
-// interpolated, as the reference adds it per node before interpolation).
-// ============================================================================
-template <int N>
-__global__ void __launch_bounds__(PT<N>::T) k_fields(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
-                                                     const double *__restrict__ ubcp, double *__restrict__ diffn,
-                                                     double *__restrict__ omega, double *__restrict__ pgr) {
-    extern __shared__ double2 sm[];
-    double2 *buf = sm, *tws = sm + g.PS;
-    load_tw<N>(tws, g);
-    const int i = blockIdx.x;
-    const Tw tw{tws, N, 1};
-    const int nx = g.nx, PS = g.PS, RS = g.RS, my = g.my, my2 = g.my2;
-    const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
-    const double tdx = 2.0 * g.dx;
-    for (int t = 0; t < 9; ++t) {
-        for (int e = threadIdx.x; e < PS; e += blockDim.x) {
-            const int k = e / my2, j = e - k * my2;
-            const double ky = g.ky[j], kz = g.kz[k];
-            double2 f;
-            if (t < 3) {
-                const double2 *un = u + (size_t)t * nx * PS;
-                const double2 a = un[(size_t)im * PS + e], b = un[(size_t)i * PS + e], c = un[(size_t)ip * PS + e];
-                double2 s = make_double2(g.rdx2 * ((a.x - 2.0 * b.x) + c.x), g.rdx2 * ((a.y - 2.0 * b.y) + c.y));
+                const double2 a = uc[(size_t)im * PS + e], bb = uc[(size_t)i * PS + e], cv = uc[(size_t)ip * PS + e];
+                double2 df = make_double2(g.rdx2 * ((a.x - 2.0 * bb.x) + cv.x), g.rdx2 * ((a.y - 2.0 * bb.y) + cv.y));
                 const double w2 = g.w2[e];
-                s = make_double2(s.x - w2 * b.x, s.y - w2 * b.y);
-                f = make_double2(s.x * g.vis, s.y * g.vis);
-            } else if (t == 3) {   // wy*u1
-                const double2 a = u[(size_t)i * PS + e];
-                f = make_double2(-ky * a.y, ky * a.x);
-            } else if (t == 4) {   // wz*u1
-                const double2 a = u[(size_t)i * PS + e];
-                f = make_double2(-kz * a.y, kz * a.x);
-            } else if (t == 5) {   // wy*u3 - wz*u2
-                const double2 a = u[((size_t)2 * nx + i) * PS + e], b = u[((size_t)1 * nx + i) * PS + e];
-                f = make_double2(-ky * a.y - (-kz * b.y), ky * a.x - kz * b.x);
-            } else if (t == 6) {
-                const double2 a = p[(size_t)ip * PS + e], b = p[(size_t)im * PS + e];
-                f = make_double2((a.x - b.x) / tdx, (a.y - b.y) / tdx);
-            } else if (t == 7) {
-                const double2 a = p[(size_t)i * PS + e];
-                f = make_double2(-a.y * ky, a.x * ky);
-            } else {
-                const double2 a = p[(size_t)i * PS + e];
-                f = make_double2(-a.y * kz, a.x * kz);
+                df = make_double2((df.x - w2 * bb.x) * g.vis, (df.y - w2 * bb.y) * g.vis);
+                const double2 o = on[e];
+                buf[e] = make_double2((-g.c3 * v.x - g.c4 * o.x) - c12 * df.x, (-g.c3 * v.y - g.c4 * o.y) - c12 * df.y);
             }
-            buf[e] = f;
         }
         __syncthreads();
-        plane_c2r<N>(buf, g, tw);
-        for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-            const int k = e / my, j = e - k * my;
-            const double v = rv(buf, my2, k, j);
-            if (t < 3) diffn[((size_t)t * nx + i) * RS + e] = v;
-            else if (t == 3) {
-                const double *u2 = ubcp + (size_t)1 * nx * RS;
-                omega[((size_t)2 * nx + i) * RS + e] = (u2[(size_t)ip * RS + e] - u2[(size_t)im * RS + e]) / tdx - v;
-            } else if (t == 4) {
-                const double *u3 = ubcp + (size_t)2 * nx * RS;
-                omega[((size_t)1 * nx + i) * RS + e] = v - (u3[(size_t)ip * RS + e] - u3[(size_t)im * RS + e]) / tdx;
-            } else if (t == 5) omega[((size_t)0 * nx + i) * RS + e] = v;
-            else pgr[((size_t)(t - 6) * nx + i) * RS + e] = v;
-        }
+        plane_c2r<N>(buf, tw);
+        double *rd = Q + ((size_t)c * nx + i) * RS;
+        for (int e = threadIdx.x; e < RS; e += blockDim.x) rd[e] = real_from_smem<N>(buf, e);
         __syncthreads();
     }
 }
@@ -414,47 +374,50 @@ __device__ __forceinline__ void make_sten(const Geo &g, const double pos[3], Ste
     }
 }
 
-// value at node (i,j,k) of a physical field f (one component)
-__device__ __forceinline__ double fat(const Geo &g, const double *f, int i, int j, int k) {
-    return __ldg(f + (size_t)i * g.RS + (size_t)k * g.my + j);
+// value at node (x=i, y=j, z=k) of a physical field (one component)
+template <int N>
+__device__ __forceinline__ double fat(const double *f, int i, int j, int k) {
+    return __ldg(f + (size_t)i * (N * N) + real_off<N>(k, j));
 }
 // interpolator order (k, j, i)
-__device__ __forceinline__ double interp_kji(const Geo &g, const Sten &s, const double *f, double add = 0.0) {
+template <int N>
+__device__ __forceinline__ double interp_kji(const Sten &s, const double *f, double add = 0.0) {
     double r = 0.0;
 #pragma unroll
     for (int c = 0; c < 2; ++c)
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
-            for (int a = 0; a < 2; ++a) r = r + (fat(g, f, s.ii[a], s.jj[b], s.kk[c]) + add) * s.w(a, b, c);
+            for (int a = 0; a < 2; ++a) r = r + (fat<N>(f, s.ii[a], s.jj[b], s.kk[c]) + add) * s.w(a, b, c);
     return r;
 }
 // array_dot_product order (i, j, k)
-__device__ __forceinline__ double dot_ijk(const Geo &g, const Sten &s, const double *f) {
+template <int N>
+__device__ __forceinline__ double dot_ijk(const Sten &s, const double *f) {
     double r = 0.0;
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
-            for (int c = 0; c < 2; ++c) r = r + fat(g, f, s.ii[a], s.jj[b], s.kk[c]) * s.w(a, b, c);
+            for (int c = 0; c < 2; ++c) r = r + fat<N>(f, s.ii[a], s.jj[b], s.kk[c]) * s.w(a, b, c);
     return r;
 }
 
 // ============================================================================
 // k_drag: per-sphere pressure and viscous force from the surface quadrature
 // (calc_pres_visc_drag, boundary_condition.F90:1481-1645).  One CTA per sphere.
-// out[0..3*nbody): pres(m,d) ; then visc ; then +pl*cd*da1 sums (pres_total share)
 // ============================================================================
+template <int N>
 __global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ pbcp, const double *__restrict__ omega,
                                               double *__restrict__ pres, double *__restrict__ visc, double *__restrict__ ptot,
                                               const Scal *__restrict__ sc) {
     __shared__ double scr[32];
     const int m = blockIdx.x;
     const int NB = g.nbody;
-    double xcm[3] = {g.xc[m], g.xc[m + NB], g.xc[m + 2 * NB]};
+    const double xcm[3] = {g.xc[m], g.xc[m + NB], g.xc[m + 2 * NB]};
     double sa[3] = {0, 0, 0}, sb[3] = {0, 0, 0};
-    const size_t CR = (size_t)g.nx * g.RS;
+    const size_t CR = (size_t)g.nx * N * N;
     for (int l = threadIdx.x; l < g.nbnd; l += blockDim.x) {
         double xl[3], xpb[3], cdl[3];
 #pragma unroll
@@ -463,10 +426,10 @@ __global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ 
         Sten sp, sv;
         make_sten(g, xpb, sp);
         make_sten(g, xl, sv);
-        const double pl = dot_ijk(g, sp, pbcp);
+        const double pl = dot_ijk<N>(sp, pbcp);
         double vort[3];
 #pragma unroll
-        for (int n = 0; n < 3; ++n) vort[n] = interp_kji(g, sv, omega + n * CR);
+        for (int n = 0; n < 3; ++n) vort[n] = interp_kji<N>(sv, omega + n * CR);
         double df[3];
         df[0] = vort[2] * cdl[1]; df[0] = df[0] - vort[1] * cdl[2];
         df[1] = vort[0] * cdl[2]; df[1] = df[1] - vort[2] * cdl[0];
@@ -549,16 +512,16 @@ __device__ __forceinline__ void inner_point(const Geo &g, int m, int l, double x
     for (int d = 0; d < 3; ++d) xli[d] = __dadd_rn(g.xc[m + d * NB], __dmul_rn(g.bnd[3 * l + d], g.ri));
 }
 
+template <int N>
 __global__ void __launch_bounds__(256) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
-                                             const double *__restrict__ nlbc, const double *__restrict__ onlbc,
-                                             const double *__restrict__ diffn, const Scal *__restrict__ sc,
+                                             const double *__restrict__ Q, const Scal *__restrict__ sc,
                                              double *__restrict__ rec, double *__restrict__ blockpart) {
     __shared__ double scr[32];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     double fm[3] = {0, 0, 0}, ffl[3] = {0, 0, 0};
     if (p < g.npts && !sc->status) {
         const int m = g.pt_m[p], l = g.pt_l[p], NB = g.nbody;
-        const size_t CR = (size_t)g.nx * g.RS;
+        const size_t CR = (size_t)g.nx * N * N;
         double xli[3], xlo[3], xpi[3], snorm[3];
         inner_point(g, m, l, xli);
         double rad = 0.0;
@@ -576,15 +539,13 @@ __global__ void __launch_bounds__(256) k_rev(Geo g, const double *__restrict__ u
         make_sten(g, xlo, so);
         make_sten(g, xpi, spi);
         make_sten(g, xli, si);
-        double ulo[3], ppll[3], uli[3], nll[3], onll[3], dfll[3];
+        double ulo[3], ppll[3], uli[3], qll[3];
 #pragma unroll
         for (int n = 0; n < 3; ++n) {
-            ulo[n] = interp_kji(g, so, ubcp + n * CR);
-            ppll[n] = interp_kji(g, spi, pgr + n * CR, sc->mpg[n]);
-            uli[n] = interp_kji(g, si, ubcp + n * CR);
-            nll[n] = dot_ijk(g, si, nlbc + n * CR);
-            onll[n] = dot_ijk(g, si, onlbc + n * CR);
-            dfll[n] = dot_ijk(g, si, diffn + n * CR);
+            ulo[n] = interp_kji<N>(so, ubcp + n * CR);
+            ppll[n] = interp_kji<N>(spi, pgr + n * CR, sc->mpg[n]);
+            uli[n] = interp_kji<N>(si, ubcp + n * CR);
+            qll[n] = dot_ijk<N>(si, Q + n * CR);
         }
         double linvel[3];
 #pragma unroll
@@ -609,8 +570,8 @@ __global__ void __launch_bounds__(256) k_rev(Geo g, const double *__restrict__ u
 #pragma unroll
         for (int n = 0; n < 3; ++n) {
             double f = cf * (-ucar[n] + uli[n]);
-            f = f - g.c3 * nll[n] - g.c4 * onll[n];
-            f = f + c12 * (ppll[n] - dfll[n]);
+            f = f + qll[n];
+            f = f + c12 * ppll[n];
             ft[n] = f * da2 * g.dr * g.dx;
         }
         int count_fl = 0;
@@ -621,7 +582,7 @@ __global__ void __launch_bounds__(256) k_rev(Geo g, const double *__restrict__ u
             for (int b = 0; b < 2; ++b)
 #pragma unroll
                 for (int a = 0; a < 2; ++a) {
-                    const bool fl = g.fluid[(size_t)si.ii[a] * g.RS + (size_t)si.kk[c] * g.my + si.jj[b]] != 0;
+                    const bool fl = g.fluid[(size_t)si.ii[a] * (N * N) + real_off<N>(si.kk[c], si.jj[b])] != 0;
                     const double w = si.w(a, b, c);
 #pragma unroll
                     for (int n = 0; n < 3; ++n) {
@@ -661,7 +622,7 @@ __global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *b
 
 // k_spread: fr at every forced node, accumulated over its (point, corner)
 // contributions in the reference's (sphere, point) order
-// (boundary_condition.F90:1425-1462).
+// (boundary_condition.F90:1425-1462).  sp_node holds physical offsets.
 __global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, double *__restrict__ fr,
                                                 const Scal *__restrict__ sc) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -691,23 +652,18 @@ __global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict_
 
 // k_ff: ff = r2c(fr - frmean) (boundary_condition.F90:678-700).
 template <int N>
-__global__ void __launch_bounds__(PT<N>::T) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
-                                                 const Scal *__restrict__ sc) {
+__global__ void __launch_bounds__(Plan<N>::T) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
+                                                   const Scal *__restrict__ sc) {
     extern __shared__ double2 sm[];
-    double2 *buf = sm, *tws = sm + g.PS;
+    constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
+    double2 *buf = sm, *tws = sm + PS;
     load_tw<N>(tws, g);
-    const int i = blockIdx.x;
-    const Tw tw{tws, N, 1};
-    const int nx = g.nx, PS = g.PS, RS = g.RS, my = g.my, my2 = g.my2;
+    const int i = blockIdx.x, nx = g.nx;
+    const TwT tw{tws, N};
     for (int n = 0; n < 3; ++n) {
-        const double fmn = sc->frmean[n];
-        const double *src = fr + ((size_t)n * nx + i) * RS;
-        for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-            const int k = e / my, j = e - k * my;
-            rv(buf, my2, k, j) = src[e] - fmn;
-        }
+        real_to_smem<N>(buf, fr + ((size_t)n * nx + i) * RS, sc->frmean[n]);
         __syncthreads();
-        plane_r2c<N>(buf, g, tw);
+        plane_r2c<N>(buf, tw);
         double2 *dst = ff + ((size_t)n * nx + i) * PS;
         for (int e = threadIdx.x; e < PS; e += blockDim.x) dst[e] = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
         __syncthreads();
@@ -991,7 +947,7 @@ __global__ void k_scal_d(Geo g, Scal *sc) {
 
 // ============================================================================
 // Layout conversion between the reference's Fortran arrays and the device
-// layout (used only by get/set state): u(nx+1,my2,mz,ncomp) <-> [comp][i][k][j].
+// layout (get/set state): u(nx+1,my2,mz,ncomp) <-> [comp][i][kz][ky].
 // Tiled 32x32 transpose through shared memory.
 // ============================================================================
 __global__ void k_f2d(const double2 *__restrict__ f, double2 *__restrict__ d, int nx, int nxf, int PS, int ncomp) {
@@ -1027,46 +983,53 @@ __global__ void k_d2f(const double2 *__restrict__ d, double2 *__restrict__ f, in
     }
 }
 
-// Standalone batched plane transforms (pibm_ff2rc / pibm_ff2cr), planes contiguous.
+// Standalone batched plane transforms (pibm_ff2rc / pibm_ff2cr) on natural
+// host layouts: real a[z*my + y], complex b[kz*my2 + ky].
 template <int N>
-__global__ void __launch_bounds__(PT<N>::T) k_ff2cr(Geo g, const double2 *__restrict__ a, double *__restrict__ b) {
+__global__ void __launch_bounds__(Plan<N>::T) k_ff2cr(Geo g, const double2 *__restrict__ a, double *__restrict__ b) {
     extern __shared__ double2 sm[];
-    double2 *buf = sm, *tws = sm + g.PS;
+    constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
+    double2 *buf = sm, *tws = sm + PS;
     load_tw<N>(tws, g);
-    const Tw tw{tws, N, 1};
+    const TwT tw{tws, N};
     const size_t q = blockIdx.x;
-    for (int e = threadIdx.x; e < g.PS; e += blockDim.x) buf[e] = a[q * g.PS + e];
+    for (int e = threadIdx.x; e < PS; e += blockDim.x) buf[e] = a[q * PS + e];
     __syncthreads();
-    plane_c2r<N>(buf, g, tw);
-    for (int e = threadIdx.x; e < g.RS; e += blockDim.x) { const int k = e / g.my, j = e - k * g.my; b[q * g.RS + e] = rv(buf, g.my2, k, j); }
+    plane_c2r<N>(buf, tw);
+    for (int e = threadIdx.x; e < RS; e += blockDim.x) {
+        const int z = e / N, y = e - z * N;
+        b[q * RS + e] = ((const double *)buf)[smem_real_off<N>(z, y)];
+    }
 }
 template <int N>
-__global__ void __launch_bounds__(PT<N>::T) k_ff2rc(Geo g, const double *__restrict__ a, double2 *__restrict__ b) {
+__global__ void __launch_bounds__(Plan<N>::T) k_ff2rc(Geo g, const double *__restrict__ a, double2 *__restrict__ b) {
     extern __shared__ double2 sm[];
-    double2 *buf = sm, *tws = sm + g.PS;
+    constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
+    double2 *buf = sm, *tws = sm + PS;
     load_tw<N>(tws, g);
-    const Tw tw{tws, N, 1};
+    const TwT tw{tws, N};
     const size_t q = blockIdx.x;
-    for (int e = threadIdx.x; e < g.RS; e += blockDim.x) { const int k = e / g.my, j = e - k * g.my; rv(buf, g.my2, k, j) = a[q * g.RS + e]; }
+    for (int e = threadIdx.x; e < RS; e += blockDim.x) {
+        const int z = e / N, y = e - z * N;
+        ((double *)buf)[smem_real_off<N>(z, y)] = a[q * RS + e];
+    }
     __syncthreads();
-    plane_r2c<N>(buf, g, tw);
-    for (int e = threadIdx.x; e < g.PS; e += blockDim.x) b[q * g.PS + e] = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
+    plane_r2c<N>(buf, tw);
+    for (int e = threadIdx.x; e < PS; e += blockDim.x) b[q * PS + e] = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
 }
 
 // ============================================================================
 // Host-side launch helpers
 // ============================================================================
-
 template <int N>
-static size_t plane_smem(const Geo &g) { return (size_t)(g.PS + N) * sizeof(double2); }
+static size_t plane_smem() { return (size_t)((N / 2 + 1) * N + N) * sizeof(double2); }
 
 template <int N>
 static cudaError_t set_attrs() {
-    const int maxs = (int)((size_t)(((N / 2 + 1) * N) + N) * sizeof(double2));
+    const int maxs = (int)plane_smem<N>();
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(k_a0<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_nl<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_fields<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_ff<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_ff2cr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_ff2rc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
@@ -1086,47 +1049,57 @@ cudaError_t configure_kernels(int n) {
 
 bool supported_size(int n) { return n == 32 || n == 64 || n == 96 || n == 128; }
 
-// Enqueue one full step on stream s.  cur = index of the nl/nlbc buffers that
-// receive this step's nonlinear term (the other holds the previous step's).
+// Physical offset of real node (z, y) in one plane (host side of real_off).
+int real_offset(int n, int z, int y) {
+    switch (n) {
+        case 32: return real_off<32>(z, y);
+        case 64: return real_off<64>(z, y);
+        case 96: return real_off<96>(z, y);
+        case 128: return real_off<128>(z, y);
+        default: return -1;
+    }
+}
+
+// Enqueue one full step on stream s.  cur = index of the nl buffer that
+// receives this step's nonlinear term (the other holds the previous step's).
 template <int N>
 static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev) {
-    const size_t sm = plane_smem<N>(g);
-    constexpr int T = PT<N>::T;
+    const size_t sm = plane_smem<N>();
+    constexpr int T = Plan<N>::T;
     const int old = 1 - cur;
     auto mark = [&](int q) { if (ev) cudaEventRecord(ev[q], s); };
     mark(0);
-    k_a0<N><<<g.nx, T, sm, s>>>(g, b.u, b.p, b.ubcp, b.pbcp, b.sc, b.part);
+    k_a0<N><<<g.nx, T, sm, s>>>(g, b.u, b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
     k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
     mark(1);
-    k_nl<N><<<g.nx, T, sm, s>>>(g, b.ubcp, b.nl[cur], b.nlbc[cur], b.sc);
+    k_nl<N><<<g.nx, T, sm, s>>>(g, b.ubcp, b.u, b.nl[old], b.nl[cur], b.Q, b.sc);
     mark(2);
     if (g.nbody > 0) {
-        k_fields<N><<<g.nx, T, sm, s>>>(g, b.u, b.p, b.ubcp, b.diffn, b.omega, b.pgr);
-        mark(3);
-        k_drag<<<g.nbody, 256, 0, s>>>(g, b.pbcp, b.omega, b.pres, b.visc, b.ptot, b.sc);
+        k_drag<N><<<g.nbody, 256, 0, s>>>(g, b.pbcp, b.omega, b.pres, b.visc, b.ptot, b.sc);
         k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force);
-        mark(4);
+        mark(3);
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {
-            k_rev<<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.nlbc[cur], b.nlbc[old], b.diffn, b.sc, b.rec, b.blockpart);
+            k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.blockpart);
             k_scal_c<<<1, 256, 0, s>>>(g, b.sc, b.blockpart, nbk);
             if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.fr, b.sc);
         }
-        mark(5);
+        mark(4);
         k_ff<N><<<g.nx, T, sm, s>>>(g, b.fr, b.ff, b.sc);
     } else {
-        mark(3); mark(4); mark(5);
+        mark(3); mark(4);
     }
-    mark(6);
-    k_lines<N, LinesCfg<N>::LT><<<(g.PS + LinesCfg<N>::LT - 1) / LinesCfg<N>::LT, LinesCfg<N>::LT * 32, lines_smem<N>(), s>>>(g, b.u, b.p, b.nl[cur], b.nl[old], b.ff, b.sc);
+    mark(5);
+    k_lines<N, LinesCfg<N>::LT><<<(g.PS + LinesCfg<N>::LT - 1) / LinesCfg<N>::LT, LinesCfg<N>::LT * 32, lines_smem<N>(), s>>>(
+        g, b.u, b.p, b.nl[cur], b.nl[old], b.ff, b.sc);
     k_scal_d<<<1, 32, 0, s>>>(g, b.sc);
-    mark(7);
+    mark(6);
 }
 
 // Kernels launched per step (for launch accounting).
 int kernels_per_step(const Geo &g) {
     int n = 5;   // a0, scal_a, nl, lines, scal_d
-    if (g.nbody > 0) n += 4 + (g.npts > 0 ? 2 + (g.sp_nnodes > 0 ? 1 : 0) : 0);
+    if (g.nbody > 0) n += 3 + (g.npts > 0 ? 2 + (g.sp_nnodes > 0 ? 1 : 0) : 0);
     return n;
 }
 
@@ -1139,10 +1112,9 @@ void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t
     }
 }
 
-// nlbc of a given spectral nl (used after set_state to rebuild the AB2 history).
 template <int N>
 static void enqueue_c2r_t(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s) {
-    k_ff2cr<N><<<nplanes, PT<N>::T, plane_smem<N>(g), s>>>(g, a, b);
+    k_ff2cr<N><<<nplanes, Plan<N>::T, plane_smem<N>(), s>>>(g, a, b);
 }
 void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s) {
     switch (g.my) {
@@ -1154,7 +1126,7 @@ void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStr
 }
 template <int N>
 static void enqueue_r2c_t(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s) {
-    k_ff2rc<N><<<nplanes, PT<N>::T, plane_smem<N>(g), s>>>(g, a, b);
+    k_ff2rc<N><<<nplanes, Plan<N>::T, plane_smem<N>(), s>>>(g, a, b);
 }
 void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s) {
     switch (g.my) {
