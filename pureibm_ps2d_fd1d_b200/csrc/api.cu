@@ -110,7 +110,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     Geo &g = h->g;
     std::memset(&g, 0, sizeof(g));
     g.nx = S.nx; g.my = S.my; g.mz = S.mz; g.my2 = S.my2;
-    g.PS = S.my2 * S.mz; g.RS = S.my * S.mz;
+    g.PS = S.my2 * S.mz; g.RS = (S.my + 2) * S.mz;   // physical real plane: rows of my+2 doubles
     g.dx = S.dx; g.dx2 = S.dx2; g.rdx2 = 1.0 / S.dx2; g.dx3 = S.dx3; g.vis = S.vis;
     g.nrm = (double)(float)(S.my * S.mz);
     g.c1 = S.coef[0]; g.c2 = S.coef[1]; g.c3 = S.coef[2]; g.c4 = S.coef[3];
@@ -133,15 +133,16 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     const size_t NC = (size_t)g.nx * g.PS, NR = (size_t)g.nx * g.RS;
     // physical fields are stored in the plane-transform order: permute the
     // solid mask and the spreading targets accordingly
-    std::vector<int> roff((size_t)g.RS);
+    const int nat = S.my * S.mz;   // natural plane size of the set-up arrays
+    std::vector<int> roff((size_t)nat);
     for (int z = 0; z < S.mz; ++z)
         for (int y = 0; y < S.my; ++y) roff[(size_t)z * S.my + y] = real_offset(S.my, z, y);
-    std::vector<uint8_t> fluid_p(S.fluid.size());
+    std::vector<uint8_t> fluid_p((size_t)S.nx * g.RS, 1);
     for (int i = 0; i < S.nx; ++i)
-        for (int e = 0; e < g.RS; ++e) fluid_p[(size_t)i * g.RS + roff[e]] = S.fluid[(size_t)i * g.RS + e];
+        for (int e = 0; e < nat; ++e) fluid_p[(size_t)i * g.RS + roff[e]] = S.fluid[(size_t)i * nat + e];
     std::vector<int> sp_node_p(S.sp_node.size());
     for (size_t q = 0; q < S.sp_node.size(); ++q) {
-        const int node = S.sp_node[q], i = node / g.RS, e = node - i * g.RS;
+        const int node = S.sp_node[q], i = node / nat, e = node - i * nat;
         sp_node_p[q] = i * g.RS + roff[e];
     }
     DevBufs &b = h->b;

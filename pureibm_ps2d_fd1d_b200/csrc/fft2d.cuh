@@ -256,10 +256,10 @@ __device__ __forceinline__ void plane_r2c(double2 *buf, const TwT &tw) {
 }
 
 // Offset of real node (z, y) inside one physical plane of the HBM real fields,
-// which are stored exactly as plane_c2r leaves them (row pitch my doubles), so
-// plane loads and stores are straight copies.
+// which are stored exactly as plane_c2r leaves the shared-memory buffer (rows
+// of my+2 doubles), so plane loads and stores are single bulk copies.
 template <int N> __device__ __host__ __forceinline__ int real_off(int z, int y) {
-    return (Plan<N>::BZ * (z % Plan<N>::AZ) + z / Plan<N>::AZ) * N + 2 * (Plan<N>::BY * ((y >> 1) % Plan<N>::AY) + (y >> 1) / Plan<N>::AY) + (y & 1);
+    return (Plan<N>::BZ * (z % Plan<N>::AZ) + z / Plan<N>::AZ) * (N + 2) + 2 * (Plan<N>::BY * ((y >> 1) % Plan<N>::AY) + (y >> 1) / Plan<N>::AY) + (y & 1);
 }
 
 }  // namespace pibm

@@ -29,6 +29,7 @@
 // once in spectral space (Q) instead of three separately interpolated fields.
 #include "engine.cuh"
 #include "fft2d.cuh"
+#include "bulk.cuh"
 #include "../../include/pibm.h"
 
 namespace pibm {
@@ -39,16 +40,13 @@ template <int N>
 __device__ __forceinline__ void load_tw(double2 *tws, const Geo &g) {
     for (int t = threadIdx.x; t < N; t += blockDim.x) tws[t] = g.tw[t];
 }
-// real plane (transform order, N x N doubles) <-> shared memory rows of pitch N+2 doubles
-template <int N>
-__device__ __forceinline__ void real_to_smem(double2 *buf, const double *__restrict__ src, double sub = 0.0) {
-    double *b = (double *)buf;
-    for (int e = threadIdx.x; e < N * N; e += blockDim.x) { const int r = e / N, c = e - r * N; b[r * (N + 2) + c] = src[e] - sub; }
-}
-template <int N>
-__device__ __forceinline__ double real_from_smem(const double2 *buf, int e) {
-    const int r = e / N, c = e - r * N;
-    return ((const double *)buf)[r * (N + 2) + c];
+// Physical real planes are RSP = N*(N+2) doubles: the shared-memory image of a
+// transformed plane (rows of N data doubles + 2 unused).
+template <int N> struct RP { static constexpr int RSP = N * (N + 2); static constexpr uint32_t BYTES = RSP * 8; };
+// Bounded wait on the CTA's load barrier; records a timeout in the status word.
+__device__ __forceinline__ void load_wait(uint64_t *mb, uint32_t &phase, Scal *sc) {
+    if (!mbar_wait(mb, phase)) atomicCAS(&sc->status, 0, PIBM_ERR_TIMEOUT);
+    phase ^= 1u;
 }
 // smem double offset of real node (z, y) (plane_c2r output order)
 template <int N> __device__ __forceinline__ int smem_real_off(int z, int y) {
@@ -103,68 +101,79 @@ template <int N>
 __global__ void __launch_bounds__(Plan<N>::T) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
                                                    double *__restrict__ ubcp, double *__restrict__ pbcp,
                                                    double *__restrict__ omega, double *__restrict__ pgr,
-                                                   const Scal *__restrict__ sc, double *__restrict__ part) {
+                                                   Scal *__restrict__ sc, double *__restrict__ part) {
     extern __shared__ double2 sm[];
-    constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
+    constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
     double2 *buf = sm, *tws = sm + PS;
     __shared__ double scr[32];
+    __shared__ uint64_t mb;
+    if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
+    __syncthreads();
+    uint32_t phase = 0;
     const int i = blockIdx.x, nx = g.nx;
     const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
     const TwT tw{tws, N};
     const double tdx = 2.0 * g.dx;
     const double2 *U0 = u + (size_t)i * PS, *U1 = u + ((size_t)nx + i) * PS, *U2 = u + ((size_t)2 * nx + i) * PS;
+    const double2 *Pp = p + (size_t)i * PS;
     double acc[12];
 #pragma unroll
     for (int q = 0; q < 9; ++q) acc[q] = 0.0;
     acc[9] = acc[10] = acc[11] = kSmallD;
     for (int t = 0; t < 10; ++t) {
-        for (int e = threadIdx.x; e < PS; e += blockDim.x) {
-            const int kz = e / my2, j = e - kz * my2;
-            const double ky = g.ky[j], kzv = g.kz[kz];
-            double2 f;
-            switch (t) {
-                case 0: f = U0[e]; break;
-                case 1: f = U1[e]; break;
-                case 2: f = U2[e]; break;
-                case 3: f = p[(size_t)i * PS + e]; break;
-                case 4: { const double2 a = U2[e], b = U1[e];   // wy*u3 - wz*u2
-                          f = make_double2(-ky * a.y - (-kzv * b.y), ky * a.x - kzv * b.x); } break;
-                case 5: { const double2 a = U0[e];              // wz*u1 - d(u3)/dx
-                          const double2 hp = u[((size_t)2 * nx + ip) * PS + e], hm = u[((size_t)2 * nx + im) * PS + e];
-                          const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
-                          f = make_double2(-kzv * a.y - d.x, kzv * a.x - d.y); } break;
-                case 6: { const double2 a = U0[e];              // d(u2)/dx - wy*u1
-                          const double2 hp = u[((size_t)nx + ip) * PS + e], hm = u[((size_t)nx + im) * PS + e];
-                          const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
-                          f = make_double2(d.x - (-ky * a.y), d.y - ky * a.x); } break;
-                case 7: { const double2 a = p[(size_t)ip * PS + e], b = p[(size_t)im * PS + e];
-                          f = make_double2((a.x - b.x) / tdx, (a.y - b.y) / tdx); } break;
-                case 8: { const double2 a = p[(size_t)i * PS + e]; f = make_double2(-a.y * ky, a.x * ky); } break;
-                default: { const double2 a = p[(size_t)i * PS + e]; f = make_double2(-a.y * kzv, a.x * kzv); } break;
+        if (t < 4) {
+            if (threadIdx.x == 0) bulk_load(buf, t == 0 ? U0 : t == 1 ? U1 : t == 2 ? U2 : Pp, PS * 16, &mb);
+            load_wait(&mb, phase, sc);
+        } else {
+            for (int e = threadIdx.x; e < PS; e += blockDim.x) {
+                const int kz = e / my2, j = e - kz * my2;
+                const double ky = g.ky[j], kzv = g.kz[kz];
+                double2 f;
+                if (t == 4) {   // wy*u3 - wz*u2
+                    const double2 a = U2[e], b = U1[e];
+                    f = make_double2(-ky * a.y - (-kzv * b.y), ky * a.x - kzv * b.x);
+                } else if (t == 5) {   // wz*u1 - d(u3)/dx
+                    const double2 a = U0[e];
+                    const double2 hp = u[((size_t)2 * nx + ip) * PS + e], hm = u[((size_t)2 * nx + im) * PS + e];
+                    const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
+                    f = make_double2(-kzv * a.y - d.x, kzv * a.x - d.y);
+                } else if (t == 6) {   // d(u2)/dx - wy*u1
+                    const double2 a = U0[e];
+                    const double2 hp = u[((size_t)nx + ip) * PS + e], hm = u[((size_t)nx + im) * PS + e];
+                    const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
+                    f = make_double2(d.x - (-ky * a.y), d.y - ky * a.x);
+                } else if (t == 7) {
+                    const double2 a = p[(size_t)ip * PS + e], b = p[(size_t)im * PS + e];
+                    f = make_double2((a.x - b.x) / tdx, (a.y - b.y) / tdx);
+                } else if (t == 8) { const double2 a = Pp[e]; f = make_double2(-a.y * ky, a.x * ky); }
+                else { const double2 a = Pp[e]; f = make_double2(-a.y * kzv, a.x * kzv); }
+                buf[e] = f;
             }
-            buf[e] = f;
+            __syncthreads();
         }
-        __syncthreads();
         plane_c2r<N>(buf, tw);
         if (t < 3) {
             const double um = sc->umean[t];
-            double *dst = ubcp + ((size_t)t * nx + i) * RS;
-            const uint8_t *fl = g.fluid + (size_t)i * RS;
-            for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-                const double v = real_from_smem<N>(buf, e) + um;
-                dst[e] = v;
+            double *b = (double *)buf;
+            const uint8_t *fl = g.fluid + (size_t)i * RSP;
+            for (int e = threadIdx.x; e < RSP; e += blockDim.x) {
+                if (e % (N + 2) >= N) continue;
+                const double v = b[e] + um;
+                b[e] = v;
                 if (fl[e]) acc[t] += v; else acc[3 + t] += v;
                 acc[6 + t] += v;
                 acc[9 + t] = fmax(acc[9 + t], fabs(v));
             }
-        } else {
-            double *dst = t == 3 ? pbcp + (size_t)i * RS
-                        : (t < 7 ? omega + ((size_t)(t - 4) * nx + i) * RS : pgr + ((size_t)(t - 7) * nx + i) * RS);
-            for (int e = threadIdx.x; e < RS; e += blockDim.x) dst[e] = real_from_smem<N>(buf, e);
+            __syncthreads();
         }
+        double *dst = t < 3 ? ubcp + ((size_t)t * nx + i) * RSP
+                    : t == 3 ? pbcp + (size_t)i * RSP
+                    : (t < 7 ? omega + ((size_t)(t - 4) * nx + i) * RSP : pgr + ((size_t)(t - 7) * nx + i) * RSP);
+        if (threadIdx.x == 0) { bulk_store(dst, buf, RP<N>::BYTES); bulk_wait_read(); }
         __syncthreads();
     }
+    if (threadIdx.x == 0) bulk_wait_all();
     for (int q = 0; q < 9; ++q) {
         const double s = block_sum(acc[q], scr);
         if (threadIdx.x == 0) part[(size_t)i * 12 + q] = s;
@@ -275,12 +284,13 @@ __device__ __forceinline__ double xflux_diff(const Geo &g, const double *__restr
 template <int N>
 __global__ void __launch_bounds__(Plan<N>::T) k_nl(Geo g, const double *__restrict__ ubcp, const double2 *__restrict__ u,
                                                    const double2 *__restrict__ onl, double2 *__restrict__ nl_new,
-                                                   double *__restrict__ Q, const Scal *__restrict__ sc) {
+                                                   double *__restrict__ Q, Scal *__restrict__ sc) {
     extern __shared__ double2 sm[];
-    constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
+    constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = RP<N>::RSP;
     constexpr int EPT = Plan<N>::EPT, T = Plan<N>::T;
     double2 *buf = sm, *tws = sm + PS;
     load_tw<N>(tws, g);
+    __syncthreads();
     const int i = blockIdx.x, nx = g.nx;
     const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
     const TwT tw{tws, N};
@@ -297,8 +307,7 @@ __global__ void __launch_bounds__(Plan<N>::T) k_nl(Geo g, const double *__restri
                 if (q == 0) v = Uc[pa0[c]][e] * Uc[pa1[c]][e];
                 else if (q == 1) v = Uc[pb0[c]][e] * Uc[pb1[c]][e];
                 else v = xflux_diff(g, ubcp, i, e, c);
-                const int r = e / N, cc = e - r * N;
-                b[r * (N + 2) + cc] = v;
+                b[e] = v;
             }
             __syncthreads();
             plane_r2c<N>(buf, tw);
@@ -335,10 +344,10 @@ __global__ void __launch_bounds__(Plan<N>::T) k_nl(Geo g, const double *__restri
         }
         __syncthreads();
         plane_c2r<N>(buf, tw);
-        double *rd = Q + ((size_t)c * nx + i) * RS;
-        for (int e = threadIdx.x; e < RS; e += blockDim.x) rd[e] = real_from_smem<N>(buf, e);
+        if (threadIdx.x == 0) { bulk_store(Q + ((size_t)c * nx + i) * RS, buf, RP<N>::BYTES); bulk_wait_read(); }
         __syncthreads();
     }
+    if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // ============================================================================
@@ -377,7 +386,7 @@ __device__ __forceinline__ void make_sten(const Geo &g, const double pos[3], Ste
 // value at node (x=i, y=j, z=k) of a physical field (one component)
 template <int N>
 __device__ __forceinline__ double fat(const double *f, int i, int j, int k) {
-    return __ldg(f + (size_t)i * (N * N) + real_off<N>(k, j));
+    return __ldg(f + (size_t)i * RP<N>::RSP + real_off<N>(k, j));
 }
 // interpolator order (k, j, i)
 template <int N>
@@ -417,7 +426,7 @@ __global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ 
     const int NB = g.nbody;
     const double xcm[3] = {g.xc[m], g.xc[m + NB], g.xc[m + 2 * NB]};
     double sa[3] = {0, 0, 0}, sb[3] = {0, 0, 0};
-    const size_t CR = (size_t)g.nx * N * N;
+    const size_t CR = (size_t)g.nx * RP<N>::RSP;
     for (int l = threadIdx.x; l < g.nbnd; l += blockDim.x) {
         double xl[3], xpb[3], cdl[3];
 #pragma unroll
@@ -521,7 +530,7 @@ __global__ void __launch_bounds__(256) k_rev(Geo g, const double *__restrict__ u
     double fm[3] = {0, 0, 0}, ffl[3] = {0, 0, 0};
     if (p < g.npts && !sc->status) {
         const int m = g.pt_m[p], l = g.pt_l[p], NB = g.nbody;
-        const size_t CR = (size_t)g.nx * N * N;
+        const size_t CR = (size_t)g.nx * RP<N>::RSP;
         double xli[3], xlo[3], xpi[3], snorm[3];
         inner_point(g, m, l, xli);
         double rad = 0.0;
@@ -582,7 +591,7 @@ __global__ void __launch_bounds__(256) k_rev(Geo g, const double *__restrict__ u
             for (int b = 0; b < 2; ++b)
 #pragma unroll
                 for (int a = 0; a < 2; ++a) {
-                    const bool fl = g.fluid[(size_t)si.ii[a] * (N * N) + real_off<N>(si.kk[c], si.jj[b])] != 0;
+                    const bool fl = g.fluid[(size_t)si.ii[a] * RP<N>::RSP + real_off<N>(si.kk[c], si.jj[b])] != 0;
                     const double w = si.w(a, b, c);
 #pragma unroll
                     for (int n = 0; n < 3; ++n) {
@@ -653,21 +662,31 @@ __global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict_
 // k_ff: ff = r2c(fr - frmean) (boundary_condition.F90:678-700).
 template <int N>
 __global__ void __launch_bounds__(Plan<N>::T) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
-                                                   const Scal *__restrict__ sc) {
+                                                   Scal *__restrict__ sc) {
     extern __shared__ double2 sm[];
-    constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
+    constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
     double2 *buf = sm, *tws = sm + PS;
+    __shared__ uint64_t mb;
+    if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
+    __syncthreads();
+    uint32_t phase = 0;
     const int i = blockIdx.x, nx = g.nx;
     const TwT tw{tws, N};
     for (int n = 0; n < 3; ++n) {
-        real_to_smem<N>(buf, fr + ((size_t)n * nx + i) * RS, sc->frmean[n]);
+        if (threadIdx.x == 0) bulk_load(buf, fr + ((size_t)n * nx + i) * RSP, RP<N>::BYTES, &mb);
+        load_wait(&mb, phase, sc);
+        const double fmn = sc->frmean[n];
+        double *b = (double *)buf;
+        for (int e = threadIdx.x; e < RSP; e += blockDim.x) b[e] = b[e] - fmn;
         __syncthreads();
         plane_r2c<N>(buf, tw);
-        double2 *dst = ff + ((size_t)n * nx + i) * PS;
-        for (int e = threadIdx.x; e < PS; e += blockDim.x) dst[e] = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
+        for (int e = threadIdx.x; e < PS; e += blockDim.x) buf[e] = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
+        __syncthreads();
+        if (threadIdx.x == 0) { bulk_store(ff + ((size_t)n * nx + i) * PS, buf, PS * 16); bulk_wait_read(); }
         __syncthreads();
     }
+    if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // ============================================================================
