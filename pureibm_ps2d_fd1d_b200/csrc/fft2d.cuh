@@ -95,164 +95,234 @@ template <> struct Dft<12> : DftComp<4, 3> {};
 template <> struct Dft<16> : DftComp<4, 4> {};
 
 // ---------------------------------------------------------------------------
-// Passes over S sequences: element e of sequence s at buf[s*ss + e*es].
-// Work units are distributed with the sequence index fastest so that
-// consecutive threads touch consecutive rows/columns.  Ends with __syncthreads.
+// Per-size plans: z length N = AZ*BZ, y half length M = N/2 = AY*BY, T threads.
+// EPT = spectral elements per thread (ceil(my2*N / T)).
 // ---------------------------------------------------------------------------
-template <int A, int B>
-__device__ __forceinline__ void fft_v1(double2 *buf, int S, int ss, int es, double s, const TwT &tw) {
-    constexpr int L = A * B;
-    const int T = blockDim.x;
-    for (int u = threadIdx.x; u < S * B; u += T) {
-        const int q = u % S, n2 = u / S;
-        double2 *base = buf + (size_t)q * ss + n2 * es;
-        double2 v[A];
-#pragma unroll
-        for (int n1 = 0; n1 < A; ++n1) v[n1] = base[(size_t)(B * n1) * es];
-        Dft<A>::run(v, s, tw);
-#pragma unroll
-        for (int k1 = 1; k1 < A; ++k1) v[k1] = cmul(v[k1], tw.w(n2 * k1, L, s));
-#pragma unroll
-        for (int k1 = 0; k1 < A; ++k1) base[(size_t)(B * k1) * es] = v[k1];
-    }
-    __syncthreads();
-    for (int u = threadIdx.x; u < S * A; u += T) {
-        const int q = u % S, k1 = u / S;
-        double2 *base = buf + (size_t)q * ss + (size_t)(B * k1) * es;
-        double2 v[B];
-#pragma unroll
-        for (int n2 = 0; n2 < B; ++n2) v[n2] = base[(size_t)n2 * es];
-        Dft<B>::run(v, s, tw);
-#pragma unroll
-        for (int k2 = 0; k2 < B; ++k2) base[(size_t)k2 * es] = v[k2];
-    }
-    __syncthreads();
-}
+template <int N> struct Plan;
+template <> struct Plan<32>  { static constexpr int AZ = 8,  BZ = 4, AY = 4,  BY = 4, T = 256, EPT = 3; };
+template <> struct Plan<64>  { static constexpr int AZ = 8,  BZ = 8, AY = 8,  BY = 4, T = 256, EPT = 9; };
+template <> struct Plan<96>  { static constexpr int AZ = 12, BZ = 8, AY = 12, BY = 4, T = 512, EPT = 10; };
+template <> struct Plan<128> { static constexpr int AZ = 16, BZ = 8, AY = 8,  BY = 8, T = 512, EPT = 17; };
 
-template <int A, int B>
-__device__ __forceinline__ void fft_v2(double2 *buf, int S, int ss, int es, double s, const TwT &tw) {
-    constexpr int L = A * B;
-    const int T = blockDim.x;
-    for (int u = threadIdx.x; u < S * A; u += T) {
-        const int q = u % S, n1 = u / S;
-        double2 *base = buf + (size_t)q * ss + (size_t)(B * n1) * es;
-        double2 v[B];
-#pragma unroll
-        for (int n2 = 0; n2 < B; ++n2) v[n2] = base[(size_t)n2 * es];
-        Dft<B>::run(v, s, tw);
-#pragma unroll
-        for (int k2 = 1; k2 < B; ++k2) v[k2] = cmul(v[k2], tw.w(n1 * k2, L, s));
-#pragma unroll
-        for (int k2 = 0; k2 < B; ++k2) base[(size_t)k2 * es] = v[k2];
-    }
-    __syncthreads();
-    for (int u = threadIdx.x; u < S * B; u += T) {
-        const int q = u % S, k2 = u / S;
-        double2 *base = buf + (size_t)q * ss + k2 * es;
-        double2 v[A];
-#pragma unroll
-        for (int n1 = 0; n1 < A; ++n1) v[n1] = base[(size_t)(B * n1) * es];
-        Dft<A>::run(v, s, tw);
-#pragma unroll
-        for (int k1 = 0; k1 < A; ++k1) base[(size_t)(B * k1) * es] = v[k1];
-    }
-    __syncthreads();
-}
+// smem row of physical z after an inverse z pass (bfft_v1 output order), and
+// the slot of real pair index m in a row (bfft_v1 output / bfft_v2 input order).
+template <int N> __device__ __forceinline__ int zrow(int z) { return perm_ab<Plan<N>::AZ, Plan<N>::BZ>(z); }
+template <int N> __device__ __forceinline__ int yslot(int m) { return perm_ab<Plan<N>::AY, Plan<N>::BY>(m); }
 
-// c2r reconstruction of the half-length complex sequence of every row (natural
-// order): Z[n] = (X[n] + conj X[M-n]) + i w+^n (X[n] - conj X[M-n]), n < M,
-// with Im X[0] = Im X[M] = 0 (FFTW / numpy irfft semantics).
+// c2r reconstruction of one element pair: Z[n] = (X[n] + conj X[M-n]) + i w+^n (X[n] - conj X[M-n]).
 __device__ __forceinline__ double2 c2r_pre_one(double2 xk, double2 xm, double2 wp) {
     const double2 e = make_double2(xk.x + xm.x, xk.y - xm.y);
     const double2 d = make_double2(xk.x - xm.x, xk.y + xm.y);
     const double2 od = cmul(d, wp);
     return make_double2(e.x - od.y, e.y + od.x);
 }
-__device__ __forceinline__ void y_c2r_pre(double2 *buf, int rows, int pitch, int M, const TwT &tw) {
-    const int T = blockDim.x;
-    const int npair = M / 2 + 1;
-    for (int u = threadIdx.x; u < rows * npair; u += T) {
-        const int k = u % rows, n = u / rows;
-        double2 *row = buf + (size_t)k * pitch;
-        if (n == 0) {
-            double2 x0 = row[0], xM = row[M];
-            x0.y = 0.0; xM.y = 0.0;
-            row[0] = c2r_pre_one(x0, xM, make_double2(1.0, 0.0));
-        } else if (2 * n == M) {
-            const double2 x = row[n];
-            row[n] = c2r_pre_one(x, x, tw.w(n, 2 * M, +1.0));
-        } else {
-            const double2 xa = row[n], xb = row[M - n];
-            row[n] = c2r_pre_one(xa, xb, tw.w(n, 2 * M, +1.0));
-            row[M - n] = c2r_pre_one(xb, xa, tw.w(M - n, 2 * M, +1.0));
-        }
-    }
-    __syncthreads();
-}
-
-// r2c split of every row: X[n] = (Z[n] + conj Z[M-n])/2 + w-^n (Z[n] - conj Z[M-n])/(2i),
-// n = 0..M, Z[M] = Z[0].
+// r2c split of one element pair: X[n] = (Z[n] + conj Z[M-n])/2 + w-^n (Z[n] - conj Z[M-n])/(2i).
 __device__ __forceinline__ double2 r2c_post_one(double2 zk, double2 zm, double2 wm) {
     const double2 e = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
     const double2 o = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
     return cadd(e, cmul(wm, o));
 }
-__device__ __forceinline__ void y_r2c_post(double2 *buf, int rows, int pitch, int M, const TwT &tw) {
-    const int T = blockDim.x;
-    const int npair = M / 2 + 1;
-    for (int u = threadIdx.x; u < rows * npair; u += T) {
-        const int k = u % rows, n = u / rows;
-        double2 *row = buf + (size_t)k * pitch;
-        if (n == 0) {
-            const double2 z0 = row[0];
-            row[0] = make_double2(z0.x + z0.y, 0.0);
-            row[M] = make_double2(z0.x - z0.y, 0.0);
-        } else if (2 * n == M) {
-            const double2 z = row[n];
-            row[n] = r2c_post_one(z, z, tw.w(n, 2 * M, -1.0));
-        } else {
-            const double2 za = row[n], zb = row[M - n];
-            row[n] = r2c_post_one(za, zb, tw.w(n, 2 * M, -1.0));
-            row[M - n] = r2c_post_one(zb, za, tw.w(M - n, 2 * M, -1.0));
+
+// ---------------------------------------------------------------------------
+// Block-wide passes over S sequences (element e of sequence q at
+// buf[q*ss + e*es]) with a compile-time thread count T, so that the rounds a
+// thread executes are unrolled and interleaved.  Units are distributed with
+// the sequence index fastest: consecutive threads touch consecutive columns
+// (stride 1) or rows (stride pitch = my2, 4 banks apart), conflict-free.
+// Each pass ends with __syncthreads.
+// ---------------------------------------------------------------------------
+template <int A, int B, int S, int T>
+__device__ __forceinline__ void bfft_v1(double2 *buf, int ss, int es, double s, const TwT &tw) {
+    constexpr int L = A * B;
+#pragma unroll
+    for (int u0 = 0; u0 < S * B; u0 += T) {
+        const int u = u0 + (int)threadIdx.x;
+        if (u < S * B) {
+            const int q = u % S, n2 = u / S;
+            double2 *base = buf + (size_t)q * ss + n2 * es;
+            double2 v[A];
+#pragma unroll
+            for (int n1 = 0; n1 < A; ++n1) v[n1] = base[(size_t)(B * n1) * es];
+            Dft<A>::run(v, s, tw);
+#pragma unroll
+            for (int k1 = 1; k1 < A; ++k1) v[k1] = cmul(v[k1], tw.w(n2 * k1, L, s));
+#pragma unroll
+            for (int k1 = 0; k1 < A; ++k1) base[(size_t)(B * k1) * es] = v[k1];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u0 = 0; u0 < S * A; u0 += T) {
+        const int u = u0 + (int)threadIdx.x;
+        if (u < S * A) {
+            const int q = u % S, k1 = u / S;
+            double2 *base = buf + (size_t)q * ss + (size_t)(B * k1) * es;
+            double2 v[B];
+#pragma unroll
+            for (int n2 = 0; n2 < B; ++n2) v[n2] = base[(size_t)n2 * es];
+            Dft<B>::run(v, s, tw);
+#pragma unroll
+            for (int k2 = 0; k2 < B; ++k2) base[(size_t)k2 * es] = v[k2];
+        }
+    }
+    __syncthreads();
+}
+
+template <int A, int B, int S, int T>
+__device__ __forceinline__ void bfft_v2(double2 *buf, int ss, int es, double s, const TwT &tw) {
+    constexpr int L = A * B;
+#pragma unroll
+    for (int u0 = 0; u0 < S * A; u0 += T) {
+        const int u = u0 + (int)threadIdx.x;
+        if (u < S * A) {
+            const int q = u % S, n1 = u / S;
+            double2 *base = buf + (size_t)q * ss + (size_t)(B * n1) * es;
+            double2 v[B];
+#pragma unroll
+            for (int n2 = 0; n2 < B; ++n2) v[n2] = base[(size_t)n2 * es];
+            Dft<B>::run(v, s, tw);
+#pragma unroll
+            for (int k2 = 1; k2 < B; ++k2) v[k2] = cmul(v[k2], tw.w(n1 * k2, L, s));
+#pragma unroll
+            for (int k2 = 0; k2 < B; ++k2) base[(size_t)k2 * es] = v[k2];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u0 = 0; u0 < S * B; u0 += T) {
+        const int u = u0 + (int)threadIdx.x;
+        if (u < S * B) {
+            const int q = u % S, k2 = u / S;
+            double2 *base = buf + (size_t)q * ss + k2 * es;
+            double2 v[A];
+#pragma unroll
+            for (int n1 = 0; n1 < A; ++n1) v[n1] = base[(size_t)(B * n1) * es];
+            Dft<A>::run(v, s, tw);
+#pragma unroll
+            for (int k1 = 0; k1 < A; ++k1) base[(size_t)(B * k1) * es] = v[k1];
         }
     }
     __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
-// Per-size plans: z length N = A_z*B_z, y half length M = N/2 = A_y*B_y.
+// Packed ky = 0 / ky = M columns.  The two columns share one complex z
+// transform held in column 0:
+//  c2r: only Re of their inverse z transforms is used (the y reconstruction
+//       drops the imaginary parts of ky = 0 and ky = M), and
+//       Re(IFFT X) = IFFT(Herm X), Herm X[k] = (X[k] + conj X[-k])/2, so
+//       column 0 <- Herm X0 + i Herm XM; the y reconstruction reads
+//       Re -> ky = 0 and Im -> ky = M back from column 0.
+//  r2c: both columns are real after the y pass, column 0 <- X0 + i XM; the
+//       spectrum is read back with unpack_col (A = (Y[k] + conj Y[-k])/2,
+//       B = (Y[k] - conj Y[-k])/(2i)).
 // ---------------------------------------------------------------------------
-template <int N> struct Plan;  // AZ*BZ = N, AY*BY = N/2
-template <> struct Plan<32>  { static constexpr int AZ = 8,  BZ = 4, AY = 4,  BY = 4, T = 256, EPT = 3; };
-template <> struct Plan<64>  { static constexpr int AZ = 8,  BZ = 8, AY = 8,  BY = 4, T = 256, EPT = 9; };
-template <> struct Plan<96>  { static constexpr int AZ = 12, BZ = 8, AY = 12, BY = 4, T = 512, EPT = 10; };
-template <> struct Plan<128> { static constexpr int AZ = 16, BZ = 8, AY = 8,  BY = 8, T = 512, EPT = 17; };
+__device__ __forceinline__ double2 herm_pack(double2 a, double2 am, double2 b, double2 bm) {
+    const double2 h0 = make_double2(0.5 * (a.x + am.x), 0.5 * (a.y - am.y));
+    const double2 hm = make_double2(0.5 * (b.x + bm.x), 0.5 * (b.y - bm.y));
+    return make_double2(h0.x - hm.y, h0.y + hm.x);
+}
+// In place on a natural spectrum in buf (warp 0 only; caller synchronises).
+template <int N>
+__device__ __forceinline__ void pack_col0_warp(double2 *buf) {
+    constexpr int M = N / 2, P = N / 2 + 1, R = (N + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    double2 y[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        if (k < N) {
+            const int km = (N - k) % N;
+            y[r] = herm_pack(buf[(size_t)k * P], buf[(size_t)km * P], buf[(size_t)k * P + M], buf[(size_t)km * P + M]);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        if (k < N) buf[(size_t)k * P] = y[r];
+    }
+}
+// Spectral value (kz, j) of an r2c result whose ky = 0 / M columns are packed.
+template <int N>
+__device__ __forceinline__ double2 unpack_col(const double2 *buf, int kz, int j) {
+    constexpr int M = N / 2, P = N / 2 + 1;
+    if (j != 0 && j != M) return buf[(size_t)kz * P + j];
+    const double2 y = buf[(size_t)kz * P], ym = buf[(size_t)((N - kz) % N) * P];
+    if (j == 0) return make_double2(0.5 * (y.x + ym.x), 0.5 * (y.y - ym.y));
+    return make_double2(0.5 * (y.y + ym.y), -0.5 * (y.x - ym.x));
+}
 
-// smem row of spectral z index kz after a z pass (fft_v1 output order), and
-// the slot of real pair index m in a row (fft_v1 output / fft_v2 input order).
-template <int N> __device__ __forceinline__ int zrow(int kz) { return perm_ab<Plan<N>::AZ, Plan<N>::BZ>(kz); }
-template <int N> __device__ __forceinline__ int yslot(int m) { return perm_ab<Plan<N>::AY, Plan<N>::BY>(m); }
-// inverse of zrow: the kz held by smem row p
-template <int N> __device__ __forceinline__ int kz_of_row(int p) { return p / Plan<N>::BZ + Plan<N>::AZ * (p % Plan<N>::BZ); }
+// c2r reconstruction of every row with the packed ky = 0 / M column.
+template <int N, int T>
+__device__ __forceinline__ void b_c2r_pre(double2 *buf, const TwT &tw) {
+    constexpr int M = N / 2, P = N / 2 + 1, NP = M / 2 + 1;
+#pragma unroll 3
+    for (int u0 = 0; u0 < N * NP; u0 += T) {
+        const int u = u0 + (int)threadIdx.x;
+        if (u < N * NP) {
+            const int k = u % N, n = u / N;
+            double2 *row = buf + (size_t)k * P;
+            if (n == 0) {
+                const double2 y = row[0];
+                row[0] = c2r_pre_one(make_double2(y.x, 0.0), make_double2(y.y, 0.0), make_double2(1.0, 0.0));
+            } else if (2 * n == M) {
+                const double2 x = row[n];
+                row[n] = c2r_pre_one(x, x, tw.w(n, 2 * M, +1.0));
+            } else {
+                const double2 xa = row[n], xb = row[M - n];
+                row[n] = c2r_pre_one(xa, xb, tw.w(n, 2 * M, +1.0));
+                row[M - n] = c2r_pre_one(xb, xa, tw.w(M - n, 2 * M, +1.0));
+            }
+        }
+    }
+    __syncthreads();
+}
+// r2c split of every row; ky = 0 and ky = M (both real) are packed into slot 0.
+template <int N, int T>
+__device__ __forceinline__ void b_r2c_post(double2 *buf, const TwT &tw) {
+    constexpr int M = N / 2, P = N / 2 + 1, NP = M / 2 + 1;
+#pragma unroll 3
+    for (int u0 = 0; u0 < N * NP; u0 += T) {
+        const int u = u0 + (int)threadIdx.x;
+        if (u < N * NP) {
+            const int k = u % N, n = u / N;
+            double2 *row = buf + (size_t)k * P;
+            if (n == 0) {
+                const double2 z0 = row[0];
+                row[0] = make_double2(z0.x + z0.y, z0.x - z0.y);
+            } else if (2 * n == M) {
+                const double2 z = row[n];
+                row[n] = r2c_post_one(z, z, tw.w(n, 2 * M, -1.0));
+            } else {
+                const double2 za = row[n], zb = row[M - n];
+                row[n] = r2c_post_one(za, zb, tw.w(n, 2 * M, -1.0));
+                row[M - n] = r2c_post_one(zb, za, tw.w(M - n, 2 * M, -1.0));
+            }
+        }
+    }
+    __syncthreads();
+}
 
-// c2r of the plane in buf (natural spectral rows kz, columns ky).  On return,
+// c2r of a natural spectrum whose ky = 0 / M columns are packed into column 0
+// (see pack_col0_warp / herm_pack); call after a __syncthreads.  On return
 // real value (z, y) is ((double*)&buf[zrow(z)*pitch + yslot(y/2)])[y&1].
 template <int N>
 __device__ __forceinline__ void plane_c2r(double2 *buf, const TwT &tw) {
-    constexpr int my2 = N / 2 + 1, M = N / 2;
-    fft_v1<Plan<N>::AZ, Plan<N>::BZ>(buf, my2, 1, my2, +1.0, tw);
-    y_c2r_pre(buf, N, my2, M, tw);
-    fft_v1<Plan<N>::AY, Plan<N>::BY>(buf, N, my2, 1, +1.0, tw);
+    constexpr int P = N / 2 + 1, M = N / 2, T = Plan<N>::T;
+    bfft_v1<Plan<N>::AZ, Plan<N>::BZ, M, T>(buf, 1, P, +1.0, tw);
+    b_c2r_pre<N, T>(buf, tw);
+    bfft_v1<Plan<N>::AY, Plan<N>::BY, N, T>(buf, P, 1, +1.0, tw);
 }
-// r2c of the plane whose real value (z, y) is stored in the c2r output order
-// above.  On return the unscaled spectrum (kz, ky) is at buf[kz*pitch + ky]
-// (natural order).
+// r2c of a plane stored in the c2r output order; call after a __syncthreads.
+// On return the unscaled spectrum is natural with ky = 0 / M packed into
+// column 0: read it with unpack_col.
 template <int N>
 __device__ __forceinline__ void plane_r2c(double2 *buf, const TwT &tw) {
-    constexpr int my2 = N / 2 + 1, M = N / 2;
-    fft_v2<Plan<N>::AY, Plan<N>::BY>(buf, N, my2, 1, -1.0, tw);
-    y_r2c_post(buf, N, my2, M, tw);
-    fft_v2<Plan<N>::AZ, Plan<N>::BZ>(buf, my2, 1, my2, -1.0, tw);
+    constexpr int P = N / 2 + 1, M = N / 2, T = Plan<N>::T;
+    bfft_v2<Plan<N>::AY, Plan<N>::BY, N, T>(buf, P, 1, -1.0, tw);
+    b_r2c_post<N, T>(buf, tw);
+    bfft_v2<Plan<N>::AZ, Plan<N>::BZ, M, T>(buf, 1, P, -1.0, tw);
 }
 
 // Offset of real node (z, y) inside one physical plane of the HBM real fields,

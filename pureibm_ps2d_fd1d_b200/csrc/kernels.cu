@@ -98,7 +98,7 @@ __device__ __forceinline__ double block_max(double v, double *scr) {
 // part[i*12 + q]: q 0-2 fluid sums, 3-5 solid sums, 6-8 all sums, 9-11 max |u|.
 // ============================================================================
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
+__global__ void __launch_bounds__(Plan<N>::T, 1) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
                                                    double *__restrict__ ubcp, double *__restrict__ pbcp,
                                                    double *__restrict__ omega, double *__restrict__ pgr,
                                                    Scal *__restrict__ sc, double *__restrict__ part) {
@@ -152,6 +152,8 @@ __global__ void __launch_bounds__(Plan<N>::T) k_a0(Geo g, const double2 *__restr
             }
             __syncthreads();
         }
+        if (threadIdx.x < 32) pack_col0_warp<N>(buf);
+        __syncthreads();
         plane_c2r<N>(buf, tw);
         if (t < 3) {
             const double um = sc->umean[t];
@@ -282,7 +284,7 @@ __device__ __forceinline__ double xflux_diff(const Geo &g, const double *__restr
 }
 
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T) k_nl(Geo g, const double *__restrict__ ubcp, const double2 *__restrict__ u,
+__global__ void __launch_bounds__(Plan<N>::T, 1) k_nl(Geo g, const double *__restrict__ ubcp, const double2 *__restrict__ u,
                                                    const double2 *__restrict__ onl, double2 *__restrict__ nl_new,
                                                    double *__restrict__ Q, Scal *__restrict__ sc) {
     extern __shared__ double2 sm[];
@@ -315,8 +317,9 @@ __global__ void __launch_bounds__(Plan<N>::T) k_nl(Geo g, const double *__restri
             for (int s = 0; s < EPT; ++s) {
                 const int e = threadIdx.x + s * T;
                 if (e < PS) {
-                    const double2 X = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
                     const int kz = e / my2, j = e - kz * my2;
+                    const double2 Xr = unpack_col<N>(buf, kz, j);
+                    const double2 X = make_double2(Xr.x / g.nrm, Xr.y / g.nrm);
                     if (q == 0) { const double ky = g.ky[j]; acc[s] = make_double2(-ky * X.y, ky * X.x); }
                     else if (q == 1) { const double kzv = g.kz[kz]; acc[s] = cadd(acc[s], make_double2(-kzv * X.y, kzv * X.x)); }
                     else acc[s] = cadd(acc[s], X);
@@ -342,6 +345,8 @@ __global__ void __launch_bounds__(Plan<N>::T) k_nl(Geo g, const double *__restri
                 buf[e] = make_double2((-g.c3 * v.x - g.c4 * o.x) - c12 * df.x, (-g.c3 * v.y - g.c4 * o.y) - c12 * df.y);
             }
         }
+        __syncthreads();
+        if (threadIdx.x < 32) pack_col0_warp<N>(buf);
         __syncthreads();
         plane_c2r<N>(buf, tw);
         if (threadIdx.x == 0) { bulk_store(Q + ((size_t)c * nx + i) * RS, buf, RP<N>::BYTES); bulk_wait_read(); }
@@ -661,7 +666,7 @@ __global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict_
 
 // k_ff: ff = r2c(fr - frmean) (boundary_condition.F90:678-700).
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
+__global__ void __launch_bounds__(Plan<N>::T, 1) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
                                                    Scal *__restrict__ sc) {
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
@@ -681,9 +686,12 @@ __global__ void __launch_bounds__(Plan<N>::T) k_ff(Geo g, const double *__restri
         for (int e = threadIdx.x; e < RSP; e += blockDim.x) b[e] = b[e] - fmn;
         __syncthreads();
         plane_r2c<N>(buf, tw);
-        for (int e = threadIdx.x; e < PS; e += blockDim.x) buf[e] = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
-        __syncthreads();
-        if (threadIdx.x == 0) { bulk_store(ff + ((size_t)n * nx + i) * PS, buf, PS * 16); bulk_wait_read(); }
+        double2 *dst = ff + ((size_t)n * nx + i) * PS;
+        for (int e = threadIdx.x; e < PS; e += blockDim.x) {
+            const int kz = e / my2, j = e - kz * my2;
+            const double2 X = unpack_col<N>(buf, kz, j);
+            dst[e] = make_double2(X.x / g.nrm, X.y / g.nrm);
+        }
         __syncthreads();
     }
     if (threadIdx.x == 0) bulk_wait_all();
@@ -1005,7 +1013,7 @@ __global__ void k_d2f(const double2 *__restrict__ d, double2 *__restrict__ f, in
 // Standalone batched plane transforms (pibm_ff2rc / pibm_ff2cr) on natural
 // host layouts: real a[z*my + y], complex b[kz*my2 + ky].
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T) k_ff2cr(Geo g, const double2 *__restrict__ a, double *__restrict__ b) {
+__global__ void __launch_bounds__(Plan<N>::T, 1) k_ff2cr(Geo g, const double2 *__restrict__ a, double *__restrict__ b) {
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
     double2 *buf = sm, *tws = sm + PS;
@@ -1014,6 +1022,8 @@ __global__ void __launch_bounds__(Plan<N>::T) k_ff2cr(Geo g, const double2 *__re
     const size_t q = blockIdx.x;
     for (int e = threadIdx.x; e < PS; e += blockDim.x) buf[e] = a[q * PS + e];
     __syncthreads();
+    if (threadIdx.x < 32) pack_col0_warp<N>(buf);
+    __syncthreads();
     plane_c2r<N>(buf, tw);
     for (int e = threadIdx.x; e < RS; e += blockDim.x) {
         const int z = e / N, y = e - z * N;
@@ -1021,7 +1031,7 @@ __global__ void __launch_bounds__(Plan<N>::T) k_ff2cr(Geo g, const double2 *__re
     }
 }
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T) k_ff2rc(Geo g, const double *__restrict__ a, double2 *__restrict__ b) {
+__global__ void __launch_bounds__(Plan<N>::T, 1) k_ff2rc(Geo g, const double *__restrict__ a, double2 *__restrict__ b) {
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
     double2 *buf = sm, *tws = sm + PS;
@@ -1034,7 +1044,11 @@ __global__ void __launch_bounds__(Plan<N>::T) k_ff2rc(Geo g, const double *__res
     }
     __syncthreads();
     plane_r2c<N>(buf, tw);
-    for (int e = threadIdx.x; e < PS; e += blockDim.x) b[q * PS + e] = make_double2(buf[e].x / g.nrm, buf[e].y / g.nrm);
+    for (int e = threadIdx.x; e < PS; e += blockDim.x) {
+        const int kz = e / my2, j = e - kz * my2;
+        const double2 X = unpack_col<N>(buf, kz, j);
+        b[q * PS + e] = make_double2(X.x / g.nrm, X.y / g.nrm);
+    }
 }
 
 // ============================================================================
