@@ -156,13 +156,14 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
               guard(h->alloc(&b.u, 3 * NC), "u") && guard(h->alloc(&b.p, NC), "p") &&
               guard(h->alloc(&b.nl[0], 3 * NC), "nl0") && guard(h->alloc(&b.nl[1], 3 * NC), "nl1") &&
               guard(h->alloc(&b.ff, 3 * NC), "ff") && guard(h->alloc(&b.ubcp, 3 * NR), "ubcp") &&
-              guard(h->alloc(&b.pbcp, NR), "pbcp") && guard(h->alloc(&b.Q, 3 * NR), "Q") &&
+              guard(h->alloc(&b.pbcp, NR), "pbcp") && guard(h->alloc(&b.Q, 3 * NR), "Q") && guard(h->alloc(&b.Dx, 3 * NR), "Dx") &&
               guard(h->alloc(&b.omega, 3 * NR), "omega") && guard(h->alloc(&b.pgr, 3 * NR), "pgr") &&
               (S.nbody == 0 || guard(h->alloc(&b.fr, 3 * NR), "fr")) &&
               guard(h->alloc(&b.part, (size_t)g.nx * 12), "part") &&
               guard(h->alloc(&b.pres, 3 * (size_t)S.nbody), "pres") && guard(h->alloc(&b.visc, 3 * (size_t)S.nbody), "visc") &&
               guard(h->alloc(&b.ptot, 3 * (size_t)S.nbody), "ptot") && guard(h->alloc(&b.force, 3 * (size_t)S.nbody), "force") &&
-              guard(h->alloc(&b.rec, 6 * (size_t)g.npts), "rec") &&
+              guard(h->alloc(&b.rec, 6 * (size_t)g.npts), "rec") && guard(h->alloc(&b.ctb, 24 * (size_t)g.npts), "ctb") &&
+              guard(h->alloc(&b.dpart, 6 * 8 * (size_t)S.nbody), "dpart") &&
               guard(h->alloc(&b.blockpart, 6 * (size_t)((g.npts + 255) / 256 + 1)), "blockpart") &&
               guard(h->alloc(&b.sc, 1), "scalars");
     if (!ok) { delete h; return rc; }

@@ -49,8 +49,8 @@ struct Scal {
 // Device buffers of one run.
 struct DevBufs {
     double2 *u, *p, *nl[2], *ff;
-    double *ubcp, *pbcp, *Q, *omega, *pgr, *fr;
-    double *part, *pres, *visc, *ptot, *force, *rec, *blockpart;
+    double *ubcp, *pbcp, *Q, *omega, *pgr, *fr, *Dx;
+    double *part, *pres, *visc, *ptot, *force, *rec, *ctb, *dpart, *blockpart;
     Scal *sc;
 };
 

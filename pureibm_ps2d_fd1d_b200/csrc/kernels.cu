@@ -283,16 +283,102 @@ __device__ __forceinline__ double xflux_diff(const Geo &g, const double *__restr
     return (F[1] - F[0]) / dx;
 }
 
+// ============================================================================
+// k_flux: x-flux differences D_c(i) = (F_c(i) - F_c(i-1))/dx of the conservative
+// nonlinear term for all nodes (nl_allflow.F90:121-310).  One thread owns one
+// (y,z) node and a segment of SEG x-planes and streams along x with a rolling
+// window, so every ubcp value is read once per segment (plus a 4-plane halo).
+// Upwind: MUSCL states with optional minmod limiter and a Rusanov flux; the
+// periodic interface between cells nx and 1 accumulates its two halves in the
+// reference's order (cell 1's contribution first).  Center: (f(i+1)-f(i-1))/(2dx).
+// ============================================================================
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T, 1) k_nl(Geo g, const double *__restrict__ ubcp, const double2 *__restrict__ u,
+__global__ void __launch_bounds__(256) k_flux(Geo g, const double *__restrict__ ubcp, double *__restrict__ Dx,
+                                              const Scal *__restrict__ sc) {
+    constexpr int RSP = RP<N>::RSP, SEG = 32;
+    const int nx = g.nx, nseg = nx / SEG;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= RSP * nseg || sc->status) return;
+    const int e = t % RSP, i0 = (t / RSP) * SEG;
+    if (e % (N + 2) >= N) return;   // row padding
+    const size_t CR = (size_t)nx * RSP;
+    auto U = [&](int c, int ii) -> double {
+        ii = ii < 0 ? ii + nx : (ii >= nx ? ii - nx : ii);
+        return __ldg(ubcp + c * CR + (size_t)ii * RSP + e);
+    };
+    const double dx = g.dx, h = dx / 2.0;
+    if (g.scheme == PIBM_SCHEME_CENTER) {
+        for (int i = i0; i < i0 + SEG; ++i) {
+            const double ap = U(0, i + 1), am = U(0, i - 1);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double fp = ap * (c == 0 ? ap : U(c, i + 1)), fm = am * (c == 0 ? am : U(c, i - 1));
+                Dx[c * CR + (size_t)i * RSP + e] = (fp - fm) / (2.0 * dx);
+            }
+        }
+        return;
+    }
+    const int lim = g.limiter;
+    // window: w[c][k] = u_c(i-1+k), k = 0..3 ; slopes sl[c][0] = s(i), sl[c][1] = s(i+1)
+    double w[3][4], sl[3][2], Fm[3];
+    auto flux = [&](int c, int m, double a0, double a1, double sa0, double sa1, double b0, double b1, double sb0, double sb1) {
+        const double uminus = a0 + sa0 * h, uplus = a1 - sa1 * h;
+        const double Um = (c == 0) ? uminus : b0 + sb0 * h;
+        const double Up = (c == 0) ? uplus : b1 - sb1 * h;
+        const double Am = 0.5 * uminus * Um, Ap = 0.5 * uplus * Up;
+        const double ms = fmax(fabs(uminus), fabs(uplus));
+        const double s0 = (m == nx - 1) ? ((0.0 + Ap) + Am) : ((0.0 + Am) + Ap);
+        return s0 - 0.5 * ms * (Up - Um);
+    };
+    // prologue: cells i0-2 .. i0+1
+    double um2[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        um2[c] = U(c, i0 - 2);
+        w[c][0] = U(c, i0 - 1); w[c][1] = U(c, i0); w[c][2] = U(c, i0 + 1);
+    }
+    double sprev[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        sprev[c] = slope_lim(um2[c], w[c][0], w[c][1], dx, lim);     // s(i0-1)
+        sl[c][0] = slope_lim(w[c][0], w[c][1], w[c][2], dx, lim);     // s(i0)
+    }
+    {
+        const int m = (i0 - 1 + nx) % nx;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            Fm[c] = flux(c, m, w[0][0], w[0][1], sprev[0], sl[0][0], w[c][0], w[c][1], sprev[c], sl[c][0]);
+    }
+    for (int i = i0; i < i0 + SEG; ++i) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) w[c][3] = U(c, i + 2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sl[c][1] = slope_lim(w[c][1], w[c][2], w[c][3], dx, lim);   // s(i+1)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double F = flux(c, i, w[0][1], w[0][2], sl[0][0], sl[0][1], w[c][1], w[c][2], sl[c][0], sl[c][1]);
+            Dx[c * CR + (size_t)i * RSP + e] = (F - Fm[c]) / dx;
+            Fm[c] = F;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { w[c][0] = w[c][1]; w[c][1] = w[c][2]; w[c][2] = w[c][3]; sl[c][0] = sl[c][1]; }
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(Plan<N>::T, 1) k_nl(Geo g, const double *__restrict__ ubcp, const double *__restrict__ Dx,
+                                                      const double2 *__restrict__ u,
                                                    const double2 *__restrict__ onl, double2 *__restrict__ nl_new,
                                                    double *__restrict__ Q, Scal *__restrict__ sc) {
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = RP<N>::RSP;
     constexpr int EPT = Plan<N>::EPT, T = Plan<N>::T;
     double2 *buf = sm, *tws = sm + PS;
+    __shared__ uint64_t mb;
+    if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
     __syncthreads();
+    uint32_t phase = 0;
     const int i = blockIdx.x, nx = g.nx;
     const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
     const TwT tw{tws, N};
@@ -303,15 +389,16 @@ __global__ void __launch_bounds__(Plan<N>::T, 1) k_nl(Geo g, const double *__res
     for (int c = 0; c < 3; ++c) {
         double2 acc[EPT];
         for (int q = 0; q < 3; ++q) {
-            double *b = (double *)buf;
-            for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-                double v;
-                if (q == 0) v = Uc[pa0[c]][e] * Uc[pa1[c]][e];
-                else if (q == 1) v = Uc[pb0[c]][e] * Uc[pb1[c]][e];
-                else v = xflux_diff(g, ubcp, i, e, c);
-                b[e] = v;
+            if (q < 2) {
+                double *b = (double *)buf;
+                const double *A = q == 0 ? Uc[pa0[c]] : Uc[pb0[c]], *B = q == 0 ? Uc[pa1[c]] : Uc[pb1[c]];
+#pragma unroll 4
+                for (int e = threadIdx.x; e < RS; e += blockDim.x) b[e] = A[e] * B[e];
+                __syncthreads();
+            } else {
+                if (threadIdx.x == 0) bulk_load(buf, Dx + ((size_t)c * nx + i) * RS, RP<N>::BYTES, &mb);
+                load_wait(&mb, phase, sc);
             }
-            __syncthreads();
             plane_r2c<N>(buf, tw);
 #pragma unroll
             for (int s = 0; s < EPT; ++s) {
@@ -422,17 +509,20 @@ __device__ __forceinline__ double dot_ijk(const Sten &s, const double *f) {
 // k_drag: per-sphere pressure and viscous force from the surface quadrature
 // (calc_pres_visc_drag, boundary_condition.F90:1481-1645).  One CTA per sphere.
 // ============================================================================
+constexpr int kDragSplit = 8;   // CTAs per sphere in k_drag
+
 template <int N>
 __global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ pbcp, const double *__restrict__ omega,
-                                              double *__restrict__ pres, double *__restrict__ visc, double *__restrict__ ptot,
-                                              const Scal *__restrict__ sc) {
+                                              double *__restrict__ dpart, const Scal *__restrict__ sc) {
     __shared__ double scr[32];
-    const int m = blockIdx.x;
+    const int m = blockIdx.x / kDragSplit, part = blockIdx.x % kDragSplit;
     const int NB = g.nbody;
     const double xcm[3] = {g.xc[m], g.xc[m + NB], g.xc[m + 2 * NB]};
     double sa[3] = {0, 0, 0}, sb[3] = {0, 0, 0};
     const size_t CR = (size_t)g.nx * RP<N>::RSP;
-    for (int l = threadIdx.x; l < g.nbnd; l += blockDim.x) {
+    const int chunk = (g.nbnd + kDragSplit - 1) / kDragSplit;
+    const int l0 = part * chunk, l1 = min(g.nbnd, l0 + chunk);
+    for (int l = l0 + threadIdx.x; l < l1; l += blockDim.x) {
         double xl[3], xpb[3], cdl[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) { xl[d] = __dadd_rn(xcm[d], __dmul_rn(g.bnd[3 * l + d], g.rb)); cdl[d] = g.cd[3 * l + d]; }
@@ -456,17 +546,25 @@ __global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ 
     }
     for (int d = 0; d < 3; ++d) {
         const double a = block_sum(sa[d], scr), b = block_sum(sb[d], scr);
-        if (threadIdx.x == 0) { pres[m + d * NB] = -a; ptot[m + d * NB] = a; visc[m + d * NB] = b; }
+        if (threadIdx.x == 0) { dpart[(size_t)blockIdx.x * 6 + d] = a; dpart[(size_t)blockIdx.x * 6 + 3 + d] = b; }
     }
 }
 
 // compute_mpg_at_n tail + bcset diagnostics (boundary_condition.F90:356-464, 701-884).
-__global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, const double *pres, const double *visc, const double *ptot,
-                                                double *force) {
+__global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, double *visc, double *ptot,
+                                                double *force, const double *dpart) {
     __shared__ double scr[32];
     __shared__ double tot[12];
     if (sc->status) return;
     const int NB = g.nbody;
+    // per-sphere sums of the k_drag partials (fixed order)
+    for (int m = threadIdx.x; m < NB; m += blockDim.x) {
+        double a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+        for (int q = 0; q < kDragSplit; ++q)
+            for (int d = 0; d < 3; ++d) { a[d] += dpart[((size_t)m * kDragSplit + q) * 6 + d]; b[d] += dpart[((size_t)m * kDragSplit + q) * 6 + 3 + d]; }
+        for (int d = 0; d < 3; ++d) { pres[m + d * NB] = -a[d]; ptot[m + d * NB] = a[d]; visc[m + d * NB] = b[d]; }
+    }
+    __syncthreads();
     for (int d = 0; d < 3; ++d) {
         double a = 0, b = 0, c = 0;
         for (int m = threadIdx.x; m < NB; m += blockDim.x) { a += ptot[m + d * NB]; b += visc[m + d * NB]; c += pres[m + d * NB]; }
@@ -517,7 +615,8 @@ __global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, const double *p
 // ============================================================================
 // k_rev: direct forcing at the inner reversal points
 // (calc_inner_reversal_forcing, boundary_condition.F90:1104-1479).
-// rec[p*6 + 0..2] = force_tmp, rec[p*6 + 3..5] = force_dist; blockpart = sums of
+// rec[p*6 + 0..2] = force_tmp, rec[p*6 + 3..5] = force_dist,
+// ctb[(p*8 + corner)*3 + n] = weight*force_tmp/dx^3 per stencil corner; blockpart = sums of
 // tmppa/dx^3 over all corners (frmean) and over fluid corners (frmeanfluid).
 // ============================================================================
 __device__ __forceinline__ void inner_point(const Geo &g, int m, int l, double xli[3]) {
@@ -527,9 +626,9 @@ __device__ __forceinline__ void inner_point(const Geo &g, int m, int l, double x
 }
 
 template <int N>
-__global__ void __launch_bounds__(256) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
-                                             const double *__restrict__ Q, const Scal *__restrict__ sc,
-                                             double *__restrict__ rec, double *__restrict__ blockpart) {
+__global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
+                                                const double *__restrict__ Q, const Scal *__restrict__ sc,
+                                                double *__restrict__ rec, double *__restrict__ ctb, double *__restrict__ blockpart) {
     __shared__ double scr[32];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     double fm[3] = {0, 0, 0}, ffl[3] = {0, 0, 0};
@@ -603,6 +702,7 @@ __global__ void __launch_bounds__(256) k_rev(Geo g, const double *__restrict__ u
                         const double t = (w * ft[n]) / g.dx3;
                         if (fl) { force_fl[n] = force_fl[n] + t; ffl[n] += t; }
                         fm[n] += t;
+                        ctb[((size_t)p * 8 + a + 2 * b + 4 * c) * 3 + n] = t;
                     }
                     count_fl += fl ? 1 : 0;
                 }
@@ -637,26 +737,23 @@ __global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *b
 // k_spread: fr at every forced node, accumulated over its (point, corner)
 // contributions in the reference's (sphere, point) order
 // (boundary_condition.F90:1425-1462).  sp_node holds physical offsets.
-__global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, double *__restrict__ fr,
-                                                const Scal *__restrict__ sc) {
+__global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, const double *__restrict__ ctb,
+                                                double *__restrict__ fr, const Scal *__restrict__ sc) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.sp_nnodes || sc->status) return;
     const int node = g.sp_node[q];
     double acc[3] = {0.0, 0.0, 0.0};
-    for (int e = g.sp_ptr[q]; e < g.sp_ptr[q + 1]; ++e) {
-        const int ent = g.sp_ent[e];
-        const int p = ent >> 3, corner = ent & 7;
-        double xli[3];
-        inner_point(g, g.pt_m[p], g.pt_l[p], xli);
-        Sten s;
-        make_sten(g, xli, s);
-        const double w = s.w(corner & 1, (corner >> 1) & 1, (corner >> 2) & 1);
-        const double *r = rec + (size_t)p * 6;
+    const int e0 = g.sp_ptr[q], e1 = g.sp_ptr[q + 1];
+    for (int e = e0; e < e1; ++e) {
+        const int ent = __ldg(g.sp_ent + e);
+        const double *t = ctb + (size_t)ent * 3;
+        if (g.include_frmeanfluid) {
 #pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            const double t = (w * r[n]) / g.dx3;
-            if (g.include_frmeanfluid) acc[n] = acc[n] + t;
-            else acc[n] = (acc[n] + t) + r[3 + n];
+            for (int n = 0; n < 3; ++n) acc[n] = acc[n] + __ldg(t + n);
+        } else {
+            const double *r = rec + (size_t)(ent >> 3) * 6 + 3;
+#pragma unroll
+            for (int n = 0; n < 3; ++n) acc[n] = (acc[n] + __ldg(t + n)) + __ldg(r + n);
         }
     }
     const size_t CR = (size_t)g.nx * g.RS;
@@ -1105,17 +1202,18 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
     k_a0<N><<<g.nx, T, sm, s>>>(g, b.u, b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
     k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
     mark(1);
-    k_nl<N><<<g.nx, T, sm, s>>>(g, b.ubcp, b.u, b.nl[old], b.nl[cur], b.Q, b.sc);
+    k_flux<N><<<(RP<N>::RSP * (g.nx / 32) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
+    k_nl<N><<<g.nx, T, sm, s>>>(g, b.ubcp, b.Dx, b.u, b.nl[old], b.nl[cur], b.Q, b.sc);
     mark(2);
     if (g.nbody > 0) {
-        k_drag<N><<<g.nbody, 256, 0, s>>>(g, b.pbcp, b.omega, b.pres, b.visc, b.ptot, b.sc);
-        k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force);
+        k_drag<N><<<g.nbody * kDragSplit, 256, 0, s>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
+        k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
         mark(3);
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {
-            k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.blockpart);
+            k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.ctb, b.blockpart);
             k_scal_c<<<1, 256, 0, s>>>(g, b.sc, b.blockpart, nbk);
-            if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.fr, b.sc);
+            if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.ctb, b.fr, b.sc);
         }
         mark(4);
         k_ff<N><<<g.nx, T, sm, s>>>(g, b.fr, b.ff, b.sc);
@@ -1131,7 +1229,7 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
 
 // Kernels launched per step (for launch accounting).
 int kernels_per_step(const Geo &g) {
-    int n = 5;   // a0, scal_a, nl, lines, scal_d
+    int n = 6;   // a0, scal_a, flux, nl, lines, scal_d
     if (g.nbody > 0) n += 3 + (g.npts > 0 ? 2 + (g.sp_nnodes > 0 ? 1 : 0) : 0);
     return n;
 }
