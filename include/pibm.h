@@ -177,6 +177,28 @@ const char *pibm_last_error(void);
 int  pibm_ff2rc(int my, int mz, int nplanes, const double *a, double *b);
 int  pibm_ff2cr(int my, int mz, int nplanes, const double *a, double *b);
 
+/* Allocation-free ff2cr on DEVICE buffers.  No counterpart in the reference
+ * (its ff2cr works on host arrays through FFTW plans); it exists for callers
+ * that keep their spectral fields on the GPU and cannot allocate per call:
+ * pibm_ff2cr above allocates and frees three device buffers each time, and
+ * cudaFree waits for the whole device, which stalls a host that runs other
+ * streams, and cudaMalloc competes with a host whose device memory is already
+ * carved into its own pool (a caching allocator, pre-registered buffers).
+ * This entry point allocates nothing: the only data it needs besides a and b
+ * is a twiddle table kept in a static device array of 320 complex doubles
+ * (5 KiB per GPU, held until the process exits) that covers every supported
+ * size, my = mz in {32, 64, 96, 128}; larger or other sizes are rejected with
+ * PIBM_ERR_ARG.  Set-up: the FIRST call on each device looks up that array's
+ * address, writes the whole table with a blocking copy and waits for it, so
+ * make that first call before starting any stream capture.  After it the
+ * table is only read, so nothing in it must start at zero and calls on
+ * different streams share it safely.
+ * d_a: nplanes * mz * (my/2+1) complex (interleaved doubles); d_b: nplanes *
+ * mz * my doubles; both device pointers with the layout of pibm_ff2cr.  The
+ * transform is enqueued on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and the call returns without waiting for it. */
+int  pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *d_b, void *stream);
+
 /* ---- batched independent realizations (the MIS ensemble of
  *      sample_inputs/set_mis_3d, run as one graph-captured launch stream) ---- */
 typedef struct pibm_batch pibm_batch;

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -391,6 +392,73 @@ static int plane_transform(int my, int mz, int nplanes, const double *a, double 
 
 int pibm_ff2rc(int my, int mz, int nplanes, const double *a, double *b) { return plane_transform(my, mz, nplanes, a, b, true); }
 int pibm_ff2cr(int my, int mz, int nplanes, const double *a, double *b) { return plane_transform(my, mz, nplanes, a, b, false); }
+
+}  // extern "C"
+
+// ---- allocation-free ff2cr: twiddles for every supported size live in one
+// static device array, written once per device by the first call ----
+namespace {
+constexpr int kNoAllocSizes[4] = {32, 64, 96, 128};
+constexpr int kNoAllocMaxN = 128;
+constexpr int kNoAllocEntries = 32 + 64 + 96 + 128;
+static __device__ __align__(256) double2 g_noalloc_twiddles[kNoAllocEntries];
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double2 *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Offset of the size-n table inside g_noalloc_twiddles, or -1.
+int noalloc_offset(int n) {
+    int off = 0;
+    for (int s : kNoAllocSizes) {
+        if (s == n) return off;
+        off += s;
+    }
+    return -1;
+}
+}  // namespace
+
+extern "C" {
+
+int pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *d_b, void *stream) {
+    if (my > kNoAllocMaxN || mz > kNoAllocMaxN)
+        return fail(PIBM_ERR_ARG, "pibm_ff2cr_noalloc: plane " + std::to_string(my) + "x" + std::to_string(mz) +
+                                      " exceeds the static twiddle table (largest size 128)");
+    if (my != mz || noalloc_offset(my) < 0)
+        return fail(PIBM_ERR_ARG, "pibm_ff2cr_noalloc: unsupported plane size (my = mz in {32, 64, 96, 128})");
+    if (nplanes < 0 || (nplanes > 0 && (!d_a || !d_b))) return fail(PIBM_ERR_ARG, "pibm_ff2cr_noalloc: bad argument");
+    int dev = 0;
+    CUDA_OR_FAIL(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(PIBM_ERR_ARG, "pibm_ff2cr_noalloc: device index out of range");
+    double2 *table = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            // first call on this device (it is current): resolve the array, fill every size, wait
+            void *p = nullptr;
+            CUDA_OR_FAIL(cudaGetSymbolAddress(&p, g_noalloc_twiddles));
+            std::vector<double2> host;
+            host.reserve(kNoAllocEntries);
+            for (int s : kNoAllocSizes) {
+                std::vector<double2> t = twiddles(s);
+                host.insert(host.end(), t.begin(), t.end());
+            }
+            CUDA_OR_FAIL(cudaMemcpy(p, host.data(), host.size() * sizeof(double2), cudaMemcpyHostToDevice));
+            CUDA_OR_FAIL(cudaDeviceSynchronize());
+            g_noalloc_ptr[dev] = (double2 *)p;
+        }
+        table = g_noalloc_ptr[dev];
+    }
+    if (nplanes == 0) return PIBM_OK;
+    CUDA_OR_FAIL(configure_kernels(my));
+    Geo g;
+    std::memset(&g, 0, sizeof(g));
+    g.nx = 1; g.my = my; g.mz = mz; g.my2 = my / 2 + 1; g.PS = g.my2 * mz; g.RS = my * mz;
+    g.nrm = (double)(float)(my * mz);
+    g.tw = table + noalloc_offset(my);
+    enqueue_c2r(g, (const double2 *)d_a, d_b, nplanes, (cudaStream_t)stream);
+    CUDA_OR_FAIL(cudaGetLastError());
+    return PIBM_OK;
+}
 
 // ---- batched independent realizations ----
 struct pibm_batch {
