@@ -47,6 +47,21 @@ KERNEL_NAMES = {
 }
 
 
+def max_over_ranks(x: float, dist, device: str) -> float:
+    """Max of a per-rank time over all ranks (every rank calls this)."""
+    if not dist:
+        return float(x)
+    import torch
+    tt = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def aggregate_mcells(ncell: int, steps: int, world: int, t_ms: float) -> float:
+    """Whole-job Mcell-steps/s: every rank steps its own replica of ncell cells."""
+    return ncell * steps * world / (t_ms / 1e3) / 1e6
+
+
 def _peak_gbs():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -213,12 +228,8 @@ def run_gpu(args):
     barrier()
     if rc != 0:
         raise RuntimeError("pibm_run_profiled failed: %d %s" % (rc, lib.pibm_last_error().decode()))
-    t_ms = total.value
-    if dist:
-        tt = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
-    value = ncell * args.steps * world / (t_ms / 1e3) / 1e6
+    t_ms = max_over_ranks(total.value, dist, "cuda")
+    value = aggregate_mcells(ncell, args.steps, world, t_ms)
     phase_ms = {abi.PHASE_NAMES[q]: phases[q] / args.steps for q in range(abi.PIBM_NPHASE)}
 
     # end-to-end through the C ABI with host buffers: every step uploads the
@@ -241,11 +252,7 @@ def run_gpu(args):
         assert lib.pibm_step(s.h, 1, C.byref(rep)) == 0
         assert lib.pibm_get_state(s.h, C.byref(view)) == 0
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
     bytes_state = (hu.numel() + hnl.numel() + hp.numel()) * 8
 
     if rank != 0:
