@@ -870,12 +870,13 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
                                                    const double2 *__restrict__ nl, const double2 *__restrict__ onl,
                                                    const double2 *__restrict__ ff, Scal *__restrict__ sc) {
     constexpr int R = NX / 32;
+    constexpr int NP = NX + 1;                // tile row pitch: rows of consecutive lines start 4 banks apart
     extern __shared__ double2 sm[];
     double2 *tws = sm;
     double2 *RHS = tws + NX;
-    double2 *P = RHS + LT * NX;
-    double2 *U = P + LT * NX;                 // [comp][line][i]
-    double *gam = (double *)(U + 3 * LT * NX);
+    double2 *P = RHS + LT * NP;
+    double2 *U = P + LT * NP;                 // [comp][line][i]
+    double *gam = (double *)(U + 3 * LT * NP);
     if (sc->status) return;
     for (int t = threadIdx.x; t < NX; t += blockDim.x) tws[t] = g.tw[t];
     const int PS = g.PS, nx = NX;
@@ -914,8 +915,8 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
         tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
         d = mwz(cadd(G(onl, 2, i + 1, q), G(onl, 2, i, q)));
         tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
-        RHS[line * NX + i] = make_double2(tt.x / (c1 + c2), tt.y / (c1 + c2));
-        P[line * NX + i] = p[(size_t)i * PS + q];
+        RHS[line * NP + i] = make_double2(tt.x / (c1 + c2), tt.y / (c1 + c2));
+        P[line * NP + i] = p[(size_t)i * PS + q];
     }
     __syncthreads();
     const int qw = q0 + w;
@@ -923,7 +924,7 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
     const double w2w = wact ? g.w2[qw] : 0.0;
     {
         const double a = 1.0 / dx2 - 0.25 * w2w, bd = -2.0 / dx2 - 0.5 * w2w, c = 1.0 / dx2 - 0.25 * w2w;
-        double2 *row = RHS + w * NX;
+        double2 *row = RHS + w * NP;
         if (wact) {
             if (qw == 0) {
                 if (lane == 0) ok = thomas_real(row, gam, a, bd, c, NX - 1) && ok;
@@ -934,8 +935,8 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int i = lane + 32 * r;
-                const double2 po = P[w * NX + i], tp = row[i];
-                P[w * NX + i] = make_double2(po.x + 1.0 * (tp.x - po.x), po.y + 1.0 * (tp.y - po.y));
+                const double2 po = P[w * NP + i], tp = row[i];
+                P[w * NP + i] = make_double2(po.x + 1.0 * (tp.x - po.x), po.y + 1.0 * (tp.y - po.y));
             }
         }
     }
@@ -954,7 +955,7 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
             const double2 nn = G(nl, n, i, q), f = G(ff, n, i, q), on = G(onl, n, i, q);
             r = make_double2(r.x + (dt * c3) * nn.x + dt * f.x, r.y + (dt * c3) * nn.y + dt * f.y);
             r = make_double2(r.x + (dt * c4) * on.x, r.y + (dt * c4) * on.y);
-            const double2 pm = P[line * NX + (i == 0 ? nx - 1 : i - 1)], p0 = P[line * NX + i];
+            const double2 pm = P[line * NP + (i == 0 ? nx - 1 : i - 1)], p0 = P[line * NP + i];
             double2 gp;
             if (n == 0) gp = make_double2((alp * (p0.x - pm.x)) / dx, (alp * (p0.y - pm.y)) / dx);
             else {
@@ -966,16 +967,16 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
             double2 lap;
             if (i == 0) lap = make_double2((up.x - 2.0 * ui.x) + um.x, (up.y - 2.0 * ui.y) + um.y);
             else lap = make_double2((um.x + up.x) - 2.0 * ui.x, (um.y + up.y) - 2.0 * ui.y);
-            RHS[line * NX + i] = make_double2(r.x + (gd * lap.x) / dx2, r.y + (gd * lap.y) / dx2);
+            RHS[line * NP + i] = make_double2(r.x + (gd * lap.x) / dx2, r.y + (gd * lap.y) / dx2);
         }
         __syncthreads();
         if (wact) {
             const double a = -(1.0 * dt * vis * c2 / dx2);
             const double bd = 1.0 + dt * vis * c2 * (1.0 * 2.0 / dx2 + w2w);
-            double2 *row = RHS + w * NX;
+            double2 *row = RHS + w * NP;
             circulant_solve<R>(row, a, bd, tw, lane);
 #pragma unroll
-            for (int r = 0; r < R; ++r) U[(n * LT + w) * NX + lane + 32 * r] = row[lane + 32 * r];
+            for (int r = 0; r < R; ++r) U[(n * LT + w) * NP + lane + 32 * r] = row[lane + 32 * r];
         }
         __syncthreads();
     }
@@ -986,26 +987,26 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
         if (q >= PS) continue;
         const double ky = KY(q), kz = KZ(q);
         const int ip = i == nx - 1 ? 0 : i + 1;
-        const double2 *U1 = U + (0 * LT + line) * NX, *U2 = U + (1 * LT + line) * NX, *U3 = U + (2 * LT + line) * NX;
+        const double2 *U1 = U + (0 * LT + line) * NP, *U2 = U + (1 * LT + line) * NP, *U3 = U + (2 * LT + line) * NP;
         double2 tt = make_double2((U1[ip].x - U1[i].x) / dx, (U1[ip].y - U1[i].y) / dx);
         double2 sy = cscale(cadd(U2[i], U2[ip]), 0.5), sz = cscale(cadd(U3[i], U3[ip]), 0.5);
         tt = cadd(tt, make_double2(-ky * sy.y, ky * sy.x));
         tt = cadd(tt, make_double2(-kz * sz.y, kz * sz.x));
-        RHS[line * NX + i] = make_double2((0.5 * (1.0 + 1.0) * tt.x) / alpc, (0.5 * (1.0 + 1.0) * tt.y) / alpc);
+        RHS[line * NP + i] = make_double2((0.5 * (1.0 + 1.0) * tt.x) / alpc, (0.5 * (1.0 + 1.0) * tt.y) / alpc);
     }
     __syncthreads();
     if (wact) {
         const double a = 1.0 / dx2 - 0.25 * w2w, bd = -2.0 / dx2 - 0.5 * w2w, c = 1.0 / dx2 - 0.25 * w2w;
         const double ky = KY(qw), kz = KZ(qw);
-        double2 *row = RHS + w * NX;
+        double2 *row = RHS + w * NP;
         if (qw == 0) {
             if (lane == 0) ok = thomas_real(row, gam, a, bd, c, NX - 1) && ok;
             __syncwarp();
         } else {
             circulant_solve<R>(row, a, bd, tw, lane);
         }
-        double2 *U1 = U + (0 * LT + w) * NX, *U2 = U + (1 * LT + w) * NX, *U3 = U + (2 * LT + w) * NX;
-        double2 *Pw = P + w * NX;
+        double2 *U1 = U + (0 * LT + w) * NP, *U2 = U + (1 * LT + w) * NP, *U3 = U + (2 * LT + w) * NP;
+        double2 *Pw = P + w * NP;
         const double c2dtv = (c2 * dt) * vis;
         double2 nu1[R], nu2[R], nu3[R], np[R];
 #pragma unroll
@@ -1050,15 +1051,15 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
         const int line = t % LT, i = t / LT, q = q0 + line;
         if (q >= PS) continue;
 #pragma unroll
-        for (int n = 0; n < 3; ++n) u[((size_t)n * nx + i) * PS + q] = U[(n * LT + line) * NX + i];
-        p[(size_t)i * PS + q] = P[line * NX + i];
+        for (int n = 0; n < 3; ++n) u[((size_t)n * nx + i) * PS + q] = U[(n * LT + line) * NP + i];
+        p[(size_t)i * PS + q] = P[line * NP + i];
     }
     if (!ok) atomicCAS(&sc->status, 0, PIBM_ERR_PIVOT);
 }
 
 template <int NX> struct LinesCfg { static constexpr int LT = NX >= 256 ? 4 : 8; };
 template <int NX>
-static size_t lines_smem() { return (size_t)(NX + 5 * LinesCfg<NX>::LT * NX) * sizeof(double2) + NX * sizeof(double); }
+static size_t lines_smem() { return (size_t)(NX + 5 * LinesCfg<NX>::LT * (NX + 1)) * sizeof(double2) + NX * sizeof(double); }
 
 // velstep tail: umean update (steptheflow.F90:99) and the NaN check.
 __global__ void k_scal_d(Geo g, Scal *sc) {
