@@ -28,6 +28,7 @@ void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStr
 void enqueue_f2d(const double2 *f, double2 *d, int nx, int nxf, int PS, int ncomp, cudaStream_t s);
 void enqueue_d2f(const double2 *d, double2 *f, int nx, int nxf, int PS, int ncomp, cudaStream_t s);
 int real_offset(int n, int z, int y);
+int plane_ctas(int n);
 }  // namespace pibm
 
 using namespace pibm;
@@ -114,6 +115,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     g.PS = S.my2 * S.mz; g.RS = (S.my + 2) * S.mz;   // physical real plane: rows of my+2 doubles
     g.dx = S.dx; g.dx2 = S.dx2; g.rdx2 = 1.0 / S.dx2; g.dx3 = S.dx3; g.vis = S.vis;
     g.nrm = (double)(float)(S.my * S.mz);
+    g.plane_ctas = plane_ctas(S.my);
     g.c1 = S.coef[0]; g.c2 = S.coef[1]; g.c3 = S.coef[2]; g.c4 = S.coef[3];
     g.scheme = prm->discr_scheme; g.limiter = prm->limiter;
     g.include_frmeanfluid = prm->include_frmeanfluid; g.revernorm = prm->revernorm;
@@ -160,7 +162,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
               guard(h->alloc(&b.pbcp, NR), "pbcp") && guard(h->alloc(&b.Q, 3 * NR), "Q") && guard(h->alloc(&b.Dx, 3 * NR), "Dx") &&
               guard(h->alloc(&b.omega, 3 * NR), "omega") && guard(h->alloc(&b.pgr, 3 * NR), "pgr") &&
               (S.nbody == 0 || guard(h->alloc(&b.fr, 3 * NR), "fr")) &&
-              guard(h->alloc(&b.part, (size_t)g.nx * 12), "part") &&
+              guard(h->alloc(&b.part, (size_t)g.nx * 8 * 12), "part") &&
               guard(h->alloc(&b.pres, 3 * (size_t)S.nbody), "pres") && guard(h->alloc(&b.visc, 3 * (size_t)S.nbody), "visc") &&
               guard(h->alloc(&b.ptot, 3 * (size_t)S.nbody), "ptot") && guard(h->alloc(&b.force, 3 * (size_t)S.nbody), "force") &&
               guard(h->alloc(&b.rec, 6 * (size_t)g.npts), "rec") && guard(h->alloc(&b.ctb, 24 * (size_t)g.npts), "ctb") &&
@@ -365,6 +367,7 @@ static int plane_transform(int my, int mz, int nplanes, const double *a, double 
     std::memset(&g, 0, sizeof(g));
     g.nx = 1; g.my = my; g.mz = mz; g.my2 = my / 2 + 1; g.PS = g.my2 * mz; g.RS = my * mz;
     g.nrm = (double)(float)(my * mz);
+    g.plane_ctas = plane_ctas(my);
     CUDA_OR_FAIL(configure_kernels(my));
     std::vector<double2> tw = twiddles(my);
     double2 *dtw = nullptr, *dc = nullptr;
@@ -454,6 +457,7 @@ int pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *d
     std::memset(&g, 0, sizeof(g));
     g.nx = 1; g.my = my; g.mz = mz; g.my2 = my / 2 + 1; g.PS = g.my2 * mz; g.RS = my * mz;
     g.nrm = (double)(float)(my * mz);
+    g.plane_ctas = plane_ctas(my);
     g.tw = table + noalloc_offset(my);
     enqueue_c2r(g, (const double2 *)d_a, d_b, nplanes, (cudaStream_t)stream);
     CUDA_OR_FAIL(cudaGetLastError());

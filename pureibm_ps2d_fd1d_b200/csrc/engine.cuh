@@ -15,6 +15,7 @@ struct Geo {
     int scheme, limiter, include_frmeanfluid, revernorm, set_mpg, adaptive;
     double cfl_max, ramp_frac_time, ucharmod, char_length, voldom, maxvolfrac, mean_volfrac;
     long long count_fluid, ncell;
+    int plane_ctas;     // CTAs per plane in the plane kernels
     double ufmean_des[3], usmean_des[3], usmean_act[3];
     // particles
     int nbody, nbnd, npts;

@@ -29,6 +29,7 @@
 // once in spectral space (Q) instead of three separately interpolated fields.
 #include "engine.cuh"
 #include "fft2d.cuh"
+#include "plane_cl.cuh"
 #include "bulk.cuh"
 #include "../../include/pibm.h"
 
@@ -98,92 +99,89 @@ __device__ __forceinline__ double block_max(double v, double *scr) {
 // part[i*12 + q]: q 0-2 fluid sums, 3-5 solid sums, 6-8 all sums, 9-11 max |u|.
 // ============================================================================
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T, 1) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
                                                    double *__restrict__ ubcp, double *__restrict__ pbcp,
                                                    double *__restrict__ omega, double *__restrict__ pgr,
                                                    Scal *__restrict__ sc, double *__restrict__ part) {
+    using L = PL<N>;
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
-    double2 *buf = sm, *tws = sm + PS;
+    double2 *buf = sm, *tws = sm + L::BUF;
     __shared__ double scr[32];
-    __shared__ uint64_t mb;
-    if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
     __syncthreads();
-    uint32_t phase = 0;
-    const int i = blockIdx.x, nx = g.nx;
+    const int i = blockIdx.x / L::C, rank = blockIdx.x % L::C, nx = g.nx;
     const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
+    const size_t roff = (size_t)rank * L::RL;
     const TwT tw{tws, N};
     const double tdx = 2.0 * g.dx;
     const double2 *U0 = u + (size_t)i * PS, *U1 = u + ((size_t)nx + i) * PS, *U2 = u + ((size_t)2 * nx + i) * PS;
     const double2 *Pp = p + (size_t)i * PS;
-    double acc[12];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) acc[q] = 0.0;
-    acc[9] = acc[10] = acc[11] = kSmallD;
+    const size_t slot = ((size_t)i * L::C + rank) * 12;
     for (int t = 0; t < 10; ++t) {
-        if (t < 4) {
-            if (threadIdx.x == 0) bulk_load(buf, t == 0 ? U0 : t == 1 ? U1 : t == 2 ? U2 : Pp, PS * 16, &mb);
-            load_wait(&mb, phase, sc);
-        } else {
-            for (int e = threadIdx.x; e < PS; e += blockDim.x) {
-                const int kz = e / my2, j = e - kz * my2;
+        // spectral input of this CTA's columns
+#pragma unroll 4
+        for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
+            const int kz = e / L::PZ, jl = e - kz * L::PZ;
+            if (jl == L::MC && rank != 0) continue;
+            const int j = cl_col<N>(jl, rank), ge = kz * my2 + j;
+            double2 f;
+            if (t == 0) f = U0[ge];
+            else if (t == 1) f = U1[ge];
+            else if (t == 2) f = U2[ge];
+            else if (t == 3) f = Pp[ge];
+            else {
                 const double ky = g.ky[j], kzv = g.kz[kz];
-                double2 f;
                 if (t == 4) {   // wy*u3 - wz*u2
-                    const double2 a = U2[e], b = U1[e];
+                    const double2 a = U2[ge], b = U1[ge];
                     f = make_double2(-ky * a.y - (-kzv * b.y), ky * a.x - kzv * b.x);
                 } else if (t == 5) {   // wz*u1 - d(u3)/dx
-                    const double2 a = U0[e];
-                    const double2 hp = u[((size_t)2 * nx + ip) * PS + e], hm = u[((size_t)2 * nx + im) * PS + e];
+                    const double2 a = U0[ge];
+                    const double2 hp = u[((size_t)2 * nx + ip) * PS + ge], hm = u[((size_t)2 * nx + im) * PS + ge];
                     const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
                     f = make_double2(-kzv * a.y - d.x, kzv * a.x - d.y);
                 } else if (t == 6) {   // d(u2)/dx - wy*u1
-                    const double2 a = U0[e];
-                    const double2 hp = u[((size_t)nx + ip) * PS + e], hm = u[((size_t)nx + im) * PS + e];
+                    const double2 a = U0[ge];
+                    const double2 hp = u[((size_t)nx + ip) * PS + ge], hm = u[((size_t)nx + im) * PS + ge];
                     const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
                     f = make_double2(d.x - (-ky * a.y), d.y - ky * a.x);
                 } else if (t == 7) {
-                    const double2 a = p[(size_t)ip * PS + e], b = p[(size_t)im * PS + e];
+                    const double2 a = p[(size_t)ip * PS + ge], b = p[(size_t)im * PS + ge];
                     f = make_double2((a.x - b.x) / tdx, (a.y - b.y) / tdx);
-                } else if (t == 8) { const double2 a = Pp[e]; f = make_double2(-a.y * ky, a.x * ky); }
-                else { const double2 a = Pp[e]; f = make_double2(-a.y * kzv, a.x * kzv); }
-                buf[e] = f;
+                } else if (t == 8) { const double2 a = Pp[ge]; f = make_double2(-a.y * ky, a.x * ky); }
+                else { const double2 a = Pp[ge]; f = make_double2(-a.y * kzv, a.x * kzv); }
             }
-            __syncthreads();
+            buf[e] = f;
         }
-        if (threadIdx.x < 32) pack_col0_warp<N>(buf);
         __syncthreads();
-        plane_c2r<N>(buf, tw);
+        cl_c2r<N>(buf, tw, rank);
         if (t < 3) {
+            // u + umean; fluid, solid and total sums and max |u| of this CTA's rows
             const double um = sc->umean[t];
             double *b = (double *)buf;
-            const uint8_t *fl = g.fluid + (size_t)i * RSP;
-            for (int e = threadIdx.x; e < RSP; e += blockDim.x) {
+            const uint8_t *fl = g.fluid + (size_t)i * RSP + roff;
+            double sf = 0.0, ss = 0.0, sa = 0.0, mx = kSmallD;
+            for (int e = threadIdx.x; e < L::RL; e += L::T) {
                 if (e % (N + 2) >= N) continue;
                 const double v = b[e] + um;
                 b[e] = v;
-                if (fl[e]) acc[t] += v; else acc[3 + t] += v;
-                acc[6 + t] += v;
-                acc[9 + t] = fmax(acc[9 + t], fabs(v));
+                if (fl[e]) sf += v; else ss += v;
+                sa += v;
+                mx = fmax(mx, fabs(v));
             }
-            __syncthreads();
+            sf = block_sum(sf, scr);
+            ss = block_sum(ss, scr);
+            sa = block_sum(sa, scr);
+            mx = block_max(mx, scr);
+            if (threadIdx.x == 0) { part[slot + t] = sf; part[slot + 3 + t] = ss; part[slot + 6 + t] = sa; part[slot + 9 + t] = mx; }
         }
         double *dst = t < 3 ? ubcp + ((size_t)t * nx + i) * RSP
                     : t == 3 ? pbcp + (size_t)i * RSP
                     : (t < 7 ? omega + ((size_t)(t - 4) * nx + i) * RSP : pgr + ((size_t)(t - 7) * nx + i) * RSP);
-        if (threadIdx.x == 0) { bulk_store(dst, buf, RP<N>::BYTES); bulk_wait_read(); }
+        if (threadIdx.x == 0) { bulk_store(dst + roff, buf, L::RBYTES); bulk_wait_read(); }
         __syncthreads();
     }
     if (threadIdx.x == 0) bulk_wait_all();
-    for (int q = 0; q < 9; ++q) {
-        const double s = block_sum(acc[q], scr);
-        if (threadIdx.x == 0) part[(size_t)i * 12 + q] = s;
-    }
-    for (int q = 9; q < 12; ++q) {
-        const double s = block_max(acc[q], scr);
-        if (threadIdx.x == 0) part[(size_t)i * 12 + q] = s;
-    }
 }
 
 // compute_new_timestep's scalar tail (dependent_functions.F90:1137-1280).
@@ -193,7 +191,7 @@ __global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *p
     if (sc->status) return;
     for (int d = 0; d < 3; ++d) {
         double a = 0.0, m = kSmallD;
-        for (int i = threadIdx.x; i < g.nx; i += blockDim.x) { a += part[(size_t)i * 12 + d]; m = fmax(m, part[(size_t)i * 12 + 9 + d]); }
+        for (int i = threadIdx.x; i < g.nx * g.plane_ctas; i += blockDim.x) { a += part[(size_t)i * 12 + d]; m = fmax(m, part[(size_t)i * 12 + 9 + d]); }
         a = block_sum(a, scr);
         m = block_max(m, scr);
         if (threadIdx.x == 0) { red[d] = a; red[3 + d] = m; }
@@ -366,77 +364,92 @@ __global__ void __launch_bounds__(256) k_flux(Geo g, const double *__restrict__ 
 }
 
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T, 1) k_nl(Geo g, const double *__restrict__ ubcp, const double *__restrict__ Dx,
-                                                      const double2 *__restrict__ u,
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const double *__restrict__ ubcp, const double *__restrict__ Dx,
+                                                   const double2 *__restrict__ u,
                                                    const double2 *__restrict__ onl, double2 *__restrict__ nl_new,
                                                    double *__restrict__ Q, Scal *__restrict__ sc) {
+    using L = PL<N>;
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = RP<N>::RSP;
-    constexpr int EPT = Plan<N>::EPT, T = Plan<N>::T;
-    double2 *buf = sm, *tws = sm + PS;
+    double2 *buf = sm, *tws = sm + L::BUF;
     __shared__ uint64_t mb;
     if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
     __syncthreads();
     uint32_t phase = 0;
-    const int i = blockIdx.x, nx = g.nx;
+    const int i = blockIdx.x / L::C, rank = blockIdx.x % L::C, nx = g.nx;
     const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
+    const size_t roff = (size_t)rank * L::RL;
     const TwT tw{tws, N};
-    const double *Uc[3] = {ubcp + (size_t)i * RS, ubcp + ((size_t)nx + i) * RS, ubcp + ((size_t)2 * nx + i) * RS};
-    // product pairs: component c uses (wy: pa) and (wz: pb)
-    const int pa0[3] = {0, 1, 1}, pa1[3] = {1, 1, 2}, pb0[3] = {0, 1, 2}, pb1[3] = {2, 2, 2};
+    // real component n of this CTA's rows
+    auto Uc = [&](int n) { return ubcp + ((size_t)n * nx + i) * RS + roff; };
     const double c12 = g.c1 + g.c2;
     for (int c = 0; c < 3; ++c) {
-        double2 acc[EPT];
+        // nl_new of this plane accumulates i ky F(pa) + i kz F(pb) + F(D_c) in place
+        double2 *dst = nl_new + ((size_t)c * nx + i) * PS;
         for (int q = 0; q < 3; ++q) {
             if (q < 2) {
                 double *b = (double *)buf;
-                const double *A = q == 0 ? Uc[pa0[c]] : Uc[pb0[c]], *B = q == 0 ? Uc[pa1[c]] : Uc[pb1[c]];
+                // product pairs of component c: wy term (u1 u1, u2 u2... as (0,1),(1,1),(1,2)), wz term (c, 2)
+                const int na = q == 0 ? (c == 0 ? 0 : 1) : c, nb = q == 0 ? (c == 2 ? 2 : 1) : 2;
+                const double *A = Uc(na), *B = Uc(nb);
 #pragma unroll 4
-                for (int e = threadIdx.x; e < RS; e += blockDim.x) b[e] = A[e] * B[e];
+                for (int e = threadIdx.x; e < L::RL; e += L::T) b[e] = A[e] * B[e];
                 __syncthreads();
             } else {
-                if (threadIdx.x == 0) bulk_load(buf, Dx + ((size_t)c * nx + i) * RS, RP<N>::BYTES, &mb);
+                if (threadIdx.x == 0) {
+                    fence_async_smem();
+                    bulk_load(buf, Dx + ((size_t)c * nx + i) * RS + roff, L::RBYTES, &mb);
+                }
                 load_wait(&mb, phase, sc);
             }
-            plane_r2c<N>(buf, tw);
-#pragma unroll
-            for (int s = 0; s < EPT; ++s) {
-                const int e = threadIdx.x + s * T;
-                if (e < PS) {
-                    const int kz = e / my2, j = e - kz * my2;
-                    const double2 Xr = unpack_col<N>(buf, kz, j);
+            cl_r2c<N>(buf, tw, rank);
+            if (q < 2) {
+#pragma unroll 4
+                for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
+                    const int kz = e / L::PZ, jl = e - kz * L::PZ;
+                    if (jl == L::MC && rank != 0) continue;
+                    const int ge = kz * my2 + cl_col<N>(jl, rank);
+                    const double2 Xr = cl_unpack<N>(buf, kz, jl, rank);
                     const double2 X = make_double2(Xr.x / g.nrm, Xr.y / g.nrm);
-                    if (q == 0) { const double ky = g.ky[j]; acc[s] = make_double2(-ky * X.y, ky * X.x); }
-                    else if (q == 1) { const double kzv = g.kz[kz]; acc[s] = cadd(acc[s], make_double2(-kzv * X.y, kzv * X.x)); }
-                    else acc[s] = cadd(acc[s], X);
+                    if (q == 0) { const double ky = g.ky[cl_col<N>(jl, rank)]; dst[ge] = make_double2(-ky * X.y, ky * X.x); }
+                    else { const double kzv = g.kz[kz]; dst[ge] = cadd(dst[ge], make_double2(-kzv * X.y, kzv * X.x)); }
                 }
+                __syncthreads();
             }
-            __syncthreads();
         }
         // nl = -(...) (nl.F90:146-152); Q = -c3 nl - c4 onl - c12 diffn (calc_visc spectrum)
-        double2 *dst = nl_new + ((size_t)c * nx + i) * PS;
         const double2 *on = onl + ((size_t)c * nx + i) * PS;
         const double2 *uc = u + (size_t)c * nx * PS;
-#pragma unroll
-        for (int s = 0; s < EPT; ++s) {
-            const int e = threadIdx.x + s * T;
-            if (e < PS) {
-                const double2 v = make_double2(-acc[s].x, -acc[s].y);
-                dst[e] = v;
-                const double2 a = uc[(size_t)im * PS + e], bb = uc[(size_t)i * PS + e], cv = uc[(size_t)ip * PS + e];
+#pragma unroll 4
+        for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
+            const int kz = e / L::PZ, jl = e - kz * L::PZ;
+            if (jl == L::MC && rank != 0) continue;
+            const int ge = kz * my2 + cl_col<N>(jl, rank);
+            const double2 Xr = cl_unpack<N>(buf, kz, jl, rank);
+            const double2 X = make_double2(Xr.x / g.nrm, Xr.y / g.nrm);
+            const double2 a = cadd(dst[ge], X);
+            dst[ge] = make_double2(-a.x, -a.y);
+        }
+        __syncthreads();   // every read of the r2c result is done; each thread re-reads its own nl values
+#pragma unroll 4
+        for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
+            {
+                const int kz = e / L::PZ, jl = e - kz * L::PZ;
+                if (jl == L::MC && rank != 0) continue;
+                const int ge = kz * my2 + cl_col<N>(jl, rank);
+                const double2 v = dst[ge];
+                const double2 a = uc[(size_t)im * PS + ge], bb = uc[(size_t)i * PS + ge], cv = uc[(size_t)ip * PS + ge];
                 double2 df = make_double2(g.rdx2 * ((a.x - 2.0 * bb.x) + cv.x), g.rdx2 * ((a.y - 2.0 * bb.y) + cv.y));
-                const double w2 = g.w2[e];
+                const double w2 = g.w2[ge];
                 df = make_double2((df.x - w2 * bb.x) * g.vis, (df.y - w2 * bb.y) * g.vis);
-                const double2 o = on[e];
+                const double2 o = on[ge];
                 buf[e] = make_double2((-g.c3 * v.x - g.c4 * o.x) - c12 * df.x, (-g.c3 * v.y - g.c4 * o.y) - c12 * df.y);
             }
         }
         __syncthreads();
-        if (threadIdx.x < 32) pack_col0_warp<N>(buf);
-        __syncthreads();
-        plane_c2r<N>(buf, tw);
-        if (threadIdx.x == 0) { bulk_store(Q + ((size_t)c * nx + i) * RS, buf, RP<N>::BYTES); bulk_wait_read(); }
+        cl_c2r<N>(buf, tw, rank);
+        if (threadIdx.x == 0) { bulk_store(Q + ((size_t)c * nx + i) * RS + roff, buf, L::RBYTES); bulk_wait_read(); }
         __syncthreads();
     }
     if (threadIdx.x == 0) bulk_wait_all();
@@ -763,31 +776,38 @@ __global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict_
 
 // k_ff: ff = r2c(fr - frmean) (boundary_condition.F90:678-700).
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T, 1) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
                                                    Scal *__restrict__ sc) {
+    using L = PL<N>;
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
-    double2 *buf = sm, *tws = sm + PS;
+    double2 *buf = sm, *tws = sm + L::BUF;
     __shared__ uint64_t mb;
     if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
     __syncthreads();
     uint32_t phase = 0;
-    const int i = blockIdx.x, nx = g.nx;
+    const int i = blockIdx.x / L::C, rank = blockIdx.x % L::C, nx = g.nx;
+    const size_t roff = (size_t)rank * L::RL;
     const TwT tw{tws, N};
     for (int n = 0; n < 3; ++n) {
-        if (threadIdx.x == 0) bulk_load(buf, fr + ((size_t)n * nx + i) * RSP, RP<N>::BYTES, &mb);
+        if (threadIdx.x == 0) {
+            fence_async_smem();
+            bulk_load(buf, fr + ((size_t)n * nx + i) * RSP + roff, L::RBYTES, &mb);
+        }
         load_wait(&mb, phase, sc);
         const double fmn = sc->frmean[n];
         double *b = (double *)buf;
-        for (int e = threadIdx.x; e < RSP; e += blockDim.x) b[e] = b[e] - fmn;
+        for (int e = threadIdx.x; e < L::RL; e += L::T) b[e] = b[e] - fmn;
         __syncthreads();
-        plane_r2c<N>(buf, tw);
+        cl_r2c<N>(buf, tw, rank);
         double2 *dst = ff + ((size_t)n * nx + i) * PS;
-        for (int e = threadIdx.x; e < PS; e += blockDim.x) {
-            const int kz = e / my2, j = e - kz * my2;
-            const double2 X = unpack_col<N>(buf, kz, j);
-            dst[e] = make_double2(X.x / g.nrm, X.y / g.nrm);
+#pragma unroll 4
+        for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
+            const int kz = e / L::PZ, jl = e - kz * L::PZ;
+            if (jl == L::MC && rank != 0) continue;
+            const double2 X = cl_unpack<N>(buf, kz, jl, rank);
+            dst[kz * my2 + cl_col<N>(jl, rank)] = make_double2(X.x / g.nrm, X.y / g.nrm);
         }
         __syncthreads();
     }
@@ -1111,41 +1131,52 @@ __global__ void k_d2f(const double2 *__restrict__ d, double2 *__restrict__ f, in
 // Standalone batched plane transforms (pibm_ff2rc / pibm_ff2cr) on natural
 // host layouts: real a[z*my + y], complex b[kz*my2 + ky].
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T, 1) k_ff2cr(Geo g, const double2 *__restrict__ a, double *__restrict__ b) {
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff2cr(Geo g, const double2 *__restrict__ a, double *__restrict__ b) {
+    using L = PL<N>;
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
-    double2 *buf = sm, *tws = sm + PS;
+    double2 *buf = sm, *tws = sm + L::BUF;
     load_tw<N>(tws, g);
     const TwT tw{tws, N};
-    const size_t q = blockIdx.x;
-    for (int e = threadIdx.x; e < PS; e += blockDim.x) buf[e] = a[q * PS + e];
+    const size_t q = blockIdx.x / L::C;
+    const int rank = blockIdx.x % L::C;
+    for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
+        const int kz = e / L::PZ, jl = e - kz * L::PZ;
+        if (jl == L::MC && rank != 0) continue;
+        buf[e] = a[q * PS + kz * my2 + cl_col<N>(jl, rank)];
+    }
     __syncthreads();
-    if (threadIdx.x < 32) pack_col0_warp<N>(buf);
-    __syncthreads();
-    plane_c2r<N>(buf, tw);
-    for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-        const int z = e / N, y = e - z * N;
-        b[q * RS + e] = ((const double *)buf)[smem_real_off<N>(z, y)];
+    cl_c2r<N>(buf, tw, rank);
+    const double *rb = (const double *)buf;
+    for (int e = threadIdx.x; e < L::NR * N; e += L::T) {
+        const int r = e / N, y = e - r * N;
+        const int z = zinv<N>(rank * L::NR + r);
+        b[q * RS + (size_t)z * N + y] = rb[r * (N + 2) + 2 * yslot<N>(y >> 1) + (y & 1)];
     }
 }
 template <int N>
-__global__ void __launch_bounds__(Plan<N>::T, 1) k_ff2rc(Geo g, const double *__restrict__ a, double2 *__restrict__ b) {
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff2rc(Geo g, const double *__restrict__ a, double2 *__restrict__ b) {
+    using L = PL<N>;
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RS = N * N;
-    double2 *buf = sm, *tws = sm + PS;
+    double2 *buf = sm, *tws = sm + L::BUF;
     load_tw<N>(tws, g);
     const TwT tw{tws, N};
-    const size_t q = blockIdx.x;
-    for (int e = threadIdx.x; e < RS; e += blockDim.x) {
-        const int z = e / N, y = e - z * N;
-        ((double *)buf)[smem_real_off<N>(z, y)] = a[q * RS + e];
+    const size_t q = blockIdx.x / L::C;
+    const int rank = blockIdx.x % L::C;
+    double *rb = (double *)buf;
+    for (int e = threadIdx.x; e < L::NR * N; e += L::T) {
+        const int r = e / N, y = e - r * N;
+        const int z = zinv<N>(rank * L::NR + r);
+        rb[r * (N + 2) + 2 * yslot<N>(y >> 1) + (y & 1)] = a[q * RS + (size_t)z * N + y];
     }
     __syncthreads();
-    plane_r2c<N>(buf, tw);
-    for (int e = threadIdx.x; e < PS; e += blockDim.x) {
-        const int kz = e / my2, j = e - kz * my2;
-        const double2 X = unpack_col<N>(buf, kz, j);
-        b[q * PS + e] = make_double2(X.x / g.nrm, X.y / g.nrm);
+    cl_r2c<N>(buf, tw, rank);
+    for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
+        const int kz = e / L::PZ, jl = e - kz * L::PZ;
+        if (jl == L::MC && rank != 0) continue;
+        const double2 X = cl_unpack<N>(buf, kz, jl, rank);
+        b[q * PS + kz * my2 + cl_col<N>(jl, rank)] = make_double2(X.x / g.nrm, X.y / g.nrm);
     }
 }
 
@@ -1153,7 +1184,27 @@ __global__ void __launch_bounds__(Plan<N>::T, 1) k_ff2rc(Geo g, const double *__
 // Host-side launch helpers
 // ============================================================================
 template <int N>
-static size_t plane_smem() { return (size_t)((N / 2 + 1) * N + N) * sizeof(double2); }
+static size_t plane_smem() { return cl_smem<N>(); }
+
+// Launch a plane kernel on nplanes planes: PL<N>::C CTAs per plane, grouped
+// into clusters of that size (the plane's CTAs exchange data through
+// distributed shared memory).
+template <int N, typename... KArgs, typename... Args>
+static void launch_planes(void (*k)(KArgs...), int nplanes, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(nplanes * PL<N>::C), 1, 1);
+    cfg.blockDim = dim3(PL<N>::T, 1, 1);
+    cfg.dynamicSmemBytes = plane_smem<N>();
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = PL<N>::C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, args...);
+}
 
 template <int N>
 static cudaError_t set_attrs() {
@@ -1180,6 +1231,17 @@ cudaError_t configure_kernels(int n) {
 
 bool supported_size(int n) { return n == 32 || n == 64 || n == 96 || n == 128; }
 
+// CTAs that share one plane in the plane kernels (per-plane partial sums come in that many parts).
+int plane_ctas(int n) {
+    switch (n) {
+        case 32: return PL<32>::C;
+        case 64: return PL<64>::C;
+        case 96: return PL<96>::C;
+        case 128: return PL<128>::C;
+        default: return 1;
+    }
+}
+
 // Physical offset of real node (z, y) in one plane (host side of real_off).
 int real_offset(int n, int z, int y) {
     switch (n) {
@@ -1195,16 +1257,15 @@ int real_offset(int n, int z, int y) {
 // receives this step's nonlinear term (the other holds the previous step's).
 template <int N>
 static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev) {
-    const size_t sm = plane_smem<N>();
-    constexpr int T = Plan<N>::T;
     const int old = 1 - cur;
     auto mark = [&](int q) { if (ev) cudaEventRecord(ev[q], s); };
     mark(0);
-    k_a0<N><<<g.nx, T, sm, s>>>(g, b.u, b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
+    launch_planes<N>(k_a0<N>, g.nx, s, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
     k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
     mark(1);
     k_flux<N><<<(RP<N>::RSP * (g.nx / 32) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
-    k_nl<N><<<g.nx, T, sm, s>>>(g, b.ubcp, b.Dx, b.u, b.nl[old], b.nl[cur], b.Q, b.sc);
+    launch_planes<N>(k_nl<N>, g.nx, s, g, (const double *)b.ubcp, (const double *)b.Dx, (const double2 *)b.u,
+                     (const double2 *)b.nl[old], b.nl[cur], b.Q, b.sc);
     mark(2);
     if (g.nbody > 0) {
         k_drag<N><<<g.nbody * kDragSplit, 256, 0, s>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
@@ -1217,7 +1278,7 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
             if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.ctb, b.fr, b.sc);
         }
         mark(4);
-        k_ff<N><<<g.nx, T, sm, s>>>(g, b.fr, b.ff, b.sc);
+        launch_planes<N>(k_ff<N>, g.nx, s, g, (const double *)b.fr, b.ff, b.sc);
     } else {
         mark(3); mark(4);
     }
@@ -1246,7 +1307,7 @@ void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t
 
 template <int N>
 static void enqueue_c2r_t(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s) {
-    k_ff2cr<N><<<nplanes, Plan<N>::T, plane_smem<N>(), s>>>(g, a, b);
+    launch_planes<N>(k_ff2cr<N>, nplanes, s, g, a, b);
 }
 void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s) {
     switch (g.my) {
@@ -1258,7 +1319,7 @@ void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStr
 }
 template <int N>
 static void enqueue_r2c_t(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s) {
-    k_ff2rc<N><<<nplanes, Plan<N>::T, plane_smem<N>(), s>>>(g, a, b);
+    launch_planes<N>(k_ff2rc<N>, nplanes, s, g, a, b);
 }
 void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s) {
     switch (g.my) {

@@ -1,0 +1,240 @@
+// plane_cl.cuh -- y-z plane transforms split over a thread-block cluster.
+//
+// A whole complex half-plane (N rows kz x N/2+1 columns ky, FP64) is 133 KB
+// at N = 128, so a CTA that holds one leaves room for no second CTA on the SM
+// and its loads, stores and barriers cannot overlap anything.  Here a plane
+// is shared by a cluster of C CTAs, each holding 1/C of it:
+//
+//   column phase (z transforms)  CTA r holds columns ky in [r*MC, (r+1)*MC) of
+//                                all N rows at pitch PZ = MC+1; CTA 0 also
+//                                keeps column ky = M = N/2 in slot MC.
+//   row phase (y transforms)     CTA r holds rows [r*NR, (r+1)*NR) of the plane
+//                                in z-transform output order at pitch P = M+1:
+//                                exactly those rows of the single-CTA image,
+//                                so a real plane keeps its HBM layout and CTA r
+//                                moves its rows with one contiguous bulk copy.
+//
+// Between the phases every CTA reads the part it needs from the other CTAs'
+// shared memory (distributed shared memory, map_shared_rank) between two
+// cluster barriers, then rewrites its own buffer in the other layout.  The
+// arithmetic of every element is the same as in the single-CTA transform.
+#pragma once
+#include <cooperative_groups.h>
+
+#include "fft2d.cuh"
+
+namespace pibm {
+
+namespace cg = cooperative_groups;
+
+// CTAs per plane (C) and threads per CTA (T) for each supported size.
+template <int N> struct ClCfg;
+template <> struct ClCfg<32>  { static constexpr int C = 1, T = 256; };
+template <> struct ClCfg<64>  { static constexpr int C = 2, T = 128; };
+template <> struct ClCfg<96>  { static constexpr int C = 2, T = 256; };
+template <> struct ClCfg<128> { static constexpr int C = 2, T = 256; };
+
+template <int N> struct PL {
+    static constexpr int C = ClCfg<N>::C, T = ClCfg<N>::T;
+    static constexpr int M = N / 2, P = M + 1;          // row-phase pitch (complex slots)
+    static constexpr int MC = M / C, PZ = MC + 1;       // columns per CTA, column-phase pitch
+    static constexpr int NR = N / C;                    // rows per CTA in the row phase
+    static constexpr int BUF = (N * PZ > NR * P) ? N * PZ : NR * P;   // complex slots of the buffer
+    static constexpr int RL = NR * (N + 2);             // doubles of one CTA's real rows
+    static constexpr uint32_t RBYTES = RL * 8;
+    static constexpr int NOUT = N * PZ;                 // column-phase slots (slot MC: rank 0 only)
+    static constexpr int EPT = (NOUT + T - 1) / T;
+    static constexpr int MINB = 512 / T;                // CTAs per SM the register budget is sized for
+    static_assert(M % C == 0 && N % C == 0, "plane split");
+    static_assert(RBYTES % 16 == 0, "bulk copies move 16-byte multiples");
+};
+// Dynamic shared memory of a plane kernel: buffer + twiddle table.
+template <int N> constexpr size_t cl_smem() { return (size_t)(PL<N>::BUF + N) * sizeof(double2); }
+
+// Physical z of shared-memory row R (inverse of zrow), and pair index m of
+// row slot s (inverse of yslot).
+template <int N> __device__ __forceinline__ int zinv(int R) { return (R % Plan<N>::BZ) * Plan<N>::AZ + R / Plan<N>::BZ; }
+template <int N> __device__ __forceinline__ int yinv(int s) { return (s % Plan<N>::BY) * Plan<N>::AY + s / Plan<N>::BY; }
+
+// Global column ky of column-phase slot jl of CTA `rank`.
+template <int N> __device__ __forceinline__ int cl_col(int jl, int rank) {
+    return jl == PL<N>::MC ? PL<N>::M : rank * PL<N>::MC + jl;
+}
+
+// CTA 0, warp 0: column 0 <- Herm(ky = 0) + i Herm(ky = M) (see herm_pack).
+template <int N>
+__device__ __forceinline__ void cl_pack_col0(double2 *buf) {
+    using L = PL<N>;
+    constexpr int R = (N + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    double2 y[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        if (k < N) {
+            const int km = (N - k) % N;
+            y[r] = herm_pack(buf[k * L::PZ], buf[km * L::PZ], buf[k * L::PZ + L::MC], buf[km * L::PZ + L::MC]);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int k = lane + 32 * r;
+        if (k < N) buf[k * L::PZ] = y[r];
+    }
+}
+
+// Spectral value of column-phase slot (kz, jl) after cl_r2c (unscaled).
+// CTA 0 reads ky = 0 (jl = 0) and ky = M (jl = MC) from the packed column 0.
+template <int N>
+__device__ __forceinline__ double2 cl_unpack(const double2 *buf, int kz, int jl, int rank) {
+    using L = PL<N>;
+    if (rank != 0 || (jl != 0 && jl != L::MC)) return buf[kz * L::PZ + jl];
+    const double2 y = buf[kz * L::PZ], ym = buf[((N - kz) % N) * L::PZ];
+    if (jl == 0) return make_double2(0.5 * (y.x + ym.x), 0.5 * (y.y - ym.y));
+    return make_double2(0.5 * (y.y + ym.y), -0.5 * (y.x - ym.x));
+}
+
+// Column phase -> row phase (after the z pass of a c2r).
+template <int N>
+__device__ __forceinline__ void cl_cols_to_rows(double2 *buf, int rank) {
+    using L = PL<N>;
+    if constexpr (L::C > 1) {
+        constexpr int TOT = L::NR * L::M, K = (TOT + L::T - 1) / L::T;
+        cg::cluster_group cl = cg::this_cluster();
+        cl.sync();   // every CTA of the plane finished its z pass
+        double2 v[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int u = (int)threadIdx.x + k * L::T;
+            if (u < TOT) {
+                const int r = u / L::M, c = u - r * L::M, h = c / L::MC;
+                const double2 *src = cl.map_shared_rank(buf, h);
+                v[k] = src[(rank * L::NR + r) * L::PZ + (c - h * L::MC)];
+            }
+        }
+        cl.sync();   // every CTA finished reading: buffers may be rewritten
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int u = (int)threadIdx.x + k * L::T;
+            if (u < TOT) {
+                const int r = u / L::M, c = u - r * L::M;
+                buf[r * L::P + c] = v[k];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Row phase -> column phase (after the y pass of an r2c).
+template <int N>
+__device__ __forceinline__ void cl_rows_to_cols(double2 *buf, int rank) {
+    using L = PL<N>;
+    if constexpr (L::C > 1) {
+        constexpr int TOT = N * L::MC, K = (TOT + L::T - 1) / L::T;
+        cg::cluster_group cl = cg::this_cluster();
+        cl.sync();
+        double2 v[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int u = (int)threadIdx.x + k * L::T;
+            if (u < TOT) {
+                const int z = u / L::MC, c = u - z * L::MC, h = z / L::NR;
+                const double2 *src = cl.map_shared_rank(buf, h);
+                v[k] = src[(z - h * L::NR) * L::P + rank * L::MC + c];
+            }
+        }
+        cl.sync();
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int u = (int)threadIdx.x + k * L::T;
+            if (u < TOT) {
+                const int z = u / L::MC, c = u - z * L::MC;
+                buf[z * L::PZ + c] = v[k];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// c2r reconstruction (see b_c2r_pre) of ROWS rows at pitch P.
+template <int N, int T, int ROWS>
+__device__ __forceinline__ void rows_c2r_pre(double2 *buf, const TwT &tw) {
+    constexpr int M = N / 2, P = N / 2 + 1, NP = M / 2 + 1;
+#pragma unroll 3
+    for (int u0 = 0; u0 < ROWS * NP; u0 += T) {
+        const int u = u0 + (int)threadIdx.x;
+        if (u < ROWS * NP) {
+            const int k = u % ROWS, n = u / ROWS;
+            double2 *row = buf + (size_t)k * P;
+            if (n == 0) {
+                const double2 y = row[0];
+                row[0] = c2r_pre_one(make_double2(y.x, 0.0), make_double2(y.y, 0.0), make_double2(1.0, 0.0));
+            } else if (2 * n == M) {
+                const double2 x = row[n];
+                row[n] = c2r_pre_one(x, x, tw.w(n, 2 * M, +1.0));
+            } else {
+                const double2 xa = row[n], xb = row[M - n];
+                row[n] = c2r_pre_one(xa, xb, tw.w(n, 2 * M, +1.0));
+                row[M - n] = c2r_pre_one(xb, xa, tw.w(M - n, 2 * M, +1.0));
+            }
+        }
+    }
+    __syncthreads();
+}
+// r2c split (see b_r2c_post) of ROWS rows at pitch P; ky = 0 / M packed into slot 0.
+template <int N, int T, int ROWS>
+__device__ __forceinline__ void rows_r2c_post(double2 *buf, const TwT &tw) {
+    constexpr int M = N / 2, P = N / 2 + 1, NP = M / 2 + 1;
+#pragma unroll 3
+    for (int u0 = 0; u0 < ROWS * NP; u0 += T) {
+        const int u = u0 + (int)threadIdx.x;
+        if (u < ROWS * NP) {
+            const int k = u % ROWS, n = u / ROWS;
+            double2 *row = buf + (size_t)k * P;
+            if (n == 0) {
+                const double2 z0 = row[0];
+                row[0] = make_double2(z0.x + z0.y, z0.x - z0.y);
+            } else if (2 * n == M) {
+                const double2 z = row[n];
+                row[n] = r2c_post_one(z, z, tw.w(n, 2 * M, -1.0));
+            } else {
+                const double2 za = row[n], zb = row[M - n];
+                row[n] = r2c_post_one(za, zb, tw.w(n, 2 * M, -1.0));
+                row[M - n] = r2c_post_one(zb, za, tw.w(M - n, 2 * M, -1.0));
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// c2r of the CTA's columns (natural kz, column-phase layout; CTA 0 with
+// ky = M in slot MC).  Call after a __syncthreads.  On return the CTA holds
+// rows [rank*NR, (rank+1)*NR) of the real plane image: real value (z, y) of
+// such a row R = zrow(z) is ((double*)buf)[(R - rank*NR)*(N+2) + 2*yslot(y/2) + (y&1)].
+template <int N>
+__device__ __forceinline__ void cl_c2r(double2 *buf, const TwT &tw, int rank) {
+    using L = PL<N>;
+    if (rank == 0) {
+        if (threadIdx.x < 32) cl_pack_col0<N>(buf);
+        __syncthreads();
+    }
+    bfft_v1<Plan<N>::AZ, Plan<N>::BZ, L::MC, L::T>(buf, 1, L::PZ, +1.0, tw);
+    cl_cols_to_rows<N>(buf, rank);
+    rows_c2r_pre<N, L::T, L::NR>(buf, tw);
+    bfft_v1<Plan<N>::AY, Plan<N>::BY, L::NR, L::T>(buf, L::P, 1, +1.0, tw);
+}
+
+// r2c of the CTA's real rows (row-phase layout, as cl_c2r leaves them).  Call
+// after a __syncthreads.  On return the CTA holds its columns, natural in kz,
+// unscaled; read them with cl_unpack.
+template <int N>
+__device__ __forceinline__ void cl_r2c(double2 *buf, const TwT &tw, int rank) {
+    using L = PL<N>;
+    bfft_v2<Plan<N>::AY, Plan<N>::BY, L::NR, L::T>(buf, L::P, 1, -1.0, tw);
+    rows_r2c_post<N, L::T, L::NR>(buf, tw);
+    cl_rows_to_cols<N>(buf, rank);
+    bfft_v2<Plan<N>::AZ, Plan<N>::BZ, L::MC, L::T>(buf, 1, L::PZ, -1.0, tw);
+}
+
+}  // namespace pibm
