@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
     const double2 *U0 = u + (size_t)i * PS, *U1 = u + ((size_t)nx + i) * PS, *U2 = u + ((size_t)2 * nx + i) * PS;
     const double2 *Pp = p + (size_t)i * PS;
     const size_t slot = ((size_t)i * L::C + rank) * 12;
-    for (int t = 0; t < 10; ++t) {
+    {
+        const int t = blockIdx.y;
         // spectral input of this CTA's columns
 #pragma unroll 4
         for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
@@ -178,10 +179,8 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
         double *dst = t < 3 ? ubcp + ((size_t)t * nx + i) * RSP
                     : t == 3 ? pbcp + (size_t)i * RSP
                     : (t < 7 ? omega + ((size_t)(t - 4) * nx + i) * RSP : pgr + ((size_t)(t - 7) * nx + i) * RSP);
-        if (threadIdx.x == 0) { bulk_store(dst + roff, buf, L::RBYTES); bulk_wait_read(); }
-        __syncthreads();
+        if (threadIdx.x == 0) { bulk_store(dst + roff, buf, L::RBYTES); bulk_wait_all(); }
     }
-    if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // compute_new_timestep's scalar tail (dependent_functions.F90:1137-1280).
@@ -384,7 +383,8 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const doubl
     // real component n of this CTA's rows
     auto Uc = [&](int n) { return ubcp + ((size_t)n * nx + i) * RS + roff; };
     const double c12 = g.c1 + g.c2;
-    for (int c = 0; c < 3; ++c) {
+    {
+        const int c = blockIdx.y;
         // nl_new of this plane accumulates i ky F(pa) + i kz F(pb) + F(D_c) in place
         double2 *dst = nl_new + ((size_t)c * nx + i) * PS;
         for (int q = 0; q < 3; ++q) {
@@ -449,10 +449,8 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const doubl
         }
         __syncthreads();
         cl_c2r<N>(buf, tw, rank);
-        if (threadIdx.x == 0) { bulk_store(Q + ((size_t)c * nx + i) * RS + roff, buf, L::RBYTES); bulk_wait_read(); }
-        __syncthreads();
+        if (threadIdx.x == 0) { bulk_store(Q + ((size_t)c * nx + i) * RS + roff, buf, L::RBYTES); bulk_wait_all(); }
     }
-    if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // ============================================================================
@@ -790,7 +788,8 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const doubl
     const int i = blockIdx.x / L::C, rank = blockIdx.x % L::C, nx = g.nx;
     const size_t roff = (size_t)rank * L::RL;
     const TwT tw{tws, N};
-    for (int n = 0; n < 3; ++n) {
+    {
+        const int n = blockIdx.y;
         if (threadIdx.x == 0) {
             fence_async_smem();
             bulk_load(buf, fr + ((size_t)n * nx + i) * RSP + roff, L::RBYTES, &mb);
@@ -809,9 +808,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const doubl
             const double2 X = cl_unpack<N>(buf, kz, jl, rank);
             dst[kz * my2 + cl_col<N>(jl, rank)] = make_double2(X.x / g.nrm, X.y / g.nrm);
         }
-        __syncthreads();
     }
-    if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // ============================================================================
@@ -1190,9 +1187,9 @@ static size_t plane_smem() { return cl_smem<N>(); }
 // into clusters of that size (the plane's CTAs exchange data through
 // distributed shared memory).
 template <int N, typename... KArgs, typename... Args>
-static void launch_planes(void (*k)(KArgs...), int nplanes, cudaStream_t s, Args... args) {
+static void launch_planes(void (*k)(KArgs...), int nplanes, int items, cudaStream_t s, Args... args) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(nplanes * PL<N>::C), 1, 1);
+    cfg.gridDim = dim3((unsigned)(nplanes * PL<N>::C), (unsigned)items, 1);
     cfg.blockDim = dim3(PL<N>::T, 1, 1);
     cfg.dynamicSmemBytes = plane_smem<N>();
     cfg.stream = s;
@@ -1260,11 +1257,11 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
     const int old = 1 - cur;
     auto mark = [&](int q) { if (ev) cudaEventRecord(ev[q], s); };
     mark(0);
-    launch_planes<N>(k_a0<N>, g.nx, s, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
+    launch_planes<N>(k_a0<N>, g.nx, 10, s, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
     k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
     mark(1);
     k_flux<N><<<(RP<N>::RSP * (g.nx / 32) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
-    launch_planes<N>(k_nl<N>, g.nx, s, g, (const double *)b.ubcp, (const double *)b.Dx, (const double2 *)b.u,
+    launch_planes<N>(k_nl<N>, g.nx, 3, s, g, (const double *)b.ubcp, (const double *)b.Dx, (const double2 *)b.u,
                      (const double2 *)b.nl[old], b.nl[cur], b.Q, b.sc);
     mark(2);
     if (g.nbody > 0) {
@@ -1278,7 +1275,7 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
             if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.ctb, b.fr, b.sc);
         }
         mark(4);
-        launch_planes<N>(k_ff<N>, g.nx, s, g, (const double *)b.fr, b.ff, b.sc);
+        launch_planes<N>(k_ff<N>, g.nx, 3, s, g, (const double *)b.fr, b.ff, b.sc);
     } else {
         mark(3); mark(4);
     }
@@ -1307,7 +1304,7 @@ void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t
 
 template <int N>
 static void enqueue_c2r_t(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s) {
-    launch_planes<N>(k_ff2cr<N>, nplanes, s, g, a, b);
+    launch_planes<N>(k_ff2cr<N>, nplanes, 1, s, g, a, b);
 }
 void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s) {
     switch (g.my) {
@@ -1319,7 +1316,7 @@ void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStr
 }
 template <int N>
 static void enqueue_r2c_t(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s) {
-    launch_planes<N>(k_ff2rc<N>, nplanes, s, g, a, b);
+    launch_planes<N>(k_ff2rc<N>, nplanes, 1, s, g, a, b);
 }
 void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s) {
     switch (g.my) {
