@@ -169,6 +169,26 @@ def cpu_baseline(prm, xc, steps=2, warmup=1, threads=None):
             "s_per_step": el / steps}
 
 
+def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024):
+    """Batched multiple-independent-simulation throughput against the plain
+    per-realization loop on the same GPU: 16 seeded realizations (grids from
+    {64, 96, 128}^3, phi ~ U[0.1, 0.4], d ~ U{12..20} cells, Re ~ U[10, 100]),
+    `steps` steps of every member each way, device-timed."""
+    import pureibm_ps2d_fd1d_b200 as pk
+    from pureibm_ps2d_fd1d_b200 import config
+    ens = config.mis_ensemble(n=n, seed=seed)
+    b = pk.Batch([(p, x) for p, x, _ in ens])
+    b.run(warmup)
+    cells = sum(p["my"] ** 3 for p, _, _ in ens) * steps
+    t_plain = b.time(steps, sequential=True)
+    t_batch = b.time(steps, sequential=False)
+    b.close()
+    return {"unit": "Mcell-steps/s", "plain": cells / (t_plain / 1e3) / 1e6, "batched": cells / (t_batch / 1e3) / 1e6,
+            "ratio": t_plain / t_batch, "members": n, "steps": steps, "seed": seed,
+            "grids": [p["my"] for p, _, _ in ens], "nbody": [len(x) for _, x, _ in ens],
+            "phi": [round(f, 4) for _, _, f in ens]}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -245,6 +265,10 @@ def run_gpu(args):
     view.p = C.cast(hp.data_ptr(), C.POINTER(C.c_double))
     assert lib.pibm_get_state(s.h, C.byref(view)) == 0
     e2e_steps = max(1, min(args.steps, 10))
+    for _ in range(2):   # untimed: first calls load the layout kernels and touch the pinned pages
+        assert lib.pibm_set_state(s.h, C.byref(view)) == 0
+        assert lib.pibm_step(s.h, 1, C.byref(rep)) == 0
+        assert lib.pibm_get_state(s.h, C.byref(view)) == 0
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -300,6 +324,8 @@ def run_gpu(args):
         "maxvolfrac": info.maxvolfrac,
         "last_step": {"divmax": rep.divmax, "norm_drag": rep.norm_drag, "dt": rep.dt},
     }
+    if not args.no_mis and world == 1:
+        line["batched_mis"] = batched_mis()
     if not args.no_cpu_baseline and world == 1:
         cb = cpu_baseline(prm, xc, steps=2, warmup=1)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -316,6 +342,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mis", action="store_true", help="skip the batched-realization measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

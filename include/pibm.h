@@ -203,7 +203,15 @@ int  pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *
  *      sample_inputs/set_mis_3d, run as one graph-captured launch stream) ---- */
 typedef struct pibm_batch pibm_batch;
 int  pibm_batch_create(int n, const pibm_params *prm, const pibm_particles *parts, pibm_batch **out);
+/* nsteps steps of every member: one CUDA graph launch per step, in which the
+ * members' steps are independent branches that the GPU runs concurrently.
+ * Members may also be stepped on their own between batch runs. */
 int  pibm_batch_run(pibm_batch *b, int nsteps);
+/* Device time (CUDA events on the batch stream) of nsteps steps of every
+ * member: sequential != 0 runs the plain per-realization loop (member after
+ * member, each replaying its own step graphs); sequential == 0 runs the batch
+ * graph.  *ms = elapsed milliseconds; members advance nsteps steps either way. */
+int  pibm_batch_time(pibm_batch *b, int nsteps, int sequential, double *ms);
 pibm_handle *pibm_batch_member(pibm_batch *b, int i);
 void pibm_batch_destroy(pibm_batch *b);
 

@@ -19,7 +19,7 @@ from . import abi
 from .abi import pibm_params, pibm_state_view, pibm_step_report, pibm_info
 from . import config
 
-__all__ = ["Solver", "load_library", "ff2rc", "ff2cr", "config", "abi", "PibmError"]
+__all__ = ["Solver", "Batch", "load_library", "ff2rc", "ff2cr", "config", "abi", "PibmError"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libpibm.so")
@@ -78,6 +78,20 @@ class Solver:
         self.particles = config.Particles(np.zeros((0, 3)) if xc is None else xc, vel)
         h = C.c_void_p()
         _check(lib.pibm_create(C.byref(self.params), C.byref(self.particles.struct), C.byref(h)))
+        self._owned = True
+        self._attach(h)
+
+    @classmethod
+    def _member(cls, h, owner):
+        """A view of a batch member's handle (owned and freed by the batch)."""
+        s = cls.__new__(cls)
+        s._owned = False
+        s._owner = owner
+        s._attach(h)
+        return s
+
+    def _attach(self, h):
+        lib = load_library()
         self.h = h
         info = pibm_info()
         _check(lib.pibm_info_get(self.h, C.byref(info)))
@@ -88,7 +102,8 @@ class Solver:
     # -- lifetime -------------------------------------------------------------
     def close(self):
         if getattr(self, "h", None):
-            load_library().pibm_destroy(self.h)
+            if getattr(self, "_owned", False):
+                load_library().pibm_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -151,3 +166,47 @@ class Solver:
         out = np.zeros(self.nx * self.my * self.mz, dtype=np.uint8)
         _check(load_library().pibm_get_fluid_mask(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8))))
         return out.reshape(self.mz, self.my, self.nx)
+
+
+class Batch:
+    """Independent realizations (e.g. a multiple-independent-simulation
+    ensemble) stepped together: one CUDA graph launch per step runs every
+    member's step as a concurrent branch (pibm_batch_*)."""
+
+    def __init__(self, members):
+        """members: list of (params, centres) pairs, as config.mis_ensemble makes them."""
+        lib = load_library()
+        n = len(members)
+        if n == 0:
+            raise ValueError("empty batch")
+        self._params = (pibm_params * n)(*[p if isinstance(p, pibm_params) else config.make_params(p)
+                                            for p, xc in members])
+        self._parts = [config.Particles(np.asarray(xc)) for _, xc in members]
+        parts = (abi.pibm_particles * n)(*[pp.struct for pp in self._parts])
+        h = C.c_void_p()
+        _check(lib.pibm_batch_create(n, self._params, parts, C.byref(h)))
+        self.h = h
+        self.members = [Solver._member(C.c_void_p(lib.pibm_batch_member(h, i)), self) for i in range(n)]
+
+    def run(self, nsteps: int):
+        _check(load_library().pibm_batch_run(self.h, int(nsteps)))
+
+    def time(self, nsteps: int, sequential: bool) -> float:
+        """Device milliseconds of nsteps steps of every member: the plain
+        per-realization loop (sequential) or the batch graph."""
+        ms = C.c_double()
+        _check(load_library().pibm_batch_time(self.h, int(nsteps), int(bool(sequential)), C.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            for m in self.members:
+                m.h = None
+            load_library().pibm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -102,7 +102,8 @@ EXPORTED = [
     "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run",
     "pibm_run_profiled", "pibm_get_state", "pibm_get_particles", "pibm_get_if_rev", "pibm_get_fluid_mask",
     "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
-    "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_member", "pibm_batch_destroy",
+    "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time", "pibm_batch_member",
+    "pibm_batch_destroy",
 ]
 
 
@@ -129,12 +130,13 @@ def bind(lib):
     lib.pibm_ff2cr_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, vp]
     lib.pibm_batch_create.argtypes = [C.c_int, P(pibm_params), P(pibm_particles), P(vp)]
     lib.pibm_batch_run.argtypes = [vp, C.c_int]
+    lib.pibm_batch_time.argtypes = [vp, C.c_int, C.c_int, P(C.c_double)]
     lib.pibm_batch_member.argtypes = [vp, C.c_int]
     lib.pibm_batch_member.restype = vp
     lib.pibm_batch_destroy.argtypes = [vp]
     lib.pibm_batch_destroy.restype = None
     for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_profiled",
                  "pibm_get_state", "pibm_get_particles", "pibm_get_if_rev", "pibm_get_fluid_mask",
-                 "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run"):
+                 "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
         getattr(lib, name).restype = C.c_int
     return lib

@@ -240,3 +240,56 @@ def random_array(my: int = 128, dia_cells: float = 20.0, phi: float = 0.2, re: f
     pts = random_sequential_addition(nbody, float(my), dia_cells, rng)
     pts, _ = hard_sphere_mc(pts, float(my), dia_cells, rng, mc_moves, 0.1 * dia_cells)
     return prm, pts
+
+
+def fcc_subset(n: int, L: float, dia: float, rng, origin=1.0):
+    """n sphere centres on randomly chosen sites of the densest periodic FCC
+    lattice of the box whose nearest-neighbour distance is >= dia.  Returns
+    None when the lattice has fewer than n sites."""
+    k = int(np.floor(L / (dia * np.sqrt(2.0)) + 1e-12))
+    if k < 1 or 4 * k ** 3 < n:
+        return None
+    a = L / k
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    cells = np.stack(np.meshgrid(np.arange(k), np.arange(k), np.arange(k), indexing="ij"), -1).reshape(-1, 1, 3)
+    sites = ((cells + base[None]) * a).reshape(-1, 3)
+    pick = rng.choice(sites.shape[0], size=n, replace=False)
+    return origin + sites[np.sort(pick)]
+
+
+def mis_ensemble(n: int = 16, seed: int = 2024, grids=(64, 96, 128), phi_range=(0.1, 0.4),
+                 dia_range=(12, 20), re_range=(10.0, 100.0), mc_moves: int = 200, vis: float = 0.012,
+                 cfl: float = 0.1):
+    """Seeded ensemble of independent fixed-sphere realizations (multiple
+    independent simulations, MIS): per member a grid from `grids`, a volume
+    fraction ~ U(phi_range), an integer diameter ~ U(dia_range) cells and a
+    particle Reynolds number ~ U(re_range).  Positions: random sequential
+    addition up to phi = 0.3; above it (beyond what RSA reaches reliably) a
+    random subset of the densest fitting FCC lattice, capped at the lattice's
+    capacity; then hard-sphere Monte Carlo moves (step 0.1 d).  Returns a list
+    of (params dict, centres (nbody, 3) grid units, achieved phi)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        my = int(rng.choice(np.asarray(grids)))
+        phi = float(rng.uniform(*phi_range))
+        dia = float(rng.integers(dia_range[0], dia_range[1] + 1))
+        re = float(rng.uniform(*re_range))
+        prm = default_params()
+        prm.update(my=my, lybyd=my / dia, dbydx=dia, re=re, vis=vis, cfl=cfl, cfl_max=0.5,
+                   discr_scheme="upwind", initialize_zero=True, dobnd=False, ramp_frac_steps=0)
+        vsph = np.pi / 6.0 * dia ** 3
+        nb = max(1, int(round(phi * my ** 3 / vsph)))
+        pts = None
+        if phi <= 0.3:
+            try:
+                pts = random_sequential_addition(nb, float(my), dia, rng, max_tries=200_000)
+            except RuntimeError:
+                pts = None
+        if pts is None:
+            k = int(np.floor(my / (dia * np.sqrt(2.0)) + 1e-12))
+            nb = min(nb, 4 * k ** 3)
+            pts = fcc_subset(nb, float(my), dia, rng)
+        pts, _ = hard_sphere_mc(pts, float(my), dia, rng, mc_moves, 0.1 * dia)
+        out.append((prm, pts, pts.shape[0] * vsph / my ** 3))
+    return out

@@ -465,37 +465,133 @@ int pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *d
 }
 
 // ---- batched independent realizations ----
+// All members step together through ONE CUDA graph per step parity: the graph
+// forks from the batch stream into every member's stream, runs one step of
+// each member as an independent branch, and joins back, so the GPU overlaps
+// the members' kernels (small grids leave most SMs idle when run alone).
 struct pibm_batch {
     std::vector<pibm_handle *> members;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    std::vector<int> base;      // each member's parity when the graphs were captured
+    int flip = 0;               // graph[flip] is the next batch step
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    ~pibm_batch() {
+        for (auto &gx : graph) if (gx) cudaGraphExecDestroy(gx);
+        if (fork) cudaEventDestroy(fork);
+        for (auto e : join) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+        for (auto *h : members) pibm_destroy(h);
+    }
 };
 
 int pibm_batch_create(int n, const pibm_params *prm, const pibm_particles *parts, pibm_batch **out) {
     if (n <= 0 || !prm || !out) return fail(PIBM_ERR_ARG, "bad argument");
+    *out = nullptr;
     pibm_batch *bt = new pibm_batch();
     for (int q = 0; q < n; ++q) {
         pibm_handle *h = nullptr;
         int rc = pibm_create(&prm[q], parts ? &parts[q] : nullptr, &h);
-        if (rc) { for (auto *m : bt->members) pibm_destroy(m); delete bt; return rc; }
+        if (rc) { delete bt; return rc; }
         bt->members.push_back(h);
     }
+    bt->join.resize((size_t)n, nullptr);
+    cudaError_t e = cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&bt->fork, cudaEventDisableTiming);
+    for (int q = 0; q < n && e == cudaSuccess; ++q) e = cudaEventCreateWithFlags(&bt->join[q], cudaEventDisableTiming);
+    if (e != cudaSuccess) { delete bt; return fail(PIBM_ERR_CUDA, std::string("batch stream/events: ") + cudaGetErrorString(e)); }
     *out = bt;
     return PIBM_OK;
 }
 
-int pibm_batch_run(pibm_batch *bt, int nsteps) {
-    if (!bt) return fail(PIBM_ERR_ARG, "null batch");
-    // every member replays its own graphs on its own stream; launches interleave
-    for (auto *h : bt->members)
-        for (int par = 0; par < 2; ++par)
-            if (!h->graph[par]) { int rc = pibm_run(h, 0, nullptr); if (rc) return rc; }
-    for (int s = 0; s < nsteps; ++s)
-        for (auto *h : bt->members) {
-            CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], h->stream));
-            h->cur ^= 1;
+// (Re)capture the two batch graphs if any member's parity no longer matches them.
+static int batch_graphs(pibm_batch *bt) {
+    const int n = (int)bt->members.size();
+    bool ok = bt->graph[0] && bt->graph[1] && (int)bt->base.size() == n;
+    for (int q = 0; ok && q < n; ++q) ok = bt->members[q]->cur == (bt->base[q] ^ bt->flip);
+    if (ok) return PIBM_OK;
+    for (auto &gx : bt->graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+    bt->base.resize((size_t)n);
+    for (int q = 0; q < n; ++q) bt->base[q] = bt->members[q]->cur;
+    bt->flip = 0;
+    for (int par = 0; par < 2; ++par) {
+        cudaGraph_t gr;
+        CUDA_OR_FAIL(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
+        CUDA_OR_FAIL(cudaEventRecord(bt->fork, bt->stream));
+        for (int q = 0; q < n; ++q) {
+            pibm_handle *h = bt->members[q];
+            CUDA_OR_FAIL(cudaStreamWaitEvent(h->stream, bt->fork, 0));
+            enqueue_step(h->g, h->b, bt->base[q] ^ par, h->stream, nullptr);
+            CUDA_OR_FAIL(cudaEventRecord(bt->join[q], h->stream));
+            CUDA_OR_FAIL(cudaStreamWaitEvent(bt->stream, bt->join[q], 0));
         }
+        CUDA_OR_FAIL(cudaStreamEndCapture(bt->stream, &gr));
+        const cudaError_t e = cudaGraphInstantiate(&bt->graph[par], gr, 0);
+        cudaGraphDestroy(gr);
+        CUDA_OR_FAIL(e);
+    }
+    return PIBM_OK;
+}
+
+// Enqueue nsteps batch steps on the batch stream (no synchronisation).
+static int batch_enqueue(pibm_batch *bt, int nsteps) {
+    int rc = batch_graphs(bt);
+    if (rc) return rc;
+    for (int s = 0; s < nsteps; ++s) {
+        CUDA_OR_FAIL(cudaGraphLaunch(bt->graph[bt->flip], bt->stream));
+        bt->flip ^= 1;
+        for (auto *h : bt->members) h->cur ^= 1;
+    }
+    return PIBM_OK;
+}
+
+// Every member's status after the batch stream has drained.
+static int batch_reports(pibm_batch *bt) {
+    CUDA_OR_FAIL(cudaStreamSynchronize(bt->stream));
     int rc = PIBM_OK;
     for (auto *h : bt->members) { int r = fill_report(h, nullptr); if (r && !rc) rc = r; }
     return rc;
+}
+
+int pibm_batch_run(pibm_batch *bt, int nsteps) {
+    if (!bt || nsteps < 0) return fail(PIBM_ERR_ARG, "bad argument");
+    int rc = batch_enqueue(bt, nsteps);
+    if (rc) return rc;
+    return batch_reports(bt);
+}
+
+int pibm_batch_time(pibm_batch *bt, int nsteps, int sequential, double *ms) {
+    if (!bt || nsteps <= 0 || !ms) return fail(PIBM_ERR_ARG, "bad argument");
+    for (auto *h : bt->members)
+        if (!h->graph[0] || !h->graph[1]) { int rc = pibm_run(h, 0, nullptr); if (rc) return rc; }
+    int rc = batch_graphs(bt);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    CUDA_OR_FAIL(cudaEventCreate(&e0));
+    CUDA_OR_FAIL(cudaEventCreate(&e1));
+    CUDA_OR_FAIL(cudaStreamSynchronize(bt->stream));
+    for (auto *h : bt->members) CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    CUDA_OR_FAIL(cudaEventRecord(e0, bt->stream));
+    if (sequential) {
+        // the plain loop: one realization after another, each on its own graphs
+        for (auto *h : bt->members)
+            for (int s = 0; s < nsteps; ++s) {
+                CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], bt->stream));
+                h->cur ^= 1;
+            }
+    } else {
+        rc = batch_enqueue(bt, nsteps);
+        if (rc) return rc;
+    }
+    CUDA_OR_FAIL(cudaEventRecord(e1, bt->stream));
+    CUDA_OR_FAIL(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CUDA_OR_FAIL(cudaEventElapsedTime(&t, e0, e1));
+    *ms = t;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return batch_reports(bt);
 }
 
 pibm_handle *pibm_batch_member(pibm_batch *bt, int i) {
@@ -503,10 +599,6 @@ pibm_handle *pibm_batch_member(pibm_batch *bt, int i) {
     return bt->members[i];
 }
 
-void pibm_batch_destroy(pibm_batch *bt) {
-    if (!bt) return;
-    for (auto *h : bt->members) pibm_destroy(h);
-    delete bt;
-}
+void pibm_batch_destroy(pibm_batch *bt) { delete bt; }
 
 }  // extern "C"
