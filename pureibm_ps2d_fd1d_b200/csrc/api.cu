@@ -101,7 +101,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     std::string err;
     if (!setup_run(*prm, parts, h->S, err)) { delete h; return fail(PIBM_ERR_ARG, err); }
     RunSetup &S = h->S;
-    if (!supported_size(S.my)) { delete h; return fail(PIBM_ERR_ARG, "MY must be one of 32, 64, 96, 128"); }
+    if (!supported_size(S.my)) { delete h; return fail(PIBM_ERR_ARG, "MY must be one of 32, 64, 96, 128, 256"); }
     int rc;
     auto guard = [&](cudaError_t e, const char *what) -> bool {
         if (e != cudaSuccess) { rc = fail(PIBM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)); return false; }

@@ -103,6 +103,7 @@ template <> struct Plan<32>  { static constexpr int AZ = 8,  BZ = 4, AY = 4,  BY
 template <> struct Plan<64>  { static constexpr int AZ = 8,  BZ = 8, AY = 8,  BY = 4, T = 256, EPT = 9; };
 template <> struct Plan<96>  { static constexpr int AZ = 12, BZ = 8, AY = 12, BY = 4, T = 512, EPT = 10; };
 template <> struct Plan<128> { static constexpr int AZ = 16, BZ = 8, AY = 8,  BY = 8, T = 512, EPT = 17; };
+template <> struct Plan<256> { static constexpr int AZ = 16, BZ = 16, AY = 16, BY = 8, T = 512, EPT = 65; };
 
 // smem row of physical z after an inverse z pass (bfft_v1 output order), and
 // the slot of real pair index m in a row (bfft_v1 output / bfft_v2 input order).
@@ -214,7 +215,7 @@ __device__ __forceinline__ void bfft_v2(double2 *buf, int ss, int es, double s, 
 //       column 0 <- Herm X0 + i Herm XM; the y reconstruction reads
 //       Re -> ky = 0 and Im -> ky = M back from column 0.
 //  r2c: both columns are real after the y pass, column 0 <- X0 + i XM; the
-//       spectrum is read back with unpack_col (A = (Y[k] + conj Y[-k])/2,
+//       spectrum is read back with cl_unpack (A = (Y[k] + conj Y[-k])/2,
 //       B = (Y[k] - conj Y[-k])/(2i)).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double2 herm_pack(double2 a, double2 am, double2 b, double2 bm) {
@@ -222,112 +223,9 @@ __device__ __forceinline__ double2 herm_pack(double2 a, double2 am, double2 b, d
     const double2 hm = make_double2(0.5 * (b.x + bm.x), 0.5 * (b.y - bm.y));
     return make_double2(h0.x - hm.y, h0.y + hm.x);
 }
-// In place on a natural spectrum in buf (warp 0 only; caller synchronises).
-template <int N>
-__device__ __forceinline__ void pack_col0_warp(double2 *buf) {
-    constexpr int M = N / 2, P = N / 2 + 1, R = (N + 31) / 32;
-    const int lane = threadIdx.x & 31;
-    double2 y[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int k = lane + 32 * r;
-        if (k < N) {
-            const int km = (N - k) % N;
-            y[r] = herm_pack(buf[(size_t)k * P], buf[(size_t)km * P], buf[(size_t)k * P + M], buf[(size_t)km * P + M]);
-        }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int k = lane + 32 * r;
-        if (k < N) buf[(size_t)k * P] = y[r];
-    }
-}
-// Spectral value (kz, j) of an r2c result whose ky = 0 / M columns are packed.
-template <int N>
-__device__ __forceinline__ double2 unpack_col(const double2 *buf, int kz, int j) {
-    constexpr int M = N / 2, P = N / 2 + 1;
-    if (j != 0 && j != M) return buf[(size_t)kz * P + j];
-    const double2 y = buf[(size_t)kz * P], ym = buf[(size_t)((N - kz) % N) * P];
-    if (j == 0) return make_double2(0.5 * (y.x + ym.x), 0.5 * (y.y - ym.y));
-    return make_double2(0.5 * (y.y + ym.y), -0.5 * (y.x - ym.x));
-}
-
-// c2r reconstruction of every row with the packed ky = 0 / M column.
-template <int N, int T>
-__device__ __forceinline__ void b_c2r_pre(double2 *buf, const TwT &tw) {
-    constexpr int M = N / 2, P = N / 2 + 1, NP = M / 2 + 1;
-#pragma unroll 3
-    for (int u0 = 0; u0 < N * NP; u0 += T) {
-        const int u = u0 + (int)threadIdx.x;
-        if (u < N * NP) {
-            const int k = u % N, n = u / N;
-            double2 *row = buf + (size_t)k * P;
-            if (n == 0) {
-                const double2 y = row[0];
-                row[0] = c2r_pre_one(make_double2(y.x, 0.0), make_double2(y.y, 0.0), make_double2(1.0, 0.0));
-            } else if (2 * n == M) {
-                const double2 x = row[n];
-                row[n] = c2r_pre_one(x, x, tw.w(n, 2 * M, +1.0));
-            } else {
-                const double2 xa = row[n], xb = row[M - n];
-                row[n] = c2r_pre_one(xa, xb, tw.w(n, 2 * M, +1.0));
-                row[M - n] = c2r_pre_one(xb, xa, tw.w(M - n, 2 * M, +1.0));
-            }
-        }
-    }
-    __syncthreads();
-}
-// r2c split of every row; ky = 0 and ky = M (both real) are packed into slot 0.
-template <int N, int T>
-__device__ __forceinline__ void b_r2c_post(double2 *buf, const TwT &tw) {
-    constexpr int M = N / 2, P = N / 2 + 1, NP = M / 2 + 1;
-#pragma unroll 3
-    for (int u0 = 0; u0 < N * NP; u0 += T) {
-        const int u = u0 + (int)threadIdx.x;
-        if (u < N * NP) {
-            const int k = u % N, n = u / N;
-            double2 *row = buf + (size_t)k * P;
-            if (n == 0) {
-                const double2 z0 = row[0];
-                row[0] = make_double2(z0.x + z0.y, z0.x - z0.y);
-            } else if (2 * n == M) {
-                const double2 z = row[n];
-                row[n] = r2c_post_one(z, z, tw.w(n, 2 * M, -1.0));
-            } else {
-                const double2 za = row[n], zb = row[M - n];
-                row[n] = r2c_post_one(za, zb, tw.w(n, 2 * M, -1.0));
-                row[M - n] = r2c_post_one(zb, za, tw.w(M - n, 2 * M, -1.0));
-            }
-        }
-    }
-    __syncthreads();
-}
-
-// c2r of a natural spectrum whose ky = 0 / M columns are packed into column 0
-// (see pack_col0_warp / herm_pack); call after a __syncthreads.  On return
-// real value (z, y) is ((double*)&buf[zrow(z)*pitch + yslot(y/2)])[y&1].
-template <int N>
-__device__ __forceinline__ void plane_c2r(double2 *buf, const TwT &tw) {
-    constexpr int P = N / 2 + 1, M = N / 2, T = Plan<N>::T;
-    bfft_v1<Plan<N>::AZ, Plan<N>::BZ, M, T>(buf, 1, P, +1.0, tw);
-    b_c2r_pre<N, T>(buf, tw);
-    bfft_v1<Plan<N>::AY, Plan<N>::BY, N, T>(buf, P, 1, +1.0, tw);
-}
-// r2c of a plane stored in the c2r output order; call after a __syncthreads.
-// On return the unscaled spectrum is natural with ky = 0 / M packed into
-// column 0: read it with unpack_col.
-template <int N>
-__device__ __forceinline__ void plane_r2c(double2 *buf, const TwT &tw) {
-    constexpr int P = N / 2 + 1, M = N / 2, T = Plan<N>::T;
-    bfft_v2<Plan<N>::AY, Plan<N>::BY, N, T>(buf, P, 1, -1.0, tw);
-    b_r2c_post<N, T>(buf, tw);
-    bfft_v2<Plan<N>::AZ, Plan<N>::BZ, M, T>(buf, 1, P, -1.0, tw);
-}
-
 // Offset of real node (z, y) inside one physical plane of the HBM real fields,
-// which are stored exactly as plane_c2r leaves the shared-memory buffer (rows
-// of my+2 doubles), so plane loads and stores are single bulk copies.
+// which are stored exactly as the c2r plane transform leaves its rows in
+// shared memory (rows of my+2 doubles), so plane loads and stores are bulk copies.
 template <int N> __device__ __host__ __forceinline__ int real_off(int z, int y) {
     return (Plan<N>::BZ * (z % Plan<N>::AZ) + z / Plan<N>::AZ) * (N + 2) + 2 * (Plan<N>::BY * ((y >> 1) % Plan<N>::AY) + (y >> 1) / Plan<N>::AY) + (y & 1);
 }

@@ -49,10 +49,6 @@ __device__ __forceinline__ void load_wait(uint64_t *mb, uint32_t &phase, Scal *s
     if (!mbar_wait(mb, phase)) atomicCAS(&sc->status, 0, PIBM_ERR_TIMEOUT);
     phase ^= 1u;
 }
-// smem double offset of real node (z, y) (plane_c2r output order)
-template <int N> __device__ __forceinline__ int smem_real_off(int z, int y) {
-    return zrow<N>(z) * (N + 2) + 2 * yslot<N>(y >> 1) + (y & 1);
-}
 
 // Deterministic block sum (fixed lane/warp tree).
 __device__ __forceinline__ double block_sum(double v, double *scr) {
@@ -1222,11 +1218,12 @@ cudaError_t configure_kernels(int n) {
         case 64: return set_attrs<64>();
         case 96: return set_attrs<96>();
         case 128: return set_attrs<128>();
+        case 256: return set_attrs<256>();
         default: return cudaErrorInvalidValue;
     }
 }
 
-bool supported_size(int n) { return n == 32 || n == 64 || n == 96 || n == 128; }
+bool supported_size(int n) { return n == 32 || n == 64 || n == 96 || n == 128 || n == 256; }
 
 // CTAs that share one plane in the plane kernels (per-plane partial sums come in that many parts).
 int plane_ctas(int n) {
@@ -1235,6 +1232,7 @@ int plane_ctas(int n) {
         case 64: return PL<64>::C;
         case 96: return PL<96>::C;
         case 128: return PL<128>::C;
+        case 256: return PL<256>::C;
         default: return 1;
     }
 }
@@ -1246,6 +1244,7 @@ int real_offset(int n, int z, int y) {
         case 64: return real_off<64>(z, y);
         case 96: return real_off<96>(z, y);
         case 128: return real_off<128>(z, y);
+        case 256: return real_off<256>(z, y);
         default: return -1;
     }
 }
@@ -1299,6 +1298,7 @@ void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t
         case 64: enqueue_step_t<64>(g, b, cur, s, ev); break;
         case 96: enqueue_step_t<96>(g, b, cur, s, ev); break;
         case 128: enqueue_step_t<128>(g, b, cur, s, ev); break;
+        case 256: enqueue_step_t<256>(g, b, cur, s, ev); break;
     }
 }
 
@@ -1312,6 +1312,7 @@ void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStr
         case 64: enqueue_c2r_t<64>(g, a, b, nplanes, s); break;
         case 96: enqueue_c2r_t<96>(g, a, b, nplanes, s); break;
         case 128: enqueue_c2r_t<128>(g, a, b, nplanes, s); break;
+        case 256: enqueue_c2r_t<256>(g, a, b, nplanes, s); break;
     }
 }
 template <int N>
@@ -1324,6 +1325,7 @@ void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStr
         case 64: enqueue_r2c_t<64>(g, a, b, nplanes, s); break;
         case 96: enqueue_r2c_t<96>(g, a, b, nplanes, s); break;
         case 128: enqueue_r2c_t<128>(g, a, b, nplanes, s); break;
+        case 256: enqueue_r2c_t<256>(g, a, b, nplanes, s); break;
     }
 }
 

@@ -33,6 +33,7 @@ template <> struct ClCfg<32>  { static constexpr int C = 1, T = 256; };
 template <> struct ClCfg<64>  { static constexpr int C = 2, T = 128; };
 template <> struct ClCfg<96>  { static constexpr int C = 2, T = 256; };
 template <> struct ClCfg<128> { static constexpr int C = 2, T = 256; };
+template <> struct ClCfg<256> { static constexpr int C = 8, T = 256; };
 
 template <int N> struct PL {
     static constexpr int C = ClCfg<N>::C, T = ClCfg<N>::T;
@@ -157,7 +158,10 @@ __device__ __forceinline__ void cl_rows_to_cols(double2 *buf, int rank) {
     }
 }
 
-// c2r reconstruction (see b_c2r_pre) of ROWS rows at pitch P.
+// c2r reconstruction of ROWS rows at pitch P: each row's M+1 spectral values
+// X[0..M] (ky = 0 in Re and ky = M in Im of slot 0) become the M complex
+// points Z[n] = (X[n] + conj X[M-n]) + i w+^n (X[n] - conj X[M-n]) of the
+// half-length inverse transform.
 template <int N, int T, int ROWS>
 __device__ __forceinline__ void rows_c2r_pre(double2 *buf, const TwT &tw) {
     constexpr int M = N / 2, P = N / 2 + 1, NP = M / 2 + 1;
@@ -182,7 +186,9 @@ __device__ __forceinline__ void rows_c2r_pre(double2 *buf, const TwT &tw) {
     }
     __syncthreads();
 }
-// r2c split (see b_r2c_post) of ROWS rows at pitch P; ky = 0 / M packed into slot 0.
+// r2c split of ROWS rows at pitch P: the half-length transform Z[0..M-1] of a
+// real row becomes X[n] = (Z[n] + conj Z[M-n])/2 + w-^n (Z[n] - conj Z[M-n])/(2i);
+// the two real values X[0] and X[M] are packed into slot 0 as X[0] + i X[M].
 template <int N, int T, int ROWS>
 __device__ __forceinline__ void rows_r2c_post(double2 *buf, const TwT &tw) {
     constexpr int M = N / 2, P = N / 2 + 1, NP = M / 2 + 1;

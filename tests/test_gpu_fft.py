@@ -36,3 +36,26 @@ def test_round_trip_many_planes(n):
     a = rng.standard_normal((37, n, n))
     back = pk.ff2cr(pk.ff2rc(a), n)
     assert rel(back, a) < TOL
+
+
+def _numpy_pair_256(rng):
+    n = 256
+    a = rng.standard_normal((3, n, n))
+    ky = np.arange(n // 2 + 1)[None, None, :]
+    kz = np.minimum(np.arange(n), n - np.arange(n))[None, :, None]
+    amp = (1.0 + ky ** 2 + kz ** 2) ** (-5.0 / 6.0)
+    b = (rng.standard_normal((3, n, n // 2 + 1)) + 1j * rng.standard_normal((3, n, n // 2 + 1))) * amp
+    return a, b
+
+
+@pytest.mark.gpu
+def test_plane_transforms_256_against_numpy():
+    """256^2 planes (8-CTA clusters): same conventions as the golden fixtures,
+    with numpy computed here."""
+    n = 256
+    a, b = _numpy_pair_256(np.random.default_rng(256))
+    got = pk.ff2rc(a)
+    assert rel(got, np.fft.rfft2(a, axes=(1, 2)) / float(np.float32(n * n))) < TOL
+    got = pk.ff2cr(b, n)
+    assert rel(got, np.fft.irfft2(b, s=(n, n), axes=(1, 2)) * (n * n)) < TOL
+    assert rel(pk.ff2cr(pk.ff2rc(a), n), a) < TOL

@@ -123,3 +123,15 @@ def test_deterministic_rerun():
         s.run(5)
         outs.append(s.get_state()["u"])
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.gpu
+def test_random_array_256_two_steps():
+    """256^3 grid (8-CTA plane clusters, 4-line x tiles), 6 spheres of d=20:
+    two steps against the oracle."""
+    prm, xc = config.random_array(my=256, dia_cells=20, nbody=6, seed=3, mc_moves=20)
+    gpu, cpu = make_pair(prm, xc)
+    for _ in range(2):
+        gpu.step()
+        cpu.step()
+    compare(gpu, cpu)
