@@ -120,6 +120,8 @@ typedef struct pibm_step_report {
     double pres_drag, visc_drag, total_drag;
     double mixmeanslipmod;
     int64_t nrpr_active_total;
+    double heat_ratio;       /* scalar: phi(x + Lx) = phi(x) / heat_ratio (1 without scalar) */
+    double nusselt;          /* scalar: nusselt_avg(3) of bcsetscal, bc_scalar.F90:361-363 */
 } pibm_step_report;
 
 /* Static description of a handle's grid and geometry. */
@@ -152,7 +154,7 @@ int  pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last);
  * the handle's stream: *total_ms = first-to-last event time; phase_ms[q]
  * (q < nphase <= PIBM_NPHASE) = summed duration of phase q over the steps.
  * One host synchronisation at the end. */
-#define PIBM_NPHASE 6   /* 0 u,p,omega,grad p -> real  1 nonlinear + IBM field  2 drag+mpg  3 reversal+spread  4 forcing FFT  5 x-lines */
+#define PIBM_NPHASE 7   /* 0 u,p,omega,grad p -> real  1 nonlinear + IBM field  2 drag+mpg  3 reversal+spread  4 forcing FFT  5 x-lines  6 passive scalar */
 int  pibm_run_profiled(pibm_handle *h, int nsteps, pibm_step_report *last,
                        double *total_ms, double *phase_ms, int nphase);
 int  pibm_get_state(pibm_handle *h, pibm_state_view *s);
@@ -160,6 +162,12 @@ int  pibm_get_state(pibm_handle *h, pibm_state_view *s);
  * xc, vel: positions (grid units) and velocities.  Any pointer may be NULL. */
 int  pibm_get_particles(pibm_handle *h, double *pres, double *visc, double *force,
                         double *xc, double *vel);
+/* Passive scalar (ISCALON = 1; scalstep, SRC/SCALAR/stepthescalar.F90:51-94):
+ * phif complex (nx+1,my2,mz) interleaved in the reference layout (plane nx+1
+ * is phif(1)/heat_ratio), flux_body (nbody) = sum over surface points of
+ * grad phi . n (calc_bndrev_data), ratios[0..2] = heat_ratio,
+ * heat_ratio_old, Nusselt number.  Any pointer may be NULL. */
+int  pibm_get_scalar(pibm_handle *h, double *phif, double *flux_body, double *ratios);
 /* Active reversal-point flags (part_array(m)%if_rev), (nbnd, nbody) column-major. */
 int  pibm_get_if_rev(pibm_handle *h, uint8_t *if_rev);
 /* Solid mask fluid_atijk(1:nx,1:my,1:mz) as 0/1 bytes, x fastest. */

@@ -45,6 +45,7 @@ def lib():
         L.orc_get_fluid_mask.argtypes = [vp, P(C.c_uint8)]
         L.orc_get_geometry.argtypes = [vp, P(C.c_double), P(C.c_double)]
         L.orc_get_field.argtypes = [vp, C.c_int, P(C.c_double)]
+        L.orc_get_scalar.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_double)]
         L.orc_ff2rc.argtypes = [C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
         L.orc_ff2cr.argtypes = [C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
         L.orc_cyclic_solve.argtypes = [C.c_int] + [P(C.c_double)] * 7
@@ -187,3 +188,18 @@ class OracleSolver:
             raise ValueError(which)
         lib().orc_get_field(self.h, which, out.ctypes.data_as(C.POINTER(C.c_double)))
         return out
+
+
+def get_scalar(solver) -> dict:
+    """Scalar state of an OracleSolver: phif complex (mz, my2, nx+1) (the
+    reference's (nx+1,my2,mz) array viewed in C order), per-sphere surface
+    flux, heat_ratio, heat_ratio_old and the Nusselt number."""
+    nx, my2, mz = solver.nx, solver.my2, solver.mz
+    phif = np.zeros((mz, my2, nx + 1), dtype=np.complex128)
+    flux = np.zeros(max(solver.nbody, 1))
+    ratios = np.zeros(3)
+    rc = lib().orc_get_scalar(solver.h, phif.ctypes.data_as(C.POINTER(C.c_double)), _dp(flux), _dp(ratios))
+    if rc != 0:
+        raise RuntimeError("oracle has no scalar (ISCALON = 0)")
+    return dict(phif=phif, flux_body=flux[:solver.nbody], heat_ratio=ratios[0], heat_ratio_old=ratios[1],
+                nusselt=ratios[2])

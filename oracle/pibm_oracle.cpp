@@ -82,6 +82,16 @@ struct Orc {
     std::vector<double> ubcp, pbcp, nlbc, onlbc, diffn, omega, ppr, fr;
     // ---- per-particle ---------------------------------------------------------
     std::vector<double> pres, visc, force;
+    // ---- passive scalar (ISCALON = 1, one species) ------------------------------
+    bool scal = false;
+    double gamma_s = 0, phisurf = 0, phistream = 0;
+    double heat_ratio = 1, heat_ratio_old = 1, heat_ratio_new = 1;
+    std::vector<cplx> phif, nlphif, onlphif, ffphi;        // (nx+1,my2,mz)
+    std::vector<double> phir, nlphir, onlphir, sdiffn;     // (nx+1,my,mz)
+    std::vector<double> gradphi;                           // (nx+1,my,mz,3)
+    std::vector<double> sfr;                               // fr(0:nx+1,my,mz)
+    std::vector<double> flux_body;                         // (nbody)
+    double flux_global = 0, nusselt = 0;
     int nthreads = 1;
 
     // index helpers, 1-based like the reference
@@ -91,6 +101,7 @@ struct Orc {
     size_t QI(int i, int j, int k, int n) const { return (size_t)(i - 1) + (size_t)nx * ((size_t)(j - 1) + (size_t)my * ((size_t)(k - 1) + (size_t)mz * (size_t)(n - 1))); }
     bool FL(int i, int j, int k) const { return fluid[(size_t)i + (size_t)(nx + 2) * ((size_t)(j - 1) + (size_t)my * (size_t)(k - 1))] != 0; }
     void SETFL(int i, int j, int k, bool v) { fluid[(size_t)i + (size_t)(nx + 2) * ((size_t)(j - 1) + (size_t)my * (size_t)(k - 1))] = v ? 1 : 0; }
+    size_t SF(int i, int j, int k) const { return (size_t)i + (size_t)(nx + 2) * ((size_t)(j - 1) + (size_t)my * (size_t)(k - 1)); }
     double XC(int m, int n) const { return xc[(size_t)(m - 1) + (size_t)nbody * (n - 1)]; }
     double &XCr(int m, int n) { return xc[(size_t)(m - 1) + (size_t)nbody * (n - 1)]; }
     double VB(int m, int n) const { return velbdy[(size_t)(m - 1) + (size_t)nbody * (n - 1)]; }
@@ -365,6 +376,14 @@ bool setup(Orc &o, const pibm_params *prm, const pibm_particles *parts) {
     double dt_tmp_conv = o.dx / umax_tmp;
     double dt_tmp_vis = LARGE_NUMBER, dt_tmp_grav = LARGE_NUMBER, dt_tmp_diff = LARGE_NUMBER, dtcoll = LARGE_NUMBER;
     if (prm->re < 1.0) dt_tmp_vis = prm->re * prm->dbydx * dt_tmp_conv / (prm->cfl * prm->vfl);
+    if (prm->iscalon) {
+        // initscal: SRC/SCALAR/scalar_init.F90:58-122 (gamma = vis/Pr, diffusive dt limit)
+        o.scal = true;
+        o.gamma_s = o.vis / prm->pr_or_sc_nu;
+        o.phisurf = prm->phisurf;
+        o.phistream = prm->phistream;
+        dt_tmp_diff = (o.dx * o.dx * (1.0 - o.maxvolfrac)) / o.gamma_s;
+    }
     neighbor_search(o);
     update_nrpr(o);
     o.dt = std::min(std::min(dt_tmp_conv, dt_tmp_vis), std::min(dt_tmp_grav, dt_tmp_diff));
@@ -399,6 +418,17 @@ bool setup(Orc &o, const pibm_params *prm, const pibm_particles *parts) {
     o.ppr.assign((size_t)o.nx * o.my * o.mz * 3, 0.0);
     o.pres.assign((size_t)o.nbody * 3, 0.0); o.visc.assign((size_t)o.nbody * 3, 0.0); o.force.assign((size_t)o.nbody * 3, 0.0);
     o.mixmeanslipmod = 0; o.meanslipmod = 0; o.umax_last = 0; o.divmax = 0; o.norm_drag = 0;
+    if (o.scal) {
+        // phi = 1 on every plane (scalar_init.F90:136-152): ff2rc of a constant
+        // plane is exactly 1 at ky = kz = 0 and 0 elsewhere
+        const size_t SC = (size_t)(o.nx + 1) * o.my2 * o.mz, SR = (size_t)(o.nx + 1) * o.my * o.mz;
+        o.phif.assign(SC, 0.0); o.nlphif.assign(SC, 0.0); o.onlphif.assign(SC, 0.0); o.ffphi.assign(SC, 0.0);
+        for (int i = 1; i <= o.nx + 1; ++i) o.phif[o.CI(i, 1, 1, 1)] = 1.0;
+        o.phir.assign(SR, 0.0); o.nlphir.assign(SR, 0.0); o.onlphir.assign(SR, 0.0); o.sdiffn.assign(SR, 0.0);
+        o.gradphi.assign(SR * 3, 0.0);
+        o.sfr.assign((size_t)(o.nx + 2) * o.my * o.mz, 0.0);
+        o.flux_body.assign(o.nbody, 0.0);
+    }
 #ifdef _OPENMP
     o.nthreads = omp_get_max_threads();
 #endif
@@ -1159,12 +1189,419 @@ int velstep(Orc &o, int rks) {
     return bad ? PIBM_ERR_PIVOT : PIBM_OK;
 }
 
+// ============================================================================
+// Passive scalar, one species (ISCALON = 1): scalstep, SRC/SCALAR/stepthescalar.F90:51-94.
+// The scalar is periodic in x up to the factor heat_ratio (fully developed
+// heat transfer): phi(x + L) = phi(x) / heat_ratio, so every x wrap below
+// carries that factor.  Array roles follow the reference's aliases: phir is
+// the real scalar (ubcp(:,:,:,1) there), nlphir/onlphir the real nonlinear
+// terms (nlbcp/onlbcp), sdiffn the real diffusion term (diffn), gradphi the
+// real gradient (ppr), sfr the real forcing (fr(0:nx+1)).
+// ============================================================================
+
+// form_nlphi + compute_phim_heat_ratio: SRC/SCALAR/nl_allphi.F90:59-253, 256-330 (serial).
+void form_nlphi(Orc &o) {
+    const int nx = o.nx, my = o.my, mz = o.mz, my2 = o.my2, mxf = o.mxf;
+    const bool center = o.prm.discr_scheme == PIBM_SCHEME_CENTER;
+    const double h = o.heat_ratio, dx = o.dx;
+    std::vector<double> pb((size_t)(nx + 1) * my * mz);            // phirbcp (nlbcp there), planes 1..nx+1
+    std::vector<double> fd((size_t)(nx + 2) * my * mz, 0.0);       // fdderiv(0:nx+1)
+    auto PB = [&](int i, int j, int k) -> double & { return pb[o.RI(i, j, k, 1)]; };
+    auto FD = [&](int i, int j, int k) -> double & { return fd[o.SF(i, j, k)]; };
+    auto U = [&](int i, int j, int k, int n) { return o.ubcp[o.RI(i, j, k, n)]; };
+#pragma omp parallel
+    {
+        std::vector<cplx> f2((size_t)my2 * mz), f3((size_t)my2 * mz);
+#pragma omp for schedule(static)
+        for (int i = 1; i <= nx + 1; ++i) {
+            c2r_with(o, [&](int j, int k) { return o.phif[o.CI(i, j, k, 1)]; }, [&](int j, int k, double v) { PB(i, j, k) = v; });
+            r2c_with(o, [&](int j, int k) { return U(i, j, k, 2) * PB(i, j, k); },
+                     [&](int j, int k, cplx v) { f2[(j - 1) + (size_t)my2 * (k - 1)] = v; });
+            r2c_with(o, [&](int j, int k) { return U(i, j, k, 3) * PB(i, j, k); },
+                     [&](int j, int k, cplx v) { f3[(j - 1) + (size_t)my2 * (k - 1)] = v; });
+            for (int k = 1; k <= mz; ++k)
+                for (int j = 1; j <= my2; ++j) {
+                    const size_t q = (j - 1) + (size_t)my2 * (k - 1);
+                    o.nlphif[o.CI(i, j, k, 1)] = o.wy[j - 1] * f2[q] + o.wz[k - 1] * f3[q];
+                }
+            for (int k = 1; k <= mz; ++k)
+                for (int j = 1; j <= my; ++j) FD(i, j, k) = center ? U(i, j, k, 1) * PB(i, j, k) : 0.0;
+        }
+    }
+    // compute_phim_heat_ratio(.TRUE.): only the last plane's mixed mean sets heat_ratio_new
+    {
+        const int i = nx + 1;
+        double phim = 0.0, um = 0.0;
+        long long cnt = 0;
+        for (int k = 1; k <= mz; ++k)
+            for (int j = 1; j <= my; ++j)
+                if (o.FL(i, j, k)) {
+                    phim = phim + U(i, j, k, 1) * PB(i, j, k);
+                    um = um + U(i, j, k, 1);
+                    cnt = cnt + 1;
+                }
+        um = um / (double)cnt;
+        phim = phim / (um * (double)cnt);
+        o.heat_ratio_new = 1.0 / phim;
+    }
+    for (int k = 1; k <= mz; ++k)
+        for (int j = 1; j <= my; ++j) FD(0, j, k) = center ? FD(nx, j, k) * h : 0.0;
+    if (!center) {
+#pragma omp parallel
+        {
+            std::vector<double> uplus(nx + 2), uminus(nx + 2), Up(nx + 2), Um(nx + 2), sp(nx + 2), su(nx + 2);
+#pragma omp for schedule(static)
+            for (int k = 1; k <= mz; ++k)
+                for (int j = 1; j <= my; ++j) {
+                    sp[0] = (PB(1, j, k) - PB(nx - 1, j, k) * h) / (2.0 * dx);
+                    Um[0] = PB(nx, j, k) * h + sp[0] * (dx / 2.0);
+                    sp[nx + 1] = (PB(2, j, k) / h - PB(nx, j, k)) / (2.0 * dx);
+                    Up[nx] = PB(1, j, k) / h - sp[nx + 1] * (dx / 2.0);
+                    su[0] = (U(1, j, k, 1) - U(nx - 1, j, k, 1)) / (2.0 * dx);
+                    uminus[0] = U(nx, j, k, 1) + su[0] * (dx / 2.0);
+                    su[nx + 1] = (U(2, j, k, 1) - U(nx, j, k, 1)) / (2.0 * dx);
+                    uplus[nx] = U(1, j, k, 1) - su[nx + 1] * (dx / 2.0);
+                    for (int i = 1; i <= nx; ++i) {
+                        int im1 = i - 1, ip1 = i + 1;
+                        double pfm = 1.0, pfp = 1.0;
+                        if (im1 < 1) { im1 = mxf + im1 - 1; pfm = h; }
+                        if (ip1 > mxf) { ip1 = ip1 - (mxf - 1); pfp = 1.0 / h; }
+                        sp[i] = (pfp * PB(ip1, j, k) - pfm * PB(im1, j, k)) / (2.0 * dx);
+                        su[i] = (U(ip1, j, k, 1) - U(im1, j, k, 1)) / (2.0 * dx);
+                        uplus[i - 1] = U(i, j, k, 1) - su[i] * (dx / 2.0);
+                        uminus[i] = U(i, j, k, 1) + su[i] * (dx / 2.0);
+                        Up[i - 1] = PB(i, j, k) - sp[i] * (dx / 2.0);
+                        Um[i] = PB(i, j, k) + sp[i] * (dx / 2.0);
+                    }
+                    for (int i = 0; i <= nx; ++i) {
+                        const double ms = std::max(std::fabs(uminus[i]), std::fabs(uplus[i]));
+                        double f = 0.5 * (uplus[i] * Up[i]) + 0.5 * (uminus[i] * Um[i]);
+                        FD(i, j, k) = f - 0.5 * ms * (Up[i] - Um[i]);
+                    }
+                }
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i <= nx; ++i)
+        r2c_with(o, [&](int j, int k) {
+                     if (center) return (FD(i + 1, j, k) - FD(i - 1, j, k)) / (2.0 * dx);
+                     return (FD(i, j, k) - FD(i - 1, j, k)) / dx; },
+                 [&](int j, int k, cplx v) { cplx &d = o.nlphif[o.CI(i, j, k, 1)]; d = d + v; });
+    for (int k = 1; k <= mz; ++k)
+        for (int j = 1; j <= my2; ++j) o.nlphif[o.CI(nx + 1, j, k, 1)] = o.nlphif[o.CI(1, j, k, 1)] / h;
+    for (int i = 1; i <= nx; ++i)
+        for (int k = 1; k <= mz; ++k) {
+            for (int j = 1; j <= my; ++j) o.phir[o.RI(i, j, k, 1)] = PB(i, j, k);
+            for (int j = 1; j <= my2; ++j) { cplx &v = o.nlphif[o.CI(i, j, k, 1)]; v = -v; }
+        }
+    for (int k = 1; k <= mz; ++k) {
+        for (int j = 1; j <= my2; ++j) { cplx &v = o.nlphif[o.CI(nx + 1, j, k, 1)]; v = -v; }
+        for (int j = 1; j <= my; ++j) o.phir[o.RI(nx + 1, j, k, 1)] = o.phir[o.RI(1, j, k, 1)] / h;
+    }
+}
+
+// calc_diffn: SRC/SCALAR/bc_scalar.F90:935-1033 (serial branch, planes 1..nx+1).
+void calc_diffn_scal(Orc &o) {
+    const int nx = o.nx, my2 = o.my2, mz = o.mz;
+    const double h = o.heat_ratio, dx = o.dx, dx2 = o.dx2;
+    auto PF = [&](int i, int j, int k) { return o.phif[o.CI(i, j, k, 1)]; };
+#pragma omp parallel
+    {
+        std::vector<cplx> f1((size_t)my2 * mz), f2((size_t)my2 * mz), f3((size_t)my2 * mz), f4((size_t)my2 * mz);
+#pragma omp for schedule(static)
+        for (int i = 1; i <= nx + 1; ++i) {
+            for (int k = 1; k <= mz; ++k)
+                for (int j = 1; j <= my2; ++j) {
+                    const size_t q = (j - 1) + (size_t)my2 * (k - 1);
+                    cplx a;
+                    if (i == 1) a = (1.0 / dx2) * (PF(nx, j, k) * h - 2.0 * PF(1, j, k) + PF(2, j, k));
+                    else if (i == nx) a = (1.0 / dx2) * (PF(i - 1, j, k) - 2.0 * PF(i, j, k) + PF(1, j, k) / h);
+                    else if (i == nx + 1) a = (1.0 / dx2) * (PF(i - 1, j, k) - 2.0 * PF(i, j, k) + PF(2, j, k) / h);
+                    else a = (1.0 / dx2) * (PF(i - 1, j, k) - 2.0 * PF(i, j, k) + PF(i + 1, j, k));
+                    a = a - o.W2(j, k) * PF(i, j, k);
+                    f1[q] = a * o.gamma_s;
+                    if (i == 1) f2[q] = (PF(2, j, k) - PF(nx, j, k) * h) / (2.0 * dx);
+                    else if (i == nx) f2[q] = (PF(1, j, k) / h - PF(i - 1, j, k)) / (2.0 * dx);
+                    else if (i == nx + 1) f2[q] = (PF(2, j, k) / h - PF(i - 1, j, k)) / (2.0 * dx);
+                    else f2[q] = (PF(i + 1, j, k) - PF(i - 1, j, k)) / (2.0 * dx);
+                    f3[q] = PF(i, j, k) * o.wy[j - 1];
+                    f4[q] = PF(i, j, k) * o.wz[k - 1];
+                }
+            auto out = [&](std::vector<cplx> &f, std::vector<double> &dst, int n) {
+                c2r_with(o, [&](int j, int k) { return f[(j - 1) + (size_t)my2 * (k - 1)]; },
+                         [&](int j, int k, double v) { dst[o.RI(i, j, k, n)] = v; });
+            };
+            out(f1, o.sdiffn, 1); out(f2, o.gradphi, 1); out(f3, o.gradphi, 2); out(f4, o.gradphi, 3);
+        }
+    }
+}
+
+// set_interpolation_stencil ('lpi', order 2, x periodic; dependent_functions.F90:45-158)
+// without wrapping, and the weights of interp_threed with shape2.
+struct RawSten {
+    int ib, jb, kb;
+    double w[2][2][2];
+};
+inline void raw_stencil(const Orc &o, const int pc[3], const double pos[3], RawSten &s) {
+    int ib = std::max(1, pc[0]), ie = std::min(o.mxf, pc[0] + 1);
+    if (ib == 1) ib = ie - 2 + 1;
+    int jb = std::max(1, pc[1]), je = std::min(o.my, pc[1] + 1);
+    if (jb == 1) jb = je - 2 + 1;
+    int kb = std::max(1, pc[2]), ke = std::min(o.mz, pc[2] + 1);
+    if (kb == 1) kb = ke - 2 + 1;
+    s.ib = ib; s.jb = jb; s.kb = kb;
+    const double zx = (pos[0] - (double)ib) / (double)((ib + 1) - ib);
+    const double zy = (pos[1] - (double)jb) / (double)((jb + 1) - jb);
+    const double zz = (pos[2] - (double)kb) / (double)((kb + 1) - kb);
+    const double xv[2] = {1.0 - zx, zx}, yv[2] = {1.0 - zy, zy}, zv[2] = {1.0 - zz, zz};
+    for (int k = 0; k < 2; ++k) for (int j = 0; j < 2; ++j) for (int i = 0; i < 2; ++i) s.w[i][j][k] = xv[i] * yv[j] * zv[k];
+}
+inline int wrap_yz(int v, int n) { return v < 1 ? v + n : (v > n ? v - n : v); }
+
+// interpolate_phidata: SRC/SCALAR/bc_scalar.F90:1036-1153 (serial).  x indices
+// below 1 wrap with the factor heat_ratio (heat_ratio_old for onlphir), above
+// mxf with 1/heat_ratio.  flag 1 also interpolates nl, onl and diffn.
+void interp_phi(const Orc &o, const int pc[3], const double pos[3], int flag, RawSten &s,
+                double &ul, double &nll, double &onll, double &dfll) {
+    raw_stencil(o, pc, pos, s);
+    double v[2][2][2], nl[2][2][2], onl[2][2][2], df[2][2][2];
+    for (int k = 0; k < 2; ++k)
+        for (int j = 0; j < 2; ++j)
+            for (int i = 0; i < 2; ++i) {
+                int ii = s.ib + i, jj = wrap_yz(s.jb + j, o.my), kk = wrap_yz(s.kb + k, o.mz);
+                double pf = 1.0, pfo = 1.0;
+                if (ii < 1) { ii = o.mxf + ii - 1; pf = o.heat_ratio; pfo = o.heat_ratio_old; }
+                else if (ii > o.mxf) { ii = ii - o.mxf + 1; pf = 1.0 / o.heat_ratio; }
+                v[i][j][k] = o.phir[o.RI(ii, jj, kk, 1)] * pf;
+                if (flag == 1) {
+                    nl[i][j][k] = o.nlphir[o.RI(ii, jj, kk, 1)] * pf;
+                    onl[i][j][k] = o.onlphir[o.RI(ii, jj, kk, 1)] * pfo;
+                    df[i][j][k] = o.sdiffn[o.RI(ii, jj, kk, 1)] * pf;
+                }
+            }
+    ul = 0.0;
+    for (int k = 0; k < 2; ++k) for (int j = 0; j < 2; ++j) for (int i = 0; i < 2; ++i) ul = ul + v[i][j][k] * s.w[i][j][k];
+    if (flag == 1) {
+        nll = 0.0; onll = 0.0; dfll = 0.0;
+        for (int i = 0; i < 2; ++i) for (int j = 0; j < 2; ++j) for (int k = 0; k < 2; ++k) nll = nll + nl[i][j][k] * s.w[i][j][k];
+        for (int i = 0; i < 2; ++i) for (int j = 0; j < 2; ++j) for (int k = 0; k < 2; ++k) onll = onll + onl[i][j][k] * s.w[i][j][k];
+        for (int i = 0; i < 2; ++i) for (int j = 0; j < 2; ++j) for (int k = 0; k < 2; ++k) dfll = dfll + df[i][j][k] * s.w[i][j][k];
+    }
+}
+
+// calc_bndrev_data with DOBND = F: surface flux of sphere m from the
+// interpolated gradient (SRC/SCALAR/bc_scalar.F90:385-556, serial branch).
+double scal_surface_flux(const Orc &o, int m) {
+    double fluxloc = 0.0;
+    for (int l = 1; l <= o.nbnd; ++l) {
+        double xl[3];
+        int is[3];
+        for (int n = 1; n <= 3; ++n) {
+            xl[n - 1] = o.XC(m, n) + o.BND(n, l) * o.radbdy[m - 1];
+            is[n - 1] = cell_of(xl[n - 1]);
+        }
+        // CELL_IN_BOX / WEST_PERIODIC_IMAGE / EAST_PERIODIC_IMAGE (ibm.h:147-149)
+        if (!(1 <= is[0] && is[0] <= o.nx)) {
+            if (is[0] < 1) { xl[0] = o.mxf + xl[0] - 1; is[0] = o.mxf + is[0] - 1; }
+            else if (is[0] >= o.mxf) { xl[0] = xl[0] - (o.mxf - 1); is[0] = is[0] - (o.mxf - 1); }
+        }
+        RawSten s;
+        raw_stencil(o, is, xl, s);
+        double g[3][2][2][2];
+        for (int k = 0; k < 2; ++k)
+            for (int j = 0; j < 2; ++j)
+                for (int i = 0; i < 2; ++i) {
+                    int ii = s.ib + i, jj = wrap_yz(s.jb + j, o.my), kk = wrap_yz(s.kb + k, o.mz);
+                    double pf = 1.0;
+                    if (ii < 1) { ii = o.mxf + ii - 1; pf = o.heat_ratio; }
+                    if (ii > o.mxf) { ii = ii - o.mxf + 1; pf = 1.0 / o.heat_ratio; }
+                    for (int n = 1; n <= 3; ++n) g[n - 1][i][j][k] = o.gradphi[o.RI(ii, jj, kk, n)] * pf;
+                }
+        double gb[3];
+        for (int n = 0; n < 3; ++n) {
+            double r = 0.0;
+            for (int i = 0; i < 2; ++i) for (int j = 0; j < 2; ++j) for (int k = 0; k < 2; ++k) r = r + g[n][i][j][k] * s.w[i][j][k];
+            gb[n] = r;
+        }
+        double d = 0.0;
+        for (int n = 1; n <= 3; ++n) d = d + gb[n - 1] * o.BND(n, l);
+        fluxloc = fluxloc + d;
+    }
+    return fluxloc;
+}
+
+// calc_inner_rev_data: SRC/SCALAR/bc_scalar.F90:558-932 (serial branch).  A
+// point whose cell is the last one (i = nx) is evaluated twice, as itself and
+// shifted one period west; each evaluation spreads onto its own stencil and
+// the forcing on planes 0 and nx+1 is not transformed.
+void scal_inner_forcing(Orc &o, int m, double da2) {
+    const double dx3 = std::pow(o.dx, 3.0), drm = 1.0;
+    const double c1 = o.coef[0], c2 = o.coef[1], c3 = o.coef[2], c4 = o.coef[3];
+    const double rb = o.radbdy[m - 1], ri = o.radibdy[m - 1], ro = o.radobdy[m - 1];
+    for (int l = 1; l <= o.nbnd; ++l) {
+        if (!o.if_rev[(size_t)(l - 1) + (size_t)o.nbnd * (m - 1)]) continue;
+        double xli[3];
+        int iii[3];
+        for (int n = 1; n <= 3; ++n) {
+            xli[n - 1] = o.XC(m, n) + o.BND(n, l) * ri;
+            iii[n - 1] = cell_of(xli[n - 1]);
+        }
+        int pct = iii[0];
+        double xlt = xli[0];
+        if (!(1 <= pct && pct <= o.nx)) {
+            if (iii[0] < 1) { pct = o.mxf + iii[0] - 1; xlt = o.mxf + xli[0] - 1; }
+            else if (iii[0] >= o.mxf) { pct = iii[0] - (o.mxf - 1); xlt = xli[0] - (o.mxf - 1); }
+        }
+        const int nev = pct == o.nx ? 2 : 1;
+        for (int ev = 1; ev <= nev; ++ev) {
+            if (ev == 1) { iii[0] = pct; xli[0] = xlt; }
+            else if (iii[0] >= o.mxf - 1) { iii[0] = iii[0] - (o.mxf - 1); xli[0] = xli[0] - (o.mxf - 1); }
+            double xlo[3];
+            int io[3];
+            for (int n = 1; n <= 3; ++n) {
+                xlo[n - 1] = xli[n - 1] + o.BND(n, l) * (ro - ri);
+                io[n - 1] = cell_of(xlo[n - 1]);
+            }
+            RawSten so, si;
+            double philo, phili, nll = 0, onll = 0, dfll = 0, dum;
+            interp_phi(o, io, xlo, 0, so, philo, dum, dum, dum);
+            interp_phi(o, iii, xli, 1, si, phili, nll, onll, dfll);
+            philo = o.phisurf * (ro - ri) - philo * (rb - ri);
+            philo = philo / (ro - rb);
+            const double phil = o.cf * (-philo + phili);
+            double t = 0.0;
+            t = t + phil;
+            t = t - c3 * nll - c4 * onll;
+            t = t - (c2 + c1) * dfll;
+            t = t * da2 * drm * o.dx;
+            int count_fl = 0;
+            double force_fl = 0.0;
+            auto node = [&](int i, int j, int k, int &ii, int &jj, int &kk) {
+                ii = si.ib + i; jj = wrap_yz(si.jb + j, o.my); kk = wrap_yz(si.kb + k, o.mz);
+                if (ii < 0) ii = o.mxf + ii - 1;
+            };
+            for (int k = 0; k < 2; ++k)
+                for (int j = 0; j < 2; ++j)
+                    for (int i = 0; i < 2; ++i) {
+                        int ii, jj, kk;
+                        node(i, j, k, ii, jj, kk);
+                        if (o.FL(ii, jj, kk)) { count_fl += 1; force_fl = force_fl + si.w[i][j][k] * t / dx3; }
+                    }
+            const int count_so = 8 - count_fl;
+            const double force_dist = force_fl / (double)count_so;
+            for (int k = 0; k < 2; ++k)
+                for (int j = 0; j < 2; ++j)
+                    for (int i = 0; i < 2; ++i) {
+                        int ii, jj, kk;
+                        node(i, j, k, ii, jj, kk);
+                        double &f = o.sfr[o.SF(ii, jj, kk)];
+                        if (o.prm.include_frmeanfluid) f = f + si.w[i][j][k] * t / dx3;
+                        else if (!o.FL(ii, jj, kk)) f = f + si.w[i][j][k] * t / dx3 + force_dist;
+                    }
+        }
+    }
+}
+
+// bcsetscal (SRC/SCALAR/bc_scalar.F90:65-383) after nlphi_graduphi's
+// transforms of the nonlinear terms (SRC/SCALAR/nlphi.F90:56-155).
+void bcsetscal(Orc &o) {
+    const int nx = o.nx;
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i <= nx + 1; ++i) {
+        c2r_with(o, [&](int j, int k) { return o.nlphif[o.CI(i, j, k, 1)]; }, [&](int j, int k, double v) { o.nlphir[o.RI(i, j, k, 1)] = v; });
+        c2r_with(o, [&](int j, int k) { return o.onlphif[o.CI(i, j, k, 1)]; }, [&](int j, int k, double v) { o.onlphir[o.RI(i, j, k, 1)] = v; });
+    }
+    std::fill(o.sfr.begin(), o.sfr.end(), 0.0);
+    calc_diffn_scal(o);
+    o.flux_global = 0.0;
+    for (int m = 1; m <= o.nbody; ++m) {
+        const double da1 = 4.0 * PI * ((o.radbdy[m - 1] * o.dx) * (o.radbdy[m - 1] * o.dx)) / (double)o.nbnd;
+        const double da2 = 4.0 * PI * ((o.radibdy[m - 1] * o.dx) * (o.radibdy[m - 1] * o.dx)) / (double)o.nrpr_active[m - 1];
+        o.flux_body[m - 1] = scal_surface_flux(o, m);
+        if (o.prm.dorpr) scal_inner_forcing(o, m, da2);
+        o.flux_global = o.flux_global + o.flux_body[m - 1] * da1;
+    }
+    o.nusselt = -(o.flux_global * o.char_length * o.char_length) / (6.0 * o.voldom * o.maxvolfrac * (o.phisurf - o.phistream));
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i <= nx; ++i)
+        r2c_with(o, [&](int j, int k) { return o.sfr[o.SF(i, j, k)]; }, [&](int j, int k, cplx v) { o.ffphi[o.CI(i, j, k, 1)] = v; });
+}
+
+// phistep: SRC/SCALAR/stepthescalar.F90:99-213 (serial branch): per (ky,kz)
+// line a cyclic Crank-Nicolson solve whose corners carry heat_ratio_new,
+// by Thomas (tridag3) + Sherman-Morrison.
+bool phistep(Orc &o) {
+    const int nx = o.nx, my2 = o.my2, mz = o.mz;
+    const double dt = o.dt, g = o.gamma_s, dx2 = o.dx2;
+    const double c1 = o.coef[0], c2 = o.coef[1], c3 = o.coef[2], c4 = o.coef[3];
+    const double hn = o.heat_ratio_new, h = o.heat_ratio;
+    bool ok = true;
+#pragma omp parallel reduction(&& : ok)
+    {
+        std::vector<double> a(nx), b(nx), c(nx), tr(nx), ti(nx), ur(nx), ui(nx), auxu(nx), auxv(nx), auxz(nx), gam(nx + 1);
+        std::vector<cplx> r1(nx);
+#pragma omp for schedule(static)
+        for (int k = 1; k <= mz; ++k)
+            for (int j = 1; j <= my2; ++j) {
+                auto PF = [&](int i) { return o.phif[o.CI(i, j, k, 1)]; };
+                const double alpha = hn, beta = 1.0 / hn, w2 = o.W2(j, k);
+                for (int i = 1; i <= nx; ++i) {
+                    a[i - 1] = -(dt * g * c2 / dx2);
+                    b[i - 1] = 1.0 + dt * g * c2 * (2.0 / dx2 + w2);
+                    c[i - 1] = -(dt * g * c2 / dx2);
+                    auxu[i - 1] = 0.0; auxv[i - 1] = 0.0; auxz[i - 1] = 0.0;
+                    cplx r = PF(i) * (1.0 - dt * c1 * g * w2);
+                    r = r + dt * c3 * o.nlphif[o.CI(i, j, k, 1)] + dt * o.ffphi[o.CI(i, j, k, 1)];
+                    r = r + dt * c4 * o.onlphif[o.CI(i, j, k, 1)];
+                    r1[i - 1] = r;
+                }
+                a[0] = a[0] * hn;
+                c[nx - 1] = c[nx - 1] / hn;
+                for (int i = 2; i <= nx; ++i)
+                    r1[i - 1] = r1[i - 1] + dt * g * c1 * (PF(i - 1) + PF(i + 1) - 2.0 * PF(i)) / dx2;
+                r1[0] = r1[0] + dt * g * c1 * (PF(2) - 2.0 * PF(1) + PF(nx) * h) / dx2;
+                for (int i = 0; i < nx; ++i) { tr[i] = r1[i].real(); ti[i] = r1[i].imag(); }
+                auxu[0] = alpha;
+                auxu[nx - 1] = beta;
+                auxv[0] = c[nx - 1] / auxu[nx - 1];
+                auxv[nx - 1] = a[0] / auxu[0];
+                b[0] = b[0] - auxu[0] * auxv[0];
+                b[nx - 1] = b[nx - 1] - auxu[nx - 1] * auxv[nx - 1];
+                if (!tridag3(a.data(), b.data(), c.data(), tr.data(), auxu.data(), ti.data(), ur.data(), auxz.data(), ui.data(), nx, gam.data())) {
+                    ok = false;
+                    continue;
+                }
+                const double vdotz = auxv[0] * auxz[0] + auxv[nx - 1] * auxz[nx - 1];
+                const double vdotyr = auxv[0] * ur[0] + auxv[nx - 1] * ur[nx - 1];
+                const double vdotyi = auxv[0] * ui[0] + auxv[nx - 1] * ui[nx - 1];
+                for (int i = 1; i <= nx; ++i)
+                    o.phif[o.CI(i, j, k, 1)] = cplx(ur[i - 1] - vdotyr * auxz[i - 1] / (1.0 + vdotz),
+                                                    ui[i - 1] - vdotyi * auxz[i - 1] / (1.0 + vdotz));
+                o.phif[o.CI(nx + 1, j, k, 1)] = o.phif[o.CI(1, j, k, 1)] / hn;
+            }
+    }
+    return ok;
+}
+
+// scalstep: SRC/SCALAR/stepthescalar.F90:51-94 (one species).
+int scalstep(Orc &o) {
+    std::swap(o.onlphif, o.nlphif);
+    std::fill(o.nlphif.begin(), o.nlphif.end(), cplx(0.0, 0.0));
+    form_nlphi(o);
+    bcsetscal(o);
+    if (!phistep(o)) return PIBM_ERR_PIVOT;
+    o.heat_ratio_old = o.heat_ratio;
+    o.heat_ratio = o.heat_ratio_new;
+    return PIBM_OK;
+}
+
 int step(Orc &o, pibm_step_report *rep) {
     const int rks = 1;
     compute_new_timestep(o, rks);
     int rc = nonlinear(o, rks);
     if (rc) return rc;
     rc = velstep(o, rks);
+    if (!rc && o.scal) rc = scalstep(o);
     if (rep) {
         std::memset(rep, 0, sizeof(*rep));
         rep->dt = o.dt; rep->t = o.t; rep->cf = o.cf; rep->umax = o.umax_last; rep->divmax = o.divmax;
@@ -1178,6 +1615,8 @@ int step(Orc &o, pibm_step_report *rep) {
         rep->mixmeanslipmod = o.mixmeanslipmod;
         long long s = 0; for (int v : o.nrpr_active) s += v;
         rep->nrpr_active_total = s;
+        rep->heat_ratio = o.heat_ratio;
+        rep->nusselt = o.nusselt;
     }
     for (const cplx &v : o.u) if (!std::isfinite(v.real()) || !std::isfinite(v.imag())) return PIBM_ERR_NAN;
     return rc;
@@ -1318,6 +1757,17 @@ int orc_cyclic_solve(int n, const double *a, const double *b, const double *c, c
 }
 
 }  // extern "C"
+
+// Passive scalar state: phif complex (nx+1,my2,mz) interleaved, flux_body (nbody),
+// ratios[0..2] = heat_ratio, heat_ratio_old, nusselt.  Any pointer may be NULL.
+extern "C" int orc_get_scalar(void *h, double *phif, double *flux_body, double *ratios) {
+    Orc &o = *(Orc *)h;
+    if (!o.scal) return PIBM_ERR_ARG;
+    if (phif) std::memcpy((void *)phif, o.phif.data(), o.phif.size() * sizeof(cplx));
+    if (flux_body) for (int m = 0; m < o.nbody; ++m) flux_body[m] = o.flux_body[m];
+    if (ratios) { ratios[0] = o.heat_ratio; ratios[1] = o.heat_ratio_old; ratios[2] = o.nusselt; }
+    return PIBM_OK;
+}
 
 // sizes of the ABI structs as compiled from include/pibm.h (for the ctypes mirror test)
 extern "C" int orc_sizeof(int which) {

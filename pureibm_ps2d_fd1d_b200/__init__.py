@@ -157,6 +157,18 @@ class Solver:
         _check(load_library().pibm_get_particles(self.h, *[_dp(a) for a in out]))
         return [a.reshape(3, n).T.copy() for a in out]
 
+    def get_scalar(self) -> dict:
+        """Passive scalar: phif complex (mz, my2, nx+1) (the reference's
+        (nx+1,my2,mz) array in C order), per-sphere surface flux, heat_ratio,
+        heat_ratio_old and the Nusselt number."""
+        nx, my2, mz = self.nx, self.my2, self.mz
+        phif = np.zeros((mz, my2, nx + 1), dtype=np.complex128)
+        flux = np.zeros(max(self.nbody, 1))
+        ratios = np.zeros(3)
+        _check(load_library().pibm_get_scalar(self.h, phif.ctypes.data_as(C.POINTER(C.c_double)), _dp(flux), _dp(ratios)))
+        return dict(phif=phif, flux_body=flux[:self.nbody], heat_ratio=ratios[0], heat_ratio_old=ratios[1],
+                    nusselt=ratios[2])
+
     def get_if_rev(self) -> np.ndarray:
         out = np.zeros(self.nbnd * self.nbody, dtype=np.uint8)
         _check(load_library().pibm_get_if_rev(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8))))

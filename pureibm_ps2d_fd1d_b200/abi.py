@@ -32,8 +32,8 @@ PIBM_SCHEME_CENTER = 0
 PIBM_SCHEME_UPWIND = 1
 PIBM_LIMITER_NONE = 0
 PIBM_LIMITER_MINMOD = 1
-PIBM_NPHASE = 6
-PHASE_NAMES = ["a0_fields_to_real", "nonlinear", "drag_mpg", "reversal_spread", "forcing_fft", "x_lines"]
+PIBM_NPHASE = 7
+PHASE_NAMES = ["a0_fields_to_real", "nonlinear", "drag_mpg", "reversal_spread", "forcing_fft", "x_lines", "scalar"]
 
 _i32 = C.c_int32
 _f64 = C.c_double
@@ -78,6 +78,7 @@ class pibm_step_report(C.Structure):
         ("pres_drag", _f64), ("visc_drag", _f64), ("total_drag", _f64),
         ("mixmeanslipmod", _f64),
         ("nrpr_active_total", C.c_int64),
+        ("heat_ratio", _f64), ("nusselt", _f64),
     ]
 
     def as_dict(self):
@@ -100,7 +101,8 @@ class pibm_info(C.Structure):
 # Exported symbols of libpibm (declared in include/pibm.h).
 EXPORTED = [
     "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run",
-    "pibm_run_profiled", "pibm_get_state", "pibm_get_particles", "pibm_get_if_rev", "pibm_get_fluid_mask",
+    "pibm_run_profiled", "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev",
+    "pibm_get_fluid_mask",
     "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
     "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time", "pibm_batch_member",
     "pibm_batch_destroy",
@@ -119,6 +121,7 @@ def bind(lib):
     lib.pibm_get_state.argtypes = [vp, P(pibm_state_view)]
     lib.pibm_run_profiled.argtypes = [vp, C.c_int, P(pibm_step_report), P(_f64), P(_f64), C.c_int]
     lib.pibm_get_particles.argtypes = [vp] + [P(_f64)] * 5
+    lib.pibm_get_scalar.argtypes = [vp, P(_f64), P(_f64), P(_f64)]
     lib.pibm_get_if_rev.argtypes = [vp, P(C.c_uint8)]
     lib.pibm_get_fluid_mask.argtypes = [vp, P(C.c_uint8)]
     lib.pibm_destroy.argtypes = [vp]
@@ -136,7 +139,7 @@ def bind(lib):
     lib.pibm_batch_destroy.argtypes = [vp]
     lib.pibm_batch_destroy.restype = None
     for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_profiled",
-                 "pibm_get_state", "pibm_get_particles", "pibm_get_if_rev", "pibm_get_fluid_mask",
+                 "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev", "pibm_get_fluid_mask",
                  "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
         getattr(lib, name).restype = C.c_int
     return lib

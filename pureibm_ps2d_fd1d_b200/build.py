@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libpibm.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels.cu", "api.cu"]
+CU_SOURCES = ["kernels.cu", "scalar.cu", "api.cu"]
 CPP_SOURCES = ["host_setup.cpp"]
 
 

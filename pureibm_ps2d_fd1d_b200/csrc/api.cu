@@ -29,6 +29,9 @@ void enqueue_f2d(const double2 *f, double2 *d, int nx, int nxf, int PS, int ncom
 void enqueue_d2f(const double2 *d, double2 *f, int nx, int nxf, int PS, int ncomp, cudaStream_t s);
 int real_offset(int n, int z, int y);
 int plane_ctas(int n);
+void enqueue_scalar(const Geo &g, DevBufs &b, int cur, cudaStream_t s);
+int scalar_kernels_per_step(const Geo &g);
+cudaError_t configure_scalar_kernels(int n);
 }  // namespace pibm
 
 using namespace pibm;
@@ -170,10 +173,42 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
               guard(h->alloc(&b.blockpart, 6 * (size_t)((g.npts + 255) / 256 + 1)), "blockpart") &&
               guard(h->alloc(&b.sc, 1), "scalars");
     if (!ok) { delete h; return rc; }
+    if (S.scal) {
+        // passive scalar: geometry of the reversal-point evaluations, the
+        // spreading map in plane-transform order, and phi = 1 (scalar_init.F90:136-152)
+        g.scal = 1; g.gamma_s = S.gamma_s; g.phisurf = S.phisurf; g.phistream = S.phistream;
+        g.nsev = (int)S.sev_m.size();
+        g.ssp_nnodes = (int)S.ssp_node.size();
+        std::vector<int> ssp_node_p(S.ssp_node.size());
+        for (size_t q = 0; q < S.ssp_node.size(); ++q) {
+            const int node = S.ssp_node[q], i = node / nat, e = node - i * nat;
+            ssp_node_p[q] = i * g.RS + roff[e];
+        }
+        std::vector<double2> phi0(NC, make_double2(0.0, 0.0));
+        for (int i = 0; i < g.nx; ++i) phi0[(size_t)i * g.PS] = make_double2(1.0, 0.0);
+        const size_t NR1 = (size_t)(g.nx + 1) * g.RS, nsev = (size_t)g.nsev;
+        ok = guard(h->upload(&g.sev_m, S.sev_m), "sev_m") && guard(h->upload(&g.sev_l, S.sev_l), "sev_l") &&
+             guard(h->upload(&g.sev_c, S.sev_c), "sev_c") && guard(h->upload(&g.sev_x, S.sev_x), "sev_x") &&
+             guard(h->upload(&g.ssp_node, ssp_node_p), "ssp_node") && guard(h->upload(&g.ssp_ptr, S.ssp_ptr), "ssp_ptr") &&
+             guard(h->upload(&g.ssp_ent, S.ssp_ent), "ssp_ent") &&
+             guard(h->alloc(&b.phif, NC), "phif") && guard(h->alloc(&b.nls[0], NC), "nls0") &&
+             guard(h->alloc(&b.nls[1], NC), "nls1") && guard(h->alloc(&b.ffs, NC), "ffs") &&
+             guard(h->alloc(&b.phr, NR), "phr") && guard(h->alloc(&b.phimg, (size_t)g.RS), "phimg") &&
+             guard(h->alloc(&b.nlr[0], NR1), "nlr0") && guard(h->alloc(&b.nlr[1], NR1), "nlr1") &&
+             guard(h->alloc(&b.sdf, NR1), "sdf") && guard(h->alloc(&b.gph, 3 * NR1), "gph") &&
+             guard(h->alloc(&b.sfr, NR), "sfr") && guard(h->alloc(&b.dsx, NR), "dsx") &&
+             guard(h->alloc(&b.spart, 8 * 3), "spart") && guard(h->alloc(&b.sctb, 8 * nsev), "sctb") &&
+             guard(h->alloc(&b.sfd, nsev), "sfd") && guard(h->alloc(&b.sdpart, 8 * (size_t)S.nbody), "sdpart") &&
+             guard(h->alloc(&b.flux_body, (size_t)S.nbody), "flux_body") &&
+             guard(cudaMemcpy(b.phif, phi0.data(), NC * sizeof(double2), cudaMemcpyHostToDevice), "phi0") &&
+             guard(configure_scalar_kernels(S.my), "configure_scalar_kernels");
+        if (!ok) { delete h; return rc; }
+    }
     Scal sc;
     std::memset(&sc, 0, sizeof(sc));
     for (int d = 0; d < 3; ++d) { sc.umean[d] = S.umean0[d]; sc.mpg[d] = prm->mpg[d]; }
     sc.dt = S.dt; sc.cf = S.cf; sc.cforig = S.cf; sc.t = 0.0; sc.fold = 0.0; sc.ferror = 1.0;
+    sc.heat_ratio = sc.heat_ratio_old = sc.heat_ratio_new = 1.0;
     if (!guard(cudaMemcpy(b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice), "scalars")) { delete h; return rc; }
     *out = h;
     return PIBM_OK;
@@ -207,6 +242,8 @@ static int fill_report(pibm_handle *h, pibm_step_report *rep) {
         rep->norm_drag = sc.norm_drag; rep->ferror = sc.ferror;
         rep->pres_drag = sc.pres_drag; rep->visc_drag = sc.visc_drag; rep->total_drag = sc.total_drag;
         rep->mixmeanslipmod = sc.mixmeanslipmod;
+        rep->heat_ratio = sc.heat_ratio;
+        rep->nusselt = sc.nusselt;
         long long s = 0;
         for (int v : h->S.nrpr_active) s += v;
         rep->nrpr_active_total = s;
@@ -339,6 +376,38 @@ int pibm_get_particles(pibm_handle *h, double *pres, double *visc, double *force
     CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
     if (xc) std::memcpy(xc, h->S.xc.data(), n * sizeof(double));
     if (vel) std::memcpy(vel, h->S.vel.data(), n * sizeof(double));
+    return PIBM_OK;
+}
+
+int pibm_get_scalar(pibm_handle *h, double *phif, double *flux_body, double *ratios) {
+    if (!h) return fail(PIBM_ERR_ARG, "null handle");
+    if (!h->g.scal) return fail(PIBM_ERR_ARG, "this run has no scalar (ISCALON = 0)");
+    const Geo &g = h->g;
+    Scal sc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<double2> dev((size_t)g.nx * g.PS);
+    if (phif) CUDA_OR_FAIL(cudaMemcpyAsync(dev.data(), h->b.phif, dev.size() * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<double> fb((size_t)g.nbody);
+    if (flux_body && g.nbody) CUDA_OR_FAIL(cudaMemcpyAsync(fb.data(), h->b.flux_body, fb.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    if (phif) {
+        // reference layout phif(nx+1, my2, mz), x fastest; plane nx+1 = phif(1)/heat_ratio
+        const size_t nxf = (size_t)g.nx + 1;
+        for (int k = 0; k < g.mz; ++k)
+            for (int j = 0; j < g.my2; ++j) {
+                const size_t e = (size_t)k * g.my2 + j;
+                for (int i = 0; i < g.nx; ++i) {
+                    const double2 v = dev[(size_t)i * g.PS + e];
+                    phif[2 * (i + nxf * e)] = v.x;
+                    phif[2 * (i + nxf * e) + 1] = v.y;
+                }
+                const double2 v = dev[e];
+                phif[2 * (g.nx + nxf * e)] = v.x / sc.heat_ratio;
+                phif[2 * (g.nx + nxf * e) + 1] = v.y / sc.heat_ratio;
+            }
+    }
+    if (flux_body) for (int m = 0; m < g.nbody; ++m) flux_body[m] = fb[m];
+    if (ratios) { ratios[0] = sc.heat_ratio; ratios[1] = sc.heat_ratio_old; ratios[2] = sc.nusselt; }
     return PIBM_OK;
 }
 

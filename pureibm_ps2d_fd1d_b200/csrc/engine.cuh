@@ -31,6 +31,14 @@ struct Geo {
     const double *da2;          // per sphere
     const int *sp_node, *sp_ptr, *sp_ent;   // spreading map
     int sp_nnodes;
+    // passive scalar (iscalon)
+    int scal;
+    double gamma_s, phisurf, phistream;
+    int nsev;                        // scalar reversal-point evaluations
+    const int *sev_m, *sev_l, *sev_c;
+    const double *sev_x;
+    const int *ssp_node, *ssp_ptr, *ssp_ent;
+    int ssp_nnodes;
 };
 
 // Evolving scalars of a run (one struct in device memory).
@@ -45,6 +53,8 @@ struct Scal {
     int status;
     int pad;
     long long nsteps;
+    // passive scalar: phi(x + Lx) = phi(x) / heat_ratio
+    double heat_ratio, heat_ratio_old, heat_ratio_new, flux_global, nusselt;
 };
 
 // Device buffers of one run.
@@ -53,6 +63,13 @@ struct DevBufs {
     double *ubcp, *pbcp, *Q, *omega, *pgr, *fr, *Dx;
     double *part, *pres, *visc, *ptot, *force, *rec, *ctb, *dpart, *blockpart;
     Scal *sc;
+    // passive scalar: spectral phi, nlphi (two steps), ffphi over planes 1..nx;
+    // real phi (planes 1..nx) and its c2r image plane nx+1; real nlphi of
+    // the two steps, diffusion and gradient over planes 1..nx+1; forcing and
+    // x-flux difference over planes 1..nx
+    double2 *phif, *nls[2], *ffs;
+    double *phr, *phimg, *nlr[2], *sdf, *gph, *sfr, *dsx;
+    double *spart, *sctb, *sfd, *sdpart, *flux_body;
 };
 
 }  // namespace pibm

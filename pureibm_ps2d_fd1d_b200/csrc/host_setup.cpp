@@ -229,13 +229,68 @@ void build_spread_map(RunSetup &S, bool all_nodes) {
 
 }  // namespace
 
+// Scalar reversal-point evaluations and their spreading map
+// (calc_inner_rev_data, SRC/SCALAR/bc_scalar.F90:558-932, serial branch):
+// inner point x = xc + bnd*radibdy, its cell wrapped into 1..nx with
+// WEST/EAST_PERIODIC_IMAGE (ibm.h:148-149); a point in cell nx is evaluated
+// again shifted by -nx (EAST_PERIODIC_IMAGE_MOD, ibm.h:150).  Stencil corners
+// below plane 0 wrap by mxf-1; corners on planes 0 and nx+1 are never
+// transformed (ff2rc runs over planes 1..nx), so the map leaves them out.
+void build_scalar_evals(RunSetup &S, bool all_nodes) {
+    const int N = S.nbody, nb = S.nbnd, nx = S.nx, my = S.my, mz = S.mz, mxf = S.mxf;
+    S.sev_m.clear(); S.sev_l.clear(); S.sev_c.clear(); S.sev_x.clear();
+    std::vector<std::pair<long long, int>> ent;
+    for (int m = 0; m < N; ++m)
+        for (int l = 0; l < nb; ++l) {
+            if (!S.if_rev[(size_t)l + (size_t)nb * m]) continue;
+            double x[3];
+            int c[3];
+            for (int d = 0; d < 3; ++d) {
+                x[d] = S.xc[m + (size_t)d * N] + S.bnd[3 * l + d] * S.radibdy;
+                c[d] = cell_index(x[d]);
+            }
+            int pct = c[0];
+            double xlt = x[0];
+            if (!(1 <= pct && pct <= nx)) {
+                if (c[0] < 1) { pct = mxf + c[0] - 1; xlt = mxf + x[0] - 1; }
+                else if (c[0] >= mxf) { pct = c[0] - (mxf - 1); xlt = x[0] - (mxf - 1); }
+            }
+            const int nev = pct == nx ? 2 : 1;
+            for (int ev = 1; ev <= nev; ++ev) {
+                if (ev == 1) { c[0] = pct; x[0] = xlt; }
+                else if (c[0] >= mxf - 1) { c[0] = c[0] - (mxf - 1); x[0] = x[0] - (mxf - 1); }
+                const int e = (int)S.sev_m.size();
+                S.sev_m.push_back(m); S.sev_l.push_back(l);
+                for (int d = 0; d < 3; ++d) { S.sev_x.push_back(x[d]); S.sev_c.push_back(c[d]); }
+                for (int ck = 0; ck < 2; ++ck)
+                    for (int cj = 0; cj < 2; ++cj)
+                        for (int ci = 0; ci < 2; ++ci) {
+                            int i = c[0] + ci, j = c[1] + cj, k = c[2] + ck;
+                            if (i < 0) i = mxf + i - 1;
+                            if (i < 1 || i > nx) continue;
+                            j = j < 1 ? j + my : (j > my ? j - my : j);
+                            k = k < 1 ? k + mz : (k > mz ? k - mz : k);
+                            const long long node = (long long)(i - 1) * my * mz + (long long)(k - 1) * my + (j - 1);
+                            if (!all_nodes && S.fluid[(size_t)node]) continue;
+                            ent.push_back({node, e * 8 + ci + 2 * cj + 4 * ck});
+                        }
+            }
+        }
+    std::stable_sort(ent.begin(), ent.end(), [](const std::pair<long long, int> &a, const std::pair<long long, int> &b) { return a.first < b.first; });
+    S.ssp_node.clear(); S.ssp_ptr.clear(); S.ssp_ent.clear();
+    for (size_t q = 0; q < ent.size(); ++q) {
+        if (q == 0 || ent[q].first != ent[q - 1].first) { S.ssp_node.push_back((int)ent[q].first); S.ssp_ptr.push_back((int)q); }
+        S.ssp_ent.push_back(ent[q].second);
+    }
+    S.ssp_ptr.push_back((int)ent.size());
+}
+
 bool setup_run(const pibm_params &prm, const pibm_particles *parts, RunSetup &S, std::string &err) {
     if (prm.my < 4 || (prm.my % 2) != 0) { err = "MY must be an even integer >= 4"; return false; }
     const int mz = prm.mz > 0 ? prm.mz : prm.my;
     if (mz != prm.my) { err = "only MZ == MY is supported"; return false; }
     if (prm.discr_scheme != PIBM_SCHEME_UPWIND && prm.discr_scheme != PIBM_SCHEME_CENTER) { err = "bad discr_scheme"; return false; }
     if (prm.imove != 0) { err = "moving particles (IMOVE=1) are not supported by this build"; return false; }
-    if (prm.iscalon != 0) { err = "the passive scalar (ISCALON=1) is not supported by this build"; return false; }
     S.my = prm.my; S.mz = mz; S.mx = S.my + 1; S.mxf = S.mx; S.nx = S.mx - 1; S.my2 = S.my / 2 + 1;
     S.nbody = parts ? parts->nbody : 0;
     if (S.nbody < 0 || (S.nbody > 0 && !parts->xc)) { err = "bad particle list"; return false; }
@@ -279,7 +334,18 @@ bool setup_run(const pibm_params &prm, const pibm_particles *parts, RunSetup &S,
     build_neighbours(S);
     build_if_rev(S);
     build_spread_map(S, prm.include_frmeanfluid != 0);
-    S.dt = prm.cfl * std::min(std::min(dt_conv, dt_vis), kLarge);
+    double dt_diff = kLarge;
+    if (prm.iscalon) {
+        // initscal: SRC/SCALAR/scalar_init.F90:58-122
+        if (!(prm.pr_or_sc_nu > 0.0)) { err = "PR_OR_SC_NU must be positive"; return false; }
+        S.scal = true;
+        S.gamma_s = S.vis / prm.pr_or_sc_nu;
+        S.phisurf = prm.phisurf;
+        S.phistream = prm.phistream;
+        dt_diff = (S.dx * S.dx * (1.0 - S.maxvolfrac)) / S.gamma_s;
+        build_scalar_evals(S, prm.include_frmeanfluid != 0);
+    }
+    S.dt = prm.cfl * std::min(std::min(dt_conv, dt_vis), std::min(kLarge, dt_diff));
     S.dt = std::min(S.dt, kLarge);
     S.cf = -1.0 / S.dt;
     S.ramp_frac_time = prm.ramp_frac_steps * S.ucharmod * S.dt / ((double)(float)(S.mx - 1) * S.dx);

@@ -37,6 +37,16 @@ struct RunSetup {
     // spreading map: nodes (device layout linear index i*my*mz + k*my + j), CSR rows of
     // (point index * 8 + corner) in ascending point order
     std::vector<int> sp_node, sp_ptr, sp_ent;
+    // passive scalar (iscalon): diffusivity, surface and stream values, and the
+    // reversal-point evaluations of calc_inner_rev_data: each active point once,
+    // a second time one period west when its cell is the last one; positions
+    // (after the x wrap) and cells per evaluation, and the spreading map of
+    // (evaluation * 8 + corner) per node of planes 1..nx in reference order
+    bool scal = false;
+    double gamma_s = 0, phisurf = 0, phistream = 0;
+    std::vector<int> sev_m, sev_l, sev_c;     // sev_c: 3 cells per evaluation
+    std::vector<double> sev_x;                // 3 coordinates per evaluation
+    std::vector<int> ssp_node, ssp_ptr, ssp_ent;
 };
 
 bool setup_run(const pibm_params &prm, const pibm_particles *parts, RunSetup &S, std::string &err);
