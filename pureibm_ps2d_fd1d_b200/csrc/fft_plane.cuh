@@ -42,15 +42,33 @@ template <int L> __device__ __forceinline__ int bitrev(int l) {
 }
 
 // Twiddle lookup: w_N^m with sign s (table holds e^{-2 pi i m / N}; s>0 takes the conjugate).
+// st holds the twiddles of the cross-lane stages contiguously, st[h-1+q] =
+// w_{2h}^q (h = 1, 2, ..., L/2): lanes of one stage read consecutive entries,
+// so the reads are free of shared-memory bank conflicts.
 struct Tw {
     const double2 *t;   // table of e^{-2 pi i m/(N*stride)}
     int N;              // transform length this view describes
     int stride;         // table step: w_N^m = t[m*stride]
+    const double2 *st;  // stage table (see above)
     __device__ __forceinline__ double2 get(int m, double s) const {
         double2 w = t[m * stride];
         return s > 0 ? make_double2(w.x, -w.y) : w;
     }
+    __device__ __forceinline__ double2 stage(int h, int q, double s) const {
+        double2 w = st[h - 1 + q];
+        return s > 0 ? make_double2(w.x, -w.y) : w;
+    }
 };
+// Fill a stage table for L lanes from a table of N = L*R entries (block-wide, caller syncs).
+template <int L>
+__device__ __forceinline__ void fill_stage_table(double2 *st, const double2 *t, int N) {
+    for (int e = threadIdx.x; e < L - 1; e += blockDim.x) {
+        int h = 1;
+        while (h - 1 + h <= e) h <<= 1;   // e in [h-1, 2h-1)
+        const int q = e - (h - 1);
+        st[e] = t[q * (N / (2 * h))];
+    }
+}
 
 // In-lane R-point DFT (sign s) of v[0..R-1].
 template <int R> __device__ __forceinline__ void dft_inlane(double2 (&v)[R], double s, const Tw &tw);
@@ -101,119 +119,12 @@ __device__ __forceinline__ void group_fft(double2 (&v)[R], int l, double s, cons
     for (int h = L / 2; h >= 1; h >>= 1) {
         const bool upper = (l & h) == 0;
         const int q = l & (h - 1);
-        const double2 w = tw.get(q * (N / (2 * h)), s);
+        const double2 w = tw.stage(h, q, s);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             double2 pv = shfl_xor2(v[r], h, L);
             v[r] = upper ? cadd(v[r], pv) : cmul(csub(pv, v[r]), w);
         }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Plane transforms.  buf: mz rows x my2 complex slots (pitch my2).
-// twz: table for N=mz; twy: table for N=my (the y half-length transform uses
-// w_{my/2}^m = w_my^{2m}).  Called by all threads of the CTA; nwarps warps.
-// ---------------------------------------------------------------------------
-template <int RZ, int LZ>
-__device__ __forceinline__ void z_pass(double2 *buf, int my2, int mz, double s, const Tw &twz) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    constexpr int G = 32 / LZ;       // columns per warp
-    const int sub = lane / LZ, l = lane % LZ;
-    for (int j0 = warp * G; j0 < my2; j0 += nwarps * G) {
-        const int j = j0 + sub;
-        const bool act = j < my2;
-        double2 v[RZ];
-#pragma unroll
-        for (int r = 0; r < RZ; ++r) v[r] = act ? buf[(size_t)(l + LZ * r) * my2 + j] : make_double2(0.0, 0.0);
-        group_fft<RZ, LZ>(v, l, s, twz);
-        __syncwarp();
-        const int br = bitrev<LZ>(l);
-        if (act) {
-#pragma unroll
-            for (int r = 0; r < RZ; ++r) buf[(size_t)(r + RZ * br) * my2 + j] = v[r];
-        }
-        __syncwarp();
-    }
-}
-
-// y direction complex-to-real on every row: X[0..M] (M = my/2) -> x[0..my-1]
-// stored as complex pairs z[n] = x[2n] + i x[2n+1] in slots 0..M-1.
-template <int RY, int LY>
-__device__ __forceinline__ void y_c2r_pass(double2 *buf, int my2, int mz, const Tw &twy) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    constexpr int M = RY * LY;
-    constexpr int G = 32 / LY;
-    const int sub = lane / LY, l = lane % LY;
-    for (int k0 = warp * G; k0 < mz; k0 += nwarps * G) {
-        const int k = k0 + sub;
-        const bool act = k < mz;
-        double2 *row = buf + (size_t)(act ? k : 0) * my2;
-        double2 v[RY];
-#pragma unroll
-        for (int r = 0; r < RY; ++r) {
-            const int n = l + LY * r;
-            double2 xk = row[n], xm = row[M - n];
-            if (n == 0) { xk.y = 0.0; xm.y = 0.0; }     // ignore Im of ky=0 and ky=M
-            // Z[n] = (X[n] + conj X[M-n]) + i w+^n (X[n] - conj X[M-n]),  w+ = e^{+2 pi i/my}
-            double2 e = make_double2(xk.x + xm.x, xk.y - xm.y);
-            double2 d = make_double2(xk.x - xm.x, xk.y + xm.y);
-            double2 od = cmul(d, twy.get(n, +1.0));
-            v[r] = make_double2(e.x - od.y, e.y + od.x);
-        }
-        __syncwarp();
-        group_fft<RY, LY>(v, l, +1.0, Tw{twy.t, M, 2 * twy.stride});   // w_M^m = w_my^{2m}
-        const int br = bitrev<LY>(l);
-        if (act) {
-#pragma unroll
-            for (int r = 0; r < RY; ++r) row[r + RY * br] = v[r];
-        }
-        __syncwarp();
-    }
-}
-
-// y direction real-to-complex on every row: x (as pairs in slots 0..M-1) -> X[0..M].
-template <int RY, int LY>
-__device__ __forceinline__ void y_r2c_pass(double2 *buf, int my2, int mz, const Tw &twy) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    constexpr int M = RY * LY;
-    constexpr int G = 32 / LY;
-    const int sub = lane / LY, l = lane % LY;
-    for (int k0 = warp * G; k0 < mz; k0 += nwarps * G) {
-        const int k = k0 + sub;
-        const bool act = k < mz;
-        double2 *row = buf + (size_t)(act ? k : 0) * my2;
-        double2 v[RY];
-#pragma unroll
-        for (int r = 0; r < RY; ++r) v[r] = row[l + LY * r];
-        group_fft<RY, LY>(v, l, -1.0, Tw{twy.t, M, 2 * twy.stride});
-        __syncwarp();
-        const int br = bitrev<LY>(l);
-        if (act) {
-#pragma unroll
-            for (int r = 0; r < RY; ++r) row[r + RY * br] = v[r];
-        }
-        __syncwarp();
-        // post-process X[n] = (Z[n] + conj Z[M-n])/2 + w-^n (Z[n] - conj Z[M-n])/(2i), n = 0..M
-        double2 out[RY];
-        double2 nyq = make_double2(0.0, 0.0);
-#pragma unroll
-        for (int r = 0; r < RY; ++r) {
-            const int n = l + LY * r;
-            double2 zk = row[n], zm = row[(M - n) % M];
-            double2 e = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
-            double2 o = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));   // (zk - conj zm)/(2i)
-            double2 wo = cmul(twy.get(n, -1.0), o);
-            out[r] = cadd(e, wo);
-            if (n == 0) nyq = make_double2(zk.x - zk.y, 0.0);
-        }
-        __syncwarp();
-        if (act) {
-#pragma unroll
-            for (int r = 0; r < RY; ++r) row[l + LY * r] = out[r];
-            if (l == 0) row[M] = nyq;
-        }
-        __syncwarp();
     }
 }
 

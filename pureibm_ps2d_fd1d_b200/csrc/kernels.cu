@@ -726,7 +726,7 @@ __device__ __forceinline__ void circulant_solve(double2 *row, double a, double b
     for (int h = 1; h < 32; h <<= 1) {
         const bool upper = (lane & h) == 0;
         const int q = lane & (h - 1);
-        const double2 w = tw.get(q * (N / (2 * h)), +1.0);
+        const double2 w = tw.stage(h, q, +1.0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const double2 pv = shfl_xor2(v[r], h, 32);
@@ -773,14 +773,16 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
     double2 *P = RHS + LT * NP;
     double2 *U = P + LT * NP;                 // [comp][line][i]
     double *gam = (double *)(U + 3 * LT * NP);
+    double2 *st = (double2 *)(gam + NX);      // cross-lane stage twiddles
     if (sc->status) return;
     for (int t = threadIdx.x; t < NX; t += blockDim.x) tws[t] = g.tw[t];
+    fill_stage_table<32>(st, g.tw, NX);
     const int PS = g.PS, nx = NX;
     const int q0 = blockIdx.x * LT;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const double dx = g.dx, dx2 = g.dx2, dt = sc->dt, vis = g.vis;
     const double c1 = g.c1, c2 = g.c2, c3 = g.c3, c4 = g.c4;
-    const Tw tw{tws, NX, 1};
+    const Tw tw{tws, NX, 1, st};
     auto KY = [&](int q) { return g.ky[q % g.my2]; };
     auto KZ = [&](int q) { return g.kz[q / g.my2]; };
     auto G = [&](const double2 *f, int comp, int i, int q) -> double2 {
@@ -955,7 +957,7 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
 
 template <int NX> struct LinesCfg { static constexpr int LT = NX >= 256 ? 4 : 8; };
 template <int NX>
-static size_t lines_smem() { return (size_t)(NX + 5 * LinesCfg<NX>::LT * (NX + 1)) * sizeof(double2) + NX * sizeof(double); }
+static size_t lines_smem() { return (size_t)(NX + 5 * LinesCfg<NX>::LT * (NX + 1) + 32) * sizeof(double2) + NX * sizeof(double); }
 
 // velstep tail: umean update (steptheflow.F90:99) and the NaN check.
 __global__ void k_scal_d(Geo g, Scal *sc) {

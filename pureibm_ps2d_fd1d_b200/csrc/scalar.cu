@@ -559,7 +559,7 @@ __device__ __forceinline__ void twisted_solve(double2 *row, double a, double b, 
     for (int h = 1; h < 32; h <<= 1) {
         const bool upper = (lane & h) == 0;
         const int q = lane & (h - 1);
-        const double2 w = tw.get(q * (N / (2 * h)), +1.0);
+        const double2 w = tw.stage(h, q, +1.0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const double2 pv = shfl_xor2(v[r], h, 32);
@@ -588,7 +588,9 @@ __global__ void __launch_bounds__(LT * 32) k_slines(Geo g, double2 *__restrict__
     double2 *RHS = tws + NX;                       // [line][i], pitch NP
     double *pw = (double *)(RHS + LT * NP);        // mu^(i+1)
     double *ipw = pw + NX;                         // mu^-(i+1)
+    double2 *st = (double2 *)(ipw + NX);           // cross-lane stage twiddles
     if (sc->status) return;
+    fill_stage_table<32>(st, g.tw, NX);
     const int PS = g.PS, nx = NX;
     const double h = sc->heat_ratio, H = sc->heat_ratio_new;
     for (int t = threadIdx.x; t < NX; t += blockDim.x) {
@@ -633,7 +635,7 @@ __global__ void __launch_bounds__(LT * 32) k_slines(Geo g, double2 *__restrict__
     if (qw < PS) {
         const double a = -(dt * gm * c2 / dx2);
         const double bd = 1.0 + dt * gm * c2 * (2.0 / dx2 + g.w2[qw]);
-        const Tw tw{tws, NX, 1};
+        const Tw tw{tws, NX, 1, st};
         twisted_solve<R>(RHS + w * NP, a, bd, mu + imu, mu - imu, pw, ipw, tw, lane);
     }
     __syncthreads();
@@ -645,7 +647,7 @@ __global__ void __launch_bounds__(LT * 32) k_slines(Geo g, double2 *__restrict__
 }
 template <int NX> struct SLinesCfg { static constexpr int LT = NX >= 256 ? 4 : 8; };
 template <int NX>
-static size_t slines_smem() { return (size_t)(NX + SLinesCfg<NX>::LT * (NX + 1)) * sizeof(double2) + 2 * NX * sizeof(double); }
+static size_t slines_smem() { return (size_t)(NX + SLinesCfg<NX>::LT * (NX + 1) + 32) * sizeof(double2) + 2 * NX * sizeof(double); }
 
 // heat_ratio update, surface flux and Nusselt number (bcsetscal, bc_scalar.F90:186-190,
 // 361-363; stepthescalar.F90:90-91), status.
