@@ -150,6 +150,9 @@ int  pibm_set_state(pibm_handle *h, const pibm_state_view *s);
 int  pibm_step(pibm_handle *h, int rks, pibm_step_report *rep);
 /* nsteps steps without per-step host synchronisation (graph-launched). */
 int  pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last);
+/* nsteps graph-launched steps (as pibm_run) timed with CUDA events recorded on
+ * the handle's stream around the launches: *total_ms = device time. */
+int  pibm_run_timed(pibm_handle *h, int nsteps, pibm_step_report *last, double *total_ms);
 /* nsteps steps launched without graphs, timed with CUDA events recorded on
  * the handle's stream: *total_ms = first-to-last event time; phase_ms[q]
  * (q < nphase <= PIBM_NPHASE) = summed duration of phase q over the steps.

@@ -100,7 +100,7 @@ class pibm_info(C.Structure):
 
 # Exported symbols of libpibm (declared in include/pibm.h).
 EXPORTED = [
-    "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run",
+    "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed",
     "pibm_run_profiled", "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev",
     "pibm_get_fluid_mask",
     "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
@@ -119,6 +119,7 @@ def bind(lib):
     lib.pibm_step.argtypes = [vp, C.c_int, P(pibm_step_report)]
     lib.pibm_run.argtypes = [vp, C.c_int, P(pibm_step_report)]
     lib.pibm_get_state.argtypes = [vp, P(pibm_state_view)]
+    lib.pibm_run_timed.argtypes = [vp, C.c_int, P(pibm_step_report), P(_f64)]
     lib.pibm_run_profiled.argtypes = [vp, C.c_int, P(pibm_step_report), P(_f64), P(_f64), C.c_int]
     lib.pibm_get_particles.argtypes = [vp] + [P(_f64)] * 5
     lib.pibm_get_scalar.argtypes = [vp, P(_f64), P(_f64), P(_f64)]
@@ -138,7 +139,7 @@ def bind(lib):
     lib.pibm_batch_member.restype = vp
     lib.pibm_batch_destroy.argtypes = [vp]
     lib.pibm_batch_destroy.restype = None
-    for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_profiled",
+    for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed", "pibm_run_profiled",
                  "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev", "pibm_get_fluid_mask",
                  "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
         getattr(lib, name).restype = C.c_int

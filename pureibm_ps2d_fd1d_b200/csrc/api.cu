@@ -21,7 +21,7 @@
 namespace pibm {
 cudaError_t configure_kernels(int n);
 bool supported_size(int n);
-void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev);
+void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss);
 int kernels_per_step(const Geo &g);
 void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s);
 void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s);
@@ -70,6 +70,8 @@ struct pibm_handle {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int cur = 0;          // buffer index the next step writes its nonlinear term to
     int device = 0;
+    double2 *stage = nullptr;   // reference-layout staging buffer of get/set_state (allocated once)
+    StepStreams ss;             // side streams of the forked step (graphs and pibm_step)
 
     template <class T> cudaError_t alloc(T **p, size_t n) {
         void *q = nullptr;
@@ -88,6 +90,9 @@ struct pibm_handle {
     ~pibm_handle() {
         for (auto &gx : graph) if (gx) cudaGraphExecDestroy(gx);
         if (stream) cudaStreamDestroy(stream);
+        if (ss.side) cudaStreamDestroy(ss.side);
+        if (ss.scal) cudaStreamDestroy(ss.scal);
+        for (cudaEvent_t e : {ss.fork, ss.drag_done, ss.scal_done}) if (e) cudaEventDestroy(e);
         for (void *q : allocs) cudaFree(q);
     }
 };
@@ -111,7 +116,12 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
         return true;
     };
     if (!guard(cudaGetDevice(&h->device), "cudaGetDevice") || !guard(configure_kernels(S.my), "configure_kernels") ||
-        !guard(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate")) { delete h; return rc; }
+        !guard(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate") ||
+        !guard(cudaStreamCreateWithFlags(&h->ss.side, cudaStreamNonBlocking), "cudaStreamCreate") ||
+        !guard(cudaStreamCreateWithFlags(&h->ss.scal, cudaStreamNonBlocking), "cudaStreamCreate") ||
+        !guard(cudaEventCreateWithFlags(&h->ss.fork, cudaEventDisableTiming), "cudaEventCreate") ||
+        !guard(cudaEventCreateWithFlags(&h->ss.drag_done, cudaEventDisableTiming), "cudaEventCreate") ||
+        !guard(cudaEventCreateWithFlags(&h->ss.scal_done, cudaEventDisableTiming), "cudaEventCreate")) { delete h; return rc; }
     Geo &g = h->g;
     std::memset(&g, 0, sizeof(g));
     g.nx = S.nx; g.my = S.my; g.mz = S.mz; g.my2 = S.my2;
@@ -255,7 +265,7 @@ static int fill_report(pibm_handle *h, pibm_step_report *rep) {
 int pibm_step(pibm_handle *h, int rks, pibm_step_report *rep) {
     if (!h) return fail(PIBM_ERR_ARG, "null handle");
     if (rks != 1) return fail(PIBM_ERR_ARG, "AB2 has a single sub-step (rks = 1)");
-    enqueue_step(h->g, h->b, h->cur, h->stream, nullptr);
+    enqueue_step(h->g, h->b, h->cur, h->stream, nullptr, &h->ss);
     CUDA_OR_FAIL(cudaGetLastError());
     h->cur ^= 1;
     return fill_report(h, rep);
@@ -267,7 +277,7 @@ int pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last) {
         if (h->graph[par]) continue;
         cudaGraph_t gr;
         CUDA_OR_FAIL(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_step(h->g, h->b, par, h->stream, nullptr);
+        enqueue_step(h->g, h->b, par, h->stream, nullptr, &h->ss);
         CUDA_OR_FAIL(cudaStreamEndCapture(h->stream, &gr));
         CUDA_OR_FAIL(cudaGraphInstantiate(&h->graph[par], gr, 0));
         cudaGraphDestroy(gr);
@@ -279,12 +289,34 @@ int pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last) {
     return fill_report(h, last);
 }
 
+int pibm_run_timed(pibm_handle *h, int nsteps, pibm_step_report *last, double *total_ms) {
+    if (!h || nsteps <= 0 || !total_ms) return fail(PIBM_ERR_ARG, "bad argument");
+    int rc = pibm_run(h, 0, nullptr);   // captures the step graphs on first use
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    CUDA_OR_FAIL(cudaEventCreate(&e0));
+    CUDA_OR_FAIL(cudaEventCreate(&e1));
+    CUDA_OR_FAIL(cudaEventRecord(e0, h->stream));
+    for (int s = 0; s < nsteps; ++s) {
+        CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], h->stream));
+        h->cur ^= 1;
+    }
+    CUDA_OR_FAIL(cudaEventRecord(e1, h->stream));
+    CUDA_OR_FAIL(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CUDA_OR_FAIL(cudaEventElapsedTime(&ms, e0, e1));
+    *total_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return fill_report(h, last);
+}
+
 int pibm_run_profiled(pibm_handle *h, int nsteps, pibm_step_report *last, double *total_ms, double *phase_ms, int nphase) {
     if (!h || nsteps <= 0 || nphase < 0 || nphase > PIBM_NPHASE) return fail(PIBM_ERR_ARG, "bad argument");
     std::vector<cudaEvent_t> ev((size_t)nsteps * (PIBM_NPHASE + 1));
     for (auto &e : ev) CUDA_OR_FAIL(cudaEventCreate(&e));
     for (int s = 0; s < nsteps; ++s) {
-        enqueue_step(h->g, h->b, h->cur, h->stream, &ev[(size_t)s * (PIBM_NPHASE + 1)]);
+        enqueue_step(h->g, h->b, h->cur, h->stream, &ev[(size_t)s * (PIBM_NPHASE + 1)], nullptr);
         h->cur ^= 1;
     }
     CUDA_OR_FAIL(cudaGetLastError());
@@ -310,8 +342,8 @@ int pibm_get_state(pibm_handle *h, pibm_state_view *s) {
     const Geo &g = h->g;
     const int nxf = g.nx + 1;
     const size_t nfu = (size_t)nxf * g.PS * 3, nfp = (size_t)g.nx * g.PS;
-    double2 *tmp = nullptr;
-    CUDA_OR_FAIL(cudaMallocAsync(&tmp, nfu * sizeof(double2), h->stream));
+    if (!h->stage) CUDA_OR_FAIL(h->alloc(&h->stage, nfu));
+    double2 *tmp = h->stage;
     const int prev = h->cur ^ 1;   // buffer holding the latest nl
     if (s->u) {
         enqueue_d2f(h->b.u, tmp, g.nx, nxf, g.PS, 3, h->stream);
@@ -327,7 +359,6 @@ int pibm_get_state(pibm_handle *h, pibm_state_view *s) {
     }
     Scal sc;
     CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
-    CUDA_OR_FAIL(cudaFreeAsync(tmp, h->stream));
     CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
     for (int d = 0; d < 3; ++d) { s->umean[d] = sc.umean[d]; s->mpg[d] = sc.mpg[d]; s->ufmean[d] = sc.ufmean[d]; }
     s->t = sc.t; s->dt = sc.dt; s->cf = sc.cf;
@@ -339,8 +370,8 @@ int pibm_set_state(pibm_handle *h, const pibm_state_view *s) {
     const Geo &g = h->g;
     const int nxf = g.nx + 1;
     const size_t nfu = (size_t)nxf * g.PS * 3, nfp = (size_t)g.nx * g.PS;
-    double2 *tmp = nullptr;
-    CUDA_OR_FAIL(cudaMallocAsync(&tmp, nfu * sizeof(double2), h->stream));
+    if (!h->stage) CUDA_OR_FAIL(h->alloc(&h->stage, nfu));
+    double2 *tmp = h->stage;
     const int prev = h->cur ^ 1;
     if (s->u) {
         CUDA_OR_FAIL(cudaMemcpyAsync(tmp, s->u, nfu * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
@@ -361,7 +392,6 @@ int pibm_set_state(pibm_handle *h, const pibm_state_view *s) {
     sc.t = s->t; sc.dt = s->dt; sc.cf = s->cf;
     sc.status = 0;
     CUDA_OR_FAIL(cudaMemcpyAsync(h->b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, h->stream));
-    CUDA_OR_FAIL(cudaFreeAsync(tmp, h->stream));
     CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
     return PIBM_OK;
 }
@@ -591,7 +621,7 @@ static int batch_graphs(pibm_batch *bt) {
         for (int q = 0; q < n; ++q) {
             pibm_handle *h = bt->members[q];
             CUDA_OR_FAIL(cudaStreamWaitEvent(h->stream, bt->fork, 0));
-            enqueue_step(h->g, h->b, bt->base[q] ^ par, h->stream, nullptr);
+            enqueue_step(h->g, h->b, bt->base[q] ^ par, h->stream, nullptr, &h->ss);
             CUDA_OR_FAIL(cudaEventRecord(bt->join[q], h->stream));
             CUDA_OR_FAIL(cudaStreamWaitEvent(bt->stream, bt->join[q], 0));
         }

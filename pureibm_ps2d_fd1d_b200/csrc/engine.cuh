@@ -72,4 +72,12 @@ struct DevBufs {
     double *spart, *sctb, *sfd, *sdpart, *flux_body;
 };
 
+// Side streams of one run: after compute_new_timestep's scalars are known,
+// the drag quadrature (and mpg) and the passive-scalar step depend only on
+// the real fields of that step, so they run beside the nonlinear term.
+struct StepStreams {
+    cudaStream_t side = nullptr, scal = nullptr;
+    cudaEvent_t fork = nullptr, drag_done = nullptr, scal_done = nullptr;
+};
+
 }  // namespace pibm

@@ -1114,20 +1114,41 @@ int real_offset(int n, int z, int y) {
 // Enqueue one full step on stream s.  cur = index of the nl buffer that
 // receives this step's nonlinear term (the other holds the previous step's).
 template <int N>
-static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev) {
+static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss) {
     const int old = 1 - cur;
     auto mark = [&](int q) { if (ev) cudaEventRecord(ev[q], s); };
+    // forked: drag + mpg on ss->side and the scalar step on ss->scal run beside the
+    // nonlinear term; the per-phase timed variant (ev) keeps one serial stream
+    const bool fork = ss && !ev;
     mark(0);
     launch_planes<N>(k_a0<N>, g.nx, 10, s, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
     k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
     mark(1);
+    if (fork) {
+        cudaEventRecord(ss->fork, s);
+        if (g.nbody > 0) {
+            cudaStreamWaitEvent(ss->side, ss->fork, 0);
+            k_drag<N><<<g.nbody * kDragSplit, 256, 0, ss->side>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
+            k_scal_b<<<1, 256, 0, ss->side>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
+            cudaEventRecord(ss->drag_done, ss->side);
+        }
+        if (g.scal) {
+            cudaStreamWaitEvent(ss->scal, ss->fork, 0);
+            enqueue_scalar(g, b, cur, ss->scal);
+            cudaEventRecord(ss->scal_done, ss->scal);
+        }
+    }
     k_flux<N><<<(RP<N>::RSP * (g.nx / 32) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
     launch_planes<N>(k_nl<N>, g.nx, 3, s, g, (const double *)b.ubcp, (const double *)b.Dx, (const double2 *)b.u,
                      (const double2 *)b.nl[old], b.nl[cur], b.Q, b.sc);
     mark(2);
     if (g.nbody > 0) {
-        k_drag<N><<<g.nbody * kDragSplit, 256, 0, s>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
-        k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
+        if (fork) {
+            cudaStreamWaitEvent(s, ss->drag_done, 0);
+        } else {
+            k_drag<N><<<g.nbody * kDragSplit, 256, 0, s>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
+            k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
+        }
         mark(3);
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {
@@ -1145,7 +1166,10 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
         g, b.u, b.p, b.nl[cur], b.nl[old], b.ff, b.sc);
     k_scal_d<<<1, 32, 0, s>>>(g, b.sc);
     mark(6);
-    if (g.scal) enqueue_scalar(g, b, cur, s);
+    if (g.scal) {
+        if (fork) cudaStreamWaitEvent(s, ss->scal_done, 0);
+        else enqueue_scalar(g, b, cur, s);
+    }
     mark(7);
 }
 
@@ -1156,13 +1180,13 @@ int kernels_per_step(const Geo &g) {
     return n + scalar_kernels_per_step(g);
 }
 
-void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev) {
+void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss) {
     switch (g.my) {
-        case 32: enqueue_step_t<32>(g, b, cur, s, ev); break;
-        case 64: enqueue_step_t<64>(g, b, cur, s, ev); break;
-        case 96: enqueue_step_t<96>(g, b, cur, s, ev); break;
-        case 128: enqueue_step_t<128>(g, b, cur, s, ev); break;
-        case 256: enqueue_step_t<256>(g, b, cur, s, ev); break;
+        case 32: enqueue_step_t<32>(g, b, cur, s, ev, ss); break;
+        case 64: enqueue_step_t<64>(g, b, cur, s, ev, ss); break;
+        case 96: enqueue_step_t<96>(g, b, cur, s, ev, ss); break;
+        case 128: enqueue_step_t<128>(g, b, cur, s, ev, ss); break;
+        case 256: enqueue_step_t<256>(g, b, cur, s, ev, ss); break;
     }
 }
 
