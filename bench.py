@@ -365,6 +365,7 @@ def run_gpu(args):
     }
     if not args.no_mis and world == 1:
         line["batched_mis"] = batched_mis()
+    if not args.no_scalar and world == 1:
         line["with_scalar"] = with_scalar()
     if not args.no_cpu_baseline and world == 1:
         cb = cpu_baseline(prm, xc, steps=2, warmup=1)
@@ -383,6 +384,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mis", action="store_true", help="skip the batched-realization measurement")
+    ap.add_argument("--no-scalar", action="store_true", help="skip the flow + passive-scalar measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

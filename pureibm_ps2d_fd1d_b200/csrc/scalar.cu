@@ -156,16 +156,20 @@ template <int N>
 __global__ void __launch_bounds__(256) k_sflux(Geo g, const double *__restrict__ ubcp, const double *__restrict__ phr,
                                                const double *__restrict__ phimg, double *__restrict__ dsx,
                                                const Scal *__restrict__ sc) {
-    constexpr int RSP = RP<N>::RSP;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= RSP || (e % (N + 2)) >= N || sc->status) return;
-    const int nx = g.nx;
+    // one thread per (y,z) node and segment of SEG planes
+    constexpr int RSP = RP<N>::RSP, SEG = 32;
+    const int nx = g.nx, nseg = (nx + SEG - 1) / SEG;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = t % RSP, sg = t / RSP;
+    if (sg >= nseg || (e % (N + 2)) >= N || sc->status) return;
+    const int i0 = sg * SEG + 1, i1 = min(nx, (sg + 1) * SEG);
     const double h = sc->heat_ratio, dx = g.dx, hdx = dx / 2.0, tdx = 2.0 * dx;
-    auto U = [&](int i) { return __ldg(ubcp + (size_t)((i - 1) % nx) * RSP + e); };          // i in 1..nx+1
-    auto PB = [&](int i) { return i <= nx ? __ldg(phr + (size_t)(i - 1) * RSP + e) : __ldg(phimg + e); };
+    auto U = [&](int i) { return __ldg(ubcp + (size_t)(i <= nx ? i - 1 : i - 1 - nx) * RSP + e); };   // i in 1..nx+2
+    auto PB = [&](int i) { return i <= nx ? __ldg(phr + (size_t)(i - 1) * RSP + e) : __ldg(phimg + e); };  // i in 1..nx+1
     if (g.scheme == PIBM_SCHEME_CENTER) {
-        double fm = (U(nx) * PB(nx)) * h, f0 = U(1) * PB(1);   // fdderiv(0), fdderiv(1)
-        for (int i = 1; i <= nx; ++i) {
+        double fm = i0 == 1 ? (U(nx) * PB(nx)) * h : U(i0 - 1) * PB(i0 - 1);   // fdderiv(i0-1), fdderiv(0) = fdderiv(nx)*h
+        double f0 = U(i0) * PB(i0);
+        for (int i = i0; i <= i1; ++i) {
             const double fp = U(i + 1) * PB(i + 1);
             dsx[(size_t)(i - 1) * RSP + e] = (fp - fm) / tdx;
             fm = f0;
@@ -173,38 +177,34 @@ __global__ void __launch_bounds__(256) k_sflux(Geo g, const double *__restrict__
         }
         return;
     }
-    // slopes of cell i (1..nx): (pfp phi(i+1) - pfm phi(i-1)) / 2dx, pfm = heat_ratio at i = 1
-    auto slope_phi = [&](int i) {
-        return i == 1 ? (1.0 * PB(2) - h * PB(nx)) / tdx : (1.0 * PB(i + 1) - 1.0 * PB(i - 1)) / tdx;
+    // slopes of cell c (1..nx): (pfp phi(c+1) - pfm phi(c-1)) / 2dx, pfm = heat_ratio at c = 1
+    auto slope_phi = [&](int c) {
+        return c == 1 ? (1.0 * PB(2) - h * PB(nx)) / tdx : (1.0 * PB(c + 1) - 1.0 * PB(c - 1)) / tdx;
     };
-    auto slope_u = [&](int i) { return (U(i + 1) - U(i == 1 ? nx : i - 1)) / tdx; };
+    auto slope_u = [&](int c) { return (U(c + 1) - U(c == 1 ? nx : c - 1)) / tdx; };
     auto flux = [](double up, double um, double Up, double Um) {
         const double ms = fmax(fabs(um), fabs(up));
         const double f = 0.5 * (up * Up) + 0.5 * (um * Um);
         return f - 0.5 * ms * (Up - Um);
     };
-    // interface 0 (the west image of interface nx)
-    const double sp0 = (PB(1) - PB(nx - 1) * h) / tdx, su0 = (U(1) - U(nx - 1)) / tdx;
-    double spc = slope_phi(1), suc = slope_u(1);
-    double Fm = flux(U(1) - suc * hdx, U(nx) + su0 * hdx, PB(1) - spc * hdx, PB(nx) * h + sp0 * hdx);
-    for (int i = 1; i <= nx; ++i) {
-        double up, Up;
-        double spn = 0.0, sun = 0.0;
-        if (i < nx) {
-            spn = slope_phi(i + 1);
-            sun = slope_u(i + 1);
-            up = U(i + 1) - sun * hdx;
-            Up = PB(i + 1) - spn * hdx;
-        } else {
-            const double spm = (PB(2) / h - PB(nx)) / tdx, sum = (U(2) - U(nx)) / tdx;
-            up = U(1) - sum * hdx;
-            Up = PB(1) / h - spm * hdx;
+    // Rusanov flux at interface i (between cells i and i+1); 0 and nx are the periodic ends
+    auto F = [&](int i) {
+        if (i == 0) {
+            const double sp0 = (PB(1) - PB(nx - 1) * h) / tdx, su0 = (U(1) - U(nx - 1)) / tdx;
+            return flux(U(1) - slope_u(1) * hdx, U(nx) + su0 * hdx, PB(1) - slope_phi(1) * hdx, PB(nx) * h + sp0 * hdx);
         }
-        const double F = flux(up, U(i) + suc * hdx, Up, PB(i) + spc * hdx);
-        dsx[(size_t)(i - 1) * RSP + e] = (F - Fm) / dx;
-        Fm = F;
-        spc = spn;
-        suc = sun;
+        if (i == nx) {
+            const double spm = (PB(2) / h - PB(nx)) / tdx, sum = (U(2) - U(nx)) / tdx;
+            return flux(U(1) - sum * hdx, U(nx) + slope_u(nx) * hdx, PB(1) / h - spm * hdx, PB(nx) + slope_phi(nx) * hdx);
+        }
+        return flux(U(i + 1) - slope_u(i + 1) * hdx, U(i) + slope_u(i) * hdx, PB(i + 1) - slope_phi(i + 1) * hdx,
+                    PB(i) + slope_phi(i) * hdx);
+    };
+    double Fm = F(i0 - 1);
+    for (int i = i0; i <= i1; ++i) {
+        const double Fi = F(i);
+        dsx[(size_t)(i - 1) * RSP + e] = (Fi - Fm) / dx;
+        Fm = Fi;
     }
 }
 
@@ -651,16 +651,18 @@ static size_t slines_smem() { return (size_t)(NX + SLinesCfg<NX>::LT * (NX + 1) 
 
 // heat_ratio update, surface flux and Nusselt number (bcsetscal, bc_scalar.F90:186-190,
 // 361-363; stepthescalar.F90:90-91), status.
-__global__ void k_sfin(Geo g, Scal *sc, const double *sdpart, double *flux_body) {
-    if (threadIdx.x != 0 || blockIdx.x != 0 || sc->status) return;
-    const double da1 = g.da1;
-    double fg = 0.0;
-    for (int m = 0; m < g.nbody; ++m) {
+__global__ void __launch_bounds__(256) k_sfin(Geo g, Scal *sc, const double *sdpart, double *flux_body) {
+    if (sc->status) return;
+    for (int m = threadIdx.x; m < g.nbody; m += blockDim.x) {
         double f = 0.0;
         for (int q = 0; q < kDragSplit; ++q) f += sdpart[(size_t)m * kDragSplit + q];
         flux_body[m] = f;
-        fg = fg + f * da1;
     }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const double da1 = g.da1;
+    double fg = 0.0;
+    for (int m = 0; m < g.nbody; ++m) fg = fg + flux_body[m] * da1;
     sc->flux_global = fg;
     sc->nusselt = -(fg * g.char_length * g.char_length) / (6.0 * g.voldom * g.maxvolfrac * (g.phisurf - g.phistream));
     const double hn = sc->heat_ratio_new;
@@ -678,7 +680,7 @@ static void enqueue_scalar_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s) 
     launch_planes<N>(k_sa<N>, g.nx + 1, 5, s, g, (const double2 *)b.phif, (const double *)b.ubcp, b.phr, b.phimg,
                      b.sdf, b.gph, (const Scal *)b.sc, b.spart);
     k_sheat<<<1, 32, 0, s>>>(g, b.sc, b.spart);
-    k_sflux<N><<<(RP<N>::RSP + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.phr, b.phimg, b.dsx, b.sc);
+    k_sflux<N><<<(RP<N>::RSP * ((g.nx + 31) / 32) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.phr, b.phimg, b.dsx, b.sc);
     launch_planes<N>(k_snl<N>, g.nx, 1, s, g, (const double *)b.ubcp, (const double *)b.phr, (const double *)b.dsx,
                      b.nls[cur], b.nlr[cur], b.sc);
     launch_planes<N>(k_simg<N>, 1, 1, s, g, (const double2 *)b.nls[cur], b.nlr[cur], (const Scal *)b.sc);
@@ -690,7 +692,7 @@ static void enqueue_scalar_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s) 
     launch_planes<N>(k_sff<N>, g.nx, 1, s, g, (const double *)b.sfr, b.ffs, b.sc);
     constexpr int LT = SLinesCfg<N>::LT;
     k_slines<N, LT><<<(g.PS + LT - 1) / LT, LT * 32, slines_smem<N>(), s>>>(g, b.phif, b.nls[cur], b.nls[old], b.ffs, b.sc);
-    k_sfin<<<1, 32, 0, s>>>(g, b.sc, b.sdpart, b.flux_body);
+    k_sfin<<<1, 256, 0, s>>>(g, b.sc, b.sdpart, b.flux_body);
 }
 
 void enqueue_scalar(const Geo &g, DevBufs &b, int cur, cudaStream_t s) {
