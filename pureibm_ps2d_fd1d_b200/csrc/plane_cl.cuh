@@ -45,7 +45,10 @@ template <int N> struct PL {
     static constexpr uint32_t RBYTES = RL * 8;
     static constexpr int NOUT = N * PZ;                 // column-phase slots (slot MC: rank 0 only)
     static constexpr int EPT = (NOUT + T - 1) / T;
-    static constexpr int MINB = 512 / T;                // CTAs per SM the register budget is sized for
+    // CTAs per SM the register budget is sized for: at 128^3 three CTAs of
+    // 256 threads (80 registers, 24 warps per SM) measured faster than two
+    // (128 registers), spills of the nonlinear kernels' epilogue included
+    static constexpr int MINB = (N == 128) ? 3 : 512 / T;
     static_assert(M % C == 0 && N % C == 0, "plane split");
     static_assert(RBYTES % 16 == 0, "bulk copies move 16-byte multiples");
 };
