@@ -618,12 +618,18 @@ static int batch_graphs(pibm_batch *bt) {
         cudaGraph_t gr;
         CUDA_OR_FAIL(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
         CUDA_OR_FAIL(cudaEventRecord(bt->fork, bt->stream));
+        // members whose plane kernels alone fill the GPU (nx*C CTAs per transform item
+        // of at least one per SM slot) form one chain, one after the other; the
+        // smaller members run as parallel branches beside that chain
+        int prev_big = -1;
         for (int q = 0; q < n; ++q) {
             pibm_handle *h = bt->members[q];
-            CUDA_OR_FAIL(cudaStreamWaitEvent(h->stream, bt->fork, 0));
+            const bool big = h->g.my >= 128;
+            CUDA_OR_FAIL(cudaStreamWaitEvent(h->stream, (big && prev_big >= 0) ? bt->join[prev_big] : bt->fork, 0));
             enqueue_step(h->g, h->b, bt->base[q] ^ par, h->stream, nullptr, &h->ss);
             CUDA_OR_FAIL(cudaEventRecord(bt->join[q], h->stream));
             CUDA_OR_FAIL(cudaStreamWaitEvent(bt->stream, bt->join[q], 0));
+            if (big) prev_big = q;
         }
         CUDA_OR_FAIL(cudaStreamEndCapture(bt->stream, &gr));
         const cudaError_t e = cudaGraphInstantiate(&bt->graph[par], gr, 0);

@@ -47,7 +47,9 @@ template <int N> struct PL {
     static constexpr int EPT = (NOUT + T - 1) / T;
     // CTAs per SM the register budget is sized for: at 128^3 three CTAs of
     // 256 threads (80 registers, 24 warps per SM) measured faster than two
-    // (128 registers), spills of the nonlinear kernels' epilogue included
+    // (128 registers), spills of the nonlinear kernels' epilogue included;
+    // the other sizes keep 128 registers (their nonlinear kernels spill more,
+    // and the batched ensemble measured slower with them at 80)
     static constexpr int MINB = (N == 128) ? 3 : 512 / T;
     static_assert(M % C == 0 && N % C == 0, "plane split");
     static_assert(RBYTES % 16 == 0, "bulk copies move 16-byte multiples");
