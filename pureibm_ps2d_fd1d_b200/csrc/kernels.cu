@@ -815,6 +815,14 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
         tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
         RHS[line * NP + i] = make_double2(tt.x / (c1 + c2), tt.y / (c1 + c2));
         P[line * NP + i] = p[(size_t)i * PS + q];
+        // explicit part of the ustep right-hand sides, dt*(c3 nl + ff + c4 onl) per component
+        // (usteptime.F90:291-297), kept in the velocity tiles until each component is solved
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            const double2 nn = G(nl, n, i, q), f = G(ff, n, i, q), on = G(onl, n, i, q);
+            U[(n * LT + line) * NP + i] = make_double2(((dt * c3) * nn.x + dt * f.x) + (dt * c4) * on.x,
+                                                       ((dt * c3) * nn.y + dt * f.y) + (dt * c4) * on.y);
+        }
     }
     __syncthreads();
     const int qw = q0 + w;
@@ -840,19 +848,28 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
     }
     __syncthreads();
     // ---------------- ustep per component (usteptime.F90:73-470) ----------------
+    constexpr int EPT = (LT * NX) / (LT * 32);   // tile elements per thread
     for (int n = 0; n < 3; ++n) {
+        // stage u_n of the tile, then form every right-hand side from the staged
+        // neighbours before overwriting the tile with them
         for (int t = threadIdx.x; t < LT * NX; t += blockDim.x) {
+            const int line = t % LT, i = t / LT, q = q0 + line;
+            RHS[line * NP + i] = q < PS ? G(u, n, i, q) : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        double2 rr[EPT];
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const int t = threadIdx.x + k * LT * 32;
             const int line = t % LT, i = t / LT, q = q0 + line;
             if (q >= PS) continue;
             const double ky = KY(q), kz = KZ(q), w2 = g.w2[q];
             const double alp = dt * (c1 + c2);
             const double fy = 1.0 - dt * vis * c1 * w2;
             const double gd = 1.0 * dt * vis * c1;
-            const double2 ui = G(u, n, i, q);
-            double2 r = make_double2(ui.x * fy, ui.y * fy);
-            const double2 nn = G(nl, n, i, q), f = G(ff, n, i, q), on = G(onl, n, i, q);
-            r = make_double2(r.x + (dt * c3) * nn.x + dt * f.x, r.y + (dt * c3) * nn.y + dt * f.y);
-            r = make_double2(r.x + (dt * c4) * on.x, r.y + (dt * c4) * on.y);
+            const double2 ui = RHS[line * NP + i];
+            const double2 ex = U[(n * LT + line) * NP + i];
+            double2 r = make_double2(ui.x * fy + ex.x, ui.y * fy + ex.y);
             const double2 pm = P[line * NP + (i == 0 ? nx - 1 : i - 1)], p0 = P[line * NP + i];
             double2 gp;
             if (n == 0) gp = make_double2((alp * (p0.x - pm.x)) / dx, (alp * (p0.y - pm.y)) / dx);
@@ -861,11 +878,18 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
                 gp = (n == 1) ? make_double2(-ky * sp.y, ky * sp.x) : make_double2(-kz * sp.y, kz * sp.x);
             }
             r = csub(r, gp);
-            const double2 um = G(u, n, i - 1, q), up = G(u, n, i + 1, q);
+            const double2 um = RHS[line * NP + (i == 0 ? nx - 1 : i - 1)], up = RHS[line * NP + (i == nx - 1 ? 0 : i + 1)];
             double2 lap;
             if (i == 0) lap = make_double2((up.x - 2.0 * ui.x) + um.x, (up.y - 2.0 * ui.y) + um.y);
             else lap = make_double2((um.x + up.x) - 2.0 * ui.x, (um.y + up.y) - 2.0 * ui.y);
-            RHS[line * NP + i] = make_double2(r.x + (gd * lap.x) / dx2, r.y + (gd * lap.y) / dx2);
+            rr[k] = make_double2(r.x + (gd * lap.x) / dx2, r.y + (gd * lap.y) / dx2);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const int t = threadIdx.x + k * LT * 32;
+            const int line = t % LT, i = t / LT, q = q0 + line;
+            if (q < PS) RHS[line * NP + i] = rr[k];
         }
         __syncthreads();
         if (wact) {
