@@ -791,27 +791,44 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
     };
     bool ok = true;
     // ---------------- pressure: source (poisson.F90:97-116) and old p ----------------
+    // Thread t holds (line t % LT, plane t / LT): for LT = 8 the plane i+1 of a lane
+    // sits LT lanes higher in the same warp, except in the warp's last plane row.
+    static_assert(LT == 8 || LT == 4, "tile width");
     for (int t = threadIdx.x; t < LT * NX; t += blockDim.x) {
-        const int line = t % LT, i = t / LT, q = q0 + line;
-        if (q >= PS) continue;
+        const int line = t % LT, i = t / LT;
+        const int q = min(q0 + line, PS - 1);   // clamped: every lane takes part in the shuffles
         const double ky = KY(q), kz = KZ(q);
         auto mwy = [&](double2 z) { return make_double2(-ky * z.y, ky * z.x); };
         auto mwz = [&](double2 z) { return make_double2(-kz * z.y, kz * z.x); };
+        double2 x0[9], x1[9];   // nl, ff, onl (3 components each) at planes i and i+1
+#pragma unroll
+        for (int n = 0; n < 3; ++n) { x0[n] = G(nl, n, i, q); x0[3 + n] = G(ff, n, i, q); x0[6 + n] = G(onl, n, i, q); }
+        const bool last_row = lane >= 32 - LT;
+#pragma unroll
+        for (int f = 0; f < 9; ++f) {
+            x1[f].x = __shfl_down_sync(0xffffffffu, x0[f].x, LT);
+            x1[f].y = __shfl_down_sync(0xffffffffu, x0[f].y, LT);
+        }
+        if (last_row) {
+#pragma unroll
+            for (int n = 0; n < 3; ++n) { x1[n] = G(nl, n, i + 1, q); x1[3 + n] = G(ff, n, i + 1, q); x1[6 + n] = G(onl, n, i + 1, q); }
+        }
+        if (q0 + line >= PS) continue;
         double2 tt = make_double2(0.0, 0.0), d, s;
-        d = csub(G(nl, 0, i + 1, q), G(nl, 0, i, q));
-        s = csub(G(ff, 0, i + 1, q), G(ff, 0, i, q));
+        d = csub(x1[0], x0[0]);
+        s = csub(x1[3], x0[3]);
         tt = make_double2(tt.x + (c3 * d.x) / dx + s.x / dx, tt.y + (c3 * d.y) / dx + s.y / dx);
-        d = mwy(cadd(G(nl, 1, i + 1, q), G(nl, 1, i, q)));
-        s = mwy(cadd(G(ff, 1, i + 1, q), G(ff, 1, i, q)));
+        d = mwy(cadd(x1[1], x0[1]));
+        s = mwy(cadd(x1[4], x0[4]));
         tt = make_double2(tt.x + (c3 * d.x) / 2.0 + s.x / 2.0, tt.y + (c3 * d.y) / 2.0 + s.y / 2.0);
-        d = mwz(cadd(G(nl, 2, i + 1, q), G(nl, 2, i, q)));
-        s = mwz(cadd(G(ff, 2, i + 1, q), G(ff, 2, i, q)));
+        d = mwz(cadd(x1[2], x0[2]));
+        s = mwz(cadd(x1[5], x0[5]));
         tt = make_double2(tt.x + (c3 * d.x) / 2.0 + s.x / 2.0, tt.y + (c3 * d.y) / 2.0 + s.y / 2.0);
-        d = csub(G(onl, 0, i + 1, q), G(onl, 0, i, q));
+        d = csub(x1[6], x0[6]);
         tt = make_double2(tt.x + (c4 * d.x) / dx, tt.y + (c4 * d.y) / dx);
-        d = mwy(cadd(G(onl, 1, i + 1, q), G(onl, 1, i, q)));
+        d = mwy(cadd(x1[7], x0[7]));
         tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
-        d = mwz(cadd(G(onl, 2, i + 1, q), G(onl, 2, i, q)));
+        d = mwz(cadd(x1[8], x0[8]));
         tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
         RHS[line * NP + i] = make_double2(tt.x / (c1 + c2), tt.y / (c1 + c2));
         P[line * NP + i] = p[(size_t)i * PS + q];
@@ -819,7 +836,7 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
         // (usteptime.F90:291-297), kept in the velocity tiles until each component is solved
 #pragma unroll
         for (int n = 0; n < 3; ++n) {
-            const double2 nn = G(nl, n, i, q), f = G(ff, n, i, q), on = G(onl, n, i, q);
+            const double2 nn = x0[n], f = x0[3 + n], on = x0[6 + n];
             U[(n * LT + line) * NP + i] = make_double2(((dt * c3) * nn.x + dt * f.x) + (dt * c4) * on.x,
                                                        ((dt * c3) * nn.y + dt * f.y) + (dt * c4) * on.y);
         }
