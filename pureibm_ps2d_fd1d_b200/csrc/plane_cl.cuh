@@ -14,10 +14,12 @@
 //                                so a real plane keeps its HBM layout and CTA r
 //                                moves its rows with one contiguous bulk copy.
 //
-// Between the phases every CTA reads the part it needs from the other CTAs'
-// shared memory (distributed shared memory, map_shared_rank) between two
-// cluster barriers, then rewrites its own buffer in the other layout.  The
-// arithmetic of every element is the same as in the single-CTA transform.
+// Between the phases the elements cross between the CTAs' shared memory
+// (distributed shared memory, map_shared_rank) between two cluster barriers,
+// fused with the half-length real-transform step of the y direction (c2r:
+// each CTA pulls its rows; r2c: each CTA pushes its rows to the column
+// owners).  The arithmetic of every element is the same as in the single-CTA
+// transform.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -67,6 +69,17 @@ template <int N> __device__ __forceinline__ int cl_col(int jl, int rank) {
     return jl == PL<N>::MC ? PL<N>::M : rank * PL<N>::MC + jl;
 }
 
+// 32-bit shared::cluster address of element `slot` of CTA `rank`'s buffer,
+// and a 16-byte store through it (distributed shared memory).
+__device__ __forceinline__ uint32_t cl_addr(const double2 *buf, int slot, int rank) {
+    uint32_t r;
+    asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"((uint32_t)__cvta_generic_to_shared(buf + slot)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cl_st(uint32_t addr, double2 v) {
+    asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(v.x), "d"(v.y) : "memory");
+}
+
 // CTA 0, warp 0: column 0 <- Herm(ky = 0) + i Herm(ky = M) (see herm_pack).
 template <int N>
 __device__ __forceinline__ void cl_pack_col0(double2 *buf) {
@@ -99,68 +112,6 @@ __device__ __forceinline__ double2 cl_unpack(const double2 *buf, int kz, int jl,
     const double2 y = buf[kz * L::PZ], ym = buf[((N - kz) % N) * L::PZ];
     if (jl == 0) return make_double2(0.5 * (y.x + ym.x), 0.5 * (y.y - ym.y));
     return make_double2(0.5 * (y.y + ym.y), -0.5 * (y.x - ym.x));
-}
-
-// Column phase -> row phase (after the z pass of a c2r).
-template <int N>
-__device__ __forceinline__ void cl_cols_to_rows(double2 *buf, int rank) {
-    using L = PL<N>;
-    if constexpr (L::C > 1) {
-        constexpr int TOT = L::NR * L::M, K = (TOT + L::T - 1) / L::T;
-        cg::cluster_group cl = cg::this_cluster();
-        cl.sync();   // every CTA of the plane finished its z pass
-        double2 v[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int u = (int)threadIdx.x + k * L::T;
-            if (u < TOT) {
-                const int r = u / L::M, c = u - r * L::M, h = c / L::MC;
-                const double2 *src = cl.map_shared_rank(buf, h);
-                v[k] = src[(rank * L::NR + r) * L::PZ + (c - h * L::MC)];
-            }
-        }
-        cl.sync();   // every CTA finished reading: buffers may be rewritten
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int u = (int)threadIdx.x + k * L::T;
-            if (u < TOT) {
-                const int r = u / L::M, c = u - r * L::M;
-                buf[r * L::P + c] = v[k];
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// Row phase -> column phase (after the y pass of an r2c).
-template <int N>
-__device__ __forceinline__ void cl_rows_to_cols(double2 *buf, int rank) {
-    using L = PL<N>;
-    if constexpr (L::C > 1) {
-        constexpr int TOT = N * L::MC, K = (TOT + L::T - 1) / L::T;
-        cg::cluster_group cl = cg::this_cluster();
-        cl.sync();
-        double2 v[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int u = (int)threadIdx.x + k * L::T;
-            if (u < TOT) {
-                const int z = u / L::MC, c = u - z * L::MC, h = z / L::NR;
-                const double2 *src = cl.map_shared_rank(buf, h);
-                v[k] = src[(z - h * L::NR) * L::P + rank * L::MC + c];
-            }
-        }
-        cl.sync();
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int u = (int)threadIdx.x + k * L::T;
-            if (u < TOT) {
-                const int z = u / L::MC, c = u - z * L::MC;
-                buf[z * L::PZ + c] = v[k];
-            }
-        }
-        __syncthreads();
-    }
 }
 
 // c2r reconstruction of ROWS rows at pitch P: each row's M+1 spectral values
@@ -219,6 +170,92 @@ __device__ __forceinline__ void rows_r2c_post(double2 *buf, const TwT &tw) {
     __syncthreads();
 }
 
+// The exchanges fused with the half-length real-transform step.  Row r of a
+// CTA's row phase is processed as M/2 units: unit j = 0 takes slot 0 (ky = 0
+// in Re, ky = M in Im after the packed z pass) and slot M/2, unit j in
+// [1, M/2) the mirror pair (j, M - j).  Each unit produces its two outputs
+// from its two inputs, so the separate row pass of rows_c2r_pre /
+// rows_r2c_post disappears and every element crosses shared memory once.
+template <int N> __device__ __forceinline__ int cl_mirror(int j) { return j == 0 ? N / 4 : N / 2 - j; }
+
+// c2r: column phase -> row phase with the reconstruction Z[n] of rows_c2r_pre.
+// Pull: every CTA reads its rows' mirror pairs from the column owners, then
+// rewrites its own buffer in the row layout.
+template <int N>
+__device__ __forceinline__ void cl_cols_to_rows_pre(double2 *buf, const TwT &tw, int rank) {
+    using L = PL<N>;
+    constexpr int H = L::M / 2, TOT = L::NR * H, K = (TOT + L::T - 1) / L::T;
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();   // every CTA of the plane finished its z pass
+    double2 va[K], vb[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int u = (int)threadIdx.x + k * L::T;
+        if (u < TOT) {
+            const int r = u / H, j = u - r * H, nb = cl_mirror<N>(j);
+            const int ha = j / L::MC, hb = nb / L::MC, row = (rank * L::NR + r) * L::PZ;
+            const double2 xa = cl.map_shared_rank(buf, ha)[row + j - ha * L::MC];
+            const double2 xb = cl.map_shared_rank(buf, hb)[row + nb - hb * L::MC];
+            if (j == 0) {
+                va[k] = c2r_pre_one(make_double2(xa.x, 0.0), make_double2(xa.y, 0.0), make_double2(1.0, 0.0));
+                vb[k] = c2r_pre_one(xb, xb, tw.w(H, N, +1.0));
+            } else {
+                va[k] = c2r_pre_one(xa, xb, tw.w(j, N, +1.0));
+                vb[k] = c2r_pre_one(xb, xa, tw.w(nb, N, +1.0));
+            }
+        }
+    }
+    cl.sync();   // every CTA finished reading: buffers may be rewritten
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int u = (int)threadIdx.x + k * L::T;
+        if (u < TOT) {
+            const int r = u / H, j = u - r * H;
+            buf[r * L::P + j] = va[k];
+            buf[r * L::P + cl_mirror<N>(j)] = vb[k];
+        }
+    }
+    __syncthreads();
+}
+
+// r2c: row phase -> column phase with the split X[n] of rows_r2c_post.
+// Push: every CTA forms the outputs of its own rows, and after a cluster
+// barrier (all rows read) stores them into the column owners' buffers.
+template <int N>
+__device__ __forceinline__ void cl_rows_to_cols_post(double2 *buf, const TwT &tw, int rank) {
+    using L = PL<N>;
+    constexpr int H = L::M / 2, TOT = L::NR * H, K = (TOT + L::T - 1) / L::T;
+    cg::cluster_group cl = cg::this_cluster();
+    double2 va[K], vb[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int u = (int)threadIdx.x + k * L::T;
+        if (u < TOT) {
+            const int r = u / H, j = u - r * H, nb = cl_mirror<N>(j);
+            const double2 za = buf[r * L::P + j], zb = buf[r * L::P + nb];
+            if (j == 0) {
+                va[k] = make_double2(za.x + za.y, za.x - za.y);
+                vb[k] = r2c_post_one(zb, zb, tw.w(H, N, -1.0));
+            } else {
+                va[k] = r2c_post_one(za, zb, tw.w(j, N, -1.0));
+                vb[k] = r2c_post_one(zb, za, tw.w(nb, N, -1.0));
+            }
+        }
+    }
+    cl.sync();   // every CTA read its rows: buffers may be rewritten
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int u = (int)threadIdx.x + k * L::T;
+        if (u < TOT) {
+            const int r = u / H, j = u - r * H, nb = cl_mirror<N>(j);
+            const int ha = j / L::MC, hb = nb / L::MC, row = (rank * L::NR + r) * L::PZ;
+            cl_st(cl_addr(buf, row + j - ha * L::MC, ha), va[k]);
+            cl_st(cl_addr(buf, row + nb - hb * L::MC, hb), vb[k]);
+        }
+    }
+    cl.sync();   // every column of the plane is in place
+}
+
 // c2r of the CTA's columns (natural kz, column-phase layout; CTA 0 with
 // ky = M in slot MC).  Call after a __syncthreads.  On return the CTA holds
 // rows [rank*NR, (rank+1)*NR) of the real plane image: real value (z, y) of
@@ -231,8 +268,11 @@ __device__ __forceinline__ void cl_c2r(double2 *buf, const TwT &tw, int rank) {
         __syncthreads();
     }
     bfft_v1<Plan<N>::AZ, Plan<N>::BZ, L::MC, L::T>(buf, 1, L::PZ, +1.0, tw);
-    cl_cols_to_rows<N>(buf, rank);
-    rows_c2r_pre<N, L::T, L::NR>(buf, tw);
+    if constexpr (L::C > 1) {
+        cl_cols_to_rows_pre<N>(buf, tw, rank);
+    } else {
+        rows_c2r_pre<N, L::T, L::NR>(buf, tw);
+    }
     bfft_v1<Plan<N>::AY, Plan<N>::BY, L::NR, L::T>(buf, L::P, 1, +1.0, tw);
 }
 
@@ -243,8 +283,11 @@ template <int N>
 __device__ __forceinline__ void cl_r2c(double2 *buf, const TwT &tw, int rank) {
     using L = PL<N>;
     bfft_v2<Plan<N>::AY, Plan<N>::BY, L::NR, L::T>(buf, L::P, 1, -1.0, tw);
-    rows_r2c_post<N, L::T, L::NR>(buf, tw);
-    cl_rows_to_cols<N>(buf, rank);
+    if constexpr (L::C > 1) {
+        cl_rows_to_cols_post<N>(buf, tw, rank);
+    } else {
+        rows_r2c_post<N, L::T, L::NR>(buf, tw);
+    }
     bfft_v2<Plan<N>::AZ, Plan<N>::BZ, L::MC, L::T>(buf, 1, L::PZ, -1.0, tw);
 }
 
