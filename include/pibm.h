@@ -37,6 +37,7 @@ extern "C" {
 #define PIBM_ERR_TIMEOUT        (-7)  /* a bounded device wait ran out                              */
 #define PIBM_ERR_CUDA           (-8)  /* CUDA runtime error                                         */
 #define PIBM_ERR_NOMEM          (-9)  /* allocation failed                                          */
+#define PIBM_ERR_SPREAD_OVERFLOW (-10) /* more force contributions on one node than the spreading buckets hold */
 
 /* x-flux discretisation (Part_propt DISCR_SCHEME, nl_allflow.F90:98-100,192-207). */
 #define PIBM_SCHEME_CENTER 0
@@ -171,6 +172,14 @@ int  pibm_get_particles(pibm_handle *h, double *pres, double *visc, double *forc
  * grad phi . n (calc_bndrev_data), ratios[0..2] = heat_ratio,
  * heat_ratio_old, Nusselt number.  Any pointer may be NULL. */
 int  pibm_get_scalar(pibm_handle *h, double *phif, double *flux_body, double *ratios);
+/* Moving particles (IMOVE = 1): the DEM lists of the last step in the
+ * reference layout NEIGHBOURS / PN / PV (nbody, maxn) column-major
+ * (dem_mod.F90; collision_mod.F90:807-1062, soft_sphere_coll.F90:120-420):
+ * column 1 holds the count (PV: 1), columns 2.. the 1-based particle numbers
+ * (-1 after the last; PV: the contact flags, 0 after the last).  maxn = 37
+ * (MAXNEIGHBORS = MN + 1 + NWALLS) always suffices; PIBM_ERR_ARG if a list
+ * does not fit or the run has fixed particles.  Any pointer may be NULL. */
+int  pibm_get_contacts(pibm_handle *h, int32_t maxn, int32_t *neigh, int32_t *pn, int32_t *pv);
 /* Active reversal-point flags (part_array(m)%if_rev), (nbnd, nbody) column-major. */
 int  pibm_get_if_rev(pibm_handle *h, uint8_t *if_rev);
 /* Solid mask fluid_atijk(1:nx,1:my,1:mz) as 0/1 bytes, x fastest. */

@@ -46,6 +46,7 @@ def lib():
         L.orc_get_geometry.argtypes = [vp, P(C.c_double), P(C.c_double)]
         L.orc_get_field.argtypes = [vp, C.c_int, P(C.c_double)]
         L.orc_get_scalar.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_double)]
+        L.orc_get_contacts.argtypes = [vp, C.c_int, P(C.c_int32), P(C.c_int32), P(C.c_int32)]
         L.orc_ff2rc.argtypes = [C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
         L.orc_ff2cr.argtypes = [C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
         L.orc_cyclic_solve.argtypes = [C.c_int] + [P(C.c_double)] * 7
@@ -203,3 +204,19 @@ def get_scalar(solver) -> dict:
         raise RuntimeError("oracle has no scalar (ISCALON = 0)")
     return dict(phif=phif, flux_body=flux[:solver.nbody], heat_ratio=ratios[0], heat_ratio_old=ratios[1],
                 nusselt=ratios[2])
+
+
+MAXNEIGHBORS = 37   # MN + 1 + NWALLS (collision_mod.F90:508)
+
+
+def get_contacts(solver, maxn: int = MAXNEIGHBORS) -> dict:
+    """DEM lists of an OracleSolver with moving particles, in the reference
+    layout (nbody, maxn) read as arrays [column][particle]: column 0 the count,
+    then 1-based particle numbers (-1 fill; PV: flags, 0 fill)."""
+    n = solver.nbody
+    out = {k: np.zeros((maxn, n), dtype=np.int32) for k in ("neighbours", "pn", "pv")}
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+    rc = lib().orc_get_contacts(solver.h, maxn, ip(out["neighbours"]), ip(out["pn"]), ip(out["pv"]))
+    if rc != 0:
+        raise RuntimeError("oracle has no DEM lists (IMOVE = 0) or maxn too small")
+    return out

@@ -43,6 +43,25 @@ thread_local std::string g_err;
 
 inline int fint(double x) { return (int)x; }   // Fortran INT: truncation toward zero
 
+// Soft-sphere DEM state (IMOVE = 1, COLLISION_TYPE = 'softsphere'): dem_mod.F90
+// arrays for one phase.  Particle indices are 0-based here; list order is the
+// reference's.  Positions and velocities are physical (DES_POS = (XC-1)*dx).
+struct Dem {
+    int N = 0;
+    int cx = 0, cy = 0, cz = 0;               // coarse grid nodes; physical cells 2..c (IMAX1 = cx)
+    double dxc = 0, dyc = 0, dzc = 0;
+    double LXs = 0, LYs = 0, LZs = 0;         // search periods XE(IMAX1)-XE(1) (collision_mod.F90:823-825)
+    double XL = 0, YL = 0, ZL = 0;            // XLENGTH/YLENGTH/ZLENGTH = wall positions EX2/TY2/NZ2
+    double kn = 0, kt = 0, eta_n = 0, eta_t = 0, mew = 0;
+    double dtsolid_orig = 0, max_radius = 0, rhof = 0;
+    int maxneigh = 0;
+    std::vector<double> pos, pos_old, vel, vel_old, om, om_old;   // [3*l + d]
+    std::vector<double> rad, pmass, pvol;
+    std::vector<int> pijk;                                        // [3*l + d], cells 2..c
+    std::vector<std::vector<int>> neigh;                          // NEIGHBOURS(l, 2..): mirrors, self, found
+    std::vector<std::vector<int>> pn, pv;                         // PN(l, 2..), PV(l, 2..)
+};
+
 struct Orc {
     // ---- parameters -------------------------------------------------------
     pibm_params prm;
@@ -63,6 +82,8 @@ struct Orc {
     std::vector<uint8_t> if_rev;    // (nbnd, nbody)
     std::vector<int> nrpr_active;   // (nbody)
     std::vector<std::vector<int>> neighbours;  // DEM neighbour lists incl. self
+    bool moving = false;            // IMOVE = 1: particles move (DEM every step)
+    Dem dem;
     double mean_volfrac, maxvolfrac;
     long long count_solid, count_fluid;
     std::vector<uint8_t> fluid;     // fluid_atijk(0:nx+1, my, mz)
@@ -315,6 +336,282 @@ void update_nrpr(Orc &o) {
     }
 }
 
+// ============================================================================
+// Soft-sphere DEM for moving particles (IMOVE = 1, COLLISION_TYPE =
+// 'softsphere', one phase, x/y/z-periodic walls, no wall contacts since
+// WALLDTSPLIT = F).  initialize_coarse_grid sets MEW = MEW_W = 0
+// (collision_mod.F90:388-389), so CFSLIDE always returns a tangential force of
+// (signed) zero and the tangential history PFN/PFT never reaches a force; the
+// rotation update is commented out (CFNEWVALUES, :1388), so OMEGA stays 0.
+// What moves the particles is the normal spring-dashpot force of each contact
+// pair; the contact lists PN/PV are kept exactly as the reference keeps them.
+// ============================================================================
+
+// initialize_coarse_grid (collision_mod.F90:346-492), DES_INIT_ARRAYS (:1203-1316)
+// and CFASSIGN (:582-741) for the 'default' particle input.
+void dem_init(Orc &o) {
+    Dem &D = o.dem;
+    const int N = o.nbody;
+    D.N = N;
+    D.XL = o.doml[0]; D.YL = o.doml[1]; D.ZL = o.doml[2];
+    double rmax = 0.0;
+    for (int m = 0; m < N; ++m) rmax = std::max(rmax, o.radbdy[m]);
+    const double dxeff = 2.0 * rmax * 1.5 * o.dx;                  // cgrid_fac = 1.5
+    D.cy = std::max((int)std::lround(D.YL / dxeff), 2);
+    D.cx = std::max((int)std::lround(D.XL / dxeff), 2);
+    D.cz = std::max((int)std::lround(D.ZL / dxeff), 2);
+    D.dyc = D.YL / (double)(D.cy - 1);
+    D.dxc = D.XL / (double)(D.cx - 1);
+    D.dzc = D.ZL / (double)(D.cz - 1);
+    // XE(1) = 0, XE(i) = XE(i-1) + dxc (i = 2..IMAX2); period = XE(IMAX1) - XE(1)
+    double e = 0.0;
+    for (int i = 2; i <= D.cx; ++i) e = e + D.dxc;
+    D.LXs = e;
+    e = 0.0;
+    for (int j = 2; j <= D.cy; ++j) e = e + D.dyc;
+    D.LYs = e;
+    e = 0.0;
+    for (int k = 2; k <= D.cz; ++k) e = e + D.dzc;
+    D.LZs = e;
+    D.kn = 800000.0;                                              // KN (:384-386)
+    D.kt = (2.0 / 7.0) * D.kn;                                    // KT (CFASSIGN :627)
+    D.mew = 0.0;
+    D.maxneigh = 30 + 1 + 6;                                      // MN + 1 + NWALLS (:508)
+    D.rhof = o.prm.rhof;
+    D.pos.assign(3 * (size_t)N, 0.0); D.vel.assign(3 * (size_t)N, 0.0); D.om.assign(3 * (size_t)N, 0.0);
+    D.rad.assign(N, 0.0); D.pmass.assign(N, 0.0); D.pvol.assign(N, 0.0);
+    D.max_radius = 0.0;
+    for (int l = 0; l < N; ++l) {
+        D.pos[3 * l + 0] = (o.XC(l + 1, 1) + 0.0 - 1.0) * o.dx;   // foffset = 0
+        D.pos[3 * l + 1] = (o.XC(l + 1, 2) - 1.0) * o.dy;
+        D.pos[3 * l + 2] = (o.XC(l + 1, 3) - 1.0) * o.dz;
+        D.rad[l] = o.radbdy[l] * o.dx;
+        for (int d = 0; d < 3; ++d) D.vel[3 * l + d] = o.VB(l + 1, d + 1);
+        const double r2 = D.rad[l] * D.rad[l];
+        D.pvol[l] = (4.0 / 3.0) * PI * r2 * D.rad[l];
+        D.pmass[l] = D.pvol[l] * o.prm.rhos;
+        D.max_radius = std::max(D.max_radius, D.rad[l]);
+    }
+    D.pos_old = D.pos; D.vel_old = D.vel; D.om_old = D.om;
+    // collision time from the phase diameter (CFASSIGN :664-680); DTSOLID = TCOLL/50
+    const double en = o.prm.coeff_rest, len = std::log(en);
+    {
+        const double mi = (PI * std::pow(o.prm.dia_phys, 3.0) * o.prm.rhos) / 6.0;
+        const double meff = (mi * mi) / (mi + mi);
+        double etan = 2.0 * std::sqrt(D.kn * meff) * std::fabs(len);
+        etan = etan / std::sqrt(PI * PI + std::pow(len, 2.0));
+        const double tcoll = PI / std::sqrt(D.kn / meff - std::pow(etan / meff, 2.0) / 4.0);
+        D.dtsolid_orig = std::min(tcoll, LARGE_NUMBER) / 50.0;
+    }
+    // pair damping of CALC_FORCE_DES (soft_sphere_coll.F90:408-414): one phase,
+    // so every pair has the same masses
+    if (N > 0) {
+        const double mi = (PI * std::pow(2.0 * D.rad[0], 3.0) * o.prm.rhos) / 6.0;
+        const double meff = (mi * mi) / (mi + mi);
+        D.eta_n = 2.0 * std::sqrt(D.kn * meff) * std::fabs(len);
+        D.eta_n = D.eta_n / std::sqrt(PI * PI + std::pow(len, 2.0));
+        D.eta_t = 0.5 * D.eta_n;
+    }
+    D.pn.assign(N, {}); D.pv.assign(N, {});
+}
+
+// FIND_CELL_INDEX (collision_mod.F90:743-762).
+void dem_cells(Dem &D) {
+    D.pijk.assign(3 * (size_t)D.N, 0);
+    for (int l = 0; l < D.N; ++l) {
+        D.pijk[3 * l + 0] = std::min(fint(D.pos[3 * l + 0] / D.dxc) + 2, D.cx);
+        D.pijk[3 * l + 1] = std::min(fint(D.pos[3 * l + 1] / D.dyc) + 2, D.cy);
+        D.pijk[3 * l + 2] = std::min(fint(D.pos[3 * l + 2] / D.dzc) + 2, D.cz);
+    }
+}
+
+// PARTICLES_IN_CELL + GRID_BASED_NEIGHBOR_SEARCH (collision_mod.F90:764-1062).
+// NEIGHBOURS(LL) ends up as: entries appended by lower particles' searches
+// (ascending), LL itself, then LL's own finds in cell-scan order.
+bool dem_search(Dem &D) {
+    const int N = D.N;
+    const int W = D.cx + 2, H = D.cy + 2;
+    std::vector<std::vector<int>> pic((size_t)W * H * (D.cz + 2));
+    auto bin = [&](int i, int j, int k) -> std::vector<int> & { return pic[(size_t)i + (size_t)W * ((size_t)j + (size_t)H * k)]; };
+    for (int l = 0; l < N; ++l) bin(D.pijk[3 * l], D.pijk[3 * l + 1], D.pijk[3 * l + 2]).push_back(l);
+    D.neigh.assign(N, {});
+    for (int LL = 0; LL < N; ++LL) {
+        D.neigh[LL].push_back(LL);
+        if ((int)D.neigh[LL].size() + 1 > D.maxneigh) { g_err = "DEM neighbour list overflow"; return false; }
+        const int II = D.pijk[3 * LL], JJ = D.pijk[3 * LL + 1], KK = D.pijk[3 * LL + 2];
+        for (int kk = KK - 1; kk <= KK + 1; ++kk)
+            for (int jj = JJ - 1; jj <= JJ + 1; ++jj)
+                for (int ii = II - 1; ii <= II + 1; ++ii) {
+                    int I = ii, J = jj, K = kk;
+                    double xper = 0.0, yper = 0.0, zper = 0.0;
+                    if (ii > D.cx) { I = 2; xper = 1.0; }
+                    if (ii < 2) { I = D.cx; xper = -1.0; }
+                    if (jj > D.cy) { J = 2; yper = 1.0; }
+                    if (jj < 2) { J = D.cy; yper = -1.0; }
+                    if (kk > D.cz) { K = 2; zper = 1.0; }
+                    if (kk < 2) { K = D.cz; zper = -1.0; }
+                    for (int PNO : bin(I, J, K)) {
+                        if (PNO <= LL) continue;
+                        const double rlm = 1.2 * (D.rad[LL] + D.rad[PNO]);   // FACTOR_RLM
+                        const double c0 = D.pos[3 * PNO + 0] + xper * D.LXs;
+                        const double c1 = D.pos[3 * PNO + 1] + yper * D.LYs;
+                        const double c2 = D.pos[3 * PNO + 2] + zper * D.LZs;
+                        const double d0 = c0 - D.pos[3 * LL + 0], d1 = c1 - D.pos[3 * LL + 1], d2 = c2 - D.pos[3 * LL + 2];
+                        double dd = 0.0;
+                        dd = dd + d0 * d0; dd = dd + d1 * d1; dd = dd + d2 * d2;
+                        const double distmag = std::sqrt(dd);
+                        bool already = false;
+                        for (size_t q = 0; q < D.neigh[LL].size(); ++q) if (D.neigh[LL][q] == PNO) already = true;
+                        if (rlm - distmag > SMALL_NUMBER && !already) {
+                            D.neigh[LL].push_back(PNO);
+                            if ((int)D.neigh[LL].size() + 1 > D.maxneigh) { g_err = "DEM neighbour list overflow"; return false; }
+                            D.neigh[PNO].push_back(LL);
+                            if ((int)D.neigh[PNO].size() + 1 > D.maxneigh) { g_err = "DEM neighbour list overflow"; return false; }
+                        }
+                    }
+                }
+    }
+    return true;
+}
+
+// CALC_FORCE_DES (soft_sphere_coll.F90:52-551) without walls: contact-list
+// upkeep and the contact force FC of every particle.
+bool dem_forces(Dem &D, double dtsolid, std::vector<double> &fc) {
+    const int N = D.N;
+    const double L[3] = {D.XL, D.YL, D.ZL};
+    fc.assign(3 * (size_t)N, 0.0);
+    for (int LL = 0; LL < N; ++LL) {
+        std::vector<int> &pn = D.pn[LL], &pv = D.pv[LL];
+        {   // drop the entries whose contact ended (PV = 0), keeping the order
+            size_t w = 0;
+            for (size_t q = 0; q < pn.size(); ++q)
+                if (pv[q] != 0) { pn[w] = pn[q]; pv[w] = pv[q]; ++w; }
+            pn.resize(w); pv.resize(w);
+        }
+        std::fill(pv.begin(), pv.end(), 0);
+        for (int I : D.neigh[LL]) {
+            if (I <= LL) continue;
+            int ni = -1, ni_i = -1;
+            for (size_t q = 0; q < pn.size(); ++q) if (pn[q] == I) { ni = (int)q; break; }
+            if (ni >= 0)
+                for (size_t q = 0; q < D.pn[I].size(); ++q) if (D.pn[I][q] == LL) { ni_i = (int)q; break; }
+            double pI[3];
+            for (int d = 0; d < 3; ++d) {
+                pI[d] = D.pos[3 * I + d];
+                const double tempd = std::fabs(D.pos[3 * LL + d] - D.pos[3 * I + d]);
+                if (tempd > 4.0 * D.max_radius) pI[d] = pI[d] > D.pos[3 * LL + d] ? pI[d] - L[d] : pI[d] + L[d];
+            }
+            const double rlm = D.rad[LL] + D.rad[I];
+            double dist[3], dd = 0.0;
+            for (int d = 0; d < 3; ++d) dist[d] = pI[d] - D.pos[3 * LL + d];
+            for (int d = 0; d < 3; ++d) dd = dd + dist[d] * dist[d];
+            const double distmod = std::sqrt(dd);
+            if (!(rlm - distmod > SMALL_NUMBER)) continue;
+            if (distmod == 0.0) { g_err = "DEM: coincident particle centres"; return false; }
+            double nrm[3];
+            for (int d = 0; d < 3; ++d) nrm[d] = dist[d] / distmod;
+            // CFRELVEL (:728-776)
+            double vrel[3], osum[3], vrot[3];
+            for (int d = 0; d < 3; ++d) vrel[d] = D.vel[3 * LL + d] - D.vel[3 * I + d];
+            for (int d = 0; d < 3; ++d) osum[d] = D.om[3 * LL + d] * D.rad[LL] + D.om[3 * I + d] * D.rad[I];
+            vrot[0] = osum[1] * nrm[2] - osum[2] * nrm[1];
+            vrot[1] = osum[2] * nrm[0] - osum[0] * nrm[2];
+            vrot[2] = osum[0] * nrm[1] - osum[1] * nrm[0];
+            for (int d = 0; d < 3; ++d) vrel[d] = vrel[d] + vrot[d];
+            double vrn = 0.0;
+            for (int d = 0; d < 3; ++d) vrn = vrn + vrel[d] * nrm[d];
+            double ov_n;
+            if (ni >= 0) {
+                pv[ni] = 1;
+                if (ni_i >= 0) D.pv[I][ni_i] = 1;
+                ov_n = rlm - distmod;
+            } else {
+                pn.push_back(I); pv.push_back(1);
+                D.pn[I].push_back(LL); D.pv[I].push_back(1);
+                ov_n = rlm - distmod;
+            }
+            if ((int)pn.size() + 1 > D.maxneigh || (int)D.pn[I].size() + 1 > D.maxneigh) { g_err = "DEM contact list overflow"; return false; }
+            // normal force FNS1 + FNS2; the tangential force is zero (MEW = 0)
+            for (int d = 0; d < 3; ++d) {
+                const double fns1 = -(D.kn * ov_n) * nrm[d];
+                const double fns2 = -(D.eta_n * vrn) * nrm[d];
+                const double fn = fns1 + fns2;
+                fc[3 * LL + d] = fc[3 * LL + d] + fn;       // CFFCTOW (:873-905)
+                fc[3 * I + d] = fc[3 * I + d] - fn;
+            }
+        }
+    }
+    return true;
+}
+
+// des_time_march(.FALSE.) for 'softsphere' (collision_mod.F90:272-294) and
+// IBMUPDATE (:1464-1474): FACTOR sub-steps of SOFT_SPHERE_COLLISION
+// (CALC_FORCE_DES + CFNEWVALUES, :1658-1761), CFUPDATEOLD, FIND_CELL_INDEX,
+// PARTICLES_IN_CELL and GRID_BASED_NEIGHBOR_SEARCH.
+int des_time_march(Orc &o) {
+    Dem &D = o.dem;
+    const int N = D.N;
+    const double L[3] = {D.XL, D.YL, D.ZL};
+    if (!o.prm.collision_softsphere) {
+        // COLLISION_TYPE = 'none' (:295-328): DTSOLID = dt, velocities kept,
+        // positions advanced by CFNEWVALUES; the neighbour lists are not rebuilt
+        for (int l = 0; l < N; ++l) {
+            double dd = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                D.vel[3 * l + d] = D.vel_old[3 * l + d];
+                D.om[3 * l + d] = D.om_old[3 * l + d];
+                D.pos[3 * l + d] = D.pos_old[3 * l + d] + D.vel[3 * l + d] * o.dt;
+                const double t = D.pos[3 * l + d] - D.pos_old[3 * l + d];
+                dd = dd + t * t;
+            }
+            if (std::sqrt(dd) >= D.rad[l]) { g_err = "DEM: particle moved a radius in one sub-step"; return PIBM_ERR_DEM_MOVE; }
+            for (int d = 0; d < 3; ++d) {
+                if (D.pos[3 * l + d] > L[d]) D.pos[3 * l + d] = D.pos[3 * l + d] - (L[d] - 0.0);
+                else if (D.pos[3 * l + d] < 0.0) D.pos[3 * l + d] = D.pos[3 * l + d] + (L[d] - 0.0);
+            }
+            for (int d = 0; d < 3; ++d) { D.pos_old[3 * l + d] = D.pos[3 * l + d]; D.vel_old[3 * l + d] = D.vel[3 * l + d]; }
+        }
+    } else {
+    int factor = fint(o.dt / D.dtsolid_orig);
+    double dts = D.dtsolid_orig;
+    if (factor < 1) { factor = 1; dts = o.dt; }
+    std::vector<double> fc;
+    for (int ifac = 1; ifac <= factor; ++ifac) {
+        if (!dem_forces(D, dts, fc)) return PIBM_ERR_NEIGH_OVERFLOW;
+        // CFNEWVALUES (:1335-1462), softsphere, coupled to the flow
+        for (int l = 0; l < N; ++l) {
+            for (int d = 0; d < 3; ++d) {
+                const size_t q = (size_t)l + (size_t)N * d;
+                double a = fc[3 * l + d] / D.pmass[l] + (D.rhof * (o.pres[q] + o.visc[q])) / D.pmass[l];
+                a = a - o.frame_accln[d];
+                a = a - (o.mpg[d] * D.pvol[l]) / D.pmass[l];
+                D.vel[3 * l + d] = D.vel_old[3 * l + d] + a * dts;
+                D.om[3 * l + d] = D.om_old[3 * l + d];
+                D.pos[3 * l + d] = D.pos_old[3 * l + d] + D.vel[3 * l + d] * dts;
+            }
+            double dd = 0.0;
+            for (int d = 0; d < 3; ++d) { const double t = D.pos[3 * l + d] - D.pos_old[3 * l + d]; dd = dd + t * t; }
+            if (std::sqrt(dd) >= D.rad[l]) { g_err = "DEM: particle moved a radius in one sub-step"; return PIBM_ERR_DEM_MOVE; }
+            for (int d = 0; d < 3; ++d) {
+                if (D.pos[3 * l + d] > L[d]) D.pos[3 * l + d] = D.pos[3 * l + d] - (L[d] - 0.0);
+                else if (D.pos[3 * l + d] < 0.0) D.pos[3 * l + d] = D.pos[3 * l + d] + (L[d] - 0.0);
+            }
+        }
+        D.pos_old = D.pos; D.vel_old = D.vel; D.om_old = D.om;   // CFUPDATEOLD
+        dem_cells(D);
+        if (!dem_search(D)) return PIBM_ERR_NEIGH_OVERFLOW;
+    }
+    }
+    for (int m = 1; m <= N; ++m) {
+        o.XCr(m, 1) = D.pos[3 * (m - 1) + 0] / o.dx + 1.0 - 0.0;
+        o.XCr(m, 2) = D.pos[3 * (m - 1) + 1] / o.dy + 1.0;
+        o.XCr(m, 3) = D.pos[3 * (m - 1) + 2] / o.dz + 1.0;
+        for (int d = 0; d < 3; ++d) o.velbdy[(size_t)(m - 1) + (size_t)N * d] = D.vel[3 * (m - 1) + d];
+    }
+    o.neighbours = D.neigh;
+    return PIBM_OK;
+}
+
 bool setup(Orc &o, const pibm_params *prm, const pibm_particles *parts) {
     o.prm = *prm;
     if (prm->my <= 0 || (prm->my % 2) != 0) { g_err = "my must be positive and even"; return false; }
@@ -384,7 +681,17 @@ bool setup(Orc &o, const pibm_params *prm, const pibm_particles *parts) {
         o.phistream = prm->phistream;
         dt_tmp_diff = (o.dx * o.dx * (1.0 - o.maxvolfrac)) / o.gamma_s;
     }
-    neighbor_search(o);
+    o.moving = prm->imove == 1 && o.nbody > 0;
+    if (o.moving) {
+        // des_time_march(.TRUE.) (initialize_flo.F90:631-639): the DEM arrays,
+        // cells and the first neighbour search
+        dem_init(o);
+        dem_cells(o.dem);
+        if (!dem_search(o.dem)) return false;
+        o.neighbours = o.dem.neigh;
+    } else {
+        neighbor_search(o);
+    }
     update_nrpr(o);
     o.dt = std::min(std::min(dt_tmp_conv, dt_tmp_vis), std::min(dt_tmp_grav, dt_tmp_diff));
     o.dt = prm->cfl * o.dt;
@@ -509,6 +816,17 @@ void compute_new_timestep(Orc &o, int rks) {
     double dtnew;
     if (umax_tmp * o.dt / o.dx > o.cfl_max) dtnew = o.cfl_max * o.dx / umax_tmp;
     else dtnew = o.dt;
+    if (o.moving) {
+        // particle speed limit (dependent_functions.F90:1156-1164); the new dt
+        // is taken from the fluid speed, as the reference writes it
+        double up_max = SMALL_NUMBER;
+        for (int m = 1; m <= o.nbody; ++m) {
+            double s2 = 0.0;
+            for (int d = 1; d <= 3; ++d) s2 = s2 + o.VB(m, d) * o.VB(m, d);
+            up_max = std::max(up_max, std::sqrt(s2));
+        }
+        if (up_max * o.dt / o.dx > o.cfl_max) dtnew = o.cfl_max * o.dx / umax_tmp;
+    }
     double ufmean_temp[3];
     for (int d = 0; d < 3; ++d) ufmean_temp[d] = uf[d] / (double)o.count_fluid;
     for (int d = 0; d < 3; ++d) { o.ufmean_old[d] = o.ufmean[d]; o.ufmean[d] = ufmean_temp[d]; }
@@ -825,11 +1143,25 @@ void compute_mpg_at_n(Orc &o, int rks) {
     o.pres_drag = std::sqrt(pa[0] * pa[0] + pa[1] * pa[1] + pa[2] * pa[2]) / norm_factor / (1.0 - o.maxvolfrac);
     o.visc_drag = std::sqrt(va[0] * va[0] + va[1] * va[1] + va[2] * va[2]) / norm_factor / (1.0 - o.maxvolfrac);
     o.total_drag = o.pres_drag + o.visc_drag;
+    const double rhof = o.prm.rhof, rhos = o.prm.rhos, mvf = o.mean_volfrac;
     if (!o.prm.set_mpg) {
-        for (int d = 0; d < 3; ++d)
-            o.mpg[d] = o.cf * (o.ufmean_des[d] - o.ufmean[d]) + (o.pres_total[d] / o.voldom - (o.visc_total[d]) / o.voldom) / (1.0 - o.maxvolfrac);
+        if (o.moving) {
+            for (int d = 0; d < 3; ++d) {
+                double g = o.cf * (o.ufmean_des[d] - o.ufmean[d]) + o.cf * (o.usmean[d] - o.usmean_des[d]);
+                g = g + (o.pres_total[d] - (o.visc_total[d])) * (1.0 / (rhof * (1.0 - mvf)) + 1.0 / (mvf * rhos)) / o.voldom;
+                g = g / (1.0 / rhof - 1.0 / rhos);
+                o.mpg[d] = g;
+                o.frame_accln[d] = -o.mpg[d] / rhos - (o.pres_total[d] - o.visc_total[d]) / (mvf * rhos * o.voldom) + o.cf * (o.usmean_des[d] - o.usmean[d]);
+            }
+        } else {
+            for (int d = 0; d < 3; ++d)
+                o.mpg[d] = o.cf * (o.ufmean_des[d] - o.ufmean[d]) + (o.pres_total[d] / o.voldom - (o.visc_total[d]) / o.voldom) / (1.0 - o.maxvolfrac);
+        }
         if (o.prm.include_frmeanfluid)
             for (int d = 0; d < 3; ++d) o.mpg[d] = o.mpg[d] + o.frmeanfluid[d];
+    } else if (o.moving) {
+        for (int d = 0; d < 3; ++d)
+            o.frame_accln[d] = -o.mpg[d] / rhos - (o.pres_total[d] - o.visc_total[d]) / (mvf * rhos * o.voldom) + o.cf * (o.usmean_des[d] - o.usmean[d]);
     }
     const double c12 = o.coef[0] + o.coef[1];
     for (int m = 1; m <= o.nbody; ++m) {
@@ -937,6 +1269,12 @@ void calc_inner_reversal_forcing(Orc &o, int m, double da2) {
 int bcset(Orc &o, int rks) {
     calc_visc(o);
     compute_mpg_at_n(o, rks);
+    if (o.moving) {
+        const int rc = des_time_march(o);
+        if (rc) return rc;
+        grid_nodes_insphere(o);
+        update_nrpr(o);
+    }
     calc_pgrad(o);
     std::fill(o.fr.begin(), o.fr.end(), 0.0);
     for (int d = 0; d < 3; ++d) { o.frmean[d] = 0; o.frmeanfluid[d] = 0; }
@@ -1186,6 +1524,8 @@ int velstep(Orc &o, int rks) {
     o.divmax = 0.0;
     for (double v : divline) o.divmax = std::max(o.divmax, v);
     for (int d = 0; d < 3; ++d) o.umean[d] = o.umean[d] + (-o.mpg[d] + o.frmean[d] - o.frame_accln[d]) * dt;
+    if (o.moving)
+        for (int d = 0; d < 3; ++d) { o.frame_vel[d] = o.frame_vel[d] + o.frame_accln[d] * dt; o.frame_pos[d] = o.frame_pos[d] + o.frame_vel[d] * dt; }
     return bad ? PIBM_ERR_PIVOT : PIBM_OK;
 }
 
@@ -1770,6 +2110,29 @@ extern "C" int orc_get_scalar(void *h, double *phif, double *flux_body, double *
 }
 
 // sizes of the ABI structs as compiled from include/pibm.h (for the ctypes mirror test)
+// DEM lists in the reference layout NEIGHBOURS/PN/PV(nbody, maxn): column 1 the
+// count (PV: 1), columns 2.. 1-based particle numbers, then -1 (PV: 0).
+extern "C" int orc_get_contacts(void *h, int maxn, int32_t *neigh, int32_t *pn, int32_t *pv) {
+    Orc &o = *(Orc *)h;
+    if (!o.moving) return PIBM_ERR_ARG;
+    const Dem &D = o.dem;
+    const int N = D.N;
+    for (int l = 0; l < N; ++l)
+        if ((int)D.neigh[l].size() + 1 > maxn || (int)D.pn[l].size() + 1 > maxn) return PIBM_ERR_ARG;
+    for (int l = 0; l < N; ++l) {
+        neigh[l] = (int32_t)D.neigh[l].size();
+        pn[l] = (int32_t)D.pn[l].size();
+        pv[l] = 1;
+        for (int c = 1; c < maxn; ++c) {
+            const size_t q = (size_t)l + (size_t)N * c;
+            neigh[q] = c - 1 < (int)D.neigh[l].size() ? D.neigh[l][c - 1] + 1 : -1;
+            pn[q] = c - 1 < (int)D.pn[l].size() ? D.pn[l][c - 1] + 1 : -1;
+            pv[q] = c - 1 < (int)D.pv[l].size() ? D.pv[l][c - 1] : 0;
+        }
+    }
+    return PIBM_OK;
+}
+
 extern "C" int orc_sizeof(int which) {
     switch (which) {
         case 0: return (int)sizeof(pibm_params);

@@ -157,6 +157,16 @@ class Solver:
         _check(load_library().pibm_get_particles(self.h, *[_dp(a) for a in out]))
         return [a.reshape(3, n).T.copy() for a in out]
 
+    def get_contacts(self, maxn: int = 37) -> dict:
+        """Moving particles: the DEM lists NEIGHBOURS, PN, PV in the reference
+        layout (nbody, maxn), returned as arrays [column][particle] (column 0
+        the count, then 1-based particle numbers; -1 / 0 fill)."""
+        n = self.nbody
+        out = {k: np.zeros((maxn, n), dtype=np.int32) for k in ("neighbours", "pn", "pv")}
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        _check(load_library().pibm_get_contacts(self.h, maxn, ip(out["neighbours"]), ip(out["pn"]), ip(out["pv"])))
+        return out
+
     def get_scalar(self) -> dict:
         """Passive scalar: phif complex (mz, my2, nx+1) (the reference's
         (nx+1,my2,mz) array in C order), per-sphere surface flux, heat_ratio,

@@ -15,6 +15,7 @@ PIBM_ERR_NEIGH_OVERFLOW = -6
 PIBM_ERR_TIMEOUT = -7
 PIBM_ERR_CUDA = -8
 PIBM_ERR_NOMEM = -9
+PIBM_ERR_SPREAD_OVERFLOW = -10
 
 ERROR_NAMES = {
     PIBM_ERR_ARG: "PIBM_ERR_ARG",
@@ -26,6 +27,7 @@ ERROR_NAMES = {
     PIBM_ERR_TIMEOUT: "PIBM_ERR_TIMEOUT",
     PIBM_ERR_CUDA: "PIBM_ERR_CUDA",
     PIBM_ERR_NOMEM: "PIBM_ERR_NOMEM",
+    PIBM_ERR_SPREAD_OVERFLOW: "PIBM_ERR_SPREAD_OVERFLOW",
 }
 
 PIBM_SCHEME_CENTER = 0
@@ -102,7 +104,7 @@ class pibm_info(C.Structure):
 EXPORTED = [
     "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed",
     "pibm_run_profiled", "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev",
-    "pibm_get_fluid_mask",
+    "pibm_get_fluid_mask", "pibm_get_contacts",
     "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
     "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time", "pibm_batch_member",
     "pibm_batch_destroy",
@@ -125,6 +127,7 @@ def bind(lib):
     lib.pibm_get_scalar.argtypes = [vp, P(_f64), P(_f64), P(_f64)]
     lib.pibm_get_if_rev.argtypes = [vp, P(C.c_uint8)]
     lib.pibm_get_fluid_mask.argtypes = [vp, P(C.c_uint8)]
+    lib.pibm_get_contacts.argtypes = [vp, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32)]
     lib.pibm_destroy.argtypes = [vp]
     lib.pibm_destroy.restype = None
     lib.pibm_last_error.argtypes = []
@@ -141,6 +144,7 @@ def bind(lib):
     lib.pibm_batch_destroy.restype = None
     for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed", "pibm_run_profiled",
                  "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev", "pibm_get_fluid_mask",
+                 "pibm_get_contacts",
                  "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
         getattr(lib, name).restype = C.c_int
     return lib

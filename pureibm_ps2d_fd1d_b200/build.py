@@ -17,7 +17,10 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libpibm.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels.cu", "scalar.cu", "api.cu"]
+CU_SOURCES = ["kernels.cu", "scalar.cu", "moving.cu", "api.cu"]
+# per-source nvcc flags: the DEM and the moving-geometry rebuild are compiled
+# without multiply-add contraction (bit-equal to a serial evaluation)
+CU_FLAGS = {"moving.cu": ["--fmad=false"]}
 CPP_SOURCES = ["host_setup.cpp"]
 
 
@@ -45,7 +48,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     for src in CU_SOURCES:
         obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
         cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
-               "-Xptxas", "-v" if verbose else "-O3", "-c", os.path.join(CSRC, src), "-o", obj]
+               *CU_FLAGS.get(src, []), "-Xptxas", "-v" if verbose else "-O3", "-c", os.path.join(CSRC, src), "-o", obj]
         subprocess.run(cmd, check=True)
         objs.append(obj)
     for src in CPP_SOURCES:

@@ -242,6 +242,22 @@ def random_array(my: int = 128, dia_cells: float = 20.0, phi: float = 0.2, re: f
     return prm, pts
 
 
+def moving_array(my: int = 64, dia_cells: float = 12.0, nbody: int = 12, seed: int = 11, re: float = 20.0,
+                 rhos: float = 100.0, coeff_rest: float = 0.9, vel_spread: float = 0.1, mc_moves: int = 200,
+                 collision_type: str = "softsphere", vis: float = 0.012):
+    """Freely moving spheres (IMOVE = 1): a random array as random_array and
+    seeded Maxwellian particle velocities of standard deviation
+    vel_spread * uchar per component, with zero mean (the VEL_DISTRIB =
+    'maxwellian' set-up of a freely evolving suspension)."""
+    prm, pts = random_array(my=my, dia_cells=dia_cells, re=re, seed=seed, mc_moves=mc_moves, vis=vis, nbody=nbody)
+    prm.update(imove=1, collision_type=collision_type, rhos=rhos, rhof=1.0, coeff_rest=coeff_rest)
+    rng = np.random.default_rng(seed + 1)
+    uchar = re * vis / float(prm.get("dia_phys", 1.0))
+    vel = rng.normal(0.0, vel_spread * uchar, size=(pts.shape[0], 3))
+    vel -= vel.mean(axis=0, keepdims=True)
+    return prm, pts, vel
+
+
 def fcc_subset(n: int, L: float, dia: float, rng, origin=1.0):
     """n sphere centres on randomly chosen sites of the densest periodic FCC
     lattice of the box whose nearest-neighbour distance is >= dia.  Returns

@@ -7,6 +7,7 @@
 // synchronisation; pibm_step launches one step and reads the diagnostics.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -22,7 +23,9 @@ namespace pibm {
 cudaError_t configure_kernels(int n);
 bool supported_size(int n);
 void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss);
-int kernels_per_step(const Geo &g);
+int kernels_per_step(const Geo &g, const Mov &m);
+void enqueue_dem_init(const Mov &m, Scal *sc, cudaStream_t s);
+cudaError_t configure_moving_kernels(const Mov &m);
 void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s);
 void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStream_t s);
 void enqueue_f2d(const double2 *f, double2 *d, int nx, int nxf, int PS, int ncomp, cudaStream_t s);
@@ -97,6 +100,83 @@ struct pibm_handle {
     }
 };
 
+// Moving particles: DEM state on the device and the first neighbour search
+// of des_time_march(.TRUE.) (DES_INIT_ARRAYS positions, FIND_CELL_INDEX).
+static int setup_moving(pibm_handle *h) {
+    const RunSetup &S = h->S;
+    Geo &g = h->g;
+    Mov &m = h->b.mov;
+    std::memset(&m, 0, sizeof(m));
+    const int N = S.nbody;
+    m.N = N;
+    m.maxn = 30 + 1 + 6;   // MN + 1 + NWALLS (collision_mod.F90:508)
+    m.soft = S.dem_soft;
+    m.cx = S.dem_cx; m.cy = S.dem_cy; m.cz = S.dem_cz;
+    m.ncell = (m.cx - 1) * (m.cy - 1) * (m.cz - 1);
+    m.dxc = S.dem_dxc; m.dyc = S.dem_dyc; m.dzc = S.dem_dzc;
+    m.LXs = S.dem_LXs; m.LYs = S.dem_LYs; m.LZs = S.dem_LZs;
+    m.XL = S.doml[0]; m.YL = S.doml[1]; m.ZL = S.doml[2];
+    m.kn = S.dem_kn; m.eta_n = S.dem_eta_n; m.rad = S.dem_rad; m.pmass = S.dem_pmass; m.pvol = S.dem_pvol;
+    m.rhof = h->prm.rhof; m.dtsolid = S.dem_dtsolid; m.max_radius = S.dem_rad;
+    m.max_factor = m.soft ? std::max(1, (int)(S.dt / m.dtsolid)) : 1;
+    m.kmax = S.my >= 256 ? 32 : 48;
+    if (m.ncell > 8192 || 3 * m.ncell + 1 + N > 40000)
+        return fail(PIBM_ERR_ARG, "moving particles: coarse DEM grid or particle count too large for the binning kernel");
+    std::vector<double> pos(3 * (size_t)N);
+    std::vector<int> pijk(3 * (size_t)N);
+    const double dc[3] = {m.dxc, m.dyc, m.dzc};
+    const int cm[3] = {m.cx, m.cy, m.cz};
+    for (int l = 0; l < N; ++l) {
+        pos[3 * l + 0] = (S.xc[l] + 0.0 - 1.0) * S.dx;
+        pos[3 * l + 1] = (S.xc[l + (size_t)N] - 1.0) * S.dx;
+        pos[3 * l + 2] = (S.xc[l + 2 * (size_t)N] - 1.0) * S.dx;
+        for (int d = 0; d < 3; ++d) pijk[3 * l + d] = std::min((int)(pos[3 * l + d] / dc[d]) + 2, cm[d]);
+    }
+    std::vector<double> vel(3 * (size_t)N);
+    for (int l = 0; l < N; ++l)
+        for (int d = 0; d < 3; ++d) vel[3 * l + d] = S.vel[l + (size_t)d * N];
+    int rc = PIBM_OK;
+    auto guard = [&](cudaError_t e, const char *what) -> bool {
+        if (e != cudaSuccess) { rc = fail(PIBM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)); return false; }
+        return true;
+    };
+    const size_t NL = (size_t)N * m.maxn, nodes = (size_t)g.nx * g.RS;
+    const int one = 1;
+    bool ok = guard(h->alloc(&m.pos, 3 * (size_t)N), "dem pos") && guard(h->alloc(&m.pos_old, 3 * (size_t)N), "dem pos") &&
+              guard(h->alloc(&m.vel, 3 * (size_t)N), "dem vel") && guard(h->alloc(&m.vel_old, 3 * (size_t)N), "dem vel") &&
+              guard(h->alloc(&m.pijk, 3 * (size_t)N), "dem cells") && guard(h->alloc(&m.neigh, NL), "dem neighbours") &&
+              guard(h->alloc(&m.ncnt, (size_t)N), "dem neighbours") && guard(h->alloc(&m.pn, NL), "dem contacts") &&
+              guard(h->alloc(&m.pv, NL), "dem contacts") && guard(h->alloc(&m.pncnt, (size_t)N), "dem contacts") &&
+              guard(h->alloc(&m.pn2, NL), "dem contacts") && guard(h->alloc(&m.pv2, NL), "dem contacts") &&
+              guard(h->alloc(&m.pncnt2, (size_t)N), "dem contacts") && guard(h->alloc(&m.cstart, (size_t)m.ncell + 1), "dem cells") &&
+              guard(h->alloc(&m.clist, (size_t)N), "dem cells") && guard(h->alloc(&m.factor, 1), "dem factor") &&
+              guard(h->alloc(&m.dts, 1), "dem dts") && guard(h->alloc(&m.revflag, (size_t)N * S.nbnd), "revflag") &&
+              guard(h->alloc(&m.nrpr, (size_t)N), "nrpr") && guard(h->alloc(&m.ptoff, (size_t)N), "ptoff") &&
+              guard(h->alloc(&m.spcnt, nodes), "spread counts") && guard(h->alloc(&m.spbuf, nodes * (size_t)m.kmax), "spread buckets") &&
+              guard(cudaMemcpy(m.pos, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice), "dem pos") &&
+              guard(cudaMemcpy(m.pos_old, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice), "dem pos") &&
+              guard(cudaMemcpy(m.vel, vel.data(), vel.size() * sizeof(double), cudaMemcpyHostToDevice), "dem vel") &&
+              guard(cudaMemcpy(m.vel_old, vel.data(), vel.size() * sizeof(double), cudaMemcpyHostToDevice), "dem vel") &&
+              guard(cudaMemcpy(m.pijk, pijk.data(), pijk.size() * sizeof(int), cudaMemcpyHostToDevice), "dem cells") &&
+              guard(cudaMemcpy(m.factor, &one, sizeof(int), cudaMemcpyHostToDevice), "dem factor") &&
+              guard(cudaMemcpy(m.revflag, S.if_rev.data(), S.if_rev.size(), cudaMemcpyHostToDevice), "revflag");
+    if (!ok) return rc;
+    m.xc = const_cast<double *>(g.xc);
+    m.vel_ibm = const_cast<double *>(g.vel);
+    m.fluid = const_cast<uint8_t *>(g.fluid);
+    m.pt_m = const_cast<int *>(g.pt_m);
+    m.pt_l = const_cast<int *>(g.pt_l);
+    m.da2 = const_cast<double *>(g.da2);
+    CUDA_OR_FAIL(configure_moving_kernels(m));
+    enqueue_dem_init(m, h->b.sc, h->stream);
+    CUDA_OR_FAIL(cudaGetLastError());
+    Scal sc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    if (sc.status) return fail(sc.status, "moving particles: the first DEM neighbour search failed (list overflow)");
+    return PIBM_OK;
+}
+
 extern "C" {
 
 const char *pibm_last_error(void) { return g_last_error.c_str(); }
@@ -138,6 +218,11 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     g.count_fluid = S.count_fluid; g.ncell = (long long)S.nx * S.my * S.mz;
     for (int d = 0; d < 3; ++d) { g.ufmean_des[d] = S.ufmean_des[d]; g.usmean_des[d] = S.usmean_des[d]; g.usmean_act[d] = S.usmean_des[d]; }
     g.nbody = S.nbody; g.nbnd = S.nbnd; g.npts = (int)S.pt_m.size();
+    g.rhof = prm->rhof; g.rhos = prm->rhos;
+    g.moving = S.moving ? 1 : 0;
+    // moving particles: the point lists are rebuilt every step, sized for all points
+    std::vector<int> pt_m = S.pt_m, pt_l = S.pt_l;
+    if (g.moving) { g.npts = S.nbody * S.nbnd; pt_m.resize((size_t)g.npts, 0); pt_l.resize((size_t)g.npts, 0); }
     g.rb = S.radbdy; g.ri = S.radibdy; g.ro = S.radobdy; g.dr = S.dr;
     g.da1 = 4.0 * 3.14159265358979323846 * ((S.radbdy * S.dx) * (S.radbdy * S.dx)) / (double)S.nbnd;
     g.sphere_vol = 3.14159265358979323846 * std::pow(2.0 * S.radbdy * S.dx, 3.0) / 6.0;
@@ -166,7 +251,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
               guard(h->upload(&g.w2, S.w2), "w2") && guard(h->upload(&g.fluid, fluid_p), "mask") &&
               guard(h->upload(&g.xc, S.xc), "xc") && guard(h->upload(&g.vel, S.vel), "vel") &&
               guard(h->upload(&g.bnd, S.bnd), "bnd") && guard(h->upload(&g.cd, S.cd), "cd") &&
-              guard(h->upload(&g.pt_m, S.pt_m), "pt_m") && guard(h->upload(&g.pt_l, S.pt_l), "pt_l") &&
+              guard(h->upload(&g.pt_m, pt_m), "pt_m") && guard(h->upload(&g.pt_l, pt_l), "pt_l") &&
               guard(h->upload(&g.da2, da2), "da2") && guard(h->upload(&g.sp_node, sp_node_p), "sp_node") &&
               guard(h->upload(&g.sp_ptr, S.sp_ptr), "sp_ptr") && guard(h->upload(&g.sp_ent, S.sp_ent), "sp_ent") &&
               guard(h->alloc(&b.u, 3 * NC), "u") && guard(h->alloc(&b.p, NC), "p") &&
@@ -219,7 +304,11 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     for (int d = 0; d < 3; ++d) { sc.umean[d] = S.umean0[d]; sc.mpg[d] = prm->mpg[d]; }
     sc.dt = S.dt; sc.cf = S.cf; sc.cforig = S.cf; sc.t = 0.0; sc.fold = 0.0; sc.ferror = 1.0;
     sc.heat_ratio = sc.heat_ratio_old = sc.heat_ratio_new = 1.0;
+    sc.count_solid = S.count_solid; sc.count_fluid = S.count_fluid; sc.maxvolfrac = S.maxvolfrac;
+    sc.npts = (int)S.pt_m.size();
+    for (int d = 0; d < 3; ++d) { sc.usmean_act[d] = S.usmean_des[d]; sc.frame_vel[d] = 0.0; sc.frame_pos[d] = 1.0; }
     if (!guard(cudaMemcpy(b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice), "scalars")) { delete h; return rc; }
+    if (g.moving && (rc = setup_moving(h)) != PIBM_OK) { delete h; return rc; }
     *out = h;
     return PIBM_OK;
 }
@@ -231,7 +320,7 @@ int pibm_info_get(pibm_handle *h, pibm_info *info) {
     info->dx = S.dx; info->dt = S.dt; info->radbdy = S.radbdy; info->maxvolfrac = S.maxvolfrac;
     info->count_solid = S.count_solid; info->count_fluid = S.count_fluid;
     info->npts_active = (int32_t)S.pt_m.size();
-    info->kernels_per_step = kernels_per_step(h->g);
+    info->kernels_per_step = kernels_per_step(h->g, h->b.mov);
     return PIBM_OK;
 }
 
@@ -256,7 +345,7 @@ static int fill_report(pibm_handle *h, pibm_step_report *rep) {
         rep->nusselt = sc.nusselt;
         long long s = 0;
         for (int v : h->S.nrpr_active) s += v;
-        rep->nrpr_active_total = s;
+        rep->nrpr_active_total = h->g.moving ? (long long)sc.npts : s;
     }
     if (sc.status) return fail(sc.status, "step reported a solver stop condition");
     return PIBM_OK;
@@ -391,6 +480,15 @@ int pibm_set_state(pibm_handle *h, const pibm_state_view *s) {
     for (int d = 0; d < 3; ++d) { sc.umean[d] = s->umean[d]; sc.mpg[d] = s->mpg[d]; sc.ufmean[d] = s->ufmean[d]; }
     sc.t = s->t; sc.dt = s->dt; sc.cf = s->cf;
     sc.status = 0;
+    if (h->g.moving && h->S.dem_soft) {
+        // the step graphs hold max_factor DEM sub-steps; a larger dt needs more
+        Mov &m = h->b.mov;
+        const int need = std::max(1, (int)(s->dt / m.dtsolid));
+        if (need > m.max_factor) {
+            m.max_factor = need;
+            for (auto &gx : h->graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+        }
+    }
     CUDA_OR_FAIL(cudaMemcpyAsync(h->b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, h->stream));
     CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
     return PIBM_OK;
@@ -403,9 +501,43 @@ int pibm_get_particles(pibm_handle *h, double *pres, double *visc, double *force
     if (pres) CUDA_OR_FAIL(cudaMemcpyAsync(pres, h->b.pres, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (visc) CUDA_OR_FAIL(cudaMemcpyAsync(visc, h->b.visc, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (force) CUDA_OR_FAIL(cudaMemcpyAsync(force, h->b.force, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (h->g.moving) {   // the positions and velocities the DEM has advanced
+        if (xc) CUDA_OR_FAIL(cudaMemcpyAsync(xc, h->g.xc, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        if (vel) CUDA_OR_FAIL(cudaMemcpyAsync(vel, h->g.vel, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
     CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
-    if (xc) std::memcpy(xc, h->S.xc.data(), n * sizeof(double));
-    if (vel) std::memcpy(vel, h->S.vel.data(), n * sizeof(double));
+    if (!h->g.moving) {
+        if (xc) std::memcpy(xc, h->S.xc.data(), n * sizeof(double));
+        if (vel) std::memcpy(vel, h->S.vel.data(), n * sizeof(double));
+    }
+    return PIBM_OK;
+}
+
+int pibm_get_contacts(pibm_handle *h, int32_t maxn, int32_t *neigh, int32_t *pn, int32_t *pv) {
+    if (!h) return fail(PIBM_ERR_ARG, "null handle");
+    if (!h->g.moving) return fail(PIBM_ERR_ARG, "this run has no DEM (IMOVE = 0)");
+    const Mov &m = h->b.mov;
+    const int N = m.N, MX = m.maxn;
+    std::vector<int> nb((size_t)N * MX), nc(N), cn((size_t)N * MX), cv((size_t)N * MX), cc(N);
+    CUDA_OR_FAIL(cudaMemcpyAsync(nb.data(), m.neigh, nb.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaMemcpyAsync(nc.data(), m.ncnt, nc.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaMemcpyAsync(cn.data(), m.pn, cn.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaMemcpyAsync(cv.data(), m.pv, cv.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaMemcpyAsync(cc.data(), m.pncnt, cc.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    for (int l = 0; l < N; ++l)
+        if (nc[l] + 1 > maxn || cc[l] + 1 > maxn) return fail(PIBM_ERR_ARG, "maxn is smaller than a list");
+    for (int l = 0; l < N; ++l) {
+        if (neigh) neigh[l] = nc[l];
+        if (pn) pn[l] = cc[l];
+        if (pv) pv[l] = 1;
+        for (int c = 1; c < maxn; ++c) {
+            const size_t q = (size_t)l + (size_t)N * c;
+            if (neigh) neigh[q] = c - 1 < nc[l] ? nb[(size_t)l * MX + c - 1] + 1 : -1;
+            if (pn) pn[q] = c - 1 < cc[l] ? cn[(size_t)l * MX + c - 1] + 1 : -1;
+            if (pv) pv[q] = c - 1 < cc[l] ? cv[(size_t)l * MX + c - 1] : 0;
+        }
+    }
     return PIBM_OK;
 }
 
@@ -443,6 +575,11 @@ int pibm_get_scalar(pibm_handle *h, double *phif, double *flux_body, double *rat
 
 int pibm_get_if_rev(pibm_handle *h, uint8_t *if_rev) {
     if (!h || !if_rev) return fail(PIBM_ERR_ARG, "null argument");
+    if (h->g.moving) {   // flags of the last step's geometry rebuild
+        CUDA_OR_FAIL(cudaMemcpyAsync(if_rev, h->b.mov.revflag, h->S.if_rev.size(), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+        return PIBM_OK;
+    }
     std::memcpy(if_rev, h->S.if_rev.data(), h->S.if_rev.size());
     return PIBM_OK;
 }
@@ -450,6 +587,16 @@ int pibm_get_if_rev(pibm_handle *h, uint8_t *if_rev) {
 int pibm_get_fluid_mask(pibm_handle *h, uint8_t *mask) {
     if (!h || !mask) return fail(PIBM_ERR_ARG, "null argument");
     const RunSetup &S = h->S;
+    if (h->g.moving) {   // the device mask, stored in plane-transform order
+        std::vector<uint8_t> dev((size_t)S.nx * h->g.RS);
+        CUDA_OR_FAIL(cudaMemcpyAsync(dev.data(), h->g.fluid, dev.size(), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+        for (int i = 0; i < S.nx; ++i)
+            for (int k = 0; k < S.mz; ++k)
+                for (int j = 0; j < S.my; ++j)
+                    mask[(size_t)i + (size_t)S.nx * ((size_t)j + (size_t)S.my * k)] = dev[(size_t)i * h->g.RS + real_offset(S.my, k, j)];
+        return PIBM_OK;
+    }
     for (int i = 0; i < S.nx; ++i)
         for (int k = 0; k < S.mz; ++k)
             for (int j = 0; j < S.my; ++j)

@@ -13,12 +13,13 @@ struct Geo {
     double dx, dx2, rdx2, dx3, vis, nrm;   // nrm = float(my*mz) as in ff2rc
     double c1, c2, c3, c4;
     int scheme, limiter, include_frmeanfluid, revernorm, set_mpg, adaptive;
-    double cfl_max, ramp_frac_time, ucharmod, char_length, voldom, maxvolfrac, mean_volfrac;
+    double cfl_max, ramp_frac_time, ucharmod, char_length, voldom, maxvolfrac, mean_volfrac, rhof, rhos;
     long long count_fluid, ncell;
     int plane_ctas;     // CTAs per plane in the plane kernels
     double ufmean_des[3], usmean_des[3], usmean_act[3];
-    // particles
-    int nbody, nbnd, npts;
+    // particles (moving: the geometry arrays below are rebuilt on the device
+    // every step and npts is the capacity nbody*nbnd; Scal::npts is the count)
+    int nbody, nbnd, npts, moving;
     double rb, ri, ro, dr, da1, sphere_vol;
     // device arrays (read-only)
     const double2 *tw;          // e^{-2 pi i m/my}, m < my (my == mz)
@@ -55,6 +56,40 @@ struct Scal {
     long long nsteps;
     // passive scalar: phi(x + Lx) = phi(x) / heat_ratio
     double heat_ratio, heat_ratio_old, heat_ratio_new, flux_global, nusselt;
+    // particle geometry of the current step (constant for fixed particles):
+    // solid/fluid node counts, solid fraction, active reversal points, mean
+    // particle velocity; frame motion of moving particles
+    long long count_solid, count_fluid;
+    double maxvolfrac;
+    int npts;
+    int dem_substeps;
+    double usmean_act[3], frame_vel[3], frame_pos[3];
+};
+
+
+
+// Moving particles (IMOVE = 1): soft-sphere DEM state and the scratch of the
+// per-step geometry rebuild.  Particle indices are 0-based; list order is the
+// reference's (collision_mod.F90 NEIGHBOURS / PN / PV).
+struct Mov {
+    int N, maxn, soft, max_factor;
+    int cx, cy, cz, ncell;            // coarse grid nodes per direction; physical cells 2..c
+    double dxc, dyc, dzc, LXs, LYs, LZs, XL, YL, ZL;
+    double kn, eta_n, rad, pmass, pvol, rhof, dtsolid, max_radius;
+    double *pos, *pos_old, *vel, *vel_old;    // [3*l + d], physical units
+    int *pijk;                                 // [3*l + d]
+    int *neigh, *ncnt;                         // NEIGHBOURS: [l*maxn + q], q < ncnt[l]
+    int *pn, *pv, *pncnt;                      // contact lists at the start of a sub-step
+    int *pn2, *pv2, *pncnt2;                   // contact lists written by the sub-step
+    int *cstart, *clist;                       // particles per coarse cell, ascending
+    int *factor;                               // [0] sub-steps of this flow step
+    double *dts;                               // [0] sub-step size
+    double *xc, *vel_ibm;                      // the step's xc (grid units) and velbdy, (nbody,3)
+    uint8_t *fluid, *revflag;                  // solid mask; reversal-point activity [m*nbnd + l]
+    int *nrpr, *ptoff, *pt_m, *pt_l;
+    double *da2;
+    int *spcnt, *spbuf;                        // spreading buckets: count and entries per node
+    int kmax;                                  // bucket capacity per node
 };
 
 // Device buffers of one run.
@@ -70,6 +105,7 @@ struct DevBufs {
     double2 *phif, *nls[2], *ffs;
     double *phr, *phimg, *nlr[2], *sdf, *gph, *sfr, *dsx;
     double *spart, *sctb, *sfd, *sdpart, *flux_body;
+    Mov mov;   // moving particles (Geo::moving)
 };
 
 // Side streams of one run: after compute_new_timestep's scalars are known,

@@ -285,12 +285,60 @@ void build_scalar_evals(RunSetup &S, bool all_nodes) {
     S.ssp_ptr.push_back((int)ent.size());
 }
 
+// DEM constants for moving particles: initialize_coarse_grid
+// (collision_mod.F90:346-492: cgrid_fac 1.5, KN = 800000, MEW = 0),
+// DES_INIT_ARRAYS / CFASSIGN (:582-741: masses, KT, the collision time and
+// DTSOLID = TCOLL/50 from the phase diameter) and the pair damping of
+// CALC_FORCE_DES (soft_sphere_coll.F90:408-414), all spheres of one phase.
+static void build_dem(RunSetup &S, const pibm_params &prm) {
+    S.moving = true;
+    S.dem_soft = prm.collision_softsphere ? 1 : 0;
+    const double dxeff = 2.0 * S.radbdy * 1.5 * S.dx;
+    S.dem_cy = std::max((int)std::lround(S.doml[1] / dxeff), 2);
+    S.dem_cx = std::max((int)std::lround(S.doml[0] / dxeff), 2);
+    S.dem_cz = std::max((int)std::lround(S.doml[2] / dxeff), 2);
+    S.dem_dyc = S.doml[1] / (double)(S.dem_cy - 1);
+    S.dem_dxc = S.doml[0] / (double)(S.dem_cx - 1);
+    S.dem_dzc = S.doml[2] / (double)(S.dem_cz - 1);
+    // search periods XE(IMAX1) - XE(1), XE accumulated cell by cell (:471-483, 823-825)
+    double e = 0.0;
+    for (int i = 2; i <= S.dem_cx; ++i) e = e + S.dem_dxc;
+    S.dem_LXs = e;
+    e = 0.0;
+    for (int j = 2; j <= S.dem_cy; ++j) e = e + S.dem_dyc;
+    S.dem_LYs = e;
+    e = 0.0;
+    for (int k = 2; k <= S.dem_cz; ++k) e = e + S.dem_dzc;
+    S.dem_LZs = e;
+    S.dem_kn = 800000.0;
+    S.dem_rad = S.radbdy * S.dx;
+    const double r2 = S.dem_rad * S.dem_rad;
+    S.dem_pvol = (4.0 / 3.0) * kPi * r2 * S.dem_rad;
+    S.dem_pmass = S.dem_pvol * prm.rhos;
+    const double len = std::log(prm.coeff_rest);
+    {
+        const double mi = (kPi * std::pow(prm.dia_phys, 3.0) * prm.rhos) / 6.0;
+        const double meff = (mi * mi) / (mi + mi);
+        double etan = 2.0 * std::sqrt(S.dem_kn * meff) * std::fabs(len);
+        etan = etan / std::sqrt(kPi * kPi + std::pow(len, 2.0));
+        const double tcoll = kPi / std::sqrt(S.dem_kn / meff - std::pow(etan / meff, 2.0) / 4.0);
+        S.dem_dtsolid = std::min(tcoll, kLarge) / 50.0;
+    }
+    {
+        const double mi = (kPi * std::pow(2.0 * S.dem_rad, 3.0) * prm.rhos) / 6.0;
+        const double meff = (mi * mi) / (mi + mi);
+        S.dem_eta_n = 2.0 * std::sqrt(S.dem_kn * meff) * std::fabs(len);
+        S.dem_eta_n = S.dem_eta_n / std::sqrt(kPi * kPi + std::pow(len, 2.0));
+    }
+}
+
 bool setup_run(const pibm_params &prm, const pibm_particles *parts, RunSetup &S, std::string &err) {
     if (prm.my < 4 || (prm.my % 2) != 0) { err = "MY must be an even integer >= 4"; return false; }
     const int mz = prm.mz > 0 ? prm.mz : prm.my;
     if (mz != prm.my) { err = "only MZ == MY is supported"; return false; }
     if (prm.discr_scheme != PIBM_SCHEME_UPWIND && prm.discr_scheme != PIBM_SCHEME_CENTER) { err = "bad discr_scheme"; return false; }
-    if (prm.imove != 0) { err = "moving particles (IMOVE=1) are not supported by this build"; return false; }
+    if (prm.imove != 0 && prm.imove != 1) { err = "IMOVE must be 0 or 1"; return false; }
+    if (prm.imove == 1 && prm.iscalon) { err = "the passive scalar with moving particles (IMOVE=1, ISCALON=1) is not supported by this build"; return false; }
     S.my = prm.my; S.mz = mz; S.mx = S.my + 1; S.mxf = S.mx; S.nx = S.mx - 1; S.my2 = S.my / 2 + 1;
     S.nbody = parts ? parts->nbody : 0;
     if (S.nbody < 0 || (S.nbody > 0 && !parts->xc)) { err = "bad particle list"; return false; }
@@ -344,6 +392,11 @@ bool setup_run(const pibm_params &prm, const pibm_particles *parts, RunSetup &S,
         S.phistream = prm.phistream;
         dt_diff = (S.dx * S.dx * (1.0 - S.maxvolfrac)) / S.gamma_s;
         build_scalar_evals(S, prm.include_frmeanfluid != 0);
+    }
+    if (prm.imove == 1 && S.nbody > 0) {
+        if (!(prm.rhos > 0.0) || !(prm.rhof > 0.0)) { err = "RHOF and RHOS must be positive with IMOVE=1"; return false; }
+        if (prm.collision_softsphere && !(prm.coeff_rest > 0.0)) { err = "COEFF_REST must be positive"; return false; }
+        build_dem(S, prm);
     }
     S.dt = prm.cfl * std::min(std::min(dt_conv, dt_vis), std::min(kLarge, dt_diff));
     S.dt = std::min(S.dt, kLarge);

@@ -47,6 +47,14 @@ struct RunSetup {
     std::vector<int> sev_m, sev_l, sev_c;     // sev_c: 3 cells per evaluation
     std::vector<double> sev_x;                // 3 coordinates per evaluation
     std::vector<int> ssp_node, ssp_ptr, ssp_ent;
+    // moving particles (IMOVE = 1): soft-sphere DEM constants of
+    // initialize_coarse_grid / CFASSIGN (collision_mod.F90:346-741) for one
+    // phase; positions are physical, DES_POS = (XC - 1) * dx
+    bool moving = false;
+    int dem_soft = 0;                          // COLLISION_TYPE = 'softsphere' (else 'none')
+    int dem_cx = 0, dem_cy = 0, dem_cz = 0;    // coarse grid nodes (physical cells 2..c)
+    double dem_dxc = 0, dem_dyc = 0, dem_dzc = 0, dem_LXs = 0, dem_LYs = 0, dem_LZs = 0;
+    double dem_kn = 0, dem_eta_n = 0, dem_rad = 0, dem_pmass = 0, dem_pvol = 0, dem_dtsolid = 0;
 };
 
 bool setup_run(const pibm_params &prm, const pibm_particles *parts, RunSetup &S, std::string &err);

@@ -41,6 +41,10 @@ int scalar_kernels_per_step(const Geo &g);
 // grad p are taken on the spectral planes before the transform (linear).
 // part[i*12 + q]: q 0-2 fluid sums, 3-5 solid sums, 6-8 all sums, 9-11 max |u|.
 // ============================================================================
+void enqueue_moving(const Geo &g, const Mov &m, Scal *sc, const double *pres, const double *visc, cudaStream_t s);
+void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, const double *ctb, double *fr, Scal *sc, cudaStream_t s);
+int moving_kernels_per_step(const Mov &m);
+
 template <int N>
 __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
                                                    double *__restrict__ ubcp, double *__restrict__ pbcp,
@@ -144,15 +148,33 @@ __global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *p
     sc->umax = umax;
     double dtnew = sc->dt;
     if (umax * sc->dt / g.dx > g.cfl_max) dtnew = g.cfl_max * g.dx / umax;
+    if (g.moving) {
+        // particle speed limit (dependent_functions.F90:1156-1164; the new dt
+        // is taken from the fluid speed, as the reference writes it) and the
+        // mean particle velocity (:1185-1193), serial sums over the spheres
+        const int NB = g.nbody;
+        double up_max = kSmallD;
+        for (int m = 0; m < NB; ++m) {
+            double s2 = 0.0;
+            for (int d = 0; d < 3; ++d) s2 = __dadd_rn(s2, __dmul_rn(g.vel[m + d * NB], g.vel[m + d * NB]));
+            up_max = fmax(up_max, sqrt(s2));
+        }
+        if (up_max * sc->dt / g.dx > g.cfl_max) dtnew = g.cfl_max * g.dx / umax;
+        for (int d = 0; d < 3; ++d) {
+            double a = 0.0;
+            for (int m = 0; m < NB; ++m) a = a + g.vel[m + d * NB];
+            sc->usmean_act[d] = a / (double)NB;
+        }
+    }
     for (int d = 0; d < 3; ++d) {
         sc->ufmean_old[d] = sc->ufmean[d];
-        sc->ufmean[d] = red[d] / (double)g.count_fluid;
+        sc->ufmean[d] = red[d] / (double)sc->count_fluid;
         sc->dufmeandt[d] = -sc->cf * (sc->ufmean[d] - sc->ufmean_old[d]);
     }
     double ms[3];
     for (int d = 0; d < 3; ++d) {
-        sc->usmean[d] = g.nbody > 0 ? (g.mean_volfrac * g.usmean_act[d]) / g.mean_volfrac : 0.0;
-        ms[d] = (1.0 - g.maxvolfrac) * (sc->usmean[d] - sc->ufmean[d]);
+        sc->usmean[d] = g.nbody > 0 ? (g.mean_volfrac * sc->usmean_act[d]) / g.mean_volfrac : 0.0;
+        ms[d] = (1.0 - sc->maxvolfrac) * (sc->usmean[d] - sc->ufmean[d]);
     }
     sc->mixmeanslipmod = sqrt(ms[0] * ms[0] + ms[1] * ms[1] + ms[2] * ms[2]);
     if (g.adaptive) sc->dt = dtnew;
@@ -467,15 +489,29 @@ __global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, d
         const double nf = (3.0 * 3.14159265358979323846 * g.vis * (sc->mixmeanslipmod + kSmallD) * g.char_length) * (double)NB;
         const double pa = sqrt(tot[6] * tot[6] + tot[7] * tot[7] + tot[8] * tot[8]);
         const double va = sqrt(tot[3] * tot[3] + tot[4] * tot[4] + tot[5] * tot[5]);
-        sc->pres_drag = pa / nf / (1.0 - g.maxvolfrac);
-        sc->visc_drag = va / nf / (1.0 - g.maxvolfrac);
+        sc->pres_drag = pa / nf / (1.0 - sc->maxvolfrac);
+        sc->visc_drag = va / nf / (1.0 - sc->maxvolfrac);
         sc->total_drag = sc->pres_drag + sc->visc_drag;
+        const double rhof = g.rhof, rhos = g.rhos, mvf = g.mean_volfrac;
         if (!g.set_mpg) {
             for (int d = 0; d < 3; ++d) {
-                sc->mpg[d] = sc->cf * (g.ufmean_des[d] - sc->ufmean[d]) +
-                             (sc->pres_total[d] / g.voldom - (sc->visc_total[d]) / g.voldom) / (1.0 - g.maxvolfrac);
+                if (g.moving) {
+                    // moving particles: mpg and the frame acceleration (:389-398)
+                    double m = sc->cf * (g.ufmean_des[d] - sc->ufmean[d]) + sc->cf * (sc->usmean[d] - g.usmean_des[d]);
+                    m = m + (sc->pres_total[d] - (sc->visc_total[d])) * (1.0 / (rhof * (1.0 - mvf)) + 1.0 / (mvf * rhos)) / g.voldom;
+                    sc->mpg[d] = m / (1.0 / rhof - 1.0 / rhos);
+                    sc->frame_accln[d] = -sc->mpg[d] / rhos - (sc->pres_total[d] - sc->visc_total[d]) / (mvf * rhos * g.voldom) +
+                                         sc->cf * (g.usmean_des[d] - sc->usmean[d]);
+                } else {
+                    sc->mpg[d] = sc->cf * (g.ufmean_des[d] - sc->ufmean[d]) +
+                                 (sc->pres_total[d] / g.voldom - (sc->visc_total[d]) / g.voldom) / (1.0 - sc->maxvolfrac);
+                }
                 if (g.include_frmeanfluid) sc->mpg[d] = sc->mpg[d] + sc->frmeanfluid[d];
             }
+        } else if (g.moving) {
+            for (int d = 0; d < 3; ++d)
+                sc->frame_accln[d] = -sc->mpg[d] / rhos - (sc->pres_total[d] - sc->visc_total[d]) / (mvf * rhos * g.voldom) +
+                                     sc->cf * (g.usmean_des[d] - sc->usmean[d]);
         }
     }
     __syncthreads();
@@ -522,7 +558,7 @@ __global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict_
     __shared__ double scr[32];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     double fm[3] = {0, 0, 0}, ffl[3] = {0, 0, 0};
-    if (p < g.npts && !sc->status) {
+    if (p < sc->npts && !sc->status) {
         const int m = g.pt_m[p], l = g.pt_l[p], NB = g.nbody;
         const size_t CR = (size_t)g.nx * RP<N>::RSP;
         double xli[3], xlo[3], xpi[3], snorm[3];
@@ -619,7 +655,7 @@ __global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *b
         a = block_sum(a, scr);
         if (threadIdx.x == 0) {
             if (q < 3) sc->frmean[q] = a / (double)g.ncell;
-            else sc->frmeanfluid[q - 3] = a / (double)g.count_fluid;
+            else sc->frmeanfluid[q - 3] = a / (double)sc->count_fluid;
         }
     }
 }
@@ -1004,6 +1040,11 @@ static size_t lines_smem() { return (size_t)(NX + 5 * LinesCfg<NX>::LT * (NX + 1
 __global__ void k_scal_d(Geo g, Scal *sc) {
     if (threadIdx.x != 0 || sc->status) return;
     for (int d = 0; d < 3; ++d) sc->umean[d] = sc->umean[d] + (-sc->mpg[d] + sc->frmean[d] - sc->frame_accln[d]) * sc->dt;
+    if (g.moving)
+        for (int d = 0; d < 3; ++d) {   // steptheflow.F90:101-104
+            sc->frame_vel[d] = sc->frame_vel[d] + sc->frame_accln[d] * sc->dt;
+            sc->frame_pos[d] = sc->frame_pos[d] + sc->frame_vel[d] * sc->dt;
+        }
     const double dm = __longlong_as_double((long long)sc->divmax_bits);
     if (!(dm == dm) || !(sc->umean[0] == sc->umean[0]) || !(sc->mpg[0] == sc->mpg[0])) sc->status = PIBM_ERR_NAN;
     sc->nsteps += 1;
@@ -1190,12 +1231,14 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
             k_drag<N><<<g.nbody * kDragSplit, 256, 0, s>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
             k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
         }
+        if (g.moving) enqueue_moving(g, b.mov, b.sc, b.pres, b.visc, s);
         mark(3);
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {
             k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.ctb, b.blockpart);
             k_scal_c<<<1, 256, 0, s>>>(g, b.sc, b.blockpart, nbk);
-            if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.ctb, b.fr, b.sc);
+            if (g.moving) enqueue_spread_dyn(g, b.mov, b.rec, b.ctb, b.fr, b.sc, s);
+            else if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.ctb, b.fr, b.sc);
         }
         mark(4);
         launch_planes<N>(k_ff<N>, g.nx, 3, s, g, (const double *)b.fr, b.ff, b.sc);
@@ -1215,9 +1258,10 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
 }
 
 // Kernels launched per step (for launch accounting).
-int kernels_per_step(const Geo &g) {
+int kernels_per_step(const Geo &g, const Mov &m) {
     int n = 6;   // a0, scal_a, flux, nl, lines, scal_d
-    if (g.nbody > 0) n += 3 + (g.npts > 0 ? 2 + (g.sp_nnodes > 0 ? 1 : 0) : 0);
+    if (g.nbody > 0) n += 3 + (g.npts > 0 ? 2 + (g.sp_nnodes > 0 || g.moving ? 1 : 0) : 0);
+    if (g.moving) n += moving_kernels_per_step(m);
     return n + scalar_kernels_per_step(g);
 }
 
