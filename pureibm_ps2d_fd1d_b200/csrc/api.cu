@@ -95,7 +95,7 @@ struct pibm_handle {
         if (stream) cudaStreamDestroy(stream);
         if (ss.side) cudaStreamDestroy(ss.side);
         if (ss.scal) cudaStreamDestroy(ss.scal);
-        for (cudaEvent_t e : {ss.fork, ss.drag_done, ss.scal_done}) if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : {ss.fork, ss.drag_done, ss.scal_done, ss.geo_done}) if (e) cudaEventDestroy(e);
         for (void *q : allocs) cudaFree(q);
     }
 };
@@ -161,6 +161,14 @@ static int setup_moving(pibm_handle *h) {
               guard(cudaMemcpy(m.factor, &one, sizeof(int), cudaMemcpyHostToDevice), "dem factor") &&
               guard(cudaMemcpy(m.revflag, S.if_rev.data(), S.if_rev.size(), cudaMemcpyHostToDevice), "revflag");
     if (!ok) return rc;
+    if (g.scal) {
+        ok = guard(h->alloc(&m.sev_cnt, (size_t)N), "sev counts") && guard(h->alloc(&m.sev_off, (size_t)N), "sev offsets") &&
+             guard(h->alloc(&m.sspcnt, nodes), "scalar spread counts") &&
+             guard(h->alloc(&m.sspbuf, nodes * (size_t)m.kmax), "scalar spread buckets");
+        if (!ok) return rc;
+        m.sev_m = const_cast<int *>(g.sev_m); m.sev_l = const_cast<int *>(g.sev_l);
+        m.sev_c = const_cast<int *>(g.sev_c); m.sev_x = const_cast<double *>(g.sev_x);
+    }
     m.xc = const_cast<double *>(g.xc);
     m.vel_ibm = const_cast<double *>(g.vel);
     m.fluid = const_cast<uint8_t *>(g.fluid);
@@ -201,7 +209,8 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
         !guard(cudaStreamCreateWithFlags(&h->ss.scal, cudaStreamNonBlocking), "cudaStreamCreate") ||
         !guard(cudaEventCreateWithFlags(&h->ss.fork, cudaEventDisableTiming), "cudaEventCreate") ||
         !guard(cudaEventCreateWithFlags(&h->ss.drag_done, cudaEventDisableTiming), "cudaEventCreate") ||
-        !guard(cudaEventCreateWithFlags(&h->ss.scal_done, cudaEventDisableTiming), "cudaEventCreate")) { delete h; return rc; }
+        !guard(cudaEventCreateWithFlags(&h->ss.scal_done, cudaEventDisableTiming), "cudaEventCreate") ||
+        !guard(cudaEventCreateWithFlags(&h->ss.geo_done, cudaEventDisableTiming), "cudaEventCreate")) { delete h; return rc; }
     Geo &g = h->g;
     std::memset(&g, 0, sizeof(g));
     g.nx = S.nx; g.my = S.my; g.mz = S.mz; g.my2 = S.my2;
@@ -273,6 +282,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
         // spreading map in plane-transform order, and phi = 1 (scalar_init.F90:136-152)
         g.scal = 1; g.gamma_s = S.gamma_s; g.phisurf = S.phisurf; g.phistream = S.phistream;
         g.nsev = (int)S.sev_m.size();
+        if (g.moving) g.nsev = 2 * S.nbody * S.nbnd;   // rebuilt every step: capacity
         g.ssp_nnodes = (int)S.ssp_node.size();
         std::vector<int> ssp_node_p(S.ssp_node.size());
         for (size_t q = 0; q < S.ssp_node.size(); ++q) {
@@ -282,8 +292,11 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
         std::vector<double2> phi0(NC, make_double2(0.0, 0.0));
         for (int i = 0; i < g.nx; ++i) phi0[(size_t)i * g.PS] = make_double2(1.0, 0.0);
         const size_t NR1 = (size_t)(g.nx + 1) * g.RS, nsev = (size_t)g.nsev;
-        ok = guard(h->upload(&g.sev_m, S.sev_m), "sev_m") && guard(h->upload(&g.sev_l, S.sev_l), "sev_l") &&
-             guard(h->upload(&g.sev_c, S.sev_c), "sev_c") && guard(h->upload(&g.sev_x, S.sev_x), "sev_x") &&
+        std::vector<int> sev_m = S.sev_m, sev_l = S.sev_l, sev_c = S.sev_c;
+        std::vector<double> sev_x = S.sev_x;
+        if (g.moving) { sev_m.resize(nsev, 0); sev_l.resize(nsev, 0); sev_c.resize(3 * nsev, 0); sev_x.resize(3 * nsev, 0.0); }
+        ok = guard(h->upload(&g.sev_m, sev_m), "sev_m") && guard(h->upload(&g.sev_l, sev_l), "sev_l") &&
+             guard(h->upload(&g.sev_c, sev_c), "sev_c") && guard(h->upload(&g.sev_x, sev_x), "sev_x") &&
              guard(h->upload(&g.ssp_node, ssp_node_p), "ssp_node") && guard(h->upload(&g.ssp_ptr, S.ssp_ptr), "ssp_ptr") &&
              guard(h->upload(&g.ssp_ent, S.ssp_ent), "ssp_ent") &&
              guard(h->alloc(&b.phif, NC), "phif") && guard(h->alloc(&b.nls[0], NC), "nls0") &&
@@ -306,6 +319,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     sc.heat_ratio = sc.heat_ratio_old = sc.heat_ratio_new = 1.0;
     sc.count_solid = S.count_solid; sc.count_fluid = S.count_fluid; sc.maxvolfrac = S.maxvolfrac;
     sc.npts = (int)S.pt_m.size();
+    sc.nsev = (int)S.sev_m.size();
     for (int d = 0; d < 3; ++d) { sc.usmean_act[d] = S.usmean_des[d]; sc.frame_vel[d] = 0.0; sc.frame_pos[d] = 1.0; }
     if (!guard(cudaMemcpy(b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice), "scalars")) { delete h; return rc; }
     if (g.moving && (rc = setup_moving(h)) != PIBM_OK) { delete h; return rc; }

@@ -63,6 +63,7 @@ struct Scal {
     double maxvolfrac;
     int npts;
     int dem_substeps;
+    int nsev, pad2;
     double usmean_act[3], frame_vel[3], frame_pos[3];
 };
 
@@ -90,6 +91,11 @@ struct Mov {
     double *da2;
     int *spcnt, *spbuf;                        // spreading buckets: count and entries per node
     int kmax;                                  // bucket capacity per node
+    // passive scalar with moving particles: reversal-point evaluations per
+    // sphere and in total, and the scalar forcing's spreading buckets
+    int *sev_cnt, *sev_off, *sev_m, *sev_l, *sev_c;
+    double *sev_x;
+    int *sspcnt, *sspbuf;
 };
 
 // Device buffers of one run.
@@ -110,10 +116,12 @@ struct DevBufs {
 
 // Side streams of one run: after compute_new_timestep's scalars are known,
 // the drag quadrature (and mpg) and the passive-scalar step depend only on
-// the real fields of that step, so they run beside the nonlinear term.
+// the real fields of that step, so they run beside the nonlinear term (with
+// moving particles the scalar waits for the step's new geometry).
 struct StepStreams {
     cudaStream_t side = nullptr, scal = nullptr;
     cudaEvent_t fork = nullptr, drag_done = nullptr, scal_done = nullptr;
+    cudaEvent_t geo_done = nullptr;   // moving particles: the step's geometry is rebuilt
 };
 
 }  // namespace pibm

@@ -338,7 +338,6 @@ bool setup_run(const pibm_params &prm, const pibm_particles *parts, RunSetup &S,
     if (mz != prm.my) { err = "only MZ == MY is supported"; return false; }
     if (prm.discr_scheme != PIBM_SCHEME_UPWIND && prm.discr_scheme != PIBM_SCHEME_CENTER) { err = "bad discr_scheme"; return false; }
     if (prm.imove != 0 && prm.imove != 1) { err = "IMOVE must be 0 or 1"; return false; }
-    if (prm.imove == 1 && prm.iscalon) { err = "the passive scalar with moving particles (IMOVE=1, ISCALON=1) is not supported by this build"; return false; }
     S.my = prm.my; S.mz = mz; S.mx = S.my + 1; S.mxf = S.mx; S.nx = S.mx - 1; S.my2 = S.my / 2 + 1;
     S.nbody = parts ? parts->nbody : 0;
     if (S.nbody < 0 || (S.nbody > 0 && !parts->xc)) { err = "bad particle list"; return false; }

@@ -1214,7 +1214,7 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
             k_scal_b<<<1, 256, 0, ss->side>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
             cudaEventRecord(ss->drag_done, ss->side);
         }
-        if (g.scal) {
+        if (g.scal && !g.moving) {
             cudaStreamWaitEvent(ss->scal, ss->fork, 0);
             enqueue_scalar(g, b, cur, ss->scal);
             cudaEventRecord(ss->scal_done, ss->scal);
@@ -1231,7 +1231,15 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
             k_drag<N><<<g.nbody * kDragSplit, 256, 0, s>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
             k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
         }
-        if (g.moving) enqueue_moving(g, b.mov, b.sc, b.pres, b.visc, s);
+        if (g.moving) {
+            enqueue_moving(g, b.mov, b.sc, b.pres, b.visc, s);
+            if (fork && g.scal) {   // the scalar step needs the new geometry
+                cudaEventRecord(ss->geo_done, s);
+                cudaStreamWaitEvent(ss->scal, ss->geo_done, 0);
+                enqueue_scalar(g, b, cur, ss->scal);
+                cudaEventRecord(ss->scal_done, ss->scal);
+            }
+        }
         mark(3);
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {

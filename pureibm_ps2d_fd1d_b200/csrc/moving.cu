@@ -571,6 +571,163 @@ __global__ void __launch_bounds__(256) k_spread_dyn(Geo g, Mov m, const double *
     for (int n = 0; n < 3; ++n) fr[n * CR + node] = acc[n];
 }
 
+// ---------------------------------------------------------------------------
+// Passive scalar with moving particles: the reversal-point evaluations of
+// calc_inner_rev_data (SRC/SCALAR/bc_scalar.F90:558-932, serial branch) for
+// the step's active points.  Inner point x = xc + bnd*radibdy, its cell
+// wrapped into 1..nx (WEST/EAST_PERIODIC_IMAGE, ibm.h:148-149); a point in
+// cell nx is evaluated a second time one period west (EAST_PERIODIC_IMAGE_MOD,
+// ibm.h:150).  Evaluations are ordered (sphere, point, evaluation).
+// ---------------------------------------------------------------------------
+struct ScalEval {
+    double x[3];
+    int c[3], nev;
+};
+__device__ __forceinline__ ScalEval scal_eval(const Geo &g, const Mov &m, int s, int l) {
+    ScalEval e;
+    const int NB = g.nbody, nx = g.nx, mxf = g.nx + 1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        e.x[d] = m.xc[s + d * NB] + g.bnd[3 * l + d] * g.ri;
+        e.c[d] = cell_of(e.x[d]);
+    }
+    int pct = e.c[0];
+    double xlt = e.x[0];
+    if (!(1 <= pct && pct <= nx)) {
+        if (e.c[0] < 1) { pct = mxf + e.c[0] - 1; xlt = mxf + e.x[0] - 1; }
+        else if (e.c[0] >= mxf) { pct = e.c[0] - (mxf - 1); xlt = e.x[0] - (mxf - 1); }
+    }
+    e.nev = pct == nx ? 2 : 1;
+    e.c[0] = pct;
+    e.x[0] = xlt;
+    return e;
+}
+
+// Evaluations per sphere.
+__global__ void __launch_bounds__(256) k_sev_count(Geo g, Mov m, Scal *sc) {
+    __shared__ double scr[32];
+    if (sc->status) return;
+    const int s = blockIdx.x, nb = g.nbnd;
+    double n = 0.0;
+    for (int l = threadIdx.x; l < nb; l += blockDim.x)
+        if (m.revflag[(size_t)s * nb + l]) n += (double)scal_eval(g, m, s, l).nev;
+    n = block_sum(n, scr);
+    if (threadIdx.x == 0) m.sev_cnt[s] = (int)n;
+}
+
+// Offsets of every sphere's evaluations and their total.
+__global__ void __launch_bounds__(1024) k_sev_scan(Geo g, Mov m, Scal *sc) {
+    __shared__ int wsum[32];
+    if (sc->status) return;
+    const int T = blockDim.x, t = threadIdx.x, NB = g.nbody;
+    const int per = (NB + T - 1) / T, c0 = min(t * per, NB), c1 = min(c0 + per, NB);
+    int s = 0;
+    for (int c = c0; c < c1; ++c) s += m.sev_cnt[c];
+    int x = s;
+    const int lane = t & 31, wid = t >> 5;
+    for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int v = lane < (T >> 5) ? wsum[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += y; }
+        wsum[lane] = v;
+    }
+    __syncthreads();
+    int run = x - s + (wid > 0 ? wsum[wid - 1] : 0);
+    for (int c = c0; c < c1; ++c) { m.sev_off[c] = run; run += m.sev_cnt[c]; }
+    if (t == T - 1) sc->nsev = run;
+}
+
+// One sphere's evaluations written in (point, evaluation) order at its offset.
+__global__ void __launch_bounds__(256) k_sev_write(Geo g, Mov m, Scal *sc) {
+    __shared__ int wsum[8];
+    __shared__ int base;
+    if (sc->status) return;
+    const int s = blockIdx.x, nb = g.nbnd, t = threadIdx.x, lane = t & 31, wid = t >> 5, mxf = g.nx + 1;
+    if (t == 0) base = m.sev_off[s];
+    __syncthreads();
+    for (int l0 = 0; l0 < nb; l0 += blockDim.x) {
+        const int l = l0 + t;
+        ScalEval e;
+        int n = 0;
+        if (l < nb && m.revflag[(size_t)s * nb + l]) { e = scal_eval(g, m, s, l); n = e.nev; }
+        int x = n;
+        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        if (lane == 31) wsum[wid] = x;
+        __syncthreads();
+        int before = 0;
+        for (int w = 0; w < wid; ++w) before += wsum[w];
+        int q = base + before + x - n;
+        for (int ev = 1; ev <= n; ++ev, ++q) {
+            if (ev == 2 && e.c[0] >= mxf - 1) { e.c[0] = e.c[0] - (mxf - 1); e.x[0] = e.x[0] - (mxf - 1); }
+            m.sev_m[q] = s;
+            m.sev_l[q] = l;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) { m.sev_x[3 * (size_t)q + d] = e.x[d]; m.sev_c[3 * (size_t)q + d] = e.c[d]; }
+        }
+        __syncthreads();
+        if (t == 0) { int a = 0; for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += wsum[w]; base += a; }
+        __syncthreads();
+    }
+}
+
+// Scalar spreading targets: stencil corners on planes 1..nx (planes 0 and
+// nx+1 are never transformed), solid nodes unless INCLUDE_FRMEANFLUID.
+template <int N>
+__global__ void __launch_bounds__(256) k_ssp_count(Geo g, Mov m, Scal *sc) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sc->status || e >= sc->nsev) return;
+    const int nx = g.nx, mxf = g.nx + 1;
+    const int c0 = m.sev_c[3 * (size_t)e], c1 = m.sev_c[3 * (size_t)e + 1], c2 = m.sev_c[3 * (size_t)e + 2];
+    for (int ck = 0; ck < 2; ++ck)
+        for (int cj = 0; cj < 2; ++cj)
+            for (int ci = 0; ci < 2; ++ci) {
+                int i = c0 + ci;
+                if (i < 0) i = mxf + i - 1;
+                if (i < 1 || i > nx) continue;
+                const int j = wrapi(c1 + cj, N), k = wrapi(c2 + ck, N);
+                const size_t node = (size_t)(i - 1) * RP<N>::RSP + real_off<N>(k - 1, j - 1);
+                if (!g.include_frmeanfluid && m.fluid[node]) continue;
+                const int slot = atomicAdd(&m.sspcnt[node], 1);
+                if (slot < m.kmax) m.sspbuf[node * m.kmax + slot] = e * 8 + ci + 2 * cj + 4 * ck;
+                else atomicCAS(&sc->status, 0, PIBM_ERR_SPREAD_OVERFLOW);
+            }
+}
+
+// Scalar forcing at every node of planes 1..nx in (evaluation, corner) order.
+__global__ void __launch_bounds__(256) k_sspread_dyn(Geo g, Mov m, const double *__restrict__ sctb,
+                                                     const double *__restrict__ sfd, double *__restrict__ sfr, Scal *sc) {
+    const size_t node = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= (size_t)g.nx * g.RS || sc->status) return;
+    double v = 0.0;
+    const int c = min(m.sspcnt[node], m.kmax);
+    if (c > 0) {
+        int e[64];
+        const int cc = min(c, 64);
+        for (int q = 0; q < cc; ++q) {
+            const int x = m.sspbuf[node * m.kmax + q];
+            int b = q - 1;
+            while (b >= 0 && e[b] > x) { e[b + 1] = e[b]; --b; }
+            e[b + 1] = x;
+        }
+        for (int q = 0; q < cc; ++q) {
+            v = v + sctb[e[q]];
+            if (!g.include_frmeanfluid) v = v + sfd[e[q] >> 3];
+        }
+    }
+    sfr[node] = v;
+}
+
+template <int N>
+void enqueue_moving_scalar_t(const Geo &g, const Mov &m, Scal *sc, cudaStream_t s) {
+    k_sev_count<<<g.nbody, 256, 0, s>>>(g, m, sc);
+    k_sev_scan<<<1, 1024, 0, s>>>(g, m, sc);
+    k_sev_write<<<g.nbody, 256, 0, s>>>(g, m, sc);
+    cudaMemsetAsync(m.sspcnt, 0, (size_t)g.nx * RP<N>::RSP * sizeof(int), s);
+    k_ssp_count<N><<<(g.nsev + 255) / 256, 256, 0, s>>>(g, m, sc);
+}
+
 template <int N>
 void enqueue_moving_t(const Geo &g, const Mov &m, Scal *sc, const double *pres, const double *visc, cudaStream_t s) {
     const int pb = (m.N + 127) / 128;
@@ -609,6 +766,22 @@ void enqueue_moving(const Geo &g, const Mov &m, Scal *sc, const double *pres, co
     }
 }
 int moving_kernels_per_step(const Mov &m) { return 1 + (m.soft ? 3 * m.max_factor : 1) + 6; }
+
+// Scalar geometry of the step (before calc_inner_rev_data) and its spreading.
+void enqueue_moving_scalar(const Geo &g, const Mov &m, Scal *sc, cudaStream_t s) {
+    switch (g.my) {
+        case 32: enqueue_moving_scalar_t<32>(g, m, sc, s); break;
+        case 64: enqueue_moving_scalar_t<64>(g, m, sc, s); break;
+        case 96: enqueue_moving_scalar_t<96>(g, m, sc, s); break;
+        case 128: enqueue_moving_scalar_t<128>(g, m, sc, s); break;
+        case 256: enqueue_moving_scalar_t<256>(g, m, sc, s); break;
+    }
+}
+void enqueue_sspread_dyn(const Geo &g, const Mov &m, const double *sctb, const double *sfd, double *sfr, Scal *sc, cudaStream_t s) {
+    const size_t CR = (size_t)g.nx * g.RS;
+    k_sspread_dyn<<<(unsigned)((CR + 255) / 256), 256, 0, s>>>(g, m, sctb, sfd, sfr, sc);
+}
+int moving_scalar_kernels_per_step() { return 4; }
 
 void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, const double *ctb, double *fr, Scal *sc, cudaStream_t s) {
     const size_t CR = (size_t)g.nx * g.RS;

@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(256, 3) k_srev(Geo g, const double *__restrict
                                                  const Scal *__restrict__ sc, double *__restrict__ sctb,
                                                  double *__restrict__ sfd) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= g.nsev || sc->status) return;
+    if (e >= sc->nsev || sc->status) return;
     const int m = g.sev_m[e], l = g.sev_l[e], nx = g.nx;
     const double h = sc->heat_ratio, hold = sc->heat_ratio_old;
     double xli[3], xlo[3];
@@ -664,7 +664,7 @@ __global__ void __launch_bounds__(256) k_sfin(Geo g, Scal *sc, const double *sdp
     double fg = 0.0;
     for (int m = 0; m < g.nbody; ++m) fg = fg + flux_body[m] * da1;
     sc->flux_global = fg;
-    sc->nusselt = -(fg * g.char_length * g.char_length) / (6.0 * g.voldom * g.maxvolfrac * (g.phisurf - g.phistream));
+    sc->nusselt = -(fg * g.char_length * g.char_length) / (6.0 * g.voldom * sc->maxvolfrac * (g.phisurf - g.phistream));
     const double hn = sc->heat_ratio_new;
     if (!isfinite(hn) || !(hn > 0.0)) { atomicCAS(&sc->status, 0, PIBM_ERR_NAN); return; }
     sc->heat_ratio_old = sc->heat_ratio;
@@ -674,6 +674,10 @@ __global__ void __launch_bounds__(256) k_sfin(Geo g, Scal *sc, const double *sdp
 // ============================================================================
 // Host-side enqueue of the scalar step (after the flow step, same stream).
 // ============================================================================
+void enqueue_moving_scalar(const Geo &g, const Mov &m, Scal *sc, cudaStream_t s);
+void enqueue_sspread_dyn(const Geo &g, const Mov &m, const double *sctb, const double *sfd, double *sfr, Scal *sc, cudaStream_t s);
+int moving_scalar_kernels_per_step();
+
 template <int N>
 static void enqueue_scalar_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s) {
     const int old = 1 - cur;
@@ -685,9 +689,11 @@ static void enqueue_scalar_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s) 
                      b.nls[cur], b.nlr[cur], b.sc);
     launch_planes<N>(k_simg<N>, 1, 1, s, g, (const double2 *)b.nls[cur], b.nlr[cur], (const Scal *)b.sc);
     if (g.nbody > 0) k_sbnd<N><<<g.nbody * kDragSplit, 256, 0, s>>>(g, b.gph, b.sc, b.sdpart);
+    if (g.moving) enqueue_moving_scalar(g, b.mov, b.sc, s);
     if (g.nsev > 0) {
         k_srev<N><<<(g.nsev + 255) / 256, 256, 0, s>>>(g, b.phr, b.nlr[cur], b.nlr[old], b.sdf, b.sc, b.sctb, b.sfd);
-        if (g.ssp_nnodes > 0) k_sspread<<<(g.ssp_nnodes + 255) / 256, 256, 0, s>>>(g, b.sctb, b.sfd, b.sfr, b.sc);
+        if (g.moving) enqueue_sspread_dyn(g, b.mov, b.sctb, b.sfd, b.sfr, b.sc, s);
+        else if (g.ssp_nnodes > 0) k_sspread<<<(g.ssp_nnodes + 255) / 256, 256, 0, s>>>(g, b.sctb, b.sfd, b.sfr, b.sc);
     }
     launch_planes<N>(k_sff<N>, g.nx, 1, s, g, (const double *)b.sfr, b.ffs, b.sc);
     constexpr int LT = SLinesCfg<N>::LT;
@@ -709,7 +715,8 @@ int scalar_kernels_per_step(const Geo &g) {
     if (!g.scal) return 0;
     int n = 8;   // sa, sheat, sflux, snl, simg, sff, slines, sfin
     if (g.nbody > 0) n += 1;
-    if (g.nsev > 0) n += 1 + (g.ssp_nnodes > 0 ? 1 : 0);
+    if (g.nsev > 0) n += 1 + (g.ssp_nnodes > 0 || g.moving ? 1 : 0);
+    if (g.moving) n += moving_scalar_kernels_per_step();
     return n;
 }
 
