@@ -34,6 +34,9 @@ namespace pibm {
 
 void enqueue_scalar(const Geo &g, DevBufs &b, int cur, cudaStream_t s);
 int scalar_kernels_per_step(const Geo &g);
+void enqueue_moving(const Geo &g, const Mov &m, Scal *sc, const double *pres, const double *visc, cudaStream_t s);
+void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, const double *ctb, double *fr, Scal *sc, cudaStream_t s);
+int moving_kernels_per_step(const Mov &m);
 
 // ============================================================================
 // k_a0: 10 c2r per plane (dependent_functions.F90:1085-1122, 336-349;
@@ -41,10 +44,6 @@ int scalar_kernels_per_step(const Geo &g);
 // grad p are taken on the spectral planes before the transform (linear).
 // part[i*12 + q]: q 0-2 fluid sums, 3-5 solid sums, 6-8 all sums, 9-11 max |u|.
 // ============================================================================
-void enqueue_moving(const Geo &g, const Mov &m, Scal *sc, const double *pres, const double *visc, cudaStream_t s);
-void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, const double *ctb, double *fr, Scal *sc, cudaStream_t s);
-int moving_kernels_per_step(const Mov &m);
-
 template <int N>
 __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
                                                    double *__restrict__ ubcp, double *__restrict__ pbcp,
@@ -142,6 +141,28 @@ __global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *p
         m = block_max(m, scr);
         if (threadIdx.x == 0) { red[d] = a; red[3 + d] = m; }
     }
+    __shared__ double vmean[3], upmax;
+    if (g.moving) {
+        // particle speed limit (dependent_functions.F90:1156-1164) and the mean
+        // particle velocity (:1185-1193): the maximum in any order, the sums
+        // serial over the spheres as in the reference (one thread per component)
+        const int NB = g.nbody;
+        double um = kSmallD;
+        for (int m = threadIdx.x; m < NB; m += blockDim.x) {
+            double s2 = 0.0;
+            for (int d = 0; d < 3; ++d) s2 = __dadd_rn(s2, __dmul_rn(g.vel[m + d * NB], g.vel[m + d * NB]));
+            um = fmax(um, sqrt(s2));
+        }
+        um = block_max(um, scr);
+        if (threadIdx.x < 3) {
+            const double *v = g.vel + (size_t)threadIdx.x * NB;
+            double a = 0.0;
+#pragma unroll 8
+            for (int m = 0; m < NB; ++m) a = a + v[m];
+            vmean[threadIdx.x] = a / (double)NB;
+        }
+        if (threadIdx.x == 0) upmax = um;
+    }
     __syncthreads();
     if (threadIdx.x != 0) return;
     const double umax = fmax(fmax(red[3], red[4]), red[5]);
@@ -149,22 +170,9 @@ __global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *p
     double dtnew = sc->dt;
     if (umax * sc->dt / g.dx > g.cfl_max) dtnew = g.cfl_max * g.dx / umax;
     if (g.moving) {
-        // particle speed limit (dependent_functions.F90:1156-1164; the new dt
-        // is taken from the fluid speed, as the reference writes it) and the
-        // mean particle velocity (:1185-1193), serial sums over the spheres
-        const int NB = g.nbody;
-        double up_max = kSmallD;
-        for (int m = 0; m < NB; ++m) {
-            double s2 = 0.0;
-            for (int d = 0; d < 3; ++d) s2 = __dadd_rn(s2, __dmul_rn(g.vel[m + d * NB], g.vel[m + d * NB]));
-            up_max = fmax(up_max, sqrt(s2));
-        }
-        if (up_max * sc->dt / g.dx > g.cfl_max) dtnew = g.cfl_max * g.dx / umax;
-        for (int d = 0; d < 3; ++d) {
-            double a = 0.0;
-            for (int m = 0; m < NB; ++m) a = a + g.vel[m + d * NB];
-            sc->usmean_act[d] = a / (double)NB;
-        }
+        // the new dt is taken from the fluid speed, as the reference writes it
+        if (upmax * sc->dt / g.dx > g.cfl_max) dtnew = g.cfl_max * g.dx / umax;
+        for (int d = 0; d < 3; ++d) sc->usmean_act[d] = vmean[d];
     }
     for (int d = 0; d < 3; ++d) {
         sc->ufmean_old[d] = sc->ufmean[d];

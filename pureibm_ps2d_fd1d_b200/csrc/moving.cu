@@ -97,29 +97,51 @@ __global__ void k_dem_start(Mov m, Scal *sc) {
     sc->dem_substeps = factor;
 }
 
-// CALC_FORCE_DES + CFNEWVALUES for particle L (see the file comment).
-__global__ void __launch_bounds__(128) k_dem_update(Mov m, Scal *sc, const double *__restrict__ pres,
-                                                    const double *__restrict__ visc, int ifac) {
-    const int L = blockIdx.x * blockDim.x + threadIdx.x;
-    if (L >= m.N || ifac > m.factor[0] || sc->status) return;
-    const int MX = m.maxn;
-    int wl[40];
-    uint8_t wv[40];
+// CALC_FORCE_DES + CFNEWVALUES for particle L (see the file comment), one warp
+// per particle: the lanes evaluate L's pairs (every entry of NEIGHBOURS(L)
+// other than L), lane 0 then applies them in the serial order.
+constexpr int kUpdWarps = 4;
+constexpr int kMaxList = 40;   // >= MAXNEIGHBORS
+__global__ void __launch_bounds__(32 * kUpdWarps) k_dem_update(Mov m, Scal *sc, const double *__restrict__ pres,
+                                                               const double *__restrict__ visc, int ifac) {
+    if (ifac > m.factor[0] || sc->status) return;
+    __shared__ double fn_s[kUpdWarps][kMaxList][3];
+    __shared__ int cf_s[kUpdWarps][kMaxList], wl_s[kUpdWarps][kMaxList], wv_s[kUpdWarps][kMaxList];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int L = blockIdx.x * kUpdWarps + wid;
+    if (L >= m.N) return;
+    const int MX = m.maxn, nc = m.ncnt[L];
+    // pair (J, L) for J < L as at J's turn (flag bit 0 contact, bit 1 "already
+    // in J's contact list"), pair (L, I) for I > L as at L's turn
+    for (int q = lane; q < nc; q += 32) {
+        const int P = m.neigh[L * MX + q];
+        int f = 0;
+        double fn[3] = {0.0, 0.0, 0.0};
+        if (P < L) {
+            if (pair_force(m, P, L, fn, sc)) {
+                f = 1;
+                for (int p = 0; p < m.pncnt[P]; ++p)
+                    if (m.pn[P * MX + p] == L) { if (m.pv[P * MX + p] == 1) f |= 2; break; }
+            }
+        } else if (P > L) {
+            if (pair_force(m, L, P, fn, sc)) f = 1;
+        }
+        cf_s[wid][q] = f;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) fn_s[wid][q][d] = fn[d];
+    }
+    __syncwarp();
+    if (lane != 0) return;
+    int *wl = wl_s[wid], *wv = wv_s[wid];
     int wc = m.pncnt[L];
-    for (int q = 0; q < wc; ++q) { wl[q] = m.pn[L * MX + q]; wv[q] = (uint8_t)m.pv[L * MX + q]; }
+    for (int q = 0; q < wc; ++q) { wl[q] = m.pn[L * MX + q]; wv[q] = m.pv[L * MX + q]; }
     double fc[3] = {0.0, 0.0, 0.0};
-    const int nc = m.ncnt[L];
     bool over = false;
     // turns of the lower partners J (ascending: they precede L in NEIGHBOURS(L))
     for (int q = 0; q < nc; ++q) {
         const int J = m.neigh[L * MX + q];
-        if (J >= L) continue;
-        double fn[3];
-        if (!pair_force(m, J, L, fn, sc)) continue;
-        bool already = false;
-        for (int p = 0; p < m.pncnt[J]; ++p)
-            if (m.pn[J * MX + p] == L) { already = m.pv[J * MX + p] == 1; break; }
-        if (already) {
+        if (J >= L || !(cf_s[wid][q] & 1)) continue;
+        if (cf_s[wid][q] & 2) {
             for (int p = 0; p < wc; ++p) if (wl[p] == J) { wv[p] = 1; break; }
         } else if (wc + 1 < MX) {
             wl[wc] = J; wv[wc] = 1; ++wc;
@@ -127,7 +149,7 @@ __global__ void __launch_bounds__(128) k_dem_update(Mov m, Scal *sc, const doubl
             over = true;
         }
 #pragma unroll
-        for (int d = 0; d < 3; ++d) fc[d] = fc[d] - fn[d];
+        for (int d = 0; d < 3; ++d) fc[d] = fc[d] - fn_s[wid][q][d];
     }
     // L's turn: drop the entries whose contact ended, clear the flags, own pairs
     int w = 0;
@@ -136,9 +158,7 @@ __global__ void __launch_bounds__(128) k_dem_update(Mov m, Scal *sc, const doubl
     for (int p = 0; p < wc; ++p) wv[p] = 0;
     for (int q = 0; q < nc; ++q) {
         const int I = m.neigh[L * MX + q];
-        if (I <= L) continue;
-        double fn[3];
-        if (!pair_force(m, L, I, fn, sc)) continue;
+        if (I <= L || !(cf_s[wid][q] & 1)) continue;
         int found = -1;
         for (int p = 0; p < wc; ++p) if (wl[p] == I) { found = p; break; }
         if (found >= 0) {
@@ -149,7 +169,7 @@ __global__ void __launch_bounds__(128) k_dem_update(Mov m, Scal *sc, const doubl
             over = true;
         }
 #pragma unroll
-        for (int d = 0; d < 3; ++d) fc[d] = fc[d] + fn[d];
+        for (int d = 0; d < 3; ++d) fc[d] = fc[d] + fn_s[wid][q][d];
     }
     if (over) atomicCAS(&sc->status, 0, PIBM_ERR_NEIGH_OVERFLOW);
     m.pncnt2[L] = wc;
@@ -287,8 +307,23 @@ __device__ __forceinline__ bool near_img(const Mov &m, int LL, int PNO, const do
     return rlm - sqrt(dd) > kSmallD;
 }
 
+// The image factor through which a search from cell cJ sees cell cL along one
+// direction when the coarse grid has at least 3 cells there (then exactly one
+// of the offsets -1, 0, +1 wraps onto cL).
+__device__ __forceinline__ double img_dir(int cJ, int cL, int cmax) {
+    if (cJ - 1 >= 2 && cJ - 1 == cL) return 0.0;
+    if (cJ + 1 <= cmax && cJ + 1 == cL) return 0.0;
+    if (cJ == cL) return 0.0;
+    return cJ + 1 > cmax ? 1.0 : -1.0;   // the wrapped neighbour: across the upper or the lower boundary
+}
+
 // GRID_BASED_NEIGHBOR_SEARCH (collision_mod.F90:807-1062) for one particle per
 // warp, then CFUPDATEOLD and the contact lists of the next sub-step.
+//  - coarse grids with >= 3 cells per direction: the 27 neighbourhood cells
+//    are distinct, so lane o < 27 scans cell o; finds are placed by a prefix
+//    sum over the lanes, which keeps the reference's cell-scan order
+//  - smaller grids (cells repeat through the periodic wrap): lane 0 follows
+//    the serial loop, first accepted image of a particle only
 constexpr int kSearchWarps = 4;
 __global__ void __launch_bounds__(32 * kSearchWarps) k_dem_search(Mov m, Scal *sc, int ifac) {
     if (ifac > m.factor[0] || sc->status) return;
@@ -300,59 +335,81 @@ __global__ void __launch_bounds__(32 * kSearchWarps) k_dem_search(Mov m, Scal *s
     int *own = own_s[wid], *mir = mir_s[wid];
     const int ci = m.pijk[3 * L], cj = m.pijk[3 * L + 1], ck = m.pijk[3 * L + 2];
     const int cL = cell_id(m, ci, cj, ck);
-    // L's own finds: PNO > L in the 27 cells in scan order, each cell ascending,
-    // first accepted image only
-    int nown = 0;
-    bool over = false;
-    for (int o = 0; o < 27; ++o) {
-        double sh[3];
-        const int c = nb_cell(m, ci, cj, ck, o, sh);
-        const int s0 = m.cstart[c], s1 = m.cstart[c + 1];
-        for (int b = s0; b < s1; b += 32) {
-            const int e = b + lane;
-            const int P = e < s1 ? m.clist[e] : -1;
-            bool acc = P > L && near_img(m, L, P, sh);
-            if (acc) for (int q = 0; q < nown && q < 64; ++q) if (own[q] == P) { acc = false; break; }
-            const unsigned bal = __ballot_sync(0xffffffffu, acc);
-            if (acc) {
-                const int pos = nown + __popc(bal & ((1u << lane) - 1u));
-                if (pos < 64) own[pos] = P;
-            }
-            nown += __popc(bal);
-            __syncwarp();
+    int nown = 0, nmir = 0;
+    const bool fast = m.cx >= 4 && m.cy >= 4 && m.cz >= 4;
+    if (fast) {
+        double sh[3] = {0.0, 0.0, 0.0};
+        int c = 0, s0 = 0, s1 = 0;
+        if (lane < 27) { c = nb_cell(m, ci, cj, ck, lane, sh); s0 = m.cstart[c]; s1 = m.cstart[c + 1]; }
+        // own finds P > L of this lane's cell
+        int cnt = 0;
+        for (int e = s0; e < s1; ++e) { const int P = m.clist[e]; if (P > L && near_img(m, L, P, sh)) ++cnt; }
+        int x = cnt;
+        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        nown = __shfl_sync(0xffffffffu, x, 31);
+        int pos = x - cnt;
+        for (int e = s0; e < s1; ++e) {
+            const int P = m.clist[e];
+            if (P > L && near_img(m, L, P, sh)) { if (pos < 64) own[pos] = P; ++pos; }
         }
-    }
-    // entries appended by lower particles' searches: J < L whose search
-    // accepts L through one of its 27 cells (any image), ascending J
-    int nmir = 0;
-    for (int o = 0; o < 27; ++o) {
-        double sh[3];
-        const int c = nb_cell(m, ci, cj, ck, o, sh);
-        bool seen = false;
-        for (int o2 = 0; o2 < o; ++o2) { double t[3]; if (nb_cell(m, ci, cj, ck, o2, t) == c) { seen = true; break; } }
-        if (seen) continue;
-        const int s0 = m.cstart[c], s1 = m.cstart[c + 1];
-        for (int b = s0; b < s1; b += 32) {
-            const int e = b + lane;
-            const int J = e < s1 ? m.clist[e] : -1;
-            bool acc = false;
-            if (J >= 0 && J < L) {
+        // lower particles J whose search accepts L: J sees cell cL through one image
+        cnt = 0;
+        for (int e = s0; e < s1; ++e) {
+            const int J = m.clist[e];
+            if (J >= L) continue;
+            const double shj[3] = {img_dir(m.pijk[3 * J], ci, m.cx), img_dir(m.pijk[3 * J + 1], cj, m.cy),
+                                   img_dir(m.pijk[3 * J + 2], ck, m.cz)};
+            if (near_img(m, J, L, shj)) ++cnt;
+        }
+        x = cnt;
+        for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        nmir = __shfl_sync(0xffffffffu, x, 31);
+        pos = x - cnt;
+        for (int e = s0; e < s1; ++e) {
+            const int J = m.clist[e];
+            if (J >= L) continue;
+            const double shj[3] = {img_dir(m.pijk[3 * J], ci, m.cx), img_dir(m.pijk[3 * J + 1], cj, m.cy),
+                                   img_dir(m.pijk[3 * J + 2], ck, m.cz)};
+            if (near_img(m, J, L, shj)) { if (pos < 64) mir[pos] = J; ++pos; }
+        }
+        __syncwarp();
+    } else if (lane == 0) {
+        for (int o = 0; o < 27; ++o) {
+            double sh[3];
+            const int c = nb_cell(m, ci, cj, ck, o, sh);
+            for (int e = m.cstart[c]; e < m.cstart[c + 1]; ++e) {
+                const int P = m.clist[e];
+                if (P <= L || !near_img(m, L, P, sh)) continue;
+                bool already = false;
+                for (int q = 0; q < nown && q < 64; ++q) if (own[q] == P) { already = true; break; }
+                if (!already) { if (nown < 64) own[nown] = P; ++nown; }
+            }
+        }
+        for (int o = 0; o < 27; ++o) {
+            double sh[3];
+            const int c = nb_cell(m, ci, cj, ck, o, sh);
+            bool seen = false;
+            for (int o2 = 0; o2 < o; ++o2) { double t[3]; if (nb_cell(m, ci, cj, ck, o2, t) == c) { seen = true; break; } }
+            if (seen) continue;
+            for (int e = m.cstart[c]; e < m.cstart[c + 1]; ++e) {
+                const int J = m.clist[e];
+                if (J >= L) continue;
                 const int ji = m.pijk[3 * J], jj = m.pijk[3 * J + 1], jk = m.pijk[3 * J + 2];
+                bool acc = false;
                 for (int oj = 0; oj < 27 && !acc; ++oj) {
                     double shj[3];
                     if (nb_cell(m, ji, jj, jk, oj, shj) == cL && near_img(m, J, L, shj)) acc = true;
                 }
+                if (acc) { if (nmir < 64) mir[nmir] = J; ++nmir; }
             }
-            const unsigned bal = __ballot_sync(0xffffffffu, acc);
-            if (acc) {
-                const int pos = nmir + __popc(bal & ((1u << lane) - 1u));
-                if (pos < 64) mir[pos] = J;
-            }
-            nmir += __popc(bal);
-            __syncwarp();
         }
     }
-    if (nmir > 64 || nown > 64 || nmir + 1 + nown + 1 > MX) over = true;
+    if (!fast) {   // counts of the serial path are in lane 0
+        nown = __shfl_sync(0xffffffffu, nown, 0);
+        nmir = __shfl_sync(0xffffffffu, nmir, 0);
+    }
+    __syncwarp();
+    const bool over = nmir > 64 || nown > 64 || nmir + 1 + nown + 1 > MX;
     if (lane == 0 && !over) {
         for (int a = 1; a < nmir; ++a) {   // ascending J
             const int v = mir[a];
@@ -549,7 +606,7 @@ __global__ void __launch_bounds__(256) k_spread_dyn(Geo g, Mov m, const double *
     if (c > 0) {
         int e[64];
         const int cc = min(c, 64);
-        for (int q = 0; q < cc; ++q) {
+        for (int q = 0; q < cc; ++q) {   // the bucket in ascending (point, corner) order
             const int v = m.spbuf[node * m.kmax + q];
             int b = q - 1;
             while (b >= 0 && e[b] > v) { e[b + 1] = e[b]; --b; }
@@ -705,7 +762,7 @@ __global__ void __launch_bounds__(256) k_sspread_dyn(Geo g, Mov m, const double 
     if (c > 0) {
         int e[64];
         const int cc = min(c, 64);
-        for (int q = 0; q < cc; ++q) {
+        for (int q = 0; q < cc; ++q) {   // the bucket in ascending (evaluation, corner) order
             const int x = m.sspbuf[node * m.kmax + q];
             int b = q - 1;
             while (b >= 0 && e[b] > x) { e[b + 1] = e[b]; --b; }
@@ -735,7 +792,7 @@ void enqueue_moving_t(const Geo &g, const Mov &m, Scal *sc, const double *pres, 
     if (m.soft) {
         const size_t bin_smem = (size_t)(3 * m.ncell + 1 + m.N) * sizeof(int);
         for (int ifac = 1; ifac <= m.max_factor; ++ifac) {
-            k_dem_update<<<pb, 128, 0, s>>>(m, sc, pres, visc, ifac);
+            k_dem_update<<<(m.N + kUpdWarps - 1) / kUpdWarps, 32 * kUpdWarps, 0, s>>>(m, sc, pres, visc, ifac);
             k_dem_bin<<<1, 1024, bin_smem, s>>>(m, sc, ifac);
             k_dem_search<<<(m.N + kSearchWarps - 1) / kSearchWarps, 32 * kSearchWarps, 0, s>>>(m, sc, ifac);
         }

@@ -87,11 +87,13 @@ def test_no_collision_translation_matches_oracle():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("my,dia,nbody,seed,spread", [(32, 6.0, 50, 4, 2.0), (64, 10.0, 60, 9, 1.5)])
+@pytest.mark.parametrize("my,dia,nbody,seed,spread", [(32, 6.0, 50, 4, 2.0), (64, 10.0, 60, 9, 1.5), (96, 8.0, 300, 21, 2.0)])
 def test_moving_array_matches_oracle(my, dia, nbody, seed, spread):
     """A freely moving random array with Maxwellian velocities (several
     collisions, spheres crossing the periodic boundaries, reversal points
-    switched off inside neighbours), 12 steps."""
+    switched off inside neighbours), 12 steps.  The DEM coarse grid has one
+    cell per direction at 32^3 and 64^3 (serial search path) and seven at
+    96^3 with d = 8 (the lane-per-cell search path)."""
     prm, xc, vel = config.moving_array(my=my, dia_cells=dia, nbody=nbody, seed=seed, vel_spread=spread)
     gpu, cpu = make_pair(prm, xc, vel)
     for _ in range(12):
