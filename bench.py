@@ -202,6 +202,45 @@ def with_scalar(steps: int = 20, warmup: int = 3):
     return out
 
 
+def moving_suspension(steps: int = 10, warmup: int = 3):
+    """The moving-particle configuration with scalar transport: 256^3, 1202
+    spheres of diameter 20 cells (phi = 0.3), density ratio 100, seeded
+    Maxwellian velocities (spread 0.1 uchar), soft-sphere DEM with
+    restitution 0.9, passive scalar Pr 0.7 with sphere surfaces at
+    phisurf = 1 in a stream at 0.  Flow + DEM + geometry rebuild + scalar
+    step throughput, device-timed on the step graphs, and the serial phase
+    split."""
+    import ctypes as C
+    import pureibm_ps2d_fd1d_b200 as pk
+    from pureibm_ps2d_fd1d_b200 import config, abi
+    prm, xc, vel = config.moving_array(my=256, dia_cells=20.0, nbody=1202, seed=2024, rhos=100.0, coeff_rest=0.9,
+                                       vel_spread=0.1, mc_moves=1000)
+    prm.update(iscalon=1, pr_or_sc_nu=0.7, phisurf=1.0, phistream=0.0, initialize_zero=False)
+    s = pk.Solver(config.make_params(prm), xc, vel)
+    s.run(warmup)
+    lib = pk.load_library()
+    rep = abi.pibm_step_report()
+    total = C.c_double()
+    rc = lib.pibm_run_timed(s.h, steps, C.byref(rep), C.byref(total))
+    if rc != 0:
+        raise RuntimeError("pibm_run_timed (moving) failed: %d %s" % (rc, lib.pibm_last_error().decode()))
+    phases = (C.c_double * abi.PIBM_NPHASE)()
+    ptotal = C.c_double()
+    rc = lib.pibm_run_profiled(s.h, 3, C.byref(rep), C.byref(ptotal), phases, abi.PIBM_NPHASE)
+    if rc != 0:
+        raise RuntimeError("pibm_run_profiled (moving) failed: %d %s" % (rc, lib.pibm_last_error().decode()))
+    contacts = s.get_contacts()
+    ncell = s.nx * s.my * s.mz
+    out = {"unit": UNIT, "value": ncell * steps / (total.value / 1e3) / 1e6, "ms_per_step": total.value / steps,
+           "steps": steps, "serial_phase_ms_per_step": {abi.PHASE_NAMES[q]: phases[q] / 3 for q in range(abi.PIBM_NPHASE)},
+           "active_reversal_points": rep.nrpr_active_total, "contact_entries": int(contacts["pn"][0].sum()),
+           "dt": rep.dt, "nusselt": rep.nusselt,
+           "config": "256^3, 1202 moving spheres d=20 (phi 0.3), rhos/rhof 100, Maxwellian velocities, "
+                     "soft-sphere DEM e=0.9, passive scalar Pr 0.7"}
+    s.close()
+    return out
+
+
 def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024):
     """Batched multiple-independent-simulation throughput against the plain
     per-realization loop on the same GPU: 16 seeded realizations (grids from
@@ -367,6 +406,8 @@ def run_gpu(args):
         line["batched_mis"] = batched_mis()
     if not args.no_scalar and world == 1:
         line["with_scalar"] = with_scalar()
+    if not args.no_moving and world == 1:
+        line["moving_suspension"] = moving_suspension()
     if not args.no_cpu_baseline and world == 1:
         cb = cpu_baseline(prm, xc, steps=2, warmup=1)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -385,6 +426,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mis", action="store_true", help="skip the batched-realization measurement")
     ap.add_argument("--no-scalar", action="store_true", help="skip the flow + passive-scalar measurement")
+    ap.add_argument("--no-moving", action="store_true", help="skip the moving-particle suspension measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
