@@ -85,7 +85,8 @@ typedef struct pibm_params {
     double  pr_or_sc_nu;     /* PR_OR_SC_NU                                    */
     double  phisurf;         /* PHISURF                                        */
     double  phistream;       /* PHISTREAM                                      */
-    int32_t reserved[8];
+    int32_t rk3;             /* RK3: 3-stage Runge-Kutta (coef, itrmax = 3, initialize_flo.F90:861-877); 0 = AB2/CN */
+    int32_t reserved[7];
 } pibm_params;
 
 /* Particle list (the reference's sphr_center.inp after scaling by DBYDX:

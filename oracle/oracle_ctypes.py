@@ -38,6 +38,7 @@ def lib():
         L.orc_destroy.restype = None
         L.orc_info.argtypes = [vp, P(pibm_info)]
         L.orc_step.argtypes = [vp, P(pibm_step_report)]
+        L.orc_step_rks.argtypes = [vp, C.c_int, P(pibm_step_report)]
         L.orc_get_state.argtypes = [vp, P(pibm_state_view)]
         L.orc_set_state.argtypes = [vp, P(pibm_state_view)]
         L.orc_get_particles.argtypes = [vp] + [P(C.c_double)] * 5
@@ -122,10 +123,19 @@ class OracleSolver:
             pass
 
     def step(self) -> dict:
+        """One full time step (every rks stage)."""
         rep = pibm_step_report()
         rc = lib().orc_step(self.h, C.byref(rep))
         if rc != 0:
             raise RuntimeError("orc_step failed with code %d" % rc)
+        return rep.as_dict()
+
+    def step_rks(self, rks: int) -> dict:
+        """One stage rks of the driver's loop."""
+        rep = pibm_step_report()
+        rc = lib().orc_step_rks(self.h, int(rks), C.byref(rep))
+        if rc != 0:
+            raise RuntimeError("orc_step_rks failed with code %d" % rc)
         return rep.as_dict()
 
     def get_state(self):

@@ -67,7 +67,9 @@ struct Orc {
     pibm_params prm;
     int nx, my, mz, my2, mx, mxf;
     double dx, dy, dz, dx2, vis, doml[3], voldom;
-    double coef[4];                 // coef(1,1:4) AB2: initialize_flo.F90:880-884
+    double coef[4];                 // coef(rks,1:4) of the current stage
+    double coef_tab[3][4];          // AB2 (one stage) or RK3 (three): initialize_flo.F90:861-884
+    int itrmax = 1;
     double char_length, uchar[3], ucharmod, umeanslip;
     double cfl, cfl_max;
     double ramp_frac_time;
@@ -713,7 +715,18 @@ bool setup(Orc &o, const pibm_params *prm, const pibm_particles *parts) {
             cplx s = o.wy[j - 1] * o.wy[j - 1] + o.wz[k - 1] * o.wz[k - 1];
             o.w2[(size_t)(j - 1) + (size_t)o.my2 * (k - 1)] = -s.real();
         }
-    o.coef[0] = 0.5; o.coef[1] = 0.5; o.coef[2] = 3.0 / 2.0; o.coef[3] = -0.5;
+    if (prm->rk3) {
+        const double t[3][4] = {{4.0 / 15.0, 4.0 / 15.0, 8.0 / 15.0, 0.0},
+                                {1.0 / 15.0, 1.0 / 15.0, 5.0 / 12.0, -17.0 / 60.0},
+                                {1.0 / 6.0, 1.0 / 6.0, 3.0 / 4.0, -5.0 / 12.0}};
+        std::memcpy(o.coef_tab, t, sizeof(t));
+        o.itrmax = 3;
+    } else {
+        const double t[4] = {0.5, 0.5, 3.0 / 2.0, -0.5};
+        for (int r = 0; r < 3; ++r) std::memcpy(o.coef_tab[r], t, sizeof(t));
+        o.itrmax = 1;
+    }
+    std::memcpy(o.coef, o.coef_tab[0], sizeof(o.coef));
     o.t = 0.0;
     const size_t NC = (size_t)(o.nx + 1) * o.my2 * o.mz * 3;
     o.u.assign(NC, 0.0); o.nl.assign(NC, 0.0); o.onl.assign(NC, 0.0); o.ff.assign(NC, 0.0);
@@ -850,7 +863,7 @@ void compute_new_timestep(Orc &o, int rks) {
     for (int i = 1; i <= nx; ++i)
         c2r_with(o, [&](int j, int k) { return o.p[o.PI3(i, j, k)]; },
                  [&](int j, int k, double v) { o.pbcp[o.QI(i, j, k, 1)] = v; });
-    if (rks == 1 && o.prm.adaptive) o.dt = dtnew;
+    if (rks == o.itrmax && o.prm.adaptive) o.dt = dtnew;
     o.t = o.t + o.dt * (o.coef[0] + o.coef[1]);
     double utemp = o.ucharmod;
     double tempt = o.ramp_frac_time * (double)(float)(o.mx - 1) * o.dx / utemp;
@@ -1935,31 +1948,44 @@ int scalstep(Orc &o) {
     return PIBM_OK;
 }
 
-int step(Orc &o, pibm_step_report *rep) {
-    const int rks = 1;
+void fill_report(Orc &o, pibm_step_report *rep) {
+    std::memset(rep, 0, sizeof(*rep));
+    rep->dt = o.dt; rep->t = o.t; rep->cf = o.cf; rep->umax = o.umax_last; rep->divmax = o.divmax;
+    for (int d = 0; d < 3; ++d) {
+        rep->ufmean[d] = o.ufmean[d]; rep->usmean[d] = o.usmean[d]; rep->umean[d] = o.umean[d];
+        rep->mpg[d] = o.mpg[d]; rep->frmean[d] = o.frmean[d];
+        rep->pres_total[d] = o.pres_total[d]; rep->visc_total[d] = o.visc_total[d];
+    }
+    rep->norm_drag = o.norm_drag; rep->ferror = o.ferror;
+    rep->pres_drag = o.pres_drag; rep->visc_drag = o.visc_drag; rep->total_drag = o.total_drag;
+    rep->mixmeanslipmod = o.mixmeanslipmod;
+    long long s = 0; for (int v : o.nrpr_active) s += v;
+    rep->nrpr_active_total = s;
+    rep->heat_ratio = o.heat_ratio;
+    rep->nusselt = o.nusselt;
+}
+
+// One iteration of the driver's rks loop (dtibm_main_scal_flo.F90:426-527)
+// with the stage's coefficients coef(rks, 1:4).
+int step_stage(Orc &o, int rks, pibm_step_report *rep) {
+    std::memcpy(o.coef, o.coef_tab[rks - 1], sizeof(o.coef));
     compute_new_timestep(o, rks);
     int rc = nonlinear(o, rks);
     if (rc) return rc;
     rc = velstep(o, rks);
     if (!rc && o.scal) rc = scalstep(o);
-    if (rep) {
-        std::memset(rep, 0, sizeof(*rep));
-        rep->dt = o.dt; rep->t = o.t; rep->cf = o.cf; rep->umax = o.umax_last; rep->divmax = o.divmax;
-        for (int d = 0; d < 3; ++d) {
-            rep->ufmean[d] = o.ufmean[d]; rep->usmean[d] = o.usmean[d]; rep->umean[d] = o.umean[d];
-            rep->mpg[d] = o.mpg[d]; rep->frmean[d] = o.frmean[d];
-            rep->pres_total[d] = o.pres_total[d]; rep->visc_total[d] = o.visc_total[d];
-        }
-        rep->norm_drag = o.norm_drag; rep->ferror = o.ferror;
-        rep->pres_drag = o.pres_drag; rep->visc_drag = o.visc_drag; rep->total_drag = o.total_drag;
-        rep->mixmeanslipmod = o.mixmeanslipmod;
-        long long s = 0; for (int v : o.nrpr_active) s += v;
-        rep->nrpr_active_total = s;
-        rep->heat_ratio = o.heat_ratio;
-        rep->nusselt = o.nusselt;
-    }
+    if (rep) fill_report(o, rep);
     for (const cplx &v : o.u) if (!std::isfinite(v.real()) || !std::isfinite(v.imag())) return PIBM_ERR_NAN;
     return rc;
+}
+
+// One time step: rks = 1..itrmax.
+int step(Orc &o, pibm_step_report *rep) {
+    for (int rks = 1; rks <= o.itrmax; ++rks) {
+        const int rc = step_stage(o, rks, rep);
+        if (rc) return rc;
+    }
+    return PIBM_OK;
 }
 
 }  // namespace
@@ -2000,6 +2026,11 @@ int orc_info(void *h, pibm_info *info) {
 }
 
 int orc_step(void *h, pibm_step_report *rep) { return step(*(Orc *)h, rep); }
+int orc_step_rks(void *h, int rks, pibm_step_report *rep) {
+    Orc &o = *(Orc *)h;
+    if (rks < 1 || rks > o.itrmax) { g_err = "rks out of range"; return PIBM_ERR_ARG; }
+    return step_stage(o, rks, rep);
+}
 
 int orc_get_state(void *h, pibm_state_view *s) {
     Orc &o = *(Orc *)h;

@@ -155,8 +155,7 @@ def make_params(prm: Dict) -> pibm_params:
     p.pr_or_sc_nu = float(prm.get("pr_or_sc_nu", 0.7))
     p.phisurf = float(prm.get("phisurf", 0.0))
     p.phistream = float(prm.get("phistream", 1.0))
-    if prm.get("rk3"):
-        raise ValueError("RK3=T is not supported by this engine (AB2 only)")
+    p.rk3 = int(bool(prm.get("rk3", False)))
     if not prm.get("xperiodic", True):
         raise ValueError("XPERIODIC=F is not supported (x-periodic only)")
     return p

@@ -66,7 +66,10 @@ std::vector<double2> twiddles(int n) {
 struct pibm_handle {
     RunSetup S;
     pibm_params prm;
-    Geo g;
+    Geo g;                // the run's constants (stage 1)
+    Geo gs[3];            // per stage rks: coef(rks, 1:4) and the dt update of the last stage
+    int itrmax = 1;       // 1 (AB2) or 3 (RK3)
+    int next_rks = 1;     // the rks the next pibm_step call is expected to run
     DevBufs b;
     std::vector<void *> allocs;
     cudaStream_t stream = nullptr;
@@ -185,6 +188,12 @@ static int setup_moving(pibm_handle *h) {
     return PIBM_OK;
 }
 
+// One time step = stages rks = 1..itrmax; stage k writes the nonlinear term
+// into buffer cur ^ (k & 1) (the onl = nl swap of every nonlinear call).
+static void enqueue_time_step(pibm_handle *h, int cur, cudaStream_t s, const StepStreams *ss) {
+    for (int k = 0; k < h->itrmax; ++k) enqueue_step(h->gs[k], h->b, cur ^ (k & 1), s, nullptr, ss);
+}
+
 extern "C" {
 
 const char *pibm_last_error(void) { return g_last_error.c_str(); }
@@ -221,7 +230,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     g.c1 = S.coef[0]; g.c2 = S.coef[1]; g.c3 = S.coef[2]; g.c4 = S.coef[3];
     g.scheme = prm->discr_scheme; g.limiter = prm->limiter;
     g.include_frmeanfluid = prm->include_frmeanfluid; g.revernorm = prm->revernorm;
-    g.set_mpg = prm->set_mpg; g.adaptive = prm->adaptive;
+    g.set_mpg = prm->set_mpg; g.adaptive = prm->adaptive; g.dt_update = 1;
     g.cfl_max = prm->cfl_max; g.ramp_frac_time = S.ramp_frac_time; g.ucharmod = S.ucharmod;
     g.char_length = S.char_length; g.voldom = S.voldom; g.maxvolfrac = S.maxvolfrac; g.mean_volfrac = S.mean_volfrac;
     g.count_fluid = S.count_fluid; g.ncell = (long long)S.nx * S.my * S.mz;
@@ -323,6 +332,19 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     for (int d = 0; d < 3; ++d) { sc.usmean_act[d] = S.usmean_des[d]; sc.frame_vel[d] = 0.0; sc.frame_pos[d] = 1.0; }
     if (!guard(cudaMemcpy(b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice), "scalars")) { delete h; return rc; }
     if (g.moving && (rc = setup_moving(h)) != PIBM_OK) { delete h; return rc; }
+    // time-integration stages (initialize_flo.F90:861-884)
+    static const double kAB2[4] = {0.5, 0.5, 3.0 / 2.0, -0.5};
+    static const double kRK3[3][4] = {{4.0 / 15.0, 4.0 / 15.0, 8.0 / 15.0, 0.0},
+                                      {1.0 / 15.0, 1.0 / 15.0, 5.0 / 12.0, -17.0 / 60.0},
+                                      {1.0 / 6.0, 1.0 / 6.0, 3.0 / 4.0, -5.0 / 12.0}};
+    h->itrmax = prm->rk3 ? 3 : 1;
+    for (int k = 0; k < h->itrmax; ++k) {
+        const double *c = prm->rk3 ? kRK3[k] : kAB2;
+        h->gs[k] = g;
+        h->gs[k].c1 = c[0]; h->gs[k].c2 = c[1]; h->gs[k].c3 = c[2]; h->gs[k].c4 = c[3];
+        h->gs[k].dt_update = k == h->itrmax - 1;
+    }
+    g = h->gs[0];
     *out = h;
     return PIBM_OK;
 }
@@ -334,7 +356,7 @@ int pibm_info_get(pibm_handle *h, pibm_info *info) {
     info->dx = S.dx; info->dt = S.dt; info->radbdy = S.radbdy; info->maxvolfrac = S.maxvolfrac;
     info->count_solid = S.count_solid; info->count_fluid = S.count_fluid;
     info->npts_active = (int32_t)S.pt_m.size();
-    info->kernels_per_step = kernels_per_step(h->g, h->b.mov);
+    info->kernels_per_step = kernels_per_step(h->g, h->b.mov) * h->itrmax;
     return PIBM_OK;
 }
 
@@ -367,20 +389,23 @@ static int fill_report(pibm_handle *h, pibm_step_report *rep) {
 
 int pibm_step(pibm_handle *h, int rks, pibm_step_report *rep) {
     if (!h) return fail(PIBM_ERR_ARG, "null handle");
-    if (rks != 1) return fail(PIBM_ERR_ARG, "AB2 has a single sub-step (rks = 1)");
-    enqueue_step(h->g, h->b, h->cur, h->stream, nullptr, &h->ss);
+    if (rks < 1 || rks > h->itrmax) return fail(PIBM_ERR_ARG, h->itrmax == 1 ? "AB2 has a single stage (rks = 1)" : "rks must be 1, 2 or 3 (RK3)");
+    if (rks != h->next_rks) return fail(PIBM_ERR_ARG, "stages must run in the order rks = 1..itrmax");
+    enqueue_step(h->gs[rks - 1], h->b, h->cur, h->stream, nullptr, &h->ss);
     CUDA_OR_FAIL(cudaGetLastError());
     h->cur ^= 1;
+    h->next_rks = rks == h->itrmax ? 1 : rks + 1;
     return fill_report(h, rep);
 }
 
 int pibm_run(pibm_handle *h, int nsteps, pibm_step_report *last) {
     if (!h || nsteps < 0) return fail(PIBM_ERR_ARG, "bad argument");
+    if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "pibm_run starts at a step boundary (finish the rks stages with pibm_step)");
     for (int par = 0; par < 2; ++par) {
         if (h->graph[par]) continue;
         cudaGraph_t gr;
         CUDA_OR_FAIL(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_step(h->g, h->b, par, h->stream, nullptr, &h->ss);
+        enqueue_time_step(h, par, h->stream, &h->ss);
         CUDA_OR_FAIL(cudaStreamEndCapture(h->stream, &gr));
         CUDA_OR_FAIL(cudaGraphInstantiate(&h->graph[par], gr, 0));
         cudaGraphDestroy(gr);
@@ -416,16 +441,18 @@ int pibm_run_timed(pibm_handle *h, int nsteps, pibm_step_report *last, double *t
 
 int pibm_run_profiled(pibm_handle *h, int nsteps, pibm_step_report *last, double *total_ms, double *phase_ms, int nphase) {
     if (!h || nsteps <= 0 || nphase < 0 || nphase > PIBM_NPHASE) return fail(PIBM_ERR_ARG, "bad argument");
-    std::vector<cudaEvent_t> ev((size_t)nsteps * (PIBM_NPHASE + 1));
+    if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "pibm_run_profiled starts at a step boundary");
+    const int nst = nsteps * h->itrmax;   // stages, each with its own phase events
+    std::vector<cudaEvent_t> ev((size_t)nst * (PIBM_NPHASE + 1));
     for (auto &e : ev) CUDA_OR_FAIL(cudaEventCreate(&e));
-    for (int s = 0; s < nsteps; ++s) {
-        enqueue_step(h->g, h->b, h->cur, h->stream, &ev[(size_t)s * (PIBM_NPHASE + 1)], nullptr);
+    for (int s = 0; s < nst; ++s) {
+        enqueue_step(h->gs[s % h->itrmax], h->b, h->cur, h->stream, &ev[(size_t)s * (PIBM_NPHASE + 1)], nullptr);
         h->cur ^= 1;
     }
     CUDA_OR_FAIL(cudaGetLastError());
     CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
     for (int q = 0; q < nphase; ++q) phase_ms[q] = 0.0;
-    for (int s = 0; s < nsteps; ++s)
+    for (int s = 0; s < nst; ++s)
         for (int q = 0; q < nphase; ++q) {
             float ms = 0.f;
             CUDA_OR_FAIL(cudaEventElapsedTime(&ms, ev[(size_t)s * (PIBM_NPHASE + 1) + q], ev[(size_t)s * (PIBM_NPHASE + 1) + q + 1]));
@@ -494,6 +521,7 @@ int pibm_set_state(pibm_handle *h, const pibm_state_view *s) {
     for (int d = 0; d < 3; ++d) { sc.umean[d] = s->umean[d]; sc.mpg[d] = s->mpg[d]; sc.ufmean[d] = s->ufmean[d]; }
     sc.t = s->t; sc.dt = s->dt; sc.cf = s->cf;
     sc.status = 0;
+    h->next_rks = 1;   // a restart begins a time step
     if (h->g.moving && h->S.dem_soft) {
         // the step graphs hold max_factor DEM sub-steps; a larger dt needs more
         Mov &m = h->b.mov;
@@ -787,7 +815,7 @@ static int batch_graphs(pibm_batch *bt) {
             pibm_handle *h = bt->members[q];
             const bool big = h->g.my >= 128;
             CUDA_OR_FAIL(cudaStreamWaitEvent(h->stream, (big && prev_big >= 0) ? bt->join[prev_big] : bt->fork, 0));
-            enqueue_step(h->g, h->b, bt->base[q] ^ par, h->stream, nullptr, &h->ss);
+            enqueue_time_step(h, bt->base[q] ^ par, h->stream, &h->ss);
             CUDA_OR_FAIL(cudaEventRecord(bt->join[q], h->stream));
             CUDA_OR_FAIL(cudaStreamWaitEvent(bt->stream, bt->join[q], 0));
             if (big) prev_big = q;

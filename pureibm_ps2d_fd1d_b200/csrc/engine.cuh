@@ -11,8 +11,9 @@ struct Geo {
     int PS;             // complex elements per spectral plane (my2*mz)
     int RS;             // real elements per physical plane (my*mz)
     double dx, dx2, rdx2, dx3, vis, nrm;   // nrm = float(my*mz) as in ff2rc
-    double c1, c2, c3, c4;
+    double c1, c2, c3, c4;   // coef(rks, 1:4) of the stage this Geo is launched for
     int scheme, limiter, include_frmeanfluid, revernorm, set_mpg, adaptive;
+    int dt_update;      // this stage takes the new dt (rks == itrmax, dependent_functions.F90:1246-1250)
     double cfl_max, ramp_frac_time, ucharmod, char_length, voldom, maxvolfrac, mean_volfrac, rhof, rhos;
     long long count_fluid, ncell;
     int plane_ctas;     // CTAs per plane in the plane kernels

@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *p
         ms[d] = (1.0 - sc->maxvolfrac) * (sc->usmean[d] - sc->ufmean[d]);
     }
     sc->mixmeanslipmod = sqrt(ms[0] * ms[0] + ms[1] * ms[1] + ms[2] * ms[2]);
-    if (g.adaptive) sc->dt = dtnew;
+    if (g.adaptive && g.dt_update) sc->dt = dtnew;
     sc->t = sc->t + sc->dt * (g.c1 + g.c2);
     const double tempt = g.ramp_frac_time * (double)(float)(g.nx) * g.dx / g.ucharmod;
     sc->cf = -1.0 / sc->dt;
