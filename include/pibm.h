@@ -173,6 +173,16 @@ int  pibm_get_particles(pibm_handle *h, double *pres, double *visc, double *forc
  * grad phi . n (calc_bndrev_data), ratios[0..2] = heat_ratio,
  * heat_ratio_old, Nusselt number.  Any pointer may be NULL. */
 int  pibm_get_scalar(pibm_handle *h, double *phif, double *flux_body, double *ratios);
+/* Desired mean particle and fluid velocities of a restarted run (the u
+ * restart file's usmean_des, ufmean_des: restart_funcs.F90:450-452). */
+int  pibm_set_desired_means(pibm_handle *h, const double usmean_des[3], const double ufmean_des[3]);
+/* The scalar's nonlinear term of the last step, nlphif complex (nx+1,my2,mz)
+ * interleaved (plane nx+1 = nlphif(1)/heat_ratio of that step). */
+int  pibm_get_scalar_nl(pibm_handle *h, double *nlphif);
+/* Scalar restart (read_unformatted, restart_funcs.F90:560-590): phif and
+ * nlphif complex (nx+1,my2,mz) interleaved, ratios[0..1] = heat_ratio,
+ * heat_ratio_old.  Call after pibm_set_state. */
+int  pibm_set_scalar(pibm_handle *h, const double *phif, const double *nlphif, const double *ratios);
 /* Moving particles (IMOVE = 1): the DEM lists of the last step in the
  * reference layout NEIGHBOURS / PN / PV (nbody, maxn) column-major
  * (dem_mod.F90; collision_mod.F90:807-1062, soft_sphere_coll.F90:120-420):

@@ -48,6 +48,9 @@ def lib():
         L.orc_get_field.argtypes = [vp, C.c_int, P(C.c_double)]
         L.orc_get_scalar.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_double)]
         L.orc_get_contacts.argtypes = [vp, C.c_int, P(C.c_int32), P(C.c_int32), P(C.c_int32)]
+        L.orc_get_scalar_nl.argtypes = [vp, P(C.c_double)]
+        L.orc_set_scalar.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_double)]
+        L.orc_set_desired_means.argtypes = [vp, P(C.c_double), P(C.c_double)]
         L.orc_ff2rc.argtypes = [C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
         L.orc_ff2cr.argtypes = [C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
         L.orc_cyclic_solve.argtypes = [C.c_int] + [P(C.c_double)] * 7
@@ -128,7 +131,33 @@ class OracleSolver:
         rc = lib().orc_step(self.h, C.byref(rep))
         if rc != 0:
             raise RuntimeError("orc_step failed with code %d" % rc)
-        return rep.as_dict()
+        self.last_report = rep.as_dict()
+        return self.last_report
+
+    @property
+    def params(self):
+        return self._keep[0]
+
+    def get_scalar(self) -> dict:
+        out = get_scalar(self)
+        nl = np.zeros_like(out["phif"])
+        if lib().orc_get_scalar_nl(self.h, nl.ctypes.data_as(C.POINTER(C.c_double))) != 0:
+            raise RuntimeError("oracle has no scalar (ISCALON = 0)")
+        out["nlphif"] = nl
+        return out
+
+    def set_desired_means(self, usmean_des, ufmean_des):
+        a = np.ascontiguousarray(usmean_des, dtype=np.float64)
+        b = np.ascontiguousarray(ufmean_des, dtype=np.float64)
+        lib().orc_set_desired_means(self.h, _dp(a), _dp(b))
+
+    def set_scalar(self, phif, nlphif, heat_ratio, heat_ratio_old):
+        a = np.ascontiguousarray(phif, dtype=np.complex128)
+        b = np.ascontiguousarray(nlphif, dtype=np.complex128)
+        r = np.array([heat_ratio, heat_ratio_old], dtype=np.float64)
+        if lib().orc_set_scalar(self.h, a.ctypes.data_as(C.POINTER(C.c_double)),
+                                b.ctypes.data_as(C.POINTER(C.c_double)), _dp(r)) != 0:
+            raise RuntimeError("oracle has no scalar (ISCALON = 0)")
 
     def step_rks(self, rks: int) -> dict:
         """One stage rks of the driver's loop."""

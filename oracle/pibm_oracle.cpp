@@ -2140,6 +2140,31 @@ extern "C" int orc_get_scalar(void *h, double *phif, double *flux_body, double *
     return PIBM_OK;
 }
 
+extern "C" int orc_get_scalar_nl(void *h, double *nlphif) {
+    Orc &o = *(Orc *)h;
+    if (!o.scal) return PIBM_ERR_ARG;
+    std::memcpy((void *)nlphif, o.nlphif.data(), o.nlphif.size() * sizeof(cplx));
+    return PIBM_OK;
+}
+
+// usmean_des / ufmean_des read from a restart (restart_funcs.F90:450-452).
+extern "C" int orc_set_desired_means(void *h, const double *usd, const double *ufd) {
+    Orc &o = *(Orc *)h;
+    for (int d = 0; d < 3; ++d) { o.usmean_des[d] = usd[d]; o.ufmean_des[d] = ufd[d]; }
+    return PIBM_OK;
+}
+
+// read_unformatted's scalar part (restart_funcs.F90:560-590).
+extern "C" int orc_set_scalar(void *h, const double *phif, const double *nlphif, const double *ratios) {
+    Orc &o = *(Orc *)h;
+    if (!o.scal) return PIBM_ERR_ARG;
+    std::memcpy((void *)o.phif.data(), phif, o.phif.size() * sizeof(cplx));
+    std::memcpy((void *)o.nlphif.data(), nlphif, o.nlphif.size() * sizeof(cplx));
+    o.heat_ratio = ratios[0];
+    o.heat_ratio_old = ratios[1];
+    return PIBM_OK;
+}
+
 // sizes of the ABI structs as compiled from include/pibm.h (for the ctypes mirror test)
 // DEM lists in the reference layout NEIGHBOURS/PN/PV(nbody, maxn): column 1 the
 // count (PV: 1), columns 2.. 1-based particle numbers, then -1 (PV: 0).

@@ -93,6 +93,7 @@ class Solver:
     def _attach(self, h):
         lib = load_library()
         self.h = h
+        self.last_report = None
         info = pibm_info()
         _check(lib.pibm_info_get(self.h, C.byref(info)))
         self.info = info
@@ -117,13 +118,15 @@ class Solver:
         """compute_new_timestep -> nonlinear -> bcset -> velstep (one rks iteration)."""
         rep = pibm_step_report()
         _check(load_library().pibm_step(self.h, rks, C.byref(rep)))
-        return rep.as_dict()
+        self.last_report = rep.as_dict()
+        return self.last_report
 
     def run(self, nsteps: int) -> dict:
         """nsteps steps replayed from CUDA graphs, diagnostics of the last one."""
         rep = pibm_step_report()
         _check(load_library().pibm_run(self.h, int(nsteps), C.byref(rep)))
-        return rep.as_dict()
+        self.last_report = rep.as_dict()
+        return self.last_report
 
     # -- state in the reference layout -------------------------------------------
     def get_state(self) -> dict:
@@ -176,8 +179,24 @@ class Solver:
         flux = np.zeros(max(self.nbody, 1))
         ratios = np.zeros(3)
         _check(load_library().pibm_get_scalar(self.h, phif.ctypes.data_as(C.POINTER(C.c_double)), _dp(flux), _dp(ratios)))
-        return dict(phif=phif, flux_body=flux[:self.nbody], heat_ratio=ratios[0], heat_ratio_old=ratios[1],
-                    nusselt=ratios[2])
+        nlphif = np.zeros_like(phif)
+        _check(load_library().pibm_get_scalar_nl(self.h, nlphif.ctypes.data_as(C.POINTER(C.c_double))))
+        return dict(phif=phif, nlphif=nlphif, flux_body=flux[:self.nbody], heat_ratio=ratios[0],
+                    heat_ratio_old=ratios[1], nusselt=ratios[2])
+
+    def set_desired_means(self, usmean_des, ufmean_des):
+        """usmean_des / ufmean_des of a restarted run."""
+        a = np.ascontiguousarray(usmean_des, dtype=np.float64)
+        b = np.ascontiguousarray(ufmean_des, dtype=np.float64)
+        _check(load_library().pibm_set_desired_means(self.h, _dp(a), _dp(b)))
+
+    def set_scalar(self, phif, nlphif, heat_ratio: float, heat_ratio_old: float):
+        """Scalar restart: phif and the last step's nlphif as (mz, my2, nx+1)."""
+        a = np.ascontiguousarray(phif, dtype=np.complex128)
+        b = np.ascontiguousarray(nlphif, dtype=np.complex128)
+        r = np.array([heat_ratio, heat_ratio_old], dtype=np.float64)
+        _check(load_library().pibm_set_scalar(self.h, a.ctypes.data_as(C.POINTER(C.c_double)),
+                                              b.ctypes.data_as(C.POINTER(C.c_double)), _dp(r)))
 
     def get_if_rev(self) -> np.ndarray:
         out = np.zeros(self.nbnd * self.nbody, dtype=np.uint8)

@@ -104,8 +104,8 @@ class pibm_info(C.Structure):
 EXPORTED = [
     "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed",
     "pibm_run_profiled", "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev",
-    "pibm_get_fluid_mask", "pibm_get_contacts",
-    "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
+    "pibm_get_fluid_mask", "pibm_get_contacts", "pibm_get_scalar_nl", "pibm_set_scalar",
+    "pibm_set_desired_means", "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
     "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time", "pibm_batch_member",
     "pibm_batch_destroy",
 ]
@@ -128,6 +128,9 @@ def bind(lib):
     lib.pibm_get_if_rev.argtypes = [vp, P(C.c_uint8)]
     lib.pibm_get_fluid_mask.argtypes = [vp, P(C.c_uint8)]
     lib.pibm_get_contacts.argtypes = [vp, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32)]
+    lib.pibm_get_scalar_nl.argtypes = [vp, P(_f64)]
+    lib.pibm_set_scalar.argtypes = [vp, P(_f64), P(_f64), P(_f64)]
+    lib.pibm_set_desired_means.argtypes = [vp, P(_f64), P(_f64)]
     lib.pibm_destroy.argtypes = [vp]
     lib.pibm_destroy.restype = None
     lib.pibm_last_error.argtypes = []
@@ -144,7 +147,7 @@ def bind(lib):
     lib.pibm_batch_destroy.restype = None
     for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed", "pibm_run_profiled",
                  "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev", "pibm_get_fluid_mask",
-                 "pibm_get_contacts",
+                 "pibm_get_contacts", "pibm_get_scalar_nl", "pibm_set_scalar", "pibm_set_desired_means",
                  "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
         getattr(lib, name).restype = C.c_int
     return lib

@@ -33,6 +33,7 @@ void enqueue_d2f(const double2 *d, double2 *f, int nx, int nxf, int PS, int ncom
 int real_offset(int n, int z, int y);
 int plane_ctas(int n);
 void enqueue_scalar(const Geo &g, DevBufs &b, int cur, cudaStream_t s);
+void enqueue_scalar_c2r(const Geo &g, const double2 *src, double *dst, int nplanes, cudaStream_t s);
 int scalar_kernels_per_step(const Geo &g);
 cudaError_t configure_scalar_kernels(int n);
 }  // namespace pibm
@@ -612,6 +613,73 @@ int pibm_get_scalar(pibm_handle *h, double *phif, double *flux_body, double *rat
     }
     if (flux_body) for (int m = 0; m < g.nbody; ++m) flux_body[m] = fb[m];
     if (ratios) { ratios[0] = sc.heat_ratio; ratios[1] = sc.heat_ratio_old; ratios[2] = sc.nusselt; }
+    return PIBM_OK;
+}
+
+// usmean_des / ufmean_des of a restarted run (read_unformatted reads them from
+// the u file, restart_funcs.F90:450-452) instead of the set-up's values.
+int pibm_set_desired_means(pibm_handle *h, const double *usmean_des, const double *ufmean_des) {
+    if (!h || !usmean_des || !ufmean_des) return fail(PIBM_ERR_ARG, "null argument");
+    for (Geo *g : {&h->g, &h->gs[0], &h->gs[1], &h->gs[2]})
+        for (int d = 0; d < 3; ++d) { g->usmean_des[d] = usmean_des[d]; g->ufmean_des[d] = ufmean_des[d]; }
+    for (auto &gx : h->graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }   // kernels take Geo by value
+    return PIBM_OK;
+}
+
+// The scalar's nonlinear term of the last step, nlphif(nx+1, my2, mz) in the
+// reference layout; plane nx+1 is nlphif(1)/heat_ratio of that step
+// (nl_allphi.F90:219), i.e. /heat_ratio_old after the step.
+int pibm_get_scalar_nl(pibm_handle *h, double *nlphif) {
+    if (!h || !nlphif) return fail(PIBM_ERR_ARG, "null argument");
+    if (!h->g.scal) return fail(PIBM_ERR_ARG, "this run has no scalar (ISCALON = 0)");
+    const Geo &g = h->g;
+    Scal sc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    std::vector<double2> dev((size_t)g.nx * g.PS);
+    CUDA_OR_FAIL(cudaMemcpyAsync(dev.data(), h->b.nls[h->cur ^ 1], dev.size() * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    const size_t nxf = (size_t)g.nx + 1;
+    for (int k = 0; k < g.mz; ++k)
+        for (int j = 0; j < g.my2; ++j) {
+            const size_t e = (size_t)k * g.my2 + j;
+            for (int i = 0; i < g.nx; ++i) {
+                const double2 v = dev[(size_t)i * g.PS + e];
+                nlphif[2 * (i + nxf * e)] = v.x;
+                nlphif[2 * (i + nxf * e) + 1] = v.y;
+            }
+            nlphif[2 * (g.nx + nxf * e)] = dev[e].x / sc.heat_ratio_old;
+            nlphif[2 * (g.nx + nxf * e) + 1] = dev[e].y / sc.heat_ratio_old;
+        }
+    return PIBM_OK;
+}
+
+// Restart of the scalar (read_unformatted, restart_funcs.F90:560-590): phif and
+// the last step's nlphif in the reference layout (nx+1, my2, mz), and
+// ratios[0..1] = heat_ratio, heat_ratio_old.  The real nonlinear term the next
+// step's forcing reads is the c2r of nlphif's nx+1 planes.
+int pibm_set_scalar(pibm_handle *h, const double *phif, const double *nlphif, const double *ratios) {
+    if (!h || !phif || !nlphif || !ratios) return fail(PIBM_ERR_ARG, "null argument");
+    if (!h->g.scal) return fail(PIBM_ERR_ARG, "this run has no scalar (ISCALON = 0)");
+    const Geo &g = h->g;
+    const int nxf = g.nx + 1;
+    const size_t nf = (size_t)nxf * g.PS;
+    if (!h->stage) CUDA_OR_FAIL(h->alloc(&h->stage, 3 * nf));
+    double2 *fin = h->stage, *dplanes = h->stage + nf;   // reference layout in, device planes out
+    const int prev = h->cur ^ 1;
+    CUDA_OR_FAIL(cudaMemcpyAsync(fin, phif, nf * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    enqueue_f2d(fin, h->b.phif, g.nx, nxf, g.PS, 1, h->stream);
+    CUDA_OR_FAIL(cudaMemcpyAsync(fin, nlphif, nf * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    enqueue_f2d(fin, dplanes, nxf, nxf, g.PS, 1, h->stream);
+    CUDA_OR_FAIL(cudaMemcpyAsync(h->b.nls[prev], dplanes, (size_t)g.nx * g.PS * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    enqueue_scalar_c2r(g, dplanes, h->b.nlr[prev], nxf, h->stream);
+    CUDA_OR_FAIL(cudaGetLastError());
+    Scal sc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    sc.heat_ratio = ratios[0];
+    sc.heat_ratio_old = ratios[1];
+    CUDA_OR_FAIL(cudaMemcpyAsync(h->b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
     return PIBM_OK;
 }
 

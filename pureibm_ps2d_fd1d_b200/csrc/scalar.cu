@@ -296,6 +296,28 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_simg(Geo g, const dou
     if (threadIdx.x == 0) { bulk_store(nlr + (size_t)g.nx * RSP + (size_t)rank * L::RL, buf, L::RBYTES); bulk_wait_all(); }
 }
 
+// k_sreal: c2r of spectral planes into the real-field layout of the step
+// (transform order, RSP doubles per plane): restores the real nonlinear term
+// of a restarted scalar (pibm_set_scalar).
+template <int N>
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_sreal(Geo g, const double2 *__restrict__ src, double *__restrict__ dst) {
+    using L = PL<N>;
+    extern __shared__ double2 sm[];
+    constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
+    double2 *buf = sm, *tws = sm + L::BUF;
+    load_tw<N>(tws, g);
+    const int p = blockIdx.x / L::C, rank = blockIdx.x % L::C;
+    const TwT tw{tws, N};
+    for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
+        const int kz = e / L::PZ, jl = e - kz * L::PZ;
+        if (jl == L::MC && rank != 0) continue;
+        buf[e] = src[(size_t)p * PS + kz * my2 + cl_col<N>(jl, rank)];
+    }
+    __syncthreads();
+    cl_c2r<N>(buf, tw, rank);
+    if (threadIdx.x == 0) { bulk_store(dst + (size_t)p * RSP + (size_t)rank * L::RL, buf, L::RBYTES); bulk_wait_all(); }
+}
+
 // ============================================================================
 // Scalar interpolation (interpolate_phidata, SRC/SCALAR/bc_scalar.F90:1036-1153,
 // serial): stencil [pc, pc+1] on raw x cells; a corner below plane 1 wraps by
@@ -711,6 +733,21 @@ void enqueue_scalar(const Geo &g, DevBufs &b, int cur, cudaStream_t s) {
     }
 }
 
+template <int N>
+static void enqueue_scalar_c2r_t(const Geo &g, const double2 *src, double *dst, int nplanes, cudaStream_t s) {
+    launch_planes<N>(k_sreal<N>, nplanes, 1, s, g, src, dst);
+}
+// c2r of nplanes spectral planes into the step's real layout.
+void enqueue_scalar_c2r(const Geo &g, const double2 *src, double *dst, int nplanes, cudaStream_t s) {
+    switch (g.my) {
+        case 32: enqueue_scalar_c2r_t<32>(g, src, dst, nplanes, s); break;
+        case 64: enqueue_scalar_c2r_t<64>(g, src, dst, nplanes, s); break;
+        case 96: enqueue_scalar_c2r_t<96>(g, src, dst, nplanes, s); break;
+        case 128: enqueue_scalar_c2r_t<128>(g, src, dst, nplanes, s); break;
+        case 256: enqueue_scalar_c2r_t<256>(g, src, dst, nplanes, s); break;
+    }
+}
+
 int scalar_kernels_per_step(const Geo &g) {
     if (!g.scal) return 0;
     int n = 8;   // sa, sheat, sflux, snl, simg, sff, slines, sfin
@@ -727,6 +764,7 @@ static cudaError_t set_scalar_attrs() {
     if ((e = cudaFuncSetAttribute(k_sa<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_snl<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_simg<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_sreal<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_sff<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_slines<N, SLinesCfg<N>::LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slines_smem<N>());
 }
