@@ -57,6 +57,7 @@ def lib():
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_set_threads.restype = None
         L.orc_last_error.restype = C.c_char_p
+        L.orc_adjoint.argtypes = [vp, C.c_int] + [P(C.c_double)] * 8
         L.orc_sizeof.argtypes = [C.c_int]
         L.orc_sizeof.restype = C.c_int
         _lib = L
@@ -192,6 +193,30 @@ class OracleSolver:
             s.umean[d] = st["umean"][d]; s.mpg[d] = st["mpg"][d]; s.ufmean[d] = st["ufmean"][d]
         s.t, s.dt, s.cf = st["t"], st["dt"], st["cf"]
         lib().orc_set_state(self.h, C.byref(s))
+
+    def adjoint(self, nsteps: int, direction=(1.0, 0.0, 0.0), state_grad: bool = False):
+        """K = nsteps AB2 steps from the current state and the discrete
+        adjoint of J = (1/K) sum_n e . sum_m (pres_m + visc_m).  Returns
+        dict(J, g_xc (nbody,3), g_mpg (3,)) and, with state_grad, lambda of the
+        initial u, p, nl (state layout) and umean.  The solver ends at the state
+        after K steps."""
+        e = np.ascontiguousarray(direction, dtype=np.float64)
+        J = C.c_double()
+        g = np.zeros(3 * self.nbody)
+        gm = np.zeros(3)
+        st = self.get_state() if state_grad else None
+        lu = np.zeros_like(st["u"]) if state_grad else None
+        lp = np.zeros_like(st["p"]) if state_grad else None
+        lnl = np.zeros_like(st["nl"]) if state_grad else None
+        lum = np.zeros(3) if state_grad else None
+        cp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+        rc = lib().orc_adjoint(self.h, int(nsteps), _dp(e), C.byref(J), _dp(g), _dp(gm), cp(lu), cp(lp), cp(lnl), cp(lum))
+        if rc != 0:
+            raise RuntimeError("orc_adjoint failed with code %d: %s" % (rc, lib().orc_last_error().decode()))
+        out = dict(J=J.value, g_xc=g.reshape(3, self.nbody).T.copy(), g_mpg=gm)
+        if state_grad:
+            out.update(lu=lu, lp=lp, lnl=lnl, lumean=lum)
+        return out
 
     def get_particles(self):
         n = self.nbody

@@ -1988,6 +1988,8 @@ int step(Orc &o, pibm_step_report *rep) {
     return PIBM_OK;
 }
 
+#include "adjoint_oracle.inc"
+
 }  // namespace
 
 // ============================================================================
@@ -2168,6 +2170,23 @@ extern "C" int orc_set_scalar(void *h, const double *phif, const double *nlphif,
 // sizes of the ABI structs as compiled from include/pibm.h (for the ctypes mirror test)
 // DEM lists in the reference layout NEIGHBOURS/PN/PV(nbody, maxn): column 1 the
 // count (PV: 1), columns 2.. 1-based particle numbers, then -1 (PV: 0).
+// Discrete adjoint (test infrastructure): K AB2 steps from the current state,
+// J = (1/K) sum_n e . sum_m (pres + visc), gradients w.r.t. xc (nbody,3) and
+// mpg(3); lu0/lp0/lnl0 (optional) receive lambda of the initial u, p, nl in
+// the state layout, lumean0 lambda of the initial umean.
+extern "C" int orc_adjoint(void *h, int K, const double *e, double *J, double *gxc, double *gmpg,
+                           double *lu0, double *lp0, double *lnl0, double *lumean0) {
+    Orc &o = *(Orc *)h;
+    AdjState A;
+    const int rc = adjoint_run(o, K, e, J, gxc, gmpg, &A);
+    if (rc) return rc;
+    if (lu0) std::memcpy(lu0, A.lu.data(), A.lu.size() * sizeof(cplx));
+    if (lp0) std::memcpy(lp0, A.lp.data(), A.lp.size() * sizeof(cplx));
+    if (lnl0) std::memcpy(lnl0, A.lnl.data(), A.lnl.size() * sizeof(cplx));
+    if (lumean0) for (int d = 0; d < 3; ++d) lumean0[d] = A.lumean[d];
+    return PIBM_OK;
+}
+
 extern "C" int orc_get_contacts(void *h, int maxn, int32_t *neigh, int32_t *pn, int32_t *pv) {
     Orc &o = *(Orc *)h;
     if (!o.moving) return PIBM_ERR_ARG;

@@ -241,6 +241,29 @@ def random_array(my: int = 128, dia_cells: float = 20.0, phi: float = 0.2, re: f
     return prm, pts
 
 
+def adjoint_case(my: int = 96, dia_cells: float = 16.0, nbody: int = 30, seed: int = 4242, re: float = 20.0,
+                 vis: float = 0.012, cfl: float = 0.1, mc_moves: int = 200):
+    """Fixed random sphere array for gradient (adjoint) runs: SET_MPG with an
+    imposed mean pressure gradient, a fixed time step (ADAPTIVE = F) and the
+    upwind x flux.  The run starts from a uniform mean flow umean0 = (uchar,
+    0, 0) (returned as prm['umean0']); the imposed mpg is about the Stokes
+    drag of the array per unit fluid volume, so the mean flow stays of order
+    uchar.  96^3 with 30 spheres of 16 cells is phi = 0.073."""
+    prm = default_params()
+    uchar = re * vis / 1.0
+    volume = (my / dia_cells) ** 3
+    mpg_x = -nbody * 3.0 * np.pi * vis * uchar * 2.0 / volume
+    prm.update(my=my, lybyd=my / dia_cells, dbydx=dia_cells, re=re, vis=vis, cfl=cfl, cfl_max=0.5,
+               discr_scheme="upwind", initialize_zero=True, dobnd=False, ramp_frac_steps=0,
+               set_mpg=True, adaptive=False, mpg=(mpg_x, 0.0, 0.0))
+    prm["umean0"] = (uchar, 0.0, 0.0)
+    rng = np.random.default_rng(seed)
+    pts = random_sequential_addition(nbody, float(my), dia_cells, rng)
+    if mc_moves:
+        pts, _ = hard_sphere_mc(pts, float(my), dia_cells, rng, mc_moves, 0.1 * dia_cells)
+    return prm, pts
+
+
 def moving_array(my: int = 64, dia_cells: float = 12.0, nbody: int = 12, seed: int = 11, re: float = 20.0,
                  rhos: float = 100.0, coeff_rest: float = 0.9, vel_spread: float = 0.1, mc_moves: int = 200,
                  collision_type: str = "softsphere", vis: float = 0.012):
