@@ -230,6 +230,33 @@ int  pibm_ff2cr(int my, int mz, int nplanes, const double *a, double *b);
  * stream) and the call returns without waiting for it. */
 int  pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *d_b, void *stream);
 
+/* ---- discrete adjoint (no counterpart in the reference) ----
+ * K = nsteps AB2 steps from the handle's current state, then the exact
+ * discrete adjoint of the step sequence for the objective
+ *     J = (1/K) sum_{n=1..K} e . sum_m (pres_m + visc_m),
+ * the summed pressure + viscous surface force of calc_pres_visc_drag
+ * (boundary_condition.F90:1481-1645) evaluated inside step n and projected on
+ * e = direction[3].  Returns dJ/dxc in g_xc (nbody,3) column-major (grid
+ * units, the layout of pibm_particles.xc) and dJ/dmpg in g_mpg[3].  The
+ * forward trajectory is kept as checkpoints every checkpoint_every steps and
+ * recomputed segment by segment in the reverse sweep.  The handle ends at the
+ * state after the K steps, as after pibm_run(h, K).
+ * Supported runs: fixed spheres, AB2, SET_MPG (imposed mean pressure
+ * gradient), ADAPTIVE = F (fixed dt), DORPR, INCLUDE_FRMEANFLUID = F, no
+ * scalar; otherwise PIBM_ERR_ARG.  The solid mask, the active reversal
+ * points and the upwind branches are those of the forward run (the gradient
+ * of the piecewise-smooth map on the trajectory's branch). */
+typedef struct pibm_adjoint_report {
+    double J;                 /* the objective */
+    double forward_ms;        /* device time of the K forward steps with checkpoints */
+    double reverse_ms;        /* device time of the reverse sweep: recomputation + adjoint steps */
+    int32_t nsteps, checkpoint_every;
+    int32_t adjoint_kernels_per_step;   /* own kernel launches per reverse step (without the recomputed forward step) */
+    int32_t reserved;
+} pibm_adjoint_report;
+int  pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const double direction[3],
+                      double *g_xc, double g_mpg[3], pibm_adjoint_report *rep);
+
 /* ---- batched independent realizations (the MIS ensemble of
  *      sample_inputs/set_mis_3d, run as one graph-captured launch stream) ---- */
 typedef struct pibm_batch pibm_batch;

@@ -16,7 +16,7 @@ from typing import Optional
 import numpy as np
 
 from . import abi
-from .abi import pibm_params, pibm_state_view, pibm_step_report, pibm_info
+from .abi import pibm_params, pibm_state_view, pibm_step_report, pibm_info, pibm_adjoint_report
 from . import config
 
 __all__ = ["Solver", "Batch", "load_library", "ff2rc", "ff2cr", "config", "abi", "PibmError"]
@@ -183,6 +183,20 @@ class Solver:
         _check(load_library().pibm_get_scalar_nl(self.h, nlphif.ctypes.data_as(C.POINTER(C.c_double))))
         return dict(phif=phif, nlphif=nlphif, flux_body=flux[:self.nbody], heat_ratio=ratios[0],
                     heat_ratio_old=ratios[1], nusselt=ratios[2])
+
+    def adjoint(self, nsteps: int, direction=(1.0, 0.0, 0.0), checkpoint_every: int = 20) -> dict:
+        """nsteps steps from the current state and the discrete adjoint of
+        J = (1/K) sum_n e . sum_m (pres_m + visc_m) (pibm_adjoint_run).
+        Returns dict(J, g_xc (nbody,3), g_mpg (3,), forward_ms, reverse_ms)."""
+        lib = load_library()
+        e = np.ascontiguousarray(direction, dtype=np.float64)
+        g = np.zeros(3 * self.nbody)
+        gm = np.zeros(3)
+        rep = pibm_adjoint_report()
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        _check(lib.pibm_adjoint_run(self.h, int(nsteps), int(checkpoint_every), dp(e), dp(g), dp(gm), C.byref(rep)))
+        return dict(J=rep.J, g_xc=g.reshape(3, self.nbody).T.copy(), g_mpg=gm, forward_ms=rep.forward_ms,
+                    reverse_ms=rep.reverse_ms, adjoint_kernels_per_step=rep.adjoint_kernels_per_step)
 
     def set_desired_means(self, usmean_des, ufmean_des):
         """usmean_des / ufmean_des of a restarted run."""

@@ -36,6 +36,10 @@ void enqueue_scalar(const Geo &g, DevBufs &b, int cur, cudaStream_t s);
 void enqueue_scalar_c2r(const Geo &g, const double2 *src, double *dst, int nplanes, cudaStream_t s);
 int scalar_kernels_per_step(const Geo &g);
 cudaError_t configure_scalar_kernels(int n);
+void enqueue_adjoint_step(const Geo &g, const DevBufs &b, const AdjBufs &a, const double e[3], double wJ, cudaStream_t s);
+void enqueue_adjoint_jacc(const Scal *sc, AdjScal *as, const double e[3], cudaStream_t s);
+int adjoint_kernels_per_step(const Geo &g);
+cudaError_t configure_adjoint_kernels(int n);
 }  // namespace pibm
 
 using namespace pibm;
@@ -79,6 +83,8 @@ struct pibm_handle {
     int device = 0;
     double2 *stage = nullptr;   // reference-layout staging buffer of get/set_state (allocated once)
     StepStreams ss;             // side streams of the forked step (graphs and pibm_step)
+    AdjBufs adj{};              // adjoint work arrays (allocated by the first pibm_adjoint_run)
+    bool adj_ready = false;
 
     template <class T> cudaError_t alloc(T **p, size_t n) {
         void *q = nullptr;
@@ -552,6 +558,149 @@ int pibm_get_particles(pibm_handle *h, double *pres, double *visc, double *force
     if (!h->g.moving) {
         if (xc) std::memcpy(xc, h->S.xc.data(), n * sizeof(double));
         if (vel) std::memcpy(vel, h->S.vel.data(), n * sizeof(double));
+    }
+    return PIBM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint: forward with checkpoints, reverse sweep segment by segment.
+// A state slot holds u, p, the latest nl (the next step's onl) and Scal; the
+// parity of the nl ping-pong at the slot is kept on the host.
+// ---------------------------------------------------------------------------
+namespace {
+struct SlotSet {
+    char *base = nullptr;
+    size_t bytes = 0;          // per slot
+    std::vector<int> cur;
+};
+size_t slot_bytes(const pibm_handle *h) {
+    const size_t SC = (size_t)h->g.nx * h->g.PS * sizeof(double2);
+    return 7 * SC + ((sizeof(Scal) + 255) / 256) * 256;
+}
+void slot_save(pibm_handle *h, char *slot) {
+    const size_t SC = (size_t)h->g.nx * h->g.PS * sizeof(double2);
+    cudaMemcpyAsync(slot, h->b.u, 3 * SC, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(slot + 3 * SC, h->b.p, SC, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(slot + 4 * SC, h->b.nl[h->cur ^ 1], 3 * SC, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(slot + 7 * SC, h->b.sc, sizeof(Scal), cudaMemcpyDeviceToDevice, h->stream);
+}
+void slot_restore(pibm_handle *h, const char *slot, int cur) {
+    const size_t SC = (size_t)h->g.nx * h->g.PS * sizeof(double2);
+    h->cur = cur;
+    cudaMemcpyAsync(h->b.u, slot, 3 * SC, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->b.p, slot + 3 * SC, SC, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->b.nl[h->cur ^ 1], slot + 4 * SC, 3 * SC, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->b.sc, slot + 7 * SC, sizeof(Scal), cudaMemcpyDeviceToDevice, h->stream);
+}
+}  // namespace
+
+int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const double direction[3], double *g_xc, double g_mpg[3],
+                     pibm_adjoint_report *rep) {
+    if (!h || nsteps < 1 || checkpoint_every < 1 || !direction || !g_xc || !g_mpg) return fail(PIBM_ERR_ARG, "bad argument");
+    const Geo &g = h->g;
+    if (g.moving || g.scal || h->itrmax != 1 || !g.set_mpg || g.adaptive || g.include_frmeanfluid || !h->prm.dorpr || g.nbody < 1)
+        return fail(PIBM_ERR_ARG, "adjoint: fixed spheres, AB2, SET_MPG, ADAPTIVE = F, DORPR, INCLUDE_FRMEANFLUID = F and no scalar only");
+    if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "pibm_adjoint_run starts at a step boundary");
+    int rc = pibm_run(h, 0, nullptr);   // step graphs
+    if (rc) return rc;
+    AdjBufs &a = h->adj;
+    const size_t SC = (size_t)g.nx * g.PS, CR = (size_t)g.nx * (size_t)(g.my * (g.my + 2));
+    if (!h->adj_ready) {
+        CUDA_OR_FAIL(configure_adjoint_kernels(g.my));
+        double *R10 = nullptr;
+        const bool ok = h->alloc(&a.lu, 3 * SC) == cudaSuccess && h->alloc(&a.lp, SC) == cudaSuccess &&
+                        h->alloc(&a.lnl, 3 * SC) == cudaSuccess && h->alloc(&a.lu2, 3 * SC) == cudaSuccess &&
+                        h->alloc(&a.lp2, SC) == cudaSuccess && h->alloc(&a.lnl_new, 3 * SC) == cudaSuccess &&
+                        h->alloc(&a.lonl, 3 * SC) == cudaSuccess && h->alloc(&a.lff, 3 * SC) == cudaSuccess &&
+                        h->alloc(&a.T, 10 * SC) == cudaSuccess && h->alloc(&a.lfr, 3 * CR) == cudaSuccess &&
+                        h->alloc(&R10, 10 * CR) == cudaSuccess && h->alloc(&a.lQ, 3 * CR) == cudaSuccess &&
+                        h->alloc(&a.W8, 8 * CR) == cudaSuccess && h->alloc(&a.gxc, 3 * (size_t)g.nbody) == cudaSuccess &&
+                        h->alloc(&a.as, 1) == cudaSuccess;
+        if (!ok) return fail(PIBM_ERR_NOMEM, "adjoint work arrays");
+        a.lubcp = R10; a.lomega = R10 + 3 * CR; a.lpbcp = R10 + 6 * CR; a.lpgr = R10 + 7 * CR;
+        h->adj_ready = true;
+    }
+    const int K = nsteps, ck = checkpoint_every, nseg = (K + ck - 1) / ck;
+    const int seglen = std::min(ck, K);
+    const size_t sb = slot_bytes(h);
+    char *pool = nullptr;
+    CUDA_OR_FAIL(cudaMalloc(&pool, sb * (size_t)(nseg + seglen + 1)));
+    std::vector<int> cur_ck((size_t)nseg), cur_seg((size_t)seglen);
+    char *slots_ck = pool, *slots_seg = pool + sb * (size_t)nseg, *slot_fin = pool + sb * (size_t)(nseg + seglen);
+    const double e[3] = {direction[0], direction[1], direction[2]};
+    cudaStream_t s = h->stream;
+    cudaEvent_t ev[3];
+    for (auto &x : ev) CUDA_OR_FAIL(cudaEventCreate(&x));
+    // zero the adjoint state and the gradients
+    cudaMemsetAsync(a.lu, 0, 3 * SC * sizeof(double2), s);
+    cudaMemsetAsync(a.lp, 0, SC * sizeof(double2), s);
+    cudaMemsetAsync(a.lnl, 0, 3 * SC * sizeof(double2), s);
+    cudaMemsetAsync(a.gxc, 0, 3 * (size_t)g.nbody * sizeof(double), s);
+    cudaMemsetAsync(a.as, 0, sizeof(AdjScal), s);
+    // forward: K steps, a checkpoint every ck steps, J accumulated on the device
+    CUDA_OR_FAIL(cudaEventRecord(ev[0], s));
+    for (int n = 0; n < K; ++n) {
+        if (n % ck == 0) { slot_save(h, slots_ck + sb * (size_t)(n / ck)); cur_ck[(size_t)(n / ck)] = h->cur; }
+        CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));
+        h->cur ^= 1;
+        enqueue_adjoint_jacc(h->b.sc, a.as, e, s);
+    }
+    slot_save(h, slot_fin);
+    const int cur_fin = h->cur;
+    CUDA_OR_FAIL(cudaEventRecord(ev[1], s));
+    // reverse sweep
+    AdjBufs w = a;
+    const double wJ = 1.0 / (double)K;
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        const int n0 = sg * ck, n1 = std::min(K, n0 + ck);
+        slot_restore(h, slots_ck + sb * (size_t)sg, cur_ck[(size_t)sg]);
+        for (int n = n0; n < n1; ++n) {
+            slot_save(h, slots_seg + sb * (size_t)(n - n0));
+            cur_seg[(size_t)(n - n0)] = h->cur;
+            if (n + 1 < n1) {
+                CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));
+                h->cur ^= 1;
+            }
+        }
+        for (int n = n1 - 1; n >= n0; --n) {
+            slot_restore(h, slots_seg + sb * (size_t)(n - n0), cur_seg[(size_t)(n - n0)]);
+            CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));   // step n's fields
+            h->cur ^= 1;
+            enqueue_adjoint_step(g, h->b, w, e, wJ, s);
+            std::swap(w.lu, w.lu2);
+            std::swap(w.lp, w.lp2);
+            std::swap(w.lnl, w.lonl);
+        }
+    }
+    CUDA_OR_FAIL(cudaEventRecord(ev[2], s));
+    CUDA_OR_FAIL(cudaGetLastError());
+    Scal sc_rev;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc_rev, h->b.sc, sizeof(Scal), cudaMemcpyDeviceToHost, s));
+    slot_restore(h, slot_fin, cur_fin);
+    AdjScal as;
+    std::vector<double> gx(3 * (size_t)g.nbody);
+    CUDA_OR_FAIL(cudaMemcpyAsync(&as, a.as, sizeof(AdjScal), cudaMemcpyDeviceToHost, s));
+    CUDA_OR_FAIL(cudaMemcpyAsync(gx.data(), a.gxc, gx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_OR_FAIL(cudaStreamSynchronize(s));
+    float fms = 0.f, rms = 0.f;
+    cudaEventElapsedTime(&fms, ev[0], ev[1]);
+    cudaEventElapsedTime(&rms, ev[1], ev[2]);
+    for (auto &x : ev) cudaEventDestroy(x);
+    cudaFree(pool);
+    // the adjoint buffers are swapped an even or odd number of times: keep
+    // the handle's pointers valid for the next call
+    a = w;
+    if (sc_rev.status) return fail(sc_rev.status, "adjoint: a recomputed step reported a solver stop condition");
+    for (size_t q = 0; q < gx.size(); ++q) g_xc[q] = gx[q];
+    for (int d = 0; d < 3; ++d) g_mpg[d] = as.gmpg[d];
+    if (rep) {
+        std::memset(rep, 0, sizeof(*rep));
+        rep->J = as.J / (double)K;
+        rep->forward_ms = fms;
+        rep->reverse_ms = rms;
+        rep->nsteps = K;
+        rep->checkpoint_every = ck;
+        rep->adjoint_kernels_per_step = adjoint_kernels_per_step(g);
     }
     return PIBM_OK;
 }

@@ -125,4 +125,25 @@ struct StepStreams {
     cudaEvent_t geo_done = nullptr;   // moving particles: the step's geometry is rebuilt
 };
 
+// Discrete adjoint of the AB2 step (fixed spheres, imposed mpg, fixed dt).
+// Scalars of the reverse sweep in device memory.
+struct AdjScal {
+    double lumean[3];    // lambda of umean
+    double lfrmean[3];   // lambda of frmean of the step being reversed
+    double gmpg[3];      // dJ/dmpg
+    double J;            // sum over the forward steps of e . (visc_total - pres_total)
+};
+// Adjoint work arrays.  Spectral arrays are [comp][i][kz][ky] like u; real
+// arrays [comp][i][transform-order plane] like ubcp.
+struct AdjBufs {
+    double2 *lu, *lp, *lnl;              // lambda of the state (u, p, nl) after the step being reversed
+    double2 *lu2, *lp2;                  // lambda of the state before it (being formed)
+    double2 *lnl_new, *lonl, *lff;       // lambda of the step's new nl, of its onl (-> lnl of the earlier state), of ff
+    double2 *T;                          // 10 components: adjoint plane transforms of the real lambdas
+    double *lfr, *lubcp, *lQ, *lpgr, *lpbcp, *lomega;   // real lambdas (3,3,3,3,1,3 components)
+    double *W8;                          // 8 real components: products and x-flux lambdas of the nonlinear term
+    double *gxc;                         // dJ/dxc (nbody,3) column-major
+    AdjScal *as;
+};
+
 }  // namespace pibm

@@ -28,6 +28,7 @@
 // points; by linearity of the transform and of the interpolation it is formed
 // once in spectral space (Q) instead of three separately interpolated fields.
 #include "step_common.cuh"
+#include "line_solve.cuh"
 #include "../../include/pibm.h"
 
 namespace pibm {
@@ -751,60 +752,6 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const doubl
 // Tiles live in shared memory as [line][i]; global loads and stores run over
 // consecutive lines (contiguous in the [i][k][j] layout).
 // ============================================================================
-template <int R>
-__device__ __forceinline__ void circulant_solve(double2 *row, double a, double b, const Tw &tw, int lane) {
-    constexpr int N = R * 32;
-    double2 v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = row[lane + 32 * r];
-    group_fft<R, 32>(v, lane, -1.0, tw);
-    const int br = bitrev<32>(lane);
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int m = r + R * br;
-        const double lam = ((double)N) * (b + 2.0 * a * tw.t[m * tw.stride].x);
-        v[r] = make_double2(v[r].x / lam, v[r].y / lam);
-    }
-    // exact inverse of group_fft's stages (unnormalised; 1/N folded into lam)
-#pragma unroll
-    for (int h = 1; h < 32; h <<= 1) {
-        const bool upper = (lane & h) == 0;
-        const int q = lane & (h - 1);
-        const double2 w = tw.stage(h, q, +1.0);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const double2 pv = shfl_xor2(v[r], h, 32);
-            v[r] = upper ? cadd(v[r], cmul(pv, w)) : csub(pv, cmul(v[r], w));
-        }
-    }
-#pragma unroll
-    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw.get((lane * r) % N, +1.0));
-    dft_inlane<R>(v, +1.0, tw);
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < R; ++r) row[lane + 32 * r] = v[r];
-    __syncwarp();
-}
-
-// Thomas recursion (tridag, tridiagonal.F90:47-87) on the real parts of
-// row[0..n-1]; constant a, b, c; result in row[].x, row[].y = 0, row[n] = 0.
-__device__ __forceinline__ bool thomas_real(double2 *row, double *gam, double a, double b, double c, int n) {
-    double bet = b;
-    if (bet == 0.0) return false;
-    double prev = row[0].x / bet;
-    row[0] = make_double2(prev, 0.0);
-    for (int j = 1; j < n; ++j) {
-        gam[j] = c / bet;
-        bet = b - a * gam[j];
-        if (bet == 0.0) return false;
-        prev = (row[j].x - a * prev) / bet;
-        row[j] = make_double2(prev, 0.0);
-    }
-    for (int j = n - 2; j >= 0; --j) row[j].x = row[j].x - gam[j + 1] * row[j + 1].x;
-    row[n] = make_double2(0.0, 0.0);
-    return true;
-}
-
 template <int NX, int LT>
 __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ u, double2 *__restrict__ p,
                                                    const double2 *__restrict__ nl, const double2 *__restrict__ onl,
