@@ -241,6 +241,90 @@ def moving_suspension(steps: int = 10, warmup: int = 3):
     return out
 
 
+def adjoint_gradient(nsteps: int = 200, checkpoint_every: int = 20, warm: int = 100, fd: bool = True):
+    """The gradient configuration: 96^3, 30 fixed spheres of diameter 16 cells
+    (phi = 0.073, seeded), Re 20, imposed mean pressure gradient (SET_MPG),
+    fixed dt, upwind x flux.  After `warm` steps from a uniform mean flow, J =
+    time average over `nsteps` steps of the summed drag along x and its
+    gradient w.r.t. all 90 sphere coordinates and the 3 mpg components
+    (pibm_adjoint_run, checkpoints every `checkpoint_every` steps).  Reported:
+    the forward time of the same steps on the step graphs, the adjoint run's
+    forward (with checkpoints) and reverse sweep, their ratios, and central
+    finite differences of the engine's forward run for four coordinates and
+    mpg_x against the adjoint gradient, with steps of 1e-6 and 1e-7
+    diameters (J is piecewise smooth in xc: a surface point crossing a grid
+    cell face is a kink of the trilinear interpolation, and an interval that
+    straddles one shows in the coarser difference)."""
+    import ctypes as C
+    import numpy as np
+    import pureibm_ps2d_fd1d_b200 as pk
+    from pureibm_ps2d_fd1d_b200 import config, abi
+    prm, xc = config.adjoint_case()
+    e = np.array([1.0, 0.0, 0.0])
+    s = pk.Solver(config.make_params(prm), xc)
+    st = s.get_state()
+    st["umean"] = np.array(prm["umean0"])
+    s.set_state(st)
+    s.run(warm)
+    st = s.get_state()
+    lib = pk.load_library()
+    rep = abi.pibm_step_report()
+    total = C.c_double()
+    rc = lib.pibm_run_timed(s.h, nsteps, C.byref(rep), C.byref(total))
+    if rc != 0:
+        raise RuntimeError("pibm_run_timed (adjoint case) failed: %d %s" % (rc, lib.pibm_last_error().decode()))
+    fwd_ms = total.value
+    s.set_state(st)
+    out = s.adjoint(nsteps, e, checkpoint_every)
+    s.close()
+    res = {"config": "96^3, 30 fixed spheres d=16 (phi 0.073), Re 20, SET_MPG, fixed dt, upwind; %d steps after %d, "
+                     "checkpoints every %d" % (nsteps, warm, checkpoint_every),
+           "objective": "J = mean over the steps of e . sum_m (pres_m + visc_m), e = x",
+           "J": out["J"], "forward_ms": fwd_ms, "adjoint_forward_ms": out["forward_ms"], "reverse_ms": out["reverse_ms"],
+           "reverse_over_forward": out["reverse_ms"] / fwd_ms,
+           "gradient_over_forward": (out["forward_ms"] + out["reverse_ms"]) / fwd_ms,
+           "forward_ms_per_step": fwd_ms / nsteps, "reverse_ms_per_step": out["reverse_ms"] / nsteps,
+           "adjoint_kernels_per_step": out["adjoint_kernels_per_step"],
+           "g_mpg": list(out["g_mpg"]), "g_xc_norm": float(np.linalg.norm(out["g_xc"]))}
+    if fd:
+        def J_of(xcv, mpg=None):
+            p = dict(prm)
+            st2 = dict(st)
+            if mpg is not None:
+                p["mpg"] = tuple(mpg)
+                st2["mpg"] = np.asarray(mpg, dtype=np.float64)
+            t = pk.Solver(config.make_params(p), xcv)
+            t.set_state(st2)
+            J = 0.0
+            for _ in range(nsteps):
+                r = t.step(1)
+                J += float(np.dot(e, np.asarray(r["visc_total"]) - np.asarray(r["pres_total"])))
+            t.close()
+            return J / nsteps
+        checks = []
+        for rel_h in (1e-6, 1e-7):
+            h = rel_h * 16.0
+            for m, d in ((0, 0), (7, 1), (19, 2), (3, 0)):
+                xp, xm = xc.copy(), xc.copy()
+                xp[m, d] += h
+                xm[m, d] -= h
+                f = (J_of(xp) - J_of(xm)) / (2 * h)
+                checks.append({"param": "xc[%d,%d]" % (m, d), "step_diameters": rel_h, "adjoint": float(out["g_xc"][m, d]),
+                               "fd": f, "rel_err": abs(out["g_xc"][m, d] - f) / max(abs(f), 1e-300)})
+            mp = np.array(prm["mpg"], dtype=np.float64)
+            dm = rel_h * abs(mp[0])
+            a, b = mp.copy(), mp.copy()
+            a[0] += dm
+            b[0] -= dm
+            f = (J_of(xc, a) - J_of(xc, b)) / (2 * dm)
+            checks.append({"param": "mpg[0]", "step_rel": rel_h, "adjoint": float(out["g_mpg"][0]), "fd": f,
+                           "rel_err": abs(out["g_mpg"][0] - f) / max(abs(f), 1e-300)})
+        res["fd_check"] = checks
+        res["fd_max_rel_err_step_1e-6"] = max(c["rel_err"] for c in checks if c.get("step_diameters", c.get("step_rel")) == 1e-6)
+        res["fd_max_rel_err_step_1e-7"] = max(c["rel_err"] for c in checks if c.get("step_diameters", c.get("step_rel")) == 1e-7)
+    return res
+
+
 def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024):
     """Batched multiple-independent-simulation throughput against the plain
     per-realization loop on the same GPU: 16 seeded realizations (grids from
@@ -408,6 +492,8 @@ def run_gpu(args):
         line["with_scalar"] = with_scalar()
     if not args.no_moving and world == 1:
         line["moving_suspension"] = moving_suspension()
+    if not args.no_adjoint and world == 1:
+        line["adjoint"] = adjoint_gradient()
     if not args.no_cpu_baseline and world == 1:
         cb = cpu_baseline(prm, xc, steps=2, warmup=1)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -427,6 +513,7 @@ def main():
     ap.add_argument("--no-mis", action="store_true", help="skip the batched-realization measurement")
     ap.add_argument("--no-scalar", action="store_true", help="skip the flow + passive-scalar measurement")
     ap.add_argument("--no-moving", action="store_true", help="skip the moving-particle suspension measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

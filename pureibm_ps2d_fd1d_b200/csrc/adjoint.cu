@@ -18,9 +18,9 @@
 // transpose; interpolation (trilinear gather) and spreading swap roles, and
 // the weights' derivatives give the sphere-position gradient.
 //
-// One reverse step (enqueue_adjoint_step), after the forward step n has been
-// recomputed from its checkpointed state so that ubcp, pbcp, omega, pgr, Q
-// and rec hold step n's fields:
+// One reverse step (enqueue_adjoint_step) reads step n's forward fields
+// (ubcp, pbcp, omega, pgr, Q, the point forces rec and the step's Scal),
+// stored while the segment holding step n was recomputed from its checkpoint:
 //   k_adj_begin   umean update^T (steptheflow.F90:99)
 //   k_adj_lines   velstep^T per (ky,kz) line: divcorr^T, ustep^T, pressure^T
 //   k_adj_c2r     ff = r2c(fr - frmean) ^T  -> lambda fr;  k_adj_sum -> lambda frmean
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_adj_c2r(Geo g, const 
 // over nplanes consecutive real planes (grid.x = nplanes * C).
 template <int N>
 __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_adj_r2c(Geo g, const double *__restrict__ src, double2 *__restrict__ dst,
-                                                        Scal *__restrict__ sc) {
+                                                        AdjScal *as) {
     using L = PL<N>;
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_adj_r2c(Geo g, const 
     if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
     __syncthreads();
-    uint32_t phase = 0;
+    const uint32_t phase = 0;
     const size_t pl = blockIdx.x / L::C;
     const int rank = blockIdx.x % L::C;
     const TwT tw{tws, N};
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_adj_r2c(Geo g, const 
         fence_async_smem();
         bulk_load(buf, src + pl * RSP + (size_t)rank * L::RL, L::RBYTES, &mb);
     }
-    load_wait(&mb, phase, sc);
+    if (!mbar_wait(&mb, phase)) atomicCAS(&as->status, 0, PIBM_ERR_TIMEOUT);
     __syncthreads();
     cl_r2c<N>(buf, tw, rank);
     for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
@@ -683,12 +683,12 @@ static void enqueue_adjoint_step_t(const Geo &g, const DevBufs &b, const AdjBufs
     if (g.npts > 0)
         k_adj_rev<N><<<(g.npts + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.rec, a.lfr, b.sc, a.as, a.lubcp, a.lQ, a.lpgr, a.gxc);
     k_adj_drag<N><<<(g.nbody * g.nbnd + 255) / 256, 256, 0, s>>>(g, b.pbcp, b.omega, a.lpbcp, a.lomega, a.gxc, e[0], e[1], e[2], wJ);
-    launch_planes<N>(k_adj_r2c<N>, 3 * g.nx, 1, s, g, (const double *)a.lQ, a.T, b.sc);
+    launch_planes<N>(k_adj_r2c<N>, 3 * g.nx, 1, s, g, (const double *)a.lQ, a.T, a.as);
     k_adj_q<<<(unsigned)((3 * SC + 255) / 256), 256, 0, s>>>(g, a.T, a.lnl_new, a.lonl, a.lu2);
     launch_planes<N>(k_adj_c2r<N>, g.nx, 8, s, g, (const double2 *)a.lnl_new, a.W8, 1);
     k_adj_flux<N><<<(unsigned)((CR + 255) / 256), 256, 0, s>>>(g, b.ubcp, a.W8, a.lubcp);
     k_adj_sum<N><<<dim3(nsum, 3), 256, 0, s>>>(g, a.lubcp, lumean, 1.0);
-    launch_planes<N>(k_adj_r2c<N>, 10 * g.nx, 1, s, g, (const double *)a.lubcp, a.T, b.sc);
+    launch_planes<N>(k_adj_r2c<N>, 10 * g.nx, 1, s, g, (const double *)a.lubcp, a.T, a.as);
     k_adj_assemble<<<(unsigned)((SC + 255) / 256), 256, 0, s>>>(g, a.T, a.lu2, a.lp2);
 }
 

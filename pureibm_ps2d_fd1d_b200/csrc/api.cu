@@ -622,13 +622,39 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     }
     const int K = nsteps, ck = checkpoint_every, nseg = (K + ck - 1) / ck;
     const int seglen = std::min(ck, K);
+    // state slots (checkpoints and the final state) and, for one segment, the
+    // forward fields every reverse step reads: ubcp(3) pbcp omega(3) pgr(3)
+    // Q(3) real components, the point forces rec and the step's Scal
     const size_t sb = slot_bytes(h);
+    const size_t CRb = CR * sizeof(double);
+    const size_t recb = ((6 * (size_t)g.npts * sizeof(double) + 255) / 256) * 256;
+    const size_t fb = 13 * CRb + recb + ((sizeof(Scal) + 255) / 256) * 256;
     char *pool = nullptr;
-    CUDA_OR_FAIL(cudaMalloc(&pool, sb * (size_t)(nseg + seglen + 1)));
-    std::vector<int> cur_ck((size_t)nseg), cur_seg((size_t)seglen);
-    char *slots_ck = pool, *slots_seg = pool + sb * (size_t)nseg, *slot_fin = pool + sb * (size_t)(nseg + seglen);
-    const double e[3] = {direction[0], direction[1], direction[2]};
+    CUDA_OR_FAIL(cudaMalloc(&pool, sb * (size_t)(nseg + 1) + fb * (size_t)seglen));
+    std::vector<int> cur_ck((size_t)nseg);
+    char *slots_ck = pool, *slot_fin = pool + sb * (size_t)nseg, *fslots = pool + sb * (size_t)(nseg + 1);
     cudaStream_t s = h->stream;
+    auto save_fields = [&](char *f) {
+        cudaMemcpyAsync(f, h->b.ubcp, 3 * CRb, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(f + 3 * CRb, h->b.pbcp, CRb, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(f + 4 * CRb, h->b.omega, 3 * CRb, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(f + 7 * CRb, h->b.pgr, 3 * CRb, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(f + 10 * CRb, h->b.Q, 3 * CRb, cudaMemcpyDeviceToDevice, s);
+        if (g.npts > 0) cudaMemcpyAsync(f + 13 * CRb, h->b.rec, 6 * (size_t)g.npts * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(f + 13 * CRb + recb, h->b.sc, sizeof(Scal), cudaMemcpyDeviceToDevice, s);
+    };
+    auto fields_view = [&](char *f) {
+        DevBufs v = h->b;
+        v.ubcp = (double *)f;
+        v.pbcp = (double *)(f + 3 * CRb);
+        v.omega = (double *)(f + 4 * CRb);
+        v.pgr = (double *)(f + 7 * CRb);
+        v.Q = (double *)(f + 10 * CRb);
+        v.rec = (double *)(f + 13 * CRb);
+        v.sc = (Scal *)(f + 13 * CRb + recb);
+        return v;
+    };
+    const double e[3] = {direction[0], direction[1], direction[2]};
     cudaEvent_t ev[3];
     for (auto &x : ev) CUDA_OR_FAIL(cudaEventCreate(&x));
     // zero the adjoint state and the gradients
@@ -648,25 +674,20 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     slot_save(h, slot_fin);
     const int cur_fin = h->cur;
     CUDA_OR_FAIL(cudaEventRecord(ev[1], s));
-    // reverse sweep
+    // reverse sweep: per segment, recompute its steps from the checkpoint
+    // keeping each step's fields, then run the adjoint steps backwards
     AdjBufs w = a;
     const double wJ = 1.0 / (double)K;
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int n0 = sg * ck, n1 = std::min(K, n0 + ck);
         slot_restore(h, slots_ck + sb * (size_t)sg, cur_ck[(size_t)sg]);
         for (int n = n0; n < n1; ++n) {
-            slot_save(h, slots_seg + sb * (size_t)(n - n0));
-            cur_seg[(size_t)(n - n0)] = h->cur;
-            if (n + 1 < n1) {
-                CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));
-                h->cur ^= 1;
-            }
+            CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));
+            h->cur ^= 1;
+            save_fields(fslots + fb * (size_t)(n - n0));
         }
         for (int n = n1 - 1; n >= n0; --n) {
-            slot_restore(h, slots_seg + sb * (size_t)(n - n0), cur_seg[(size_t)(n - n0)]);
-            CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));   // step n's fields
-            h->cur ^= 1;
-            enqueue_adjoint_step(g, h->b, w, e, wJ, s);
+            enqueue_adjoint_step(g, fields_view(fslots + fb * (size_t)(n - n0)), w, e, wJ, s);
             std::swap(w.lu, w.lu2);
             std::swap(w.lp, w.lp2);
             std::swap(w.lnl, w.lonl);
@@ -674,11 +695,11 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     }
     CUDA_OR_FAIL(cudaEventRecord(ev[2], s));
     CUDA_OR_FAIL(cudaGetLastError());
-    Scal sc_rev;
-    CUDA_OR_FAIL(cudaMemcpyAsync(&sc_rev, h->b.sc, sizeof(Scal), cudaMemcpyDeviceToHost, s));
     slot_restore(h, slot_fin, cur_fin);
+    Scal sc_fin;
     AdjScal as;
     std::vector<double> gx(3 * (size_t)g.nbody);
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc_fin, h->b.sc, sizeof(Scal), cudaMemcpyDeviceToHost, s));
     CUDA_OR_FAIL(cudaMemcpyAsync(&as, a.as, sizeof(AdjScal), cudaMemcpyDeviceToHost, s));
     CUDA_OR_FAIL(cudaMemcpyAsync(gx.data(), a.gxc, gx.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     CUDA_OR_FAIL(cudaStreamSynchronize(s));
@@ -687,10 +708,10 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     cudaEventElapsedTime(&rms, ev[1], ev[2]);
     for (auto &x : ev) cudaEventDestroy(x);
     cudaFree(pool);
-    // the adjoint buffers are swapped an even or odd number of times: keep
-    // the handle's pointers valid for the next call
+    // the work buffers were swapped K times: keep the handle's set consistent
     a = w;
-    if (sc_rev.status) return fail(sc_rev.status, "adjoint: a recomputed step reported a solver stop condition");
+    if (sc_fin.status) return fail(sc_fin.status, "adjoint: a forward step reported a solver stop condition");
+    if (as.status) return fail(as.status, "adjoint: a bounded wait in an adjoint kernel ran out");
     for (size_t q = 0; q < gx.size(); ++q) g_xc[q] = gx[q];
     for (int d = 0; d < 3; ++d) g_mpg[d] = as.gmpg[d];
     if (rep) {

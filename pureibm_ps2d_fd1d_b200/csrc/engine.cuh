@@ -132,6 +132,8 @@ struct AdjScal {
     double lfrmean[3];   // lambda of frmean of the step being reversed
     double gmpg[3];      // dJ/dmpg
     double J;            // sum over the forward steps of e . (visc_total - pres_total)
+    int status;          // PIBM_ERR_TIMEOUT if a bounded wait of an adjoint kernel ran out
+    int pad;
 };
 // Adjoint work arrays.  Spectral arrays are [comp][i][kz][ky] like u; real
 // arrays [comp][i][transform-order plane] like ubcp.

@@ -115,3 +115,22 @@ def test_adjoint_rejects_unsupported_runs():
     s = pk.Solver(config.make_params(prm), xc)
     with pytest.raises(pk.PibmError):
         s.adjoint(2, E)
+
+
+def test_torch_autograd_function_returns_the_adjoint_gradients():
+    import torch
+    from pureibm_ps2d_fd1d_b200.adjoint import drag_objective
+    prm, xc = _case("upwind")
+    st = _start_state(prm, xc, warm=4)
+    K = 5
+    ref = _gpu(prm, xc, st).adjoint(K, E, checkpoint_every=2)
+    x = torch.tensor(xc, dtype=torch.float64, requires_grad=True)
+    g = torch.tensor(prm["mpg"], dtype=torch.float64, requires_grad=True)
+    J = drag_objective(x, g, prm, st, K, E, checkpoint_every=2)
+    (2.0 * J).backward()
+    assert abs(J.item() - ref["J"]) <= 1e-12 * abs(ref["J"])
+    assert np.max(np.abs(x.grad.numpy() - 2.0 * ref["g_xc"])) <= 1e-12 * np.max(np.abs(ref["g_xc"]))
+    assert np.max(np.abs(g.grad.numpy() - 2.0 * ref["g_mpg"])) <= 1e-12 * np.max(np.abs(ref["g_mpg"]))
+    with torch.no_grad():
+        J0 = drag_objective(x, g, prm, st, K, E)
+    assert abs(J0.item() - ref["J"]) <= 1e-12 * abs(ref["J"])
