@@ -554,87 +554,123 @@ __device__ __forceinline__ double slope_d(double um1, double u0, double up1, dou
 
 // ============================================================================
 // k_adj_flux: products and x flux of the nonlinear term, transposed, into
-// lambda ubcp (one thread per node; nl_allflow.F90:97-310 transposed).
-// W8 items 0..4 = lambda of the products u0u1, u0u2, u1u1, u1u2, u2u2; items
-// 5..7 = lambda of the x-flux differences D_c.  Upwind: D_c(i) = (F(i) -
-// F(i-1))/dx with F(m) the Rusanov flux at the face between cells m and m+1,
+// lambda ubcp (nl_allflow.F90:97-310 transposed).  W8 items 0..4 = lambda of
+// the products u0u1, u0u2, u1u1, u1u2, u2u2; items 5..7 = lambda of the
+// x-flux differences D_c.  Upwind: D_c(i) = (F(i) - F(i-1))/dx with F(m) the
+// Rusanov flux at the face between cells m and m+1,
 // F = (a A + b B - max(|a|,|b|) (B - A)) / 2, a, b the MUSCL states of u0 and
-// A, B those of u_c; cell i reaches the faces i-2 .. i+1.
+// A, B those of u_c; face m reads cells m-1 .. m+2.  One thread owns one
+// (y,z) node and a segment of SEG cells and streams along x like k_flux:
+// each face's partials are formed once and added to a rolling window of the
+// four cells it reads; a cell is complete once the face after it is done.
 // ============================================================================
+constexpr int kAdjFluxSeg = 16;   // x cells per thread (divides every supported nx)
 template <int N>
 __global__ void __launch_bounds__(256) k_adj_flux(Geo g, const double *__restrict__ ubcp, const double *__restrict__ W8,
                                                   double *lubcp) {
-    constexpr int RSP = RP<N>::RSP;
-    const int nx = g.nx;
-    const size_t CR = (size_t)nx * RSP;
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= CR) return;
-    const int e = (int)(t % RSP), i = (int)(t / RSP);
+    constexpr int RSP = RP<N>::RSP, SEG = kAdjFluxSeg;
+    const int nx = g.nx, nseg = nx / SEG;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= RSP * nseg) return;
+    const int e = t % RSP, i0 = (t / RSP) * SEG;
     if (e % (N + 2) >= N) return;
+    const size_t CR = (size_t)nx * RSP;
     auto X = [&](int ii) { return ii < 0 ? ii + nx : (ii >= nx ? ii - nx : ii); };
-    auto U = [&](int c, int ii) { return ubcp[c * CR + (size_t)X(ii) * RSP + e]; };
-    auto LD = [&](int c, int ii) { return W8[(5 + c) * CR + (size_t)X(ii) * RSP + e]; };
-    const double u[3] = {U(0, i), U(1, i), U(2, i)};
-    const double P01 = W8[0 * CR + t], P02 = W8[1 * CR + t], P11 = W8[2 * CR + t], P12 = W8[3 * CR + t], P22 = W8[4 * CR + t];
-    double lu[3];
-    lu[0] = u[1] * P01 + u[2] * P02;
-    lu[1] = (u[0] * P01 + 2.0 * u[1] * P11) + u[2] * P12;
-    lu[2] = (u[0] * P02 + u[1] * P12) + 2.0 * u[2] * P22;
+    auto U = [&](int c, int ii) { return __ldg(ubcp + c * CR + (size_t)X(ii) * RSP + e); };
+    auto LD = [&](int c, int ii) { return __ldg(W8 + (5 + c) * CR + (size_t)X(ii) * RSP + e); };
     const double dx = g.dx, h = dx / 2.0;
-    if (g.scheme == PIBM_SCHEME_CENTER) {
-        // D_c(i) = (u0 u_c (i+1) - u0 u_c (i-1)) / (2 dx)
-        for (int c = 0; c < 3; ++c) {
-            const double lf = (LD(c, i - 1) - LD(c, i + 1)) / (2.0 * dx);
-            lu[0] += u[c] * lf;
-            lu[c] += u[0] * lf;
+    // pointwise part: the products, and the whole center-scheme flux
+    auto pointwise = [&](int i, double lu[3]) {
+        const size_t o = (size_t)i * RSP + e;
+        const double u0 = U(0, i), u1 = U(1, i), u2 = U(2, i);
+        const double P01 = W8[0 * CR + o], P02 = W8[1 * CR + o], P11 = W8[2 * CR + o], P12 = W8[3 * CR + o], P22 = W8[4 * CR + o];
+        lu[0] = u1 * P01 + u2 * P02;
+        lu[1] = (u0 * P01 + 2.0 * u1 * P11) + u2 * P12;
+        lu[2] = (u0 * P02 + u1 * P12) + 2.0 * u2 * P22;
+        if (g.scheme == PIBM_SCHEME_CENTER) {
+            const double uc[3] = {u0, u1, u2};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double lf = (LD(c, i - 1) - LD(c, i + 1)) / (2.0 * dx);
+                lu[0] += uc[c] * lf;
+                lu[c] += u0 * lf;
+            }
         }
-    } else {
-        double a0[7];
+    };
+    if (g.scheme == PIBM_SCHEME_CENTER) {
+        for (int i = i0; i < i0 + SEG; ++i) {
+            double lu[3];
+            pointwise(i, lu);
 #pragma unroll
-        for (int k = 0; k < 7; ++k) a0[k] = U(0, i - 3 + k);
-        double s0[5], ds0[5][3];
+            for (int c = 0; c < 3; ++c) lubcp[c * CR + (size_t)i * RSP + e] += lu[c];
+        }
+        return;
+    }
+    const int lim = g.limiter;
+    // window at face m: w[c][k] = u_c(m-1+k); sl/ds: slopes at cells m, m+1;
+    // ld: lambda D at m, m+1; acc[c][k]: lambda u_c(m-1+k)
+    double w[3][4], sl[3][2], ds[3][2][3], ld[3][2], acc[3][4];
+    int m = i0 - 2;
 #pragma unroll
-        for (int k = 0; k < 5; ++k) s0[k] = slope_d(a0[k], a0[k + 1], a0[k + 2], dx, g.limiter, ds0[k]);   // cell i-2+k
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { w[c][k] = U(c, m - 1 + k); acc[c][k] = 0.0; }
+        sl[c][0] = slope_d(w[c][0], w[c][1], w[c][2], dx, lim, ds[c][0]);
+        sl[c][1] = slope_d(w[c][1], w[c][2], w[c][3], dx, lim, ds[c][1]);
+        ld[c][0] = LD(c, m);
+        ld[c][1] = LD(c, m + 1);
+    }
+    for (; m <= i0 + SEG; ++m) {
+        const double a = w[0][1] + sl[0][0] * h, b = w[0][2] - sl[0][1] * h;
+        const double M = fmax(fabs(a), fabs(b));
+        const bool amax = !(fabs(a) < fabs(b));
+        const double sa = a > 0.0 ? 1.0 : (a < 0.0 ? -1.0 : 0.0), sb = b > 0.0 ? 1.0 : (b < 0.0 ? -1.0 : 0.0);
+        double la = 0.0, lb = 0.0;
+#pragma unroll
         for (int c = 0; c < 3; ++c) {
-            double an[7], sn[5], dsn[5][3], ld[5];
+            const double lF = (ld[c][0] - ld[c][1]) / dx;
+            const double A = w[c][1] + sl[c][0] * h, B = w[c][2] - sl[c][1] * h;
+            const double pa = (0.5 * A - 0.5 * (B - A) * (amax ? sa : 0.0)) * lF;
+            const double pb = (0.5 * B - 0.5 * (B - A) * (amax ? 0.0 : sb)) * lF;
+            const double pA = (0.5 * a + 0.5 * M) * lF, pB = (0.5 * b - 0.5 * M) * lF;
+            la += pa;
+            lb += pb;
+            // A = u_c(m) + h s_c(m), B = u_c(m+1) - h s_c(m+1)
+            acc[c][1] += pA;
+            acc[c][2] += pB;
 #pragma unroll
-            for (int k = 0; k < 7; ++k) an[k] = c == 0 ? a0[k] : U(c, i - 3 + k);
-#pragma unroll
-            for (int k = 0; k < 5; ++k) {
-                if (c == 0) { sn[k] = s0[k]; dsn[k][0] = ds0[k][0]; dsn[k][1] = ds0[k][1]; dsn[k][2] = ds0[k][2]; }
-                else sn[k] = slope_d(an[k], an[k + 1], an[k + 2], dx, g.limiter, dsn[k]);
-                ld[k] = LD(c, i - 2 + k);
+            for (int q = 0; q < 3; ++q) {
+                acc[c][q] += h * pA * ds[c][0][q];
+                acc[c][q + 1] -= h * pB * ds[c][1][q];
             }
-            double l0 = 0.0, ln = 0.0;
+        }
+        acc[0][1] += la;
+        acc[0][2] += lb;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {                 // face between cells i-2+j and i-1+j
-                const double lF = (ld[j] - ld[j + 1]) / dx;
-                const int kl = j, kr = j + 1;             // slope index of the two cells
-                const double a = a0[kl + 1] + s0[kl] * h, b = a0[kr + 1] - s0[kr] * h;
-                const double A = an[kl + 1] + sn[kl] * h, B = an[kr + 1] - sn[kr] * h;
-                const double M = fmax(fabs(a), fabs(b));
-                const bool amax = !(fabs(a) < fabs(b));
-                const double sa = a > 0.0 ? 1.0 : (a < 0.0 ? -1.0 : 0.0), sb = b > 0.0 ? 1.0 : (b < 0.0 ? -1.0 : 0.0);
-                double pa = (0.5 * A - 0.5 * (B - A) * (amax ? sa : 0.0)) * lF;
-                double pb = (0.5 * B - 0.5 * (B - A) * (amax ? 0.0 : sb)) * lF;
-                double pA = (0.5 * a + 0.5 * M) * lF, pB = (0.5 * b - 0.5 * M) * lF;
-                if (c == 0) { pa += pA; pb += pB; pA = 0.0; pB = 0.0; }
-                // d a / d u(i), d b / d u(i): cell i is slope index 2
-                const double da0 = (kl == 2 ? 1.0 : 0.0) + ((kl >= 1 && kl <= 3) ? h * ds0[kl][3 - kl] : 0.0);
-                const double db0 = (kr == 2 ? 1.0 : 0.0) - ((kr >= 1 && kr <= 3) ? h * ds0[kr][3 - kr] : 0.0);
-                l0 += pa * da0 + pb * db0;
-                if (c != 0) {
-                    const double dA = (kl == 2 ? 1.0 : 0.0) + ((kl >= 1 && kl <= 3) ? h * dsn[kl][3 - kl] : 0.0);
-                    const double dB = (kr == 2 ? 1.0 : 0.0) - ((kr >= 1 && kr <= 3) ? h * dsn[kr][3 - kr] : 0.0);
-                    ln += pA * dA + pB * dB;
-                }
-            }
-            lu[0] += l0;
-            if (c != 0) lu[c] += ln;
+        for (int q = 0; q < 3; ++q) {
+            acc[0][q] += h * la * ds[0][0][q];
+            acc[0][q + 1] -= h * lb * ds[0][1][q];
+        }
+        // cell m-1 is complete
+        const int ic = m - 1;
+        if (ic >= i0 && ic < i0 + SEG) {
+            double lu[3];
+            pointwise(ic, lu);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) lubcp[c * CR + (size_t)ic * RSP + e] += lu[c] + acc[c][0];
+        }
+        if (m == i0 + SEG) break;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            acc[c][0] = acc[c][1]; acc[c][1] = acc[c][2]; acc[c][2] = acc[c][3]; acc[c][3] = 0.0;
+            w[c][0] = w[c][1]; w[c][1] = w[c][2]; w[c][2] = w[c][3]; w[c][3] = U(c, m + 3);
+            sl[c][0] = sl[c][1];
+            ds[c][0][0] = ds[c][1][0]; ds[c][0][1] = ds[c][1][1]; ds[c][0][2] = ds[c][1][2];
+            sl[c][1] = slope_d(w[c][1], w[c][2], w[c][3], dx, lim, ds[c][1]);
+            ld[c][0] = ld[c][1];
+            ld[c][1] = LD(c, m + 2);
         }
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) lubcp[c * CR + t] += lu[c];
 }
 
 // k_adj_assemble: lambda u_{n-1}, p_{n-1} from T = c2r^T of lambda ubcp (0..2),
@@ -686,7 +722,7 @@ static void enqueue_adjoint_step_t(const Geo &g, const DevBufs &b, const AdjBufs
     launch_planes<N>(k_adj_r2c<N>, 3 * g.nx, 1, s, g, (const double *)a.lQ, a.T, a.as);
     k_adj_q<<<(unsigned)((3 * SC + 255) / 256), 256, 0, s>>>(g, a.T, a.lnl_new, a.lonl, a.lu2);
     launch_planes<N>(k_adj_c2r<N>, g.nx, 8, s, g, (const double2 *)a.lnl_new, a.W8, 1);
-    k_adj_flux<N><<<(unsigned)((CR + 255) / 256), 256, 0, s>>>(g, b.ubcp, a.W8, a.lubcp);
+    k_adj_flux<N><<<(unsigned)((RP<N>::RSP * (g.nx / kAdjFluxSeg) + 255) / 256), 256, 0, s>>>(g, b.ubcp, a.W8, a.lubcp);
     k_adj_sum<N><<<dim3(nsum, 3), 256, 0, s>>>(g, a.lubcp, lumean, 1.0);
     launch_planes<N>(k_adj_r2c<N>, 10 * g.nx, 1, s, g, (const double *)a.lubcp, a.T, a.as);
     k_adj_assemble<<<(unsigned)((SC + 255) / 256), 256, 0, s>>>(g, a.T, a.lu2, a.lp2);
