@@ -464,6 +464,23 @@ def run_gpu(args):
         pass
     b_alg_step = 30 * Fc
     info = s.info
+    # FP64 arithmetic: the reference's transform count (31 plane FFTs per
+    # x-plane, 2.5 n log2 n flops each for a real n-point plane) and the
+    # count this engine executes (25 plane transforms per x-plane; five
+    # circulant line solves per (ky,kz) line, each a forward and an inverse
+    # complex x-FFT of 5 nx log2 nx flops), against the measured DFMA peak
+    import math
+    nplane = s.my * mz
+    f_plane = 2.5 * nplane * math.log2(nplane)
+    f_ref = 31 * nx * f_plane
+    f_exec = 25 * nx * f_plane + (my2 * mz) * 5 * 2 * 5 * nx * math.log2(nx)
+    fp_peak, fp_ms = C.c_double(), C.c_double()
+    fp64 = None
+    if lib.pibm_fp64_peak(C.byref(fp_peak), C.byref(fp_ms)) == 0:
+        ach = f_exec / (t_ms / args.steps / 1e3) / 1e12
+        fp64 = {"peak_tflops": fp_peak.value, "peak_kind": "measured (DFMA chains, pibm_fp64_peak)",
+                "flops_per_step_reference_count": f_ref, "flops_per_step_executed": f_exec,
+                "achieved_tflops": ach, "frac": ach / fp_peak.value}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": t_ms / args.steps, "higher_is_better": True,
@@ -482,6 +499,7 @@ def run_gpu(args):
                 "path": "pibm_set_state(pinned host) + pibm_step + pibm_get_state(pinned host) per step"},
         "gpu_launches": int(info.kernels_per_step) * args.steps,
         "clocks": clk.summary(),
+        "fp64": fp64,
         "active_reversal_points": int(info.npts_active),
         "maxvolfrac": info.maxvolfrac,
         "last_step": {"divmax": rep.divmax, "norm_drag": rep.norm_drag, "dt": rep.dt},

@@ -50,8 +50,8 @@ extern "C" {
  * Parsed floparam.in values that define one run (namelists FLOANDGRID,
  * PART_PROPT, FLAGS; defaults in SRC/FLO/initialize.F90:73-271).
  * Grid: mx = my+1, nx = mx-1 = my, my2 = my/2+1 (initialize.F90:340-352);
- * mz = my unless given.  Only the serial x-periodic AB2 path is supported
- * (PARALLEL=0, XPERIODIC=T, RK3=F, NLCONS=T, AliasFlag=0).
+ * mz = my unless given.  Only the serial x-periodic path is supported
+ * (PARALLEL=0, XPERIODIC=T, NLCONS=T, AliasFlag=0), AB2 or RK3.
  */
 typedef struct pibm_params {
     int32_t my;              /* MY (even)                                      */
@@ -256,6 +256,12 @@ typedef struct pibm_adjoint_report {
 } pibm_adjoint_report;
 int  pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const double direction[3],
                       double *g_xc, double g_mpg[3], pibm_adjoint_report *rep);
+
+/* ---- measurement (no counterpart in the reference) ----
+ * FP64 arithmetic peak of the current device: chains of fused multiply-adds
+ * on 8 CTAs of 256 threads per SM, best of 5 event-timed runs (about 0.5 s).
+ * tflops = 2 * fma count / time; ms (optional) = the best run's time. */
+int  pibm_fp64_peak(double *tflops, double *ms);
 
 /* ---- batched independent realizations (the MIS ensemble of
  *      sample_inputs/set_mis_3d, run as one graph-captured launch stream) ---- */

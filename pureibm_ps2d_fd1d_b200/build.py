@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libpibm.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels.cu", "scalar.cu", "moving.cu", "adjoint.cu", "api.cu"]
+CU_SOURCES = ["kernels.cu", "scalar.cu", "moving.cu", "adjoint.cu", "peak.cu", "api.cu"]
 # per-source nvcc flags: the DEM and the moving-geometry rebuild are compiled
 # without multiply-add contraction (bit-equal to a serial evaluation)
 CU_FLAGS = {"moving.cu": ["--fmad=false"]}
