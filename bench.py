@@ -440,6 +440,14 @@ def run_gpu(args):
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
     bytes_state = (hu.numel() + hnl.numel() + hp.numel()) * 8
+    # the drop-in loop of a host driver that keeps the state on the device:
+    # one synchronous pibm_step per step, its report read back to the host
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        assert lib.pibm_step(s.h, 1, C.byref(rep)) == 0
+    barrier()
+    res_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
 
     if rank != 0:
         if dist:
@@ -497,6 +505,9 @@ def run_gpu(args):
         "e2e": {"value": ncell * e2e_steps * world / e2e_s / 1e6, "unit": UNIT,
                 "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state + C.sizeof(rep),
                 "path": "pibm_set_state(pinned host) + pibm_step + pibm_get_state(pinned host) per step"},
+        "e2e_resident_state": {"value": ncell * e2e_steps * world / res_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": 0,
+                               "d2h_bytes_per_step": C.sizeof(rep),
+                               "path": "one synchronous pibm_step per step with its report read back; the state stays on the device"},
         "gpu_launches": int(info.kernels_per_step) * args.steps,
         "clocks": clk.summary(),
         "fp64": fp64,
