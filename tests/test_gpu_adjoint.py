@@ -18,9 +18,9 @@ pytestmark = pytest.mark.gpu
 E = np.array([1.0, 0.3, -0.2])
 
 
-def _case(scheme="upwind", my=32, nbody=3):
+def _case(scheme="upwind", my=32, nbody=3, limiter="none"):
     prm, xc = config.adjoint_case(my=my, dia_cells=8.0, nbody=nbody, seed=11, mc_moves=20)
-    prm.update(discr_scheme=scheme)
+    prm.update(discr_scheme=scheme, limiter=limiter)
     return prm, xc
 
 
@@ -58,9 +58,9 @@ def _gpu_J(prm, xc, st, K, mpg=None):
     return J / K
 
 
-@pytest.mark.parametrize("scheme", ["upwind", "center"])
-def test_adjoint_matches_oracle_adjoint(scheme):
-    prm, xc = _case(scheme)
+@pytest.mark.parametrize("scheme,limiter", [("upwind", "none"), ("center", "none"), ("upwind", "minmod")])
+def test_adjoint_matches_oracle_adjoint(scheme, limiter):
+    prm, xc = _case(scheme, limiter=limiter)
     st = _start_state(prm, xc, warm=10)
     K = 6
     parts = config.Particles(xc)
