@@ -594,6 +594,39 @@ __global__ void __launch_bounds__(256) k_sp_count(Geo g, Mov m, Scal *sc) {
             }
 }
 
+// A node's bucket in ascending entry order, the reference's accumulation
+// order ((point, corner) or (evaluation, corner)): buckets of up to 8 entries
+// (nearly all) through a 19-comparator sorting network in registers, longer
+// ones by insertion sort.  f(entry) is called in that order.
+template <class F>
+__device__ __forceinline__ void bucket_in_order(const int *bucket, int c, F f) {
+    if (c <= 8) {
+        int v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = q < c ? bucket[q] : 0x7fffffff;
+        auto ce = [&](int a, int b) { const int x = min(v[a], v[b]), y = max(v[a], v[b]); v[a] = x; v[b] = y; };
+        ce(0, 1); ce(2, 3); ce(4, 5); ce(6, 7);
+        ce(0, 2); ce(1, 3); ce(4, 6); ce(5, 7);
+        ce(1, 2); ce(5, 6);
+        ce(0, 4); ce(1, 5); ce(2, 6); ce(3, 7);
+        ce(2, 4); ce(3, 5);
+        ce(1, 2); ce(3, 4); ce(5, 6);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (q < c) f(v[q]);
+    } else {
+        int e[64];
+        const int cc = min(c, 64);
+        for (int q = 0; q < cc; ++q) {
+            const int x = bucket[q];
+            int b = q - 1;
+            while (b >= 0 && e[b] > x) { e[b + 1] = e[b]; --b; }
+            e[b + 1] = x;
+        }
+        for (int q = 0; q < cc; ++q) f(e[q]);
+    }
+}
+
 // fr at every node: the bucket's contributions in ascending (point, corner)
 // order, the reference's accumulation order; nodes without force get zero.
 __global__ void __launch_bounds__(256) k_spread_dyn(Geo g, Mov m, const double *__restrict__ rec,
@@ -603,27 +636,18 @@ __global__ void __launch_bounds__(256) k_spread_dyn(Geo g, Mov m, const double *
     if (node >= CR || sc->status) return;
     double acc[3] = {0.0, 0.0, 0.0};
     const int c = min(m.spcnt[node], m.kmax);
-    if (c > 0) {
-        int e[64];
-        const int cc = min(c, 64);
-        for (int q = 0; q < cc; ++q) {   // the bucket in ascending (point, corner) order
-            const int v = m.spbuf[node * m.kmax + q];
-            int b = q - 1;
-            while (b >= 0 && e[b] > v) { e[b + 1] = e[b]; --b; }
-            e[b + 1] = v;
-        }
-        for (int q = 0; q < cc; ++q) {
-            const double *t = ctb + (size_t)e[q] * 3;
+    if (c > 0)
+        bucket_in_order(m.spbuf + node * m.kmax, c, [&](int ent) {
+            const double *t = ctb + (size_t)ent * 3;
             if (g.include_frmeanfluid) {
 #pragma unroll
                 for (int n = 0; n < 3; ++n) acc[n] = acc[n] + t[n];
             } else {
-                const double *r = rec + (size_t)(e[q] >> 3) * 6 + 3;
+                const double *r = rec + (size_t)(ent >> 3) * 6 + 3;
 #pragma unroll
                 for (int n = 0; n < 3; ++n) acc[n] = (acc[n] + t[n]) + r[n];
             }
-        }
-    }
+        });
 #pragma unroll
     for (int n = 0; n < 3; ++n) fr[n * CR + node] = acc[n];
 }
@@ -759,20 +783,11 @@ __global__ void __launch_bounds__(256) k_sspread_dyn(Geo g, Mov m, const double 
     if (node >= (size_t)g.nx * g.RS || sc->status) return;
     double v = 0.0;
     const int c = min(m.sspcnt[node], m.kmax);
-    if (c > 0) {
-        int e[64];
-        const int cc = min(c, 64);
-        for (int q = 0; q < cc; ++q) {   // the bucket in ascending (evaluation, corner) order
-            const int x = m.sspbuf[node * m.kmax + q];
-            int b = q - 1;
-            while (b >= 0 && e[b] > x) { e[b + 1] = e[b]; --b; }
-            e[b + 1] = x;
-        }
-        for (int q = 0; q < cc; ++q) {
-            v = v + sctb[e[q]];
-            if (!g.include_frmeanfluid) v = v + sfd[e[q] >> 3];
-        }
-    }
+    if (c > 0)
+        bucket_in_order(m.sspbuf + node * m.kmax, c, [&](int ent) {
+            v = v + sctb[ent];
+            if (!g.include_frmeanfluid) v = v + sfd[ent >> 3];
+        });
     sfr[node] = v;
 }
 
