@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(LT * 32) k_adj_lines(Geo g, const double2 *__r
                                                        const double2 *__restrict__ lnl, double2 *__restrict__ lu2,
                                                        double2 *__restrict__ lp2, double2 *__restrict__ lnl_new,
                                                        double2 *__restrict__ lonl, double2 *__restrict__ lff,
-                                                       const Scal *__restrict__ sc) {
+                                                       const Scal *__restrict__ sc, AdjScal *as) {
     constexpr int R = NX / 32;
     constexpr int NP = NX + 1;
     extern __shared__ double2 sm[];
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(LT * 32) k_adj_lines(Geo g, const double2 *__r
         }
         lp2[(size_t)i * PS + q] = make_double2(0.0, 0.0);
     }
-    (void)ok;
+    if (!ok) atomicCAS(&as->status, 0, PIBM_ERR_PIVOT);
 }
 
 template <int NX>
@@ -711,7 +711,7 @@ static void enqueue_adjoint_step_t(const Geo &g, const DevBufs &b, const AdjBufs
     const int nsum = 2 * 148;
     k_adj_begin<<<1, 32, 0, s>>>(b.sc, a.as);
     k_adj_lines<N, LT><<<(g.PS + LT - 1) / LT, LT * 32, adj_lines_smem<N>(), s>>>(g, a.lu, a.lp, a.lnl, a.lu2, a.lp2, a.lnl_new,
-                                                                                 a.lonl, a.lff, b.sc);
+                                                                                 a.lonl, a.lff, b.sc, a.as);
     launch_planes<N>(k_adj_c2r<N>, g.nx, 3, s, g, (const double2 *)a.lff, a.lfr, 0);
     k_adj_sum<N><<<dim3(nsum, 3), 256, 0, s>>>(g, a.lfr, lfrmean, -1.0);
     cudaMemsetAsync(a.lubcp, 0, 10 * CR * sizeof(double), s);   // lubcp, lomega, lpbcp, lpgr

@@ -711,7 +711,7 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     // the work buffers were swapped K times: keep the handle's set consistent
     a = w;
     if (sc_fin.status) return fail(sc_fin.status, "adjoint: a forward step reported a solver stop condition");
-    if (as.status) return fail(as.status, "adjoint: a bounded wait in an adjoint kernel ran out");
+    if (as.status) return fail(as.status, "adjoint: an adjoint kernel reported a bounded-wait timeout or a zero pivot");
     for (size_t q = 0; q < gx.size(); ++q) g_xc[q] = gx[q];
     for (int d = 0; d < 3; ++d) g_mpg[d] = as.gmpg[d];
     if (rep) {

@@ -132,7 +132,7 @@ struct AdjScal {
     double lfrmean[3];   // lambda of frmean of the step being reversed
     double gmpg[3];      // dJ/dmpg
     double J;            // sum over the forward steps of e . (visc_total - pres_total)
-    int status;          // PIBM_ERR_TIMEOUT if a bounded wait of an adjoint kernel ran out
+    int status;          // PIBM_ERR_TIMEOUT / PIBM_ERR_PIVOT from an adjoint kernel
     int pad;
 };
 // Adjoint work arrays.  Spectral arrays are [comp][i][kz][ky] like u; real
