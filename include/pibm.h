@@ -256,6 +256,17 @@ typedef struct pibm_adjoint_report {
 } pibm_adjoint_report;
 int  pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const double direction[3],
                       double *g_xc, double g_mpg[3], pibm_adjoint_report *rep);
+/* The same reverse sweep driven step by step by the host (which keeps its
+ * own checkpoints): pibm_adjoint_begin zeroes the adjoint state for an
+ * objective over nsteps steps; each pibm_adjoint_step reverses one step n =
+ * nsteps, nsteps-1, ..., 1 in that order and expects the handle to hold the
+ * state before step n (pibm_set_state of the host's copy, or the state its
+ * recomputation left): it runs step n to form the step's fields, then the
+ * adjoint of step n, and leaves the handle after step n; pibm_adjoint_end
+ * returns dJ/dxc and dJ/dmpg.  Same run restrictions as pibm_adjoint_run. */
+int  pibm_adjoint_begin(pibm_handle *h, int nsteps, const double direction[3]);
+int  pibm_adjoint_step(pibm_handle *h);
+int  pibm_adjoint_end(pibm_handle *h, double *g_xc, double g_mpg[3]);
 
 /* ---- measurement (no counterpart in the reference) ----
  * FP64 arithmetic peak of the current device: chains of fused multiply-adds

@@ -198,6 +198,22 @@ class Solver:
         return dict(J=rep.J, g_xc=g.reshape(3, self.nbody).T.copy(), g_mpg=gm, forward_ms=rep.forward_ms,
                     reverse_ms=rep.reverse_ms, adjoint_kernels_per_step=rep.adjoint_kernels_per_step)
 
+    # host-driven reverse sweep (pibm_adjoint_begin / _step / _end)
+    def adjoint_begin(self, nsteps: int, direction=(1.0, 0.0, 0.0)):
+        e = np.ascontiguousarray(direction, dtype=np.float64)
+        _check(load_library().pibm_adjoint_begin(self.h, int(nsteps), e.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def adjoint_step(self):
+        """Reverse step n (n = K, K-1, ..., 1); the solver must hold the state before step n."""
+        _check(load_library().pibm_adjoint_step(self.h))
+
+    def adjoint_end(self) -> dict:
+        g = np.zeros(3 * self.nbody)
+        gm = np.zeros(3)
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        _check(load_library().pibm_adjoint_end(self.h, dp(g), dp(gm)))
+        return dict(g_xc=g.reshape(3, self.nbody).T.copy(), g_mpg=gm)
+
     def set_desired_means(self, usmean_des, ufmean_des):
         """usmean_des / ufmean_des of a restarted run."""
         a = np.ascontiguousarray(usmean_des, dtype=np.float64)

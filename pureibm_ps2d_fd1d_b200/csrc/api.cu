@@ -83,8 +83,10 @@ struct pibm_handle {
     int device = 0;
     double2 *stage = nullptr;   // reference-layout staging buffer of get/set_state (allocated once)
     StepStreams ss;             // side streams of the forked step (graphs and pibm_step)
-    AdjBufs adj{};              // adjoint work arrays (allocated by the first pibm_adjoint_run)
+    AdjBufs adj{};              // adjoint work arrays (allocated by the first adjoint call)
     bool adj_ready = false;
+    int adj_left = 0;           // host-driven sweep: reverse steps still expected
+    double adj_e[3] = {0, 0, 0}, adj_wJ = 0.0;
 
     template <class T> cudaError_t alloc(T **p, size_t n) {
         void *q = nullptr;
@@ -594,15 +596,16 @@ void slot_restore(pibm_handle *h, const char *slot, int cur) {
 }
 }  // namespace
 
-int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const double direction[3], double *g_xc, double g_mpg[3],
-                     pibm_adjoint_report *rep) {
-    if (!h || nsteps < 1 || checkpoint_every < 1 || !direction || !g_xc || !g_mpg) return fail(PIBM_ERR_ARG, "bad argument");
+static int adjoint_check(pibm_handle *h) {
     const Geo &g = h->g;
     if (g.moving || g.scal || h->itrmax != 1 || !g.set_mpg || g.adaptive || g.include_frmeanfluid || !h->prm.dorpr || g.nbody < 1)
         return fail(PIBM_ERR_ARG, "adjoint: fixed spheres, AB2, SET_MPG, ADAPTIVE = F, DORPR, INCLUDE_FRMEANFLUID = F and no scalar only");
-    if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "pibm_adjoint_run starts at a step boundary");
-    int rc = pibm_run(h, 0, nullptr);   // step graphs
-    if (rc) return rc;
+    if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "the adjoint starts at a step boundary");
+    return PIBM_OK;
+}
+// adjoint work arrays, allocated on first use and kept by the handle
+static int adjoint_alloc(pibm_handle *h) {
+    const Geo &g = h->g;
     AdjBufs &a = h->adj;
     const size_t SC = (size_t)g.nx * g.PS, CR = (size_t)g.nx * (size_t)(g.my * (g.my + 2));
     if (!h->adj_ready) {
@@ -620,6 +623,30 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
         a.lubcp = R10; a.lomega = R10 + 3 * CR; a.lpbcp = R10 + 6 * CR; a.lpgr = R10 + 7 * CR;
         h->adj_ready = true;
     }
+    return PIBM_OK;
+}
+// zero the adjoint state and the gradients
+static void adjoint_zero(pibm_handle *h) {
+    const Geo &g = h->g;
+    AdjBufs &a = h->adj;
+    const size_t SC = (size_t)g.nx * g.PS;
+    cudaMemsetAsync(a.lu, 0, 3 * SC * sizeof(double2), h->stream);
+    cudaMemsetAsync(a.lp, 0, SC * sizeof(double2), h->stream);
+    cudaMemsetAsync(a.lnl, 0, 3 * SC * sizeof(double2), h->stream);
+    cudaMemsetAsync(a.gxc, 0, 3 * (size_t)g.nbody * sizeof(double), h->stream);
+    cudaMemsetAsync(a.as, 0, sizeof(AdjScal), h->stream);
+}
+
+int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const double direction[3], double *g_xc, double g_mpg[3],
+                     pibm_adjoint_report *rep) {
+    if (!h || nsteps < 1 || checkpoint_every < 1 || !direction || !g_xc || !g_mpg) return fail(PIBM_ERR_ARG, "bad argument");
+    const Geo &g = h->g;
+    int rc = adjoint_check(h);
+    if (rc) return rc;
+    if ((rc = pibm_run(h, 0, nullptr))) return rc;   // step graphs
+    AdjBufs &a = h->adj;
+    const size_t SC = (size_t)g.nx * g.PS, CR = (size_t)g.nx * (size_t)(g.my * (g.my + 2));
+    if ((rc = adjoint_alloc(h))) return rc;
     const int K = nsteps, ck = checkpoint_every, nseg = (K + ck - 1) / ck;
     const int seglen = std::min(ck, K);
     // state slots (checkpoints and the final state) and, for one segment, the
@@ -657,12 +684,7 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     const double e[3] = {direction[0], direction[1], direction[2]};
     cudaEvent_t ev[3];
     for (auto &x : ev) CUDA_OR_FAIL(cudaEventCreate(&x));
-    // zero the adjoint state and the gradients
-    cudaMemsetAsync(a.lu, 0, 3 * SC * sizeof(double2), s);
-    cudaMemsetAsync(a.lp, 0, SC * sizeof(double2), s);
-    cudaMemsetAsync(a.lnl, 0, 3 * SC * sizeof(double2), s);
-    cudaMemsetAsync(a.gxc, 0, 3 * (size_t)g.nbody * sizeof(double), s);
-    cudaMemsetAsync(a.as, 0, sizeof(AdjScal), s);
+    adjoint_zero(h);
     // forward: K steps, a checkpoint every ck steps, J accumulated on the device
     CUDA_OR_FAIL(cudaEventRecord(ev[0], s));
     for (int n = 0; n < K; ++n) {
@@ -723,6 +745,55 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
         rep->checkpoint_every = ck;
         rep->adjoint_kernels_per_step = adjoint_kernels_per_step(g);
     }
+    return PIBM_OK;
+}
+
+int pibm_adjoint_begin(pibm_handle *h, int nsteps, const double direction[3]) {
+    if (!h || nsteps < 1 || !direction) return fail(PIBM_ERR_ARG, "bad argument");
+    int rc = adjoint_check(h);
+    if (rc) return rc;
+    if ((rc = pibm_run(h, 0, nullptr))) return rc;   // step graphs
+    if ((rc = adjoint_alloc(h))) return rc;
+    adjoint_zero(h);
+    for (int d = 0; d < 3; ++d) h->adj_e[d] = direction[d];
+    h->adj_wJ = 1.0 / (double)nsteps;
+    h->adj_left = nsteps;
+    CUDA_OR_FAIL(cudaGetLastError());
+    return PIBM_OK;
+}
+
+int pibm_adjoint_step(pibm_handle *h) {
+    if (!h) return fail(PIBM_ERR_ARG, "null handle");
+    if (h->adj_left < 1) return fail(PIBM_ERR_ARG, "pibm_adjoint_step: call pibm_adjoint_begin first (or every step was reversed)");
+    if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "pibm_adjoint_step starts at a step boundary");
+    CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], h->stream));   // step n's fields
+    h->cur ^= 1;
+    AdjBufs &a = h->adj;
+    enqueue_adjoint_step(h->g, h->b, a, h->adj_e, h->adj_wJ, h->stream);
+    std::swap(a.lu, a.lu2);
+    std::swap(a.lp, a.lp2);
+    std::swap(a.lnl, a.lonl);
+    h->adj_left -= 1;
+    CUDA_OR_FAIL(cudaGetLastError());
+    return PIBM_OK;
+}
+
+int pibm_adjoint_end(pibm_handle *h, double *g_xc, double g_mpg[3]) {
+    if (!h || !g_xc || !g_mpg) return fail(PIBM_ERR_ARG, "bad argument");
+    if (!h->adj_ready) return fail(PIBM_ERR_ARG, "pibm_adjoint_end without pibm_adjoint_begin");
+    const Geo &g = h->g;
+    Scal sc;
+    AdjScal as;
+    std::vector<double> gx(3 * (size_t)g.nbody);
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(Scal), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaMemcpyAsync(&as, h->adj.as, sizeof(AdjScal), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaMemcpyAsync(gx.data(), h->adj.gxc, gx.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    if (sc.status) return fail(sc.status, "adjoint: a recomputed step reported a solver stop condition");
+    if (as.status) return fail(as.status, "adjoint: an adjoint kernel reported a bounded-wait timeout or a zero pivot");
+    if (h->adj_left != 0) return fail(PIBM_ERR_ARG, "pibm_adjoint_end before every step was reversed");
+    for (size_t q = 0; q < gx.size(); ++q) g_xc[q] = gx[q];
+    for (int d = 0; d < 3; ++d) g_mpg[d] = as.gmpg[d];
     return PIBM_OK;
 }
 

@@ -134,3 +134,26 @@ def test_torch_autograd_function_returns_the_adjoint_gradients():
     with torch.no_grad():
         J0 = drag_objective(x, g, prm, st, K, E)
     assert abs(J0.item() - ref["J"]) <= 1e-12 * abs(ref["J"])
+
+
+def test_host_driven_reverse_sweep_equals_adjoint_run():
+    """pibm_adjoint_begin / _step / _end with the host's own copies of every
+    state reproduce pibm_adjoint_run."""
+    prm, xc = _case("upwind")
+    st0 = _start_state(prm, xc, warm=4)
+    K = 5
+    ref = _gpu(prm, xc, st0).adjoint(K, E, checkpoint_every=2)
+    s = _gpu(prm, xc, st0)
+    states = []
+    for _ in range(K):
+        states.append(s.get_state())
+        s.step(1)
+    s.adjoint_begin(K, E)
+    for n in range(K - 1, -1, -1):
+        s.set_state(states[n])
+        s.adjoint_step()
+    out = s.adjoint_end()
+    assert np.max(np.abs(out["g_xc"] - ref["g_xc"])) <= 1e-12 * np.max(np.abs(ref["g_xc"]))
+    assert np.max(np.abs(out["g_mpg"] - ref["g_mpg"])) <= 1e-12 * np.max(np.abs(ref["g_mpg"]))
+    with pytest.raises(pk.PibmError):
+        s.adjoint_step()   # every step was reversed
