@@ -656,8 +656,17 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     const size_t CRb = CR * sizeof(double);
     const size_t recb = ((6 * (size_t)g.npts * sizeof(double) + 255) / 256) * 256;
     const size_t fb = 13 * CRb + recb + ((sizeof(Scal) + 255) / 256) * 256;
-    char *pool = nullptr;
-    CUDA_OR_FAIL(cudaMalloc(&pool, sb * (size_t)(nseg + 1) + fb * (size_t)seglen));
+    // the slot pool and the timing events live for this call only; released on every return path
+    struct Scratch {
+        char *pool = nullptr;
+        cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+        ~Scratch() {
+            for (auto &x : ev) if (x) cudaEventDestroy(x);
+            if (pool) cudaFree(pool);
+        }
+    } scratch;
+    CUDA_OR_FAIL(cudaMalloc(&scratch.pool, sb * (size_t)(nseg + 1) + fb * (size_t)seglen));
+    char *pool = scratch.pool;
     std::vector<int> cur_ck((size_t)nseg);
     char *slots_ck = pool, *slot_fin = pool + sb * (size_t)nseg, *fslots = pool + sb * (size_t)(nseg + 1);
     cudaStream_t s = h->stream;
@@ -682,8 +691,8 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
         return v;
     };
     const double e[3] = {direction[0], direction[1], direction[2]};
-    cudaEvent_t ev[3];
-    for (auto &x : ev) CUDA_OR_FAIL(cudaEventCreate(&x));
+    cudaEvent_t *ev = scratch.ev;
+    for (int q = 0; q < 3; ++q) CUDA_OR_FAIL(cudaEventCreate(&ev[q]));
     adjoint_zero(h);
     // forward: K steps, a checkpoint every ck steps, J accumulated on the device
     CUDA_OR_FAIL(cudaEventRecord(ev[0], s));
@@ -728,8 +737,6 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     float fms = 0.f, rms = 0.f;
     cudaEventElapsedTime(&fms, ev[0], ev[1]);
     cudaEventElapsedTime(&rms, ev[1], ev[2]);
-    for (auto &x : ev) cudaEventDestroy(x);
-    cudaFree(pool);
     // the work buffers were swapped K times: keep the handle's set consistent
     a = w;
     if (sc_fin.status) return fail(sc_fin.status, "adjoint: a forward step reported a solver stop condition");
