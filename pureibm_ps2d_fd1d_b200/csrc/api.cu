@@ -645,7 +645,7 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     if (rc) return rc;
     if ((rc = pibm_run(h, 0, nullptr))) return rc;   // step graphs
     AdjBufs &a = h->adj;
-    const size_t SC = (size_t)g.nx * g.PS, CR = (size_t)g.nx * (size_t)(g.my * (g.my + 2));
+    const size_t CR = (size_t)g.nx * (size_t)(g.my * (g.my + 2));
     if ((rc = adjoint_alloc(h))) return rc;
     const int K = nsteps, ck = checkpoint_every, nseg = (K + ck - 1) / ck;
     const int seglen = std::min(ck, K);
