@@ -268,6 +268,16 @@ int  pibm_adjoint_begin(pibm_handle *h, int nsteps, const double direction[3]);
 int  pibm_adjoint_step(pibm_handle *h);
 int  pibm_adjoint_end(pibm_handle *h, double *g_xc, double g_mpg[3]);
 
+/* ---- tile shapes (no counterpart in the reference) ----
+ * pibm_create times the x-line solve kernel with 4 and 8 (ky,kz) lines per
+ * CTA on the run's own grid (scratch copies of the state) and keeps the
+ * faster; results do not depend on the choice.  pibm_get_tuning returns the
+ * width in use and the best time of each candidate (ms[0]: 4, ms[1]: 8);
+ * pibm_set_tuning overrides it (4 or 8) before the next pibm_run (the
+ * handle's step graphs are recaptured; batch graphs are not). */
+int  pibm_get_tuning(pibm_handle *h, int32_t *lines_per_cta, double lines_ms[2]);
+int  pibm_set_tuning(pibm_handle *h, int32_t lines_per_cta);
+
 /* ---- measurement (no counterpart in the reference) ----
  * FP64 arithmetic peak of the current device: chains of fused multiply-adds
  * on 8 CTAs of 256 threads per SM, best of 5 event-timed runs (about 0.5 s).

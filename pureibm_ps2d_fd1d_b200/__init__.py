@@ -198,6 +198,16 @@ class Solver:
         return dict(J=rep.J, g_xc=g.reshape(3, self.nbody).T.copy(), g_mpg=gm, forward_ms=rep.forward_ms,
                     reverse_ms=rep.reverse_ms, adjoint_kernels_per_step=rep.adjoint_kernels_per_step)
 
+    def tuning(self) -> dict:
+        """x-line tile width chosen by the autotuner and the candidates' times."""
+        lt = C.c_int32()
+        ms = np.zeros(2)
+        _check(load_library().pibm_get_tuning(self.h, C.byref(lt), ms.ctypes.data_as(C.POINTER(C.c_double))))
+        return dict(lines_per_cta=lt.value, lines_ms={4: ms[0], 8: ms[1]})
+
+    def set_tuning(self, lines_per_cta: int):
+        _check(load_library().pibm_set_tuning(self.h, int(lines_per_cta)))
+
     # host-driven reverse sweep (pibm_adjoint_begin / _step / _end)
     def adjoint_begin(self, nsteps: int, direction=(1.0, 0.0, 0.0)):
         e = np.ascontiguousarray(direction, dtype=np.float64)

@@ -40,6 +40,8 @@ void enqueue_adjoint_step(const Geo &g, const DevBufs &b, const AdjBufs &a, cons
 void enqueue_adjoint_jacc(const Scal *sc, AdjScal *as, const double e[3], cudaStream_t s);
 int adjoint_kernels_per_step(const Geo &g);
 cudaError_t configure_adjoint_kernels(int n);
+cudaError_t autotune_lines(Geo &g, DevBufs &b, int cur, cudaStream_t s, double ms[2]);
+extern const int kLinesTiles[2];
 }  // namespace pibm
 
 using namespace pibm;
@@ -86,6 +88,7 @@ struct pibm_handle {
     AdjBufs adj{};              // adjoint work arrays (allocated by the first adjoint call)
     bool adj_ready = false;
     int adj_left = 0;           // host-driven sweep: reverse steps still expected
+    double lines_ms[2] = {0.0, 0.0};   // autotuner: best time of each x-line tile width
     double adj_e[3] = {0, 0, 0}, adj_wJ = 0.0;
 
     template <class T> cudaError_t alloc(T **p, size_t n) {
@@ -341,6 +344,8 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     for (int d = 0; d < 3; ++d) { sc.usmean_act[d] = S.usmean_des[d]; sc.frame_vel[d] = 0.0; sc.frame_pos[d] = 1.0; }
     if (!guard(cudaMemcpy(b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice), "scalars")) { delete h; return rc; }
     if (g.moving && (rc = setup_moving(h)) != PIBM_OK) { delete h; return rc; }
+    // x-line tile width measured on this run's grid
+    if (!guard(autotune_lines(g, h->b, h->cur, h->stream, h->lines_ms), "x-line tile autotune")) { delete h; return rc; }
     // time-integration stages (initialize_flo.F90:861-884)
     static const double kAB2[4] = {0.5, 0.5, 3.0 / 2.0, -0.5};
     static const double kRK3[3][4] = {{4.0 / 15.0, 4.0 / 15.0, 8.0 / 15.0, 0.0},
@@ -801,6 +806,23 @@ int pibm_adjoint_end(pibm_handle *h, double *g_xc, double g_mpg[3]) {
     if (h->adj_left != 0) return fail(PIBM_ERR_ARG, "pibm_adjoint_end before every step was reversed");
     for (size_t q = 0; q < gx.size(); ++q) g_xc[q] = gx[q];
     for (int d = 0; d < 3; ++d) g_mpg[d] = as.gmpg[d];
+    return PIBM_OK;
+}
+
+int pibm_get_tuning(pibm_handle *h, int32_t *lines_per_cta, double lines_ms[2]) {
+    if (!h) return fail(PIBM_ERR_ARG, "null handle");
+    if (lines_per_cta) *lines_per_cta = h->g.lines_lt;
+    if (lines_ms) for (int k = 0; k < 2; ++k) lines_ms[k] = h->lines_ms[k];
+    return PIBM_OK;
+}
+
+int pibm_set_tuning(pibm_handle *h, int32_t lines_per_cta) {
+    if (!h) return fail(PIBM_ERR_ARG, "null handle");
+    if (lines_per_cta != kLinesTiles[0] && lines_per_cta != kLinesTiles[1]) return fail(PIBM_ERR_ARG, "x-line tile width must be 4 or 8");
+    h->g.lines_lt = lines_per_cta;
+    for (int k = 0; k < h->itrmax; ++k) h->gs[k].lines_lt = lines_per_cta;
+    for (auto &gx : h->graph)
+        if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }   // recaptured by the next pibm_run
     return PIBM_OK;
 }
 

@@ -17,6 +17,7 @@ struct Geo {
     double cfl_max, ramp_frac_time, ucharmod, char_length, voldom, maxvolfrac, mean_volfrac, rhof, rhos;
     long long count_fluid, ncell;
     int plane_ctas;     // CTAs per plane in the plane kernels
+    int lines_lt;       // x-line tile width of k_lines (4 or 8; 0 = the size's default), set by the autotuner
     double ufmean_des[3], usmean_des[3], usmean_act[3];
     // particles (moving: the geometry arrays below are rebuilt on the device
     // every step and npts is the capacity nbody*nbnd; Scal::npts is the count)

@@ -987,9 +987,18 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
     if (!ok) atomicCAS(&sc->status, 0, PIBM_ERR_PIVOT);
 }
 
+// x-line tile width (lines per CTA): 4 or 8, chosen per run by autotune_lines
+// (a run that was not tuned takes the default below).
 template <int NX> struct LinesCfg { static constexpr int LT = NX >= 256 ? 4 : 8; };
 template <int NX>
-static size_t lines_smem() { return (size_t)(NX + 5 * LinesCfg<NX>::LT * (NX + 1) + 32) * sizeof(double2) + NX * sizeof(double); }
+static size_t lines_smem(int lt) { return (size_t)(NX + 5 * lt * (NX + 1) + 32) * sizeof(double2) + NX * sizeof(double); }
+template <int N>
+static void launch_lines(const Geo &g, DevBufs &b, double2 *u, double2 *p, int cur, Scal *sc, cudaStream_t s) {
+    const int old = cur ^ 1;
+    const int lt = g.lines_lt ? g.lines_lt : LinesCfg<N>::LT;
+    if (lt == 4) k_lines<N, 4><<<(g.PS + 3) / 4, 4 * 32, lines_smem<N>(4), s>>>(g, u, p, b.nl[cur], b.nl[old], b.ff, sc);
+    else k_lines<N, 8><<<(g.PS + 7) / 8, 8 * 32, lines_smem<N>(8), s>>>(g, u, p, b.nl[cur], b.nl[old], b.ff, sc);
+}
 
 // velstep tail: umean update (steptheflow.F90:99) and the NaN check.
 __global__ void k_scal_d(Geo g, Scal *sc) {
@@ -1107,7 +1116,8 @@ static cudaError_t set_attrs() {
     if ((e = cudaFuncSetAttribute(k_ff<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_ff2cr<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_ff2rc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_lines<N, LinesCfg<N>::LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>())) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_lines<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>(4))) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_lines<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>(8))) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
@@ -1209,8 +1219,7 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
         mark(3); mark(4);
     }
     mark(5);
-    k_lines<N, LinesCfg<N>::LT><<<(g.PS + LinesCfg<N>::LT - 1) / LinesCfg<N>::LT, LinesCfg<N>::LT * 32, lines_smem<N>(), s>>>(
-        g, b.u, b.p, b.nl[cur], b.nl[old], b.ff, b.sc);
+    launch_lines<N>(g, b, b.u, b.p, cur, b.sc, s);
     k_scal_d<<<1, 32, 0, s>>>(g, b.sc);
     mark(6);
     if (g.scal) {
@@ -1263,6 +1272,67 @@ void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStr
         case 128: enqueue_r2c_t<128>(g, a, b, nplanes, s); break;
         case 256: enqueue_r2c_t<256>(g, a, b, nplanes, s); break;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the x-line tile width: every candidate width runs the line
+// kernel on scratch copies of u, p and the step scalars (the run's state is
+// not touched; the line kernel's results do not depend on the width), best
+// of `reps` event-timed launches after a warm-up; the fastest width is kept
+// in g.lines_lt.  ms[k] = best time of candidate kLinesTiles[k].
+// ---------------------------------------------------------------------------
+extern const int kLinesTiles[2] = {4, 8};
+template <int N>
+static cudaError_t autotune_lines_t(Geo &g, DevBufs &b, int cur, cudaStream_t s, double ms[2]) {
+    const size_t SC = (size_t)g.nx * g.PS;
+    double2 *u = nullptr, *p = nullptr;
+    Scal *sc = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc(&u, 3 * SC * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&p, SC * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&sc, sizeof(Scal));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    const int reps = 5;
+    double best = 1e30;
+    int pick = 0;
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        Geo gt = g;
+        gt.lines_lt = kLinesTiles[k];
+        float tmin = 1e30f;
+        for (int r = 0; r <= reps && e == cudaSuccess; ++r) {
+            cudaMemcpyAsync(u, b.u, 3 * SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(p, b.p, SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(sc, b.sc, sizeof(Scal), cudaMemcpyDeviceToDevice, s);
+            cudaEventRecord(e0, s);
+            launch_lines<N>(gt, b, u, p, cur, sc, s);
+            cudaEventRecord(e1, s);
+            e = cudaEventSynchronize(e1);
+            float t = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+            if (r > 0 && t < tmin) tmin = t;   // r = 0 is the warm-up
+        }
+        ms[k] = tmin;
+        if (tmin < best) { best = tmin; pick = k; }
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) g.lines_lt = kLinesTiles[pick];
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(u);
+    cudaFree(p);
+    cudaFree(sc);
+    return e;
+}
+cudaError_t autotune_lines(Geo &g, DevBufs &b, int cur, cudaStream_t s, double ms[2]) {
+    switch (g.my) {
+        case 32: return autotune_lines_t<32>(g, b, cur, s, ms);
+        case 64: return autotune_lines_t<64>(g, b, cur, s, ms);
+        case 96: return autotune_lines_t<96>(g, b, cur, s, ms);
+        case 128: return autotune_lines_t<128>(g, b, cur, s, ms);
+        case 256: return autotune_lines_t<256>(g, b, cur, s, ms);
+    }
+    return cudaErrorInvalidValue;
 }
 
 void enqueue_f2d(const double2 *f, double2 *d, int nx, int nxf, int PS, int ncomp, cudaStream_t s) {
