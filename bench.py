@@ -526,6 +526,9 @@ def run_gpu(args):
     if not args.no_cpu_baseline and world == 1:
         cb = cpu_baseline(prm, xc, steps=2, warmup=1)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        # the reference's own serial semantics: the same oracle on one thread
+        cb1 = cpu_baseline(prm, xc, steps=1, warmup=0, threads=1)
+        line["cpu_baseline_1thread"] = {k: cb1[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
