@@ -718,7 +718,8 @@ static void enqueue_adjoint_step_t(const Geo &g, const DevBufs &b, const AdjBufs
     cudaMemsetAsync(a.lQ, 0, 3 * CR * sizeof(double), s);
     if (g.npts > 0)
         k_adj_rev<N><<<(g.npts + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.rec, a.lfr, b.sc, a.as, a.lubcp, a.lQ, a.lpgr, a.gxc);
-    k_adj_drag<N><<<(g.nbody * g.nbnd + 255) / 256, 256, 0, s>>>(g, b.pbcp, b.omega, a.lpbcp, a.lomega, a.gxc, e[0], e[1], e[2], wJ);
+    if (wJ != 0.0)   // RK3: only the step's last stage carries the objective
+        k_adj_drag<N><<<(g.nbody * g.nbnd + 255) / 256, 256, 0, s>>>(g, b.pbcp, b.omega, a.lpbcp, a.lomega, a.gxc, e[0], e[1], e[2], wJ);
     launch_planes<N>(k_adj_r2c<N>, 3 * g.nx, 1, s, g, (const double *)a.lQ, a.T, a.as);
     k_adj_q<<<(unsigned)((3 * SC + 255) / 256), 256, 0, s>>>(g, a.T, a.lnl_new, a.lonl, a.lu2);
     launch_planes<N>(k_adj_c2r<N>, g.nx, 8, s, g, (const double2 *)a.lnl_new, a.W8, 1);

@@ -89,6 +89,7 @@ struct pibm_handle {
     bool adj_ready = false;
     int adj_left = 0;           // host-driven sweep: reverse steps still expected
     double lines_ms[2] = {0.0, 0.0};   // autotuner: best time of each x-line tile width
+    char *adj_fields = nullptr;        // host-driven sweep with RK3: the fields of the step's stages
     double adj_e[3] = {0, 0, 0}, adj_wJ = 0.0;
 
     template <class T> cudaError_t alloc(T **p, size_t n) {
@@ -601,10 +602,53 @@ void slot_restore(pibm_handle *h, const char *slot, int cur) {
 }
 }  // namespace
 
+// Fields of one stage that its adjoint reads: ubcp(3) pbcp omega(3) pgr(3)
+// Q(3) real components, the point forces rec and the stage's Scal.
+static size_t fields_bytes(const pibm_handle *h, size_t *crb, size_t *recb) {
+    const Geo &g = h->g;
+    *crb = (size_t)g.nx * (size_t)g.RS * sizeof(double);
+    *recb = ((6 * (size_t)g.npts * sizeof(double) + 255) / 256) * 256;
+    return 13 * *crb + *recb + ((sizeof(Scal) + 255) / 256) * 256;
+}
+static void fields_save(pibm_handle *h, char *f) {
+    size_t CRb, recb;
+    fields_bytes(h, &CRb, &recb);
+    cudaStream_t s = h->stream;
+    cudaMemcpyAsync(f, h->b.ubcp, 3 * CRb, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(f + 3 * CRb, h->b.pbcp, CRb, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(f + 4 * CRb, h->b.omega, 3 * CRb, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(f + 7 * CRb, h->b.pgr, 3 * CRb, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(f + 10 * CRb, h->b.Q, 3 * CRb, cudaMemcpyDeviceToDevice, s);
+    if (h->g.npts > 0) cudaMemcpyAsync(f + 13 * CRb, h->b.rec, 6 * (size_t)h->g.npts * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(f + 13 * CRb + recb, h->b.sc, sizeof(Scal), cudaMemcpyDeviceToDevice, s);
+}
+static DevBufs fields_view(const pibm_handle *h, char *f) {
+    size_t CRb, recb;
+    fields_bytes(h, &CRb, &recb);
+    DevBufs v = h->b;
+    v.ubcp = (double *)f;
+    v.pbcp = (double *)(f + 3 * CRb);
+    v.omega = (double *)(f + 4 * CRb);
+    v.pgr = (double *)(f + 7 * CRb);
+    v.Q = (double *)(f + 10 * CRb);
+    v.rec = (double *)(f + 13 * CRb);
+    v.sc = (Scal *)(f + 13 * CRb + recb);
+    return v;
+}
+// The stages of one time step from the current state, each stage's fields
+// kept in slots f0 + k*fb (the parity of the nl ping-pong flips per stage).
+static void stages_with_fields(pibm_handle *h, char *f0, size_t fb) {
+    for (int k = 0; k < h->itrmax; ++k) {
+        enqueue_step(h->gs[k], h->b, h->cur, h->stream, nullptr, &h->ss);
+        h->cur ^= 1;
+        fields_save(h, f0 + fb * (size_t)k);
+    }
+}
+
 static int adjoint_check(pibm_handle *h) {
     const Geo &g = h->g;
-    if (g.moving || g.scal || h->itrmax != 1 || !g.set_mpg || g.adaptive || g.include_frmeanfluid || !h->prm.dorpr || g.nbody < 1)
-        return fail(PIBM_ERR_ARG, "adjoint: fixed spheres, AB2, SET_MPG, ADAPTIVE = F, DORPR, INCLUDE_FRMEANFLUID = F and no scalar only");
+    if (g.moving || g.scal || !g.set_mpg || g.adaptive || g.include_frmeanfluid || !h->prm.dorpr || g.nbody < 1)
+        return fail(PIBM_ERR_ARG, "adjoint: fixed spheres, SET_MPG, ADAPTIVE = F, DORPR, INCLUDE_FRMEANFLUID = F and no scalar only");
     if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "the adjoint starts at a step boundary");
     return PIBM_OK;
 }
@@ -650,17 +694,14 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     if (rc) return rc;
     if ((rc = pibm_run(h, 0, nullptr))) return rc;   // step graphs
     AdjBufs &a = h->adj;
-    const size_t CR = (size_t)g.nx * (size_t)(g.my * (g.my + 2));
     if ((rc = adjoint_alloc(h))) return rc;
-    const int K = nsteps, ck = checkpoint_every, nseg = (K + ck - 1) / ck;
+    const int K = nsteps, ck = checkpoint_every, nseg = (K + ck - 1) / ck, S = h->itrmax;
     const int seglen = std::min(ck, K);
     // state slots (checkpoints and the final state) and, for one segment, the
-    // forward fields every reverse step reads: ubcp(3) pbcp omega(3) pgr(3)
-    // Q(3) real components, the point forces rec and the step's Scal
+    // fields every reverse stage reads
     const size_t sb = slot_bytes(h);
-    const size_t CRb = CR * sizeof(double);
-    const size_t recb = ((6 * (size_t)g.npts * sizeof(double) + 255) / 256) * 256;
-    const size_t fb = 13 * CRb + recb + ((sizeof(Scal) + 255) / 256) * 256;
+    size_t CRb, recb;
+    const size_t fb = fields_bytes(h, &CRb, &recb);
     // the slot pool and the timing events live for this call only; released on every return path
     struct Scratch {
         char *pool = nullptr;
@@ -670,31 +711,11 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
             if (pool) cudaFree(pool);
         }
     } scratch;
-    CUDA_OR_FAIL(cudaMalloc(&scratch.pool, sb * (size_t)(nseg + 1) + fb * (size_t)seglen));
+    CUDA_OR_FAIL(cudaMalloc(&scratch.pool, sb * (size_t)(nseg + 1) + fb * (size_t)seglen * S));
     char *pool = scratch.pool;
     std::vector<int> cur_ck((size_t)nseg);
     char *slots_ck = pool, *slot_fin = pool + sb * (size_t)nseg, *fslots = pool + sb * (size_t)(nseg + 1);
     cudaStream_t s = h->stream;
-    auto save_fields = [&](char *f) {
-        cudaMemcpyAsync(f, h->b.ubcp, 3 * CRb, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(f + 3 * CRb, h->b.pbcp, CRb, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(f + 4 * CRb, h->b.omega, 3 * CRb, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(f + 7 * CRb, h->b.pgr, 3 * CRb, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(f + 10 * CRb, h->b.Q, 3 * CRb, cudaMemcpyDeviceToDevice, s);
-        if (g.npts > 0) cudaMemcpyAsync(f + 13 * CRb, h->b.rec, 6 * (size_t)g.npts * sizeof(double), cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(f + 13 * CRb + recb, h->b.sc, sizeof(Scal), cudaMemcpyDeviceToDevice, s);
-    };
-    auto fields_view = [&](char *f) {
-        DevBufs v = h->b;
-        v.ubcp = (double *)f;
-        v.pbcp = (double *)(f + 3 * CRb);
-        v.omega = (double *)(f + 4 * CRb);
-        v.pgr = (double *)(f + 7 * CRb);
-        v.Q = (double *)(f + 10 * CRb);
-        v.rec = (double *)(f + 13 * CRb);
-        v.sc = (Scal *)(f + 13 * CRb + recb);
-        return v;
-    };
     const double e[3] = {direction[0], direction[1], direction[2]};
     cudaEvent_t *ev = scratch.ev;
     for (int q = 0; q < 3; ++q) CUDA_OR_FAIL(cudaEventCreate(&ev[q]));
@@ -718,16 +739,22 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
         const int n0 = sg * ck, n1 = std::min(K, n0 + ck);
         slot_restore(h, slots_ck + sb * (size_t)sg, cur_ck[(size_t)sg]);
         for (int n = n0; n < n1; ++n) {
-            CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));
-            h->cur ^= 1;
-            save_fields(fslots + fb * (size_t)(n - n0));
+            char *f = fslots + fb * (size_t)(n - n0) * S;
+            if (S == 1) {   // AB2: the step graph, then its fields
+                CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));
+                h->cur ^= 1;
+                fields_save(h, f);
+            } else {
+                stages_with_fields(h, f, fb);
+            }
         }
-        for (int n = n1 - 1; n >= n0; --n) {
-            enqueue_adjoint_step(g, fields_view(fslots + fb * (size_t)(n - n0)), w, e, wJ, s);
-            std::swap(w.lu, w.lu2);
-            std::swap(w.lp, w.lp2);
-            std::swap(w.lnl, w.lonl);
-        }
+        for (int n = n1 - 1; n >= n0; --n)
+            for (int k = S - 1; k >= 0; --k) {   // the objective reads the last stage's drag
+                enqueue_adjoint_step(h->gs[k], fields_view(h, fslots + fb * ((size_t)(n - n0) * S + k)), w, e, k == S - 1 ? wJ : 0.0, s);
+                std::swap(w.lu, w.lu2);
+                std::swap(w.lp, w.lp2);
+                std::swap(w.lnl, w.lonl);
+            }
     }
     CUDA_OR_FAIL(cudaEventRecord(ev[2], s));
     CUDA_OR_FAIL(cudaGetLastError());
@@ -766,6 +793,11 @@ int pibm_adjoint_begin(pibm_handle *h, int nsteps, const double direction[3]) {
     if (rc) return rc;
     if ((rc = pibm_run(h, 0, nullptr))) return rc;   // step graphs
     if ((rc = adjoint_alloc(h))) return rc;
+    if (h->itrmax > 1 && !h->adj_fields) {
+        size_t CRb, recb;
+        const size_t fb = fields_bytes(h, &CRb, &recb);
+        if (h->alloc(&h->adj_fields, fb * (size_t)h->itrmax) != cudaSuccess) return fail(PIBM_ERR_NOMEM, "adjoint stage fields");
+    }
     adjoint_zero(h);
     for (int d = 0; d < 3; ++d) h->adj_e[d] = direction[d];
     h->adj_wJ = 1.0 / (double)nsteps;
@@ -778,13 +810,27 @@ int pibm_adjoint_step(pibm_handle *h) {
     if (!h) return fail(PIBM_ERR_ARG, "null handle");
     if (h->adj_left < 1) return fail(PIBM_ERR_ARG, "pibm_adjoint_step: call pibm_adjoint_begin first (or every step was reversed)");
     if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "pibm_adjoint_step starts at a step boundary");
-    CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], h->stream));   // step n's fields
-    h->cur ^= 1;
     AdjBufs &a = h->adj;
-    enqueue_adjoint_step(h->g, h->b, a, h->adj_e, h->adj_wJ, h->stream);
-    std::swap(a.lu, a.lu2);
-    std::swap(a.lp, a.lp2);
-    std::swap(a.lnl, a.lonl);
+    auto swap_state = [&]() {
+        std::swap(a.lu, a.lu2);
+        std::swap(a.lp, a.lp2);
+        std::swap(a.lnl, a.lonl);
+    };
+    if (h->itrmax == 1) {
+        CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], h->stream));   // step n's fields
+        h->cur ^= 1;
+        enqueue_adjoint_step(h->g, h->b, a, h->adj_e, h->adj_wJ, h->stream);
+        swap_state();
+    } else {
+        size_t CRb, recb;
+        const size_t fb = fields_bytes(h, &CRb, &recb);
+        stages_with_fields(h, h->adj_fields, fb);   // the stages of step n, each stage's fields kept
+        for (int k = h->itrmax - 1; k >= 0; --k) {
+            enqueue_adjoint_step(h->gs[k], fields_view(h, h->adj_fields + fb * (size_t)k), a, h->adj_e,
+                                 k == h->itrmax - 1 ? h->adj_wJ : 0.0, h->stream);
+            swap_state();
+        }
+    }
     h->adj_left -= 1;
     CUDA_OR_FAIL(cudaGetLastError());
     return PIBM_OK;

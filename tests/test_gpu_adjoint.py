@@ -18,9 +18,9 @@ pytestmark = pytest.mark.gpu
 E = np.array([1.0, 0.3, -0.2])
 
 
-def _case(scheme="upwind", my=32, nbody=3, limiter="none"):
+def _case(scheme="upwind", my=32, nbody=3, limiter="none", rk3=False):
     prm, xc = config.adjoint_case(my=my, dia_cells=8.0, nbody=nbody, seed=11, mc_moves=20)
-    prm.update(discr_scheme=scheme, limiter=limiter)
+    prm.update(discr_scheme=scheme, limiter=limiter, rk3=rk3)
     return prm, xc
 
 
@@ -58,9 +58,10 @@ def _gpu_J(prm, xc, st, K, mpg=None):
     return J / K
 
 
-@pytest.mark.parametrize("scheme,limiter", [("upwind", "none"), ("center", "none"), ("upwind", "minmod")])
-def test_adjoint_matches_oracle_adjoint(scheme, limiter):
-    prm, xc = _case(scheme, limiter=limiter)
+@pytest.mark.parametrize("scheme,limiter,rk3", [("upwind", "none", False), ("center", "none", False),
+                                                ("upwind", "minmod", False), ("upwind", "none", True)])
+def test_adjoint_matches_oracle_adjoint(scheme, limiter, rk3):
+    prm, xc = _case(scheme, limiter=limiter, rk3=rk3)
     st = _start_state(prm, xc, warm=10)
     K = 6
     parts = config.Particles(xc)
@@ -136,10 +137,11 @@ def test_torch_autograd_function_returns_the_adjoint_gradients():
     assert abs(J0.item() - ref["J"]) <= 1e-12 * abs(ref["J"])
 
 
-def test_host_driven_reverse_sweep_equals_adjoint_run():
+@pytest.mark.parametrize("rk3", [False, True])
+def test_host_driven_reverse_sweep_equals_adjoint_run(rk3):
     """pibm_adjoint_begin / _step / _end with the host's own copies of every
     state reproduce pibm_adjoint_run."""
-    prm, xc = _case("upwind")
+    prm, xc = _case("upwind", rk3=rk3)
     st0 = _start_state(prm, xc, warm=4)
     K = 5
     ref = _gpu(prm, xc, st0).adjoint(K, E, checkpoint_every=2)
@@ -147,7 +149,8 @@ def test_host_driven_reverse_sweep_equals_adjoint_run():
     states = []
     for _ in range(K):
         states.append(s.get_state())
-        s.step(1)
+        for rks in range(1, (3 if rk3 else 1) + 1):
+            s.step(rks)
     s.adjoint_begin(K, E)
     for n in range(K - 1, -1, -1):
         s.set_state(states[n])

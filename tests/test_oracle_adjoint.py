@@ -2,7 +2,7 @@
 summed drag J = (1/K) sum_n e . sum_m (pres_m + visc_m) with respect to the
 sphere centres and the imposed mean pressure gradient, checked against
 central finite differences of the oracle's forward step (fixed spheres,
-SET_MPG, fixed dt)."""
+SET_MPG, fixed dt; AB2, and RK3 with the drag of each step's last stage)."""
 import numpy as np
 import pytest
 
@@ -45,10 +45,11 @@ def _J(prm, xc, st, K, mpg=None):
     return J / K
 
 
-@pytest.mark.parametrize("scheme,limiter,K", [("upwind", "none", 4), ("center", "none", 3), ("upwind", "minmod", 3)])
-def test_adjoint_matches_central_differences(scheme, limiter, K):
+@pytest.mark.parametrize("scheme,limiter,K,rk3", [("upwind", "none", 4, False), ("center", "none", 3, False),
+                                                 ("upwind", "minmod", 3, False), ("upwind", "none", 3, True)])
+def test_adjoint_matches_central_differences(scheme, limiter, K, rk3):
     prm, xc = config.adjoint_case(my=16, dia_cells=6.0, nbody=2, seed=5)
-    prm.update(discr_scheme=scheme, limiter=limiter)
+    prm.update(discr_scheme=scheme, limiter=limiter, rk3=rk3)
     st = _start(prm, xc, warm=6)
     s = _solver(prm, xc)
     s.set_state(st)
