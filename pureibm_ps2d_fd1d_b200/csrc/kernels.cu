@@ -1277,9 +1277,10 @@ void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStr
 // ---------------------------------------------------------------------------
 // Autotuner of the x-line tile width: every candidate width runs the line
 // kernel on scratch copies of u, p and the step scalars (the run's state is
-// not touched; the line kernel's results do not depend on the width), best
-// of `reps` event-timed launches after a warm-up; the fastest width is kept
-// in g.lines_lt.  ms[k] = best time of candidate kLinesTiles[k].
+// not touched; the line kernel's results do not depend on the width): one
+// warm-up launch, then `reps` launches back to back timed together, as the
+// kernel runs inside the step graph; the fastest width is kept in
+// g.lines_lt.  ms[k] = mean time per launch of candidate kLinesTiles[k].
 // ---------------------------------------------------------------------------
 extern const int kLinesTiles[2] = {4, 8};
 template <int N>
@@ -1293,27 +1294,24 @@ static cudaError_t autotune_lines_t(Geo &g, DevBufs &b, int cur, cudaStream_t s,
     if (e == cudaSuccess) e = cudaMalloc(&sc, sizeof(Scal));
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
-    const int reps = 5;
+    const int reps = 10;
     double best = 1e30;
     int pick = 0;
     for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
         Geo gt = g;
         gt.lines_lt = kLinesTiles[k];
-        float tmin = 1e30f;
-        for (int r = 0; r <= reps && e == cudaSuccess; ++r) {
-            cudaMemcpyAsync(u, b.u, 3 * SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
-            cudaMemcpyAsync(p, b.p, SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
-            cudaMemcpyAsync(sc, b.sc, sizeof(Scal), cudaMemcpyDeviceToDevice, s);
-            cudaEventRecord(e0, s);
-            launch_lines<N>(gt, b, u, p, cur, sc, s);
-            cudaEventRecord(e1, s);
-            e = cudaEventSynchronize(e1);
-            float t = 0.f;
-            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
-            if (r > 0 && t < tmin) tmin = t;   // r = 0 is the warm-up
-        }
-        ms[k] = tmin;
-        if (tmin < best) { best = tmin; pick = k; }
+        cudaMemcpyAsync(u, b.u, 3 * SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(p, b.p, SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(sc, b.sc, sizeof(Scal), cudaMemcpyDeviceToDevice, s);
+        launch_lines<N>(gt, b, u, p, cur, sc, s);   // warm-up
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps; ++r) launch_lines<N>(gt, b, u, p, cur, sc, s);
+        cudaEventRecord(e1, s);
+        e = cudaEventSynchronize(e1);
+        float t = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+        ms[k] = t / reps;
+        if (ms[k] < best) { best = ms[k]; pick = k; }
     }
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) g.lines_lt = kLinesTiles[pick];

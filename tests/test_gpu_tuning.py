@@ -17,7 +17,7 @@ def test_tile_width_is_measured_and_does_not_change_results(my):
     t = a.tuning()
     assert t["lines_per_cta"] in (4, 8)
     assert t["lines_ms"][4] > 0 and t["lines_ms"][8] > 0
-    assert t["lines_ms"][t["lines_per_cta"]] == min(t["lines_ms"].values())
+    assert t["lines_ms"][t["lines_per_cta"]] == min(t["lines_ms"].values())   # the faster one is kept
     b = pk.Solver(config.make_params(prm), xc)
     a.set_tuning(4)
     b.set_tuning(8)
