@@ -325,6 +325,30 @@ def adjoint_gradient(nsteps: int = 200, checkpoint_every: int = 20, warm: int = 
     return res
 
 
+def single_sphere(steps: int = 100, warmup: int = 5):
+    """The single-sphere configuration: 64^3, one fixed sphere of diameter 16
+    cells at the box centre (phi = 0.008), Re 20, fluid at rest driven by the
+    mean pressure gradient, upwind; `steps` device-timed graph steps."""
+    import ctypes as C
+    import pureibm_ps2d_fd1d_b200 as pk
+    from pureibm_ps2d_fd1d_b200 import config, abi
+    prm, xc = config.single_sphere(my=64, dia_cells=16.0, re=20.0)
+    s = pk.Solver(config.make_params(prm), xc)
+    s.run(warmup)
+    lib = pk.load_library()
+    rep = abi.pibm_step_report()
+    total = C.c_double()
+    rc = lib.pibm_run_timed(s.h, steps, C.byref(rep), C.byref(total))
+    if rc != 0:
+        raise RuntimeError("pibm_run_timed (single sphere) failed: %d %s" % (rc, lib.pibm_last_error().decode()))
+    ncell = s.nx * s.my * s.mz
+    out = {"unit": UNIT, "value": ncell * steps / (total.value / 1e3) / 1e6, "ms_per_step": total.value / steps,
+           "steps": steps, "norm_drag": rep.norm_drag, "tuning": s.tuning()["lines_per_cta"],
+           "config": "64^3, 1 sphere d=16 at the centre, Re 20, upwind"}
+    s.close()
+    return out
+
+
 def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024):
     """Batched multiple-independent-simulation throughput against the plain
     per-realization loop on the same GPU: 16 seeded realizations (grids from
@@ -517,6 +541,8 @@ def run_gpu(args):
     }
     if not args.no_mis and world == 1:
         line["batched_mis"] = batched_mis()
+    if not args.no_mis and world == 1:
+        line["single_sphere"] = single_sphere()
     if not args.no_scalar and world == 1:
         line["with_scalar"] = with_scalar()
     if not args.no_moving and world == 1:
