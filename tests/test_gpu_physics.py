@@ -49,3 +49,13 @@ def test_stokes_drag_approaches_hasimoto_as_dt_shrinks():
     assert coarse < fine < K
     assert fine > 0.95 * K, (fine, K)
     assert abs(fine - K) < abs(coarse - K)
+
+
+def test_stokes_drag_at_higher_volume_fraction():
+    """phi = 0.065 (d = 32 cells in 64^3, the Sangani-Acrivos series gives
+    K = 2.842; Zick & Homsy's tabulated 2.81 at phi = 0.064): the engine's
+    steady drag at a viscous number of 0.075 is within 3% below it
+    (measured 2.762)."""
+    K = hasimoto(np.pi / 6.0 * (32.0 / 64.0) ** 3)
+    nd = steady_drag(12800.0, my=64, d=32.0)
+    assert 0.95 * K < nd < K, (nd, K)
