@@ -160,3 +160,39 @@ def test_host_driven_reverse_sweep_equals_adjoint_run(rk3):
     assert np.max(np.abs(out["g_mpg"] - ref["g_mpg"])) <= 1e-12 * np.max(np.abs(ref["g_mpg"]))
     with pytest.raises(pk.PibmError):
         s.adjoint_step()   # every step was reversed
+
+
+def test_adjoint_matches_oracle_at_64():
+    prm, xc = config.adjoint_case(my=64, dia_cells=12.0, nbody=4, seed=2, mc_moves=20)
+    parts = config.Particles(xc)
+    cpu = oc.OracleSolver(config.make_params(prm), parts.struct)
+    st = cpu.get_state()
+    st["umean"] = np.array(prm["umean0"])
+    cpu.set_state(st)
+    for _ in range(3):
+        cpu.step()
+    st = cpu.get_state()
+    K = 3
+    ref = cpu.adjoint(K, E)
+    out = _gpu(prm, xc, st).adjoint(K, E, checkpoint_every=2)
+    assert abs(out["J"] - ref["J"]) <= 1e-10 * abs(ref["J"])
+    assert np.max(np.abs(out["g_xc"] - ref["g_xc"])) <= 1e-8 * np.max(np.abs(ref["g_xc"]))
+    assert np.max(np.abs(out["g_mpg"] - ref["g_mpg"])) <= 1e-8 * np.max(np.abs(ref["g_mpg"]))
+
+
+@pytest.mark.parametrize("my,nbody", [(128, 12), (256, 20)])
+def test_adjoint_runs_at_large_grids(my, nbody):
+    """The adjoint's other size instantiations: J equals the forward run's
+    drag average and the gradients are finite and non-zero."""
+    prm, xc = config.adjoint_case(my=my, dia_cells=20.0, nbody=nbody, seed=9, mc_moves=0)
+    s = pk.Solver(config.make_params(prm), xc)
+    st = s.get_state()
+    st["umean"] = np.array(prm["umean0"])
+    s.set_state(st)
+    s.run(3)
+    st = s.get_state()
+    K = 2
+    out = s.adjoint(K, E, checkpoint_every=1)
+    assert abs(out["J"] - _gpu_J(prm, xc, st, K)) <= 1e-12 * abs(out["J"])
+    assert np.all(np.isfinite(out["g_xc"])) and np.all(np.isfinite(out["g_mpg"]))
+    assert np.max(np.abs(out["g_xc"])) > 0 and np.max(np.abs(out["g_mpg"])) > 0
