@@ -353,7 +353,11 @@ def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024)
     """Batched multiple-independent-simulation throughput against the plain
     per-realization loop on the same GPU: 16 seeded realizations (grids from
     {64, 96, 128}^3, phi ~ U[0.1, 0.4], d ~ U{12..20} cells, Re ~ U[10, 100]),
-    `steps` steps of every member each way, device-timed."""
+    `steps` steps of every member each way, device-timed: the plain loop as
+    each member replaying its own step graphs one after another, and the
+    batch graph.  Also the reference-style host loop (each member stepped in
+    turn through pibm_step with its report read back), wall-timed, since the
+    steps are synchronous."""
     import pureibm_ps2d_fd1d_b200 as pk
     from pureibm_ps2d_fd1d_b200 import config
     ens = config.mis_ensemble(n=n, seed=seed)
@@ -362,9 +366,18 @@ def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024)
     cells = sum(p["my"] ** 3 for p, _, _ in ens) * steps
     t_plain = b.time(steps, sequential=True)
     t_batch = b.time(steps, sequential=False)
+    # the reference-style host loop: each realization stepped in turn through
+    # the public per-step call (pibm_step, its report read back every step)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for m in b.members:
+            m.step(1)
+    t_api = (time.perf_counter() - t0) * 1e3
     b.close()
     return {"unit": "Mcell-steps/s", "plain": cells / (t_plain / 1e3) / 1e6, "batched": cells / (t_batch / 1e3) / 1e6,
-            "ratio": t_plain / t_batch, "members": n, "steps": steps, "seed": seed,
+            "ratio": t_plain / t_batch,
+            "step_api_loop": cells / (t_api / 1e3) / 1e6, "ratio_vs_step_api_loop": t_api / t_batch,
+            "members": n, "steps": steps, "seed": seed,
             "grids": [p["my"] for p, _, _ in ens], "nbody": [len(x) for _, x, _ in ens],
             "phi": [round(f, 4) for _, _, f in ens]}
 
