@@ -243,8 +243,8 @@ int  pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *
  * state after the K steps, as after pibm_run(h, K).
  * Supported runs: fixed spheres, AB2 or RK3 (with RK3 the objective reads
  * the drag of each step's last stage, the driver's record), SET_MPG (imposed
- * mean pressure gradient), ADAPTIVE = F (fixed dt), DORPR,
- * INCLUDE_FRMEANFLUID = F, no scalar; otherwise PIBM_ERR_ARG.  The solid mask, the active reversal
+ * mean pressure gradient), ADAPTIVE = F (fixed dt), DORPR, no scalar;
+ * otherwise PIBM_ERR_ARG.  The solid mask, the active reversal
  * points and the upwind branches are those of the forward run (the gradient
  * of the piecewise-smooth map on the trajectory's branch). */
 typedef struct pibm_adjoint_report {

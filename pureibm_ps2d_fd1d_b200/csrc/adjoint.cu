@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(256) k_adj_rev(Geo g, const double *__restrict
 #pragma unroll
                     for (int n = 0; n < 3; ++n) {
                         double gg = as->lfrmean[n] * rnc;
-                        if (!isfl) gg += lfr[n * CR + node];
+                        if (g.include_frmeanfluid || !isfl) gg += lfr[n * CR + node];   // INCLUDE_FRMEANFLUID: every corner keeps its share
                         else if (count_so > 0) gg += lsol[n] / (double)count_so;
                         lft[n] += w / g.dx3 * gg;
                         lw += ft[n] / g.dx3 * gg;

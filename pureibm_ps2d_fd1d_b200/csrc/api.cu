@@ -647,8 +647,8 @@ static void stages_with_fields(pibm_handle *h, char *f0, size_t fb) {
 
 static int adjoint_check(pibm_handle *h) {
     const Geo &g = h->g;
-    if (g.moving || g.scal || !g.set_mpg || g.adaptive || g.include_frmeanfluid || !h->prm.dorpr || g.nbody < 1)
-        return fail(PIBM_ERR_ARG, "adjoint: fixed spheres, SET_MPG, ADAPTIVE = F, DORPR, INCLUDE_FRMEANFLUID = F and no scalar only");
+    if (g.moving || g.scal || !g.set_mpg || g.adaptive || !h->prm.dorpr || g.nbody < 1)
+        return fail(PIBM_ERR_ARG, "adjoint: fixed spheres, SET_MPG, ADAPTIVE = F, DORPR and no scalar only");
     if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "the adjoint starts at a step boundary");
     return PIBM_OK;
 }

@@ -18,9 +18,9 @@ pytestmark = pytest.mark.gpu
 E = np.array([1.0, 0.3, -0.2])
 
 
-def _case(scheme="upwind", my=32, nbody=3, limiter="none", rk3=False):
+def _case(scheme="upwind", my=32, nbody=3, limiter="none", rk3=False, frfl=False):
     prm, xc = config.adjoint_case(my=my, dia_cells=8.0, nbody=nbody, seed=11, mc_moves=20)
-    prm.update(discr_scheme=scheme, limiter=limiter, rk3=rk3)
+    prm.update(discr_scheme=scheme, limiter=limiter, rk3=rk3, include_frmeanfluid=frfl)
     return prm, xc
 
 
@@ -58,10 +58,11 @@ def _gpu_J(prm, xc, st, K, mpg=None):
     return J / K
 
 
-@pytest.mark.parametrize("scheme,limiter,rk3", [("upwind", "none", False), ("center", "none", False),
-                                                ("upwind", "minmod", False), ("upwind", "none", True)])
-def test_adjoint_matches_oracle_adjoint(scheme, limiter, rk3):
-    prm, xc = _case(scheme, limiter=limiter, rk3=rk3)
+@pytest.mark.parametrize("scheme,limiter,rk3,frfl", [("upwind", "none", False, False), ("center", "none", False, False),
+                                                     ("upwind", "minmod", False, False), ("upwind", "none", True, False),
+                                                     ("upwind", "none", False, True)])
+def test_adjoint_matches_oracle_adjoint(scheme, limiter, rk3, frfl):
+    prm, xc = _case(scheme, limiter=limiter, rk3=rk3, frfl=frfl)
     st = _start_state(prm, xc, warm=10)
     K = 6
     parts = config.Particles(xc)

@@ -45,11 +45,12 @@ def _J(prm, xc, st, K, mpg=None):
     return J / K
 
 
-@pytest.mark.parametrize("scheme,limiter,K,rk3", [("upwind", "none", 4, False), ("center", "none", 3, False),
-                                                 ("upwind", "minmod", 3, False), ("upwind", "none", 3, True)])
-def test_adjoint_matches_central_differences(scheme, limiter, K, rk3):
+@pytest.mark.parametrize("scheme,limiter,K,rk3,frfl", [("upwind", "none", 4, False, False), ("center", "none", 3, False, False),
+                                                      ("upwind", "minmod", 3, False, False), ("upwind", "none", 3, True, False),
+                                                      ("upwind", "none", 3, False, True)])
+def test_adjoint_matches_central_differences(scheme, limiter, K, rk3, frfl):
     prm, xc = config.adjoint_case(my=16, dia_cells=6.0, nbody=2, seed=5)
-    prm.update(discr_scheme=scheme, limiter=limiter, rk3=rk3)
+    prm.update(discr_scheme=scheme, limiter=limiter, rk3=rk3, include_frmeanfluid=frfl)
     st = _start(prm, xc, warm=6)
     s = _solver(prm, xc)
     s.set_state(st)
