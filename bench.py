@@ -276,6 +276,10 @@ def adjoint_gradient(nsteps: int = 200, checkpoint_every: int = 20, warm: int = 
     fwd_ms = total.value
     s.set_state(st)
     out = s.adjoint(nsteps, e, checkpoint_every)
+    # the same gradient with the whole trajectory's fields kept in HBM
+    # (segment length from free memory: no recomputation when it fits)
+    s.set_state(st)
+    out_all = s.adjoint(nsteps, e, 0)
     s.close()
     res = {"config": "96^3, 30 fixed spheres d=16 (phi 0.073), Re 20, SET_MPG, fixed dt, upwind; %d steps after %d, "
                      "checkpoints every %d" % (nsteps, warm, checkpoint_every),
@@ -285,6 +289,10 @@ def adjoint_gradient(nsteps: int = 200, checkpoint_every: int = 20, warm: int = 
            "gradient_over_forward": (out["forward_ms"] + out["reverse_ms"]) / fwd_ms,
            "forward_ms_per_step": fwd_ms / nsteps, "reverse_ms_per_step": out["reverse_ms"] / nsteps,
            "adjoint_kernels_per_step": out["adjoint_kernels_per_step"],
+           "store_all": {"reverse_ms": out_all["reverse_ms"], "reverse_over_forward": out_all["reverse_ms"] / fwd_ms,
+                         "gradient_over_forward": (out_all["forward_ms"] + out_all["reverse_ms"]) / fwd_ms,
+                         "max_rel_diff_vs_checkpointed": float(np.max(np.abs(out_all["g_xc"] - out["g_xc"])) /
+                                                              np.max(np.abs(out["g_xc"])))},
            "g_mpg": list(out["g_mpg"]), "g_xc_norm": float(np.linalg.norm(out["g_xc"]))}
     if fd:
         def J_of(xcv, mpg=None):

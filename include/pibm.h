@@ -239,8 +239,11 @@ int  pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *
  * e = direction[3].  Returns dJ/dxc in g_xc (nbody,3) column-major (grid
  * units, the layout of pibm_particles.xc) and dJ/dmpg in g_mpg[3].  The
  * forward trajectory is kept as checkpoints every checkpoint_every steps and
- * recomputed segment by segment in the reverse sweep.  The handle ends at the
- * state after the K steps, as after pibm_run(h, K).
+ * recomputed segment by segment in the reverse sweep (the last segment's
+ * fields are kept by the forward pass itself); checkpoint_every <= 0 takes
+ * as many steps per segment as 80% of the free device memory holds, i.e. no
+ * recomputation when the whole run fits.  The handle ends at the state after
+ * the K steps, as after pibm_run(h, K).
  * Supported runs: fixed spheres, AB2 or RK3 (with RK3 the objective reads
  * the drag of each step's last stage, the driver's record), SET_MPG (imposed
  * mean pressure gradient), ADAPTIVE = F (fixed dt), DORPR, no scalar;

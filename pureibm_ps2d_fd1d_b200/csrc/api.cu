@@ -688,20 +688,28 @@ static void adjoint_zero(pibm_handle *h) {
 
 int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const double direction[3], double *g_xc, double g_mpg[3],
                      pibm_adjoint_report *rep) {
-    if (!h || nsteps < 1 || checkpoint_every < 1 || !direction || !g_xc || !g_mpg) return fail(PIBM_ERR_ARG, "bad argument");
+    if (!h || nsteps < 1 || !direction || !g_xc || !g_mpg) return fail(PIBM_ERR_ARG, "bad argument");
     const Geo &g = h->g;
     int rc = adjoint_check(h);
     if (rc) return rc;
     if ((rc = pibm_run(h, 0, nullptr))) return rc;   // step graphs
     AdjBufs &a = h->adj;
     if ((rc = adjoint_alloc(h))) return rc;
-    const int K = nsteps, ck = checkpoint_every, nseg = (K + ck - 1) / ck, S = h->itrmax;
-    const int seglen = std::min(ck, K);
+    const int K = nsteps, S = h->itrmax;
     // state slots (checkpoints and the final state) and, for one segment, the
     // fields every reverse stage reads
     const size_t sb = slot_bytes(h);
     size_t CRb, recb;
     const size_t fb = fields_bytes(h, &CRb, &recb);
+    int ck = checkpoint_every;
+    if (ck <= 0) {   // as many steps per segment as 80% of the free memory holds
+        size_t fr = 0, tot = 0;
+        CUDA_OR_FAIL(cudaMemGetInfo(&fr, &tot));
+        const double per_step = (double)fb * S + (double)sb;
+        ck = (int)std::max(1.0, std::min((double)K, 0.8 * (double)fr / per_step));
+    }
+    const int nseg = (K + ck - 1) / ck, seglen = std::min(ck, K);
+    const int last0 = (nseg - 1) * ck;   // the last segment keeps its fields in the forward pass
     // the slot pool and the timing events live for this call only; released on every return path
     struct Scratch {
         char *pool = nullptr;
@@ -724,8 +732,13 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     CUDA_OR_FAIL(cudaEventRecord(ev[0], s));
     for (int n = 0; n < K; ++n) {
         if (n % ck == 0) { slot_save(h, slots_ck + sb * (size_t)(n / ck)); cur_ck[(size_t)(n / ck)] = h->cur; }
-        CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));
-        h->cur ^= 1;
+        if (n >= last0 && S > 1) {
+            stages_with_fields(h, fslots + fb * (size_t)(n - last0) * S, fb);
+        } else {
+            CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));
+            h->cur ^= 1;
+            if (n >= last0) fields_save(h, fslots + fb * (size_t)(n - last0));
+        }
         enqueue_adjoint_jacc(h->b.sc, a.as, e, s);
     }
     slot_save(h, slot_fin);
@@ -737,8 +750,8 @@ int pibm_adjoint_run(pibm_handle *h, int nsteps, int checkpoint_every, const dou
     const double wJ = 1.0 / (double)K;
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int n0 = sg * ck, n1 = std::min(K, n0 + ck);
-        slot_restore(h, slots_ck + sb * (size_t)sg, cur_ck[(size_t)sg]);
-        for (int n = n0; n < n1; ++n) {
+        if (sg < nseg - 1) slot_restore(h, slots_ck + sb * (size_t)sg, cur_ck[(size_t)sg]);
+        for (int n = n0; n < n1 && sg < nseg - 1; ++n) {
             char *f = fslots + fb * (size_t)(n - n0) * S;
             if (S == 1) {   // AB2: the step graph, then its fields
                 CUDA_OR_FAIL(cudaGraphLaunch(h->graph[h->cur], s));
