@@ -101,8 +101,9 @@ def test_adjoint_matches_central_differences():
         assert abs(out["g_mpg"][d] - fd) <= 1e-6 * abs(fd) + 1e-9, (d, out["g_mpg"][d], fd)
 
 
-def test_adjoint_independent_of_checkpoint_interval():
-    prm, xc = _case("upwind")
+@pytest.mark.parametrize("rk3", [False, True])
+def test_adjoint_independent_of_checkpoint_interval(rk3):
+    prm, xc = _case("upwind", rk3=rk3)
     st = _start_state(prm, xc, warm=4)
     K = 7
     outs = [_gpu(prm, xc, st).adjoint(K, E, checkpoint_every=ck) for ck in (1, 3, 7, 20, 0)]   # 0: from free memory
