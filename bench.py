@@ -560,22 +560,30 @@ def run_gpu(args):
         "maxvolfrac": info.maxvolfrac,
         "last_step": {"divmax": rep.divmax, "norm_drag": rep.norm_drag, "dt": rep.dt},
     }
-    if not args.no_mis and world == 1:
-        line["batched_mis"] = batched_mis()
-    if not args.no_mis and world == 1:
-        line["single_sphere"] = single_sphere()
-    if not args.no_scalar and world == 1:
-        line["with_scalar"] = with_scalar()
-    if not args.no_moving and world == 1:
-        line["moving_suspension"] = moving_suspension()
-    if not args.no_adjoint and world == 1:
-        line["adjoint"] = adjoint_gradient()
-    if not args.no_cpu_baseline and world == 1:
-        cb = cpu_baseline(prm, xc, steps=2, warmup=1)
-        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
-        # the reference's own serial semantics: the same oracle on one thread
-        cb1 = cpu_baseline(prm, xc, steps=1, warmup=0, threads=1)
-        line["cpu_baseline_1thread"] = {k: cb1[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    def section(key, fn):
+        # a failing optional measurement is recorded, never allowed to drop the headline line
+        try:
+            line[key] = fn()
+        except Exception as ex:   # noqa: BLE001
+            line[key] = {"error": repr(ex)[:400]}
+            print("bench: section %s failed: %r" % (key, ex), file=sys.stderr)
+
+    if world == 1:
+        if not args.no_mis:
+            section("batched_mis", batched_mis)
+            section("single_sphere", single_sphere)
+        if not args.no_scalar:
+            section("with_scalar", with_scalar)
+        if not args.no_moving:
+            section("moving_suspension", moving_suspension)
+        if not args.no_adjoint:
+            section("adjoint", adjoint_gradient)
+        if not args.no_cpu_baseline:
+            keys = ("value", "unit", "cores", "kind", "sample")
+            section("cpu_baseline", lambda: {k: v for k, v in cpu_baseline(prm, xc, steps=2, warmup=1).items() if k in keys})
+            # the reference's own serial semantics: the same oracle on one thread
+            section("cpu_baseline_1thread",
+                    lambda: {k: v for k, v in cpu_baseline(prm, xc, steps=1, warmup=0, threads=1).items() if k in keys})
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
