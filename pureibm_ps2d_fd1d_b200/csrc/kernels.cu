@@ -752,12 +752,19 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const doubl
 // Tiles live in shared memory as [line][i]; global loads and stores run over
 // consecutive lines (contiguous in the [i][k][j] layout).
 // ============================================================================
+// Tile row pitch of k_lines (double2 elements).  A 16-byte shared access is
+// served per 8 threads (128 bytes = 8 slots of 4 banks); the element loops put
+// thread t on (line t % LT, plane t / LT), so 8 threads cover 8 lines of one
+// plane for LT = 8 (an odd pitch puts them in distinct slots) and 4 lines of two
+// planes for LT = 4 (a pitch of 2 mod 8 does: slot 2*line + i).
+template <int NX, int LT> __host__ __device__ constexpr int lines_pitch() { return LT == 4 ? NX + 2 : NX + 1; }
+
 template <int NX, int LT>
 __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ u, double2 *__restrict__ p,
                                                    const double2 *__restrict__ nl, const double2 *__restrict__ onl,
                                                    const double2 *__restrict__ ff, Scal *__restrict__ sc) {
     constexpr int R = NX / 32;
-    constexpr int NP = NX + 1;                // tile row pitch: rows of consecutive lines start 4 banks apart
+    constexpr int NP = lines_pitch<NX, LT>();
     extern __shared__ double2 sm[];
     double2 *tws = sm;
     double2 *RHS = tws + NX;
@@ -991,7 +998,10 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
 // (a run that was not tuned takes the default below).
 template <int NX> struct LinesCfg { static constexpr int LT = NX >= 256 ? 4 : 8; };
 template <int NX>
-static size_t lines_smem(int lt) { return (size_t)(NX + 5 * lt * (NX + 1) + 32) * sizeof(double2) + NX * sizeof(double); }
+static size_t lines_smem(int lt) {
+    const int np = lt == 4 ? lines_pitch<NX, 4>() : lines_pitch<NX, 8>();
+    return (size_t)(NX + 5 * lt * np + 32) * sizeof(double2) + NX * sizeof(double);
+}
 template <int N>
 static void launch_lines(const Geo &g, DevBufs &b, double2 *u, double2 *p, int cur, Scal *sc, cudaStream_t s) {
     const int old = cur ^ 1;
