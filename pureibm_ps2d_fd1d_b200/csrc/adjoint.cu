@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(LT * 32) k_adj_lines(Geo g, const double2 *__r
                                                        double2 *__restrict__ lonl, double2 *__restrict__ lff,
                                                        const Scal *__restrict__ sc, AdjScal *as) {
     constexpr int R = NX / 32;
-    constexpr int NP = NX + 1;
+    constexpr int NP = lines_pitch<NX, LT>();
     extern __shared__ double2 sm[];
     double2 *tws = sm;
     double2 *D = tws + NX;                 // lambda d, then lambda of the divcorr right-hand side
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(LT * 32) k_adj_lines(Geo g, const double2 *__r
 template <int NX>
 static size_t adj_lines_smem() {
     constexpr int LT = NX >= 256 ? 4 : 8;
-    return (size_t)(NX + 5 * LT * (NX + 1) + 32) * sizeof(double2) + NX * sizeof(double);
+    return (size_t)(NX + 5 * LT * lines_pitch<NX, LT>() + 32) * sizeof(double2) + NX * sizeof(double);
 }
 
 // ============================================================================

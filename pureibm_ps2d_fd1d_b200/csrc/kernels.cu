@@ -752,13 +752,6 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const doubl
 // Tiles live in shared memory as [line][i]; global loads and stores run over
 // consecutive lines (contiguous in the [i][k][j] layout).
 // ============================================================================
-// Tile row pitch of k_lines (double2 elements).  A 16-byte shared access is
-// served per 8 threads (128 bytes = 8 slots of 4 banks); the element loops put
-// thread t on (line t % LT, plane t / LT), so 8 threads cover 8 lines of one
-// plane for LT = 8 (an odd pitch puts them in distinct slots) and 4 lines of two
-// planes for LT = 4 (a pitch of 2 mod 8 does: slot 2*line + i).
-template <int NX, int LT> __host__ __device__ constexpr int lines_pitch() { return LT == 4 ? NX + 2 : NX + 1; }
-
 template <int NX, int LT>
 __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ u, double2 *__restrict__ p,
                                                    const double2 *__restrict__ nl, const double2 *__restrict__ onl,

@@ -604,7 +604,7 @@ template <int NX, int LT>
 __global__ void __launch_bounds__(LT * 32) k_slines(Geo g, double2 *__restrict__ phif, const double2 *__restrict__ nln,
                                                     const double2 *__restrict__ nlo, const double2 *__restrict__ ffs,
                                                     Scal *__restrict__ sc) {
-    constexpr int R = NX / 32, NP = NX + 1;
+    constexpr int R = NX / 32, NP = lines_pitch<NX, LT>();
     extern __shared__ double2 sm[];
     double2 *tws = sm;
     double2 *RHS = tws + NX;                       // [line][i], pitch NP
@@ -669,7 +669,10 @@ __global__ void __launch_bounds__(LT * 32) k_slines(Geo g, double2 *__restrict__
 }
 template <int NX> struct SLinesCfg { static constexpr int LT = NX >= 256 ? 4 : 8; };
 template <int NX>
-static size_t slines_smem() { return (size_t)(NX + SLinesCfg<NX>::LT * (NX + 1) + 32) * sizeof(double2) + 2 * NX * sizeof(double); }
+static size_t slines_smem() {
+    constexpr int LT = SLinesCfg<NX>::LT;
+    return (size_t)(NX + LT * lines_pitch<NX, LT>() + 32) * sizeof(double2) + 2 * NX * sizeof(double);
+}
 
 // heat_ratio update, surface flux and Nusselt number (bcsetscal, bc_scalar.F90:186-190,
 // 361-363; stepthescalar.F90:90-91), status.

@@ -154,4 +154,11 @@ inline void launch_planes(void (*k)(KArgs...), int nplanes, int items, cudaStrea
 }
 
 
+// Tile row pitch of the x-line kernels' [line][i] tiles (double2 elements).  A 16-byte shared access is
+// served per 8 threads (128 bytes = 8 slots of 4 banks); the element loops put
+// thread t on (line t % LT, plane t / LT), so 8 threads cover 8 lines of one
+// plane for LT = 8 (an odd pitch puts them in distinct slots) and 4 lines of two
+// planes for LT = 4 (a pitch of 2 mod 8 does: slot 2*line + i).
+template <int NX, int LT> __host__ __device__ constexpr int lines_pitch() { return LT == 4 ? NX + 2 : NX + 1; }
+
 }  // namespace pibm

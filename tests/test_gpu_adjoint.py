@@ -182,6 +182,23 @@ def test_adjoint_matches_oracle_at_64():
     assert np.max(np.abs(out["g_mpg"] - ref["g_mpg"])) <= 1e-8 * np.max(np.abs(ref["g_mpg"]))
 
 
+def test_adjoint_matches_oracle_at_256():
+    """256^3: the adjoint x-line solves run in 4-line tiles there."""
+    prm, xc = config.adjoint_case(my=256, dia_cells=20.0, nbody=6, seed=3, mc_moves=20)
+    parts = config.Particles(xc)
+    cpu = oc.OracleSolver(config.make_params(prm), parts.struct)
+    st = cpu.get_state()
+    st["umean"] = np.array(prm["umean0"])
+    cpu.set_state(st)
+    cpu.step()
+    st = cpu.get_state()
+    ref = cpu.adjoint(1, E)
+    out = _gpu(prm, xc, st).adjoint(1, E, checkpoint_every=1)
+    assert abs(out["J"] - ref["J"]) <= 1e-10 * abs(ref["J"])
+    assert np.max(np.abs(out["g_xc"] - ref["g_xc"])) <= 1e-8 * np.max(np.abs(ref["g_xc"]))
+    assert np.max(np.abs(out["g_mpg"] - ref["g_mpg"])) <= 1e-8 * np.max(np.abs(ref["g_mpg"]))
+
+
 @pytest.mark.parametrize("my,nbody", [(128, 12), (256, 20)])
 def test_adjoint_runs_at_large_grids(my, nbody):
     """The adjoint's other size instantiations: J equals the forward run's

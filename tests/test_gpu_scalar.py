@@ -81,6 +81,17 @@ def test_scalar_spheres_across_the_x_boundary_64():
 
 
 @pytest.mark.gpu
+def test_scalar_random_array_256_two_steps():
+    """256^3 grid: the scalar's x-line solves run in 4-line tiles there."""
+    prm, xc = config.random_array(my=256, dia_cells=20, nbody=6, seed=3, mc_moves=20)
+    gpu, cpu = make_pair(scalar_params(prm), xc)
+    for _ in range(2):
+        gpu.step()
+        cpu.step()
+    compare(gpu, cpu)
+
+
+@pytest.mark.gpu
 def test_scalar_started_on_a_developed_flow():
     """The reference starts a scalar run on a converged flow (restart with
     ISCALON = 1, phi = 1); the flow state is carried over with set_state."""
