@@ -81,15 +81,18 @@ __global__ void __launch_bounds__(LT * 32) k_adj_lines(Geo g, const double2 *__r
     double2 *U = P + LT * NP;              // [comp][line][i]: lambda u_n -> lambda Us -> lambda r
     double *gam = (double *)(U + 3 * LT * NP);
     double2 *st = (double2 *)(gam + NX);
+    double *lcs = (double *)(st + 32);        // per-lane constants of the solves
+    double2 *ltr = (double2 *)(lcs + NX);
     for (int t = threadIdx.x; t < NX; t += blockDim.x) tws[t] = g.tw[t];
     fill_stage_table<32>(st, g.tw, NX);
+    fill_line_tw<R>(lcs, ltr, g.tw);
     const int PS = g.PS, nx = NX;
     const int q0 = blockIdx.x * LT;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const double dx = g.dx, dx2 = g.dx2, dt = sc->dt, vis = g.vis;
     const double c1 = g.c1, c2 = g.c2, c3 = g.c3, c4 = g.c4;
     const double alp = (c1 + c2) * dt, c2dtv = (c2 * dt) * vis, gd = dt * vis * c1;
-    const Tw tw{tws, NX, 1, st};
+    const LineTw<R> tw{{tws, NX, 1, st}, lcs, ltr};
     auto KY = [&](int q) { return g.ky[q % g.my2]; };
     auto KZ = [&](int q) { return g.kz[q / g.my2]; };
     auto W = [&](int i) { return i < 0 ? i + nx : (i >= nx ? i - nx : i); };
@@ -222,7 +225,7 @@ __global__ void __launch_bounds__(LT * 32) k_adj_lines(Geo g, const double2 *__r
 template <int NX>
 static size_t adj_lines_smem() {
     constexpr int LT = NX >= 256 ? 4 : 8;
-    return (size_t)(NX + 5 * LT * lines_pitch<NX, LT>() + 32) * sizeof(double2) + NX * sizeof(double);
+    return (size_t)(NX + 5 * LT * lines_pitch<NX, LT>() + 32) * sizeof(double2) + NX * sizeof(double) + line_tw_bytes<NX / 32>();
 }
 
 // ============================================================================

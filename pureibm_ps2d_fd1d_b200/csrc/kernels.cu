@@ -765,15 +765,18 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
     double2 *U = P + LT * NP;                 // [comp][line][i]
     double *gam = (double *)(U + 3 * LT * NP);
     double2 *st = (double2 *)(gam + NX);      // cross-lane stage twiddles
+    double *lcs = (double *)(st + 32);        // per-lane constants of the solves
+    double2 *ltr = (double2 *)(lcs + NX);
     if (sc->status) return;
     for (int t = threadIdx.x; t < NX; t += blockDim.x) tws[t] = g.tw[t];
     fill_stage_table<32>(st, g.tw, NX);
+    fill_line_tw<R>(lcs, ltr, g.tw);
     const int PS = g.PS, nx = NX;
     const int q0 = blockIdx.x * LT;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const double dx = g.dx, dx2 = g.dx2, dt = sc->dt, vis = g.vis;
     const double c1 = g.c1, c2 = g.c2, c3 = g.c3, c4 = g.c4;
-    const Tw tw{tws, NX, 1, st};
+    const LineTw<R> tw{{tws, NX, 1, st}, lcs, ltr};
     auto KY = [&](int q) { return g.ky[q % g.my2]; };
     auto KZ = [&](int q) { return g.kz[q / g.my2]; };
     auto G = [&](const double2 *f, int comp, int i, int q) -> double2 {
@@ -993,7 +996,7 @@ template <int NX> struct LinesCfg { static constexpr int LT = NX >= 256 ? 4 : 8;
 template <int NX>
 static size_t lines_smem(int lt) {
     const int np = lt == 4 ? lines_pitch<NX, 4>() : lines_pitch<NX, 8>();
-    return (size_t)(NX + 5 * lt * np + 32) * sizeof(double2) + NX * sizeof(double);
+    return (size_t)(NX + 5 * lt * np + 32) * sizeof(double2) + NX * sizeof(double) + line_tw_bytes<NX / 32>();
 }
 template <int N>
 static void launch_lines(const Geo &g, DevBufs &b, double2 *u, double2 *p, int cur, Scal *sc, cudaStream_t s) {
