@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const doubl
                     if (jl == L::MC && rank != 0) continue;
                     const int ge = kz * my2 + cl_col<N>(jl, rank);
                     const double2 Xr = cl_unpack<N>(buf, kz, jl, rank);
-                    const double2 X = make_double2(Xr.x / g.nrm, Xr.y / g.nrm);
+                    const double2 X = r2c_norm<N>(Xr, g.nrm);
                     if (q == 0) { const double ky = g.ky[cl_col<N>(jl, rank)]; dst[ge] = make_double2(-ky * X.y, ky * X.x); }
                     else { const double kzv = g.kz[kz]; dst[ge] = cadd(dst[ge], make_double2(-kzv * X.y, kzv * X.x)); }
                 }
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const doubl
             if (jl == L::MC && rank != 0) continue;
             const int ge = kz * my2 + cl_col<N>(jl, rank);
             const double2 Xr = cl_unpack<N>(buf, kz, jl, rank);
-            const double2 X = make_double2(Xr.x / g.nrm, Xr.y / g.nrm);
+            const double2 X = r2c_norm<N>(Xr, g.nrm);
             const double2 a = cadd(dst[ge], X);
             dst[ge] = make_double2(-a.x, -a.y);
         }
@@ -730,7 +730,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const doubl
             const int kz = e / L::PZ, jl = e - kz * L::PZ;
             if (jl == L::MC && rank != 0) continue;
             const double2 X = cl_unpack<N>(buf, kz, jl, rank);
-            dst[kz * my2 + cl_col<N>(jl, rank)] = make_double2(X.x / g.nrm, X.y / g.nrm);
+            dst[kz * my2 + cl_col<N>(jl, rank)] = r2c_norm<N>(X, g.nrm);
         }
     }
 }
@@ -1106,7 +1106,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff2rc(Geo g, const do
         const int kz = e / L::PZ, jl = e - kz * L::PZ;
         if (jl == L::MC && rank != 0) continue;
         const double2 X = cl_unpack<N>(buf, kz, jl, rank);
-        b[q * PS + kz * my2 + cl_col<N>(jl, rank)] = make_double2(X.x / g.nrm, X.y / g.nrm);
+        b[q * PS + kz * my2 + cl_col<N>(jl, rank)] = r2c_norm<N>(X, g.nrm);
     }
 }
 

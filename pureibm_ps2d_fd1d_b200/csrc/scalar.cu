@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_snl(Geo g, const doub
             if (jl == L::MC && rank != 0) continue;
             const int j = cl_col<N>(jl, rank), ge = kz * my2 + j;
             const double2 Xr = cl_unpack<N>(buf, kz, jl, rank);
-            const double2 X = make_double2(Xr.x / g.nrm, Xr.y / g.nrm);
+            const double2 X = r2c_norm<N>(Xr, g.nrm);
             if (q == 0) { const double ky = g.ky[j]; dst[ge] = make_double2(-ky * X.y, ky * X.x); }
             else if (q == 1) { const double kzv = g.kz[kz]; dst[ge] = cadd(dst[ge], make_double2(-kzv * X.y, kzv * X.x)); }
             else { const double2 a = cadd(dst[ge], X); dst[ge] = make_double2(-a.x, -a.y); }
@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_sff(Geo g, const doub
         const int kz = e / L::PZ, jl = e - kz * L::PZ;
         if (jl == L::MC && rank != 0) continue;
         const double2 X = cl_unpack<N>(buf, kz, jl, rank);
-        dst[kz * my2 + cl_col<N>(jl, rank)] = make_double2(X.x / g.nrm, X.y / g.nrm);
+        dst[kz * my2 + cl_col<N>(jl, rank)] = r2c_norm<N>(X, g.nrm);
     }
 }
 

@@ -20,6 +20,18 @@ __device__ __forceinline__ void load_tw(double2 *tws, const Geo &g) {
 // Physical real planes are RSP = N*(N+2) doubles: the shared-memory image of a
 // transformed plane (rows of N data doubles + 2 unused).
 template <int N> struct RP { static constexpr int RSP = N * (N + 2); static constexpr uint32_t BYTES = RSP * 8; };
+// The r2c normalisation x / nrm, nrm = my*mz = N*N (ff2rc).  For N a power of
+// two 1/nrm is exact, so x * (1/nrm) and x / nrm are the same correctly rounded
+// value and the multiplication replaces the longer division sequence; other
+// sizes keep the division.
+template <int N> __device__ __forceinline__ double2 r2c_norm(double2 x, double nrm) {
+    if constexpr ((N & (N - 1)) == 0) {
+        constexpr double r = 1.0 / ((double)N * (double)N);
+        return make_double2(x.x * r, x.y * r);
+    } else {
+        return make_double2(x.x / nrm, x.y / nrm);
+    }
+}
 // Bounded wait on the CTA's load barrier; records a timeout in the status word.
 __device__ __forceinline__ void load_wait(uint64_t *mb, uint32_t &phase, Scal *sc) {
     if (!mbar_wait(mb, phase)) atomicCAS(&sc->status, 0, PIBM_ERR_TIMEOUT);
