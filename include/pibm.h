@@ -288,6 +288,11 @@ int  pibm_set_tuning(pibm_handle *h, int32_t lines_per_cta);
  * on 8 CTAs of 256 threads per SM, best of 5 event-timed runs (about 0.5 s).
  * tflops = 2 * fma count / time; ms (optional) = the best run's time. */
 int  pibm_fp64_peak(double *tflops, double *ms);
+/* Check of the engine's reciprocal division (no counterpart in the
+ * reference): for every pair (a[i], b[j]) the quotient that the kernels form
+ * from b's reciprocal (a*y and one FMA correction, y = 1/b) is compared bit
+ * for bit with a / b on the device; mismatches = the number that differ. */
+int  pibm_qdiv_check(const double *a, long long n, const double *b, int nb, long long *mismatches);
 
 /* ---- batched independent realizations (the MIS ensemble of
  *      sample_inputs/set_mis_3d, run as one graph-captured launch stream) ---- */

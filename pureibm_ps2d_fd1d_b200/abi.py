@@ -112,7 +112,7 @@ EXPORTED = [
     "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed",
     "pibm_run_profiled", "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev",
     "pibm_get_fluid_mask", "pibm_get_contacts", "pibm_get_scalar_nl", "pibm_set_scalar",
-    "pibm_set_desired_means", "pibm_adjoint_run", "pibm_adjoint_begin", "pibm_adjoint_step", "pibm_adjoint_end", "pibm_fp64_peak", "pibm_get_tuning", "pibm_set_tuning", "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
+    "pibm_set_desired_means", "pibm_adjoint_run", "pibm_adjoint_begin", "pibm_adjoint_step", "pibm_adjoint_end", "pibm_fp64_peak", "pibm_qdiv_check", "pibm_get_tuning", "pibm_set_tuning", "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
     "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time", "pibm_batch_member",
     "pibm_batch_destroy",
 ]
@@ -140,6 +140,7 @@ def bind(lib):
     lib.pibm_set_desired_means.argtypes = [vp, P(_f64), P(_f64)]
     lib.pibm_adjoint_run.argtypes = [vp, C.c_int, C.c_int, P(_f64), P(_f64), P(_f64), P(pibm_adjoint_report)]
     lib.pibm_fp64_peak.argtypes = [P(_f64), P(_f64)]
+    lib.pibm_qdiv_check.argtypes = [P(_f64), C.c_longlong, P(_f64), C.c_int, P(C.c_longlong)]
     lib.pibm_adjoint_begin.argtypes = [vp, C.c_int, P(_f64)]
     lib.pibm_adjoint_step.argtypes = [vp]
     lib.pibm_adjoint_end.argtypes = [vp, P(_f64), P(_f64)]
@@ -162,6 +163,6 @@ def bind(lib):
     for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed", "pibm_run_profiled",
                  "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev", "pibm_get_fluid_mask",
                  "pibm_get_contacts", "pibm_get_scalar_nl", "pibm_set_scalar", "pibm_set_desired_means",
-                 "pibm_adjoint_run", "pibm_adjoint_begin", "pibm_adjoint_step", "pibm_adjoint_end", "pibm_fp64_peak", "pibm_get_tuning", "pibm_set_tuning", "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
+                 "pibm_adjoint_run", "pibm_adjoint_begin", "pibm_adjoint_step", "pibm_adjoint_end", "pibm_fp64_peak", "pibm_qdiv_check", "pibm_get_tuning", "pibm_set_tuning", "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
         getattr(lib, name).restype = C.c_int
     return lib

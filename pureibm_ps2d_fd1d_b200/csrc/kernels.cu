@@ -208,6 +208,16 @@ __device__ __forceinline__ double slope_lim(double um1, double u0, double up1, d
     }
     return s * phi * 1.0;
 }
+// slope_lim with the divisor 2 dx given with its reciprocal (qdiv)
+__device__ __forceinline__ double slope_lim_q(double um1, double u0, double up1, double tdx, double rtdx, int limiter) {
+    double s = qdiv(up1 - um1, tdx, rtdx);
+    double phi = 1.0;
+    if (limiter == PIBM_LIMITER_MINMOD) {
+        phi = (u0 - um1) / (up1 - u0 + kSmallD);
+        phi = phi <= 0.0 ? 0.0 : fmin(1.0, phi);
+    }
+    return s * phi * 1.0;
+}
 
 // x-flux difference D_c at plane i for node e of the plane (upwind: MUSCL
 // states + Rusanov flux, nl_allflow.F90:139-294; center: nl_allflow.F90:97-124,298-310).
@@ -278,13 +288,14 @@ __global__ void __launch_bounds__(256) k_flux(Geo g, const double *__restrict__ 
         return __ldg(ubcp + c * CR + (size_t)ii * RSP + e);
     };
     const double dx = g.dx, h = dx / 2.0;
+    const double tdx = 2.0 * dx, rtdx = 1.0 / tdx, rdx = 1.0 / dx;   // divisors and reciprocals for qdiv
     if (g.scheme == PIBM_SCHEME_CENTER) {
         for (int i = i0; i < i0 + SEG; ++i) {
             const double ap = U(0, i + 1), am = U(0, i - 1);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const double fp = ap * (c == 0 ? ap : U(c, i + 1)), fm = am * (c == 0 ? am : U(c, i - 1));
-                Dx[c * CR + (size_t)i * RSP + e] = (fp - fm) / (2.0 * dx);
+                Dx[c * CR + (size_t)i * RSP + e] = qdiv(fp - fm, tdx, rtdx);
             }
         }
         return;
@@ -311,8 +322,8 @@ __global__ void __launch_bounds__(256) k_flux(Geo g, const double *__restrict__ 
     double sprev[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        sprev[c] = slope_lim(um2[c], w[c][0], w[c][1], dx, lim);     // s(i0-1)
-        sl[c][0] = slope_lim(w[c][0], w[c][1], w[c][2], dx, lim);     // s(i0)
+        sprev[c] = slope_lim_q(um2[c], w[c][0], w[c][1], tdx, rtdx, lim);     // s(i0-1)
+        sl[c][0] = slope_lim_q(w[c][0], w[c][1], w[c][2], tdx, rtdx, lim);     // s(i0)
     }
     {
         const int m = (i0 - 1 + nx) % nx;
@@ -324,11 +335,11 @@ __global__ void __launch_bounds__(256) k_flux(Geo g, const double *__restrict__ 
 #pragma unroll
         for (int c = 0; c < 3; ++c) w[c][3] = U(c, i + 2);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) sl[c][1] = slope_lim(w[c][1], w[c][2], w[c][3], dx, lim);   // s(i+1)
+        for (int c = 0; c < 3; ++c) sl[c][1] = slope_lim_q(w[c][1], w[c][2], w[c][3], tdx, rtdx, lim);   // s(i+1)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const double F = flux(c, i, w[0][1], w[0][2], sl[0][0], sl[0][1], w[c][1], w[c][2], sl[c][0], sl[c][1]);
-            Dx[c * CR + (size_t)i * RSP + e] = (F - Fm[c]) / dx;
+            Dx[c * CR + (size_t)i * RSP + e] = qdiv(F - Fm[c], dx, rdx);
             Fm[c] = F;
         }
 #pragma unroll
@@ -776,6 +787,7 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const double dx = g.dx, dx2 = g.dx2, dt = sc->dt, vis = g.vis;
     const double c1 = g.c1, c2 = g.c2, c3 = g.c3, c4 = g.c4;
+    const double c12 = c1 + c2, rdx = 1.0 / dx, rdx2 = 1.0 / dx2, rc12 = 1.0 / c12;   // divisors and reciprocals for qdiv
     const LineTw<R> tw{{tws, NX, 1, st}, lcs, ltr};
     auto KY = [&](int q) { return g.ky[q % g.my2]; };
     auto KZ = [&](int q) { return g.kz[q / g.my2]; };
@@ -811,7 +823,7 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
         double2 tt = make_double2(0.0, 0.0), d, s;
         d = csub(x1[0], x0[0]);
         s = csub(x1[3], x0[3]);
-        tt = make_double2(tt.x + (c3 * d.x) / dx + s.x / dx, tt.y + (c3 * d.y) / dx + s.y / dx);
+        tt = make_double2(tt.x + qdiv(c3 * d.x, dx, rdx) + qdiv(s.x, dx, rdx), tt.y + qdiv(c3 * d.y, dx, rdx) + qdiv(s.y, dx, rdx));
         d = mwy(cadd(x1[1], x0[1]));
         s = mwy(cadd(x1[4], x0[4]));
         tt = make_double2(tt.x + (c3 * d.x) / 2.0 + s.x / 2.0, tt.y + (c3 * d.y) / 2.0 + s.y / 2.0);
@@ -819,12 +831,12 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
         s = mwz(cadd(x1[5], x0[5]));
         tt = make_double2(tt.x + (c3 * d.x) / 2.0 + s.x / 2.0, tt.y + (c3 * d.y) / 2.0 + s.y / 2.0);
         d = csub(x1[6], x0[6]);
-        tt = make_double2(tt.x + (c4 * d.x) / dx, tt.y + (c4 * d.y) / dx);
+        tt = make_double2(tt.x + qdiv(c4 * d.x, dx, rdx), tt.y + qdiv(c4 * d.y, dx, rdx));
         d = mwy(cadd(x1[7], x0[7]));
         tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
         d = mwz(cadd(x1[8], x0[8]));
         tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
-        RHS[line * NP + i] = make_double2(tt.x / (c1 + c2), tt.y / (c1 + c2));
+        RHS[line * NP + i] = make_double2(qdiv(tt.x, c12, rc12), qdiv(tt.y, c12, rc12));
         P[line * NP + i] = p[(size_t)i * PS + q];
         // explicit part of the ustep right-hand sides, dt*(c3 nl + ff + c4 onl) per component
         // (usteptime.F90:291-297), kept in the velocity tiles until each component is solved
@@ -883,7 +895,7 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
             double2 r = make_double2(ui.x * fy + ex.x, ui.y * fy + ex.y);
             const double2 pm = P[line * NP + (i == 0 ? nx - 1 : i - 1)], p0 = P[line * NP + i];
             double2 gp;
-            if (n == 0) gp = make_double2((alp * (p0.x - pm.x)) / dx, (alp * (p0.y - pm.y)) / dx);
+            if (n == 0) gp = make_double2(qdiv(alp * (p0.x - pm.x), dx, rdx), qdiv(alp * (p0.y - pm.y), dx, rdx));
             else {
                 const double2 sp = make_double2(alp * 0.5 * (pm.x + p0.x), alp * 0.5 * (pm.y + p0.y));
                 gp = (n == 1) ? make_double2(-ky * sp.y, ky * sp.x) : make_double2(-kz * sp.y, kz * sp.x);
@@ -893,7 +905,7 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
             double2 lap;
             if (i == 0) lap = make_double2((up.x - 2.0 * ui.x) + um.x, (up.y - 2.0 * ui.y) + um.y);
             else lap = make_double2((um.x + up.x) - 2.0 * ui.x, (um.y + up.y) - 2.0 * ui.y);
-            rr[k] = make_double2(r.x + (gd * lap.x) / dx2, r.y + (gd * lap.y) / dx2);
+            rr[k] = make_double2(r.x + qdiv(gd * lap.x, dx2, rdx2), r.y + qdiv(gd * lap.y, dx2, rdx2));
         }
         __syncthreads();
 #pragma unroll
@@ -914,18 +926,18 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
         __syncthreads();
     }
     // ---------------- divcorr (poisson.F90:241-508) ----------------
-    const double alpc = (c1 + c2) * dt;
+    const double alpc = (c1 + c2) * dt, ralpc = 1.0 / alpc;
     for (int t = threadIdx.x; t < LT * NX; t += blockDim.x) {
         const int line = t % LT, i = t / LT, q = q0 + line;
         if (q >= PS) continue;
         const double ky = KY(q), kz = KZ(q);
         const int ip = i == nx - 1 ? 0 : i + 1;
         const double2 *U1 = U + (0 * LT + line) * NP, *U2 = U + (1 * LT + line) * NP, *U3 = U + (2 * LT + line) * NP;
-        double2 tt = make_double2((U1[ip].x - U1[i].x) / dx, (U1[ip].y - U1[i].y) / dx);
+        double2 tt = make_double2(qdiv(U1[ip].x - U1[i].x, dx, rdx), qdiv(U1[ip].y - U1[i].y, dx, rdx));
         double2 sy = cscale(cadd(U2[i], U2[ip]), 0.5), sz = cscale(cadd(U3[i], U3[ip]), 0.5);
         tt = cadd(tt, make_double2(-ky * sy.y, ky * sy.x));
         tt = cadd(tt, make_double2(-kz * sz.y, kz * sz.x));
-        RHS[line * NP + i] = make_double2((0.5 * (1.0 + 1.0) * tt.x) / alpc, (0.5 * (1.0 + 1.0) * tt.y) / alpc);
+        RHS[line * NP + i] = make_double2(qdiv(0.5 * (1.0 + 1.0) * tt.x, alpc, ralpc), qdiv(0.5 * (1.0 + 1.0) * tt.y, alpc, ralpc));
     }
     __syncthreads();
     if (wact) {
@@ -951,10 +963,10 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
             double2 gy, gz;
             if (i == 0) { gy = cscale(make_double2(-ky * 0.0, ky * alpc), 0.5); gz = cscale(make_double2(-kz * 0.0, kz * alpc), 0.5); }
             else { gy = make_double2(-ky * 0.0, ky * (alpc * 0.5)); gz = make_double2(-kz * 0.0, kz * (alpc * 0.5)); }
-            nu1[r] = make_double2(U1[i].x - (alpc * (d0.x - dm.x)) / dx, U1[i].y - (alpc * (d0.y - dm.y)) / dx);
+            nu1[r] = make_double2(U1[i].x - qdiv(alpc * (d0.x - dm.x), dx, rdx), U1[i].y - qdiv(alpc * (d0.y - dm.y), dx, rdx));
             nu2[r] = csub(U2[i], cmul(gy, s));
             nu3[r] = csub(U3[i], cmul(gz, s));
-            const double2 lap = make_double2(((dm.x - 2.0 * d0.x) + dp.x) / dx2 - w2w * d0.x, ((dm.y - 2.0 * d0.y) + dp.y) / dx2 - w2w * d0.y);
+            const double2 lap = make_double2(qdiv((dm.x - 2.0 * d0.x) + dp.x, dx2, rdx2) - w2w * d0.x, qdiv((dm.y - 2.0 * d0.y) + dp.y, dx2, rdx2) - w2w * d0.y);
             np[r] = make_double2((Pw[i].x + d0.x) - c2dtv * lap.x, (Pw[i].y + d0.y) - c2dtv * lap.y);
         }
         __syncwarp();
@@ -969,7 +981,7 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int i = lane + 32 * r, ip = i == nx - 1 ? 0 : i + 1;
-            double2 tt = make_double2((U1[ip].x - U1[i].x) / dx, (U1[ip].y - U1[i].y) / dx);
+            double2 tt = make_double2(qdiv(U1[ip].x - U1[i].x, dx, rdx), qdiv(U1[ip].y - U1[i].y, dx, rdx));
             double2 sy = cscale(cadd(U2[i], U2[ip]), 0.5), sz = cscale(cadd(U3[i], U3[ip]), 0.5);
             tt = cadd(tt, make_double2(-ky * sy.y, ky * sy.x));
             tt = cadd(tt, make_double2(-kz * sz.y, kz * sz.x));

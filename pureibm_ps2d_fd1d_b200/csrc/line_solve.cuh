@@ -62,8 +62,8 @@ __device__ __forceinline__ void circulant_solve(double2 *row, double a, double b
     // lane holds modes m = r + R*bitrev(lane)
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const double lam = ((double)N) * (b + 2.0 * a * lt.cs[r * 32 + lane]);
-        v[r] = make_double2(v[r].x / lam, v[r].y / lam);
+        const double lam = ((double)N) * (b + 2.0 * a * lt.cs[r * 32 + lane]), rlam = 1.0 / lam;
+        v[r] = make_double2(qdiv(v[r].x, lam, rlam), qdiv(v[r].y, lam, rlam));
     }
     // exact inverse of the forward stages (unnormalised; 1/N folded into lam)
 #pragma unroll

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/pibm.h"
+#include "step_common.cuh"
 
 namespace {
 
@@ -23,7 +24,43 @@ __global__ void __launch_bounds__(256) k_dfma_chain(double *out, int iters, doub
     if (s == 12345.678) out[blockIdx.x * blockDim.x + threadIdx.x] = s;   // keeps the chains live
 }
 
+// Bitwise comparison of qdiv(a, b, 1/b) with the division a / b.
+__global__ void k_qdiv_check(const double *a, long long n, const double *b, int nb, unsigned long long *bad) {
+    unsigned long long cnt = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * nb; t += (long long)gridDim.x * blockDim.x) {
+        const double x = a[t % n], d = b[t / n];
+        const double y = 1.0 / d;
+        if (__double_as_longlong(pibm::qdiv(x, d, y)) != __double_as_longlong(x / d)) ++cnt;
+    }
+    if (cnt) atomicAdd(bad, cnt);
+}
+
 }  // namespace
+
+extern "C" int pibm_qdiv_check(const double *a, long long n, const double *b, int nb, long long *mismatches) {
+    if (!a || !b || !mismatches || n <= 0 || nb <= 0) return PIBM_ERR_ARG;
+    double *da = nullptr, *db = nullptr;
+    unsigned long long *dbad = nullptr;
+    if (cudaMalloc(&da, (size_t)n * sizeof(double)) != cudaSuccess) return PIBM_ERR_NOMEM;
+    if (cudaMalloc(&db, (size_t)nb * sizeof(double)) != cudaSuccess || cudaMalloc(&dbad, sizeof(*dbad)) != cudaSuccess) {
+        cudaFree(da);
+        cudaFree(db);
+        return PIBM_ERR_NOMEM;
+    }
+    cudaMemcpy(da, a, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(db, b, (size_t)nb * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemset(dbad, 0, sizeof(*dbad));
+    k_qdiv_check<<<1184, 256>>>(da, n, db, nb, dbad);
+    unsigned long long bad = 0;
+    cudaMemcpy(&bad, dbad, sizeof(bad), cudaMemcpyDeviceToHost);
+    const cudaError_t err = cudaGetLastError();
+    cudaFree(da);
+    cudaFree(db);
+    cudaFree(dbad);
+    if (err != cudaSuccess) return PIBM_ERR_CUDA;
+    *mismatches = (long long)bad;
+    return PIBM_OK;
+}
 
 extern "C" int pibm_fp64_peak(double *tflops, double *ms_out) {
     if (!tflops) return PIBM_ERR_ARG;

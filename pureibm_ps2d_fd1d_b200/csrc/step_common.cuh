@@ -20,6 +20,19 @@ __device__ __forceinline__ void load_tw(double2 *tws, const Geo &g) {
 // Physical real planes are RSP = N*(N+2) doubles: the shared-memory image of a
 // transformed plane (rows of N data doubles + 2 unused).
 template <int N> struct RP { static constexpr int RSP = N * (N + 2); static constexpr uint32_t BYTES = RSP * 8; };
+// a / b from the reciprocal y = 1/b (correctly rounded, computed once by the
+// caller): q = a*y, then one correction with the exact FMA remainder,
+// q + (a - q*b)*y (Markstein, IBM J. Res. Dev. 34(1), 1990; "Markstein's
+// theorem" in Muller et al., Handbook of Floating-Point Arithmetic).  For
+// normal operands and quotients the result is the correctly rounded a / b
+// (checked against the division on the device in the tests); a zero
+// remainder means q is exact and is kept as is, sign of zero included.
+__device__ __forceinline__ double qdiv(double a, double b, double y) {
+    const double q = a * y;
+    const double e = fma(-q, b, a);
+    return e == 0.0 ? q : fma(e, y, q);
+}
+
 // The r2c normalisation x / nrm, nrm = my*mz = N*N (ff2rc).  For N a power of
 // two 1/nrm is exact, so x * (1/nrm) and x / nrm are the same correctly rounded
 // value and the multiplication replaces the longer division sequence; other
