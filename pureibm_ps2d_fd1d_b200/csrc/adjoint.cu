@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(LT * 32) k_adj_lines(Geo g, const double2 *__r
     const int PS = g.PS, nx = NX;
     const int q0 = blockIdx.x * LT;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const double dx = g.dx, dx2 = g.dx2, dt = sc->dt, vis = g.vis;
+    const double dx = g.dx, dx2 = g.dx2, dt = sc->dt, vis = g.vis, rdx2 = 1.0 / dx2;
     const double c1 = g.c1, c2 = g.c2, c3 = g.c3, c4 = g.c4;
     const double alp = (c1 + c2) * dt, c2dtv = (c2 * dt) * vis, gd = dt * vis * c1;
     const LineTw<R> tw{{tws, NX, 1, st}, lcs, ltr};
@@ -110,8 +110,8 @@ __global__ void __launch_bounds__(LT * 32) k_adj_lines(Geo g, const double2 *__r
         const double ky = KY(q), kz = KZ(q), w2 = g.w2[q];
         const double2 *Pl = P + line * NP, *U0 = U + (0 * LT + line) * NP, *U1 = U + (1 * LT + line) * NP, *U2 = U + (2 * LT + line) * NP;
         const double2 pm = Pl[W(i - 1)], p0 = Pl[i], pp = Pl[W(i + 1)];
-        double2 v = make_double2(p0.x - c2dtv * (((pm.x - 2.0 * p0.x) + pp.x) / dx2 - w2 * p0.x),
-                                 p0.y - c2dtv * (((pm.y - 2.0 * p0.y) + pp.y) / dx2 - w2 * p0.y));
+        double2 v = make_double2(p0.x - c2dtv * (qdiv((pm.x - 2.0 * p0.x) + pp.x, dx2, rdx2) - w2 * p0.x),
+                                 p0.y - c2dtv * (qdiv((pm.y - 2.0 * p0.y) + pp.y, dx2, rdx2) - w2 * p0.y));
         const double2 a0 = U0[i], a1 = U0[W(i + 1)];
         v = make_double2(v.x - (alp / dx) * (a0.x - a1.x), v.y - (alp / dx) * (a0.y - a1.y));
         // conj(-alp wy / 2) = i alp ky / 2
@@ -175,8 +175,8 @@ __global__ void __launch_bounds__(LT * 32) k_adj_lines(Geo g, const double2 *__r
 #pragma unroll
             for (int n = 0; n < 3; ++n) {
                 const double2 r0 = Rn[n][i], rm = Rn[n][im], rp = Rn[n][ip];
-                lu2[((size_t)n * nx + i) * PS + q] = make_double2(fy * r0.x + gd * ((rm.x + rp.x) - 2.0 * r0.x) / dx2,
-                                                                 fy * r0.y + gd * ((rm.y + rp.y) - 2.0 * r0.y) / dx2);
+                lu2[((size_t)n * nx + i) * PS + q] = make_double2(fy * r0.x + qdiv(gd * ((rm.x + rp.x) - 2.0 * r0.x), dx2, rdx2),
+                                                                 fy * r0.y + qdiv(gd * ((rm.y + rp.y) - 2.0 * r0.y), dx2, rdx2));
             }
         }
     }
@@ -535,8 +535,9 @@ __global__ void __launch_bounds__(256) k_adj_q(Geo g, const double2 *__restrict_
 
 // MUSCL slope of the forward flux (slope_lim) and its partials
 // d s / d (u(i-1), u(i), u(i+1)).
-__device__ __forceinline__ double slope_d(double um1, double u0, double up1, double dx, int limiter, double ds[3]) {
-    const double S = (up1 - um1) / (2.0 * dx);
+// tdx = 2 dx with its reciprocal rtdx (qdiv).
+__device__ __forceinline__ double slope_d(double um1, double u0, double up1, double tdx, double rtdx, int limiter, double ds[3]) {
+    const double S = qdiv(up1 - um1, tdx, rtdx);
     double phi = 1.0, d0 = 0.0, d1 = 0.0, d2 = 0.0;
     if (limiter == PIBM_LIMITER_MINMOD) {
         const double num = u0 - um1, den = up1 - u0 + kSmallD;
@@ -549,9 +550,9 @@ __device__ __forceinline__ double slope_d(double um1, double u0, double up1, dou
             d2 = -num / (den * den);
         }
     }
-    ds[0] = -phi / (2.0 * dx) + S * d0;
+    ds[0] = qdiv(-phi, tdx, rtdx) + S * d0;
     ds[1] = S * d1;
-    ds[2] = phi / (2.0 * dx) + S * d2;
+    ds[2] = qdiv(phi, tdx, rtdx) + S * d2;
     return S * phi;
 }
 
@@ -582,6 +583,7 @@ __global__ void __launch_bounds__(256) k_adj_flux(Geo g, const double *__restric
     auto U = [&](int c, int ii) { return __ldg(ubcp + c * CR + (size_t)X(ii) * RSP + e); };
     auto LD = [&](int c, int ii) { return __ldg(W8 + (5 + c) * CR + (size_t)X(ii) * RSP + e); };
     const double dx = g.dx, h = dx / 2.0;
+    const double tdx = 2.0 * dx, rtdx = 1.0 / tdx, rdx = 1.0 / dx;   // divisors and reciprocals for qdiv
     // pointwise part: the products, and the whole center-scheme flux
     auto pointwise = [&](int i, double lu[3]) {
         const size_t o = (size_t)i * RSP + e;
@@ -594,7 +596,7 @@ __global__ void __launch_bounds__(256) k_adj_flux(Geo g, const double *__restric
             const double uc[3] = {u0, u1, u2};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const double lf = (LD(c, i - 1) - LD(c, i + 1)) / (2.0 * dx);
+                const double lf = qdiv(LD(c, i - 1) - LD(c, i + 1), tdx, rtdx);
                 lu[0] += uc[c] * lf;
                 lu[c] += u0 * lf;
             }
@@ -618,8 +620,8 @@ __global__ void __launch_bounds__(256) k_adj_flux(Geo g, const double *__restric
     for (int c = 0; c < 3; ++c) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) { w[c][k] = U(c, m - 1 + k); acc[c][k] = 0.0; }
-        sl[c][0] = slope_d(w[c][0], w[c][1], w[c][2], dx, lim, ds[c][0]);
-        sl[c][1] = slope_d(w[c][1], w[c][2], w[c][3], dx, lim, ds[c][1]);
+        sl[c][0] = slope_d(w[c][0], w[c][1], w[c][2], tdx, rtdx, lim, ds[c][0]);
+        sl[c][1] = slope_d(w[c][1], w[c][2], w[c][3], tdx, rtdx, lim, ds[c][1]);
         ld[c][0] = LD(c, m);
         ld[c][1] = LD(c, m + 1);
     }
@@ -631,7 +633,7 @@ __global__ void __launch_bounds__(256) k_adj_flux(Geo g, const double *__restric
         double la = 0.0, lb = 0.0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const double lF = (ld[c][0] - ld[c][1]) / dx;
+            const double lF = qdiv(ld[c][0] - ld[c][1], dx, rdx);
             const double A = w[c][1] + sl[c][0] * h, B = w[c][2] - sl[c][1] * h;
             const double pa = (0.5 * A - 0.5 * (B - A) * (amax ? sa : 0.0)) * lF;
             const double pb = (0.5 * B - 0.5 * (B - A) * (amax ? 0.0 : sb)) * lF;
@@ -669,7 +671,7 @@ __global__ void __launch_bounds__(256) k_adj_flux(Geo g, const double *__restric
             w[c][0] = w[c][1]; w[c][1] = w[c][2]; w[c][2] = w[c][3]; w[c][3] = U(c, m + 3);
             sl[c][0] = sl[c][1];
             ds[c][0][0] = ds[c][1][0]; ds[c][0][1] = ds[c][1][1]; ds[c][0][2] = ds[c][1][2];
-            sl[c][1] = slope_d(w[c][1], w[c][2], w[c][3], dx, lim, ds[c][1]);
+            sl[c][1] = slope_d(w[c][1], w[c][2], w[c][3], tdx, rtdx, lim, ds[c][1]);
             ld[c][0] = ld[c][1];
             ld[c][1] = LD(c, m + 2);
         }
@@ -686,18 +688,18 @@ __global__ void __launch_bounds__(256) k_adj_assemble(Geo g, const double2 *__re
     if (t >= SC) return;
     const size_t q = t % PS, i = t / PS;
     const size_t im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
-    const double ky = g.ky[q % g.my2], kz = g.kz[q / g.my2], tdx = 2.0 * g.dx;
+    const double ky = g.ky[q % g.my2], kz = g.kz[q / g.my2], tdx = 2.0 * g.dx, rtdx = 1.0 / tdx;
     auto C = [&](int c, size_t ii) { return T[c * SC + ii * PS + q]; };
     const double2 o0 = C(3, i), o1 = C(4, i), o2 = C(5, i);
     const double2 o1m = C(4, im), o1p = C(4, ip), o2m = C(5, im), o2p = C(5, ip);
     double2 a0 = cadd(C(0, i), cadd(mul_cis(o1, kz), mul_is(o2, ky)));
-    double2 a1 = cadd(C(1, i), cadd(mul_is(o0, kz), make_double2((o2m.x - o2p.x) / tdx, (o2m.y - o2p.y) / tdx)));
-    double2 a2 = cadd(C(2, i), csub(mul_cis(o0, ky), make_double2((o1m.x - o1p.x) / tdx, (o1m.y - o1p.y) / tdx)));
+    double2 a1 = cadd(C(1, i), cadd(mul_is(o0, kz), make_double2(qdiv(o2m.x - o2p.x, tdx, rtdx), qdiv(o2m.y - o2p.y, tdx, rtdx))));
+    double2 a2 = cadd(C(2, i), csub(mul_cis(o0, ky), make_double2(qdiv(o1m.x - o1p.x, tdx, rtdx), qdiv(o1m.y - o1p.y, tdx, rtdx))));
     lu2[t] = cadd(lu2[t], a0);
     lu2[SC + t] = cadd(lu2[SC + t], a1);
     lu2[2 * SC + t] = cadd(lu2[2 * SC + t], a2);
     const double2 gm = C(7, im), gp = C(7, ip);
-    double2 pp = cadd(C(6, i), make_double2((gm.x - gp.x) / tdx, (gm.y - gp.y) / tdx));
+    double2 pp = cadd(C(6, i), make_double2(qdiv(gm.x - gp.x, tdx, rtdx), qdiv(gm.y - gp.y, tdx, rtdx)));
     pp = cadd(pp, cadd(mul_cis(C(8, i), ky), mul_cis(C(9, i), kz)));
     lp2[t] = cadd(lp2[t], pp);
 }

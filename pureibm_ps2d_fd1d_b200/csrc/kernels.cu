@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
     const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
     const size_t roff = (size_t)rank * L::RL;
     const TwT tw{tws, N};
-    const double tdx = 2.0 * g.dx;
+    const double tdx = 2.0 * g.dx, rtdx = 1.0 / tdx;   // divisor and reciprocal for qdiv
     const double2 *U0 = u + (size_t)i * PS, *U1 = u + ((size_t)nx + i) * PS, *U2 = u + ((size_t)2 * nx + i) * PS;
     const double2 *Pp = p + (size_t)i * PS;
     const size_t slot = ((size_t)i * L::C + rank) * 12;
@@ -86,16 +86,16 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
                 } else if (t == 5) {   // wz*u1 - d(u3)/dx
                     const double2 a = U0[ge];
                     const double2 hp = u[((size_t)2 * nx + ip) * PS + ge], hm = u[((size_t)2 * nx + im) * PS + ge];
-                    const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
+                    const double2 d = make_double2(qdiv(hp.x - hm.x, tdx, rtdx), qdiv(hp.y - hm.y, tdx, rtdx));
                     f = make_double2(-kzv * a.y - d.x, kzv * a.x - d.y);
                 } else if (t == 6) {   // d(u2)/dx - wy*u1
                     const double2 a = U0[ge];
                     const double2 hp = u[((size_t)nx + ip) * PS + ge], hm = u[((size_t)nx + im) * PS + ge];
-                    const double2 d = make_double2((hp.x - hm.x) / tdx, (hp.y - hm.y) / tdx);
+                    const double2 d = make_double2(qdiv(hp.x - hm.x, tdx, rtdx), qdiv(hp.y - hm.y, tdx, rtdx));
                     f = make_double2(d.x - (-ky * a.y), d.y - ky * a.x);
                 } else if (t == 7) {
                     const double2 a = p[(size_t)ip * PS + ge], b = p[(size_t)im * PS + ge];
-                    f = make_double2((a.x - b.x) / tdx, (a.y - b.y) / tdx);
+                    f = make_double2(qdiv(a.x - b.x, tdx, rtdx), qdiv(a.y - b.y, tdx, rtdx));
                 } else if (t == 8) { const double2 a = Pp[ge]; f = make_double2(-a.y * ky, a.x * ky); }
                 else { const double2 a = Pp[ge]; f = make_double2(-a.y * kzv, a.x * kzv); }
             }
@@ -581,6 +581,7 @@ __global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict_
     if (p < sc->npts && !sc->status) {
         const int m = g.pt_m[p], l = g.pt_l[p], NB = g.nbody;
         const size_t CR = (size_t)g.nx * RP<N>::RSP;
+        const double rdx3 = 1.0 / g.dx3;   // reciprocal for qdiv
         double xli[3], xlo[3], xpi[3], snorm[3];
         inner_point(g, m, l, xli);
         double rad = 0.0;
@@ -645,7 +646,7 @@ __global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict_
                     const double w = si.w(a, b, c);
 #pragma unroll
                     for (int n = 0; n < 3; ++n) {
-                        const double t = (w * ft[n]) / g.dx3;
+                        const double t = qdiv(w * ft[n], g.dx3, rdx3);
                         if (fl) { force_fl[n] = force_fl[n] + t; ffl[n] += t; }
                         fm[n] += t;
                         ctb[((size_t)p * 8 + a + 2 * b + 4 * c) * 3 + n] = t;
