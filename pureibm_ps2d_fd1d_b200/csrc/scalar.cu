@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_sa(Geo g, const doubl
     const int i = p + 1;   // reference plane index
     const size_t roff = (size_t)rank * L::RL;
     const TwT tw{tws, N};
-    const double h = sc->heat_ratio, tdx = 2.0 * g.dx;
+    const double h = sc->heat_ratio, tdx = 2.0 * g.dx, rtdx = 1.0 / tdx;   // reciprocal for qdiv
 #pragma unroll 4
     for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
         const int kz = e / L::PZ, jl = e - kz * L::PZ;
@@ -89,13 +89,13 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_sa(Geo g, const doubl
         } else if (t == 2) {
             if (i == 1) {
                 const double2 pp = phi_at(g, phif, 2, ge, h), pm = phi_at(g, phif, nx, ge, h);
-                f = make_double2((pp.x - pm.x * h) / tdx, (pp.y - pm.y * h) / tdx);
+                f = make_double2(qdiv(pp.x - pm.x * h, tdx, rtdx), qdiv(pp.y - pm.y * h, tdx, rtdx));
             } else if (i == nx || i == nx + 1) {
                 const double2 q = phi_at(g, phif, i == nx ? 1 : 2, ge, h), pm = phi_at(g, phif, i - 1, ge, h);
-                f = make_double2((q.x / h - pm.x) / tdx, (q.y / h - pm.y) / tdx);
+                f = make_double2(qdiv(q.x / h - pm.x, tdx, rtdx), qdiv(q.y / h - pm.y, tdx, rtdx));
             } else {
                 const double2 pp = phi_at(g, phif, i + 1, ge, h), pm = phi_at(g, phif, i - 1, ge, h);
-                f = make_double2((pp.x - pm.x) / tdx, (pp.y - pm.y) / tdx);
+                f = make_double2(qdiv(pp.x - pm.x, tdx, rtdx), qdiv(pp.y - pm.y, tdx, rtdx));
             }
         } else {
             const double k = t == 3 ? g.ky[j] : g.kz[kz];
@@ -164,6 +164,7 @@ __global__ void __launch_bounds__(256) k_sflux(Geo g, const double *__restrict__
     if (sg >= nseg || (e % (N + 2)) >= N || sc->status) return;
     const int i0 = sg * SEG + 1, i1 = min(nx, (sg + 1) * SEG);
     const double h = sc->heat_ratio, dx = g.dx, hdx = dx / 2.0, tdx = 2.0 * dx;
+    const double rtdx = 1.0 / tdx, rdx = 1.0 / dx;   // reciprocals for qdiv
     auto U = [&](int i) { return __ldg(ubcp + (size_t)(i <= nx ? i - 1 : i - 1 - nx) * RSP + e); };   // i in 1..nx+2
     auto PB = [&](int i) { return i <= nx ? __ldg(phr + (size_t)(i - 1) * RSP + e) : __ldg(phimg + e); };  // i in 1..nx+1
     if (g.scheme == PIBM_SCHEME_CENTER) {
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(256) k_sflux(Geo g, const double *__restrict__
         double f0 = U(i0) * PB(i0);
         for (int i = i0; i <= i1; ++i) {
             const double fp = U(i + 1) * PB(i + 1);
-            dsx[(size_t)(i - 1) * RSP + e] = (fp - fm) / tdx;
+            dsx[(size_t)(i - 1) * RSP + e] = qdiv(fp - fm, tdx, rtdx);
             fm = f0;
             f0 = fp;
         }
@@ -179,9 +180,9 @@ __global__ void __launch_bounds__(256) k_sflux(Geo g, const double *__restrict__
     }
     // slopes of cell c (1..nx): (pfp phi(c+1) - pfm phi(c-1)) / 2dx, pfm = heat_ratio at c = 1
     auto slope_phi = [&](int c) {
-        return c == 1 ? (1.0 * PB(2) - h * PB(nx)) / tdx : (1.0 * PB(c + 1) - 1.0 * PB(c - 1)) / tdx;
+        return c == 1 ? qdiv(1.0 * PB(2) - h * PB(nx), tdx, rtdx) : qdiv(1.0 * PB(c + 1) - 1.0 * PB(c - 1), tdx, rtdx);
     };
-    auto slope_u = [&](int c) { return (U(c + 1) - U(c == 1 ? nx : c - 1)) / tdx; };
+    auto slope_u = [&](int c) { return qdiv(U(c + 1) - U(c == 1 ? nx : c - 1), tdx, rtdx); };
     auto flux = [](double up, double um, double Up, double Um) {
         const double ms = fmax(fabs(um), fabs(up));
         const double f = 0.5 * (up * Up) + 0.5 * (um * Um);
@@ -190,11 +191,11 @@ __global__ void __launch_bounds__(256) k_sflux(Geo g, const double *__restrict__
     // Rusanov flux at interface i (between cells i and i+1); 0 and nx are the periodic ends
     auto F = [&](int i) {
         if (i == 0) {
-            const double sp0 = (PB(1) - PB(nx - 1) * h) / tdx, su0 = (U(1) - U(nx - 1)) / tdx;
+            const double sp0 = qdiv(PB(1) - PB(nx - 1) * h, tdx, rtdx), su0 = qdiv(U(1) - U(nx - 1), tdx, rtdx);
             return flux(U(1) - slope_u(1) * hdx, U(nx) + su0 * hdx, PB(1) - slope_phi(1) * hdx, PB(nx) * h + sp0 * hdx);
         }
         if (i == nx) {
-            const double spm = (PB(2) / h - PB(nx)) / tdx, sum = (U(2) - U(nx)) / tdx;
+            const double spm = qdiv(PB(2) / h - PB(nx), tdx, rtdx), sum = qdiv(U(2) - U(nx), tdx, rtdx);
             return flux(U(1) - sum * hdx, U(nx) + slope_u(nx) * hdx, PB(1) / h - spm * hdx, PB(nx) + slope_phi(nx) * hdx);
         }
         return flux(U(i + 1) - slope_u(i + 1) * hdx, U(i) + slope_u(i) * hdx, PB(i + 1) - slope_phi(i + 1) * hdx,
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(256) k_sflux(Geo g, const double *__restrict__
     double Fm = F(i0 - 1);
     for (int i = i0; i <= i1; ++i) {
         const double Fi = F(i);
-        dsx[(size_t)(i - 1) * RSP + e] = (Fi - Fm) / dx;
+        dsx[(size_t)(i - 1) * RSP + e] = qdiv(Fi - Fm, dx, rdx);
         Fm = Fi;
     }
 }
@@ -574,8 +575,8 @@ __device__ __forceinline__ void twisted_solve(double2 *row, double a, double b, 
         const int m = r + R * br;
         const double2 e = tw.t[m * tw.stride];   // (cos, -sin)
         const double lr = (double)N * (b + a * mpl * e.x), li = (double)N * (a * mmi * (-e.y));
-        const double den = lr * lr + li * li;
-        v[r] = make_double2((v[r].x * lr + v[r].y * li) / den, (v[r].y * lr - v[r].x * li) / den);
+        const double den = lr * lr + li * li, rden = 1.0 / den;
+        v[r] = make_double2(qdiv(v[r].x * lr + v[r].y * li, den, rden), qdiv(v[r].y * lr - v[r].x * li, den, rden));
     }
 #pragma unroll
     for (int h = 1; h < 32; h <<= 1) {
@@ -624,7 +625,7 @@ __global__ void __launch_bounds__(LT * 32) k_slines(Geo g, double2 *__restrict__
     const double mu = exp(-log(H) / (double)NX), imu = 1.0 / mu;
     const int q0 = blockIdx.x * LT;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const double dt = sc->dt, gm = g.gamma_s, dx2 = g.dx2;
+    const double dt = sc->dt, gm = g.gamma_s, dx2 = g.dx2, rdx2 = 1.0 / dx2;
     const double c1 = g.c1, c2 = g.c2, c3 = g.c3, c4 = g.c4;
     auto PF = [&](int i, int q) -> double2 {   // 1-based plane, nx+1 = phif(1)/heat_ratio_new of the last step
         if (i <= nx) return phif[(size_t)(i - 1) * PS + q];
@@ -650,7 +651,7 @@ __global__ void __launch_bounds__(LT * 32) k_slines(Geo g, double2 *__restrict__
             const double2 pp = PF(2, q), pm = PF(nx, q);
             lap = make_double2((pp.x - 2.0 * pc.x) + pm.x * h, (pp.y - 2.0 * pc.y) + pm.y * h);
         }
-        RHS[line * NP + (i - 1)] = make_double2(r.x + (k1 * lap.x) / dx2, r.y + (k1 * lap.y) / dx2);
+        RHS[line * NP + (i - 1)] = make_double2(r.x + qdiv(k1 * lap.x, dx2, rdx2), r.y + qdiv(k1 * lap.y, dx2, rdx2));
     }
     __syncthreads();
     const int qw = q0 + w;
