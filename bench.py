@@ -34,16 +34,13 @@ PEAK_FALLBACK_GBS = 6650.0
 
 # Algorithmic bytes per launch of each plane/line kernel, in units of one
 # complex spectral field F_c = nx*my2*mz*16 B and one real field F_r = nx*my*mz*8 B:
-# compulsory reads + writes of whole fields.
+# compulsory reads + writes of whole fields by that kernel alone.
 KERNEL_BYTES = {
-    "a0_fields_to_real": (4, 10),  # read u(3), p; write ubcp(3), pbcp, omega(3), grad p(3)
-    "nonlinear": (9, 6),           # read ubcp(3), u(3), onl(3); write nl(3), Q(3)
-    "forcing_fft": (3, 3),         # read fr(3); write ff(3)
-    "x_lines": (17, 0),            # read u(3), p, nl(3), onl(3), ff(3); write u(3), p
-}
-KERNEL_NAMES = {
-    "a0_fields_to_real": "k_a0", "nonlinear": "k_nl", "drag_mpg": "k_drag",
-    "reversal_spread": "k_rev", "forcing_fft": "k_ff", "x_lines": "k_lines",
+    "k_a0": (4, 10),     # read u(3), p; write ubcp(3), pbcp, omega(3), grad p(3)
+    "k_flux": (0, 6),    # read ubcp(3); write the x-flux differences Dx(3)
+    "k_nl": (9, 9),      # read ubcp(3), Dx(3), u(3), onl(3); write nl(3), Q(3)
+    "k_ff": (3, 3),      # read fr(3); write ff(3)
+    "k_lines": (17, 0),  # read u(3), p, nl(3), onl(3), ff(3); write u(3), p
 }
 
 
@@ -85,6 +82,19 @@ def _config_dict(n_gpus, xc, prm):
         "l2": "working set ~0.45 GB per replica > 126 MB L2 (no flush needed)",
         "seed": WORKLOAD["seed"],
     }
+
+
+def _smi_id(torch, dev: int) -> str:
+    """nvidia-smi -i identifier of torch device `dev` (its UUID, which does not
+    depend on CUDA_VISIBLE_DEVICES); the physical index when no UUID is known."""
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        if u:
+            return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        pass
+    vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+    return vis[dev].strip() if dev < len(vis) else str(dev)
 
 
 class ClockSampler:
@@ -414,15 +424,17 @@ def run_gpu(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
     import numpy as np
     import torch
+    # one GPU per rank: LOCAL_RANK indexes the devices this job was given (any
+    # CUDA_VISIBLE_DEVICES subset the launcher set is kept); the engine
+    # creates its handle on the current device of this thread
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
     dist = None
     if world > 1:
         import torch.distributed as dist
         import datetime
-        torch.cuda.set_device(0)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import pureibm_ps2d_fd1d_b200 as pk
     from pureibm_ps2d_fd1d_b200 import config, abi
@@ -445,7 +457,7 @@ def run_gpu(args):
     phases = (C.c_double * abi.PIBM_NPHASE)()
     barrier()
     # the timed region: the production path (one CUDA graph per step, drag/mpg on a side stream)
-    with ClockSampler(local if world > 1 else 0) as clk:
+    with ClockSampler(_smi_id(torch, dev)) as clk:
         rc = lib.pibm_run_timed(s.h, args.steps, C.byref(rep), C.byref(total))
     barrier()
     if rc != 0:
@@ -458,6 +470,14 @@ def run_gpu(args):
         raise RuntimeError("pibm_run_profiled failed: %d %s" % (rc, lib.pibm_last_error().decode()))
     value = aggregate_mcells(ncell, args.steps, world, t_ms)
     phase_ms = {abi.PHASE_NAMES[q]: phases[q] / args.steps for q in range(abi.PIBM_NPHASE)}
+    # per-kernel breakdown: the same launches, serial, a CUDA event pair on the
+    # engine's stream around every kernel (pibm_kernel_times)
+    kms = (C.c_double * abi.PIBM_NKERNEL)()
+    ktotal = C.c_double()
+    rc = lib.pibm_kernel_times(s.h, args.steps, C.byref(ktotal), kms, abi.PIBM_NKERNEL)
+    if rc != 0:
+        raise RuntimeError("pibm_kernel_times failed: %d %s" % (rc, lib.pibm_last_error().decode()))
+    kernel_ms = {abi.KERNEL_NAMES[k]: kms[k] / args.steps for k in range(abi.PIBM_NKERNEL)}
 
     # end-to-end through the C ABI with host buffers: every step uploads the
     # state (u, nl, p in the reference layout) from pinned memory, steps, and
@@ -502,19 +522,25 @@ def run_gpu(args):
     peak, peak_kind = _peak_gbs()
     Fc = nx * my2 * mz * 16
     Fr = nx * s.my * mz * 8
-    dominant = max(KERNEL_BYTES, key=lambda k: phase_ms[k])
-    nc, nr = KERNEL_BYTES[dominant]
-    alg = nc * Fc + nr * Fr
-    achieved = alg / (phase_ms[dominant] / 1e3) / 1e9
-    traffic = None
+    traffic_tab = {}
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as fh:
-            tr = json.load(fh)
-        ent = tr.get(KERNEL_NAMES[dominant])
-        if ent:
-            traffic = float(ent["bytes_per_launch_at_128"])
+            traffic_tab = json.load(fh)
     except Exception:
         pass
+
+    def kernel_roof(name):
+        nc, nr = KERNEL_BYTES[name]
+        alg = nc * Fc + nr * Fr
+        ach = alg / (kernel_ms[name] / 1e3) / 1e9
+        ent = traffic_tab.get(name) if isinstance(traffic_tab.get(name), dict) else None
+        return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": ach / peak, "ms_per_launch": kernel_ms[name],
+                "algorithmic_bytes_per_launch": alg,
+                "traffic": float(ent["bytes_per_launch_at_128"]) if ent else None}
+
+    kernel_roofline = {k: kernel_roof(k) for k in KERNEL_BYTES}
+    dominant = max(KERNEL_BYTES, key=lambda k: kernel_ms[k])
     b_alg_step = 30 * Fc
     info = s.info
     # FP64 arithmetic: the reference's transform count (31 plane FFTs per
@@ -540,13 +566,13 @@ def run_gpu(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded sphere positions, fluid initially at rest)",
         "config": _config_dict(world, xc, prm),
-        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dominant], "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": alg},
+        "roofline": kernel_roofline[dominant],
+        "kernel_roofline": kernel_roofline,
         "step_roofline": {"algorithmic_bytes_per_step": b_alg_step,
                           "achieved_GBps": b_alg_step / (t_ms / args.steps / 1e3) / 1e9,
                           "frac": b_alg_step / (t_ms / args.steps / 1e3) / 1e9 / peak},
         "phase_ms_per_step": phase_ms,
+        "kernel_ms_per_step": kernel_ms,
         "e2e": {"value": ncell * e2e_steps * world / e2e_s / 1e6, "unit": UNIT,
                 "h2d_bytes_per_step": bytes_state, "d2h_bytes_per_step": bytes_state + C.sizeof(rep),
                 "path": "pibm_set_state(pinned host) + pibm_step + pibm_get_state(pinned host) per step"},

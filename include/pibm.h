@@ -162,6 +162,33 @@ int  pibm_run_timed(pibm_handle *h, int nsteps, pibm_step_report *last, double *
 #define PIBM_NPHASE 7   /* 0 u,p,omega,grad p -> real  1 nonlinear + IBM field  2 drag+mpg  3 reversal+spread  4 forcing FFT  5 x-lines  6 passive scalar */
 int  pibm_run_profiled(pibm_handle *h, int nsteps, pibm_step_report *last,
                        double *total_ms, double *phase_ms, int nphase);
+/* Kernel slots of one flow step, in launch order (the same launches as the
+ * step graphs, run serially on the handle's stream).  Slots a step does not
+ * launch (no spheres, no active reversal points) time as zero.  With moving
+ * particles the DEM and geometry-rebuild kernels are not in any slot (the
+ * spreading rebuild is in PIBM_K_SPREAD); with the passive scalar its
+ * kernels run after PIBM_K_SCAL_D, outside every slot. */
+#define PIBM_K_A0      0   /* fields to real space          compute_new_timestep, calc_pressure, compute_omega, calc_pgrad */
+#define PIBM_K_SCAL_A  1   /* CFL dt, t, cf, means          compute_new_timestep tail                                    */
+#define PIBM_K_FLUX    2   /* x-flux differences            form_nl                                                     */
+#define PIBM_K_NL      3   /* nonlinear term + IBM field Q  nonlinear, calc_visc                                        */
+#define PIBM_K_DRAG    4   /* surface quadrature            calc_pres_visc_drag                                         */
+#define PIBM_K_SCAL_B  5   /* drag totals, mpg, force       compute_mpg_at_n                                            */
+#define PIBM_K_REV     6   /* reversal-point forcing        calc_inner_reversal_forcing                                 */
+#define PIBM_K_SCAL_C  7   /* frmean                        bcset                                                       */
+#define PIBM_K_SPREAD  8   /* spreading onto solid nodes    calc_inner_reversal_forcing (spread loop)                   */
+#define PIBM_K_FF      9   /* forcing r2c                   bcset                                                       */
+#define PIBM_K_LINES  10   /* x-line solves                 velstep: pressure, ustep, divcorr                           */
+#define PIBM_K_SCAL_D 11   /* umean update, status          velstep                                                     */
+#define PIBM_NKERNEL  12
+/* nsteps steps launched serially with a CUDA event pair around every kernel
+ * slot: kernel_ms[k] (k < nkernel <= PIBM_NKERNEL) = summed device time of
+ * slot k over the steps, *total_ms = first slot start to last slot end.  No
+ * counterpart in the reference (its per-phase CPU timers print wall time,
+ * dtibm_main_scal_flo.F90:552-566). */
+int  pibm_kernel_times(pibm_handle *h, int nsteps, double *total_ms, double *kernel_ms, int nkernel);
+/* Name of kernel slot k ("k_a0", ...), NULL outside [0, PIBM_NKERNEL). */
+const char *pibm_kernel_name(int k);
 int  pibm_get_state(pibm_handle *h, pibm_state_view *s);
 /* pres, visc, force: (nbody,3) column-major, as global_data.F90:115-117;
  * xc, vel: positions (grid units) and velocities.  Any pointer may be NULL. */
@@ -221,9 +248,12 @@ int  pibm_ff2cr(int my, int mz, int nplanes, const double *a, double *b);
  * size, my = mz in {32, 64, 96, 128}; larger or other sizes are rejected with
  * PIBM_ERR_ARG.  Set-up: the FIRST call on each device looks up that array's
  * address, writes the whole table with a blocking copy and waits for it, so
- * make that first call before starting any stream capture.  After it the
- * table is only read, so nothing in it must start at zero and calls on
- * different streams share it safely.
+ * make that first call before starting any stream capture.  A device reset
+ * (cudaDeviceReset) gives the device a new context whose copy of the array
+ * starts zeroed; the first call after it writes the table again (the cached
+ * set-up is keyed on the context's unique id).  After the set-up the table is
+ * only read, so nothing in it must start at zero and calls on different
+ * streams share it safely.
  * d_a: nplanes * mz * (my/2+1) complex (interleaved doubles); d_b: nplanes *
  * mz * my doubles; both device pointers with the layout of pibm_ff2cr.  The
  * transform is enqueued on `stream` (a cudaStream_t; NULL = legacy default

@@ -36,6 +36,10 @@ PIBM_LIMITER_NONE = 0
 PIBM_LIMITER_MINMOD = 1
 PIBM_NPHASE = 7
 PHASE_NAMES = ["a0_fields_to_real", "nonlinear", "drag_mpg", "reversal_spread", "forcing_fft", "x_lines", "scalar"]
+# kernel slots of pibm_kernel_times (PIBM_K_*), in launch order
+PIBM_NKERNEL = 12
+KERNEL_NAMES = ["k_a0", "k_scal_a", "k_flux", "k_nl", "k_drag", "k_scal_b", "k_rev", "k_scal_c", "k_spread",
+                "k_ff", "k_lines", "k_scal_d"]
 
 _i32 = C.c_int32
 _f64 = C.c_double
@@ -110,7 +114,7 @@ class pibm_adjoint_report(C.Structure):
 # Exported symbols of libpibm (declared in include/pibm.h).
 EXPORTED = [
     "pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed",
-    "pibm_run_profiled", "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev",
+    "pibm_run_profiled", "pibm_kernel_times", "pibm_kernel_name", "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev",
     "pibm_get_fluid_mask", "pibm_get_contacts", "pibm_get_scalar_nl", "pibm_set_scalar",
     "pibm_set_desired_means", "pibm_adjoint_run", "pibm_adjoint_begin", "pibm_adjoint_step", "pibm_adjoint_end", "pibm_fp64_peak", "pibm_qdiv_check", "pibm_get_tuning", "pibm_set_tuning", "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
     "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time", "pibm_batch_member",
@@ -130,6 +134,9 @@ def bind(lib):
     lib.pibm_get_state.argtypes = [vp, P(pibm_state_view)]
     lib.pibm_run_timed.argtypes = [vp, C.c_int, P(pibm_step_report), P(_f64)]
     lib.pibm_run_profiled.argtypes = [vp, C.c_int, P(pibm_step_report), P(_f64), P(_f64), C.c_int]
+    lib.pibm_kernel_times.argtypes = [vp, C.c_int, P(_f64), P(_f64), C.c_int]
+    lib.pibm_kernel_name.argtypes = [C.c_int]
+    lib.pibm_kernel_name.restype = C.c_char_p
     lib.pibm_get_particles.argtypes = [vp] + [P(_f64)] * 5
     lib.pibm_get_scalar.argtypes = [vp, P(_f64), P(_f64), P(_f64)]
     lib.pibm_get_if_rev.argtypes = [vp, P(C.c_uint8)]
@@ -161,7 +168,7 @@ def bind(lib):
     lib.pibm_batch_destroy.argtypes = [vp]
     lib.pibm_batch_destroy.restype = None
     for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed", "pibm_run_profiled",
-                 "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev", "pibm_get_fluid_mask",
+                 "pibm_kernel_times", "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev", "pibm_get_fluid_mask",
                  "pibm_get_contacts", "pibm_get_scalar_nl", "pibm_set_scalar", "pibm_set_desired_means",
                  "pibm_adjoint_run", "pibm_adjoint_begin", "pibm_adjoint_step", "pibm_adjoint_end", "pibm_fp64_peak", "pibm_qdiv_check", "pibm_get_tuning", "pibm_set_tuning", "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
         getattr(lib, name).restype = C.c_int

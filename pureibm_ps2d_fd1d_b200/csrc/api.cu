@@ -22,7 +22,8 @@
 namespace pibm {
 cudaError_t configure_kernels(int n);
 bool supported_size(int n);
-void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss);
+void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss,
+                  cudaEvent_t *kev = nullptr);
 int kernels_per_step(const Geo &g, const Mov &m);
 void enqueue_dem_init(const Mov &m, Scal *sc, cudaStream_t s);
 cudaError_t configure_moving_kernels(const Mov &m);
@@ -480,6 +481,42 @@ int pibm_run_profiled(pibm_handle *h, int nsteps, pibm_step_report *last, double
     }
     for (auto &e : ev) cudaEventDestroy(e);
     return fill_report(h, last);
+}
+
+int pibm_kernel_times(pibm_handle *h, int nsteps, double *total_ms, double *kernel_ms, int nkernel) {
+    if (!h || nsteps <= 0 || nkernel < 0 || nkernel > PIBM_NKERNEL || (nkernel > 0 && !kernel_ms))
+        return fail(PIBM_ERR_ARG, "bad argument");
+    if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "pibm_kernel_times starts at a step boundary");
+    const int nst = nsteps * h->itrmax;
+    const size_t per = 2 * (size_t)PIBM_NKERNEL;
+    std::vector<cudaEvent_t> ev((size_t)nst * per);
+    for (auto &e : ev) CUDA_OR_FAIL(cudaEventCreate(&e));
+    for (int s = 0; s < nst; ++s) {
+        enqueue_step(h->gs[s % h->itrmax], h->b, h->cur, h->stream, nullptr, nullptr, &ev[(size_t)s * per]);
+        h->cur ^= 1;
+    }
+    CUDA_OR_FAIL(cudaGetLastError());
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < nkernel; ++k) kernel_ms[k] = 0.0;
+    for (int s = 0; s < nst; ++s)
+        for (int k = 0; k < nkernel; ++k) {
+            float ms = 0.f;
+            CUDA_OR_FAIL(cudaEventElapsedTime(&ms, ev[(size_t)s * per + 2 * k], ev[(size_t)s * per + 2 * k + 1]));
+            kernel_ms[k] += ms;
+        }
+    if (total_ms) {
+        float ms = 0.f;
+        CUDA_OR_FAIL(cudaEventElapsedTime(&ms, ev.front(), ev[(size_t)(nst - 1) * per + 2 * PIBM_K_SCAL_D + 1]));
+        *total_ms = ms;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return fill_report(h, nullptr);
+}
+
+const char *pibm_kernel_name(int k) {
+    static const char *names[PIBM_NKERNEL] = {"k_a0", "k_scal_a", "k_flux", "k_nl", "k_drag", "k_scal_b",
+                                              "k_rev", "k_scal_c", "k_spread", "k_ff", "k_lines", "k_scal_d"};
+    return (k >= 0 && k < PIBM_NKERNEL) ? names[k] : nullptr;
 }
 
 int pibm_get_state(pibm_handle *h, pibm_state_view *s) {
@@ -1084,7 +1121,7 @@ int pibm_ff2cr(int my, int mz, int nplanes, const double *a, double *b) { return
 }  // extern "C"
 
 // ---- allocation-free ff2cr: twiddles for every supported size live in one
-// static device array, written once per device by the first call ----
+// static device array, written once per device context by the first call ----
 namespace {
 constexpr int kNoAllocSizes[4] = {32, 64, 96, 128};
 constexpr int kNoAllocMaxN = 128;
@@ -1093,6 +1130,10 @@ static __device__ __align__(256) double2 g_noalloc_twiddles[kNoAllocEntries];
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 double2 *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+// unique id of the context whose copy of g_noalloc_twiddles was filled (a
+// device reset destroys the context, and the next one starts with a zeroed
+// array under a new id, so the table is written again)
+unsigned long long g_noalloc_ctx[kNoAllocMaxDevices] = {};
 
 // Offset of the size-n table inside g_noalloc_twiddles, or -1.
 int noalloc_offset(int n) {
@@ -1102,6 +1143,30 @@ int noalloc_offset(int n) {
         off += s;
     }
     return -1;
+}
+
+// Unique id of the current thread's CUDA context (driver cuCtxGetId through
+// the runtime's entry-point table; no link-time dependency on libcuda).
+cudaError_t current_context_id(unsigned long long *id) {
+    typedef int (*get_cur_t)(void **);
+    typedef int (*get_id_t)(void *, unsigned long long *);
+    static get_cur_t get_cur = nullptr;
+    static get_id_t get_id = nullptr;
+    if (!get_cur || !get_id) {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa);
+        if (e != cudaSuccess) return e;
+        e = cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb);
+        if (e != cudaSuccess) return e;
+        if (qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b) return cudaErrorNotSupported;
+        get_cur = (get_cur_t)a;
+        get_id = (get_id_t)b;
+    }
+    void *ctx = nullptr;
+    if (get_cur(&ctx) != 0 || !ctx) return cudaErrorDeviceUninitialized;
+    if (get_id(ctx, id) != 0) return cudaErrorDeviceUninitialized;
+    return cudaSuccess;
 }
 }  // namespace
 
@@ -1120,10 +1185,14 @@ int pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *d
     double2 *table = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_ptr[dev]) {
-            // first call on this device (it is current): resolve the array, fill every size, wait
-            void *p = nullptr;
-            CUDA_OR_FAIL(cudaGetSymbolAddress(&p, g_noalloc_twiddles));
+        // the array's device address in the current context (this call also
+        // brings the device's context up if nothing has yet)
+        void *p = nullptr;
+        CUDA_OR_FAIL(cudaGetSymbolAddress(&p, g_noalloc_twiddles));
+        unsigned long long ctx = 0;
+        CUDA_OR_FAIL(current_context_id(&ctx));
+        if (!g_noalloc_ptr[dev] || g_noalloc_ctx[dev] != ctx) {
+            // first call in this device context (it is current): fill every size, wait
             std::vector<double2> host;
             host.reserve(kNoAllocEntries);
             for (int s : kNoAllocSizes) {
@@ -1133,6 +1202,7 @@ int pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *d
             CUDA_OR_FAIL(cudaMemcpy(p, host.data(), host.size() * sizeof(double2), cudaMemcpyHostToDevice));
             CUDA_OR_FAIL(cudaDeviceSynchronize());
             g_noalloc_ptr[dev] = (double2 *)p;
+            g_noalloc_ctx[dev] = ctx;
         }
         table = g_noalloc_ptr[dev];
     }

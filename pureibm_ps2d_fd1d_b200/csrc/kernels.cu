@@ -1179,16 +1179,28 @@ int real_offset(int n, int z, int y) {
 
 // Enqueue one full step on stream s.  cur = index of the nl buffer that
 // receives this step's nonlinear term (the other holds the previous step's).
+// ev (phase events, PIBM_NPHASE + 1) or kev (kernel events, 2 per kernel
+// slot PIBM_K_*: before and after the slot's launch) select the serial,
+// timed variant on one stream; without either, drag + mpg and the scalar
+// step fork onto the side streams of ss.
 template <int N>
-static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss) {
+static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss,
+                           cudaEvent_t *kev) {
     const int old = 1 - cur;
     auto mark = [&](int q) { if (ev) cudaEventRecord(ev[q], s); };
+    auto kb = [&](int k) { if (kev) cudaEventRecord(kev[2 * k], s); };
+    auto ke = [&](int k) { if (kev) cudaEventRecord(kev[2 * k + 1], s); };
+    auto kskip = [&](int k) { kb(k); ke(k); };
     // forked: drag + mpg on ss->side and the scalar step on ss->scal run beside the
-    // nonlinear term; the per-phase timed variant (ev) keeps one serial stream
-    const bool fork = ss && !ev;
+    // nonlinear term; the timed variants keep one serial stream
+    const bool fork = ss && !ev && !kev;
     mark(0);
+    kb(PIBM_K_A0);
     launch_planes<N>(k_a0<N>, g.nx, 10, s, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
+    ke(PIBM_K_A0);
+    kb(PIBM_K_SCAL_A);
     k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
+    ke(PIBM_K_SCAL_A);
     mark(1);
     if (fork) {
         cudaEventRecord(ss->fork, s);
@@ -1204,16 +1216,24 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
             cudaEventRecord(ss->scal_done, ss->scal);
         }
     }
+    kb(PIBM_K_FLUX);
     k_flux<N><<<(RP<N>::RSP * (g.nx / 32) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
+    ke(PIBM_K_FLUX);
+    kb(PIBM_K_NL);
     launch_planes<N>(k_nl<N>, g.nx, 3, s, g, (const double *)b.ubcp, (const double *)b.Dx, (const double2 *)b.u,
                      (const double2 *)b.nl[old], b.nl[cur], b.Q, b.sc);
+    ke(PIBM_K_NL);
     mark(2);
     if (g.nbody > 0) {
         if (fork) {
             cudaStreamWaitEvent(s, ss->drag_done, 0);
         } else {
+            kb(PIBM_K_DRAG);
             k_drag<N><<<g.nbody * kDragSplit, 256, 0, s>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
+            ke(PIBM_K_DRAG);
+            kb(PIBM_K_SCAL_B);
             k_scal_b<<<1, 256, 0, s>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
+            ke(PIBM_K_SCAL_B);
         }
         if (g.moving) {
             enqueue_moving(g, b.mov, b.sc, b.pres, b.visc, s);
@@ -1227,19 +1247,35 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
         mark(3);
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {
+            kb(PIBM_K_REV);
             k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.ctb, b.blockpart);
+            ke(PIBM_K_REV);
+            kb(PIBM_K_SCAL_C);
             k_scal_c<<<1, 256, 0, s>>>(g, b.sc, b.blockpart, nbk);
+            ke(PIBM_K_SCAL_C);
+            kb(PIBM_K_SPREAD);
             if (g.moving) enqueue_spread_dyn(g, b.mov, b.rec, b.ctb, b.fr, b.sc, s);
             else if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.ctb, b.fr, b.sc);
+            ke(PIBM_K_SPREAD);
+        } else {
+            kskip(PIBM_K_REV); kskip(PIBM_K_SCAL_C); kskip(PIBM_K_SPREAD);
         }
         mark(4);
+        kb(PIBM_K_FF);
         launch_planes<N>(k_ff<N>, g.nx, 3, s, g, (const double *)b.fr, b.ff, b.sc);
+        ke(PIBM_K_FF);
     } else {
         mark(3); mark(4);
+        kskip(PIBM_K_DRAG); kskip(PIBM_K_SCAL_B); kskip(PIBM_K_REV); kskip(PIBM_K_SCAL_C); kskip(PIBM_K_SPREAD);
+        kskip(PIBM_K_FF);
     }
     mark(5);
+    kb(PIBM_K_LINES);
     launch_lines<N>(g, b, b.u, b.p, cur, b.sc, s);
+    ke(PIBM_K_LINES);
+    kb(PIBM_K_SCAL_D);
     k_scal_d<<<1, 32, 0, s>>>(g, b.sc);
+    ke(PIBM_K_SCAL_D);
     mark(6);
     if (g.scal) {
         if (fork) cudaStreamWaitEvent(s, ss->scal_done, 0);
@@ -1256,13 +1292,14 @@ int kernels_per_step(const Geo &g, const Mov &m) {
     return n + scalar_kernels_per_step(g);
 }
 
-void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss) {
+void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss,
+                  cudaEvent_t *kev) {
     switch (g.my) {
-        case 32: enqueue_step_t<32>(g, b, cur, s, ev, ss); break;
-        case 64: enqueue_step_t<64>(g, b, cur, s, ev, ss); break;
-        case 96: enqueue_step_t<96>(g, b, cur, s, ev, ss); break;
-        case 128: enqueue_step_t<128>(g, b, cur, s, ev, ss); break;
-        case 256: enqueue_step_t<256>(g, b, cur, s, ev, ss); break;
+        case 32: enqueue_step_t<32>(g, b, cur, s, ev, ss, kev); break;
+        case 64: enqueue_step_t<64>(g, b, cur, s, ev, ss, kev); break;
+        case 96: enqueue_step_t<96>(g, b, cur, s, ev, ss, kev); break;
+        case 128: enqueue_step_t<128>(g, b, cur, s, ev, ss, kev); break;
+        case 256: enqueue_step_t<256>(g, b, cur, s, ev, ss, kev); break;
     }
 }
 

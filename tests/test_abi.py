@@ -33,3 +33,12 @@ def test_library_exports_every_header_symbol():
                                        (3, abi.pibm_step_report), (4, abi.pibm_info)])
 def test_struct_sizes_match_header(which, cls):
     assert oc.lib().orc_sizeof(which) == C.sizeof(cls)
+
+
+def test_kernel_slot_names_match_header():
+    lib = abi.bind(C.CDLL(LIB_PATH))
+    names = [lib.pibm_kernel_name(k).decode() for k in range(abi.PIBM_NKERNEL)]
+    assert names == abi.KERNEL_NAMES
+    assert lib.pibm_kernel_name(abi.PIBM_NKERNEL) is None
+    text = open(os.path.join(ROOT, "include", "pibm.h")).read()
+    assert int(re.search(r"#define PIBM_NKERNEL\s+(\d+)", text).group(1)) == abi.PIBM_NKERNEL
