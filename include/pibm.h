@@ -51,7 +51,9 @@ extern "C" {
  * PART_PROPT, FLAGS; defaults in SRC/FLO/initialize.F90:73-271).
  * Grid: mx = my+1, nx = mx-1 = my, my2 = my/2+1 (initialize.F90:340-352);
  * mz = my unless given.  Only the serial x-periodic path is supported
- * (PARALLEL=0, XPERIODIC=T, NLCONS=T, AliasFlag=0), AB2 or RK3.
+ * (PARALLEL=0, XPERIODIC=T, NLCONS=T, AliasFlag=0, DOBND=F), AB2 or RK3;
+ * pibm_create returns PIBM_ERR_ARG for the others (fields dobnd, aliasflag,
+ * nlcons_false below).
  */
 typedef struct pibm_params {
     int32_t my;              /* MY (even)                                      */
@@ -86,7 +88,14 @@ typedef struct pibm_params {
     double  phisurf;         /* PHISURF                                        */
     double  phistream;       /* PHISTREAM                                      */
     int32_t rk3;             /* RK3: 3-stage Runge-Kutta (coef, itrmax = 3, initialize_flo.F90:861-877); 0 = AB2/CN */
-    int32_t reserved[7];
+    /* Flags of the reference that select code this engine does not run.  They
+     * are part of the struct so that a host copies its namelist values in and
+     * the engine refuses the run (PIBM_ERR_ARG) instead of silently running
+     * another algorithm; 0 is the only accepted value of each. */
+    int32_t dobnd;           /* DOBND (1 = T): surface-point forcing calc_bnd_forcing, boundary_condition.F90:615,902-1102 */
+    int32_t aliasflag;       /* ALIASFLAG (1 = 2/3 dealiasing of the nonlinear term, nl.F90:146)                         */
+    int32_t nlcons_false;    /* 1 when NLCONS = F (non-conservative pressure gradient, boundary_condition.F90:1831-1880) */
+    int32_t reserved[4];
 } pibm_params;
 
 /* Particle list (the reference's sphr_center.inp after scaling by DBYDX:

@@ -58,7 +58,7 @@ class pibm_params(C.Structure):
         ("dorpr", _i32), ("revernorm", _i32), ("include_frmeanfluid", _i32),
         ("imove", _i32), ("collision_softsphere", _i32), ("iscalon", _i32),
         ("pr_or_sc_nu", _f64), ("phisurf", _f64), ("phistream", _f64),
-        ("rk3", _i32), ("reserved", _i32 * 7),
+        ("rk3", _i32), ("dobnd", _i32), ("aliasflag", _i32), ("nlcons_false", _i32), ("reserved", _i32 * 4),
     ]
 
 

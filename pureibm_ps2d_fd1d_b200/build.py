@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libpibm.so")
+MAIN = os.path.join(OUT_DIR, "pibm_main")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels.cu", "scalar.cu", "moving.cu", "adjoint.cu", "peak.cu", "api.cu"]
 # per-source nvcc flags: the DEM and the moving-geometry rebuild are compiled
@@ -43,6 +44,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     nvcc = _nvcc()
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "pibm.h")]
     if not force and not _stale(LIB, deps):
+        build_main()
         return LIB
     objs = []
     for src in CU_SOURCES:
@@ -60,7 +62,20 @@ def build(verbose: bool = False, force: bool = False) -> str:
     tmp = LIB + ".tmp"
     subprocess.run([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)
+    build_main(force=True)
     return LIB
+
+
+def build_main(force: bool = False) -> str:
+    """The C host driver (csrc/pibm_main.c): gcc against include/pibm.h,
+    linked to libpibm.so found next to it at run time."""
+    src = os.path.join(CSRC, "pibm_main.c")
+    if not force and not _stale(MAIN, [src, LIB, os.path.join(HERE, "..", "include", "pibm.h")]):
+        return MAIN
+    subprocess.run(["gcc", "-O2", "-std=gnu99", "-Wall", "-ffp-contract=off", "-o", MAIN + ".tmp", src,
+                    "-L" + OUT_DIR, "-lpibm", "-Wl,-rpath,$ORIGIN", "-lm"], check=True)
+    os.replace(MAIN + ".tmp", MAIN)
+    return MAIN
 
 
 if __name__ == "__main__":

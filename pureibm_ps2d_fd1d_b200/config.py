@@ -4,7 +4,8 @@
   for the keys the step uses.
 * ``read_floparam`` reads a ``RUN_NAME_floparam.in`` (Fortran namelists
   FLOANDGRID, PART_PROPT, FLAGS, ... read in ``read_nmls``,
-  initialize.F90:274-359) into the same dictionary.
+  initialize.F90:274-359) into the same dictionary, with the reference's
+  group order and variable lists enforced.
 * ``read_sphr_center`` reads ``RUN_NAME_sphr_center.inp`` like the
   ``input_type='default'`` branch (initialize_flo.F90:1485-1590): line 1 is
   skipped, columns are x y z r in diameters, positions are scaled by DBYDX and
@@ -74,21 +75,114 @@ def _parse_value(tok: str):
     return vals[0] if len(vals) == 1 else tuple(vals)
 
 
-def read_floparam(path: str) -> Dict:
-    """Parse the namelist groups of a floparam.in into a parameter dict.
+# Namelist groups and their variables as the reference declares them
+# (SRC/FLO/global_data.F90:300-336, SRC/SCALAR/scalar_data.F90:89-91).
+NAMELISTS = {
+    "floandgrid": ("mx mxf my mz tstart ramp_frac_steps tend nerr_steps wtime_maxhrs saveforres_time tol_ferror vis "
+                   "re rhof cpf kf archno cfl cfl_max vfl foffset mbuffer mpg ret flo_ang tol_gran_error"),
+    "part_propt": ("nbody dr f1 f2 tstartmove lybyd dbydx dia_phys rhos cps ks input_type discr_scheme limiter "
+                   "vol_frac1 min_part_sep nphases collision_type vel_distrib nl_slope_factor"),
+    "flags": ("aliasflag maxzeroflag revernorm imove iscalon irestart iscal_restart saveforrestart saveforres_time "
+              "xperiodic adaptive set_umean set_mpg nlcons rk3 mean_vel_to_particles dorpr dobnd include_frmeanfluid "
+              "impose_grav debug_check cage_simul fixed_moving gof_avg only_dem movingcv iturbon moving_from_fixed_bed "
+              "from_post change_frame use_drag_law initialize_zero"),
+    "files": "outputfile rstsave outformat saveitns minunitno maxunitno errfile rstread write_output write_snapshot",
+    "psd": "psd_type nphases sigmabydavg phiavg equal_momentum",
+    "gcg": "coeff_rest pvel_var min_colisions mis_hs",
+    "bidisperse": "volfrac_rat red1 dia_ratio yalpha",
+    "lubtest": "hbyd",
+    "matinput": "hhat mis_mat ibordel matern_treshold",
+    "riser": "volume_fraction widthbyd aspect_ratio",
+    "scal_propt": "nspmx phistream setphimean phisurf sourcepresent lumped_cap pr_or_sc_nu zero_flow_in_solid dorpr_scal",
+    "postlist": ("nmis nbins skip_num post_no_flow_mem_alloc rad_factor power sa_max_itr post_error post_small rad_ratio "
+                 "func_rad_ratio cooling_rate temp_init sa_error objective_coef1 objective_coef2 igeometry isa sa_in_itr "
+                 "rad_reduction_ratio icohesive nsmall_length lybyd_small cluster_part_min cluster_part_max rotated "
+                 "include_nmis"),
+}
+NAMELISTS = {g: frozenset(v.split()) for g, v in NAMELISTS.items()}
+# array variables among the keys the engine reads, and their lengths
+_ARRAYS = {"flo_ang": 3, "mpg": 3}
 
-    Group order and unknown keys are not enforced here (the reference aborts
-    on an unknown key); keys are matched case-insensitively.
+
+def _read_order(prm: Dict):
+    """The groups read_nmls reads, in its order (SRC/FLO/initialize.F90:287-328).
+    A generator: which groups come after GCG depends on values read before."""
+    for g in ("floandgrid", "part_propt", "flags", "files", "psd", "gcg"):
+        yield g
+    it = str(prm.get("input_type", "default")).strip().lower()
+    if it == "lubtest":
+        yield "lubtest"
+        yield "bidisperse"
+    if it == "random" and str(prm.get("psd_type", "")).strip().lower() == "bidisp":
+        yield "bidisperse"
+    if it == "mat":
+        yield "matinput"
+    if it == "risers":
+        yield "riser"
+    if int(prm.get("iscalon", 0) or 0) == 1:
+        yield "scal_propt"
+    yield "postlist"
+
+
+def _namelist_groups(text: str):
+    """(name, body, start, end) of every &NAME ... / group, comments removed."""
+    text = re.sub(r"![^\n]*", "", text)
+    out = []
+    for m in re.finditer(r"[&$](\w+)(.*?)(?:^\s*/|/\s*$|[&$]end\b)", text, flags=re.S | re.M | re.I):
+        out.append((m.group(1).lower(), m.group(2), m.start(), m.end()))
+    return out
+
+
+def _group_items(body: str):
+    """KEY = value pairs of one group body; values may span commas and lines,
+    a repeat count n*v expands to n copies, KEY(i) = v sets one element."""
+    for m in re.finditer(r"(\w+)(\(\s*\d+\s*\))?\s*=\s*(.*?)(?=[\s,]+\w+(\(\s*\d+\s*\))?\s*=|\Z)", body, flags=re.S):
+        raw = m.group(3).replace("\n", " ").strip().rstrip(",")
+        raw = re.sub(r"(\d+)\*([^\s,]+)", lambda r: ", ".join([r.group(2)] * int(r.group(1))), raw)
+        idx = int(m.group(2).strip("() \t")) if m.group(2) else None
+        yield m.group(1).lower(), idx, _parse_value(raw)
+
+
+def read_floparam(path: str) -> Dict:
+    """Read a floparam.in the way read_nmls does (SRC/FLO/initialize.F90:274-359).
+
+    The groups are read in the reference's order, each one searched for
+    after the end of the previous one (a sequential namelist read skips any
+    other group on its way, as gfortran does), so a group that sits before
+    one read earlier is never seen: that, and a group missing altogether,
+    raise ValueError like the reference's end-of-file stop.  A variable that
+    the group does not declare raises ValueError (the reference's namelist
+    read aborts on it).  Keys are case-insensitive; ``!`` starts a comment.
+    SET_UMEAN = T implies SET_MPG (initialize.F90:292).
     """
     prm = default_params()
     text = open(path).read()
-    groups = re.findall(r"&(\w+)(.*?)(?:^\s*/\s*$)", text, flags=re.S | re.M)
-    for _, body in groups:
-        # split "KEY = value" pairs; values may span commas / several numbers
-        for m in re.finditer(r"(\w+)\s*=\s*(.*?)(?=\s+\w+\s*=|\Z)", body, flags=re.S):
-            key = m.group(1).lower()
-            val = _parse_value(m.group(2).replace("\n", " "))
+    groups = _namelist_groups(text)
+    pos = 0
+    for name in _read_order(prm):
+        hit = next((g for g in groups if g[0] == name and g[2] >= pos), None)
+        if hit is None:
+            where = "before an earlier group" if any(g[0] == name for g in groups) else "missing"
+            raise ValueError(f"{path}: namelist group &{name.upper()} is {where}; read_nmls reads "
+                             "FLOANDGRID, PART_PROPT, FLAGS, FILES, PSD, GCG, [LUBTEST, BIDISPERSE, MATINPUT, "
+                             "RISER, SCAL_PROPT,] POSTLIST in that order")
+        for key, idx, val in _group_items(hit[1]):
+            if key not in NAMELISTS[name]:
+                raise ValueError(f"{path}: &{name.upper()} has no variable {key.upper()}")
+            if key in _ARRAYS:
+                # a namelist array assignment sets elements idx, idx+1, ...
+                # (from 1 without a subscript); the others keep their values
+                cur = list(prm.get(key)) if isinstance(prm.get(key), (tuple, list)) else [0.0] * _ARRAYS[key]
+                vals = list(val) if isinstance(val, (tuple, list)) else [val]
+                for k, v in enumerate(vals):
+                    if (idx or 1) - 1 + k >= len(cur):
+                        raise ValueError(f"{path}: too many values for {key.upper()}")
+                    cur[(idx or 1) - 1 + k] = v
+                val = tuple(cur)
+            elif idx is not None:
+                raise ValueError(f"{path}: {key.upper()} is not an array")
             prm[key] = val
+        pos = hit[3]
     if prm.get("set_umean"):
         prm["set_mpg"] = True
     return prm
@@ -158,6 +252,16 @@ def make_params(prm: Dict) -> pibm_params:
     p.rk3 = int(bool(prm.get("rk3", False)))
     if not prm.get("xperiodic", True):
         raise ValueError("XPERIODIC=F is not supported (x-periodic only)")
+    # options that select reference code this engine does not run: passed on so
+    # that the library refuses them (pibm_create returns PIBM_ERR_ARG)
+    p.dobnd = int(bool(prm.get("dobnd", True)))
+    p.aliasflag = int(prm.get("aliasflag", 0) or 0)
+    p.nlcons_false = int(not prm.get("nlcons", True))
+    ctype = str(prm.get("collision_type", "none")).strip().lower()
+    if ctype not in ("none", "softsphere", "eventdriven"):
+        raise ValueError(f"COLLISION_TYPE = '{ctype}' is not a reference collision model")
+    if p.imove == 1 and ctype == "eventdriven":
+        raise ValueError("COLLISION_TYPE = 'eventdriven' is not supported (soft-sphere DEM or 'none')")
     return p
 
 

@@ -338,6 +338,10 @@ bool setup_run(const pibm_params &prm, const pibm_particles *parts, RunSetup &S,
     if (mz != prm.my) { err = "only MZ == MY is supported"; return false; }
     if (prm.discr_scheme != PIBM_SCHEME_UPWIND && prm.discr_scheme != PIBM_SCHEME_CENTER) { err = "bad discr_scheme"; return false; }
     if (prm.imove != 0 && prm.imove != 1) { err = "IMOVE must be 0 or 1"; return false; }
+    // reference options whose code paths are not part of this engine: refused, never ignored
+    if (prm.dobnd) { err = "DOBND = T (surface-point forcing, calc_bnd_forcing) is not supported: set DOBND = F"; return false; }
+    if (prm.aliasflag) { err = "ALIASFLAG = 1 (dealiased nonlinear term) is not supported: set ALIASFLAG = 0"; return false; }
+    if (prm.nlcons_false) { err = "NLCONS = F is not supported: set NLCONS = T"; return false; }
     S.my = prm.my; S.mz = mz; S.mx = S.my + 1; S.mxf = S.mx; S.nx = S.mx - 1; S.my2 = S.my / 2 + 1;
     S.nbody = parts ? parts->nbody : 0;
     if (S.nbody < 0 || (S.nbody > 0 && !parts->xc)) { err = "bad particle list"; return false; }
