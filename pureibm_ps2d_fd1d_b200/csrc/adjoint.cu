@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_adj_c2r(Geo g, const 
     }
     __syncthreads();
     cl_c2r<N>(buf, tw, rank);
-    if (threadIdx.x == 0) { bulk_store(dst + ((size_t)item * nx + i) * RSP + (size_t)rank * L::RL, buf, L::RBYTES); bulk_wait_all(); }
+    if (threadIdx.x == 0) { bulk_store(dst + ((size_t)item * nx + i) * RSP + (size_t)rank * L::RL, buf, L::RBYTES); bulk_wait_read(); }
 }
 
 // k_adj_r2c: transposes of the step's c2r transforms, c2r^T(r) = c_ky (my mz) r2c(r),

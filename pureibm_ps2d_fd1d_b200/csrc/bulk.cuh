@@ -23,6 +23,24 @@ __device__ __forceinline__ void bulk_load(void *dst_smem, const void *src_gmem, 
                  : "memory");
 }
 
+// One warp: lane 0 announces n*bytes on mb, then the lanes start n
+// global -> shared bulk copies of `bytes` each, copy r from src + r*src_pitch
+// to dst + r*dst_pitch (byte pitches; addresses, pitches and bytes 16-byte
+// multiples).  The copies complete on mb like one bulk_load of n*bytes.
+__device__ __forceinline__ void bulk_load_rows(void *dst, uint32_t dst_pitch, const void *src, size_t src_pitch,
+                                               uint32_t bytes, int n, uint64_t *mb) {
+    const int lane = threadIdx.x & 31;
+    if (lane == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mb)), "r"(bytes * (uint32_t)n)
+                     : "memory");
+    __syncwarp();
+    for (int r = lane; r < n; r += 32)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_u32((char *)dst + (size_t)r * dst_pitch)),
+                     "l"((const char *)src + (size_t)r * src_pitch), "r"(bytes), "r"(smem_u32(mb))
+                     : "memory");
+}
+
 // All threads: wait for the phase with parity `phase` to complete (bounded).
 __device__ __forceinline__ bool mbar_wait(uint64_t *mb, uint32_t phase) {
     const uint32_t a = smem_u32(mb);
@@ -44,7 +62,8 @@ __device__ __forceinline__ void bulk_store(void *dst_gmem, const void *src_smem,
     asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem), "r"(smem_u32(src_smem)), "r"(bytes) : "memory");
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
-// One thread: wait until every committed bulk store has finished reading shared memory.
+// One thread: wait until every committed bulk store has finished reading shared
+// memory.  A CTA may exit after it: the global writes complete with the grid.
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 // One thread: wait until every committed bulk store has completed.
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }

@@ -55,6 +55,8 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
     double2 *buf = sm, *tws = sm + L::BUF;
     __shared__ double scr[32];
+    __shared__ uint64_t mb;
+    if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
     __syncthreads();
     const int i = blockIdx.x / L::C, rank = blockIdx.x % L::C, nx = g.nx;
@@ -67,19 +69,26 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
     const size_t slot = ((size_t)i * L::C + rank) * 12;
     {
         const int t = blockIdx.y;
-        // spectral input of this CTA's columns
+        if (t < 4) {
+            // a plain copy of u_t or p: the CTA's MC columns of every kz row as N
+            // bulk copies into the padded rows, all in flight at once; rank 0's
+            // Nyquist column (slot MC) with plain loads beside them
+            const double2 *src = t == 0 ? U0 : t == 1 ? U1 : t == 2 ? U2 : Pp;
+            uint32_t phase = 0;
+            if (threadIdx.x < 32)
+                bulk_load_rows(buf, L::PZ * 16, src + rank * L::MC, (size_t)my2 * 16, L::MC * 16, N, &mb);
+            if (rank == 0)
+                for (int kz = threadIdx.x; kz < N; kz += L::T) buf[kz * L::PZ + L::MC] = src[kz * my2 + L::M];
+            load_wait(&mb, phase, sc);
+        } else {
+            // omega and grad p: spectral differences formed from plain loads
 #pragma unroll 4
-        for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
-            const int kz = e / L::PZ, jl = e - kz * L::PZ;
-            if (jl == L::MC && rank != 0) continue;
-            const int j = cl_col<N>(jl, rank), ge = kz * my2 + j;
-            double2 f;
-            if (t == 0) f = U0[ge];
-            else if (t == 1) f = U1[ge];
-            else if (t == 2) f = U2[ge];
-            else if (t == 3) f = Pp[ge];
-            else {
+            for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
+                const int kz = e / L::PZ, jl = e - kz * L::PZ;
+                if (jl == L::MC && rank != 0) continue;
+                const int j = cl_col<N>(jl, rank), ge = kz * my2 + j;
                 const double ky = g.ky[j], kzv = g.kz[kz];
+                double2 f;
                 if (t == 4) {   // wy*u3 - wz*u2
                     const double2 a = U2[ge], b = U1[ge];
                     f = make_double2(-ky * a.y - (-kzv * b.y), ky * a.x - kzv * b.x);
@@ -98,8 +107,8 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
                     f = make_double2(qdiv(a.x - b.x, tdx, rtdx), qdiv(a.y - b.y, tdx, rtdx));
                 } else if (t == 8) { const double2 a = Pp[ge]; f = make_double2(-a.y * ky, a.x * ky); }
                 else { const double2 a = Pp[ge]; f = make_double2(-a.y * kzv, a.x * kzv); }
+                buf[e] = f;
             }
-            buf[e] = f;
         }
         __syncthreads();
         cl_c2r<N>(buf, tw, rank);
@@ -126,7 +135,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
         double *dst = t < 3 ? ubcp + ((size_t)t * nx + i) * RSP
                     : t == 3 ? pbcp + (size_t)i * RSP
                     : (t < 7 ? omega + ((size_t)(t - 4) * nx + i) * RSP : pgr + ((size_t)(t - 7) * nx + i) * RSP);
-        if (threadIdx.x == 0) { bulk_store(dst + roff, buf, L::RBYTES); bulk_wait_all(); }
+        if (threadIdx.x == 0) { bulk_store(dst + roff, buf, L::RBYTES); bulk_wait_read(); }
     }
 }
 
@@ -374,12 +383,22 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const doubl
         double2 *dst = nl_new + ((size_t)c * nx + i) * PS;
         for (int q = 0; q < 3; ++q) {
             if (q < 2) {
-                double *b = (double *)buf;
-                // product pairs of component c: wy term (u1 u1, u2 u2... as (0,1),(1,1),(1,2)), wz term (c, 2)
+                // product pairs of component c: wy term (u1 u2, u2 u2, u2 u3), wz term (c, 2);
+                // the first factor's rows arrive by one bulk copy, the second by
+                // 16-byte loads multiplied in place
                 const int na = q == 0 ? (c == 0 ? 0 : 1) : c, nb = q == 0 ? (c == 2 ? 2 : 1) : 2;
-                const double *A = Uc(na), *B = Uc(nb);
-#pragma unroll 4
-                for (int e = threadIdx.x; e < L::RL; e += L::T) b[e] = A[e] * B[e];
+                if (threadIdx.x == 0) {
+                    fence_async_smem();
+                    bulk_load(buf, Uc(na), L::RBYTES, &mb);
+                }
+                load_wait(&mb, phase, sc);
+                double2 *b2 = buf;
+                const double2 *B2 = (const double2 *)Uc(nb);
+#pragma unroll 8
+                for (int e = threadIdx.x; e < L::RL / 2; e += L::T) {
+                    const double2 x = b2[e], y = B2[e];
+                    b2[e] = make_double2(x.x * y.x, x.y * y.y);
+                }
                 __syncthreads();
             } else {
                 if (threadIdx.x == 0) {
@@ -406,35 +425,47 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const doubl
         // nl = -(...) (nl.F90:146-152); Q = -c3 nl - c4 onl - c12 diffn (calc_visc spectrum)
         const double2 *on = onl + ((size_t)c * nx + i) * PS;
         const double2 *uc = u + (size_t)c * nx * PS;
-#pragma unroll 4
+        // the nl value of element (kz, jl) and the transform input of Q there
+        auto nl_q = [&](int kz, int jl) -> double2 {
+            const int ge = kz * my2 + cl_col<N>(jl, rank);
+            const double2 X = r2c_norm<N>(cl_unpack<N>(buf, kz, jl, rank), g.nrm);
+            const double2 s = cadd(dst[ge], X);
+            const double2 v = make_double2(-s.x, -s.y);
+            dst[ge] = v;
+            const double2 a = uc[(size_t)im * PS + ge], bb = uc[(size_t)i * PS + ge], cv = uc[(size_t)ip * PS + ge];
+            double2 df = make_double2(g.rdx2 * ((a.x - 2.0 * bb.x) + cv.x), g.rdx2 * ((a.y - 2.0 * bb.y) + cv.y));
+            const double w2 = g.w2[ge];
+            df = make_double2((df.x - w2 * bb.x) * g.vis, (df.y - w2 * bb.y) * g.vis);
+            const double2 o = on[ge];
+            return make_double2((-g.c3 * v.x - g.c4 * o.x) - c12 * df.x, (-g.c3 * v.y - g.c4 * o.y) - c12 * df.y);
+        };
+        // Every element is read and rewritten by its own thread, except rank 0's
+        // column 0, which cl_unpack also reads for ky = 0 and ky = M at the
+        // mirrored kz: it is rewritten after a barrier.
+#pragma unroll 2
         for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
             const int kz = e / L::PZ, jl = e - kz * L::PZ;
-            if (jl == L::MC && rank != 0) continue;
-            const int ge = kz * my2 + cl_col<N>(jl, rank);
-            const double2 Xr = cl_unpack<N>(buf, kz, jl, rank);
-            const double2 X = r2c_norm<N>(Xr, g.nrm);
-            const double2 a = cadd(dst[ge], X);
-            dst[ge] = make_double2(-a.x, -a.y);
+            if ((jl == L::MC && rank != 0) || (jl == 0 && rank == 0)) continue;
+            buf[e] = nl_q(kz, jl);
         }
-        __syncthreads();   // every read of the r2c result is done; each thread re-reads its own nl values
-#pragma unroll 4
-        for (int e = threadIdx.x; e < L::NOUT; e += L::T) {
-            {
-                const int kz = e / L::PZ, jl = e - kz * L::PZ;
-                if (jl == L::MC && rank != 0) continue;
-                const int ge = kz * my2 + cl_col<N>(jl, rank);
-                const double2 v = dst[ge];
-                const double2 a = uc[(size_t)im * PS + ge], bb = uc[(size_t)i * PS + ge], cv = uc[(size_t)ip * PS + ge];
-                double2 df = make_double2(g.rdx2 * ((a.x - 2.0 * bb.x) + cv.x), g.rdx2 * ((a.y - 2.0 * bb.y) + cv.y));
-                const double w2 = g.w2[ge];
-                df = make_double2((df.x - w2 * bb.x) * g.vis, (df.y - w2 * bb.y) * g.vis);
-                const double2 o = on[ge];
-                buf[e] = make_double2((-g.c3 * v.x - g.c4 * o.x) - c12 * df.x, (-g.c3 * v.y - g.c4 * o.y) - c12 * df.y);
+        if (rank == 0) {
+            constexpr int K0 = (N + L::T - 1) / L::T;
+            double2 q0[K0];
+#pragma unroll
+            for (int k = 0; k < K0; ++k) {
+                const int kz = (int)threadIdx.x + k * L::T;
+                if (kz < N) q0[k] = nl_q(kz, 0);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < K0; ++k) {
+                const int kz = (int)threadIdx.x + k * L::T;
+                if (kz < N) buf[kz * L::PZ] = q0[k];
             }
         }
         __syncthreads();
         cl_c2r<N>(buf, tw, rank);
-        if (threadIdx.x == 0) { bulk_store(Q + ((size_t)c * nx + i) * RS + roff, buf, L::RBYTES); bulk_wait_all(); }
+        if (threadIdx.x == 0) { bulk_store(Q + ((size_t)c * nx + i) * RS + roff, buf, L::RBYTES); bulk_wait_read(); }
     }
 }
 

@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_sa(Geo g, const doubl
     } else {
         dst = gph + ((size_t)(t - 2) * (nx + 1) + p) * RSP;
     }
-    if (threadIdx.x == 0) { bulk_store(dst + roff, buf, L::RBYTES); bulk_wait_all(); }
+    if (threadIdx.x == 0) { bulk_store(dst + roff, buf, L::RBYTES); bulk_wait_read(); }
 }
 
 // heat_ratio_new = 1/phim(nx+1), phim = sum(u phi) / (um * count), um = sum(u)/count
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_snl(Geo g, const doub
     }
     __syncthreads();
     cl_c2r<N>(buf, tw, rank);
-    if (threadIdx.x == 0) { bulk_store(nlr + (size_t)p * RSP + roff, buf, L::RBYTES); bulk_wait_all(); }
+    if (threadIdx.x == 0) { bulk_store(nlr + (size_t)p * RSP + roff, buf, L::RBYTES); bulk_wait_read(); }
 }
 
 // k_simg: real nonlinear term of the image plane nx+1 = c2r(nlphif(1)/heat_ratio)
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_simg(Geo g, const dou
     }
     __syncthreads();
     cl_c2r<N>(buf, tw, rank);
-    if (threadIdx.x == 0) { bulk_store(nlr + (size_t)g.nx * RSP + (size_t)rank * L::RL, buf, L::RBYTES); bulk_wait_all(); }
+    if (threadIdx.x == 0) { bulk_store(nlr + (size_t)g.nx * RSP + (size_t)rank * L::RL, buf, L::RBYTES); bulk_wait_read(); }
 }
 
 // k_sreal: c2r of spectral planes into the real-field layout of the step
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_sreal(Geo g, const do
     }
     __syncthreads();
     cl_c2r<N>(buf, tw, rank);
-    if (threadIdx.x == 0) { bulk_store(dst + (size_t)p * RSP + (size_t)rank * L::RL, buf, L::RBYTES); bulk_wait_all(); }
+    if (threadIdx.x == 0) { bulk_store(dst + (size_t)p * RSP + (size_t)rank * L::RL, buf, L::RBYTES); bulk_wait_read(); }
 }
 
 // ============================================================================

@@ -24,13 +24,13 @@ def _write_case(d, floparam, xc_grid, dbydx):
     config.write_sphr_center(os.path.join(d, "RUN_sphr_center.inp"), xc_grid, dbydx)
 
 
-@pytest.mark.parametrize("variant", ["ab2", "rk3_mpg"])
+@pytest.mark.parametrize("variant", ["ab2", "rk3_center"])
 def test_c_driver_records_equal_python_driver(tmp_path, variant):
     exe = build.build_main()
     text = FLOPARAM
-    if variant == "rk3_mpg":
-        text = text.replace("RK3 = F", "RK3 = T").replace("SET_UMEAN = F", "SET_UMEAN = T").replace(
-            "MY = 32,", "MY = 32, MPG = -2.0d-3,")
+    if variant == "rk3_center":
+        text = text.replace("RK3 = F", "RK3 = T").replace("'upwind'", "'center'").replace(
+            "FLO_ANG = 0.d0, 90.d0, 90.d0", "FLO_ANG = 0.d0, 60.d0, 90.d0")
     _, xc = config.random_array(my=32, dia_cells=8, nbody=3, seed=11, mc_moves=50)
     cdir, pdir = tmp_path / "c", tmp_path / "py"
     cdir.mkdir()
