@@ -167,6 +167,16 @@ module pibm_c
        integer(c_int32_t), value :: maxn
        integer(c_int32_t), intent(out) :: neigh(*), pn(*), pv(*)   ! (nbody, maxn) like NEIGHBOURS / PN / PV
      end function
+     integer(c_int) function pibm_get_frame(h, frame_vel, frame_pos) bind(C, name="pibm_get_frame")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(out) :: frame_vel(3), frame_pos(3)
+     end function
+     integer(c_int) function pibm_set_frame(h, frame_vel, frame_pos) bind(C, name="pibm_set_frame")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(in) :: frame_vel(3), frame_pos(3)
+     end function
      integer(c_int) function pibm_get_if_rev(h, if_rev) bind(C, name="pibm_get_if_rev")
        import :: c_int, c_ptr, c_int8_t
        type(c_ptr), value :: h

@@ -227,6 +227,13 @@ int  pibm_set_scalar(pibm_handle *h, const double *phif, const double *nlphif, c
  * (MAXNEIGHBORS = MN + 1 + NWALLS) always suffices; PIBM_ERR_ARG if a list
  * does not fit or the run has fixed particles.  Any pointer may be NULL. */
 int  pibm_get_contacts(pibm_handle *h, int32_t maxn, int32_t *neigh, int32_t *pn, int32_t *pv);
+/* Frame motion of a moving-particle run (IMOVE = 1): frame_vel(3), frame_pos(3)
+ * of the reference (updated in velstep, steptheflow.F90:99-103; written to
+ * RUN_NAME_sphere_config_N.rst, restart_funcs.F90:253-254, and read back on
+ * restart, initialize_flo.F90:1891-1898).  Fixed runs keep 0 and 1.
+ * pibm_set_frame: at a step boundary; either pointer of get may be NULL. */
+int  pibm_get_frame(pibm_handle *h, double frame_vel[3], double frame_pos[3]);
+int  pibm_set_frame(pibm_handle *h, const double frame_vel[3], const double frame_pos[3]);
 /* Active reversal-point flags (part_array(m)%if_rev), (nbnd, nbody) column-major. */
 int  pibm_get_if_rev(pibm_handle *h, uint8_t *if_rev);
 /* Solid mask fluid_atijk(1:nx,1:my,1:mz) as 0/1 bytes, x fastest. */

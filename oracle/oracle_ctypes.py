@@ -51,6 +51,8 @@ def lib():
         L.orc_get_scalar_nl.argtypes = [vp, P(C.c_double)]
         L.orc_set_scalar.argtypes = [vp, P(C.c_double), P(C.c_double), P(C.c_double)]
         L.orc_set_desired_means.argtypes = [vp, P(C.c_double), P(C.c_double)]
+        L.orc_get_frame.argtypes = [vp, P(C.c_double), P(C.c_double)]
+        L.orc_set_frame.argtypes = [vp, P(C.c_double), P(C.c_double)]
         L.orc_ff2rc.argtypes = [C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
         L.orc_ff2cr.argtypes = [C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double)]
         L.orc_cyclic_solve.argtypes = [C.c_int] + [P(C.c_double)] * 7
@@ -151,6 +153,16 @@ class OracleSolver:
         a = np.ascontiguousarray(usmean_des, dtype=np.float64)
         b = np.ascontiguousarray(ufmean_des, dtype=np.float64)
         lib().orc_set_desired_means(self.h, _dp(a), _dp(b))
+
+    def get_frame(self):
+        fv, fp = np.zeros(3), np.zeros(3)
+        lib().orc_get_frame(self.h, _dp(fv), _dp(fp))
+        return fv, fp
+
+    def set_frame(self, frame_vel, frame_pos):
+        a = np.ascontiguousarray(frame_vel, dtype=np.float64)
+        b = np.ascontiguousarray(frame_pos, dtype=np.float64)
+        lib().orc_set_frame(self.h, _dp(a), _dp(b))
 
     def set_scalar(self, phif, nlphif, heat_ratio, heat_ratio_old):
         a = np.ascontiguousarray(phif, dtype=np.complex128)

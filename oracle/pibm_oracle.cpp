@@ -2156,6 +2156,19 @@ extern "C" int orc_set_desired_means(void *h, const double *usd, const double *u
     return PIBM_OK;
 }
 
+// Frame motion of a moving run (frame_vel, frame_pos: steptheflow.F90:99-103,
+// restart_funcs.F90:253-254).
+extern "C" int orc_get_frame(void *h, double *frame_vel, double *frame_pos) {
+    Orc &o = *(Orc *)h;
+    for (int d = 0; d < 3; ++d) { frame_vel[d] = o.frame_vel[d]; frame_pos[d] = o.frame_pos[d]; }
+    return PIBM_OK;
+}
+extern "C" int orc_set_frame(void *h, const double *frame_vel, const double *frame_pos) {
+    Orc &o = *(Orc *)h;
+    for (int d = 0; d < 3; ++d) { o.frame_vel[d] = frame_vel[d]; o.frame_pos[d] = frame_pos[d]; }
+    return PIBM_OK;
+}
+
 // read_unformatted's scalar part (restart_funcs.F90:560-590).
 extern "C" int orc_set_scalar(void *h, const double *phif, const double *nlphif, const double *ratios) {
     Orc &o = *(Orc *)h;

@@ -230,6 +230,18 @@ class Solver:
         b = np.ascontiguousarray(ufmean_des, dtype=np.float64)
         _check(load_library().pibm_set_desired_means(self.h, _dp(a), _dp(b)))
 
+    def get_frame(self):
+        """frame_vel(3), frame_pos(3) of a moving-particle run (0 and 1 for fixed spheres)."""
+        fv, fp = np.zeros(3), np.zeros(3)
+        _check(load_library().pibm_get_frame(self.h, _dp(fv), _dp(fp)))
+        return fv, fp
+
+    def set_frame(self, frame_vel, frame_pos):
+        """Frame motion of a restarted moving-particle run."""
+        a = np.ascontiguousarray(frame_vel, dtype=np.float64)
+        b = np.ascontiguousarray(frame_pos, dtype=np.float64)
+        _check(load_library().pibm_set_frame(self.h, _dp(a), _dp(b)))
+
     def set_scalar(self, phif, nlphif, heat_ratio: float, heat_ratio_old: float):
         """Scalar restart: phif and the last step's nlphif as (mz, my2, nx+1)."""
         a = np.ascontiguousarray(phif, dtype=np.complex128)

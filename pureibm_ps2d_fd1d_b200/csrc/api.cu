@@ -1049,6 +1049,33 @@ int pibm_set_scalar(pibm_handle *h, const double *phif, const double *nlphif, co
     return PIBM_OK;
 }
 
+// Frame motion of a moving-particle run (frame_vel, frame_pos of global_data;
+// updated in velstep, steptheflow.F90:99-103; restart records of
+// restart_funcs.F90:253-254, read back in initialize_flo.F90:1891-1898).
+int pibm_get_frame(pibm_handle *h, double *frame_vel, double *frame_pos) {
+    if (!h) return fail(PIBM_ERR_ARG, "null handle");
+    Scal sc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    for (int d = 0; d < 3; ++d) {
+        if (frame_vel) frame_vel[d] = sc.frame_vel[d];
+        if (frame_pos) frame_pos[d] = sc.frame_pos[d];
+    }
+    return PIBM_OK;
+}
+
+int pibm_set_frame(pibm_handle *h, const double *frame_vel, const double *frame_pos) {
+    if (!h || !frame_vel || !frame_pos) return fail(PIBM_ERR_ARG, "null argument");
+    if (h->next_rks != 1) return fail(PIBM_ERR_ARG, "pibm_set_frame at a step boundary only");
+    Scal sc;
+    CUDA_OR_FAIL(cudaMemcpyAsync(&sc, h->b.sc, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    for (int d = 0; d < 3; ++d) { sc.frame_vel[d] = frame_vel[d]; sc.frame_pos[d] = frame_pos[d]; }
+    CUDA_OR_FAIL(cudaMemcpyAsync(h->b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, h->stream));
+    CUDA_OR_FAIL(cudaStreamSynchronize(h->stream));
+    return PIBM_OK;
+}
+
 int pibm_get_if_rev(pibm_handle *h, uint8_t *if_rev) {
     if (!h || !if_rev) return fail(PIBM_ERR_ARG, "null argument");
     if (h->g.moving) {   // flags of the last step's geometry rebuild

@@ -5,7 +5,11 @@ WRITE: a 4-byte length marker, the data, the marker again) and alternates
 between two sets, RUN_NAME_{u,nl,p,scal}_1.rst and _2.rst, recording the set
 last written in the formatted file RUN_NAME_RESTART; RUN_NAME_sphere_config.rst
 holds the particles (and, for moving particles, RUN_NAME_sphere_config_N.rst
-the moved ones plus the frame motion).  Writing a set deletes the other one.
+the moved ones plus the frame motion frame_vel, frame_pos).  Writing a set
+deletes the other one.  A moving run resumes like the reference's: from the
+moved positions and velocities and the frame motion, its soft-sphere contact
+lists rebuilt by the neighbour search of a new run (the reference keeps no
+contact history in its restart files).
 
     write_restart(solver, directory, run_name)        # next set (1 or 2)
     data = read_restart(directory, run_name, solver)  # the set named in _RESTART
@@ -28,7 +32,6 @@ import numpy as np
 NERR_STEPS = 100   # nerr_steps (initialize_flo.F90)
 NOT_KEPT = ("ferror_array (written as the last ferror followed by 1.0)",
             "grant_error, grant_old, grant_array (moving particles; written as 1.0, 0.0, 1.0)",
-            "frame_vel, frame_pos (moving particles; written as 0 and 1, their initial values)",
             "nu_error, nu_error_array (scalar; written as 1.0)")
 
 
@@ -172,10 +175,9 @@ def write_restart(solver, directory: str, run_name: str, count: Optional[int] = 
         w.write(rad.astype("<f8"))
         w.write(np.asfortranarray(vel, dtype="<f8").ravel(order="F"))
         if name != "sphere_config":
-            fv = np.asarray(getattr(solver, "frame_vel", np.zeros(3)), dtype="<f8")
-            fp = np.asarray(getattr(solver, "frame_pos", np.ones(3)), dtype="<f8")
-            w.write(fv)
-            w.write(fp)
+            fv, fp = solver.get_frame()
+            w.write(np.asarray(fv, dtype="<f8"))
+            w.write(np.asarray(fp, dtype="<f8"))
         w.close()
     # u: scalars, convergence histories, the velocity field
     ferror = float(rep.get("ferror", 1.0))
@@ -301,6 +303,8 @@ def apply_restart(solver, data: Dict):
                       "mpg": data["mpg"], "t": data["t"], "dt": data["dt"], "cf": data["cf"],
                       "ufmean": np.zeros(3)})
     solver.set_desired_means(data["usmean_des"], data["ufmean_des"])
+    if "frame_vel" in data:
+        solver.set_frame(data["frame_vel"], data["frame_pos"])
     if "phif" in data:
         solver.set_scalar(data["phif"], data["nlphif"], data["heat_ratio"], data["heat_ratio_old"])
 

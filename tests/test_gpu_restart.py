@@ -52,3 +52,45 @@ def test_engine_resumes_oracle_files(tmp_path):
         assert d <= 1e-10, (k, d)
     d = np.abs(gpu.get_scalar()["phif"] - cpu.get_scalar()["phif"]).max()
     assert d <= 1e-10
+
+
+@pytest.mark.gpu
+def test_moving_run_resumes_on_engine_and_oracle(tmp_path):
+    """IMOVE = 1: the engine writes the moved particles and its frame motion
+    (frame_vel, frame_pos), and the engine and the oracle resumed from those
+    files track each other within the parity bar: positions and frame motion
+    to 1e-12, the flow to 1e-10, identical contact lists."""
+    prm, xc, vel = config.moving_array(my=64, dia_cells=8.0, nbody=60, seed=9, vel_spread=1.5)
+    a = pk.Solver(config.make_params(prm), xc, vel)
+    for _ in range(8):
+        a.step()
+    restart.write_restart(a, str(tmp_path), "MOV")
+    fv, fp = a.get_frame()
+    assert np.any(fv != 0.0)
+    data = restart.read_restart(str(tmp_path), "MOV", a.nx, a.my, a.mz, imove=True)
+    assert np.array_equal(data["frame_vel"], fv) and np.array_equal(data["frame_pos"], fp)
+    gpu = restart.resume(prm, str(tmp_path), "MOV")
+    assert all(np.array_equal(x, y) for x, y in zip(gpu.get_frame(), (fv, fp)))
+
+    def oracle(P, x, v):
+        parts = config.Particles(x, v)
+        s = oc.OracleSolver(P, parts.struct)
+        s._parts = parts
+        return s
+
+    cpu = restart.resume(prm, str(tmp_path), "MOV", solver_cls=oracle)
+    for _ in range(8):
+        gpu.step()
+        cpu.step()
+    xg, xo = gpu.get_particles()[3], cpu.get_particles()[3]
+    assert np.abs(xg - xo).max() <= 1e-12 * np.abs(xo).max()
+    for g, o in zip(gpu.get_frame(), cpu.get_frame()):
+        assert np.abs(g - o).max() <= 1e-12 * max(np.abs(o).max(), 1.0)
+    cg, cc = gpu.get_contacts(), oc.get_contacts(cpu)
+    for k in ("neighbours", "pn", "pv"):
+        assert np.array_equal(cg[k], cc[k]), k
+    sg, so = gpu.get_state(), cpu.get_state()
+    for k in ("u", "p"):
+        d = np.abs(sg[k] - so[k]).max() / np.abs(so[k]).max()
+        assert d <= 1e-10, (k, d)
+

@@ -73,7 +73,14 @@ def test_resume_moving_particles(tmp_path):
         a.step()
     restart.write_restart(a, str(tmp_path), "MOV")
     assert os.path.exists(os.path.join(str(tmp_path), "MOV_sphere_config_1.rst"))
+    # the frame motion of the run, not its initial values, is in the file
+    fv, fp = a.get_frame()
+    assert np.any(fv != 0.0) and np.any(fp != 1.0)
+    data = restart.read_restart(str(tmp_path), "MOV", a.nx, a.my, a.mz, imove=True)
+    assert np.array_equal(data["frame_vel"], fv) and np.array_equal(data["frame_pos"], fp)
     b = restart.resume(prm, str(tmp_path), "MOV", solver_cls=lambda P, x, v: _oracle(prm, x, v))
+    fvb, fpb = b.get_frame()
+    assert np.array_equal(fvb, fv) and np.array_equal(fpb, fp)
     for _ in range(3):
         a.step()
         b.step()
@@ -83,3 +90,6 @@ def test_resume_moving_particles(tmp_path):
     assert np.abs(xa - xb).max() <= 1e-12 * np.abs(xa).max()
     ua, ub = a.get_state()["u"], b.get_state()["u"]
     assert np.abs(ua - ub).max() <= 1e-10 * np.abs(ua).max()
+    fa, fb = a.get_frame(), b.get_frame()
+    for k in range(2):
+        assert np.abs(fa[k] - fb[k]).max() <= 1e-12 * max(np.abs(fa[k]).max(), 1.0)
