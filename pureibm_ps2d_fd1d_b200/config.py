@@ -19,6 +19,7 @@
 from __future__ import annotations
 
 import ctypes as C
+import os
 import re
 from typing import Dict, Optional
 
@@ -186,6 +187,25 @@ def read_floparam(path: str) -> Dict:
     if prm.get("set_umean"):
         prm["set_mpg"] = True
     return prm
+
+
+def load_run(directory: str, run_name: str = "") -> tuple:
+    """A run's parameters and sphere centres (grid units) from its input
+    files, as initflo reads them: RUN_NAME_floparam.in (floparam.in without a
+    run name), then for INPUT_TYPE = 'default' the centres of
+    RUN_NAME_sphr_center.inp, for INPUT_TYPE = 'random' a configuration
+    generated from RUN_NAME_seed.d (generators.load_random_run; the seed file
+    is rewritten with the next seed, as the reference does)."""
+    pre = run_name + "_" if run_name else ""
+    prm = read_floparam(os.path.join(directory, pre + "floparam.in"))
+    itype = str(prm.get("input_type", "default")).strip().lower()
+    if itype == "random":
+        from . import generators
+        return generators.load_random_run(prm, directory, run_name or "")
+    if itype != "default":
+        raise ValueError(f"INPUT_TYPE = '{itype}' is not supported ('default' or 'random')")
+    dbydx = prm["dbydx"] if prm.get("dbydx") is not None else prm["my"] / float(prm["lybyd"])
+    return prm, read_sphr_center(os.path.join(directory, pre + "sphr_center.inp"), dbydx)
 
 
 def read_sphr_center(path: str, dbydx: float) -> np.ndarray:
