@@ -167,6 +167,11 @@ module pibm_c
        integer(c_int32_t), value :: maxn
        integer(c_int32_t), intent(out) :: neigh(*), pn(*), pv(*)   ! (nbody, maxn) like NEIGHBOURS / PN / PV
      end function
+     integer(c_int) function pibm_get_surface_points(h, bnd) bind(C, name="pibm_get_surface_points")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(out) :: bnd(*)                    ! (3, nbnd): direction of point l in bnd(1:3, l)
+     end function
      integer(c_int) function pibm_get_frame(h, frame_vel, frame_pos) bind(C, name="pibm_get_frame")
        import :: c_int, c_ptr, c_double
        type(c_ptr), value :: h

@@ -227,6 +227,11 @@ int  pibm_set_scalar(pibm_handle *h, const double *phif, const double *nlphif, c
  * (MAXNEIGHBORS = MN + 1 + NWALLS) always suffices; PIBM_ERR_ARG if a list
  * does not fit or the run has fixed particles.  Any pointer may be NULL. */
 int  pibm_get_contacts(pibm_handle *h, int32_t maxn, int32_t *neigh, int32_t *pn, int32_t *pv);
+/* Surface quadrature points (quadgener, geom_init.F90:44-242): bnd (nbnd, 3)
+ * row-major, the unit direction of point l.  Sphere m's surface point l sits
+ * at xc_m + radbdy*bnd_l and its inner and outer reversal points at
+ * xc_m + (radbdy -+ dr)*bnd_l (grid units). */
+int  pibm_get_surface_points(pibm_handle *h, double *bnd);
 /* Frame motion of a moving-particle run (IMOVE = 1): frame_vel(3), frame_pos(3)
  * of the reference (updated in velstep, steptheflow.F90:99-103; written to
  * RUN_NAME_sphere_config_N.rst, restart_funcs.F90:253-254, and read back on

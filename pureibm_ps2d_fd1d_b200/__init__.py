@@ -230,6 +230,12 @@ class Solver:
         b = np.ascontiguousarray(ufmean_des, dtype=np.float64)
         _check(load_library().pibm_set_desired_means(self.h, _dp(a), _dp(b)))
 
+    def get_surface_points(self) -> np.ndarray:
+        """(nbnd, 3) unit directions of the surface quadrature points."""
+        out = np.zeros((self.info.nbnd, 3))
+        _check(load_library().pibm_get_surface_points(self.h, _dp(out)))
+        return out
+
     def get_frame(self):
         """frame_vel(3), frame_pos(3) of a moving-particle run (0 and 1 for fixed spheres)."""
         fv, fp = np.zeros(3), np.zeros(3)

@@ -118,7 +118,7 @@ EXPORTED = [
     "pibm_get_fluid_mask", "pibm_get_contacts", "pibm_get_scalar_nl", "pibm_set_scalar",
     "pibm_set_desired_means", "pibm_adjoint_run", "pibm_adjoint_begin", "pibm_adjoint_step", "pibm_adjoint_end", "pibm_fp64_peak", "pibm_qdiv_check", "pibm_get_tuning", "pibm_set_tuning", "pibm_destroy", "pibm_last_error", "pibm_ff2rc", "pibm_ff2cr",
     "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time", "pibm_batch_member",
-    "pibm_batch_destroy", "pibm_get_frame", "pibm_set_frame",
+    "pibm_batch_destroy", "pibm_get_frame", "pibm_set_frame", "pibm_get_surface_points",
 ]
 
 
@@ -144,6 +144,7 @@ def bind(lib):
     lib.pibm_get_contacts.argtypes = [vp, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32)]
     lib.pibm_get_scalar_nl.argtypes = [vp, P(_f64)]
     lib.pibm_get_frame.argtypes = [vp, P(_f64), P(_f64)]
+    lib.pibm_get_surface_points.argtypes = [vp, P(_f64)]
     lib.pibm_set_frame.argtypes = [vp, P(_f64), P(_f64)]
     lib.pibm_set_scalar.argtypes = [vp, P(_f64), P(_f64), P(_f64)]
     lib.pibm_set_desired_means.argtypes = [vp, P(_f64), P(_f64)]
@@ -172,6 +173,6 @@ def bind(lib):
     for name in ("pibm_create", "pibm_info_get", "pibm_set_state", "pibm_step", "pibm_run", "pibm_run_timed", "pibm_run_profiled",
                  "pibm_kernel_times", "pibm_get_state", "pibm_get_particles", "pibm_get_scalar", "pibm_get_if_rev", "pibm_get_fluid_mask",
                  "pibm_get_contacts", "pibm_get_scalar_nl", "pibm_set_scalar", "pibm_set_desired_means",
-                 "pibm_get_frame", "pibm_set_frame", "pibm_adjoint_run", "pibm_adjoint_begin", "pibm_adjoint_step", "pibm_adjoint_end", "pibm_fp64_peak", "pibm_qdiv_check", "pibm_get_tuning", "pibm_set_tuning", "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
+                 "pibm_get_frame", "pibm_set_frame", "pibm_get_surface_points", "pibm_adjoint_run", "pibm_adjoint_begin", "pibm_adjoint_step", "pibm_adjoint_end", "pibm_fp64_peak", "pibm_qdiv_check", "pibm_get_tuning", "pibm_set_tuning", "pibm_ff2rc", "pibm_ff2cr", "pibm_ff2cr_noalloc", "pibm_batch_create", "pibm_batch_run", "pibm_batch_time"):
         getattr(lib, name).restype = C.c_int
     return lib

@@ -1049,6 +1049,14 @@ int pibm_set_scalar(pibm_handle *h, const double *phif, const double *nlphif, co
     return PIBM_OK;
 }
 
+// Unit directions of the surface quadrature points (quadgener,
+// geom_init.F90:44-242), (nbnd, 3) row-major.
+int pibm_get_surface_points(pibm_handle *h, double *bnd) {
+    if (!h || !bnd) return fail(PIBM_ERR_ARG, "null argument");
+    std::copy(h->S.bnd.begin(), h->S.bnd.end(), bnd);
+    return PIBM_OK;
+}
+
 // Frame motion of a moving-particle run (frame_vel, frame_pos of global_data;
 // updated in velstep, steptheflow.F90:99-103; restart records of
 // restart_funcs.F90:253-254, read back in initialize_flo.F90:1891-1898).

@@ -6,6 +6,7 @@
 #include <cstring>
 
 namespace pibm {
+int real_offset(int n, int z, int y);   // plane-transform order of a real node (kernels.cu)
 
 namespace {
 const double kSmall = (double)1.0E-35f;   // SMALL_NUMBER, a REAL(4) literal (constants.F90:92)
@@ -190,7 +191,7 @@ void build_if_rev(RunSetup &S) {
 // every node that receives force, with its contributing (point, corner) pairs in
 // the reference's accumulation order.  With include_frmeanfluid=F only solid
 // nodes receive force.
-void build_spread_map(RunSetup &S, bool all_nodes) {
+void build_spread_map(RunSetup &S, bool all_nodes, bool renumber) {
     const int N = S.nbody, nb = S.nbnd, nx = S.nx, my = S.my, mz = S.mz;
     S.pt_m.clear(); S.pt_l.clear();
     for (int m = 0; m < N; ++m)
@@ -217,6 +218,37 @@ void build_spread_map(RunSetup &S, bool all_nodes) {
                     if (!all_nodes && S.fluid[(size_t)node]) continue;
                     ent.push_back({node, p * 8 + ci + 2 * cj + 4 * ck});
                 }
+    }
+    if (renumber && np > 1) {
+        // Renumber the points in the memory order of their inner stencil's base
+        // corner (x plane, then the plane-transform order of (z, y)), so that
+        // the threads of a warp in the reversal-forcing kernel gather from
+        // neighbouring sectors and its point records land near those of the
+        // spreading gather.  Each node's contributions keep the reference's
+        // (sphere, point, corner) order: only the indices change.
+        const int rsp = my * (my + 2);
+        std::vector<long long> key((size_t)np);
+        for (int p = 0; p < np; ++p) {
+            const int m = S.pt_m[p], l = S.pt_l[p];
+            int c[3];
+            for (int d = 0; d < 3; ++d) c[d] = cell_index(S.xc[m + (size_t)d * N] + S.bnd[3 * l + d] * S.radibdy);
+            const int i = c[0] < 1 ? c[0] + nx : (c[0] > nx ? c[0] - nx : c[0]);
+            const int j = c[1] < 1 ? c[1] + my : (c[1] > my ? c[1] - my : c[1]);
+            const int k = c[2] < 1 ? c[2] + mz : (c[2] > mz ? c[2] - mz : c[2]);
+            key[(size_t)p] = (long long)(i - 1) * rsp + real_offset(my, k - 1, j - 1);
+        }
+        std::vector<int> ord((size_t)np), inv((size_t)np);
+        for (int p = 0; p < np; ++p) ord[(size_t)p] = p;
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return key[(size_t)a] < key[(size_t)b]; });
+        std::vector<int> pm((size_t)np), pl((size_t)np);
+        for (int t = 0; t < np; ++t) {
+            inv[(size_t)ord[(size_t)t]] = t;
+            pm[(size_t)t] = S.pt_m[(size_t)ord[(size_t)t]];
+            pl[(size_t)t] = S.pt_l[(size_t)ord[(size_t)t]];
+        }
+        S.pt_m.swap(pm);
+        S.pt_l.swap(pl);
+        for (auto &e : ent) e.second = inv[(size_t)(e.second >> 3)] * 8 + (e.second & 7);
     }
     std::stable_sort(ent.begin(), ent.end(), [](const std::pair<long long, int> &a, const std::pair<long long, int> &b) { return a.first < b.first; });
     S.sp_node.clear(); S.sp_ptr.clear(); S.sp_ent.clear();
@@ -384,7 +416,7 @@ bool setup_run(const pibm_params &prm, const pibm_particles *parts, RunSetup &S,
     if (prm.re < 1.0) dt_vis = prm.re * prm.dbydx * dt_conv / (prm.cfl * prm.vfl);
     build_neighbours(S);
     build_if_rev(S);
-    build_spread_map(S, prm.include_frmeanfluid != 0);
+    build_spread_map(S, prm.include_frmeanfluid != 0, prm.imove == 0);   // moving runs rebuild theirs every step
     double dt_diff = kLarge;
     if (prm.iscalon) {
         // initscal: SRC/SCALAR/scalar_init.F90:58-122

@@ -182,6 +182,26 @@ def test_adjoint_matches_oracle_at_64():
     assert np.max(np.abs(out["g_mpg"] - ref["g_mpg"])) <= 1e-8 * np.max(np.abs(ref["g_mpg"]))
 
 
+def test_adjoint_matches_oracle_on_the_gradient_configuration():
+    """The benchmarked gradient geometry (96^3, 30 spheres of d = 16, SET_MPG,
+    fixed dt): engine adjoint = oracle adjoint over 2 steps."""
+    prm, xc = config.adjoint_case()
+    parts = config.Particles(xc)
+    cpu = oc.OracleSolver(config.make_params(prm), parts.struct)
+    st = cpu.get_state()
+    st["umean"] = np.array(prm["umean0"])
+    cpu.set_state(st)
+    for _ in range(2):
+        cpu.step()
+    st = cpu.get_state()
+    K = 2
+    ref = cpu.adjoint(K, E)
+    out = _gpu(prm, xc, st).adjoint(K, E, checkpoint_every=1)
+    assert abs(out["J"] - ref["J"]) <= 1e-10 * abs(ref["J"])
+    assert np.max(np.abs(out["g_xc"] - ref["g_xc"])) <= 1e-8 * np.max(np.abs(ref["g_xc"]))
+    assert np.max(np.abs(out["g_mpg"] - ref["g_mpg"])) <= 1e-8 * np.max(np.abs(ref["g_mpg"]))
+
+
 def test_adjoint_matches_oracle_at_256():
     """256^3: the adjoint x-line solves run in 4-line tiles there."""
     prm, xc = config.adjoint_case(my=256, dia_cells=20.0, nbody=6, seed=3, mc_moves=20)
