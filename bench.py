@@ -264,9 +264,9 @@ def adjoint_gradient(nsteps: int = 200, checkpoint_every: int = 20, warm: int = 
     gradient for all 93 parameters.  J is piecewise
     smooth in xc: a stencil point crossing a grid cell face is a kink of the
     trilinear interpolation and a node entering the solid mask a jump, so each
-    coordinate's difference step (at most 1e-5 diameters) stays inside the
-    smooth piece around it (kinks.smooth_interval); coordinates whose piece is
-    narrower than 1e-8 diameters are listed as skipped."""
+    coordinate's fourth-order difference (steps up to 5e-6 diameters) stays
+    inside the smooth piece around it (kinks.smooth_interval); coordinates
+    whose piece is narrower than 1e-8 diameters are listed as skipped."""
     import ctypes as C
     import numpy as np
     import pureibm_ps2d_fd1d_b200 as pk
@@ -331,25 +331,36 @@ def adjoint_gradient(nsteps: int = 200, checkpoint_every: int = 20, warm: int = 
             t.close()
             return J / nsteps
         dia = 16.0
-        # the largest step the smooth piece allows, up to 1e-5 d: the forward
-        # runs at x + h and x - h round differently, and that noise (about
-        # |J| 1e-14 / h) shrinks as the step grows
-        h_max, h_min = 1e-5 * dia, 1e-8 * dia
+        # fourth-order central differences, f' = (-J(2h) + 8J(h) - 8J(-h) + J(-2h))/(12h),
+        # with [-2h, 2h] inside the smooth piece: its truncation error is
+        # negligible at h of a few 1e-6 d, where the rounding noise of the
+        # forward runs (about |J| 1e-14 / h) still is; second order where the
+        # piece is narrower than 2e-7 d
+        h_max, h_min = 5e-6 * dia, 1e-8 * dia
         gmax = float(np.max(np.abs(out["g_xc"])))
         checks, skipped = [], []
         for m in range(xc.shape[0]):
             for d in range(3):
-                h = kinks.fd_step(xc[m], d, bnd, R, float(prm.get("dr", 1.0)), h_max)
+                lo, hi = kinks.smooth_interval(xc[m], d, bnd, R, float(prm.get("dr", 1.0)))
+                half = min(-lo, hi)
+                h4 = min(h_max, 0.45 * half)
+                order = 4 if h4 >= 1e-7 * dia else 2
+                h = h4 if order == 4 else min(h_max, 0.9 * half)
                 if h < h_min:
-                    skipped.append({"param": "xc[%d,%d]" % (m, d), "smooth_half_width_diameters": h / dia})
+                    skipped.append({"param": "xc[%d,%d]" % (m, d), "smooth_half_width_diameters": half / dia})
                     continue
-                xp, xm = xc.copy(), xc.copy()
-                xp[m, d] += h
-                xm[m, d] -= h
-                f = (J_of(xp) - J_of(xm)) / (2 * h)
+
+                def J_at(t):
+                    x = xc.copy()
+                    x[m, d] += t
+                    return J_of(x)
+                if order == 4:
+                    f = (-J_at(2 * h) + 8 * J_at(h) - 8 * J_at(-h) + J_at(-2 * h)) / (12 * h)
+                else:
+                    f = (J_at(h) - J_at(-h)) / (2 * h)
                 a_ = float(out["g_xc"][m, d])
-                checks.append({"param": "xc[%d,%d]" % (m, d), "step_diameters": h / dia, "adjoint": a_, "fd": f,
-                               "rel_err": abs(a_ - f) / max(abs(f), 1e-300), "err_over_gmax": abs(a_ - f) / gmax})
+                checks.append({"param": "xc[%d,%d]" % (m, d), "step_diameters": h / dia, "order": order, "adjoint": a_,
+                               "fd": f, "rel_err": abs(a_ - f) / max(abs(f), 1e-300), "err_over_gmax": abs(a_ - f) / gmax})
         mp = np.array(prm["mpg"], dtype=np.float64)
         dm = 1e-6 * abs(mp[0])
         a, b = mp.copy(), mp.copy()
@@ -362,8 +373,8 @@ def adjoint_gradient(nsteps: int = 200, checkpoint_every: int = 20, warm: int = 
         big = [c for c in xcs if abs(c["fd"]) >= 1e-2 * gmax]
         big10 = [c for c in xcs if abs(c["fd"]) >= 1e-1 * gmax]
         res["fd_check"] = {
-            "method": "central differences inside the smooth piece of each coordinate (step <= 1e-5 d, and "
-                      ">= 1e-8 d or skipped), mpg_x at 1e-6 relative",
+            "method": "fourth-order central differences inside the smooth piece of each coordinate (step <= 5e-6 d; "
+                      "second order where the piece is narrower; skipped below 1e-8 d), mpg_x second order at 1e-6 relative",
             "parameters_checked": len(checks), "parameters_skipped": skipped,
             "max_rel_err": max(c["rel_err"] for c in checks),
             "max_rel_err_components_above_1pct_of_max": max(c["rel_err"] for c in big) if big else None,
@@ -638,10 +649,11 @@ def run_gpu(args):
             section("adjoint", adjoint_gradient)
         if not args.no_cpu_baseline:
             keys = ("value", "unit", "cores", "kind", "sample")
-            section("cpu_baseline", lambda: {k: v for k, v in cpu_baseline(prm, xc, steps=2, warmup=1).items() if k in keys})
+            # about 10-15 s of host work each: 20 steps on all threads, 4 on one
+            section("cpu_baseline", lambda: {k: v for k, v in cpu_baseline(prm, xc, steps=20, warmup=1).items() if k in keys})
             # the reference's own serial semantics: the same oracle on one thread
             section("cpu_baseline_1thread",
-                    lambda: {k: v for k, v in cpu_baseline(prm, xc, steps=1, warmup=0, threads=1).items() if k in keys})
+                    lambda: {k: v for k, v in cpu_baseline(prm, xc, steps=4, warmup=1, threads=1).items() if k in keys})
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

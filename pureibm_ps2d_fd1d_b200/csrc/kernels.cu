@@ -141,15 +141,18 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
 
 // compute_new_timestep's scalar tail (dependent_functions.F90:1137-1280).
 __global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *part) {
-    __shared__ double scr[32];
+    __shared__ double scr[32 * 3];
     __shared__ double red[6];
     if (sc->status) return;
-    for (int d = 0; d < 3; ++d) {
-        double a = 0.0, m = kSmallD;
-        for (int i = threadIdx.x; i < g.nx * g.plane_ctas; i += blockDim.x) { a += part[(size_t)i * 12 + d]; m = fmax(m, part[(size_t)i * 12 + 9 + d]); }
-        a = block_sum(a, scr);
-        m = block_max(m, scr);
-        if (threadIdx.x == 0) { red[d] = a; red[3 + d] = m; }
+    {
+        double a[3] = {0.0, 0.0, 0.0}, m[3] = {kSmallD, kSmallD, kSmallD};
+        for (int i = threadIdx.x; i < g.nx * g.plane_ctas; i += blockDim.x)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) { a[d] += part[(size_t)i * 12 + d]; m[d] = fmax(m[d], part[(size_t)i * 12 + 9 + d]); }
+        block_reduce_k<3>(a, scr);
+        block_reduce_k<3, true>(m, scr);
+        if (threadIdx.x == 0)
+            for (int d = 0; d < 3; ++d) { red[d] = a[d]; red[3 + d] = m[d]; }
     }
     __shared__ double vmean[3], upmax;
     if (g.moving) {
@@ -516,7 +519,7 @@ __global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ 
 // compute_mpg_at_n tail + bcset diagnostics (boundary_condition.F90:356-464, 701-884).
 __global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, double *visc, double *ptot,
                                                 double *force, const double *dpart) {
-    __shared__ double scr[32];
+    __shared__ double scr[32 * 9];
     __shared__ double tot[12];
     if (sc->status) return;
     const int NB = g.nbody;
@@ -528,11 +531,14 @@ __global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, d
         for (int d = 0; d < 3; ++d) { pres[m + d * NB] = -a[d]; ptot[m + d * NB] = a[d]; visc[m + d * NB] = b[d]; }
     }
     __syncthreads();
-    for (int d = 0; d < 3; ++d) {
-        double a = 0, b = 0, c = 0;
-        for (int m = threadIdx.x; m < NB; m += blockDim.x) { a += ptot[m + d * NB]; b += visc[m + d * NB]; c += pres[m + d * NB]; }
-        a = block_sum(a, scr); b = block_sum(b, scr); c = block_sum(c, scr);
-        if (threadIdx.x == 0) { tot[d] = a; tot[3 + d] = b; tot[6 + d] = c; }
+    {
+        double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // ptot, visc, pres sums per component
+        for (int m = threadIdx.x; m < NB; m += blockDim.x)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) { v[d] += ptot[m + d * NB]; v[3 + d] += visc[m + d * NB]; v[6 + d] += pres[m + d * NB]; }
+        block_reduce_k<9>(v, scr);
+        if (threadIdx.x == 0)
+            for (int q = 0; q < 9; ++q) tot[q] = v[q];
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -575,7 +581,7 @@ __global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, d
             force[m + d * NB] = f;
             fs[d] += f;
         }
-    for (int d = 0; d < 3; ++d) fs[d] = block_sum(fs[d], scr);
+    block_reduce_k<3>(fs, scr);
     if (threadIdx.x == 0) {
         double avg[3];
         for (int d = 0; d < 3; ++d) avg[d] = (fs[d] / NB) * g.mean_volfrac / g.mean_volfrac;
@@ -606,7 +612,7 @@ template <int N>
 __global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
                                                 const double *__restrict__ Q, const Scal *__restrict__ sc,
                                                 double *__restrict__ rec, double *__restrict__ ctb, double *__restrict__ blockpart) {
-    __shared__ double scr[32];
+    __shared__ double scr[32 * 6];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     double fm[3] = {0, 0, 0}, ffl[3] = {0, 0, 0};
     if (p < sc->npts && !sc->status) {
@@ -692,24 +698,25 @@ __global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict_
             r[3 + n] = count_so > 0 ? force_fl[n] / (double)count_so : 0.0;
         }
     }
-    for (int n = 0; n < 3; ++n) {
-        const double a = block_sum(fm[n], scr), b = block_sum(ffl[n], scr);
-        if (threadIdx.x == 0) { blockpart[(size_t)blockIdx.x * 6 + n] = a; blockpart[(size_t)blockIdx.x * 6 + 3 + n] = b; }
-    }
+    double v[6] = {fm[0], fm[1], fm[2], ffl[0], ffl[1], ffl[2]};
+    block_reduce_k<6>(v, scr);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 6; ++q) blockpart[(size_t)blockIdx.x * 6 + q] = v[q];
 }
 
 __global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *blockpart, int nblocks) {
-    __shared__ double scr[32];
+    __shared__ double scr[32 * 6];
     if (sc->status) return;
-    for (int q = 0; q < 6; ++q) {
-        double a = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) a += blockpart[(size_t)b * 6 + q];
-        a = block_sum(a, scr);
-        if (threadIdx.x == 0) {
-            if (q < 3) sc->frmean[q] = a / (double)g.ncell;
-            else sc->frmeanfluid[q - 3] = a / (double)sc->count_fluid;
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) a[q] += blockpart[(size_t)b * 6 + q];
+    block_reduce_k<6>(a, scr);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 6; ++q) {
+            if (q < 3) sc->frmean[q] = a[q] / (double)g.ncell;
+            else sc->frmeanfluid[q - 3] = a[q] / (double)sc->count_fluid;
         }
-    }
 }
 
 // k_spread: fr at every forced node, accumulated over its (point, corner)
@@ -722,6 +729,7 @@ __global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict_
     const int node = g.sp_node[q];
     double acc[3] = {0.0, 0.0, 0.0};
     const int e0 = g.sp_ptr[q], e1 = g.sp_ptr[q + 1];
+#pragma unroll 4
     for (int e = e0; e < e1; ++e) {
         const int ent = __ldg(g.sp_ent + e);
         const double *t = ctb + (size_t)ent * 3;

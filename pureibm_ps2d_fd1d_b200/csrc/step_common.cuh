@@ -70,6 +70,34 @@ __device__ __forceinline__ double block_sum(double v, double *scr) {
     __syncthreads();
     return r;
 }
+// K block sums (or maxima) at once, each with block_sum's (block_max's)
+// lane/warp tree, so every result is bitwise that of a separate call; two
+// barriers for all K instead of four each.  scr holds 32*K doubles.
+template <int K, bool kMax = false>
+__device__ __forceinline__ void block_reduce_k(double (&v)[K], double *scr) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_xor_sync(0xffffffffu, v[k], o);
+            v[k] = kMax ? fmax(v[k], t) : v[k] + t;
+        }
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) scr[k * 32 + w] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double r = lane < nw ? scr[k * 32 + lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double t = __shfl_xor_sync(0xffffffffu, r, o);
+            r = kMax ? fmax(r, t) : r + t;
+        }
+        v[k] = r;   // every warp computes the same tree: no third barrier
+    }
+    __syncthreads();
+}
 __device__ __forceinline__ double block_max(double v, double *scr) {
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
