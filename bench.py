@@ -415,8 +415,10 @@ def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024)
     per-realization loop on the same GPU: 16 seeded realizations (grids from
     {64, 96, 128}^3, phi ~ U[0.1, 0.4], d ~ U{12..20} cells, Re ~ U[10, 100]),
     `steps` steps of every member each way, device-timed: the plain loop as
-    each member replaying its own step graphs one after another, and the
-    batch graph.  Also the reference-style host loop (each member stepped in
+    each member replaying its own step graphs one after another; the batch
+    graph with every member's step its own branch; and the batch graph in
+    which the members of one grid size share each kernel launch (the default
+    batch path).  Also the reference-style host loop (each member stepped in
     turn through pibm_step with its report read back), wall-timed, since the
     steps are synchronous."""
     import pureibm_ps2d_fd1d_b200 as pk
@@ -426,6 +428,9 @@ def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024)
     b.run(warmup)
     cells = sum(p["my"] ** 3 for p, _, _ in ens) * steps
     t_plain = b.time(steps, sequential=True)
+    b.time(1, sequential=False, fused=False)
+    t_branch = b.time(steps, sequential=False, fused=False)
+    b.time(1, sequential=False)
     t_batch = b.time(steps, sequential=False)
     # the reference-style host loop: each realization stepped in turn through
     # the public per-step call (pibm_step, its report read back every step)
@@ -437,6 +442,7 @@ def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024)
     b.close()
     return {"unit": "Mcell-steps/s", "plain": cells / (t_plain / 1e3) / 1e6, "batched": cells / (t_batch / 1e3) / 1e6,
             "ratio": t_plain / t_batch,
+            "branches": cells / (t_branch / 1e3) / 1e6, "ratio_branches": t_plain / t_branch,
             "step_api_loop": cells / (t_api / 1e3) / 1e6, "ratio_vs_step_api_loop": t_api / t_batch,
             "members": n, "steps": steps, "seed": seed,
             "grids": [p["my"] for p, _, _ in ens], "nbody": [len(x) for _, x, _ in ens],

@@ -349,14 +349,19 @@ int  pibm_qdiv_check(const double *a, long long n, const double *b, int nb, long
  *      sample_inputs/set_mis_3d, run as one graph-captured launch stream) ---- */
 typedef struct pibm_batch pibm_batch;
 int  pibm_batch_create(int n, const pibm_params *prm, const pibm_particles *parts, pibm_batch **out);
-/* nsteps steps of every member: one CUDA graph launch per step, in which the
- * members' steps are independent branches that the GPU runs concurrently.
- * Members may also be stepped on their own between batch runs. */
+/* nsteps steps of every member: one CUDA graph launch per step.  Members
+ * with fixed spheres and no scalar that share the grid size and the scheme
+ * (AB2 or RK3) step through one launch per kernel, the members along
+ * gridDim.z; the other members' steps are independent branches that the GPU
+ * runs beside them.  Each member's results are bitwise those of stepping it
+ * alone.  Members may also be stepped on their own between batch runs. */
 int  pibm_batch_run(pibm_batch *b, int nsteps);
 /* Device time (CUDA events on the batch stream) of nsteps steps of every
- * member: sequential != 0 runs the plain per-realization loop (member after
+ * member: sequential == 1 runs the plain per-realization loop (member after
  * member, each replaying its own step graphs); sequential == 0 runs the batch
- * graph.  *ms = elapsed milliseconds; members advance nsteps steps either way. */
+ * graph; sequential == 2 runs a batch graph in which every member's step is
+ * its own branch (no shared launches).  *ms = elapsed milliseconds; members
+ * advance nsteps steps either way. */
 int  pibm_batch_time(pibm_batch *b, int nsteps, int sequential, double *ms);
 pibm_handle *pibm_batch_member(pibm_batch *b, int i);
 void pibm_batch_destroy(pibm_batch *b);

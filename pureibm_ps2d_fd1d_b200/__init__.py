@@ -269,8 +269,9 @@ class Solver:
 
 class Batch:
     """Independent realizations (e.g. a multiple-independent-simulation
-    ensemble) stepped together: one CUDA graph launch per step runs every
-    member's step as a concurrent branch (pibm_batch_*)."""
+    ensemble) stepped together: one CUDA graph launch per step; members of one
+    grid size with fixed spheres share each kernel launch, the others run as
+    concurrent branches (pibm_batch_*)."""
 
     def __init__(self, members):
         """members: list of (params, centres) pairs, as config.mis_ensemble makes them."""
@@ -290,11 +291,13 @@ class Batch:
     def run(self, nsteps: int):
         _check(load_library().pibm_batch_run(self.h, int(nsteps)))
 
-    def time(self, nsteps: int, sequential: bool) -> float:
+    def time(self, nsteps: int, sequential: bool, fused: bool = True) -> float:
         """Device milliseconds of nsteps steps of every member: the plain
-        per-realization loop (sequential) or the batch graph."""
+        per-realization loop (sequential) or the batch graph, with members of
+        one grid size sharing launches (fused) or each member its own branch."""
         ms = C.c_double()
-        _check(load_library().pibm_batch_time(self.h, int(nsteps), int(bool(sequential)), C.byref(ms)))
+        mode = 1 if sequential else (0 if fused else 2)
+        _check(load_library().pibm_batch_time(self.h, int(nsteps), mode, C.byref(ms)))
         return ms.value
 
     def close(self):

@@ -25,6 +25,9 @@ bool supported_size(int n);
 void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss,
                   cudaEvent_t *kev = nullptr);
 int kernels_per_step(const Geo &g, const Mov &m);
+void enqueue_batch_step(int n, const Member *d_mb, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
+                        cudaEvent_t fork, cudaEvent_t join);
+int batch_kernels_per_step(const BatchShape &bs);
 void enqueue_dem_init(const Mov &m, Scal *sc, cudaStream_t s);
 cudaError_t configure_moving_kernels(const Mov &m);
 void enqueue_c2r(const Geo &g, const double2 *a, double *b, int nplanes, cudaStream_t s);
@@ -82,6 +85,7 @@ struct pibm_handle {
     std::vector<void *> allocs;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    unsigned geo_ver = 0; // bumped whenever the Geo copies change (graphs hold them by value)
     int cur = 0;          // buffer index the next step writes its nonlinear term to
     int device = 0;
     double2 *stage = nullptr;   // reference-layout staging buffer of get/set_state (allocated once)
@@ -116,6 +120,13 @@ struct pibm_handle {
         for (void *q : allocs) cudaFree(q);
     }
 };
+
+// The step graphs hold the Geo copies by value: drop them after a change
+// (recaptured by the next pibm_run; batches compare geo_ver).
+static void drop_graphs(pibm_handle *h) {
+    for (auto &gx : h->graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+    ++h->geo_ver;
+}
 
 // Moving particles: DEM state on the device and the first neighbour search
 // of des_time_march(.TRUE.) (DES_INIT_ARRAYS positions, FIND_CELL_INDEX).
@@ -580,7 +591,7 @@ int pibm_set_state(pibm_handle *h, const pibm_state_view *s) {
         const int need = std::max(1, (int)(s->dt / m.dtsolid));
         if (need > m.max_factor) {
             m.max_factor = need;
-            for (auto &gx : h->graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+            drop_graphs(h);
         }
     }
     CUDA_OR_FAIL(cudaMemcpyAsync(h->b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, h->stream));
@@ -917,8 +928,7 @@ int pibm_set_tuning(pibm_handle *h, int32_t lines_per_cta) {
     if (lines_per_cta != kLinesTiles[0] && lines_per_cta != kLinesTiles[1]) return fail(PIBM_ERR_ARG, "x-line tile width must be 4 or 8");
     h->g.lines_lt = lines_per_cta;
     for (int k = 0; k < h->itrmax; ++k) h->gs[k].lines_lt = lines_per_cta;
-    for (auto &gx : h->graph)
-        if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }   // recaptured by the next pibm_run
+    drop_graphs(h);
     return PIBM_OK;
 }
 
@@ -988,7 +998,7 @@ int pibm_set_desired_means(pibm_handle *h, const double *usmean_des, const doubl
     if (!h || !usmean_des || !ufmean_des) return fail(PIBM_ERR_ARG, "null argument");
     for (Geo *g : {&h->g, &h->gs[0], &h->gs[1], &h->gs[2]})
         for (int d = 0; d < 3; ++d) { g->usmean_des[d] = usmean_des[d]; g->ufmean_des[d] = ufmean_des[d]; }
-    for (auto &gx : h->graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }   // kernels take Geo by value
+    drop_graphs(h);
     return PIBM_OK;
 }
 
@@ -1255,26 +1265,81 @@ int pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *d
 }
 
 // ---- batched independent realizations ----
-// All members step together through ONE CUDA graph per step parity: the graph
-// forks from the batch stream into every member's stream, runs one step of
-// each member as an independent branch, and joins back, so the GPU overlaps
-// the members' kernels (small grids leave most SMs idle when run alone).
+// All members step together through ONE CUDA graph per step parity.  Members
+// with fixed spheres and no scalar are grouped by grid size and scheme; a
+// group steps through one launch per kernel with its members along gridDim.z
+// (enqueue_batch_step), so a group of small grids fills the GPU the way one
+// large grid does.  Each group is a branch of the graph; the other members
+// run one step each as further branches (members whose plane kernels alone
+// fill the GPU, my >= 128, one after the other in one chain).
+struct BatchGroup {
+    int n = 0, itrmax = 1;
+    std::vector<int> idx;       // the members in the group, in batch order
+    BatchShape shape{};
+    size_t mb_off = 0;          // the group's Member arrays: [parity][stage][member]
+    cudaStream_t s = nullptr, side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, done = nullptr;
+};
+
 struct pibm_batch {
     std::vector<pibm_handle *> members;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     std::vector<int> base;      // each member's parity when the graphs were captured
+    std::vector<unsigned> ver;  // each member's geo_ver when the graphs were captured
     int flip = 0;               // graph[flip] is the next batch step
+    bool fused = true;          // the graphs use the fused group launches
+    bool captured_fused = true;
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> join;
+    std::vector<BatchGroup> groups;
+    std::vector<char> in_group;
+    Member *d_mb = nullptr;
     ~pibm_batch() {
         for (auto &gx : graph) if (gx) cudaGraphExecDestroy(gx);
         if (fork) cudaEventDestroy(fork);
         for (auto e : join) cudaEventDestroy(e);
+        for (auto &G : groups) {
+            for (cudaEvent_t e : {G.fork, G.join, G.done}) if (e) cudaEventDestroy(e);
+            for (cudaStream_t x : {G.s, G.side}) if (x) cudaStreamDestroy(x);
+        }
+        if (d_mb) cudaFree(d_mb);
         if (stream) cudaStreamDestroy(stream);
         for (auto *h : members) pibm_destroy(h);
     }
 };
+
+// Fused groups of a new batch: members with fixed spheres (or none) and no
+// scalar, keyed by grid size and stages per step; groups of one member stay
+// on the members' own step.
+static cudaError_t batch_groups(pibm_batch *bt) {
+    const int n = (int)bt->members.size();
+    bt->in_group.assign((size_t)n, 0);
+    for (int q = 0; q < n; ++q) {
+        const pibm_handle *h = bt->members[q];
+        if (h->g.moving || h->g.scal) continue;
+        BatchGroup *G = nullptr;
+        for (auto &x : bt->groups) if (x.n == h->g.my && x.itrmax == h->itrmax) G = &x;
+        if (!G) { bt->groups.emplace_back(); G = &bt->groups.back(); G->n = h->g.my; G->itrmax = h->itrmax; }
+        G->idx.push_back(q);
+    }
+    std::vector<BatchGroup> keep;
+    for (auto &G : bt->groups) if (G.idx.size() > 1) keep.push_back(G);
+    bt->groups.swap(keep);
+    size_t off = 0;
+    for (auto &G : bt->groups) {
+        for (int q : G.idx) bt->in_group[q] = 1;
+        G.mb_off = off;
+        off += (size_t)2 * G.itrmax * G.idx.size();
+        cudaError_t e;
+        if ((e = cudaStreamCreateWithFlags(&G.s, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = cudaStreamCreateWithFlags(&G.side, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        for (cudaEvent_t *ev : {&G.fork, &G.join, &G.done})
+            if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+    }
+    if (off) return cudaMalloc(&bt->d_mb, off * sizeof(Member));
+    return cudaSuccess;
+}
 
 int pibm_batch_create(int n, const pibm_params *prm, const pibm_particles *parts, pibm_batch **out) {
     if (n <= 0 || !prm || !out) return fail(PIBM_ERR_ARG, "bad argument");
@@ -1290,30 +1355,76 @@ int pibm_batch_create(int n, const pibm_params *prm, const pibm_particles *parts
     cudaError_t e = cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&bt->fork, cudaEventDisableTiming);
     for (int q = 0; q < n && e == cudaSuccess; ++q) e = cudaEventCreateWithFlags(&bt->join[q], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = batch_groups(bt);
     if (e != cudaSuccess) { delete bt; return fail(PIBM_ERR_CUDA, std::string("batch stream/events: ") + cudaGetErrorString(e)); }
     *out = bt;
     return PIBM_OK;
 }
 
-// (Re)capture the two batch graphs if any member's parity no longer matches them.
+// The Member arrays of every group for the members' current parities and
+// Geo copies (uploaded before capture; the graphs read them at run time).
+static int batch_members(pibm_batch *bt) {
+    std::vector<Member> mb;
+    for (auto &G : bt->groups) {
+        BatchShape &bs = G.shape;
+        bs = BatchShape{(int)G.idx.size(), 0, 0, 0, bt->members[G.idx[0]]->gs[0].lines_lt};
+        for (int par = 0; par < 2; ++par)
+            for (int k = 0; k < G.itrmax; ++k)
+                for (int q : G.idx) {
+                    pibm_handle *h = bt->members[q];
+                    Member m;
+                    std::memset(&m, 0, sizeof(m));
+                    m.g = h->gs[k];
+                    m.b = h->b;
+                    m.cur = bt->base[q] ^ par ^ (k & 1);
+                    m.nbk = h->g.nbody > 0 ? (h->g.npts + 255) / 256 : 0;
+                    mb.push_back(m);
+                    bs.max_nbody = std::max(bs.max_nbody, h->g.nbody);
+                    bs.max_nbk = std::max(bs.max_nbk, m.nbk);
+                    if (h->g.nbody > 0 && h->g.npts > 0) bs.max_spn = std::max(bs.max_spn, h->g.sp_nnodes);
+                }
+    }
+    if (!mb.empty()) CUDA_OR_FAIL(cudaMemcpy(bt->d_mb, mb.data(), mb.size() * sizeof(Member), cudaMemcpyHostToDevice));
+    return PIBM_OK;
+}
+
+// (Re)capture the two batch graphs if any member's parity or Geo no longer
+// matches them.
 static int batch_graphs(pibm_batch *bt) {
     const int n = (int)bt->members.size();
-    bool ok = bt->graph[0] && bt->graph[1] && (int)bt->base.size() == n;
-    for (int q = 0; ok && q < n; ++q) ok = bt->members[q]->cur == (bt->base[q] ^ bt->flip);
+    bool ok = bt->graph[0] && bt->graph[1] && (int)bt->base.size() == n && bt->captured_fused == bt->fused;
+    for (int q = 0; ok && q < n; ++q)
+        ok = bt->members[q]->cur == (bt->base[q] ^ bt->flip) && bt->members[q]->geo_ver == bt->ver[q];
     if (ok) return PIBM_OK;
     for (auto &gx : bt->graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
     bt->base.resize((size_t)n);
-    for (int q = 0; q < n; ++q) bt->base[q] = bt->members[q]->cur;
+    bt->ver.resize((size_t)n);
+    for (int q = 0; q < n; ++q) { bt->base[q] = bt->members[q]->cur; bt->ver[q] = bt->members[q]->geo_ver; }
     bt->flip = 0;
+    bt->captured_fused = bt->fused;
+    CUDA_OR_FAIL(cudaStreamSynchronize(bt->stream));
+    int rc = batch_members(bt);
+    if (rc) return rc;
     for (int par = 0; par < 2; ++par) {
         cudaGraph_t gr;
         CUDA_OR_FAIL(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
         CUDA_OR_FAIL(cudaEventRecord(bt->fork, bt->stream));
+        if (bt->fused)
+            for (auto &G : bt->groups) {
+                CUDA_OR_FAIL(cudaStreamWaitEvent(G.s, bt->fork, 0));
+                const size_t nz = G.idx.size();
+                for (int k = 0; k < G.itrmax; ++k)
+                    enqueue_batch_step(G.n, bt->d_mb + G.mb_off + ((size_t)par * G.itrmax + k) * nz, G.shape, G.s, G.side,
+                                       G.fork, G.join);
+                CUDA_OR_FAIL(cudaEventRecord(G.done, G.s));
+                CUDA_OR_FAIL(cudaStreamWaitEvent(bt->stream, G.done, 0));
+            }
         // members whose plane kernels alone fill the GPU (nx*C CTAs per transform item
         // of at least one per SM slot) form one chain, one after the other; the
         // smaller members run as parallel branches beside that chain
         int prev_big = -1;
         for (int q = 0; q < n; ++q) {
+            if (bt->fused && bt->in_group[q]) continue;
             pibm_handle *h = bt->members[q];
             const bool big = h->g.my >= 128;
             CUDA_OR_FAIL(cudaStreamWaitEvent(h->stream, (big && prev_big >= 0) ? bt->join[prev_big] : bt->fork, 0));
@@ -1358,9 +1469,10 @@ int pibm_batch_run(pibm_batch *bt, int nsteps) {
 }
 
 int pibm_batch_time(pibm_batch *bt, int nsteps, int sequential, double *ms) {
-    if (!bt || nsteps <= 0 || !ms) return fail(PIBM_ERR_ARG, "bad argument");
+    if (!bt || nsteps <= 0 || !ms || sequential < 0 || sequential > 2) return fail(PIBM_ERR_ARG, "bad argument");
     for (auto *h : bt->members)
         if (!h->graph[0] || !h->graph[1]) { int rc = pibm_run(h, 0, nullptr); if (rc) return rc; }
+    if (sequential != 1) bt->fused = sequential == 0;
     int rc = batch_graphs(bt);
     if (rc) return rc;
     cudaEvent_t e0, e1;
@@ -1378,6 +1490,7 @@ int pibm_batch_time(pibm_batch *bt, int nsteps, int sequential, double *ms) {
             }
     } else {
         rc = batch_enqueue(bt, nsteps);
+        bt->fused = true;
         if (rc) return rc;
     }
     CUDA_OR_FAIL(cudaEventRecord(e1, bt->stream));

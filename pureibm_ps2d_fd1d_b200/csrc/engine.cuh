@@ -116,6 +116,24 @@ struct DevBufs {
     Mov mov;   // moving particles (Geo::moving)
 };
 
+// One realization of a fused batch step (several runs of one grid size
+// stepped by the same kernel launches, one launch per kernel with the runs
+// along gridDim.z): its constants, its buffers, the nl buffer the step
+// writes (nl[cur]; onl = nl[cur ^ 1]) and its reversal-forcing block count.
+struct Member {
+    Geo g;
+    DevBufs b;
+    int cur;
+    int nbk;
+};
+
+// Launch extents of a fused batch step: runs in the group and the largest
+// sphere count, reversal-forcing block count and spreading node count among
+// them; the x-line tile width all of them use.
+struct BatchShape {
+    int nz, max_nbody, max_nbk, max_spn, lines_lt;
+};
+
 // Side streams of one run: after compute_new_timestep's scalars are known,
 // the drag quadrature (and mpg) and the passive-scalar step depend only on
 // the real fields of that step, so they run beside the nonlinear term (with

@@ -46,7 +46,7 @@ int moving_kernels_per_step(const Mov &m);
 // part[i*12 + q]: q 0-2 fluid sums, 3-5 solid sums, 6-8 all sums, 9-11 max |u|.
 // ============================================================================
 template <int N>
-__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
+__device__ __forceinline__ void b_a0(const Geo &g, const double2 *__restrict__ u, const double2 *__restrict__ p,
                                                    double *__restrict__ ubcp, double *__restrict__ pbcp,
                                                    double *__restrict__ omega, double *__restrict__ pgr,
                                                    Scal *__restrict__ sc, double *__restrict__ part) {
@@ -138,9 +138,14 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
         if (threadIdx.x == 0) { bulk_store(dst + roff, buf, L::RBYTES); bulk_wait_read(); }
     }
 }
+template <int N>
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
+                                                   double *__restrict__ ubcp, double *__restrict__ pbcp,
+                                                   double *__restrict__ omega, double *__restrict__ pgr,
+                                                   Scal *__restrict__ sc, double *__restrict__ part) { b_a0<N>(g, u, p, ubcp, pbcp, omega, pgr, sc, part); }
 
 // compute_new_timestep's scalar tail (dependent_functions.F90:1137-1280).
-__global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *part) {
+__device__ __forceinline__ void b_scal_a(const Geo &g, Scal *sc, const double *part) {
     __shared__ double scr[32 * 3];
     __shared__ double red[6];
     if (sc->status) return;
@@ -206,6 +211,7 @@ __global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *p
     if (sc->t < tempt) sc->cf = sc->cf * (sc->t / tempt);
     sc->divmax_bits = 0ull;
 }
+__global__ void __launch_bounds__(256) k_scal_a(Geo g, Scal *sc, const double *part) { b_scal_a(g, sc, part); }
 
 // ============================================================================
 // k_nl: nonlinear term -div(uu) of one plane (nl_allflow.F90:71-327, nl.F90:99-173).
@@ -286,7 +292,7 @@ __device__ __forceinline__ double xflux_diff(const Geo &g, const double *__restr
 // reference's order (cell 1's contribution first).  Center: (f(i+1)-f(i-1))/(2dx).
 // ============================================================================
 template <int N>
-__global__ void __launch_bounds__(256) k_flux(Geo g, const double *__restrict__ ubcp, double *__restrict__ Dx,
+__device__ __forceinline__ void b_flux(const Geo &g, const double *__restrict__ ubcp, double *__restrict__ Dx,
                                               const Scal *__restrict__ sc) {
     constexpr int RSP = RP<N>::RSP, SEG = 32;
     const int nx = g.nx, nseg = nx / SEG;
@@ -358,9 +364,12 @@ __global__ void __launch_bounds__(256) k_flux(Geo g, const double *__restrict__ 
         for (int c = 0; c < 3; ++c) { w[c][0] = w[c][1]; w[c][1] = w[c][2]; w[c][2] = w[c][3]; sl[c][0] = sl[c][1]; }
     }
 }
+template <int N>
+__global__ void __launch_bounds__(256) k_flux(Geo g, const double *__restrict__ ubcp, double *__restrict__ Dx,
+                                              const Scal *__restrict__ sc) { b_flux<N>(g, ubcp, Dx, sc); }
 
 template <int N>
-__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const double *__restrict__ ubcp, const double *__restrict__ Dx,
+__device__ __forceinline__ void b_nl(const Geo &g, const double *__restrict__ ubcp, const double *__restrict__ Dx,
                                                    const double2 *__restrict__ u,
                                                    const double2 *__restrict__ onl, double2 *__restrict__ nl_new,
                                                    double *__restrict__ Q, Scal *__restrict__ sc) {
@@ -471,6 +480,11 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const doubl
         if (threadIdx.x == 0) { bulk_store(Q + ((size_t)c * nx + i) * RS + roff, buf, L::RBYTES); bulk_wait_read(); }
     }
 }
+template <int N>
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const double *__restrict__ ubcp, const double *__restrict__ Dx,
+                                                   const double2 *__restrict__ u,
+                                                   const double2 *__restrict__ onl, double2 *__restrict__ nl_new,
+                                                   double *__restrict__ Q, Scal *__restrict__ sc) { b_nl<N>(g, ubcp, Dx, u, onl, nl_new, Q, sc); }
 
 // ============================================================================
 // k_drag: per-sphere pressure and viscous force from the surface quadrature
@@ -478,7 +492,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_nl(Geo g, const doubl
 // ============================================================================
 
 template <int N>
-__global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ pbcp, const double *__restrict__ omega,
+__device__ __forceinline__ void b_drag(const Geo &g, const double *__restrict__ pbcp, const double *__restrict__ omega,
                                               double *__restrict__ dpart, const Scal *__restrict__ sc) {
     __shared__ double scr[32];
     const int m = blockIdx.x / kDragSplit, part = blockIdx.x % kDragSplit;
@@ -515,9 +529,12 @@ __global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ 
         if (threadIdx.x == 0) { dpart[(size_t)blockIdx.x * 6 + d] = a; dpart[(size_t)blockIdx.x * 6 + 3 + d] = b; }
     }
 }
+template <int N>
+__global__ void __launch_bounds__(256) k_drag(Geo g, const double *__restrict__ pbcp, const double *__restrict__ omega,
+                                              double *__restrict__ dpart, const Scal *__restrict__ sc) { b_drag<N>(g, pbcp, omega, dpart, sc); }
 
 // compute_mpg_at_n tail + bcset diagnostics (boundary_condition.F90:356-464, 701-884).
-__global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, double *visc, double *ptot,
+__device__ __forceinline__ void b_scal_b(const Geo &g, Scal *sc, double *pres, double *visc, double *ptot,
                                                 double *force, const double *dpart) {
     __shared__ double scr[32 * 9];
     __shared__ double tot[12];
@@ -594,6 +611,8 @@ __global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, d
         if (sc->norm_drag > 1.0e6) sc->status = PIBM_ERR_BLOWUP;
     }
 }
+__global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, double *visc, double *ptot,
+                                                double *force, const double *dpart) { b_scal_b(g, sc, pres, visc, ptot, force, dpart); }
 
 // ============================================================================
 // k_rev: direct forcing at the inner reversal points
@@ -609,7 +628,7 @@ __device__ __forceinline__ void inner_point(const Geo &g, int m, int l, double x
 }
 
 template <int N>
-__global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
+__device__ __forceinline__ void b_rev(const Geo &g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
                                                 const double *__restrict__ Q, const Scal *__restrict__ sc,
                                                 double *__restrict__ rec, double *__restrict__ ctb, double *__restrict__ blockpart) {
     __shared__ double scr[32 * 6];
@@ -703,8 +722,12 @@ __global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict_
     if (threadIdx.x == 0)
         for (int q = 0; q < 6; ++q) blockpart[(size_t)blockIdx.x * 6 + q] = v[q];
 }
+template <int N>
+__global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
+                                                const double *__restrict__ Q, const Scal *__restrict__ sc,
+                                                double *__restrict__ rec, double *__restrict__ ctb, double *__restrict__ blockpart) { b_rev<N>(g, ubcp, pgr, Q, sc, rec, ctb, blockpart); }
 
-__global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *blockpart, int nblocks) {
+__device__ __forceinline__ void b_scal_c(const Geo &g, Scal *sc, const double *blockpart, int nblocks) {
     __shared__ double scr[32 * 6];
     if (sc->status) return;
     double a[6] = {0, 0, 0, 0, 0, 0};
@@ -718,11 +741,12 @@ __global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *b
             else sc->frmeanfluid[q - 3] = a[q] / (double)sc->count_fluid;
         }
 }
+__global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *blockpart, int nblocks) { b_scal_c(g, sc, blockpart, nblocks); }
 
 // k_spread: fr at every forced node, accumulated over its (point, corner)
 // contributions in the reference's (sphere, point) order
 // (boundary_condition.F90:1425-1462).  sp_node holds physical offsets.
-__global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, const double *__restrict__ ctb,
+__device__ __forceinline__ void b_spread(const Geo &g, const double *__restrict__ rec, const double *__restrict__ ctb,
                                                 double *__restrict__ fr, const Scal *__restrict__ sc) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.sp_nnodes || sc->status) return;
@@ -746,10 +770,12 @@ __global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict_
 #pragma unroll
     for (int n = 0; n < 3; ++n) fr[n * CR + node] = acc[n];
 }
+__global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, const double *__restrict__ ctb,
+                                                double *__restrict__ fr, const Scal *__restrict__ sc) { b_spread(g, rec, ctb, fr, sc); }
 
 // k_ff: ff = r2c(fr - frmean) (boundary_condition.F90:678-700).
 template <int N>
-__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
+__device__ __forceinline__ void b_ff(const Geo &g, const double *__restrict__ fr, double2 *__restrict__ ff,
                                                    Scal *__restrict__ sc) {
     using L = PL<N>;
     extern __shared__ double2 sm[];
@@ -785,6 +811,9 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const doubl
         }
     }
 }
+template <int N>
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const double *__restrict__ fr, double2 *__restrict__ ff,
+                                                   Scal *__restrict__ sc) { b_ff<N>(g, fr, ff, sc); }
 
 // ============================================================================
 // k_lines: pressure -> ustep -> divcorr for a tile of LT (ky,kz) lines per CTA
@@ -804,7 +833,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff(Geo g, const doubl
 // consecutive lines (contiguous in the [i][k][j] layout).
 // ============================================================================
 template <int NX, int LT>
-__global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ u, double2 *__restrict__ p,
+__device__ __forceinline__ void b_lines(const Geo &g, double2 *__restrict__ u, double2 *__restrict__ p,
                                                    const double2 *__restrict__ nl, const double2 *__restrict__ onl,
                                                    const double2 *__restrict__ ff, Scal *__restrict__ sc) {
     constexpr int R = NX / 32;
@@ -1041,6 +1070,10 @@ __global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ 
     }
     if (!ok) atomicCAS(&sc->status, 0, PIBM_ERR_PIVOT);
 }
+template <int NX, int LT>
+__global__ void __launch_bounds__(LT * 32) k_lines(Geo g, double2 *__restrict__ u, double2 *__restrict__ p,
+                                                   const double2 *__restrict__ nl, const double2 *__restrict__ onl,
+                                                   const double2 *__restrict__ ff, Scal *__restrict__ sc) { b_lines<NX, LT>(g, u, p, nl, onl, ff, sc); }
 
 // x-line tile width (lines per CTA): 4 or 8, chosen per run by autotune_lines
 // (a run that was not tuned takes the default below).
@@ -1059,7 +1092,7 @@ static void launch_lines(const Geo &g, DevBufs &b, double2 *u, double2 *p, int c
 }
 
 // velstep tail: umean update (steptheflow.F90:99) and the NaN check.
-__global__ void k_scal_d(Geo g, Scal *sc) {
+__device__ __forceinline__ void b_scal_d(const Geo &g, Scal *sc) {
     if (threadIdx.x != 0 || sc->status) return;
     for (int d = 0; d < 3; ++d) sc->umean[d] = sc->umean[d] + (-sc->mpg[d] + sc->frmean[d] - sc->frame_accln[d]) * sc->dt;
     if (g.moving)
@@ -1071,6 +1104,7 @@ __global__ void k_scal_d(Geo g, Scal *sc) {
     if (!(dm == dm) || !(sc->umean[0] == sc->umean[0]) || !(sc->mpg[0] == sc->mpg[0])) sc->status = PIBM_ERR_NAN;
     sc->nsteps += 1;
 }
+__global__ void k_scal_d(Geo g, Scal *sc) { b_scal_d(g, sc); }
 
 // ============================================================================
 // Layout conversion between the reference's Fortran arrays and the device
@@ -1163,6 +1197,124 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff2rc(Geo g, const do
 }
 
 // ============================================================================
+// Fused batch step: the kernels of one time step for every run of a batch
+// that has the same grid size, one launch per kernel, the runs along
+// gridDim.z (Member array in device memory).  Each run's blocks execute the
+// same device code as its own launches, so its results are bitwise those of
+// stepping it alone.  Launches are sized for the largest run of the group;
+// blocks beyond a run's own extent return at once.
+// ============================================================================
+template <int N>
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_a0(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    b_a0<N>(m.g, m.b.u, m.b.p, m.b.ubcp, m.b.pbcp, m.b.omega, m.b.pgr, m.b.sc, m.b.part);
+}
+__global__ void __launch_bounds__(256) kb_scal_a(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    b_scal_a(m.g, m.b.sc, m.b.part);
+}
+template <int N>
+__global__ void __launch_bounds__(256) kb_flux(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    b_flux<N>(m.g, m.b.ubcp, m.b.Dx, m.b.sc);
+}
+template <int N>
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_nl(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    b_nl<N>(m.g, m.b.ubcp, m.b.Dx, m.b.u, m.b.nl[m.cur ^ 1], m.b.nl[m.cur], m.b.Q, m.b.sc);
+}
+template <int N>
+__global__ void __launch_bounds__(256) kb_drag(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    if ((int)blockIdx.x >= m.g.nbody * kDragSplit) return;
+    b_drag<N>(m.g, m.b.pbcp, m.b.omega, m.b.dpart, m.b.sc);
+}
+__global__ void __launch_bounds__(256) kb_scal_b(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    if (m.g.nbody == 0) return;
+    b_scal_b(m.g, m.b.sc, m.b.pres, m.b.visc, m.b.ptot, m.b.force, m.b.dpart);
+}
+template <int N>
+__global__ void __launch_bounds__(256, 3) kb_rev(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    if (m.g.nbody == 0 || m.g.npts == 0 || (int)blockIdx.x >= m.nbk) return;
+    b_rev<N>(m.g, m.b.ubcp, m.b.pgr, m.b.Q, m.b.sc, m.b.rec, m.b.ctb, m.b.blockpart);
+}
+__global__ void __launch_bounds__(256) kb_scal_c(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    if (m.g.nbody == 0 || m.g.npts == 0) return;
+    b_scal_c(m.g, m.b.sc, m.b.blockpart, m.nbk);
+}
+__global__ void __launch_bounds__(256) kb_spread(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    if (m.g.nbody == 0 || m.g.npts == 0) return;
+    b_spread(m.g, m.b.rec, m.b.ctb, m.b.fr, m.b.sc);
+}
+template <int N>
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_ff(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    if (m.g.nbody == 0) return;
+    b_ff<N>(m.g, m.b.fr, m.b.ff, m.b.sc);
+}
+template <int N, int LT>
+__global__ void __launch_bounds__(LT * 32) kb_lines(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    b_lines<N, LT>(m.g, m.b.u, m.b.p, m.b.nl[m.cur], m.b.nl[m.cur ^ 1], m.b.ff, m.b.sc);
+}
+__global__ void kb_scal_d(const Member *__restrict__ mb) {
+    const Member &m = mb[blockIdx.z];
+    b_scal_d(m.g, m.b.sc);
+}
+
+// One fused step of nz runs of size N (members d_mb[0..nz-1]): the drag and
+// mpg kernels on `side` beside the nonlinear term, as in a single run's graph.
+template <int N>
+static void enqueue_batch_step_t(const Member *d_mb, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
+                                 cudaEvent_t fork, cudaEvent_t join) {
+    const int nz = bs.nz;
+    launch_planes_z<N>(kb_a0<N>, N, 10, nz, s, d_mb);
+    kb_scal_a<<<dim3(1, 1, nz), 256, 0, s>>>(d_mb);
+    const bool spheres = bs.max_nbody > 0;
+    if (spheres) {
+        cudaEventRecord(fork, s);
+        cudaStreamWaitEvent(side, fork, 0);
+        kb_drag<N><<<dim3(bs.max_nbody * kDragSplit, 1, nz), 256, 0, side>>>(d_mb);
+        kb_scal_b<<<dim3(1, 1, nz), 256, 0, side>>>(d_mb);
+        cudaEventRecord(join, side);
+    }
+    kb_flux<N><<<dim3((RP<N>::RSP * (N / 32) + 255) / 256, 1, nz), 256, 0, s>>>(d_mb);
+    launch_planes_z<N>(kb_nl<N>, N, 3, nz, s, d_mb);
+    if (spheres) {
+        cudaStreamWaitEvent(s, join, 0);
+        if (bs.max_nbk > 0) {
+            kb_rev<N><<<dim3(bs.max_nbk, 1, nz), 256, 0, s>>>(d_mb);
+            kb_scal_c<<<dim3(1, 1, nz), 256, 0, s>>>(d_mb);
+            if (bs.max_spn > 0) kb_spread<<<dim3((bs.max_spn + 255) / 256, 1, nz), 256, 0, s>>>(d_mb);
+        }
+        launch_planes_z<N>(kb_ff<N>, N, 3, nz, s, d_mb);
+    }
+    const int PS = (N / 2 + 1) * N;
+    if (bs.lines_lt == 4) kb_lines<N, 4><<<dim3((PS + 3) / 4, 1, nz), 4 * 32, lines_smem<N>(4), s>>>(d_mb);
+    else kb_lines<N, 8><<<dim3((PS + 7) / 8, 1, nz), 8 * 32, lines_smem<N>(8), s>>>(d_mb);
+    kb_scal_d<<<dim3(1, 1, nz), 32, 0, s>>>(d_mb);
+}
+
+void enqueue_batch_step(int n, const Member *d_mb, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
+                        cudaEvent_t fork, cudaEvent_t join) {
+    switch (n) {
+        case 32: enqueue_batch_step_t<32>(d_mb, bs, s, side, fork, join); break;
+        case 64: enqueue_batch_step_t<64>(d_mb, bs, s, side, fork, join); break;
+        case 96: enqueue_batch_step_t<96>(d_mb, bs, s, side, fork, join); break;
+        case 128: enqueue_batch_step_t<128>(d_mb, bs, s, side, fork, join); break;
+        case 256: enqueue_batch_step_t<256>(d_mb, bs, s, side, fork, join); break;
+    }
+}
+// Kernels one fused batch step launches.
+int batch_kernels_per_step(const BatchShape &bs) {
+    return 6 + (bs.max_nbody > 0 ? 3 + (bs.max_nbk > 0 ? 2 + (bs.max_spn > 0 ? 1 : 0) : 0) : 0);
+}
+
+// ============================================================================
 // Host-side launch helpers
 // ============================================================================
 template <int N>
@@ -1176,6 +1328,11 @@ static cudaError_t set_attrs() {
     if ((e = cudaFuncSetAttribute(k_ff2rc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_lines<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>(4))) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_lines<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>(8))) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(kb_a0<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(kb_nl<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(kb_ff<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(kb_lines<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>(4))) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(kb_lines<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>(8))) != cudaSuccess) return e;
     return cudaSuccess;
 }
 

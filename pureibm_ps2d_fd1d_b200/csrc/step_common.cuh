@@ -207,6 +207,24 @@ inline void launch_planes(void (*k)(KArgs...), int nplanes, int items, cudaStrea
 }
 
 
+// launch_planes for a fused batch: nz runs of the same size along gridDim.z.
+template <int N, typename... KArgs, typename... Args>
+inline void launch_planes_z(void (*k)(KArgs...), int nplanes, int items, int nz, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(nplanes * PL<N>::C), (unsigned)items, (unsigned)nz);
+    cfg.blockDim = dim3(PL<N>::T, 1, 1);
+    cfg.dynamicSmemBytes = plane_smem<N>();
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = PL<N>::C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // Tile row pitch of the x-line kernels' [line][i] tiles (double2 elements).  A 16-byte shared access is
 // served per 8 threads (128 bytes = 8 slots of 4 banks); the element loops put
 // thread t on (line t % LT, plane t / LT), so 8 threads cover 8 lines of one
