@@ -410,20 +410,14 @@ def single_sphere(steps: int = 100, warmup: int = 5):
     return out
 
 
-def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024):
-    """Batched multiple-independent-simulation throughput against the plain
-    per-realization loop on the same GPU: 16 seeded realizations (grids from
-    {64, 96, 128}^3, phi ~ U[0.1, 0.4], d ~ U{12..20} cells, Re ~ U[10, 100]),
-    `steps` steps of every member each way, device-timed: the plain loop as
-    each member replaying its own step graphs one after another; the batch
-    graph with every member's step its own branch; and the batch graph in
-    which the members of one grid size share each kernel launch (the default
-    batch path).  Also the reference-style host loop (each member stepped in
-    turn through pibm_step with its report read back), wall-timed, since the
-    steps are synchronous."""
+def _mis_times(ens, steps: int, warmup: int, api_loop: bool):
+    """Device ms of `steps` steps of every member of ensemble `ens`: the plain
+    per-realization loop (each member replaying its own step graphs, one after
+    another), the batch graph with every member's step its own branch, and the
+    batch graph in which members of one grid size share each kernel launch;
+    with api_loop also the reference-style host loop (each member stepped in
+    turn through pibm_step, its report read back every step), wall-timed."""
     import pureibm_ps2d_fd1d_b200 as pk
-    from pureibm_ps2d_fd1d_b200 import config
-    ens = config.mis_ensemble(n=n, seed=seed)
     b = pk.Batch([(p, x) for p, x, _ in ens])
     b.run(warmup)
     cells = sum(p["my"] ** 3 for p, _, _ in ens) * steps
@@ -432,21 +426,45 @@ def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024)
     t_branch = b.time(steps, sequential=False, fused=False)
     b.time(1, sequential=False)
     t_batch = b.time(steps, sequential=False)
-    # the reference-style host loop: each realization stepped in turn through
-    # the public per-step call (pibm_step, its report read back every step)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        for m in b.members:
-            m.step(1)
-    t_api = (time.perf_counter() - t0) * 1e3
+    out = {"plain": cells / (t_plain / 1e3) / 1e6, "batched": cells / (t_batch / 1e3) / 1e6,
+           "ratio": t_plain / t_batch,
+           "branches": cells / (t_branch / 1e3) / 1e6, "ratio_branches": t_plain / t_branch,
+           "ms_per_step": {"plain": t_plain / steps, "branches": t_branch / steps, "batched": t_batch / steps}}
+    if api_loop:
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for m in b.members:
+                m.step(1)
+        t_api = (time.perf_counter() - t0) * 1e3
+        out.update({"step_api_loop": cells / (t_api / 1e3) / 1e6, "ratio_vs_step_api_loop": t_api / t_batch})
     b.close()
-    return {"unit": "Mcell-steps/s", "plain": cells / (t_plain / 1e3) / 1e6, "batched": cells / (t_batch / 1e3) / 1e6,
-            "ratio": t_plain / t_batch,
-            "branches": cells / (t_branch / 1e3) / 1e6, "ratio_branches": t_plain / t_branch,
-            "step_api_loop": cells / (t_api / 1e3) / 1e6, "ratio_vs_step_api_loop": t_api / t_batch,
-            "members": n, "steps": steps, "seed": seed,
-            "grids": [p["my"] for p, _, _ in ens], "nbody": [len(x) for _, x, _ in ens],
-            "phi": [round(f, 4) for _, _, f in ens]}
+    return out
+
+
+def batched_mis(steps: int = 10, warmup: int = 3, n: int = 16, seed: int = 2024, sweep: bool = False):
+    """Batched multiple-independent-simulation throughput against the plain
+    per-realization loop on the same GPU (_mis_times): 16 seeded realizations
+    (grids from {64, 96, 128}^3, phi ~ U[0.1, 0.4], d ~ U{12..20} cells,
+    Re ~ U[10, 100]), `steps` steps of every member each way, device-timed;
+    and the same for two small-grid ensembles of 16 (all 32^3; 32^3 and 64^3
+    mixed), where one member alone leaves most SMs idle; with sweep also
+    one-size ensembles of each grid size (seed 7)."""
+    from pureibm_ps2d_fd1d_b200 import config
+    ens = config.mis_ensemble(n=n, seed=seed)
+    out = {"unit": "Mcell-steps/s", **_mis_times(ens, steps, warmup, api_loop=True),
+           "members": n, "steps": steps, "seed": seed,
+           "grids": [p["my"] for p, _, _ in ens], "nbody": [len(x) for _, x, _ in ens],
+           "phi": [round(f, 4) for _, _, f in ens]}
+    for key, grids in (("small_grids_32", (32,)), ("small_grids_32_64", (32, 64))):
+        e = config.mis_ensemble(n=16, seed=7, grids=grids)
+        out[key] = {**_mis_times(e, steps, warmup, api_loop=False), "members": 16, "seed": 7,
+                    "grids": [p["my"] for p, _, _ in e], "nbody": [len(x) for _, x, _ in e]}
+    if sweep:
+        for g, m in ((64, 8), (96, 8), (128, 4)):
+            e = config.mis_ensemble(n=m, seed=7, grids=(g,))
+            out[f"one_size_{g}"] = {**_mis_times(e, steps, warmup, api_loop=False), "members": m, "seed": 7,
+                                    "nbody": [len(x) for _, x, _ in e]}
+    return out
 
 
 def run_reference(args):
@@ -677,9 +695,16 @@ def main():
     ap.add_argument("--no-scalar", action="store_true", help="skip the flow + passive-scalar measurement")
     ap.add_argument("--no-moving", action="store_true", help="skip the moving-particle suspension measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) measurement")
+    ap.add_argument("--mis-only", action="store_true",
+                    help="print only the batched-realization measurement (steps and warm-up from --steps/--warmup)")
+    ap.add_argument("--mis-sweep", action="store_true",
+                    help="with --mis-only: also one-size ensembles (sixteen 32^3, eight 64^3, eight 96^3, four 128^3)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mis_only:
+        print(json.dumps(batched_mis(steps=args.steps, warmup=args.warmup, sweep=args.mis_sweep)))
+        return 0
     return run_gpu(args)
 
 

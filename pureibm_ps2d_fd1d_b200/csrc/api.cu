@@ -25,7 +25,7 @@ bool supported_size(int n);
 void enqueue_step(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cudaEvent_t *ev, const StepStreams *ss,
                   cudaEvent_t *kev = nullptr);
 int kernels_per_step(const Geo &g, const Mov &m);
-void enqueue_batch_step(int n, const Member *d_mb, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
+void enqueue_batch_step(int n, const MemberSet &ms, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
                         cudaEvent_t fork, cudaEvent_t join);
 int batch_kernels_per_step(const BatchShape &bs);
 void enqueue_dem_init(const Mov &m, Scal *sc, cudaStream_t s);
@@ -1269,16 +1269,16 @@ int pibm_ff2cr_noalloc(int my, int mz, int nplanes, const double *d_a, double *d
 // with fixed spheres and no scalar are grouped by grid size and scheme; a
 // group steps through one launch per kernel with its members along gridDim.z
 // (enqueue_batch_step), so a group of small grids fills the GPU the way one
-// large grid does.  Each group is a branch of the graph; the other members
-// run one step each as further branches (members whose plane kernels alone
-// fill the GPU, my >= 128, one after the other in one chain).
+// large grid does.  The groups run one after another; then the other members
+// run one step each as branches of the graph (members whose plane kernels
+// alone fill the GPU, my >= 128, one after the other in one chain).
 struct BatchGroup {
     int n = 0, itrmax = 1;
     std::vector<int> idx;       // the members in the group, in batch order
     BatchShape shape{};
-    size_t mb_off = 0;          // the group's Member arrays: [parity][stage][member]
-    cudaStream_t s = nullptr, side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr, done = nullptr;
+    std::vector<MemberSet> sets;   // the launches' members: [parity][stage]
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 struct pibm_batch {
@@ -1294,24 +1294,22 @@ struct pibm_batch {
     std::vector<cudaEvent_t> join;
     std::vector<BatchGroup> groups;
     std::vector<char> in_group;
-    Member *d_mb = nullptr;
     ~pibm_batch() {
         for (auto &gx : graph) if (gx) cudaGraphExecDestroy(gx);
         if (fork) cudaEventDestroy(fork);
         for (auto e : join) cudaEventDestroy(e);
         for (auto &G : groups) {
-            for (cudaEvent_t e : {G.fork, G.join, G.done}) if (e) cudaEventDestroy(e);
-            for (cudaStream_t x : {G.s, G.side}) if (x) cudaStreamDestroy(x);
+            for (cudaEvent_t e : {G.fork, G.join}) if (e) cudaEventDestroy(e);
+            if (G.side) cudaStreamDestroy(G.side);
         }
-        if (d_mb) cudaFree(d_mb);
         if (stream) cudaStreamDestroy(stream);
         for (auto *h : members) pibm_destroy(h);
     }
 };
 
 // Fused groups of a new batch: members with fixed spheres (or none) and no
-// scalar, keyed by grid size and stages per step; groups of one member stay
-// on the members' own step.
+// scalar, keyed by grid size and stages per step, at most kFuseMax members
+// per group; groups of one member stay on the members' own step.
 static cudaError_t batch_groups(pibm_batch *bt) {
     const int n = (int)bt->members.size();
     bt->in_group.assign((size_t)n, 0);
@@ -1319,25 +1317,22 @@ static cudaError_t batch_groups(pibm_batch *bt) {
         const pibm_handle *h = bt->members[q];
         if (h->g.moving || h->g.scal) continue;
         BatchGroup *G = nullptr;
-        for (auto &x : bt->groups) if (x.n == h->g.my && x.itrmax == h->itrmax) G = &x;
+        for (auto &x : bt->groups)
+            if (x.n == h->g.my && x.itrmax == h->itrmax && (int)x.idx.size() < kFuseMax) G = &x;
         if (!G) { bt->groups.emplace_back(); G = &bt->groups.back(); G->n = h->g.my; G->itrmax = h->itrmax; }
         G->idx.push_back(q);
     }
     std::vector<BatchGroup> keep;
     for (auto &G : bt->groups) if (G.idx.size() > 1) keep.push_back(G);
     bt->groups.swap(keep);
-    size_t off = 0;
     for (auto &G : bt->groups) {
         for (int q : G.idx) bt->in_group[q] = 1;
-        G.mb_off = off;
-        off += (size_t)2 * G.itrmax * G.idx.size();
+        G.sets.resize((size_t)2 * G.itrmax);
         cudaError_t e;
-        if ((e = cudaStreamCreateWithFlags(&G.s, cudaStreamNonBlocking)) != cudaSuccess) return e;
         if ((e = cudaStreamCreateWithFlags(&G.side, cudaStreamNonBlocking)) != cudaSuccess) return e;
-        for (cudaEvent_t *ev : {&G.fork, &G.join, &G.done})
+        for (cudaEvent_t *ev : {&G.fork, &G.join})
             if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return e;
     }
-    if (off) return cudaMalloc(&bt->d_mb, off * sizeof(Member));
     return cudaSuccess;
 }
 
@@ -1361,31 +1356,30 @@ int pibm_batch_create(int n, const pibm_params *prm, const pibm_particles *parts
     return PIBM_OK;
 }
 
-// The Member arrays of every group for the members' current parities and
-// Geo copies (uploaded before capture; the graphs read them at run time).
-static int batch_members(pibm_batch *bt) {
-    std::vector<Member> mb;
+// The members of every group's launches for the members' current parities
+// and Geo copies (the graphs take them by value, as kernel parameters).
+static void batch_members(pibm_batch *bt) {
     for (auto &G : bt->groups) {
         BatchShape &bs = G.shape;
         bs = BatchShape{(int)G.idx.size(), 0, 0, 0, bt->members[G.idx[0]]->gs[0].lines_lt};
         for (int par = 0; par < 2; ++par)
-            for (int k = 0; k < G.itrmax; ++k)
-                for (int q : G.idx) {
+            for (int k = 0; k < G.itrmax; ++k) {
+                MemberSet &ms = G.sets[(size_t)par * G.itrmax + k];
+                std::memset(&ms, 0, sizeof(ms));
+                for (size_t z = 0; z < G.idx.size(); ++z) {
+                    const int q = G.idx[z];
                     pibm_handle *h = bt->members[q];
-                    Member m;
-                    std::memset(&m, 0, sizeof(m));
+                    Member &m = ms.m[z];
                     m.g = h->gs[k];
                     m.b = h->b;
                     m.cur = bt->base[q] ^ par ^ (k & 1);
                     m.nbk = h->g.nbody > 0 ? (h->g.npts + 255) / 256 : 0;
-                    mb.push_back(m);
                     bs.max_nbody = std::max(bs.max_nbody, h->g.nbody);
                     bs.max_nbk = std::max(bs.max_nbk, m.nbk);
                     if (h->g.nbody > 0 && h->g.npts > 0) bs.max_spn = std::max(bs.max_spn, h->g.sp_nnodes);
                 }
+            }
     }
-    if (!mb.empty()) CUDA_OR_FAIL(cudaMemcpy(bt->d_mb, mb.data(), mb.size() * sizeof(Member), cudaMemcpyHostToDevice));
-    return PIBM_OK;
 }
 
 // (Re)capture the two batch graphs if any member's parity or Geo no longer
@@ -1402,23 +1396,18 @@ static int batch_graphs(pibm_batch *bt) {
     for (int q = 0; q < n; ++q) { bt->base[q] = bt->members[q]->cur; bt->ver[q] = bt->members[q]->geo_ver; }
     bt->flip = 0;
     bt->captured_fused = bt->fused;
-    CUDA_OR_FAIL(cudaStreamSynchronize(bt->stream));
-    int rc = batch_members(bt);
-    if (rc) return rc;
+    batch_members(bt);
     for (int par = 0; par < 2; ++par) {
         cudaGraph_t gr;
         CUDA_OR_FAIL(cudaStreamBeginCapture(bt->stream, cudaStreamCaptureModeThreadLocal));
-        CUDA_OR_FAIL(cudaEventRecord(bt->fork, bt->stream));
+        // the groups one after another (run side by side, their launches
+        // compete for SMs and L2 and the step takes longer), then the others
         if (bt->fused)
-            for (auto &G : bt->groups) {
-                CUDA_OR_FAIL(cudaStreamWaitEvent(G.s, bt->fork, 0));
-                const size_t nz = G.idx.size();
+            for (auto &G : bt->groups)
                 for (int k = 0; k < G.itrmax; ++k)
-                    enqueue_batch_step(G.n, bt->d_mb + G.mb_off + ((size_t)par * G.itrmax + k) * nz, G.shape, G.s, G.side,
-                                       G.fork, G.join);
-                CUDA_OR_FAIL(cudaEventRecord(G.done, G.s));
-                CUDA_OR_FAIL(cudaStreamWaitEvent(bt->stream, G.done, 0));
-            }
+                    enqueue_batch_step(G.n, G.sets[(size_t)par * G.itrmax + k], G.shape, bt->stream, G.side, G.fork,
+                                       G.join);
+        CUDA_OR_FAIL(cudaEventRecord(bt->fork, bt->stream));
         // members whose plane kernels alone fill the GPU (nx*C CTAs per transform item
         // of at least one per SM slot) form one chain, one after the other; the
         // smaller members run as parallel branches beside that chain

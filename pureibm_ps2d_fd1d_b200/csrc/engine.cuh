@@ -101,11 +101,15 @@ struct Mov {
 };
 
 // Device buffers of one run.
-struct DevBufs {
+// The flow step's buffers (what the step kernels read and write).
+struct FlowBufs {
     double2 *u, *p, *nl[2], *ff;
     double *ubcp, *pbcp, *Q, *omega, *pgr, *fr, *Dx;
     double *part, *pres, *visc, *ptot, *force, *rec, *ctb, *dpart, *blockpart;
     Scal *sc;
+};
+
+struct DevBufs : FlowBufs {
     // passive scalar: spectral phi, nlphi (two steps), ffphi over planes 1..nx;
     // real phi (planes 1..nx) and its c2r image plane nx+1; real nlphi of
     // the two steps, diffusion and gradient over planes 1..nx+1; forcing and
@@ -122,9 +126,17 @@ struct DevBufs {
 // writes (nl[cur]; onl = nl[cur ^ 1]) and its reversal-forcing block count.
 struct Member {
     Geo g;
-    DevBufs b;
+    FlowBufs b;
     int cur;
     int nbk;
+};
+
+// The members of one fused launch, passed by value as a __grid_constant__
+// kernel parameter (constant-bank loads indexed by blockIdx.z; 12.5 KB of the
+// 32 KB parameter limit).  Larger groups are split into launches of kFuseMax.
+constexpr int kFuseMax = 16;
+struct MemberSet {
+    Member m[kFuseMax];
 };
 
 // Launch extents of a fused batch step: runs in the group and the largest

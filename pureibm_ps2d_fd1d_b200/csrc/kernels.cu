@@ -1199,114 +1199,119 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff2rc(Geo g, const do
 // ============================================================================
 // Fused batch step: the kernels of one time step for every run of a batch
 // that has the same grid size, one launch per kernel, the runs along
-// gridDim.z (Member array in device memory).  Each run's blocks execute the
+// gridDim.z.  Each run's blocks execute the
 // same device code as its own launches, so its results are bitwise those of
 // stepping it alone.  Launches are sized for the largest run of the group;
-// blocks beyond a run's own extent return at once.
+// blocks beyond a run's own extent return at once.  The Member array comes in
+// the parameter space (MemberSet), so each run's constants are read through
+// the constant cache, as a single run's Geo parameter is.
 // ============================================================================
 template <int N>
-__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_a0(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_a0(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     b_a0<N>(m.g, m.b.u, m.b.p, m.b.ubcp, m.b.pbcp, m.b.omega, m.b.pgr, m.b.sc, m.b.part);
 }
-__global__ void __launch_bounds__(256) kb_scal_a(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(256) kb_scal_a(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     b_scal_a(m.g, m.b.sc, m.b.part);
 }
 template <int N>
-__global__ void __launch_bounds__(256) kb_flux(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(256) kb_flux(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     b_flux<N>(m.g, m.b.ubcp, m.b.Dx, m.b.sc);
 }
 template <int N>
-__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_nl(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_nl(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     b_nl<N>(m.g, m.b.ubcp, m.b.Dx, m.b.u, m.b.nl[m.cur ^ 1], m.b.nl[m.cur], m.b.Q, m.b.sc);
 }
 template <int N>
-__global__ void __launch_bounds__(256) kb_drag(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(256) kb_drag(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     if ((int)blockIdx.x >= m.g.nbody * kDragSplit) return;
     b_drag<N>(m.g, m.b.pbcp, m.b.omega, m.b.dpart, m.b.sc);
 }
-__global__ void __launch_bounds__(256) kb_scal_b(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(256) kb_scal_b(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     if (m.g.nbody == 0) return;
     b_scal_b(m.g, m.b.sc, m.b.pres, m.b.visc, m.b.ptot, m.b.force, m.b.dpart);
 }
 template <int N>
-__global__ void __launch_bounds__(256, 3) kb_rev(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(256, 3) kb_rev(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     if (m.g.nbody == 0 || m.g.npts == 0 || (int)blockIdx.x >= m.nbk) return;
     b_rev<N>(m.g, m.b.ubcp, m.b.pgr, m.b.Q, m.b.sc, m.b.rec, m.b.ctb, m.b.blockpart);
 }
-__global__ void __launch_bounds__(256) kb_scal_c(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(256) kb_scal_c(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     if (m.g.nbody == 0 || m.g.npts == 0) return;
     b_scal_c(m.g, m.b.sc, m.b.blockpart, m.nbk);
 }
-__global__ void __launch_bounds__(256) kb_spread(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(256) kb_spread(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     if (m.g.nbody == 0 || m.g.npts == 0) return;
     b_spread(m.g, m.b.rec, m.b.ctb, m.b.fr, m.b.sc);
 }
 template <int N>
-__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_ff(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_ff(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     if (m.g.nbody == 0) return;
     b_ff<N>(m.g, m.b.fr, m.b.ff, m.b.sc);
 }
+// CTAs per SM of the single-run x-line kernels at their register counts,
+// kept as a bound here (the indexed parameter loads would raise the count).
+template <int N, int LT> constexpr int kb_lines_minb() { return N <= 128 ? (LT == 4 ? 4 : 2) : (LT == 4 ? 2 : 1); }
 template <int N, int LT>
-__global__ void __launch_bounds__(LT * 32) kb_lines(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void __launch_bounds__(LT * 32, kb_lines_minb<N, LT>()) kb_lines(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     b_lines<N, LT>(m.g, m.b.u, m.b.p, m.b.nl[m.cur], m.b.nl[m.cur ^ 1], m.b.ff, m.b.sc);
 }
-__global__ void kb_scal_d(const Member *__restrict__ mb) {
-    const Member &m = mb[blockIdx.z];
+__global__ void kb_scal_d(const __grid_constant__ MemberSet ms) {
+    const Member &m = ms.m[blockIdx.z];
     b_scal_d(m.g, m.b.sc);
 }
 
-// One fused step of nz runs of size N (members d_mb[0..nz-1]): the drag and
+// One fused step of nz runs of size N (ms.m[0..nz-1]): the drag and
 // mpg kernels on `side` beside the nonlinear term, as in a single run's graph.
 template <int N>
-static void enqueue_batch_step_t(const Member *d_mb, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
+static void enqueue_batch_step_t(const MemberSet &ms, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
                                  cudaEvent_t fork, cudaEvent_t join) {
     const int nz = bs.nz;
-    launch_planes_z<N>(kb_a0<N>, N, 10, nz, s, d_mb);
-    kb_scal_a<<<dim3(1, 1, nz), 256, 0, s>>>(d_mb);
+    launch_planes_z<N>(kb_a0<N>, N, 10, nz, s, ms);
+    kb_scal_a<<<dim3(1, 1, nz), 256, 0, s>>>(ms);
     const bool spheres = bs.max_nbody > 0;
     if (spheres) {
         cudaEventRecord(fork, s);
         cudaStreamWaitEvent(side, fork, 0);
-        kb_drag<N><<<dim3(bs.max_nbody * kDragSplit, 1, nz), 256, 0, side>>>(d_mb);
-        kb_scal_b<<<dim3(1, 1, nz), 256, 0, side>>>(d_mb);
+        kb_drag<N><<<dim3(bs.max_nbody * kDragSplit, 1, nz), 256, 0, side>>>(ms);
+        kb_scal_b<<<dim3(1, 1, nz), 256, 0, side>>>(ms);
         cudaEventRecord(join, side);
     }
-    kb_flux<N><<<dim3((RP<N>::RSP * (N / 32) + 255) / 256, 1, nz), 256, 0, s>>>(d_mb);
-    launch_planes_z<N>(kb_nl<N>, N, 3, nz, s, d_mb);
+    kb_flux<N><<<dim3((RP<N>::RSP * (N / 32) + 255) / 256, 1, nz), 256, 0, s>>>(ms);
+    launch_planes_z<N>(kb_nl<N>, N, 3, nz, s, ms);
     if (spheres) {
         cudaStreamWaitEvent(s, join, 0);
         if (bs.max_nbk > 0) {
-            kb_rev<N><<<dim3(bs.max_nbk, 1, nz), 256, 0, s>>>(d_mb);
-            kb_scal_c<<<dim3(1, 1, nz), 256, 0, s>>>(d_mb);
-            if (bs.max_spn > 0) kb_spread<<<dim3((bs.max_spn + 255) / 256, 1, nz), 256, 0, s>>>(d_mb);
+            kb_rev<N><<<dim3(bs.max_nbk, 1, nz), 256, 0, s>>>(ms);
+            kb_scal_c<<<dim3(1, 1, nz), 256, 0, s>>>(ms);
+            if (bs.max_spn > 0) kb_spread<<<dim3((bs.max_spn + 255) / 256, 1, nz), 256, 0, s>>>(ms);
         }
-        launch_planes_z<N>(kb_ff<N>, N, 3, nz, s, d_mb);
+        launch_planes_z<N>(kb_ff<N>, N, 3, nz, s, ms);
     }
     const int PS = (N / 2 + 1) * N;
-    if (bs.lines_lt == 4) kb_lines<N, 4><<<dim3((PS + 3) / 4, 1, nz), 4 * 32, lines_smem<N>(4), s>>>(d_mb);
-    else kb_lines<N, 8><<<dim3((PS + 7) / 8, 1, nz), 8 * 32, lines_smem<N>(8), s>>>(d_mb);
-    kb_scal_d<<<dim3(1, 1, nz), 32, 0, s>>>(d_mb);
+    if (bs.lines_lt == 4) kb_lines<N, 4><<<dim3((PS + 3) / 4, 1, nz), 4 * 32, lines_smem<N>(4), s>>>(ms);
+    else kb_lines<N, 8><<<dim3((PS + 7) / 8, 1, nz), 8 * 32, lines_smem<N>(8), s>>>(ms);
+    kb_scal_d<<<dim3(1, 1, nz), 32, 0, s>>>(ms);
 }
 
-void enqueue_batch_step(int n, const Member *d_mb, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
+void enqueue_batch_step(int n, const MemberSet &ms, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
                         cudaEvent_t fork, cudaEvent_t join) {
     switch (n) {
-        case 32: enqueue_batch_step_t<32>(d_mb, bs, s, side, fork, join); break;
-        case 64: enqueue_batch_step_t<64>(d_mb, bs, s, side, fork, join); break;
-        case 96: enqueue_batch_step_t<96>(d_mb, bs, s, side, fork, join); break;
-        case 128: enqueue_batch_step_t<128>(d_mb, bs, s, side, fork, join); break;
-        case 256: enqueue_batch_step_t<256>(d_mb, bs, s, side, fork, join); break;
+        case 32: enqueue_batch_step_t<32>(ms, bs, s, side, fork, join); break;
+        case 64: enqueue_batch_step_t<64>(ms, bs, s, side, fork, join); break;
+        case 96: enqueue_batch_step_t<96>(ms, bs, s, side, fork, join); break;
+        case 128: enqueue_batch_step_t<128>(ms, bs, s, side, fork, join); break;
+        case 256: enqueue_batch_step_t<256>(ms, bs, s, side, fork, join); break;
     }
 }
 // Kernels one fused batch step launches.
