@@ -116,7 +116,8 @@ struct pibm_handle {
         if (stream) cudaStreamDestroy(stream);
         if (ss.side) cudaStreamDestroy(ss.side);
         if (ss.scal) cudaStreamDestroy(ss.scal);
-        for (cudaEvent_t e : {ss.fork, ss.drag_done, ss.scal_done, ss.geo_done}) if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : {ss.fork, ss.drag_done, ss.scal_done, ss.geo_done, ss.rev_done, ss.frmean_done})
+            if (e) cudaEventDestroy(e);
         for (void *q : allocs) cudaFree(q);
     }
 };
@@ -244,7 +245,9 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
         !guard(cudaEventCreateWithFlags(&h->ss.fork, cudaEventDisableTiming), "cudaEventCreate") ||
         !guard(cudaEventCreateWithFlags(&h->ss.drag_done, cudaEventDisableTiming), "cudaEventCreate") ||
         !guard(cudaEventCreateWithFlags(&h->ss.scal_done, cudaEventDisableTiming), "cudaEventCreate") ||
-        !guard(cudaEventCreateWithFlags(&h->ss.geo_done, cudaEventDisableTiming), "cudaEventCreate")) { delete h; return rc; }
+        !guard(cudaEventCreateWithFlags(&h->ss.geo_done, cudaEventDisableTiming), "cudaEventCreate") ||
+        !guard(cudaEventCreateWithFlags(&h->ss.rev_done, cudaEventDisableTiming), "cudaEventCreate") ||
+        !guard(cudaEventCreateWithFlags(&h->ss.frmean_done, cudaEventDisableTiming), "cudaEventCreate")) { delete h; return rc; }
     Geo &g = h->g;
     std::memset(&g, 0, sizeof(g));
     g.nx = S.nx; g.my = S.my; g.mz = S.mz; g.my2 = S.my2;
@@ -254,6 +257,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
     g.plane_ctas = plane_ctas(S.my);
     g.c1 = S.coef[0]; g.c2 = S.coef[1]; g.c3 = S.coef[2]; g.c4 = S.coef[3];
     g.scheme = prm->discr_scheme; g.limiter = prm->limiter;
+    g.flux_seg = flux_segment(S.my, S.scal);
     g.include_frmeanfluid = prm->include_frmeanfluid; g.revernorm = prm->revernorm;
     g.set_mpg = prm->set_mpg; g.adaptive = prm->adaptive; g.dt_update = 1;
     g.cfl_max = prm->cfl_max; g.ramp_frac_time = S.ramp_frac_time; g.ucharmod = S.ucharmod;
@@ -306,7 +310,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
               guard(h->alloc(&b.part, (size_t)g.nx * 8 * 12), "part") &&
               guard(h->alloc(&b.pres, 3 * (size_t)S.nbody), "pres") && guard(h->alloc(&b.visc, 3 * (size_t)S.nbody), "visc") &&
               guard(h->alloc(&b.ptot, 3 * (size_t)S.nbody), "ptot") && guard(h->alloc(&b.force, 3 * (size_t)S.nbody), "force") &&
-              guard(h->alloc(&b.rec, 6 * (size_t)g.npts), "rec") && guard(h->alloc(&b.ctb, 24 * (size_t)g.npts), "ctb") &&
+              guard(h->alloc(&b.rec, 6 * (size_t)g.npts), "rec") && guard(h->alloc(&b.rz, 3 * (size_t)g.npts), "rz") &&
               guard(h->alloc(&b.dpart, 6 * 8 * (size_t)S.nbody), "dpart") &&
               guard(h->alloc(&b.blockpart, 6 * (size_t)((g.npts + 255) / 256 + 1)), "blockpart") &&
               guard(h->alloc(&b.sc, 1), "scalars");
@@ -1361,7 +1365,7 @@ int pibm_batch_create(int n, const pibm_params *prm, const pibm_particles *parts
 static void batch_members(pibm_batch *bt) {
     for (auto &G : bt->groups) {
         BatchShape &bs = G.shape;
-        bs = BatchShape{(int)G.idx.size(), 0, 0, 0, bt->members[G.idx[0]]->gs[0].lines_lt};
+        bs = BatchShape{(int)G.idx.size(), 0, 0, 0, bt->members[G.idx[0]]->gs[0].lines_lt, bt->members[G.idx[0]]->gs[0].flux_seg};
         for (int par = 0; par < 2; ++par)
             for (int k = 0; k < G.itrmax; ++k) {
                 MemberSet &ms = G.sets[(size_t)par * G.itrmax + k];

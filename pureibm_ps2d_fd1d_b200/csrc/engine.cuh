@@ -18,6 +18,7 @@ struct Geo {
     long long count_fluid, ncell;
     int plane_ctas;     // CTAs per plane in the plane kernels
     int lines_lt;       // x-line tile width of k_lines (4 or 8; 0 = the size's default), set by the autotuner
+    int flux_seg;       // planes per thread of k_flux (flux_segment)
     double ufmean_des[3], usmean_des[3], usmean_act[3];
     // particles (moving: the geometry arrays below are rebuilt on the device
     // every step and npts is the capacity nbody*nbnd; Scal::npts is the count)
@@ -105,7 +106,7 @@ struct Mov {
 struct FlowBufs {
     double2 *u, *p, *nl[2], *ff;
     double *ubcp, *pbcp, *Q, *omega, *pgr, *fr, *Dx;
-    double *part, *pres, *visc, *ptot, *force, *rec, *ctb, *dpart, *blockpart;
+    double *part, *pres, *visc, *ptot, *force, *rec, *rz, *dpart, *blockpart;
     Scal *sc;
 };
 
@@ -139,21 +140,33 @@ struct MemberSet {
     Member m[kFuseMax];
 };
 
+// Planes one thread of k_flux marches through (a sliding window along x; a
+// segment re-reads two planes on either side).  Short segments give grids up
+// to 128^3 enough threads to keep loads in flight when the flux is on the
+// step's critical path (k_flux 41 -> 35 us at 128^3); with the passive
+// scalar's kernels running beside it the GPU is full, and long segments, which
+// re-read less, give the shorter step.
+inline int flux_segment(int n, bool scalar) { return (scalar || n >= 256) ? 32 : 8; }
+
 // Launch extents of a fused batch step: runs in the group and the largest
 // sphere count, reversal-forcing block count and spreading node count among
-// them; the x-line tile width all of them use.
+// them; the x-line tile width and the x-flux segment all of them use.
 struct BatchShape {
-    int nz, max_nbody, max_nbk, max_spn, lines_lt;
+    int nz, max_nbody, max_nbk, max_spn, lines_lt, flux_seg;
 };
 
-// Side streams of one run: after compute_new_timestep's scalars are known,
-// the drag quadrature (and mpg) and the passive-scalar step depend only on
-// the real fields of that step, so they run beside the nonlinear term (with
-// moving particles the scalar waits for the step's new geometry).
+// Side streams of one run: the x flux and the nonlinear term need only the
+// real fields of k_a0, so compute_new_timestep's scalars (k_scal_a), the drag
+// quadrature and mpg run beside them on `side`, and the passive-scalar step,
+// once those scalars are known, on `scal` (k_scal_a then runs first, on the
+// main stream; with moving particles the scalar waits for the step's new
+// geometry); without a scalar the frmean sums (k_scal_c) run on `side`
+// beside the spreading.
 struct StepStreams {
     cudaStream_t side = nullptr, scal = nullptr;
     cudaEvent_t fork = nullptr, drag_done = nullptr, scal_done = nullptr;
     cudaEvent_t geo_done = nullptr;   // moving particles: the step's geometry is rebuilt
+    cudaEvent_t rev_done = nullptr, frmean_done = nullptr;   // k_scal_c beside k_spread
 };
 
 // Discrete adjoint of the AB2 step (fixed spheres, imposed mpg, fixed dt).

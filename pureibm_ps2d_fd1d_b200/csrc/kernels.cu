@@ -36,7 +36,7 @@ namespace pibm {
 void enqueue_scalar(const Geo &g, DevBufs &b, int cur, cudaStream_t s);
 int scalar_kernels_per_step(const Geo &g);
 void enqueue_moving(const Geo &g, const Mov &m, Scal *sc, const double *pres, const double *visc, cudaStream_t s);
-void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, const double *ctb, double *fr, Scal *sc, cudaStream_t s);
+void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, const double *rz, double *fr, Scal *sc, cudaStream_t s);
 int moving_kernels_per_step(const Mov &m);
 
 // ============================================================================
@@ -294,8 +294,8 @@ __device__ __forceinline__ double xflux_diff(const Geo &g, const double *__restr
 template <int N>
 __device__ __forceinline__ void b_flux(const Geo &g, const double *__restrict__ ubcp, double *__restrict__ Dx,
                                               const Scal *__restrict__ sc) {
-    constexpr int RSP = RP<N>::RSP, SEG = 32;
-    const int nx = g.nx, nseg = nx / SEG;
+    constexpr int RSP = RP<N>::RSP;
+    const int nx = g.nx, SEG = g.flux_seg, nseg = nx / SEG;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= RSP * nseg || sc->status) return;
     const int e = t % RSP, i0 = (t / RSP) * SEG;
@@ -617,8 +617,9 @@ __global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, d
 // ============================================================================
 // k_rev: direct forcing at the inner reversal points
 // (calc_inner_reversal_forcing, boundary_condition.F90:1104-1479).
-// rec[p*6 + 0..2] = force_tmp, rec[p*6 + 3..5] = force_dist,
-// ctb[(p*8 + corner)*3 + n] = weight*force_tmp/dx^3 per stencil corner; blockpart = sums of
+// rec[p*6 + 0..2] = force_tmp, rec[p*6 + 3..5] = force_dist, rz[p*3 + 0..2] =
+// the inner point's offsets in its cell (the spreading forms each corner's
+// weight*force_tmp/dx^3 from them, corner_contrib); blockpart = sums of
 // tmppa/dx^3 over all corners (frmean) and over fluid corners (frmeanfluid).
 // ============================================================================
 __device__ __forceinline__ void inner_point(const Geo &g, int m, int l, double xli[3]) {
@@ -630,7 +631,7 @@ __device__ __forceinline__ void inner_point(const Geo &g, int m, int l, double x
 template <int N>
 __device__ __forceinline__ void b_rev(const Geo &g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
                                                 const double *__restrict__ Q, const Scal *__restrict__ sc,
-                                                double *__restrict__ rec, double *__restrict__ ctb, double *__restrict__ blockpart) {
+                                                double *__restrict__ rec, double *__restrict__ rz, double *__restrict__ blockpart) {
     __shared__ double scr[32 * 6];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     double fm[3] = {0, 0, 0}, ffl[3] = {0, 0, 0};
@@ -705,11 +706,13 @@ __device__ __forceinline__ void b_rev(const Geo &g, const double *__restrict__ u
                         const double t = qdiv(w * ft[n], g.dx3, rdx3);
                         if (fl) { force_fl[n] = force_fl[n] + t; ffl[n] += t; }
                         fm[n] += t;
-                        ctb[((size_t)p * 8 + a + 2 * b + 4 * c) * 3 + n] = t;
                     }
                     count_fl += fl ? 1 : 0;
                 }
         const int count_so = 8 - count_fl;
+        rz[(size_t)p * 3] = si.xv[1];
+        rz[(size_t)p * 3 + 1] = si.yv[1];
+        rz[(size_t)p * 3 + 2] = si.zv[1];
         double *r = rec + (size_t)p * 6;
 #pragma unroll
         for (int n = 0; n < 3; ++n) {
@@ -725,7 +728,7 @@ __device__ __forceinline__ void b_rev(const Geo &g, const double *__restrict__ u
 template <int N>
 __global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
                                                 const double *__restrict__ Q, const Scal *__restrict__ sc,
-                                                double *__restrict__ rec, double *__restrict__ ctb, double *__restrict__ blockpart) { b_rev<N>(g, ubcp, pgr, Q, sc, rec, ctb, blockpart); }
+                                                double *__restrict__ rec, double *__restrict__ rz, double *__restrict__ blockpart) { b_rev<N>(g, ubcp, pgr, Q, sc, rec, rz, blockpart); }
 
 __device__ __forceinline__ void b_scal_c(const Geo &g, Scal *sc, const double *blockpart, int nblocks) {
     __shared__ double scr[32 * 6];
@@ -746,32 +749,34 @@ __global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *b
 // k_spread: fr at every forced node, accumulated over its (point, corner)
 // contributions in the reference's (sphere, point) order
 // (boundary_condition.F90:1425-1462).  sp_node holds physical offsets.
-__device__ __forceinline__ void b_spread(const Geo &g, const double *__restrict__ rec, const double *__restrict__ ctb,
+__device__ __forceinline__ void b_spread(const Geo &g, const double *__restrict__ rec, const double *__restrict__ rz,
                                                 double *__restrict__ fr, const Scal *__restrict__ sc) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.sp_nnodes || sc->status) return;
     const int node = g.sp_node[q];
+    const double rdx3 = 1.0 / g.dx3;
     double acc[3] = {0.0, 0.0, 0.0};
     const int e0 = g.sp_ptr[q], e1 = g.sp_ptr[q + 1];
 #pragma unroll 4
     for (int e = e0; e < e1; ++e) {
         const int ent = __ldg(g.sp_ent + e);
-        const double *t = ctb + (size_t)ent * 3;
+        double t[3];
+        corner_contrib(rz, rec, ent, g.dx3, rdx3, t);
         if (g.include_frmeanfluid) {
 #pragma unroll
-            for (int n = 0; n < 3; ++n) acc[n] = acc[n] + __ldg(t + n);
+            for (int n = 0; n < 3; ++n) acc[n] = acc[n] + t[n];
         } else {
             const double *r = rec + (size_t)(ent >> 3) * 6 + 3;
 #pragma unroll
-            for (int n = 0; n < 3; ++n) acc[n] = (acc[n] + __ldg(t + n)) + __ldg(r + n);
+            for (int n = 0; n < 3; ++n) acc[n] = (acc[n] + t[n]) + __ldg(r + n);
         }
     }
     const size_t CR = (size_t)g.nx * g.RS;
 #pragma unroll
     for (int n = 0; n < 3; ++n) fr[n * CR + node] = acc[n];
 }
-__global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, const double *__restrict__ ctb,
-                                                double *__restrict__ fr, const Scal *__restrict__ sc) { b_spread(g, rec, ctb, fr, sc); }
+__global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, const double *__restrict__ rz,
+                                                double *__restrict__ fr, const Scal *__restrict__ sc) { b_spread(g, rec, rz, fr, sc); }
 
 // k_ff: ff = r2c(fr - frmean) (boundary_condition.F90:678-700).
 template <int N>
@@ -1240,7 +1245,7 @@ template <int N>
 __global__ void __launch_bounds__(256, 3) kb_rev(const __grid_constant__ MemberSet ms) {
     const Member &m = ms.m[blockIdx.z];
     if (m.g.nbody == 0 || m.g.npts == 0 || (int)blockIdx.x >= m.nbk) return;
-    b_rev<N>(m.g, m.b.ubcp, m.b.pgr, m.b.Q, m.b.sc, m.b.rec, m.b.ctb, m.b.blockpart);
+    b_rev<N>(m.g, m.b.ubcp, m.b.pgr, m.b.Q, m.b.sc, m.b.rec, m.b.rz, m.b.blockpart);
 }
 __global__ void __launch_bounds__(256) kb_scal_c(const __grid_constant__ MemberSet ms) {
     const Member &m = ms.m[blockIdx.z];
@@ -1250,7 +1255,7 @@ __global__ void __launch_bounds__(256) kb_scal_c(const __grid_constant__ MemberS
 __global__ void __launch_bounds__(256) kb_spread(const __grid_constant__ MemberSet ms) {
     const Member &m = ms.m[blockIdx.z];
     if (m.g.nbody == 0 || m.g.npts == 0) return;
-    b_spread(m.g, m.b.rec, m.b.ctb, m.b.fr, m.b.sc);
+    b_spread(m.g, m.b.rec, m.b.rz, m.b.fr, m.b.sc);
 }
 template <int N>
 __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_ff(const __grid_constant__ MemberSet ms) {
@@ -1271,30 +1276,35 @@ __global__ void kb_scal_d(const __grid_constant__ MemberSet ms) {
     b_scal_d(m.g, m.b.sc);
 }
 
-// One fused step of nz runs of size N (ms.m[0..nz-1]): the drag and
-// mpg kernels on `side` beside the nonlinear term, as in a single run's graph.
+// One fused step of nz runs of size N (ms.m[0..nz-1]): the step's scalars,
+// the drag and mpg kernels on `side` beside the nonlinear term, and the
+// frmean sums beside the spreading, as in a single run's graph.
 template <int N>
 static void enqueue_batch_step_t(const MemberSet &ms, const BatchShape &bs, cudaStream_t s, cudaStream_t side,
                                  cudaEvent_t fork, cudaEvent_t join) {
     const int nz = bs.nz;
     launch_planes_z<N>(kb_a0<N>, N, 10, nz, s, ms);
-    kb_scal_a<<<dim3(1, 1, nz), 256, 0, s>>>(ms);
     const bool spheres = bs.max_nbody > 0;
+    cudaEventRecord(fork, s);
+    cudaStreamWaitEvent(side, fork, 0);
+    kb_scal_a<<<dim3(1, 1, nz), 256, 0, side>>>(ms);
     if (spheres) {
-        cudaEventRecord(fork, s);
-        cudaStreamWaitEvent(side, fork, 0);
         kb_drag<N><<<dim3(bs.max_nbody * kDragSplit, 1, nz), 256, 0, side>>>(ms);
         kb_scal_b<<<dim3(1, 1, nz), 256, 0, side>>>(ms);
-        cudaEventRecord(join, side);
     }
-    kb_flux<N><<<dim3((RP<N>::RSP * (N / 32) + 255) / 256, 1, nz), 256, 0, s>>>(ms);
+    cudaEventRecord(join, side);
+    kb_flux<N><<<dim3((RP<N>::RSP * (N / bs.flux_seg) + 255) / 256, 1, nz), 256, 0, s>>>(ms);
     launch_planes_z<N>(kb_nl<N>, N, 3, nz, s, ms);
+    cudaStreamWaitEvent(s, join, 0);
     if (spheres) {
-        cudaStreamWaitEvent(s, join, 0);
         if (bs.max_nbk > 0) {
             kb_rev<N><<<dim3(bs.max_nbk, 1, nz), 256, 0, s>>>(ms);
-            kb_scal_c<<<dim3(1, 1, nz), 256, 0, s>>>(ms);
+            cudaEventRecord(fork, s);
+            cudaStreamWaitEvent(side, fork, 0);
+            kb_scal_c<<<dim3(1, 1, nz), 256, 0, side>>>(ms);
+            cudaEventRecord(join, side);
             if (bs.max_spn > 0) kb_spread<<<dim3((bs.max_spn + 255) / 256, 1, nz), 256, 0, s>>>(ms);
+            cudaStreamWaitEvent(s, join, 0);
         }
         launch_planes_z<N>(kb_ff<N>, N, 3, nz, s, ms);
     }
@@ -1392,43 +1402,52 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
     auto kb = [&](int k) { if (kev) cudaEventRecord(kev[2 * k], s); };
     auto ke = [&](int k) { if (kev) cudaEventRecord(kev[2 * k + 1], s); };
     auto kskip = [&](int k) { kb(k); ke(k); };
-    // forked: drag + mpg on ss->side and the scalar step on ss->scal run beside the
-    // nonlinear term; the timed variants keep one serial stream
+    // forked: the step's scalars (k_scal_a), drag + mpg on ss->side and the scalar
+    // step on ss->scal run beside the x flux and the nonlinear term, which read
+    // only k_a0's real fields, and the frmean sums (k_scal_c) beside the
+    // spreading; the timed variants keep one serial stream.  With a passive
+    // scalar k_scal_a and k_scal_c stay on the main stream: the scalar's plane
+    // kernels then start with the x flux and fill the GPU, and the flow's short
+    // side kernels measured slower queued beside them.
     const bool fork = ss && !ev && !kev;
+    const bool scal_first = g.scal && !g.moving;
     mark(0);
     kb(PIBM_K_A0);
     launch_planes<N>(k_a0<N>, g.nx, 10, s, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
     ke(PIBM_K_A0);
-    kb(PIBM_K_SCAL_A);
-    k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
-    ke(PIBM_K_SCAL_A);
-    mark(1);
     if (fork) {
+        if (scal_first) k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
         cudaEventRecord(ss->fork, s);
-        if (g.nbody > 0) {
-            cudaStreamWaitEvent(ss->side, ss->fork, 0);
-            k_drag<N><<<g.nbody * kDragSplit, 256, 0, ss->side>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
-            k_scal_b<<<1, 256, 0, ss->side>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
-            cudaEventRecord(ss->drag_done, ss->side);
-        }
-        if (g.scal && !g.moving) {
+        cudaStreamWaitEvent(ss->side, ss->fork, 0);
+        if (scal_first) {
             cudaStreamWaitEvent(ss->scal, ss->fork, 0);
             enqueue_scalar(g, b, cur, ss->scal);
             cudaEventRecord(ss->scal_done, ss->scal);
+        } else {
+            k_scal_a<<<1, 256, 0, ss->side>>>(g, b.sc, b.part);
         }
+        if (g.nbody > 0) {
+            k_drag<N><<<g.nbody * kDragSplit, 256, 0, ss->side>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
+            k_scal_b<<<1, 256, 0, ss->side>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
+        }
+        cudaEventRecord(ss->drag_done, ss->side);
+    } else {
+        kb(PIBM_K_SCAL_A);
+        k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
+        ke(PIBM_K_SCAL_A);
     }
+    mark(1);
     kb(PIBM_K_FLUX);
-    k_flux<N><<<(RP<N>::RSP * (g.nx / 32) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
+    k_flux<N><<<(RP<N>::RSP * (g.nx / g.flux_seg) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
     ke(PIBM_K_FLUX);
     kb(PIBM_K_NL);
     launch_planes<N>(k_nl<N>, g.nx, 3, s, g, (const double *)b.ubcp, (const double *)b.Dx, (const double2 *)b.u,
                      (const double2 *)b.nl[old], b.nl[cur], b.Q, b.sc);
     ke(PIBM_K_NL);
     mark(2);
+    if (fork) cudaStreamWaitEvent(s, ss->drag_done, 0);
     if (g.nbody > 0) {
-        if (fork) {
-            cudaStreamWaitEvent(s, ss->drag_done, 0);
-        } else {
+        if (!fork) {
             kb(PIBM_K_DRAG);
             k_drag<N><<<g.nbody * kDragSplit, 256, 0, s>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
             ke(PIBM_K_DRAG);
@@ -1449,15 +1468,24 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {
             kb(PIBM_K_REV);
-            k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.ctb, b.blockpart);
+            k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.rz, b.blockpart);
             ke(PIBM_K_REV);
-            kb(PIBM_K_SCAL_C);
-            k_scal_c<<<1, 256, 0, s>>>(g, b.sc, b.blockpart, nbk);
-            ke(PIBM_K_SCAL_C);
+            if (fork && !scal_first) {
+                // frmean (read from k_ff on) beside the spreading, which does not read it
+                cudaEventRecord(ss->rev_done, s);
+                cudaStreamWaitEvent(ss->side, ss->rev_done, 0);
+                k_scal_c<<<1, 256, 0, ss->side>>>(g, b.sc, b.blockpart, nbk);
+                cudaEventRecord(ss->frmean_done, ss->side);
+            } else {
+                kb(PIBM_K_SCAL_C);
+                k_scal_c<<<1, 256, 0, s>>>(g, b.sc, b.blockpart, nbk);
+                ke(PIBM_K_SCAL_C);
+            }
             kb(PIBM_K_SPREAD);
-            if (g.moving) enqueue_spread_dyn(g, b.mov, b.rec, b.ctb, b.fr, b.sc, s);
-            else if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.ctb, b.fr, b.sc);
+            if (g.moving) enqueue_spread_dyn(g, b.mov, b.rec, b.rz, b.fr, b.sc, s);
+            else if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.rz, b.fr, b.sc);
             ke(PIBM_K_SPREAD);
+            if (fork && !scal_first) cudaStreamWaitEvent(s, ss->frmean_done, 0);
         } else {
             kskip(PIBM_K_REV); kskip(PIBM_K_SCAL_C); kskip(PIBM_K_SPREAD);
         }

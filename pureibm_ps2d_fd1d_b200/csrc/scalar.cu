@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(256) k_sflux(Geo g, const double *__restrict__
                                                const double *__restrict__ phimg, double *__restrict__ dsx,
                                                const Scal *__restrict__ sc) {
     // one thread per (y,z) node and segment of SEG planes
-    constexpr int RSP = RP<N>::RSP, SEG = 32;
+    constexpr int RSP = RP<N>::RSP, SEG = kScalarFluxSeg;
     const int nx = g.nx, nseg = (nx + SEG - 1) / SEG;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int e = t % RSP, sg = t / RSP;
@@ -710,7 +710,7 @@ static void enqueue_scalar_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s) 
     launch_planes<N>(k_sa<N>, g.nx + 1, 5, s, g, (const double2 *)b.phif, (const double *)b.ubcp, b.phr, b.phimg,
                      b.sdf, b.gph, (const Scal *)b.sc, b.spart);
     k_sheat<<<1, 32, 0, s>>>(g, b.sc, b.spart);
-    k_sflux<N><<<(RP<N>::RSP * ((g.nx + 31) / 32) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.phr, b.phimg, b.dsx, b.sc);
+    k_sflux<N><<<(RP<N>::RSP * ((g.nx + kScalarFluxSeg - 1) / kScalarFluxSeg) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.phr, b.phimg, b.dsx, b.sc);
     launch_planes<N>(k_snl<N>, g.nx, 1, s, g, (const double *)b.ubcp, (const double *)b.phr, (const double *)b.dsx,
                      b.nls[cur], b.nlr[cur], b.sc);
     launch_planes<N>(k_simg<N>, 1, 1, s, g, (const double2 *)b.nls[cur], b.nlr[cur], (const Scal *)b.sc);

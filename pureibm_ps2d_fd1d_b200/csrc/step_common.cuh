@@ -150,6 +150,24 @@ __device__ __forceinline__ void make_sten(const Geo &g, const double pos[3], Ste
     }
 }
 
+// Contribution of a reversal point to one node of its inner stencil, entry
+// ent = 8 p + a + 2 b + 4 c of the spreading lists: w * force_tmp / dx^3
+// (boundary_condition.F90:1425-1462), w the trilinear weight of corner
+// (a, b, c) formed from the point's cell offsets rz[3p..3p+2] as make_sten and
+// Sten::w form it, force_tmp = rec[6p..6p+2].  k_rev forms the same values
+// for its sums, so they are bitwise those it would have stored.
+__device__ __forceinline__ void corner_contrib(const double *__restrict__ rz, const double *__restrict__ rec, int ent,
+                                               double dx3, double rdx3, double t[3]) {
+    const size_t p = (size_t)(ent >> 3);
+    const double zx = __ldg(rz + 3 * p), zy = __ldg(rz + 3 * p + 1), zz = __ldg(rz + 3 * p + 2);
+    const double wx = (ent & 1) ? zx : __dsub_rn(1.0, zx);
+    const double wy = (ent & 2) ? zy : __dsub_rn(1.0, zy);
+    const double wz = (ent & 4) ? zz : __dsub_rn(1.0, zz);
+    const double w = __dmul_rn(__dmul_rn(wx, wy), wz);
+#pragma unroll
+    for (int n = 0; n < 3; ++n) t[n] = qdiv(w * __ldg(rec + 6 * p + n), dx3, rdx3);
+}
+
 // value at node (x=i, y=j, z=k) of a physical field (one component)
 template <int N>
 __device__ __forceinline__ double fat(const double *f, int i, int j, int k) {
@@ -206,6 +224,10 @@ inline void launch_planes(void (*k)(KArgs...), int nplanes, int items, cudaStrea
     cudaLaunchKernelEx(&cfg, k, args...);
 }
 
+
+// Planes one thread of the scalar's x-flux kernel covers (flux_segment gives
+// the flow's).
+constexpr int kScalarFluxSeg = 32;
 
 // launch_planes for a fused batch: nz runs of the same size along gridDim.z.
 template <int N, typename... KArgs, typename... Args>
