@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const doubl
 __device__ __forceinline__ void b_scal_a(const Geo &g, Scal *sc, const double *part) {
     __shared__ double scr[32 * 3];
     __shared__ double red[6];
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     {
         double a[3] = {0.0, 0.0, 0.0}, m[3] = {kSmallD, kSmallD, kSmallD};
         for (int i = threadIdx.x; i < g.nx * g.plane_ctas; i += blockDim.x)
@@ -538,7 +538,7 @@ __device__ __forceinline__ void b_scal_b(const Geo &g, Scal *sc, double *pres, d
                                                 double *force, const double *dpart) {
     __shared__ double scr[32 * 9];
     __shared__ double tot[12];
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     const int NB = g.nbody;
     // per-sphere sums of the k_drag partials (fixed order)
     for (int m = threadIdx.x; m < NB; m += blockDim.x) {
@@ -732,7 +732,7 @@ __global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict_
 
 __device__ __forceinline__ void b_scal_c(const Geo &g, Scal *sc, const double *blockpart, int nblocks) {
     __shared__ double scr[32 * 6];
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     double a[6] = {0, 0, 0, 0, 0, 0};
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
 #pragma unroll
@@ -852,7 +852,7 @@ __device__ __forceinline__ void b_lines(const Geo &g, double2 *__restrict__ u, d
     double2 *st = (double2 *)(gam + NX);      // cross-lane stage twiddles
     double *lcs = (double *)(st + 32);        // per-lane constants of the solves
     double2 *ltr = (double2 *)(lcs + NX);
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     for (int t = threadIdx.x; t < NX; t += blockDim.x) tws[t] = g.tw[t];
     fill_stage_table<32>(st, g.tw, NX);
     fill_line_tw<R>(lcs, ltr, g.tw);

@@ -452,7 +452,7 @@ __global__ void k_dem_ibm(Mov m, Scal *sc, double dx) {
 template <int N>
 __global__ void __launch_bounds__(256) k_mask(Geo g, Mov m, Scal *sc) {
     __shared__ double scr[32];
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     const int s = blockIdx.x, NB = g.nbody, nx = g.nx;
     const double cx = m.xc[s], cy = m.xc[s + NB], cz = m.xc[s + 2 * NB], r = g.rb;
     const int i0 = (int)ceil(cx - r), i1 = (int)floor(cx + r);
@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(256) k_mask(Geo g, Mov m, Scal *sc) {
 // neighbour sphere, counts the active ones and sets da(2) of bcset.
 __global__ void __launch_bounds__(256) k_nrpr(Geo g, Mov m, Scal *sc) {
     __shared__ double scr[32];
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     const int s = blockIdx.x, NB = g.nbody, nb = g.nbnd;
     const double px = (double)(g.nx + 1), py = (double)g.my, pz = (double)g.mz;
     const int nc = m.ncnt[s];
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(256) k_nrpr(Geo g, Mov m, Scal *sc) {
 // point count, and the solid/fluid counts of the new mask.
 __global__ void __launch_bounds__(1024) k_pts_scan(Geo g, Mov m, Scal *sc) {
     __shared__ int wsum[32];
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     const int T = blockDim.x, t = threadIdx.x, NB = g.nbody;
     const int per = (NB + T - 1) / T, c0 = min(t * per, NB), c1 = min(c0 + per, NB);
     int s = 0;
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(1024) k_pts_scan(Geo g, Mov m, Scal *sc) {
 __global__ void __launch_bounds__(256) k_pts_write(Geo g, Mov m, Scal *sc) {
     __shared__ int wsum[8];
     __shared__ int base;
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     const int s = blockIdx.x, nb = g.nbnd, t = threadIdx.x, lane = t & 31, wid = t >> 5;
     if (t == 0) base = m.ptoff[s];
     __syncthreads();
@@ -689,7 +689,7 @@ __device__ __forceinline__ ScalEval scal_eval(const Geo &g, const Mov &m, int s,
 // Evaluations per sphere.
 __global__ void __launch_bounds__(256) k_sev_count(Geo g, Mov m, Scal *sc) {
     __shared__ double scr[32];
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     const int s = blockIdx.x, nb = g.nbnd;
     double n = 0.0;
     for (int l = threadIdx.x; l < nb; l += blockDim.x)
@@ -701,7 +701,7 @@ __global__ void __launch_bounds__(256) k_sev_count(Geo g, Mov m, Scal *sc) {
 // Offsets of every sphere's evaluations and their total.
 __global__ void __launch_bounds__(1024) k_sev_scan(Geo g, Mov m, Scal *sc) {
     __shared__ int wsum[32];
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     const int T = blockDim.x, t = threadIdx.x, NB = g.nbody;
     const int per = (NB + T - 1) / T, c0 = min(t * per, NB), c1 = min(c0 + per, NB);
     int s = 0;
@@ -726,7 +726,7 @@ __global__ void __launch_bounds__(1024) k_sev_scan(Geo g, Mov m, Scal *sc) {
 __global__ void __launch_bounds__(256) k_sev_write(Geo g, Mov m, Scal *sc) {
     __shared__ int wsum[8];
     __shared__ int base;
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     const int s = blockIdx.x, nb = g.nbnd, t = threadIdx.x, lane = t & 31, wid = t >> 5, mxf = g.nx + 1;
     if (t == 0) base = m.sev_off[s];
     __syncthreads();

@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(LT * 32) k_slines(Geo g, double2 *__restrict__
     double *pw = (double *)(RHS + LT * NP);        // mu^(i+1)
     double *ipw = pw + NX;                         // mu^-(i+1)
     double2 *st = (double2 *)(ipw + NX);           // cross-lane stage twiddles
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     fill_stage_table<32>(st, g.tw, NX);
     const int PS = g.PS, nx = NX;
     const double h = sc->heat_ratio, H = sc->heat_ratio_new;
@@ -678,7 +678,7 @@ static size_t slines_smem() {
 // heat_ratio update, surface flux and Nusselt number (bcsetscal, bc_scalar.F90:186-190,
 // 361-363; stepthescalar.F90:90-91), status.
 __global__ void __launch_bounds__(256) k_sfin(Geo g, Scal *sc, const double *sdpart, double *flux_body) {
-    if (sc->status) return;
+    if (block_failed(sc)) return;
     for (int m = threadIdx.x; m < g.nbody; m += blockDim.x) {
         double f = 0.0;
         for (int q = 0; q < kDragSplit; ++q) f += sdpart[(size_t)m * kDragSplit + q];

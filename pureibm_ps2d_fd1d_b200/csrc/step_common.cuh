@@ -45,6 +45,12 @@ template <int N> __device__ __forceinline__ double2 r2c_norm(double2 x, double n
         return make_double2(x.x / nrm, x.y / nrm);
     }
 }
+// The run's status word for a block-wide early return: the OR over the
+// block's threads, so that every thread takes the same branch before the
+// block's barriers although another kernel, or another block of this one,
+// may set the word while the block starts.  Call with every thread present.
+__device__ __forceinline__ bool block_failed(const Scal *sc) { return __syncthreads_or(sc->status != 0) != 0; }
+
 // Bounded wait on the CTA's load barrier; records a timeout in the status word.
 __device__ __forceinline__ void load_wait(uint64_t *mb, uint32_t &phase, Scal *sc) {
     if (!mbar_wait(mb, phase)) atomicCAS(&sc->status, 0, PIBM_ERR_TIMEOUT);
