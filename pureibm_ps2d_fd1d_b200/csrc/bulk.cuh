@@ -68,4 +68,47 @@ __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.w
 // One thread: wait until every committed bulk store has completed.
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
+// ---- tensor-map (tiled) copies, this GPU's memory only, no multicast ----
+// One thread: arrive on mb announcing `bytes` of transaction.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *mb, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mb)), "r"(bytes) : "memory");
+}
+// One thread: plain arrive (completes a phase that expects no bytes).
+__device__ __forceinline__ void mbar_arrive(uint64_t *mb) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mb)) : "memory");
+}
+// One thread: load the box at element coordinates (x, y, z) of a 3-D tensor
+// map into shared memory (completes on mb).  x * element size must be a
+// multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, int x, int y, int z, uint64_t *mb) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_u32(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(mb))
+        : "memory");
+}
+// One thread: store a shared-memory box to coordinates (x, y, z) (bulk group;
+// commit with bulk_commit).  Writers of the box fence (fence_async_smem) and
+// synchronise with the issuing thread first.
+__device__ __forceinline__ void tma_store_3d(const void *tmap, const void *src, int x, int y, int z) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(tmap),
+                 "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Barrier over `count` threads (whole warps) on hardware barrier `id` that
+// also returns the AND of v over them (the same answer in every thread).
+__device__ __forceinline__ bool named_bar_and(int id, int count, bool v) {
+    int r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.s32 q, %1, 0;\n\tbar.red.and.pred p, %2, %3, q;\n\tselp.s32 %0, 1, 0, p;\n\t}"
+                 : "=r"(r)
+                 : "r"((int)v), "r"(id), "r"(count)
+                 : "memory");
+    return r != 0;
+}
+// Barrier over `count` threads (whole warps) on hardware barrier `id` (1..15; 0 is __syncthreads').
+__device__ __forceinline__ void named_bar_sync(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 }  // namespace pibm

@@ -55,7 +55,7 @@ struct Scal {
     double frame_accln[3];
     unsigned long long divmax_bits;
     int status;
-    int pad;
+    unsigned lines_done;   // persistent x-line kernel: blocks finished (0 between launches)
     long long nsteps;
     // passive scalar: phi(x + Lx) = phi(x) / heat_ratio
     double heat_ratio, heat_ratio_old, heat_ratio_new, flux_global, nusselt;
@@ -66,7 +66,8 @@ struct Scal {
     double maxvolfrac;
     int npts;
     int dem_substeps;
-    int nsev, pad2;
+    int nsev;
+    unsigned lines_next;   // persistent x-line kernel: next tile ticket (0 between launches)
     double usmean_act[3], frame_vel[3], frame_pos[3];
 };
 

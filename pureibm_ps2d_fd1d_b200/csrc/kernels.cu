@@ -27,8 +27,11 @@
 // The IBM force needs -c3 nl - c4 onl - c12 diffn only at the inner reversal
 // points; by linearity of the transform and of the interpolation it is formed
 // once in spectral space (Q) instead of three separately interpolated fields.
+#include <algorithm>
+
 #include "step_common.cuh"
 #include "line_solve.cuh"
+#include "lines_pipe.cuh"
 #include "../../include/pibm.h"
 
 namespace pibm {
@@ -878,8 +881,6 @@ __device__ __forceinline__ void b_lines(const Geo &g, double2 *__restrict__ u, d
         const int line = t % LT, i = t / LT;
         const int q = min(q0 + line, PS - 1);   // clamped: every lane takes part in the shuffles
         const double ky = KY(q), kz = KZ(q);
-        auto mwy = [&](double2 z) { return make_double2(-ky * z.y, ky * z.x); };
-        auto mwz = [&](double2 z) { return make_double2(-kz * z.y, kz * z.x); };
         double2 x0[9], x1[9];   // nl, ff, onl (3 components each) at planes i and i+1
 #pragma unroll
         for (int n = 0; n < 3; ++n) { x0[n] = G(nl, n, i, q); x0[3 + n] = G(ff, n, i, q); x0[6 + n] = G(onl, n, i, q); }
@@ -894,52 +895,41 @@ __device__ __forceinline__ void b_lines(const Geo &g, double2 *__restrict__ u, d
             for (int n = 0; n < 3; ++n) { x1[n] = G(nl, n, i + 1, q); x1[3 + n] = G(ff, n, i + 1, q); x1[6 + n] = G(onl, n, i + 1, q); }
         }
         if (q0 + line >= PS) continue;
-        double2 tt = make_double2(0.0, 0.0), d, s;
-        d = csub(x1[0], x0[0]);
-        s = csub(x1[3], x0[3]);
-        tt = make_double2(tt.x + qdiv(c3 * d.x, dx, rdx) + qdiv(s.x, dx, rdx), tt.y + qdiv(c3 * d.y, dx, rdx) + qdiv(s.y, dx, rdx));
-        d = mwy(cadd(x1[1], x0[1]));
-        s = mwy(cadd(x1[4], x0[4]));
-        tt = make_double2(tt.x + (c3 * d.x) / 2.0 + s.x / 2.0, tt.y + (c3 * d.y) / 2.0 + s.y / 2.0);
-        d = mwz(cadd(x1[2], x0[2]));
-        s = mwz(cadd(x1[5], x0[5]));
-        tt = make_double2(tt.x + (c3 * d.x) / 2.0 + s.x / 2.0, tt.y + (c3 * d.y) / 2.0 + s.y / 2.0);
-        d = csub(x1[6], x0[6]);
-        tt = make_double2(tt.x + qdiv(c4 * d.x, dx, rdx), tt.y + qdiv(c4 * d.y, dx, rdx));
-        d = mwy(cadd(x1[7], x0[7]));
-        tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
-        d = mwz(cadd(x1[8], x0[8]));
-        tt = make_double2(tt.x + (c4 * d.x) / 2.0, tt.y + (c4 * d.y) / 2.0);
+        // pressure source, its terms in the reference's order: (nl, ff) per component, then onl
+        double2 tt = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int n = 0; n < 3; ++n) {
+            tt = cadd_rn(tt, psrc_term<true>(n, c3, x0[n], x1[n], ky, kz, dx, rdx));
+            tt = cadd_rn(tt, psrc_term<false>(n, 1.0, x0[3 + n], x1[3 + n], ky, kz, dx, rdx));
+        }
+#pragma unroll
+        for (int n = 0; n < 3; ++n) tt = cadd_rn(tt, psrc_term<true>(n, c4, x0[6 + n], x1[6 + n], ky, kz, dx, rdx));
         RHS[line * NP + i] = make_double2(qdiv(tt.x, c12, rc12), qdiv(tt.y, c12, rc12));
         P[line * NP + i] = p[(size_t)i * PS + q];
         // explicit part of the ustep right-hand sides, dt*(c3 nl + ff + c4 onl) per component
         // (usteptime.F90:291-297), kept in the velocity tiles until each component is solved
 #pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            const double2 nn = x0[n], f = x0[3 + n], on = x0[6 + n];
-            U[(n * LT + line) * NP + i] = make_double2(((dt * c3) * nn.x + dt * f.x) + (dt * c4) * on.x,
-                                                       ((dt * c3) * nn.y + dt * f.y) + (dt * c4) * on.y);
-        }
+        for (int n = 0; n < 3; ++n)
+            U[(n * LT + line) * NP + i] = cadd_rn(cadd_rn(cscale_rn(x0[n], dt * c3), cscale_rn(x0[3 + n], dt)), cscale_rn(x0[6 + n], dt * c4));
     }
     __syncthreads();
     const int qw = q0 + w;
     const bool wact = qw < PS;
     const double w2w = wact ? g.w2[qw] : 0.0;
+    const LineCoef kw = line_coef(dt, vis, c1, c2, dx2, w2w);   // line qw's coefficients
     {
-        const double a = 1.0 / dx2 - 0.25 * w2w, bd = -2.0 / dx2 - 0.5 * w2w, c = 1.0 / dx2 - 0.25 * w2w;
         double2 *row = RHS + w * NP;
         if (wact) {
             if (qw == 0) {
-                if (lane == 0) ok = thomas_real(row, gam, a, bd, c, NX - 1) && ok;
+                if (lane == 0) ok = thomas_real(row, gam, kw.pa, kw.pb, kw.pc, NX - 1) && ok;
                 __syncwarp();
             } else {
-                circulant_solve<R>(row, a, bd, tw, lane);
+                circulant_solve<R>(row, kw.pa, kw.pb, tw, lane);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int i = lane + 32 * r;
-                const double2 po = P[w * NP + i], tp = row[i];
-                P[w * NP + i] = make_double2(po.x + 1.0 * (tp.x - po.x), po.y + 1.0 * (tp.y - po.y));
+                P[w * NP + i] = p_update(P[w * NP + i], row[i]);
             }
         }
     }
@@ -960,26 +950,10 @@ __device__ __forceinline__ void b_lines(const Geo &g, double2 *__restrict__ u, d
             const int t = threadIdx.x + k * LT * 32;
             const int line = t % LT, i = t / LT, q = q0 + line;
             if (q >= PS) continue;
-            const double ky = KY(q), kz = KZ(q), w2 = g.w2[q];
-            const double alp = dt * (c1 + c2);
-            const double fy = 1.0 - dt * vis * c1 * w2;
-            const double gd = 1.0 * dt * vis * c1;
-            const double2 ui = RHS[line * NP + i];
-            const double2 ex = U[(n * LT + line) * NP + i];
-            double2 r = make_double2(ui.x * fy + ex.x, ui.y * fy + ex.y);
-            const double2 pm = P[line * NP + (i == 0 ? nx - 1 : i - 1)], p0 = P[line * NP + i];
-            double2 gp;
-            if (n == 0) gp = make_double2(qdiv(alp * (p0.x - pm.x), dx, rdx), qdiv(alp * (p0.y - pm.y), dx, rdx));
-            else {
-                const double2 sp = make_double2(alp * 0.5 * (pm.x + p0.x), alp * 0.5 * (pm.y + p0.y));
-                gp = (n == 1) ? make_double2(-ky * sp.y, ky * sp.x) : make_double2(-kz * sp.y, kz * sp.x);
-            }
-            r = csub(r, gp);
-            const double2 um = RHS[line * NP + (i == 0 ? nx - 1 : i - 1)], up = RHS[line * NP + (i == nx - 1 ? 0 : i + 1)];
-            double2 lap;
-            if (i == 0) lap = make_double2((up.x - 2.0 * ui.x) + um.x, (up.y - 2.0 * ui.y) + um.y);
-            else lap = make_double2((um.x + up.x) - 2.0 * ui.x, (um.y + up.y) - 2.0 * ui.y);
-            rr[k] = make_double2(r.x + qdiv(gd * lap.x, dx2, rdx2), r.y + qdiv(gd * lap.y, dx2, rdx2));
+            const LineCoef kq = line_coef(dt, vis, c1, c2, dx2, g.w2[q]);
+            const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
+            rr[k] = ustep_rhs(n, kq, RHS[line * NP + i], RHS[line * NP + im], RHS[line * NP + ip], U[(n * LT + line) * NP + i],
+                              P[line * NP + im], P[line * NP + i], i == 0, KY(q), KZ(q), dx, rdx, dx2, rdx2);
         }
         __syncthreads();
 #pragma unroll
@@ -990,58 +964,42 @@ __device__ __forceinline__ void b_lines(const Geo &g, double2 *__restrict__ u, d
         }
         __syncthreads();
         if (wact) {
-            const double a = -(1.0 * dt * vis * c2 / dx2);
-            const double bd = 1.0 + dt * vis * c2 * (1.0 * 2.0 / dx2 + w2w);
             double2 *row = RHS + w * NP;
-            circulant_solve<R>(row, a, bd, tw, lane);
+            circulant_solve<R>(row, kw.ua, kw.ub, tw, lane);
 #pragma unroll
             for (int r = 0; r < R; ++r) U[(n * LT + w) * NP + lane + 32 * r] = row[lane + 32 * r];
         }
         __syncthreads();
     }
     // ---------------- divcorr (poisson.F90:241-508) ----------------
-    const double alpc = (c1 + c2) * dt, ralpc = 1.0 / alpc;
+    const double alpc = kw.alp, ralpc = 1.0 / alpc;
     for (int t = threadIdx.x; t < LT * NX; t += blockDim.x) {
         const int line = t % LT, i = t / LT, q = q0 + line;
         if (q >= PS) continue;
-        const double ky = KY(q), kz = KZ(q);
         const int ip = i == nx - 1 ? 0 : i + 1;
         const double2 *U1 = U + (0 * LT + line) * NP, *U2 = U + (1 * LT + line) * NP, *U3 = U + (2 * LT + line) * NP;
-        double2 tt = make_double2(qdiv(U1[ip].x - U1[i].x, dx, rdx), qdiv(U1[ip].y - U1[i].y, dx, rdx));
-        double2 sy = cscale(cadd(U2[i], U2[ip]), 0.5), sz = cscale(cadd(U3[i], U3[ip]), 0.5);
-        tt = cadd(tt, make_double2(-ky * sy.y, ky * sy.x));
-        tt = cadd(tt, make_double2(-kz * sz.y, kz * sz.x));
-        RHS[line * NP + i] = make_double2(qdiv(0.5 * (1.0 + 1.0) * tt.x, alpc, ralpc), qdiv(0.5 * (1.0 + 1.0) * tt.y, alpc, ralpc));
+        const double2 tt = div_term(U1[i], U1[ip], U2[i], U2[ip], U3[i], U3[ip], KY(q), KZ(q), dx, rdx);
+        RHS[line * NP + i] = make_double2(qdiv(tt.x, alpc, ralpc), qdiv(tt.y, alpc, ralpc));
     }
     __syncthreads();
     if (wact) {
-        const double a = 1.0 / dx2 - 0.25 * w2w, bd = -2.0 / dx2 - 0.5 * w2w, c = 1.0 / dx2 - 0.25 * w2w;
         const double ky = KY(qw), kz = KZ(qw);
         double2 *row = RHS + w * NP;
         if (qw == 0) {
-            if (lane == 0) ok = thomas_real(row, gam, a, bd, c, NX - 1) && ok;
+            if (lane == 0) ok = thomas_real(row, gam, kw.pa, kw.pb, kw.pc, NX - 1) && ok;
             __syncwarp();
         } else {
-            circulant_solve<R>(row, a, bd, tw, lane);
+            circulant_solve<R>(row, kw.pa, kw.pb, tw, lane);
         }
         double2 *U1 = U + (0 * LT + w) * NP, *U2 = U + (1 * LT + w) * NP, *U3 = U + (2 * LT + w) * NP;
         double2 *Pw = P + w * NP;
-        const double c2dtv = (c2 * dt) * vis;
         double2 nu1[R], nu2[R], nu3[R], np[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int i = lane + 32 * r;
             const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
-            const double2 d0 = row[i], dm = row[im], dp = row[ip];
-            const double2 s = cadd(dm, d0);
-            double2 gy, gz;
-            if (i == 0) { gy = cscale(make_double2(-ky * 0.0, ky * alpc), 0.5); gz = cscale(make_double2(-kz * 0.0, kz * alpc), 0.5); }
-            else { gy = make_double2(-ky * 0.0, ky * (alpc * 0.5)); gz = make_double2(-kz * 0.0, kz * (alpc * 0.5)); }
-            nu1[r] = make_double2(U1[i].x - qdiv(alpc * (d0.x - dm.x), dx, rdx), U1[i].y - qdiv(alpc * (d0.y - dm.y), dx, rdx));
-            nu2[r] = csub(U2[i], cmul(gy, s));
-            nu3[r] = csub(U3[i], cmul(gz, s));
-            const double2 lap = make_double2(qdiv((dm.x - 2.0 * d0.x) + dp.x, dx2, rdx2) - w2w * d0.x, qdiv((dm.y - 2.0 * d0.y) + dp.y, dx2, rdx2) - w2w * d0.y);
-            np[r] = make_double2((Pw[i].x + d0.x) - c2dtv * lap.x, (Pw[i].y + d0.y) - c2dtv * lap.y);
+            divcorr_update(kw, row[i], row[im], row[ip], i == 0, U1[i], U2[i], U3[i], Pw[i], ky, kz, w2w, dx, rdx, dx2, rdx2, nu1[r],
+                           nu2[r], nu3[r], np[r]);
         }
         __syncwarp();
 #pragma unroll
@@ -1055,11 +1013,7 @@ __device__ __forceinline__ void b_lines(const Geo &g, double2 *__restrict__ u, d
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int i = lane + 32 * r, ip = i == nx - 1 ? 0 : i + 1;
-            double2 tt = make_double2(qdiv(U1[ip].x - U1[i].x, dx, rdx), qdiv(U1[ip].y - U1[i].y, dx, rdx));
-            double2 sy = cscale(cadd(U2[i], U2[ip]), 0.5), sz = cscale(cadd(U3[i], U3[ip]), 0.5);
-            tt = cadd(tt, make_double2(-ky * sy.y, ky * sy.x));
-            tt = cadd(tt, make_double2(-kz * sz.y, kz * sz.x));
-            dmax = fmax(dmax, sqrt(tt.x * tt.x + tt.y * tt.y));
+            dmax = fmax(dmax, cabs_rn(div_term(U1[i], U1[ip], U2[i], U2[ip], U3[i], U3[ip], ky, kz, dx, rdx)));
         }
         for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
         if (lane == 0) atomicMax(&sc->divmax_bits, (unsigned long long)__double_as_longlong(dmax));
@@ -1088,10 +1042,65 @@ static size_t lines_smem(int lt) {
     const int np = lt == 4 ? lines_pitch<NX, 4>() : lines_pitch<NX, 8>();
     return (size_t)(NX + 5 * lt * np + 32) * sizeof(double2) + NX * sizeof(double) + line_tw_bytes<NX / 32>();
 }
+// Tensor maps of the persistent x-line kernel (lines_pipe.cuh): a field of
+// ncomp components [comp][i][PS complex] as FLOAT64 {2 PS, nx, ncomp}, box
+// {8, N, 1} (4 lines x N planes), 64-byte swizzle.  The encoder comes from
+// the driver through the runtime's entry-point query (no libcuda link).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *, const cuuint64_t *,
+                                  const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = []() -> EncodeTiledFn {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+static bool line_map(CUtensorMap *m, const void *base, int PS, int nx, int ncomp, int N) {
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t dim[3] = {(cuuint64_t)2 * PS, (cuuint64_t)nx, (cuuint64_t)ncomp};
+    const cuuint64_t stride[2] = {(cuuint64_t)PS * 16, (cuuint64_t)nx * PS * 16};
+    const cuuint32_t box[3] = {8, (cuuint32_t)N, 1}, es[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(base), dim, stride, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+// SMs of the current device (cached per device).
+static int sm_count() {
+    static int cache[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (!cache[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+// The 4-line width runs the persistent tensor-map kernel on grids up to 128
+// (three blocks of 72 KB per SM); at 256 a slab is 16 KB and the staged
+// kernel is kept.  Both give bitwise the same results.
 template <int N>
 static void launch_lines(const Geo &g, DevBufs &b, double2 *u, double2 *p, int cur, Scal *sc, cudaStream_t s) {
     const int old = cur ^ 1;
     const int lt = g.lines_lt ? g.lines_lt : LinesCfg<N>::LT;
+    if constexpr (N <= 128) {
+        if (lt == 4 && g.PS % LPipe<N>::LT == 0) {
+            LineMaps mp;
+            if (line_map(&mp.u, u, g.PS, g.nx, 3, N) && line_map(&mp.p, p, g.PS, g.nx, 1, N) &&
+                line_map(&mp.nl, b.nl[cur], g.PS, g.nx, 3, N) && line_map(&mp.onl, b.nl[old], g.PS, g.nx, 3, N) &&
+                line_map(&mp.ff, b.ff, g.PS, g.nx, 3, N)) {
+                const int grid = std::min(g.PS / LPipe<N>::LT, LPipe<N>::MINB * sm_count());
+                k_lines_pipe<N><<<grid, LPipe<N>::T, LPipe<N>::SMEM, s>>>(g, mp, sc);
+                return;
+            }
+        }
+    }
     if (lt == 4) k_lines<N, 4><<<(g.PS + 3) / 4, 4 * 32, lines_smem<N>(4), s>>>(g, u, p, b.nl[cur], b.nl[old], b.ff, sc);
     else k_lines<N, 8><<<(g.PS + 7) / 8, 8 * 32, lines_smem<N>(8), s>>>(g, u, p, b.nl[cur], b.nl[old], b.ff, sc);
 }
@@ -1343,6 +1352,8 @@ static cudaError_t set_attrs() {
     if ((e = cudaFuncSetAttribute(k_ff2rc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_lines<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>(4))) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_lines<N, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lines_smem<N>(8))) != cudaSuccess) return e;
+    if constexpr (N <= 128)
+        if ((e = cudaFuncSetAttribute(k_lines_pipe<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, LPipe<N>::SMEM)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(kb_a0<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(kb_nl<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(kb_ff<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs)) != cudaSuccess) return e;
