@@ -1571,26 +1571,35 @@ void enqueue_r2c(const Geo &g, const double *a, double2 *b, int nplanes, cudaStr
 }
 
 // ---------------------------------------------------------------------------
-// Autotuner of the x-line tile width: every candidate width runs the line
-// kernel on scratch copies of u, p and the step scalars (the run's state is
-// not touched; the line kernel's results do not depend on the width): one
-// warm-up launch, then `reps` launches back to back timed together, as the
-// kernel runs inside the step graph; the fastest width is kept in
-// g.lines_lt.  ms[k] = mean time per launch of candidate kLinesTiles[k].
+// Autotuner of the x-line tile width: every candidate width runs on scratch
+// copies of the state (the run's own state is not touched; results do not
+// depend on the width): whole steps where the state is u, p, nl and the
+// scalars, else the line kernel behind the forcing transform; two warm-up
+// units, then `reps` units timed together; the fastest width is kept in
+// g.lines_lt.  ms[k] = mean time per unit of candidate kLinesTiles[k].
 // ---------------------------------------------------------------------------
 extern const int kLinesTiles[2] = {4, 8};
 template <int N>
 static cudaError_t autotune_lines_t(Geo &g, DevBufs &b, int cur, cudaStream_t s, double ms[2]) {
     const size_t SC = (size_t)g.nx * g.PS;
-    double2 *u = nullptr, *p = nullptr;
+    // Runs whose whole state is u, p, nl and the scalars (fixed particles, no
+    // passive scalar) time complete steps on scratch copies of that state:
+    // the line kernel's cost depends on what runs beside and before it (the
+    // persistent kernel measured faster inside the step and slower in
+    // isolation than the staged one).  Other runs time the line kernel behind
+    // the forcing transform that precedes it.
+    const bool whole = !g.moving && !g.scal;
+    double2 *u = nullptr, *p = nullptr, *nl0 = nullptr, *nl1 = nullptr;
     Scal *sc = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t e = cudaMalloc(&u, 3 * SC * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&p, SC * sizeof(double2));
+    if (e == cudaSuccess && whole) e = cudaMalloc(&nl0, 3 * SC * sizeof(double2));
+    if (e == cudaSuccess && whole) e = cudaMalloc(&nl1, 3 * SC * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&sc, sizeof(Scal));
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
-    const int reps = 10;
+    const int reps = whole ? 6 : 10;
     double best = 1e30;
     int pick = 0;
     for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
@@ -1599,9 +1608,29 @@ static cudaError_t autotune_lines_t(Geo &g, DevBufs &b, int cur, cudaStream_t s,
         cudaMemcpyAsync(u, b.u, 3 * SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(p, b.p, SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(sc, b.sc, sizeof(Scal), cudaMemcpyDeviceToDevice, s);
-        launch_lines<N>(gt, b, u, p, cur, sc, s);   // warm-up
+        DevBufs bt = b;
+        if (whole) {
+            cudaMemcpyAsync(nl0, b.nl[0], 3 * SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(nl1, b.nl[1], 3 * SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+            bt.u = u; bt.p = p; bt.nl[0] = nl0; bt.nl[1] = nl1; bt.sc = sc;
+        }
+        int c = cur;
+        auto unit = [&]() {
+            if (whole) {
+                enqueue_step(gt, bt, c, s, nullptr, nullptr, nullptr);
+                c ^= 1;
+            } else {
+                // the forcing transform writes only the work field ff, which the
+                // step recomputes before its line kernel; runs without
+                // particles have no forcing (fr is not allocated, ff stays zero)
+                if (g.nbody > 0 && b.fr) launch_planes<N>(k_ff<N>, g.nx, 3, s, g, (const double *)b.fr, b.ff, sc);
+                launch_lines<N>(gt, b, u, p, cur, sc, s);
+            }
+        };
+        unit();   // warm-up
+        unit();
         cudaEventRecord(e0, s);
-        for (int r = 0; r < reps; ++r) launch_lines<N>(gt, b, u, p, cur, sc, s);
+        for (int r = 0; r < reps; ++r) unit();
         cudaEventRecord(e1, s);
         e = cudaEventSynchronize(e1);
         float t = 0.f;
@@ -1609,12 +1638,21 @@ static cudaError_t autotune_lines_t(Geo &g, DevBufs &b, int cur, cudaStream_t s,
         ms[k] = t / reps;
         if (ms[k] < best) { best = ms[k]; pick = k; }
     }
+    // the scratch steps wrote the per-particle outputs: a run that has not
+    // stepped reports zeros
+    if (e == cudaSuccess && whole && g.nbody > 0) {
+        for (double *f : {b.pres, b.visc, b.ptot, b.force})
+            if (f) cudaMemsetAsync(f, 0, 3 * (size_t)g.nbody * sizeof(double), s);
+        e = cudaStreamSynchronize(s);
+    }
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) g.lines_lt = kLinesTiles[pick];
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaFree(u);
     cudaFree(p);
+    cudaFree(nl0);
+    cudaFree(nl1);
     cudaFree(sc);
     return e;
 }

@@ -47,15 +47,19 @@ __device__ __forceinline__ void circulant_solve_reg(double2 (&v)[R], double a, d
     dft_inlane<R>(v, -1.0, tw);
 #pragma unroll
     for (int r = 1; r < R; ++r) v[r] = cmul(v[r], lt.tr[(r - 1) * 32 + lane]);
+    // Each butterfly stage in one form for both lanes of a pair (no select of
+    // two computed branches): the upper lane forms v + pv, the lower (pv - v) w,
+    // i.e. t = pv + sgn v, then t times w' with w' = 1 on the upper lane.
 #pragma unroll
     for (int h = 16; h >= 1; h >>= 1) {
         const bool upper = (lane & h) == 0;
-        const int q = lane & (h - 1);
-        const double2 w = tw.stage(h, q, -1.0);
+        const double sgn = upper ? 1.0 : -1.0;
+        const double2 w = upper ? make_double2(1.0, 0.0) : tw.stage(h, lane & (h - 1), -1.0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            double2 pv = shfl_xor2(v[r], h, 32);
-            v[r] = upper ? cadd(v[r], pv) : cmul(csub(pv, v[r]), w);
+            const double2 pv = shfl_xor2(v[r], h, 32);
+            const double2 t = make_double2(__fma_rn(sgn, v[r].x, pv.x), __fma_rn(sgn, v[r].y, pv.y));
+            v[r] = cmul(t, w);
         }
     }
     // lane holds modes m = r + R*bitrev(lane)
@@ -65,15 +69,19 @@ __device__ __forceinline__ void circulant_solve_reg(double2 (&v)[R], double a, d
         v[r] = make_double2(qdiv(v[r].x, lam, rlam), qdiv(v[r].y, lam, rlam));
     }
     // exact inverse of the forward stages (unnormalised; 1/N folded into lam)
+    // Inverse stages: the lower lane of a pair first multiplies its own value by
+    // conj w (the upper by 1), then both take pv + sgn v: upper u + l conj w,
+    // lower u - l conj w.
 #pragma unroll
     for (int h = 1; h < 32; h <<= 1) {
         const bool upper = (lane & h) == 0;
-        const int q = lane & (h - 1);
-        const double2 w = tw.stage(h, q, +1.0);
+        const double sgn = upper ? 1.0 : -1.0;
+        const double2 w = upper ? make_double2(1.0, 0.0) : tw.stage(h, lane & (h - 1), +1.0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const double2 pv = shfl_xor2(v[r], h, 32);
-            v[r] = upper ? cadd(v[r], cmul(pv, w)) : csub(pv, cmul(v[r], w));
+            const double2 m = cmul(v[r], w);
+            const double2 pv = shfl_xor2(m, h, 32);
+            v[r] = make_double2(__fma_rn(sgn, m.x, pv.x), __fma_rn(sgn, m.y, pv.y));
         }
     }
 #pragma unroll
