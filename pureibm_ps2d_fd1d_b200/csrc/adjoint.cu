@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(256) k_adj_rev(Geo g, const double *__restrict
         make_sten(g, xli, si);
         double ft[3];
 #pragma unroll
-        for (int n = 0; n < 3; ++n) ft[n] = rec[(size_t)p * kRec + kRecF + n];
+        for (int n = 0; n < 3; ++n) ft[n] = rec[(size_t)p * 6 + n];
         const double sfac = g.da2[m] * g.dr * g.dx;
         const double kap = -(g.rb - g.ri) / (g.ro - g.rb), kapn = g.revernorm == 1 ? kap : 0.0;
         const double rnc = 1.0 / (double)g.ncell;

@@ -310,7 +310,7 @@ int pibm_create(const pibm_params *prm, const pibm_particles *parts, pibm_handle
               guard(h->alloc(&b.part, (size_t)g.nx * 8 * 12), "part") &&
               guard(h->alloc(&b.pres, 3 * (size_t)S.nbody), "pres") && guard(h->alloc(&b.visc, 3 * (size_t)S.nbody), "visc") &&
               guard(h->alloc(&b.ptot, 3 * (size_t)S.nbody), "ptot") && guard(h->alloc(&b.force, 3 * (size_t)S.nbody), "force") &&
-              guard(h->alloc(&b.rec, (size_t)kRec * g.npts), "rec") &&
+              guard(h->alloc(&b.rec, 6 * (size_t)g.npts), "rec") && guard(h->alloc(&b.rz, 3 * (size_t)g.npts), "rz") &&
               guard(h->alloc(&b.dpart, 6 * 8 * (size_t)S.nbody), "dpart") &&
               guard(h->alloc(&b.blockpart, 6 * (size_t)((g.npts + 255) / 256 + 1)), "blockpart") &&
               guard(h->alloc(&b.sc, 1), "scalars");
@@ -659,7 +659,7 @@ void slot_restore(pibm_handle *h, const char *slot, int cur) {
 static size_t fields_bytes(const pibm_handle *h, size_t *crb, size_t *recb) {
     const Geo &g = h->g;
     *crb = (size_t)g.nx * (size_t)g.RS * sizeof(double);
-    *recb = (((size_t)kRec * g.npts * sizeof(double) + 255) / 256) * 256;
+    *recb = ((6 * (size_t)g.npts * sizeof(double) + 255) / 256) * 256;
     return 13 * *crb + *recb + ((sizeof(Scal) + 255) / 256) * 256;
 }
 static void fields_save(pibm_handle *h, char *f) {
@@ -671,7 +671,7 @@ static void fields_save(pibm_handle *h, char *f) {
     cudaMemcpyAsync(f + 4 * CRb, h->b.omega, 3 * CRb, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(f + 7 * CRb, h->b.pgr, 3 * CRb, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(f + 10 * CRb, h->b.Q, 3 * CRb, cudaMemcpyDeviceToDevice, s);
-    if (h->g.npts > 0) cudaMemcpyAsync(f + 13 * CRb, h->b.rec, (size_t)kRec * h->g.npts * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (h->g.npts > 0) cudaMemcpyAsync(f + 13 * CRb, h->b.rec, 6 * (size_t)h->g.npts * sizeof(double), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(f + 13 * CRb + recb, h->b.sc, sizeof(Scal), cudaMemcpyDeviceToDevice, s);
 }
 static DevBufs fields_view(const pibm_handle *h, char *f) {

@@ -102,18 +102,12 @@ struct Mov {
     int *sspcnt, *sspbuf;
 };
 
-// k_rev's record of one active reversal point for the spreading (FlowBufs::rec):
-// kRec doubles in three 32-byte sectors, read with 16-byte loads:
-//   [0..2] the inner point's offsets in its cell (zx, zy, zz), [3] 0,
-//   [4..6] force_tmp, [7] 0, [8..10] force_dist (the solid-corner share), [11] 0.
-constexpr int kRec = 12, kRecF = 4, kRecD = 8;
-
 // Device buffers of one run.
 // The flow step's buffers (what the step kernels read and write).
 struct FlowBufs {
     double2 *u, *p, *nl[2], *ff;
     double *ubcp, *pbcp, *Q, *omega, *pgr, *fr, *Dx;
-    double *part, *pres, *visc, *ptot, *force, *rec, *dpart, *blockpart;
+    double *part, *pres, *visc, *ptot, *force, *rec, *rz, *dpart, *blockpart;
     Scal *sc;
 };
 

@@ -39,7 +39,7 @@ namespace pibm {
 void enqueue_scalar(const Geo &g, DevBufs &b, int cur, cudaStream_t s);
 int scalar_kernels_per_step(const Geo &g);
 void enqueue_moving(const Geo &g, const Mov &m, Scal *sc, const double *pres, const double *visc, cudaStream_t s);
-void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, double *fr, Scal *sc, cudaStream_t s);
+void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, const double *rz, double *fr, Scal *sc, cudaStream_t s);
 int moving_kernels_per_step(const Mov &m);
 
 // ============================================================================
@@ -57,7 +57,7 @@ __device__ __forceinline__ void b_a0(const Geo &g, const double2 *__restrict__ u
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
     double2 *buf = sm, *tws = sm + L::BUF;
-    __shared__ double scr[32 * 3];
+    __shared__ double scr[32];
     __shared__ uint64_t mb;
     if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
@@ -129,10 +129,11 @@ __device__ __forceinline__ void b_a0(const Geo &g, const double2 *__restrict__ u
                 sa += v;
                 mx = fmax(mx, fabs(v));
             }
-            double v3[3] = {sf, ss, sa};
-            block_reduce_k<3>(v3, scr);   // the three sums of block_sum's tree, two barriers
+            sf = block_sum(sf, scr);
+            ss = block_sum(ss, scr);
+            sa = block_sum(sa, scr);
             mx = block_max(mx, scr);
-            if (threadIdx.x == 0) { part[slot + t] = v3[0]; part[slot + 3 + t] = v3[1]; part[slot + 6 + t] = v3[2]; part[slot + 9 + t] = mx; }
+            if (threadIdx.x == 0) { part[slot + t] = sf; part[slot + 3 + t] = ss; part[slot + 6 + t] = sa; part[slot + 9 + t] = mx; }
         }
         double *dst = t < 3 ? ubcp + ((size_t)t * nx + i) * RSP
                     : t == 3 ? pbcp + (size_t)i * RSP
@@ -619,9 +620,9 @@ __global__ void __launch_bounds__(256) k_scal_b(Geo g, Scal *sc, double *pres, d
 // ============================================================================
 // k_rev: direct forcing at the inner reversal points
 // (calc_inner_reversal_forcing, boundary_condition.F90:1104-1479).
-// rec[p*kRec ...] = the point's record (step_common.cuh): the inner point's
-// offsets in its cell, force_tmp and force_dist (the spreading forms each
-// corner's weight*force_tmp/dx^3 from them, corner_contrib); blockpart = sums of
+// rec[p*6 + 0..2] = force_tmp, rec[p*6 + 3..5] = force_dist, rz[p*3 + 0..2] =
+// the inner point's offsets in its cell (the spreading forms each corner's
+// weight*force_tmp/dx^3 from them, corner_contrib); blockpart = sums of
 // tmppa/dx^3 over all corners (frmean) and over fluid corners (frmeanfluid).
 // ============================================================================
 __device__ __forceinline__ void inner_point(const Geo &g, int m, int l, double xli[3]) {
@@ -633,7 +634,7 @@ __device__ __forceinline__ void inner_point(const Geo &g, int m, int l, double x
 template <int N>
 __device__ __forceinline__ void b_rev(const Geo &g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
                                                 const double *__restrict__ Q, const Scal *__restrict__ sc,
-                                                double *__restrict__ rec, double *__restrict__ blockpart) {
+                                                double *__restrict__ rec, double *__restrict__ rz, double *__restrict__ blockpart) {
     __shared__ double scr[32 * 6];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     double fm[3] = {0, 0, 0}, ffl[3] = {0, 0, 0};
@@ -712,16 +713,15 @@ __device__ __forceinline__ void b_rev(const Geo &g, const double *__restrict__ u
                     count_fl += fl ? 1 : 0;
                 }
         const int count_so = 8 - count_fl;
-        double fd[3];
+        rz[(size_t)p * 3] = si.xv[1];
+        rz[(size_t)p * 3 + 1] = si.yv[1];
+        rz[(size_t)p * 3 + 2] = si.zv[1];
+        double *r = rec + (size_t)p * 6;
 #pragma unroll
-        for (int n = 0; n < 3; ++n) fd[n] = count_so > 0 ? force_fl[n] / (double)count_so : 0.0;
-        double2 *r = reinterpret_cast<double2 *>(rec) + (size_t)p * (kRec / 2);
-        r[0] = make_double2(si.xv[1], si.yv[1]);
-        r[1] = make_double2(si.zv[1], 0.0);
-        r[2] = make_double2(ft[0], ft[1]);
-        r[3] = make_double2(ft[2], 0.0);
-        r[4] = make_double2(fd[0], fd[1]);
-        r[5] = make_double2(fd[2], 0.0);
+        for (int n = 0; n < 3; ++n) {
+            r[n] = ft[n];
+            r[3 + n] = count_so > 0 ? force_fl[n] / (double)count_so : 0.0;
+        }
     }
     double v[6] = {fm[0], fm[1], fm[2], ffl[0], ffl[1], ffl[2]};
     block_reduce_k<6>(v, scr);
@@ -731,7 +731,7 @@ __device__ __forceinline__ void b_rev(const Geo &g, const double *__restrict__ u
 template <int N>
 __global__ void __launch_bounds__(256, 3) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
                                                 const double *__restrict__ Q, const Scal *__restrict__ sc,
-                                                double *__restrict__ rec, double *__restrict__ blockpart) { b_rev<N>(g, ubcp, pgr, Q, sc, rec, blockpart); }
+                                                double *__restrict__ rec, double *__restrict__ rz, double *__restrict__ blockpart) { b_rev<N>(g, ubcp, pgr, Q, sc, rec, rz, blockpart); }
 
 __device__ __forceinline__ void b_scal_c(const Geo &g, Scal *sc, const double *blockpart, int nblocks) {
     __shared__ double scr[32 * 6];
@@ -752,8 +752,8 @@ __global__ void __launch_bounds__(256) k_scal_c(Geo g, Scal *sc, const double *b
 // k_spread: fr at every forced node, accumulated over its (point, corner)
 // contributions in the reference's (sphere, point) order
 // (boundary_condition.F90:1425-1462).  sp_node holds physical offsets.
-__device__ __forceinline__ void b_spread(const Geo &g, const double *__restrict__ rec, double *__restrict__ fr,
-                                         const Scal *__restrict__ sc) {
+__device__ __forceinline__ void b_spread(const Geo &g, const double *__restrict__ rec, const double *__restrict__ rz,
+                                                double *__restrict__ fr, const Scal *__restrict__ sc) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.sp_nnodes || sc->status) return;
     const int node = g.sp_node[q];
@@ -763,22 +763,23 @@ __device__ __forceinline__ void b_spread(const Geo &g, const double *__restrict_
 #pragma unroll 4
     for (int e = e0; e < e1; ++e) {
         const int ent = __ldg(g.sp_ent + e);
-        double t[3], d[3];
-        corner_contrib(rec, ent, g.dx3, rdx3, t, !g.include_frmeanfluid, d);
+        double t[3];
+        corner_contrib(rz, rec, ent, g.dx3, rdx3, t);
         if (g.include_frmeanfluid) {
 #pragma unroll
             for (int n = 0; n < 3; ++n) acc[n] = acc[n] + t[n];
         } else {
+            const double *r = rec + (size_t)(ent >> 3) * 6 + 3;
 #pragma unroll
-            for (int n = 0; n < 3; ++n) acc[n] = (acc[n] + t[n]) + d[n];
+            for (int n = 0; n < 3; ++n) acc[n] = (acc[n] + t[n]) + __ldg(r + n);
         }
     }
     const size_t CR = (size_t)g.nx * g.RS;
 #pragma unroll
     for (int n = 0; n < 3; ++n) fr[n * CR + node] = acc[n];
 }
-__global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, double *__restrict__ fr,
-                                                const Scal *__restrict__ sc) { b_spread(g, rec, fr, sc); }
+__global__ void __launch_bounds__(256) k_spread(Geo g, const double *__restrict__ rec, const double *__restrict__ rz,
+                                                double *__restrict__ fr, const Scal *__restrict__ sc) { b_spread(g, rec, rz, fr, sc); }
 
 // k_ff: ff = r2c(fr - frmean) (boundary_condition.F90:678-700).
 template <int N>
@@ -1253,7 +1254,7 @@ template <int N>
 __global__ void __launch_bounds__(256, 3) kb_rev(const __grid_constant__ MemberSet ms) {
     const Member &m = ms.m[blockIdx.z];
     if (m.g.nbody == 0 || m.g.npts == 0 || (int)blockIdx.x >= m.nbk) return;
-    b_rev<N>(m.g, m.b.ubcp, m.b.pgr, m.b.Q, m.b.sc, m.b.rec, m.b.blockpart);
+    b_rev<N>(m.g, m.b.ubcp, m.b.pgr, m.b.Q, m.b.sc, m.b.rec, m.b.rz, m.b.blockpart);
 }
 __global__ void __launch_bounds__(256) kb_scal_c(const __grid_constant__ MemberSet ms) {
     const Member &m = ms.m[blockIdx.z];
@@ -1263,7 +1264,7 @@ __global__ void __launch_bounds__(256) kb_scal_c(const __grid_constant__ MemberS
 __global__ void __launch_bounds__(256) kb_spread(const __grid_constant__ MemberSet ms) {
     const Member &m = ms.m[blockIdx.z];
     if (m.g.nbody == 0 || m.g.npts == 0) return;
-    b_spread(m.g, m.b.rec, m.b.fr, m.b.sc);
+    b_spread(m.g, m.b.rec, m.b.rz, m.b.fr, m.b.sc);
 }
 template <int N>
 __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_ff(const __grid_constant__ MemberSet ms) {
@@ -1478,7 +1479,7 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {
             kb(PIBM_K_REV);
-            k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.blockpart);
+            k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.rz, b.blockpart);
             ke(PIBM_K_REV);
             if (fork && !scal_first) {
                 // frmean (read from k_ff on) beside the spreading, which does not read it
@@ -1492,8 +1493,8 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
                 ke(PIBM_K_SCAL_C);
             }
             kb(PIBM_K_SPREAD);
-            if (g.moving) enqueue_spread_dyn(g, b.mov, b.rec, b.fr, b.sc, s);
-            else if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.fr, b.sc);
+            if (g.moving) enqueue_spread_dyn(g, b.mov, b.rec, b.rz, b.fr, b.sc, s);
+            else if (g.sp_nnodes > 0) k_spread<<<(g.sp_nnodes + 255) / 256, 256, 0, s>>>(g, b.rec, b.rz, b.fr, b.sc);
             ke(PIBM_K_SPREAD);
             if (fork && !scal_first) cudaStreamWaitEvent(s, ss->frmean_done, 0);
         } else {

@@ -629,8 +629,8 @@ __device__ __forceinline__ void bucket_in_order(const int *bucket, int c, F f) {
 
 // fr at every node: the bucket's contributions in ascending (point, corner)
 // order, the reference's accumulation order; nodes without force get zero.
-__global__ void __launch_bounds__(256) k_spread_dyn(Geo g, Mov m, const double *__restrict__ rec, double *__restrict__ fr,
-                                                    Scal *sc) {
+__global__ void __launch_bounds__(256) k_spread_dyn(Geo g, Mov m, const double *__restrict__ rec,
+                                                    const double *__restrict__ rz, double *__restrict__ fr, Scal *sc) {
     const size_t node = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t CR = (size_t)g.nx * g.RS;
     if (node >= CR || sc->status) return;
@@ -639,14 +639,15 @@ __global__ void __launch_bounds__(256) k_spread_dyn(Geo g, Mov m, const double *
     const int c = min(m.spcnt[node], m.kmax);
     if (c > 0)
         bucket_in_order(m.spbuf + node * m.kmax, c, [&](int ent) {
-            double t[3], d[3];
-            corner_contrib(rec, ent, g.dx3, rdx3, t, !g.include_frmeanfluid, d);
+            double t[3];
+            corner_contrib(rz, rec, ent, g.dx3, rdx3, t);
             if (g.include_frmeanfluid) {
 #pragma unroll
                 for (int n = 0; n < 3; ++n) acc[n] = acc[n] + t[n];
             } else {
+                const double *r = rec + (size_t)(ent >> 3) * 6 + 3;
 #pragma unroll
-                for (int n = 0; n < 3; ++n) acc[n] = (acc[n] + t[n]) + d[n];
+                for (int n = 0; n < 3; ++n) acc[n] = (acc[n] + t[n]) + r[n];
             }
         });
 #pragma unroll
@@ -856,9 +857,9 @@ void enqueue_sspread_dyn(const Geo &g, const Mov &m, const double *sctb, const d
 }
 int moving_scalar_kernels_per_step() { return 4; }
 
-void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, double *fr, Scal *sc, cudaStream_t s) {
+void enqueue_spread_dyn(const Geo &g, const Mov &m, const double *rec, const double *rz, double *fr, Scal *sc, cudaStream_t s) {
     const size_t CR = (size_t)g.nx * g.RS;
-    k_spread_dyn<<<(unsigned)((CR + 255) / 256), 256, 0, s>>>(g, m, rec, fr, sc);
+    k_spread_dyn<<<(unsigned)((CR + 255) / 256), 256, 0, s>>>(g, m, rec, rz, fr, sc);
 }
 
 // Set-up: cells and the first neighbour search of des_time_march(.TRUE.)

@@ -159,24 +159,19 @@ __device__ __forceinline__ void make_sten(const Geo &g, const double pos[3], Ste
 // Contribution of a reversal point to one node of its inner stencil, entry
 // ent = 8 p + a + 2 b + 4 c of the spreading lists: w * force_tmp / dx^3
 // (boundary_condition.F90:1425-1462), w the trilinear weight of corner
-// (a, b, c) formed from the point's cell offsets as make_sten and Sten::w form
-// it.  k_rev forms the same values for its sums, so they are bitwise those it
-// would have stored.  With dist, d = the point's force_dist.
-__device__ __forceinline__ void corner_contrib(const double *__restrict__ rec, int ent, double dx3, double rdx3, double t[3],
-                                               bool dist, double d[3]) {
-    const double2 *r = reinterpret_cast<const double2 *>(rec) + (size_t)(ent >> 3) * (kRec / 2);
-    const double2 zxy = __ldg(r), zz0 = __ldg(r + 1), f01 = __ldg(r + 2), f2 = __ldg(r + 3);
-    const double wx = (ent & 1) ? zxy.x : __dsub_rn(1.0, zxy.x);
-    const double wy = (ent & 2) ? zxy.y : __dsub_rn(1.0, zxy.y);
-    const double wz = (ent & 4) ? zz0.x : __dsub_rn(1.0, zz0.x);
+// (a, b, c) formed from the point's cell offsets rz[3p..3p+2] as make_sten and
+// Sten::w form it, force_tmp = rec[6p..6p+2].  k_rev forms the same values
+// for its sums, so they are bitwise those it would have stored.
+__device__ __forceinline__ void corner_contrib(const double *__restrict__ rz, const double *__restrict__ rec, int ent,
+                                               double dx3, double rdx3, double t[3]) {
+    const size_t p = (size_t)(ent >> 3);
+    const double zx = __ldg(rz + 3 * p), zy = __ldg(rz + 3 * p + 1), zz = __ldg(rz + 3 * p + 2);
+    const double wx = (ent & 1) ? zx : __dsub_rn(1.0, zx);
+    const double wy = (ent & 2) ? zy : __dsub_rn(1.0, zy);
+    const double wz = (ent & 4) ? zz : __dsub_rn(1.0, zz);
     const double w = __dmul_rn(__dmul_rn(wx, wy), wz);
-    t[0] = qdiv(w * f01.x, dx3, rdx3);
-    t[1] = qdiv(w * f01.y, dx3, rdx3);
-    t[2] = qdiv(w * f2.x, dx3, rdx3);
-    if (dist) {
-        const double2 d01 = __ldg(r + 4), d2 = __ldg(r + 5);
-        d[0] = d01.x; d[1] = d01.y; d[2] = d2.x;
-    }
+#pragma unroll
+    for (int n = 0; n < 3; ++n) t[n] = qdiv(w * __ldg(rec + 6 * p + n), dx3, rdx3);
 }
 
 // value at node (x=i, y=j, z=k) of a physical field (one component)
