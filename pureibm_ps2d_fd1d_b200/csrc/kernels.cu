@@ -57,7 +57,7 @@ __device__ __forceinline__ void b_a0(const Geo &g, const double2 *__restrict__ u
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
     double2 *buf = sm, *tws = sm + L::BUF;
-    __shared__ double scr[32];
+    __shared__ double scr[32 * 3];
     __shared__ uint64_t mb;
     if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
@@ -129,11 +129,10 @@ __device__ __forceinline__ void b_a0(const Geo &g, const double2 *__restrict__ u
                 sa += v;
                 mx = fmax(mx, fabs(v));
             }
-            sf = block_sum(sf, scr);
-            ss = block_sum(ss, scr);
-            sa = block_sum(sa, scr);
+            double v3[3] = {sf, ss, sa};
+            block_reduce_k<3>(v3, scr);   // the three sums of block_sum's tree, two barriers
             mx = block_max(mx, scr);
-            if (threadIdx.x == 0) { part[slot + t] = sf; part[slot + 3 + t] = ss; part[slot + 6 + t] = sa; part[slot + 9 + t] = mx; }
+            if (threadIdx.x == 0) { part[slot + t] = v3[0]; part[slot + 3 + t] = v3[1]; part[slot + 6 + t] = v3[2]; part[slot + 9 + t] = mx; }
         }
         double *dst = t < 3 ? ubcp + ((size_t)t * nx + i) * RSP
                     : t == 3 ? pbcp + (size_t)i * RSP
