@@ -115,15 +115,18 @@ __device__ __forceinline__ void group_fft(double2 (&v)[R], int l, double s, cons
     dft_inlane<R>(v, s, tw);
 #pragma unroll
     for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw.get((l * r) % N, s));
+    // each stage in one form for both lanes of a pair: the upper lane forms
+    // v + pv, the lower (pv - v) w, i.e. t = pv + sgn v, then t w' (w' = 1 on
+    // the upper lane)
 #pragma unroll
     for (int h = L / 2; h >= 1; h >>= 1) {
         const bool upper = (l & h) == 0;
-        const int q = l & (h - 1);
-        const double2 w = tw.stage(h, q, s);
+        const double sgn = upper ? 1.0 : -1.0;
+        const double2 w = upper ? make_double2(1.0, 0.0) : tw.stage(h, l & (h - 1), s);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            double2 pv = shfl_xor2(v[r], h, L);
-            v[r] = upper ? cadd(v[r], pv) : cmul(csub(pv, v[r]), w);
+            const double2 pv = shfl_xor2(v[r], h, L);
+            v[r] = cmul(make_double2(__fma_rn(sgn, v[r].x, pv.x), __fma_rn(sgn, v[r].y, pv.y)), w);
         }
     }
 }

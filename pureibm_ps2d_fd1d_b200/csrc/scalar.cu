@@ -578,15 +578,18 @@ __device__ __forceinline__ void twisted_solve(double2 *row, double a, double b, 
         const double den = lr * lr + li * li, rden = 1.0 / den;
         v[r] = make_double2(qdiv(v[r].x * lr + v[r].y * li, den, rden), qdiv(v[r].y * lr - v[r].x * li, den, rden));
     }
+    // inverse stages: the lower lane of a pair first multiplies its own value
+    // by conj w (the upper by 1), then both take pv + sgn v
 #pragma unroll
     for (int h = 1; h < 32; h <<= 1) {
         const bool upper = (lane & h) == 0;
-        const int q = lane & (h - 1);
-        const double2 w = tw.stage(h, q, +1.0);
+        const double sgn = upper ? 1.0 : -1.0;
+        const double2 w = upper ? make_double2(1.0, 0.0) : tw.stage(h, lane & (h - 1), +1.0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const double2 pv = shfl_xor2(v[r], h, 32);
-            v[r] = upper ? cadd(v[r], cmul(pv, w)) : csub(pv, cmul(v[r], w));
+            const double2 m = cmul(v[r], w);
+            const double2 pv = shfl_xor2(m, h, 32);
+            v[r] = make_double2(__fma_rn(sgn, m.x, pv.x), __fma_rn(sgn, m.y, pv.y));
         }
     }
 #pragma unroll
