@@ -52,7 +52,7 @@ template <int N>
 __device__ __forceinline__ void b_a0(const Geo &g, const double2 *__restrict__ u, const double2 *__restrict__ p,
                                                    double *__restrict__ ubcp, double *__restrict__ pbcp,
                                                    double *__restrict__ omega, double *__restrict__ pgr,
-                                                   Scal *__restrict__ sc, double *__restrict__ part, int item0) {
+                                                   Scal *__restrict__ sc, double *__restrict__ part) {
     using L = PL<N>;
     extern __shared__ double2 sm[];
     constexpr int my2 = N / 2 + 1, PS = my2 * N, RSP = RP<N>::RSP;
@@ -71,7 +71,7 @@ __device__ __forceinline__ void b_a0(const Geo &g, const double2 *__restrict__ u
     const double2 *Pp = p + (size_t)i * PS;
     const size_t slot = ((size_t)i * L::C + rank) * 12;
     {
-        const int t = (int)blockIdx.y + item0;   // launches may cover a subrange of the 10 items
+        const int t = blockIdx.y;
         if (t < 4) {
             // a plain copy of u_t or p: the CTA's MC columns of every kz row as N
             // bulk copies into the padded rows, all in flight at once; rank 0's
@@ -144,9 +144,7 @@ template <int N>
 __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_a0(Geo g, const double2 *__restrict__ u, const double2 *__restrict__ p,
                                                    double *__restrict__ ubcp, double *__restrict__ pbcp,
                                                    double *__restrict__ omega, double *__restrict__ pgr,
-                                                   Scal *__restrict__ sc, double *__restrict__ part, int item0) {
-    b_a0<N>(g, u, p, ubcp, pbcp, omega, pgr, sc, part, item0);
-}
+                                                   Scal *__restrict__ sc, double *__restrict__ part) { b_a0<N>(g, u, p, ubcp, pbcp, omega, pgr, sc, part); }
 
 // compute_new_timestep's scalar tail (dependent_functions.F90:1137-1280).
 __device__ __forceinline__ void b_scal_a(const Geo &g, Scal *sc, const double *part) {
@@ -1224,7 +1222,7 @@ __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) k_ff2rc(Geo g, const do
 template <int N>
 __global__ void __launch_bounds__(PL<N>::T, PL<N>::MINB) kb_a0(const __grid_constant__ MemberSet ms) {
     const Member &m = ms.m[blockIdx.z];
-    b_a0<N>(m.g, m.b.u, m.b.p, m.b.ubcp, m.b.pbcp, m.b.omega, m.b.pgr, m.b.sc, m.b.part, 0);
+    b_a0<N>(m.g, m.b.u, m.b.p, m.b.ubcp, m.b.pbcp, m.b.omega, m.b.pgr, m.b.sc, m.b.part);
 }
 __global__ void __launch_bounds__(256) kb_scal_a(const __grid_constant__ MemberSet ms) {
     const Member &m = ms.m[blockIdx.z];
@@ -1425,15 +1423,7 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
     const bool scal_first = g.scal && !g.moving;
     mark(0);
     kb(PIBM_K_A0);
-    // forked, the x flux and the nonlinear term wait only for the velocity
-    // items (0-2); p, omega and grad p (items 3-9, read first by the drag
-    // quadrature and the reversal forcing) are transformed on the side stream
-    // beside them
-    auto a0_items = [&](int item0, int n, cudaStream_t st) {
-        launch_planes<N>(k_a0<N>, g.nx, n, st, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc,
-                         b.part, item0);
-    };
-    a0_items(0, fork ? 3 : 10, s);
+    launch_planes<N>(k_a0<N>, g.nx, 10, s, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
     ke(PIBM_K_A0);
     if (fork) {
         if (scal_first) k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
@@ -1446,7 +1436,6 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
         } else {
             k_scal_a<<<1, 256, 0, ss->side>>>(g, b.sc, b.part);
         }
-        a0_items(3, 7, ss->side);
         if (g.nbody > 0) {
             k_drag<N><<<g.nbody * kDragSplit, 256, 0, ss->side>>>(g, b.pbcp, b.omega, b.dpart, b.sc);
             k_scal_b<<<1, 256, 0, ss->side>>>(g, b.sc, b.pres, b.visc, b.ptot, b.force, b.dpart);
