@@ -1082,7 +1082,7 @@ static int sm_count() {
     return cache[dev];
 }
 // The 4-line width runs the persistent tensor-map kernel on grids up to 128
-// (four blocks of 55 KB per SM); at 256 a slab is 16 KB and the staged
+// (three blocks of 72 KB per SM); at 256 a slab is 16 KB and the staged
 // kernel is kept.  Both give bitwise the same results.
 template <int N>
 static void launch_lines(const Geo &g, DevBufs &b, double2 *u, double2 *p, int cur, Scal *sc, cudaStream_t s) {

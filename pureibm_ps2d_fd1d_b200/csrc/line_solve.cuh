@@ -232,23 +232,4 @@ __device__ __forceinline__ bool thomas_real(double2 *row, double *gam, double a,
     return true;
 }
 
-// thomas_real on plain doubles: x[0..n-1] in, the solution out, x[n] = 0 (the
-// same operations, so the same values as thomas_real's real parts).
-__device__ __forceinline__ bool thomas_real_x(double *x, double *gam, double a, double b, double c, int n) {
-    double bet = b;
-    if (bet == 0.0) return false;
-    double prev = x[0] / bet;
-    x[0] = prev;
-    for (int j = 1; j < n; ++j) {
-        gam[j] = c / bet;
-        bet = b - a * gam[j];
-        if (bet == 0.0) return false;
-        prev = (x[j] - a * prev) / bet;
-        x[j] = prev;
-    }
-    for (int j = n - 2; j >= 0; --j) x[j] = x[j] - gam[j + 1] * x[j + 1];
-    x[n] = 0.0;
-    return true;
-}
-
 }  // namespace pibm

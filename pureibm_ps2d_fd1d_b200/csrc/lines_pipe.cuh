@@ -4,21 +4,19 @@
 //
 // The staged kernel (b_lines) loads a tile's 13 input fields with ordinary
 // loads in a few passes separated by barriers, so few bytes are in flight per
-// SM and its solves wait on its loads.  Here each tile's fields stream, one
-// field at a time, as "slabs" (one field's values over 4 lines x NX planes,
-// 64-byte rows: the 4 lines are contiguous in the [comp][i][kz][ky] layout)
-// through a ring of KR shared-memory slots filled by tiled bulk-tensor copies,
-// while the block's four warps (one line each) solve.  There is no producer
-// warp: the warp that releases a slot last (a shared counter per slot) issues
-// the copy of the slab KR further on, so the whole block's registers serve
-// the solves and four blocks fit an SM.  The warps take the fields in the
+// SM and its solves wait on its loads.  Here one producer warp streams the
+// tile's fields, one field at a time, as "slabs" (one field's values over 4
+// lines x NX planes, 64-byte rows: the 4 lines are contiguous in the
+// [comp][i][kz][ky] layout) through a ring of KR shared-memory slots with
+// tiled bulk-tensor copies, and runs ahead into the next tile while the four
+// consumer warps (one line each) solve.  The consumers take the fields in the
 // order the reference forms the pressure source -- (nl, ff) of each component,
 // then onl -- and accumulate the source (in registers) and the explicit ustep
 // terms (in the u tiles) with every rounding written out (psrc_term_rt,
 // cadd_rn), so the results are bitwise those of b_lines.  u and p leave
 // through tensor-map stores of the tile's work tiles.  Tiles are handed out
-// dynamically (an atomic ticket, drawn one tile ahead), so the block that
-// draws the (0,0) line, whose Thomas solves are serial, takes fewer tiles.
+// dynamically (an atomic ticket), so the block that draws the (0,0) line,
+// whose Thomas solves are serial, takes fewer tiles.
 //
 // Every slab and work tile is a [i][line] box with the 64-byte swizzle: line
 // l of plane i sits at byte i*64 + 16*(l ^ ((i >> 1) & 3)), so a warp reading
@@ -39,31 +37,27 @@ struct LineMaps {
 
 template <int NX> struct LPipe {
     static constexpr int R = NX / 32;          // planes per lane
-    static constexpr int LT = 4;               // lines per tile = warps per block
-    static constexpr int KR = 2;               // slab ring depth
+    static constexpr int LT = 4;               // lines per tile = consumer warps
+    static constexpr int KR = 3;               // slab ring depth
     static constexpr int NSLAB = 13;           // input slabs per tile
     static constexpr int SLAB = NX * 64;       // bytes of one field over a tile
-    static constexpr int T = LT * 32;
-    static constexpr int MINB = 4;             // blocks per SM the budget is sized for
-    // the in-lane DFT reads the twiddle table only for R = 3 (a radix-3 step)
-    static constexpr int TWSB = R == 3 ? NX * 16 : 0;
+    static constexpr int T = (LT + 1) * 32;    // consumers + producer warp
+    static constexpr int MINB = 3;             // blocks per SM the budget is sized for
     // shared-memory byte offsets from a 1024-byte aligned base
     static constexpr int O_RING = 0;
     static constexpr int O_P = O_RING + KR * SLAB;           // p tile (TMA store source)
     static constexpr int O_U = O_P + SLAB;                   // 3 u tiles (TMA store sources)
-    static constexpr int O_TWS = O_U + 3 * SLAB;             // twiddles (R = 3 only)
-    static constexpr int O_ST = O_TWS + TWSB;                // stage table, 32 double2
+    static constexpr int O_ROW = O_U + 3 * SLAB;             // per-warp rows [LT][NX] double2
+    static constexpr int O_TWS = O_ROW + LT * NX * 16;       // twiddles, NX double2
+    static constexpr int O_ST = O_TWS + NX * 16;             // stage table, 32 double2
     static constexpr int O_LCS = O_ST + 32 * 16;             // per-lane cosines, R*32 doubles
     static constexpr int O_LTR = O_LCS + R * 32 * 8;         // per-lane twiddles, (R-1)*32 double2
     static constexpr int O_GAM = O_LTR + (R - 1) * 32 * 16;  // Thomas scratch, NX doubles
-    static constexpr int O_TRW = O_GAM + NX * 8;             // Thomas row, NX doubles
-    static constexpr int O_BAR = O_TRW + NX * 8;             // full[KR]
-    static constexpr int O_REL = O_BAR + KR * 8;             // release counters, KR ints
-    static constexpr int O_TID = O_REL + 16;                 // tickets of three tiles
+    static constexpr int O_BAR = O_GAM + NX * 8;             // full[KR], empty[KR]
+    static constexpr int O_TID = O_BAR + 2 * KR * 8;         // ticket of the tile in flight, 2 ints
     static constexpr int BYTES = O_TID + 16;
     static constexpr int SMEM = BYTES + 1024;                // + alignment slack
     static_assert(SLAB % 1024 == 0, "slabs keep the swizzle's 1024-byte alignment");
-    static_assert(NSLAB >= KR, "ring depth");
 };
 
 // Byte offset of (plane i, line l) in a swizzled slab or tile.
@@ -79,108 +73,79 @@ __device__ __forceinline__ const CUtensorMap *slab_map(const LineMaps &mp, int j
     return &mp.u;
 }
 
-// Values of a lane's planes i = lane + 32 r shifted by one plane, from the
-// other lanes: dm[r] at plane i - 1, dp[r] at plane i + 1 (periodic in x).
-template <int R>
-__device__ __forceinline__ void lane_neighbours(const double2 (&d)[R], int lane, double2 (&dm)[R], double2 (&dp)[R]) {
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const double2 up = make_double2(__shfl_up_sync(0xffffffffu, d[r].x, 1), __shfl_up_sync(0xffffffffu, d[r].y, 1));
-        const double2 wr = make_double2(__shfl_sync(0xffffffffu, d[(r + R - 1) % R].x, 31), __shfl_sync(0xffffffffu, d[(r + R - 1) % R].y, 31));
-        const double2 dn = make_double2(__shfl_down_sync(0xffffffffu, d[r].x, 1), __shfl_down_sync(0xffffffffu, d[r].y, 1));
-        const double2 wl = make_double2(__shfl_sync(0xffffffffu, d[(r + 1) % R].x, 0), __shfl_sync(0xffffffffu, d[(r + 1) % R].y, 0));
-        dm[r] = lane == 0 ? wr : up;
-        dp[r] = lane == 31 ? wl : dn;
-    }
-}
-
 template <int NX>
 __device__ __forceinline__ void lines_pipe_body(const Geo &g, const LineMaps &mp, Scal *__restrict__ sc) {
     using L = LPipe<NX>;
-    constexpr int R = L::R, KR = L::KR, NS = L::NSLAB;
+    constexpr int R = L::R, KR = L::KR;
     extern __shared__ unsigned char lp_raw[];
     unsigned char *sm = lp_raw + ((1024u - (smem_u32(lp_raw) & 1023u)) & 1023u);
     unsigned char *ring = sm + L::O_RING, *Pt = sm + L::O_P, *Ut = sm + L::O_U;   // u tile n at Ut + n*SLAB
-    double2 *tws = L::TWSB ? reinterpret_cast<double2 *>(sm + L::O_TWS) : const_cast<double2 *>(g.tw);
+    double2 *tws = reinterpret_cast<double2 *>(sm + L::O_TWS);
     double2 *st = reinterpret_cast<double2 *>(sm + L::O_ST);
     double *lcs = reinterpret_cast<double *>(sm + L::O_LCS);
     double2 *ltr = reinterpret_cast<double2 *>(sm + L::O_LTR);
     double *gam = reinterpret_cast<double *>(sm + L::O_GAM);
-    double *trow = reinterpret_cast<double *>(sm + L::O_TRW);
-    uint64_t *full = reinterpret_cast<uint64_t *>(sm + L::O_BAR);
-    int *rel = reinterpret_cast<int *>(sm + L::O_REL);
-    volatile int *tid = reinterpret_cast<int *>(sm + L::O_TID);   // ticket of tile c in tid[c % 3]
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + L::O_BAR), *empty = full + KR;
+    volatile int *tid_ring = reinterpret_cast<int *>(sm + L::O_TID);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = g.PS / L::LT;
 
-    // Issue slab k (tile k / NS, field k % NS) into its slot.  Slab 0 of tile c
-    // also draws the ticket of tile c + 1 (tile c's was drawn one tile earlier,
-    // so every reader of a ticket has waited on a slab issued after it was
-    // written); a tile without a ticket gets a plain arrival on its slab 0
-    // (the consumers then stop) and none of its other slabs.
-    auto issue = [&](uint32_t k) {
-        const int c = (int)(k / NS), j = (int)(k % NS), slot = (int)(k % KR);
-        const int t = tid[c % 3];
-        if (j == 0) {
-            if (t >= 0) {
-                const int tn = (int)atomicAdd(&sc->lines_next, 1u);
-                tid[(c + 1) % 3] = tn < ntiles ? tn : -1;
-            }
-            if (t < 0) { mbar_arrive(full + slot); return; }
-        }
-        if (t < 0) return;
-        int comp;
-        const CUtensorMap *m = slab_map(mp, j, comp);
-        mbar_expect_tx(full + slot, L::SLAB);
-        tma_load_3d(ring + slot * L::SLAB, m, 8 * t, 0, comp, full + slot);
-    };
-
     if (threadIdx.x == 0)
-        for (int s = 0; s < KR; ++s) { mbar_init(full + s, 1); rel[s] = 0; }
-    if (L::TWSB)
-        for (int t = threadIdx.x; t < NX; t += blockDim.x) tws[t] = g.tw[t];
+        for (int k = 0; k < KR; ++k) { mbar_init(full + k, 1); mbar_init(empty + k, L::LT); }
+    for (int t = threadIdx.x; t < NX; t += blockDim.x) tws[t] = g.tw[t];
     fill_stage_table<32>(st, g.tw, NX);
     fill_line_tw<R>(lcs, ltr, g.tw);
     // one barrier: the early-return vote, the barrier inits and the tables
-    if (block_failed(sc)) goto done;
-    if (threadIdx.x == 0) {
-        const int t0 = (int)atomicAdd(&sc->lines_next, 1u);
-        tid[0] = t0 < ntiles ? t0 : -1;
-        for (uint32_t k = 0; k < (uint32_t)KR; ++k) issue(k);
-    }
-    __syncthreads();
-    {
+    const bool failed = block_failed(sc);
+
+    if (!failed && warp == L::LT) {
+        // ---------------- producer: tickets and slab copies ----------------
+        if (lane == 0) {
+            uint32_t k = 0;
+            for (int c = 0;; ++c) {
+                const int t = (int)atomicAdd(&sc->lines_next, 1u);
+                for (int j = 0; j < L::NSLAB; ++j, ++k) {
+                    const int slot = k % KR;
+                    if (k >= KR && !mbar_wait(empty + slot, ((k / KR) - 1) & 1)) atomicCAS(&sc->status, 0, PIBM_ERR_TIMEOUT);
+                    if (j == 0) {
+                        tid_ring[c & 1] = t < ntiles ? t : -1;
+                        if (t >= ntiles) { mbar_arrive(full + slot); break; }   // no more tiles: wake the consumers
+                    }
+                    int comp;
+                    const CUtensorMap *m = slab_map(mp, j, comp);
+                    mbar_expect_tx(full + slot, L::SLAB);
+                    tma_load_3d(ring + slot * L::SLAB, m, 8 * t, 0, comp, full + slot);
+                }
+                if (t >= ntiles) break;
+            }
+        }
+    } else if (!failed) {
+        // ---------------- consumers: warp w solves line 4 t + w ----------------
+        const int w = warp;
         const LineTw<R> tw{{tws, NX, 1, st}, lcs, ltr};
         const double dx = g.dx, dx2 = g.dx2, dt = sc->dt, vis = g.vis;
         const double c1 = g.c1, c2 = g.c2, c3 = g.c3, c4 = g.c4;
         const double c12 = c1 + c2, rdx = 1.0 / dx, rdx2 = 1.0 / dx2, rc12 = 1.0 / c12;
+        double2 *row = reinterpret_cast<double2 *>(sm + L::O_ROW) + w * NX;   // this warp's scratch row
         bool ok = true;
-        uint32_t k = 0;   // next slab to consume
-        auto wait_slab = [&]() -> unsigned char * {
-            const int slot = (int)(k % KR);
-            if (!mbar_wait(full + slot, (k / KR) & 1)) atomicCAS(&sc->status, 0, PIBM_ERR_TIMEOUT);
+        uint32_t k = 0;
+        auto next_slab = [&](bool wait_done) -> unsigned char * {
+            const int slot = k % KR;
+            if (!wait_done && !mbar_wait(full + slot, (k / KR) & 1)) atomicCAS(&sc->status, 0, PIBM_ERR_TIMEOUT);
             return ring + slot * L::SLAB;
         };
-        // every warp releases every slab it waited for; the last one refills the slot
         auto release = [&]() {
             __syncwarp();
-            if (lane == 0) {
-                const int slot = (int)(k % KR);
-                __threadfence_block();
-                if (atomicAdd(rel + slot, 1) == L::LT - 1) {
-                    rel[slot] = 0;
-                    __threadfence_block();
-                    issue(k + KR);
-                }
-            }
+            if (lane == 0) mbar_arrive(empty + (k % KR));
             ++k;
         };
         for (int c = 0;; ++c) {
-            unsigned char *S0 = wait_slab();
-            const int t = tid[c % 3];
+            if (!mbar_wait(full + (k % KR), (k / KR) & 1)) atomicCAS(&sc->status, 0, PIBM_ERR_TIMEOUT);
+            const int t = tid_ring[c & 1];
             // the previous tile's stores have read the work tiles, which this tile overwrites
             if (threadIdx.x == 0) bulk_wait_read();
-            if (!__syncthreads_and(t >= 0)) break;
+            // one decision for the four warps (they meet at the tile's named barriers)
+            if (!named_bar_and(1, L::LT * 32, t >= 0)) break;
             const int q = t * L::LT + w;
             const double ky = g.ky[q % g.my2], kz = g.kz[q / g.my2], w2w = g.w2[q];
             const LineCoef kw = line_coef(dt, vis, c1, c2, dx2, w2w);
@@ -191,7 +156,7 @@ __device__ __forceinline__ void lines_pipe_body(const Geo &g, const LineMaps &mp
             for (int r = 0; r < R; ++r) tt[r] = make_double2(0.0, 0.0);
 #pragma unroll 1
             for (int j = 0; j < 9; ++j) {
-                unsigned char *S = j == 0 ? S0 : wait_slab();
+                unsigned char *S = next_slab(j == 0);
                 const int n = j < 6 ? (j >> 1) : j - 6, kind = j < 6 ? (j & 1) : 2;   // kind: 0 nl, 1 ff, 2 onl
                 const double cf = kind == 0 ? c3 : (kind == 1 ? 1.0 : c4);
                 unsigned char *E = Ut + n * L::SLAB;
@@ -209,7 +174,7 @@ __device__ __forceinline__ void lines_pipe_body(const Geo &g, const LineMaps &mp
             // ---- pressure (poisson.F90:118-239): old p, solve, p = p + (phi - p)
             double2 po[R], v[R];
             {
-                unsigned char *S = wait_slab();
+                unsigned char *S = next_slab(false);
 #pragma unroll
                 for (int r = 0; r < R; ++r) po[r] = tel(S, lane + 32 * r, w);
                 release();
@@ -218,13 +183,12 @@ __device__ __forceinline__ void lines_pipe_body(const Geo &g, const LineMaps &mp
             for (int r = 0; r < R; ++r) v[r] = make_double2(qdiv(tt[r].x, c12, rc12), qdiv(tt[r].y, c12, rc12));
             if (q == 0) {
 #pragma unroll
-                for (int r = 0; r < R; ++r) trow[lane + 32 * r] = v[r].x;
+                for (int r = 0; r < R; ++r) row[lane + 32 * r] = v[r];
                 __syncwarp();
-                if (lane == 0) ok = thomas_real_x(trow, gam, kw.pa, kw.pb, kw.pc, NX - 1) && ok;
+                if (lane == 0) ok = thomas_real(row, gam, kw.pa, kw.pb, kw.pc, NX - 1) && ok;
                 __syncwarp();
 #pragma unroll
-                for (int r = 0; r < R; ++r) v[r] = make_double2(trow[lane + 32 * r], 0.0);
-                __syncwarp();
+                for (int r = 0; r < R; ++r) v[r] = row[lane + 32 * r];
             } else {
                 circulant_solve_reg<R>(v, kw.pa, kw.pb, tw, lane);
             }
@@ -234,7 +198,7 @@ __device__ __forceinline__ void lines_pipe_body(const Geo &g, const LineMaps &mp
             // ---- ustep per component (usteptime.F90:73-470)
 #pragma unroll 1
             for (int n = 0; n < 3; ++n) {
-                unsigned char *S = wait_slab();
+                unsigned char *S = next_slab(false);
                 unsigned char *U = Ut + n * L::SLAB;
                 double2 rr[R];
 #pragma unroll
@@ -261,25 +225,24 @@ __device__ __forceinline__ void lines_pipe_body(const Geo &g, const LineMaps &mp
             }
             if (q == 0) {
 #pragma unroll
-                for (int r = 0; r < R; ++r) trow[lane + 32 * r] = v[r].x;
+                for (int r = 0; r < R; ++r) row[lane + 32 * r] = v[r];
                 __syncwarp();
-                if (lane == 0) ok = thomas_real_x(trow, gam, kw.pa, kw.pb, kw.pc, NX - 1) && ok;
-                __syncwarp();
-#pragma unroll
-                for (int r = 0; r < R; ++r) v[r] = make_double2(trow[lane + 32 * r], 0.0);
+                if (lane == 0) ok = thomas_real(row, gam, kw.pa, kw.pb, kw.pc, NX - 1) && ok;
                 __syncwarp();
             } else {
                 circulant_solve_reg<R>(v, kw.pa, kw.pb, tw, lane);
+#pragma unroll
+                for (int r = 0; r < R; ++r) row[lane + 32 * r] = v[r];
+                __syncwarp();
             }
             {
-                double2 dm[R], dp[R];
-                lane_neighbours<R>(v, lane, dm, dp);
                 double2 nu1[R], nu2[R], nu3[R], np[R];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const int i = lane + 32 * r;
-                    divcorr_update(kw, v[r], dm[r], dp[r], i == 0, tel(U1, i, w), tel(U2, i, w), tel(U3, i, w), tel(Pt, i, w), ky, kz, w2w, dx,
-                                   rdx, dx2, rdx2, nu1[r], nu2[r], nu3[r], np[r]);
+                    const int im = i == 0 ? NX - 1 : i - 1, ip = i == NX - 1 ? 0 : i + 1;
+                    divcorr_update(kw, row[i], row[im], row[ip], i == 0, tel(U1, i, w), tel(U2, i, w), tel(U3, i, w), tel(Pt, i, w), ky, kz, w2w,
+                                   dx, rdx, dx2, rdx2, nu1[r], nu2[r], nu3[r], np[r]);
                 }
                 __syncwarp();
 #pragma unroll
@@ -301,7 +264,7 @@ __device__ __forceinline__ void lines_pipe_body(const Geo &g, const LineMaps &mp
             if (lane == 0) atomicMax(&sc->divmax_bits, (unsigned long long)__double_as_longlong(dmax));
             // ---- the tile's u and p leave through tensor-map stores
             fence_async_smem();
-            __syncthreads();
+            named_bar_sync(1, L::LT * 32);
             if (threadIdx.x == 0) {
 #pragma unroll
                 for (int n = 0; n < 3; ++n) tma_store_3d(&mp.u, Ut + n * L::SLAB, 8 * t, 0, n);
@@ -312,7 +275,6 @@ __device__ __forceinline__ void lines_pipe_body(const Geo &g, const LineMaps &mp
         if (!ok) atomicCAS(&sc->status, 0, PIBM_ERR_PIVOT);
         if (threadIdx.x == 0) bulk_wait_all();
     }
-done:
     // the last block to finish resets the tickets for the next launch
     if (threadIdx.x == 0) {
         __threadfence();
