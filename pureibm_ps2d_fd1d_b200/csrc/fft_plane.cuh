@@ -122,11 +122,12 @@ __device__ __forceinline__ void group_fft(double2 (&v)[R], int l, double s, cons
     for (int h = L / 2; h >= 1; h >>= 1) {
         const bool upper = (l & h) == 0;
         const double sgn = upper ? 1.0 : -1.0;
-        const double2 w = upper ? make_double2(1.0, 0.0) : tw.stage(h, l & (h - 1), s);
+        const double2 w = (upper || h == 1) ? make_double2(1.0, 0.0) : tw.stage(h, l & (h - 1), s);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const double2 pv = shfl_xor2(v[r], h, L);
-            v[r] = cmul(make_double2(__fma_rn(sgn, v[r].x, pv.x), __fma_rn(sgn, v[r].y, pv.y)), w);
+            const double2 t = make_double2(__fma_rn(sgn, v[r].x, pv.x), __fma_rn(sgn, v[r].y, pv.y));
+            v[r] = h == 1 ? t : cmul(t, w);   // the last stage's twiddle is 1
         }
     }
 }

@@ -49,17 +49,18 @@ __device__ __forceinline__ void circulant_solve_reg(double2 (&v)[R], double a, d
     for (int r = 1; r < R; ++r) v[r] = cmul(v[r], lt.tr[(r - 1) * 32 + lane]);
     // Each butterfly stage in one form for both lanes of a pair (no select of
     // two computed branches): the upper lane forms v + pv, the lower (pv - v) w,
-    // i.e. t = pv + sgn v, then t times w' with w' = 1 on the upper lane.
+    // i.e. t = pv + sgn v, then t times w' with w' = 1 on the upper lane.  The
+    // last stage's twiddle is 1 on every lane: no multiply.
 #pragma unroll
     for (int h = 16; h >= 1; h >>= 1) {
         const bool upper = (lane & h) == 0;
         const double sgn = upper ? 1.0 : -1.0;
-        const double2 w = upper ? make_double2(1.0, 0.0) : tw.stage(h, lane & (h - 1), -1.0);
+        const double2 w = (upper || h == 1) ? make_double2(1.0, 0.0) : tw.stage(h, lane & (h - 1), -1.0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const double2 pv = shfl_xor2(v[r], h, 32);
             const double2 t = make_double2(__fma_rn(sgn, v[r].x, pv.x), __fma_rn(sgn, v[r].y, pv.y));
-            v[r] = cmul(t, w);
+            v[r] = h == 1 ? t : cmul(t, w);
         }
     }
     // lane holds modes m = r + R*bitrev(lane)
@@ -76,10 +77,10 @@ __device__ __forceinline__ void circulant_solve_reg(double2 (&v)[R], double a, d
     for (int h = 1; h < 32; h <<= 1) {
         const bool upper = (lane & h) == 0;
         const double sgn = upper ? 1.0 : -1.0;
-        const double2 w = upper ? make_double2(1.0, 0.0) : tw.stage(h, lane & (h - 1), +1.0);
+        const double2 w = (upper || h == 1) ? make_double2(1.0, 0.0) : tw.stage(h, lane & (h - 1), +1.0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const double2 m = cmul(v[r], w);
+            const double2 m = h == 1 ? v[r] : cmul(v[r], w);
             const double2 pv = shfl_xor2(m, h, 32);
             v[r] = make_double2(__fma_rn(sgn, m.x, pv.x), __fma_rn(sgn, m.y, pv.y));
         }

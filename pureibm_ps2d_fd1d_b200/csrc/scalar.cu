@@ -584,10 +584,10 @@ __device__ __forceinline__ void twisted_solve(double2 *row, double a, double b, 
     for (int h = 1; h < 32; h <<= 1) {
         const bool upper = (lane & h) == 0;
         const double sgn = upper ? 1.0 : -1.0;
-        const double2 w = upper ? make_double2(1.0, 0.0) : tw.stage(h, lane & (h - 1), +1.0);
+        const double2 w = (upper || h == 1) ? make_double2(1.0, 0.0) : tw.stage(h, lane & (h - 1), +1.0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const double2 m = cmul(v[r], w);
+            const double2 m = h == 1 ? v[r] : cmul(v[r], w);   // the first stage's twiddle is 1
             const double2 pv = shfl_xor2(m, h, 32);
             v[r] = make_double2(__fma_rn(sgn, m.x, pv.x), __fma_rn(sgn, m.y, pv.y));
         }
