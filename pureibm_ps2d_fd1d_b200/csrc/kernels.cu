@@ -1581,20 +1581,29 @@ extern const int kLinesTiles[2] = {4, 8};
 template <int N>
 static cudaError_t autotune_lines_t(Geo &g, DevBufs &b, int cur, cudaStream_t s, double ms[2]) {
     const size_t SC = (size_t)g.nx * g.PS;
-    // Runs whose whole state is u, p, nl and the scalars (fixed particles, no
-    // passive scalar) time complete steps on scratch copies of that state:
-    // the line kernel's cost depends on what runs beside and before it (the
-    // persistent kernel measured faster inside the step and slower in
-    // isolation than the staged one).  Other runs time the line kernel behind
-    // the forcing transform that precedes it.
-    const bool whole = !g.moving && !g.scal;
-    double2 *u = nullptr, *p = nullptr, *nl0 = nullptr, *nl1 = nullptr;
+    // Runs with fixed particles time complete steps on scratch copies of their
+    // state (u, p, nl, the scalars and, with a passive scalar, its phi and
+    // nonlinear terms): the line kernel's cost depends on what runs beside
+    // and before it (the persistent kernel measured faster inside the step
+    // and slower in isolation than the staged one).  Moving-particle runs,
+    // whose state includes the particles, time the line kernel behind the
+    // forcing transform that precedes it.
+    const bool whole = !g.moving;
+    const bool scal = whole && g.scal;
+    const size_t NR1 = (size_t)(g.nx + 1) * g.RS;
+    double2 *u = nullptr, *p = nullptr, *nl0 = nullptr, *nl1 = nullptr, *phif = nullptr, *ns0 = nullptr, *ns1 = nullptr;
+    double *nr0 = nullptr, *nr1 = nullptr;
     Scal *sc = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t e = cudaMalloc(&u, 3 * SC * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&p, SC * sizeof(double2));
     if (e == cudaSuccess && whole) e = cudaMalloc(&nl0, 3 * SC * sizeof(double2));
     if (e == cudaSuccess && whole) e = cudaMalloc(&nl1, 3 * SC * sizeof(double2));
+    if (e == cudaSuccess && scal) e = cudaMalloc(&phif, SC * sizeof(double2));
+    if (e == cudaSuccess && scal) e = cudaMalloc(&ns0, SC * sizeof(double2));
+    if (e == cudaSuccess && scal) e = cudaMalloc(&ns1, SC * sizeof(double2));
+    if (e == cudaSuccess && scal) e = cudaMalloc(&nr0, NR1 * sizeof(double));
+    if (e == cudaSuccess && scal) e = cudaMalloc(&nr1, NR1 * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&sc, sizeof(Scal));
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
@@ -1612,6 +1621,14 @@ static cudaError_t autotune_lines_t(Geo &g, DevBufs &b, int cur, cudaStream_t s,
             cudaMemcpyAsync(nl0, b.nl[0], 3 * SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
             cudaMemcpyAsync(nl1, b.nl[1], 3 * SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
             bt.u = u; bt.p = p; bt.nl[0] = nl0; bt.nl[1] = nl1; bt.sc = sc;
+        }
+        if (scal) {
+            cudaMemcpyAsync(phif, b.phif, SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(ns0, b.nls[0], SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(ns1, b.nls[1], SC * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(nr0, b.nlr[0], NR1 * sizeof(double), cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(nr1, b.nlr[1], NR1 * sizeof(double), cudaMemcpyDeviceToDevice, s);
+            bt.phif = phif; bt.nls[0] = ns0; bt.nls[1] = ns1; bt.nlr[0] = nr0; bt.nlr[1] = nr1;
         }
         int c = cur;
         auto unit = [&]() {
@@ -1642,6 +1659,7 @@ static cudaError_t autotune_lines_t(Geo &g, DevBufs &b, int cur, cudaStream_t s,
     if (e == cudaSuccess && whole && g.nbody > 0) {
         for (double *f : {b.pres, b.visc, b.ptot, b.force})
             if (f) cudaMemsetAsync(f, 0, 3 * (size_t)g.nbody * sizeof(double), s);
+        if (scal && b.flux_body) cudaMemsetAsync(b.flux_body, 0, (size_t)g.nbody * sizeof(double), s);
         e = cudaStreamSynchronize(s);
     }
     if (e == cudaSuccess) e = cudaGetLastError();
@@ -1652,6 +1670,11 @@ static cudaError_t autotune_lines_t(Geo &g, DevBufs &b, int cur, cudaStream_t s,
     cudaFree(p);
     cudaFree(nl0);
     cudaFree(nl1);
+    cudaFree(phif);
+    cudaFree(ns0);
+    cudaFree(ns1);
+    cudaFree(nr0);
+    cudaFree(nr1);
     cudaFree(sc);
     return e;
 }
