@@ -111,4 +111,10 @@ __device__ __forceinline__ void named_bar_sync(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
+// Programmatic dependent launch: wait until the grids this one depends on
+// have completed and their writes are visible (a no-op in a grid launched
+// without the programmatic-serialization attribute).  Code before it may
+// read only data no earlier kernel of the stream writes.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 }  // namespace pibm

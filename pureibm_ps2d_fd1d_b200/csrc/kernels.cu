@@ -62,6 +62,7 @@ __device__ __forceinline__ void b_a0(const Geo &g, const double2 *__restrict__ u
     if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
     __syncthreads();
+    grid_dep_wait();   // the twiddles above are set-up data; the fields come from earlier kernels
     const int i = blockIdx.x / L::C, rank = blockIdx.x % L::C, nx = g.nx;
     const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
     const size_t roff = (size_t)rank * L::RL;
@@ -383,6 +384,7 @@ __device__ __forceinline__ void b_nl(const Geo &g, const double *__restrict__ ub
     if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
     __syncthreads();
+    grid_dep_wait();   // the twiddles above are set-up data; the fields come from earlier kernels
     uint32_t phase = 0;
     const int i = blockIdx.x / L::C, rank = blockIdx.x % L::C, nx = g.nx;
     const int im = (i - 1 + nx) % nx, ip = (i + 1) % nx;
@@ -792,6 +794,7 @@ __device__ __forceinline__ void b_ff(const Geo &g, const double *__restrict__ fr
     if (threadIdx.x == 0) mbar_init(&mb, 1);
     load_tw<N>(tws, g);
     __syncthreads();
+    grid_dep_wait();   // the twiddles above are set-up data; the fields come from earlier kernels
     uint32_t phase = 0;
     const int i = blockIdx.x / L::C, rank = blockIdx.x % L::C, nx = g.nx;
     const size_t roff = (size_t)rank * L::RL;
@@ -1084,6 +1087,28 @@ static int sm_count() {
 // The 4-line width runs the persistent tensor-map kernel on grids up to 128
 // (three blocks of 72 KB per SM); at 256 a slab is 16 KB and the staged
 // kernel is kept.  Both give bitwise the same results.
+// launch_planes with programmatic dependent launch: the blocks may start
+// (and run the prologue before their grid_dep_wait) while the previous kernel
+// of the stream drains.
+template <int N, typename... KArgs, typename... Args>
+inline void launch_planes_pdl(void (*k)(KArgs...), int nplanes, int items, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(nplanes * PL<N>::C), (unsigned)items, 1);
+    cfg.blockDim = dim3(PL<N>::T, 1, 1);
+    cfg.dynamicSmemBytes = plane_smem<N>();
+    cfg.stream = s;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = PL<N>::C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <int N>
 static void launch_lines(const Geo &g, DevBufs &b, double2 *u, double2 *p, int cur, Scal *sc, cudaStream_t s) {
     const int old = cur ^ 1;
@@ -1094,8 +1119,17 @@ static void launch_lines(const Geo &g, DevBufs &b, double2 *u, double2 *p, int c
             if (line_map(&mp.u, u, g.PS, g.nx, 3, N) && line_map(&mp.p, p, g.PS, g.nx, 1, N) &&
                 line_map(&mp.nl, b.nl[cur], g.PS, g.nx, 3, N) && line_map(&mp.onl, b.nl[old], g.PS, g.nx, 3, N) &&
                 line_map(&mp.ff, b.ff, g.PS, g.nx, 3, N)) {
-                const int grid = std::min(g.PS / LPipe<N>::LT, LPipe<N>::MINB * sm_count());
-                k_lines_pipe<N><<<grid, LPipe<N>::T, LPipe<N>::SMEM, s>>>(g, mp, sc);
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)std::min(g.PS / LPipe<N>::LT, LPipe<N>::MINB * sm_count()), 1, 1);
+                cfg.blockDim = dim3(LPipe<N>::T, 1, 1);
+                cfg.dynamicSmemBytes = LPipe<N>::SMEM;
+                cfg.stream = s;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                at[0].val.programmaticStreamSerializationAllowed = 1;   // prologue beside the previous kernel's tail
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                cudaLaunchKernelEx(&cfg, k_lines_pipe<N>, g, mp, sc);
                 return;
             }
         }
@@ -1423,7 +1457,7 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
     const bool scal_first = g.scal && !g.moving;
     mark(0);
     kb(PIBM_K_A0);
-    launch_planes<N>(k_a0<N>, g.nx, 10, s, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
+    launch_planes_pdl<N>(k_a0<N>, g.nx, 10, s, g, (const double2 *)b.u, (const double2 *)b.p, b.ubcp, b.pbcp, b.omega, b.pgr, b.sc, b.part);
     ke(PIBM_K_A0);
     if (fork) {
         if (scal_first) k_scal_a<<<1, 256, 0, s>>>(g, b.sc, b.part);
@@ -1451,8 +1485,8 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
     k_flux<N><<<(RP<N>::RSP * (g.nx / g.flux_seg) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
     ke(PIBM_K_FLUX);
     kb(PIBM_K_NL);
-    launch_planes<N>(k_nl<N>, g.nx, 3, s, g, (const double *)b.ubcp, (const double *)b.Dx, (const double2 *)b.u,
-                     (const double2 *)b.nl[old], b.nl[cur], b.Q, b.sc);
+    launch_planes_pdl<N>(k_nl<N>, g.nx, 3, s, g, (const double *)b.ubcp, (const double *)b.Dx, (const double2 *)b.u,
+                         (const double2 *)b.nl[old], b.nl[cur], b.Q, b.sc);
     ke(PIBM_K_NL);
     mark(2);
     if (fork) cudaStreamWaitEvent(s, ss->drag_done, 0);
@@ -1501,7 +1535,7 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
         }
         mark(4);
         kb(PIBM_K_FF);
-        launch_planes<N>(k_ff<N>, g.nx, 3, s, g, (const double *)b.fr, b.ff, b.sc);
+        launch_planes_pdl<N>(k_ff<N>, g.nx, 3, s, g, (const double *)b.fr, b.ff, b.sc);
         ke(PIBM_K_FF);
     } else {
         mark(3); mark(4);

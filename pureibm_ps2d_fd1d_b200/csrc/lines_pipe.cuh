@@ -95,6 +95,7 @@ __device__ __forceinline__ void lines_pipe_body(const Geo &g, const LineMaps &mp
     for (int t = threadIdx.x; t < NX; t += blockDim.x) tws[t] = g.tw[t];
     fill_stage_table<32>(st, g.tw, NX);
     fill_line_tw<R>(lcs, ltr, g.tw);
+    grid_dep_wait();   // the tables above are set-up data; the fields and the status come from earlier kernels
     // one barrier: the early-return vote, the barrier inits and the tables
     const bool failed = block_failed(sc);
 
