@@ -325,12 +325,14 @@ int  pibm_adjoint_end(pibm_handle *h, double *g_xc, double g_mpg[3]);
 
 /* ---- tile shapes (no counterpart in the reference) ----
  * pibm_create times the x-line solve kernel with 4 and 8 (ky,kz) lines per
- * CTA on the run's own grid (scratch copies of the state, 10 launches after
- * a warm-up, each behind the forcing transform that precedes it in the
- * step) and keeps the faster; up to 128 the 4-line width is a persistent
- * kernel fed by tensor-map copies.  Results do not depend on the choice.
- * pibm_get_tuning returns the width in use and the mean time per
- * (forcing transform + line kernel) pair of each candidate (ms[0]: 4, ms[1]: 8);
+ * CTA on the run's own grid, on scratch copies of the state (fixed
+ * particles: 6 whole steps after 2; moving particles: 10 launches after a
+ * warm-up, each behind the forcing transform that precedes it in the step),
+ * and keeps the faster; up to 128 the 4-line width is a persistent kernel
+ * fed by tensor-map copies.  Results do not depend on the choice.
+ * pibm_get_tuning returns the width in use and the mean time per timed unit
+ * (a step, or a forcing transform + line kernel pair) of each candidate
+ * (ms[0]: 4, ms[1]: 8);
  * pibm_set_tuning overrides it (4 or 8) before the next pibm_run (the
  * handle's step graphs are recaptured; batch graphs are not). */
 int  pibm_get_tuning(pibm_handle *h, int32_t *lines_per_cta, double lines_ms[2]);
