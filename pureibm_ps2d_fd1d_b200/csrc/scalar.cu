@@ -421,7 +421,8 @@ __device__ __forceinline__ double sval(const double *f, int plane, const SSten &
     return __ldg(f + (size_t)plane * RP<N>::RSP + real_off<N>(s.kk[c], s.jj[b]));
 }
 template <int N>
-__global__ void __launch_bounds__(256, 3) k_srev(Geo g, const double *__restrict__ phr, const double *__restrict__ nlr,
+// two blocks per SM (128 registers), as the flow's reversal forcing
+__global__ void __launch_bounds__(256, 2) k_srev(Geo g, const double *__restrict__ phr, const double *__restrict__ nlr,
                                                  const double *__restrict__ onlr, const double *__restrict__ sdf,
                                                  const Scal *__restrict__ sc, double *__restrict__ sctb,
                                                  double *__restrict__ sfd) {
