@@ -368,7 +368,8 @@ __device__ __forceinline__ void b_flux(const Geo &g, const double *__restrict__ 
     }
 }
 template <int N>
-__global__ void __launch_bounds__(256) k_flux(Geo g, const double *__restrict__ ubcp, double *__restrict__ Dx,
+// four blocks per SM (64 registers): 0.034 against 0.036 ms at three (74)
+__global__ void __launch_bounds__(256, 4) k_flux(Geo g, const double *__restrict__ ubcp, double *__restrict__ Dx,
                                               const Scal *__restrict__ sc) { b_flux<N>(g, ubcp, Dx, sc); }
 
 template <int N>
@@ -1265,7 +1266,7 @@ __global__ void __launch_bounds__(256) kb_scal_a(const __grid_constant__ MemberS
     b_scal_a(m.g, m.b.sc, m.b.part);
 }
 template <int N>
-__global__ void __launch_bounds__(256) kb_flux(const __grid_constant__ MemberSet ms) {
+__global__ void __launch_bounds__(256, 4) kb_flux(const __grid_constant__ MemberSet ms) {
     const Member &m = ms.m[blockIdx.z];
     b_flux<N>(m.g, m.b.ubcp, m.b.Dx, m.b.sc);
 }
