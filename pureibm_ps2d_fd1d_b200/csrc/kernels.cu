@@ -367,9 +367,14 @@ __device__ __forceinline__ void b_flux(const Geo &g, const double *__restrict__ 
         for (int c = 0; c < 3; ++c) { w[c][0] = w[c][1]; w[c][1] = w[c][2]; w[c][2] = w[c][3]; sl[c][0] = sl[c][1]; }
     }
 }
-template <int N>
-// four blocks per SM (64 registers): 0.034 against 0.036 ms at three (74)
-__global__ void __launch_bounds__(256, 4) k_flux(Geo g, const double *__restrict__ ubcp, double *__restrict__ Dx,
+// MB blocks per SM.  Flow alone: four (64 registers), 0.034 against 0.036 ms
+// at three (74).  With a passive scalar on its side stream from the start of
+// the step (fixed spheres) the pair k_flux<N, 3> + k_rev<N, 3> leaves room
+// for the scalar's blocks: step 1.088 against 1.134 ms at 128^3, while either
+// one alone gains under 0.01 ms.  A moving run forks its scalar later and
+// keeps the flow's bounds (k_rev<N, 3> cost 0.085 ms per step at 256^3 there).
+template <int N, int MB>
+__global__ void __launch_bounds__(256, MB) k_flux(Geo g, const double *__restrict__ ubcp, double *__restrict__ Dx,
                                               const Scal *__restrict__ sc) { b_flux<N>(g, ubcp, Dx, sc); }
 
 template <int N>
@@ -730,10 +735,11 @@ __device__ __forceinline__ void b_rev(const Geo &g, const double *__restrict__ u
     if (threadIdx.x == 0)
         for (int q = 0; q < 6; ++q) blockpart[(size_t)blockIdx.x * 6 + q] = v[q];
 }
-template <int N>
-// two blocks per SM (128 registers): more gathers in flight per thread beat the
-// occupancy of three blocks at 80 registers (0.069 against 0.076 ms at 128^3)
-__global__ void __launch_bounds__(256, 2) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
+// MB blocks per SM.  Flow alone: two (128 registers), more gathers in flight
+// per thread beat the occupancy of three blocks at 80 registers (0.069 against
+// 0.076 ms at 128^3); three beside a passive scalar (k_flux above).
+template <int N, int MB>
+__global__ void __launch_bounds__(256, MB) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
                                                 const double *__restrict__ Q, const Scal *__restrict__ sc,
                                                 double *__restrict__ rec, double *__restrict__ rz, double *__restrict__ blockpart) { b_rev<N>(g, ubcp, pgr, Q, sc, rec, rz, blockpart); }
 
@@ -1485,7 +1491,9 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
     }
     mark(1);
     kb(PIBM_K_FLUX);
-    k_flux<N><<<(RP<N>::RSP * (g.nx / g.flux_seg) + 255) / 256, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
+    const int fgrid = (RP<N>::RSP * (g.nx / g.flux_seg) + 255) / 256;
+    if (scal_first) k_flux<N, 3><<<fgrid, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
+    else k_flux<N, 4><<<fgrid, 256, 0, s>>>(g, b.ubcp, b.Dx, b.sc);
     ke(PIBM_K_FLUX);
     kb(PIBM_K_NL);
     launch_planes_pdl<N>(k_nl<N>, g.nx, 3, s, g, (const double *)b.ubcp, (const double *)b.Dx, (const double2 *)b.u,
@@ -1515,7 +1523,8 @@ static void enqueue_step_t(const Geo &g, DevBufs &b, int cur, cudaStream_t s, cu
         const int nbk = (g.npts + 255) / 256;
         if (g.npts > 0) {
             kb(PIBM_K_REV);
-            k_rev<N><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.rz, b.blockpart);
+            if (scal_first) k_rev<N, 3><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.rz, b.blockpart);
+            else k_rev<N, 2><<<nbk, 256, 0, s>>>(g, b.ubcp, b.pgr, b.Q, b.sc, b.rec, b.rz, b.blockpart);
             ke(PIBM_K_REV);
             if (fork && !scal_first) {
                 // frmean (read from k_ff on) beside the spreading, which does not read it
