@@ -367,8 +367,8 @@ __device__ __forceinline__ void b_flux(const Geo &g, const double *__restrict__ 
         for (int c = 0; c < 3; ++c) { w[c][0] = w[c][1]; w[c][1] = w[c][2]; w[c][2] = w[c][3]; sl[c][0] = sl[c][1]; }
     }
 }
-// MB blocks per SM.  Flow alone: four (64 registers), 0.034 against 0.036 ms
-// at three (74).  With a passive scalar on its side stream from the start of
+// MB blocks per SM.  Flow alone: four (64 registers, 28 bytes spilled),
+// 0.034 against 0.036 ms at three (74, no spills).  With a passive scalar on its side stream from the start of
 // the step (fixed spheres) the pair k_flux<N, 3> + k_rev<N, 3> leaves room
 // for the scalar's blocks: step 1.088 against 1.134 ms at 128^3, while either
 // one alone gains under 0.01 ms.  A moving run forks its scalar later and
@@ -736,8 +736,9 @@ __device__ __forceinline__ void b_rev(const Geo &g, const double *__restrict__ u
         for (int q = 0; q < 6; ++q) blockpart[(size_t)blockIdx.x * 6 + q] = v[q];
 }
 // MB blocks per SM.  Flow alone: two (128 registers), more gathers in flight
-// per thread beat the occupancy of three blocks at 80 registers (0.069 against
-// 0.076 ms at 128^3); three beside a passive scalar (k_flux above).
+// per thread beat the occupancy of three blocks at 80 registers and 32 bytes
+// spilled (0.069 against 0.076 ms at 128^3); three beside a passive scalar
+// (k_flux above).
 template <int N, int MB>
 __global__ void __launch_bounds__(256, MB) k_rev(Geo g, const double *__restrict__ ubcp, const double *__restrict__ pgr,
                                                 const double *__restrict__ Q, const Scal *__restrict__ sc,
