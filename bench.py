@@ -636,7 +636,8 @@ def run_gpu(args):
         "warmup": max(args.warmup, 3), "ms_per_step": t_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded sphere positions, fluid initially at rest)",
-        "config": dict(_config_dict(world, xc, prm), lines_per_cta=s.tuning()["lines_per_cta"]),
+        "config": _config_dict(world, xc, prm),
+        "lines_per_cta": s.tuning()["lines_per_cta"],   # x-line width the run used (tuned or pinned)
         "roofline": kernel_roofline[dominant],
         "kernel_roofline": kernel_roofline,
         "step_roofline": {"algorithmic_bytes_per_step": b_alg_step,
