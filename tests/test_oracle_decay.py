@@ -1,0 +1,116 @@
+"""Exact viscous decay of divergence-free shear waves in the oracle step.
+
+With no spheres and the mean pressure gradient held at zero, a velocity
+field with one component that does not vary along its own direction
+(u_x(y, z), or u_y(x, z)) is an exact solution of the Navier-Stokes
+equations: the conservative nonlinear term and the divergence vanish, the
+pressure stays zero and each Fourier mode decays on its own.  The step's
+Crank-Nicolson viscous solve (usteptime.F90:286-499, with coef(rks, 1:2)
+from initialize_flo.F90:861-884) then multiplies the mode by
+
+    g = (1 - c2 * nu * dt * lam) / (1 + c1 * nu * dt * lam)
+
+per stage, lam = ky^2 + kz^2 + 4 sin^2(kx dx / 2) / dx^2 (spectral in y
+and z, the three-point second difference in x).  These tests pin the
+oracle's time integration, viscous line solves and projection against that
+closed form, independently of the reference's outputs; the engine is held
+to the oracle by the GPU parity tests.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle_ctypes as oc  # noqa: E402
+from pureibm_ps2d_fd1d_b200 import config  # noqa: E402
+
+MY = 32
+LY = 4.0              # lybyd = 4 with d = 1
+DX = LY / MY
+NU = 0.05
+AMP = 0.01
+AB2_STAGES = [(0.5, 0.5)]
+RK3_STAGES = [(4.0 / 15.0, 4.0 / 15.0), (1.0 / 15.0, 1.0 / 15.0), (1.0 / 6.0, 1.0 / 6.0)]
+
+
+def _solver(scheme, rk3):
+    prm = config.default_params()
+    prm.update(my=MY, lybyd=LY, dbydx=MY / LY, re=1.0, vis=NU, cfl=0.2, cfl_max=0.5, discr_scheme=scheme,
+               initialize_zero=True, dobnd=False, ramp_frac_steps=0, set_mpg=True, mpg=(0.0, 0.0, 0.0), rk3=rk3)
+    parts = config.Particles(np.zeros((0, 3)))
+    s = oc.OracleSolver(config.make_params(prm), parts.struct)
+    s._parts = parts
+    return s
+
+
+def _wave(s, case):
+    """Initial u (reference layout [comp][kz][ky][x]), the modes it occupies
+    and their lam."""
+    st = s.get_state()
+    u = np.zeros_like(st["u"])
+    x = np.arange(s.nx + 1) * DX                 # x_i = (i - 1) dx, i = 1..nx+1 (periodic image)
+    if case == "ux_of_y":                        # u_x = A sin(2 pi 2 y / Ly): the (ky = 2, kz = 0) line
+        m = 2
+        u[0, 0, m, :] = -0.5j * AMP
+        modes = [(0, 0, m)]
+        lam = (2 * np.pi * m / LY) ** 2
+    elif case == "ux_of_yz":                     # u_x = A sin(ky y + kz z), ky = 1, kz = 3 (ky > 0: the
+                                                 # conjugate mode is implicit in the half spectrum)
+        m, n = 1, 3
+        u[0, n, m, :] = -0.5j * AMP
+        modes = [(0, n, m)]
+        lam = (2 * np.pi * m / LY) ** 2 + (2 * np.pi * n / LY) ** 2
+    elif case == "uy_of_x":                      # u_y = A sin(kx x), kx = 3: the real (0, 0) line
+        q = 3
+        u[1, 0, 0, :] = AMP * np.sin(2 * np.pi * q * x / LY)
+        modes = [(1, 0, 0)]
+        lam = 4 * np.sin(np.pi * q / s.nx) ** 2 / DX ** 2
+    elif case == "uy_of_xz":                     # u_y = A sin(kx x + kz z), kx = 5, kz = 2: a complex x line
+        q, n = 5, 2
+        e = -0.5j * AMP * np.exp(2j * np.pi * q * x / LY)
+        u[1, n, 0, :] = e
+        u[1, s.mz - n, 0, :] = np.conj(e)
+        modes = [(1, n, 0), (1, s.mz - n, 0)]
+        lam = 4 * np.sin(np.pi * q / s.nx) ** 2 / DX ** 2 + (2 * np.pi * n / LY) ** 2
+    else:
+        raise ValueError(case)
+    st["u"] = u
+    s.set_state(st)
+    return modes, lam
+
+
+@pytest.mark.parametrize("rk3", [False, True], ids=["ab2", "rk3"])
+@pytest.mark.parametrize("scheme", ["upwind", "center"])
+@pytest.mark.parametrize("case", ["ux_of_y", "ux_of_yz", "uy_of_x", "uy_of_xz"])
+def test_shear_wave_decays_by_the_crank_nicolson_factor(case, scheme, rk3):
+    s = _solver(scheme, rk3)
+    try:
+        modes, lam = _wave(s, case)
+        prev = s.get_state()["u"]
+        for _ in range(4):
+            s.step()
+            st = s.get_state()
+            g = 1.0
+            for c1, c2 in (RK3_STAGES if rk3 else AB2_STAGES):
+                g *= (1 - c2 * NU * st["dt"] * lam) / (1 + c1 * NU * st["dt"] * lam)
+            u = st["u"]
+            for (c, k, j) in modes:
+                line, line0 = u[c, k, j, :], prev[c, k, j, :]
+                # relative to the line, with a floor at the initial amplitude's
+                # rounding level for modes that decay by 10x per step
+                tol = 1e-12 * np.abs(line0).max() + 1e-15 * AMP
+                np.testing.assert_allclose(line, g * line0, rtol=0, atol=tol)
+            rest = np.abs(u).copy()
+            for (c, k, j) in modes:
+                rest[c, k, j, :] = 0
+            assert rest.max() <= 1e-14 * AMP
+            assert np.abs(st["p"]).max() <= 1e-14 * AMP
+            assert np.all(st["umean"] == 0)
+            prev = u
+    finally:
+        s.close()
