@@ -15,6 +15,18 @@ and z, the three-point second difference in x).  These tests pin the
 oracle's time integration, viscous line solves and projection against that
 closed form, independently of the reference's outputs; the engine is held
 to the oracle by the GPU parity tests.
+
+With a uniform mean flow U along x (held by the zero mean pressure
+gradient) the wave u_y = A sin(kx x) is also advected: with the centred x
+flux the conservative nonlinear term is N = i U sin(kx dx) / dx per mode,
+and each stage maps the mode amplitude a as
+
+    a_k = ((1 - c2 nu dt lam) a_{k-1} - dt (c3 N(a_{k-1}) + c4 N(a_{k-2})))
+          / (1 + c1 nu dt lam)
+
+(coef(rks, 3:4) of the same table; the old nonlinear term of the first
+stage is zero), which pins the flux form, its sign and the AB2 / RK3
+explicit coefficients.
 """
 import os
 import sys
@@ -112,5 +124,55 @@ def test_shear_wave_decays_by_the_crank_nicolson_factor(case, scheme, rk3):
             assert np.abs(st["p"]).max() <= 1e-14 * AMP
             assert np.all(st["umean"] == 0)
             prev = u
+    finally:
+        s.close()
+
+
+AB2_NL = [(1.5, -0.5)]
+RK3_NL = [(8.0 / 15.0, 0.0), (5.0 / 12.0, -17.0 / 60.0), (3.0 / 4.0, -5.0 / 12.0)]
+
+
+@pytest.mark.parametrize("rk3", [False, True], ids=["ab2", "rk3"])
+def test_advected_wave_follows_the_centred_flux_recurrence(rk3):
+    s = _solver("center", rk3)
+    try:
+        U, q = 0.3, 3
+        kx = 2 * np.pi * q / LY
+        st = s.get_state()
+        u = np.zeros_like(st["u"])
+        x = np.arange(s.nx + 1) * DX
+        u[1, 0, 0, :] = AMP * np.sin(kx * x)
+        st["u"] = u
+        st["umean"] = np.array([U, 0.0, 0.0])
+        s.set_state(st)
+        lam = 4 * np.sin(kx * DX / 2) ** 2 / DX ** 2
+        sym = 1j * U * np.sin(kx * DX) / DX
+        phase = np.exp(1j * kx * x)
+
+        def amp(line):                               # line = Re(a e^{i kx x}) up to rounding
+            return 2 * np.sum(line[:-1] * np.conj(phase[:-1])) / s.nx
+
+        a_old, a = 0.0, amp(s.get_state()["u"][1, 0, 0, :])
+        for _ in range(4):
+            for rks, ((c1, c2), (c3, c4)) in enumerate(zip(RK3_STAGES if rk3 else AB2_STAGES,
+                                                           RK3_NL if rk3 else AB2_NL), start=1):
+                if rk3:
+                    s.step_rks(rks)
+                else:
+                    s.step()
+                st = s.get_state()
+                # the dt the stage used: RK3 computes the new dt at its last
+                # stage and uses it there (the first step's stages 1-2 run at
+                # the initial dt)
+                dt = st["dt"]
+                pred = ((1 - c2 * NU * dt * lam) * a - dt * (c3 * sym * a + c4 * sym * a_old)) / (1 + c1 * NU * dt * lam)
+                line = st["u"][1, 0, 0, :]
+                np.testing.assert_allclose(line, (pred * phase).real, rtol=0, atol=1e-14 * AMP)
+                a_old, a = a, amp(line)
+                rest = np.abs(st["u"]).copy()
+                rest[1, 0, 0, :] = 0
+                assert rest.max() <= 1e-14 * AMP
+                assert np.abs(st["p"]).max() <= 1e-14 * AMP
+                assert np.array_equal(st["umean"], [U, 0.0, 0.0])
     finally:
         s.close()
