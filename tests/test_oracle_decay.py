@@ -217,3 +217,35 @@ def test_projection_removes_the_divergence_of_a_random_field(scheme, rk3):
             assert rep["divmax"] == pytest.approx(d, rel=1e-12, abs=1e-30)
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("rk3", [False, True], ids=["ab2", "rk3"])
+def test_fixed_mean_pressure_gradient_accelerates_the_mean_flow(rk3):
+    """No spheres, fluid at rest, SET_MPG with mpg = (g, 0, 0): every stage
+    adds -mpg * dt to the mean flow (steptheflow.F90:98, frmean = 0) and
+    the fluctuation stays zero.  The reference applies that update in every
+    velstep call with the full dt, so a three-stage RK3 step moves the mean
+    by 3 g dt while t advances by dt; the restatement keeps it."""
+    g = 0.02
+    prm = config.default_params()
+    prm.update(my=MY, lybyd=LY, dbydx=MY / LY, re=1.0, vis=NU, cfl=0.2, cfl_max=0.5, discr_scheme="upwind",
+               initialize_zero=True, dobnd=False, ramp_frac_steps=0, set_mpg=True, mpg=(g, 0.0, 0.0), rk3=rk3)
+    parts = config.Particles(np.zeros((0, 3)))
+    s = oc.OracleSolver(config.make_params(prm), parts.struct)
+    try:
+        expect = 0.0
+        for _ in range(4):
+            for rks in range(1, 4 if rk3 else 2):
+                if rk3:
+                    s.step_rks(rks)
+                else:
+                    s.step()
+                st = s.get_state()
+                expect -= g * st["dt"]
+                assert st["mpg"][0] == g
+                assert np.abs(st["u"]).max() == 0.0 and np.abs(st["p"]).max() == 0.0
+                assert st["umean"][0] == pytest.approx(expect, rel=1e-14)
+                assert st["umean"][1] == 0.0 and st["umean"][2] == 0.0
+        assert st["umean"][0] == pytest.approx(-g * st["t"] * (3 if rk3 else 1), rel=1e-13)
+    finally:
+        s.close()
