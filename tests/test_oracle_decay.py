@@ -18,15 +18,17 @@ closed form, independently of the reference's outputs; the engine is held
 to the oracle by the GPU parity tests.
 
 With a uniform mean flow U along x (held by the zero mean pressure
-gradient) the wave u_y = A sin(kx x) is also advected: with the centred x
-flux the conservative nonlinear term is N = i U sin(kx dx) / dx per mode,
-and each stage maps the mode amplitude a as
+gradient) the wave u_y = A sin(kx x) is also advected.  The conservative
+nonlinear term is then linear, N = S a per mode, S = i U sin(kx dx) / dx
+for the centred x flux and U (1 + i sin(kx dx) / 2)(1 - exp(-i kx dx)) / dx
+(U > 0; mirrored for U < 0) for the upwind one without a limiter, and each
+stage maps the mode amplitude a as
 
     a_k = ((1 - c2 nu dt lam) a_{k-1} - dt (c3 N(a_{k-1}) + c4 N(a_{k-2})))
           / (1 + c1 nu dt lam)
 
 (coef(rks, 3:4) of the same table; the old nonlinear term of the first
-stage is zero), which pins the flux form, its sign and the AB2 / RK3
+stage is zero), which pins both flux forms, their sign and the AB2 / RK3
 explicit coefficients.
 """
 import os
@@ -133,11 +135,25 @@ AB2_NL = [(1.5, -0.5)]
 RK3_NL = [(8.0 / 15.0, 0.0), (5.0 / 12.0, -17.0 / 60.0), (3.0 / 4.0, -5.0 / 12.0)]
 
 
+def _flux_symbol(scheme, U, theta):
+    """Per-mode symbol of the x flux divergence of u_x * v for uniform u_x = U
+    (form_nl, nl_allflow.F90:71-327): centred, F(i+1/2) - F(i-1/2) with
+    F(i) = U v(i) over 2 dx; upwind without a limiter, the face states
+    v(i) +- (v(i+1) - v(i-1)) / 4 with the Rusanov dissipation |U| / 2 times
+    their jump, i.e. full upwinding of the centred-slope reconstruction."""
+    if scheme == "center":
+        return 1j * U * np.sin(theta) / DX
+    if U > 0:
+        return U * (1 + 0.5j * np.sin(theta)) * (1 - np.exp(-1j * theta)) / DX
+    return U * (1 - 0.5j * np.sin(theta)) * (np.exp(1j * theta) - 1) / DX
+
+
 @pytest.mark.parametrize("rk3", [False, True], ids=["ab2", "rk3"])
-def test_advected_wave_follows_the_centred_flux_recurrence(rk3):
-    s = _solver("center", rk3)
+@pytest.mark.parametrize("scheme,U", [("center", 0.3), ("center", -0.3), ("upwind", 0.3), ("upwind", -0.3)])
+def test_advected_wave_follows_the_flux_recurrence(scheme, U, rk3):
+    s = _solver(scheme, rk3)
     try:
-        U, q = 0.3, 3
+        q = 3
         kx = 2 * np.pi * q / LY
         st = s.get_state()
         u = np.zeros_like(st["u"])
@@ -147,7 +163,7 @@ def test_advected_wave_follows_the_centred_flux_recurrence(rk3):
         st["umean"] = np.array([U, 0.0, 0.0])
         s.set_state(st)
         lam = 4 * np.sin(kx * DX / 2) ** 2 / DX ** 2
-        sym = 1j * U * np.sin(kx * DX) / DX
+        sym = _flux_symbol(scheme, U, kx * DX)
         phase = np.exp(1j * kx * x)
 
         def amp(line):                               # line = Re(a e^{i kx x}) up to rounding
