@@ -265,3 +265,53 @@ def test_fixed_mean_pressure_gradient_accelerates_the_mean_flow(rk3):
         assert st["umean"][0] == pytest.approx(-g * st["t"] * (3 if rk3 else 1), rel=1e-13)
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("rk3", [False, True], ids=["ab2", "rk3"])
+@pytest.mark.parametrize("direction", ["y", "z"])
+def test_spectral_advection_of_a_shear_wave(direction, rk3):
+    """Mean flow along y (u_z = A sin(ky y)) or z (u_x = A sin(kz z)): the
+    nonlinear term is the spectral derivative of the product with the mean,
+    S = i ky V (or i kz W) per mode (nonlinear, nl.F90:63-205), and the
+    modes follow the same stage recurrence as the x-advected wave."""
+    s = _solver("upwind", rk3)
+    try:
+        V, m = 0.25, 2
+        st = s.get_state()
+        u = np.zeros_like(st["u"])
+        if direction == "y":
+            st["umean"] = np.array([0.0, V, 0.0])
+            u[2, 0, m, :] = -0.5j * AMP
+            k = 2 * np.pi * m / LY
+            modes = [((2, 0, m), 1j * k * V)]
+        else:
+            st["umean"] = np.array([0.0, 0.0, V])
+            u[0, m, 0, :] = -0.5j * AMP
+            u[0, s.mz - m, 0, :] = 0.5j * AMP
+            k = 2 * np.pi * m / LY
+            modes = [((0, m, 0), 1j * k * V), ((0, s.mz - m, 0), -1j * k * V)]
+        st["u"] = u
+        s.set_state(st)
+        lam = k ** 2
+        amp = {idx: (0.0, u[idx][0]) for idx, _ in modes}
+        for _ in range(4):
+            for rks, ((c1, c2), (c3, c4)) in enumerate(zip(RK3_STAGES if rk3 else AB2_STAGES,
+                                                           RK3_NL if rk3 else AB2_NL), start=1):
+                if rk3:
+                    s.step_rks(rks)
+                else:
+                    s.step()
+                st = s.get_state()
+                dt = st["dt"]
+                rest = np.abs(st["u"]).copy()
+                for idx, sym in modes:
+                    a_old, a = amp[idx]
+                    pred = ((1 - c2 * NU * dt * lam) * a - dt * (c3 * sym * a + c4 * sym * a_old)) / (1 + c1 * NU * dt * lam)
+                    line = st["u"][idx]
+                    np.testing.assert_allclose(line, pred, rtol=0, atol=1e-14 * AMP)
+                    amp[idx] = (a, line[0])
+                    rest[idx] = 0
+                assert rest.max() <= 1e-14 * AMP
+                assert np.abs(st["p"]).max() <= 1e-14 * AMP
+    finally:
+        s.close()
