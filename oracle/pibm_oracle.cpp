@@ -9,8 +9,13 @@
 // Parity status: the reference cannot be built here (no Fortran compiler, FFTW
 // ships only as prebuilt archives), so the step itself is "parity unpinned"
 // against reference outputs.  The plane FFT conventions are pinned against
-// numpy (tests/golden), and every routine below cites the reference lines it
-// restates.  Reference paths are relative to the project root
+// numpy (tests/golden); the time integration, the viscous and scalar line
+// solves, both x fluxes, the spectral nonlinear products and the projection
+// against closed-form shear-wave solutions (tests/test_oracle_decay.py,
+// tests/test_oracle_scalar.py); the immersed-boundary set-up and forcing
+// against whole-cell translation across the periodic boundaries
+// (tests/test_oracle_invariance.py).  Every routine below cites the reference
+// lines it restates.  Reference paths are relative to the project root
 // PUReIBM_PS2D-FD1D/.
 //
 // Summation order: global sums that the reference accumulates in a single
