@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -46,19 +47,21 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if not force and not _stale(LIB, deps):
         build_main()
         return LIB
-    objs = []
+    jobs = []
     for src in CU_SOURCES:
         obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
-        cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
-               *CU_FLAGS.get(src, []), "-Xptxas", "-v" if verbose else "-O3", "-c", os.path.join(CSRC, src), "-o", obj]
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        jobs.append((obj, [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+                           *CU_FLAGS.get(src, []), "-Xptxas", "-v" if verbose else "-O3", "-c",
+                           os.path.join(CSRC, src), "-o", obj]))
     for src in CPP_SOURCES:
         obj = os.path.join(OUT_DIR, src.replace(".cpp", ".o"))
-        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I/usr/local/cuda/include", "-c",
-               os.path.join(CSRC, src), "-o", obj]
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        jobs.append((obj, ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I/usr/local/cuda/include",
+                           "-c", os.path.join(CSRC, src), "-o", obj]))
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(subprocess.run, cmd, check=True) for _, cmd in jobs]:
+            f.result()
+    objs = [obj for obj, _ in jobs]
     tmp = LIB + ".tmp"
     subprocess.run([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)
