@@ -1,5 +1,6 @@
 """Closed-form checks of the oracle step with no spheres: exact viscous
-decay and advection of shear waves, and the projection of a random field.
+decay and advection (along x, y and z) of shear waves, the projection of a
+random field, and the mean flow under a fixed mean pressure gradient.
 
 With no spheres and the mean pressure gradient held at zero, a velocity
 field with one component that does not vary along its own direction
